@@ -1,0 +1,164 @@
+/*
+ * vrt.h -- C ABI of libvrt.so, the B200 (sm_100a) volumetric path-integration
+ * library.  This is the drop-in boundary for rendervous's volume hot path: the
+ * Python map classes in rendervous_b200/ lower a map graph to the plain
+ * structs below and call these entry points through cffi.
+ *
+ * Conventions
+ *   - Every pointer argument that names tensor data is a DEVICE pointer of the
+ *     current CUDA device; `stream` is a cudaStream_t (NULL = legacy stream).
+ *   - Every call is asynchronous on `stream` and returns a status code
+ *     (VRT_OK == 0).  Argument errors are reported before any launch; device
+ *     side failures (an iteration cap hit, a non-finite value) are recorded in
+ *     the context and returned by vrt_context_sync().
+ *   - Gradient outputs ACCUMULATE into the grad buffers named in the structs
+ *     (the reference binds and accumulates into `param.grad`,
+ *     rendervous _maps.py:1049-1058); the library never zeroes them.
+ *   - Random numbers: draw k of path p is word (k & 3) of
+ *     Philox-4x32-10(key = seed, counter = {k >> 2, p_lo, stream, p_hi}), so a
+ *     call with the same seed regenerates the same paths.
+ *   - A context serialises nothing: use one context per stream.
+ */
+#ifndef VRT_H
+#define VRT_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+/* CDEF-BEGIN */
+enum {
+    VRT_OK = 0,
+    VRT_E_INVALID_ARGUMENT = 1,
+    VRT_E_NULL_POINTER = 2,
+    VRT_E_BAD_SHAPE = 3,
+    VRT_E_ITER_CAP = 4,
+    VRT_E_NONFINITE = 5,
+    VRT_E_CUDA = 6,
+    VRT_E_UNSUPPORTED = 7
+};
+
+/* Transmittance estimators (the transmittance sub-maps of the reference). */
+enum {
+    VRT_TR_RATIO_TRACKING = 0,  /* RatiotrackingTransmittance, include/vr_transmittance_RT.h */
+    VRT_TR_DELTA_TRACKING = 1,  /* DeltatrackingTransmittance, include/vr_transmittance_DT.h */
+    VRT_TR_DDA_MIDPOINT = 2,    /* GridDDATransmittance, include/vr_transmittance_DDA.h */
+    VRT_TR_DDA_EXACT = 3        /* DDA with the exact per-cell trilinear integral (no reference) */
+};
+/* Path-integrator forward passes. */
+enum { VRT_PI_NEE = 0, VRT_PI_DT = 1 };
+/* Path-replay adjoints. */
+enum { VRT_BW_NEE_DS = 0, VRT_BW_DT = 1, VRT_BW_NEE_DRT = 2 };
+
+/* A node-centred FP32 grid, the Grid3D parameter (rendervous _maps.py:2319-2365).
+   Element (z,y,x,c) is data[z*strides[0] + y*strides[1] + x*strides[2] + c]; the
+   channel stride must be 1.  grad uses the same strides and may be NULL. */
+typedef struct vrt_grid {
+    const float* data;
+    float* grad;
+    int32_t shape[4];    /* D, H, W, C */
+    int64_t strides[4];  /* element strides of D, H, W, C */
+} vrt_grid;
+
+/* A lowered medium: the sub-maps a path integrator binds
+   (rendervous _maps.py:2924-3022) reduced to the forms this library runs. */
+typedef struct vrt_medium {
+    vrt_grid sigma;                  /* Grid3D, C == 1 */
+    float bmin[3], bmax[3];          /* Grid3D box */
+    float inv_bsize[3];              /* 1/(bmax-bmin), float32 */
+    float box_min[3], box_max[3];    /* RayBoxIntersection boundary */
+    int32_t albedo_is_grid;          /* 0: albedo_const, 1: albedo grid (C 1 or 3, Grid3D box) */
+    vrt_grid albedo;
+    float albedo_const[3];
+    float emission[3];               /* constant emission */
+    float env[3];                    /* constant environment radiance */
+    int32_t has_sun;                 /* directional light (no reference counterpart) */
+    float sun_dir[3];                /* unit direction towards the light */
+    float sun_radiance[3];
+    int32_t phase_mode;              /* 0 Henyey-Greenstein, 1 HGPhase + VHGPhaseSampler (reference) */
+    float phase_g;
+    int32_t majorant_mode;           /* 0 constant [max, 1e6] (reference), 1 majorant grid */
+    float global_majorant;
+    const float* maj_grid;           /* [Mz, My, Mx] from vrt_majorant_build */
+    int32_t maj_dims[3];             /* Mx, My, Mz */
+    float maj_scale[3];              /* inv_bsize * (shape-1) / brick */
+    int32_t transmittance_mode;      /* VRT_TR_* used for NEE shadow rays */
+    int32_t max_bounces;             /* 0 = uncapped, as the reference */
+    float ds_epsilon;                /* defensive-sampling epsilon of the DS / DT adjoints */
+    int32_t ds_compat;               /* 1: reference replay majorant of NEE_DS bw */
+} vrt_medium;
+
+/* PerspectiveCameraSensor (rendervous _maps.py:1765-1802). */
+typedef struct vrt_camera {
+    const float* poses;              /* [views, 9]: origin, direction, up */
+    int32_t views, height, width;
+    float fov, znear;
+    int32_t jittered;
+} vrt_camera;
+
+typedef struct vrt_counters {
+    int64_t paths;                   /* paths started */
+    int64_t vertices;                /* real scattering collisions */
+    int64_t steps;                   /* tracking steps (free-flight samples), primary and shadow */
+    int64_t status;                  /* device error bits (VRT_E_* as 1 << code) */
+} vrt_counters;
+
+typedef struct vrt_context vrt_context;
+
+/* Context: device scratch for work queues, counters and the error word
+   (replaces the reference's global pipeline caches, _maps.py:35-66). */
+int vrt_context_create(int32_t device, vrt_context** out);
+int vrt_context_destroy(vrt_context* ctx);
+/* Waits for `stream`, copies the counters and error word out, and clears them.
+   Returns VRT_OK or the first device-side error. */
+int vrt_context_sync(vrt_context* ctx, void* stream, vrt_counters* out);
+const char* vrt_status_string(int32_t status);
+int32_t vrt_version(void);
+
+/* RayBoxIntersection forward (rendervous _maps.py:4128-4154, include/maths.h:28-38):
+   rays [n,6] -> out [n,2] = (tMin, tMax). */
+int vrt_ray_box(const float* rays, int64_t n, const float bmin[3], const float bmax[3], float* out, void* stream);
+
+/* Grid3D forward / backward (include/maps/grid3d.h:6-75): x [n,3] -> out [n,C];
+   backward accumulates dL/dgrid into g->grad. */
+int vrt_grid3d_fw(const vrt_grid* g, const float bmin[3], const float inv_bsize[3], const float* x, int64_t n,
+                  float* out, void* stream);
+int vrt_grid3d_bw(const vrt_grid* g, const float bmin[3], const float inv_bsize[3], const float* x,
+                  const float* dout, int64_t n, void* stream);
+
+/* Majorant grid of brick^3-cell bricks over sigma (the reference's only majorant
+   is the constant of _objects.py:96-101).  With out == NULL only dims_out
+   (Mx, My, Mz) is written. */
+int vrt_majorant_build(const vrt_grid* sigma, int32_t brick, float* out, int32_t dims_out[3], void* stream);
+
+/* Transmittance map forward / backward on rays [n,6] -> T [n]
+   (GridDDATransmittance _maps.py:2640-2667, RatiotrackingTransmittance
+   _maps.py:2670-2682, DeltatrackingTransmittance _maps.py:2685-2697).
+   Backward accumulates dL/dsigma into medium->sigma.grad. */
+int vrt_transmittance_fw(vrt_context* ctx, const vrt_medium* m, int32_t mode, const float* rays, int64_t n,
+                         uint64_t seed, float* T, void* stream);
+int vrt_transmittance_bw(vrt_context* ctx, const vrt_medium* m, int32_t mode, const float* rays, int64_t n,
+                         uint64_t seed, const float* dL_dT, void* stream);
+
+/* Path integrator as a map on rays [n,6] -> R [n,3] (DeltatrackingPathIntegrator,
+   DeltatrackingNEEPathIntegrator, DRTPathIntegrator, _maps.py:2886-3022; path i
+   uses Philox path id i).  Backward accumulates into sigma.grad and albedo.grad. */
+int vrt_radiance_fw(vrt_context* ctx, const vrt_medium* m, int32_t integrator, const float* rays, int64_t n,
+                    uint64_t seed, float* R, void* stream);
+int vrt_radiance_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const float* rays, int64_t n,
+                    uint64_t seed, const float* dL_dR, void* stream);
+
+/* Camera capture (SensorsBase.capture, _maps.py:1741-1749, capture kernels
+   _maps.py:509-746): rgb [views,H,W,3] = mean over spp paths; sample s of pixel p
+   is Philox path id s*npix + p.  Backward replays the same paths with
+   dL/drgb / spp and accumulates into the medium's grad buffers. */
+int vrt_capture_fw(vrt_context* ctx, const vrt_medium* m, int32_t integrator, const vrt_camera* cam, int32_t spp,
+                   uint64_t seed, float* rgb, void* stream);
+int vrt_capture_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const vrt_camera* cam, int32_t spp,
+                   uint64_t seed, const float* dL_drgb, void* stream);
+/* CDEF-END */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,34 @@
+// vrt_internal.h -- host-side declarations shared by the libvrt translation units.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "vrt_params.h"
+
+struct vrt_context {
+    int device;
+    int num_sms;
+    vrt::DScratch* scratch;  // device memory
+};
+
+namespace vrt {
+
+// Returns VRT_OK or VRT_E_CUDA after checking the launch.
+int launch_status(cudaError_t e);
+
+int persistent_blocks(const void* kernel, int block, int num_sms);
+
+int launch_transmittance_fw(const DMedium& M, int mode, const float* rays, int64_t n, uint64_t seed, float* T,
+                            DScratch* scratch, cudaStream_t stream);
+int launch_transmittance_bw(const DMedium& M, int mode, const float* rays, int64_t n, uint64_t seed,
+                            const float* dL_dT, DScratch* scratch, cudaStream_t stream);
+
+// out: rays mode writes R [n,3]; camera mode accumulates R * scale into out[pixel].
+int launch_radiance_fw(const DMedium& M, int integrator, const PathSrc& src, uint64_t n_paths, uint64_t seed,
+                       float* out, float scale, DScratch* scratch, int num_sms, cudaStream_t stream);
+// dL: rays mode dL[i]; camera mode dL[pixel] / div (div = spp, as the reference's
+// capture backward divides dL/dI by the sample count, _maps.py:707-708).
+int launch_radiance_bw(const DMedium& M, int bw_mode, const PathSrc& src, uint64_t n_paths, uint64_t seed,
+                       const float* dL, float div, DScratch* scratch, int num_sms, cudaStream_t stream);
+
+}  // namespace vrt

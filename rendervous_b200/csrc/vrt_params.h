@@ -1,0 +1,71 @@
+// vrt_params.h -- kernel-parameter forms of the C-ABI structs.
+//
+// The host validates a vrt_medium / vrt_camera once per call and converts it
+// to these POD structs, which are passed by value (they live in the kernel's
+// constant bank, so every lane reads them as uniform values).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vrt {
+
+struct DGrid {
+    const float* data;
+    float* grad;
+    int D, H, W, C;
+    int sD, sH, sW;  // element strides (channel stride is 1)
+};
+
+struct DMedium {
+    DGrid sigma;
+    DGrid albedo;
+    float3 bmin, bmax, inv_bsize;
+    float3 box_min, box_max;
+    int albedo_is_grid;
+    float3 albedo_const, emission, env;
+    int has_sun;
+    float3 sun_dir, sun_L;
+    int phase_mode;
+    float g;
+    int maj_mode;
+    float gmaj;
+    const float* maj;
+    int Mx, My, Mz;
+    float3 maj_scale;
+    int tr_mode;
+    int max_bounces;
+    float ds_eps;
+    int ds_compat;
+};
+
+struct DCamera {
+    const float* poses;
+    int views, height, width;
+    float fov, znear;
+    int jittered;
+};
+
+// Device scratch owned by a context.
+struct DScratch {
+    unsigned long long next_path;  // persistent-kernel work queue
+    unsigned long long paths;
+    unsigned long long vertices;
+    unsigned long long steps;
+    unsigned int status;           // 1 << VRT_E_* bits
+    unsigned int pad;
+};
+
+}  // namespace vrt
+
+namespace vrt {
+
+// Source of primary rays for the path kernels: a camera (capture) or an array
+// of rays [n, 6] (a path integrator evaluated as a map).
+struct PathSrc {
+    int is_camera;
+    DCamera cam;
+    long long npix;        // views * height * width (camera)
+    const float* rays;     // [n, 6] (rays)
+};
+
+}  // namespace vrt

@@ -1,0 +1,798 @@
+// vrt_path.cu -- path integrators on sm_100a: forward passes and path-replay adjoints.
+//
+// Forward NEE integrator (include/vr_path_integrator_NEE.h:1-66) as a
+// persistent state machine.  Every lane owns one path; one loop iteration
+// performs ONE free-flight step of whatever segment the lane is in (the primary
+// delta-tracking segment or a ratio/delta-tracking shadow segment), so the
+// expensive part -- the sigma gather -- is executed by the whole warp together,
+// and only the cheap event handling (collision, end of shadow ray, phase
+// sampling) diverges.  When a lane's path ends, the warp refills all dead
+// lanes at once from a global queue: one atomicAdd per warp per refill, ranks
+// from a ballot.  Each lane consumes its path's Philox stream in exactly the
+// order of the sequential definition, so results are independent of the
+// schedule.
+//
+// The adjoints (NEE_DS, DT, NEE_DRT) replay each path from its Philox stream
+// (path i re-derives every draw from (seed, i)), as the reference does from
+// saved seeds, and scatter dL/dsigma and dL/dalbedo with atomics.
+#include <cuda_runtime.h>
+
+#include "vrt_device.cuh"
+#include "vrt_internal.h"
+#include "vrt_tracking.cuh"
+
+namespace vrt {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kPathStepCap = 1 << 26;  // total free-flight steps per path before VRT_E_ITER_CAP
+
+__device__ __forceinline__ void primary_ray(const PathSrc& S, uint64_t pid, Rng& rng, float3& x, float3& w,
+                                            long long& oidx) {
+    if (S.is_camera) {
+        long long p = (long long)(pid % (uint64_t)S.npix);
+        long long hw = (long long)S.cam.height * S.cam.width;
+        int view = (int)(p / hw);
+        int rem = (int)(p - (long long)view * hw);
+        camera_ray(S.cam, view, rem / S.cam.width, rem % S.cam.width, rng, x, w);
+        oidx = p;
+    } else {
+        x = ld3(S.rays + 6 * pid);
+        w = ld3(S.rays + 6 * pid + 3);
+        oidx = (long long)pid;
+    }
+}
+
+__device__ __forceinline__ void warp_add_counters(DScratch* sc, uint32_t paths, uint32_t verts, uint32_t steps) {
+    unsigned long long p = paths, v = verts, s = steps;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        p += __shfl_down_sync(kFull, p, o);
+        v += __shfl_down_sync(kFull, v, o);
+        s += __shfl_down_sync(kFull, s, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&sc->paths, p);
+        atomicAdd(&sc->vertices, v);
+        atomicAdd(&sc->steps, s);
+    }
+}
+
+// ------------------------------------------------------------------------
+// Forward NEE: persistent state machine.
+// ------------------------------------------------------------------------
+enum : int { ST_DEAD = 0, ST_PRIMARY = 1, ST_SHADOW = 2 };
+enum : int { SH_DIRECT = 0, SH_ENV = 1, SH_SUN = 2 };
+enum : int { EV_NONE = 0, EV_COLLISION = 1, EV_ESCAPE = 2, EV_SHADOW_DONE = 3 };
+
+struct NeeLane {
+    Rng rng;
+    float3 x, w, W, R;
+    float d;
+    int bounces;
+    float3 sx, sw;  // shadow segment position / direction
+    float sd, T;
+    float3 pay;     // radiance carried by the shadow ray
+    float payph;    // phase value for it
+    int kind;
+    int state;
+    long long oidx;
+    uint32_t steps_path;
+};
+
+// Begin a transmittance segment from x0 along dir (the transmittance map's own
+// boundary test, vr_transmittance_RT.h:5-10 / _DT.h:3-8).  DDA segments are
+// deterministic and evaluated inline.
+__device__ __forceinline__ int start_shadow(const DMedium& M, NeeLane& L, float3 x0, float3 dir, uint32_t& steps) {
+    L.state = ST_SHADOW;
+    L.T = 1.0f;
+    if (M.tr_mode >= 2) {
+        L.T = M.tr_mode == 2 ? transmittance_dda<false>(M, x0, dir, steps) : transmittance_dda<true>(M, x0, dir, steps);
+        return EV_SHADOW_DONE;
+    }
+    float tMin, tMax;
+    if (!boundary(M, x0, dir, tMin, tMax)) return EV_SHADOW_DONE;
+    L.sx = x0 + dir * tMin;
+    L.sw = dir;
+    L.sd = tMax - tMin;
+    return EV_NONE;
+}
+
+// vr_path_integrator_NEE.h:57-62 plus the optional bounce cap
+__device__ __forceinline__ int after_nee(const DMedium& M, NeeLane& L) {
+    if (M.max_bounces > 0 && ++L.bounces >= M.max_bounces) return EV_ESCAPE;
+    float3 wo = phase_sample(M, L.rng, L.w);
+    L.W = L.W * 1.0f;
+    if (all_less(L.W, 0.00001f)) return EV_ESCAPE;
+    L.w = wo;
+    float tMin;
+    boundary(M, L.x, L.w, tMin, L.d);
+    L.state = ST_PRIMARY;
+    return L.d > 0.00001f ? EV_NONE : EV_ESCAPE;
+}
+
+__global__ void __launch_bounds__(256) k_nee_fw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, float* out,
+                                                 float scale, DScratch* sc) {
+    const unsigned lane = threadIdx.x & 31u;
+    const float EPS = 0.00001f;
+    NeeLane L;
+    L.state = ST_DEAD;
+    bool exhausted = false;
+    uint32_t n_paths_done = 0, n_verts = 0, n_steps = 0;
+
+    while (true) {
+        // ---- refill dead lanes from the global queue (one atomic per warp)
+        unsigned want = __ballot_sync(kFull, L.state == ST_DEAD && !exhausted);
+        if (want) {
+            int leader = __ffs(want) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(&sc->next_path, (unsigned long long)__popc(want));
+            base = __shfl_sync(kFull, base, leader);
+            if (L.state == ST_DEAD && !exhausted) {
+                uint64_t pid = base + __popc(want & ((1u << lane) - 1u));
+                if (pid >= n_paths) {
+                    exhausted = true;
+                } else {
+                    // path_integrator_NEE prologue (vr_path_integrator_NEE.h:3-14)
+                    L.rng.init(seed, pid, 0);
+                    float3 x0, w0;
+                    primary_ray(S, pid, L.rng, x0, w0, L.oidx);
+                    float tMin, tMax;
+                    boundary(M, x0, w0, tMin, tMax);
+                    L.x = x0 + w0 * tMin;
+                    L.w = w0;
+                    L.d = tMax - tMin;
+                    L.W = f3(1.0f);
+                    L.R = f3(0.0f);
+                    L.bounces = 0;
+                    L.steps_path = 0;
+                    L.kind = SH_DIRECT;
+                    ++n_paths_done;
+                    int ev = start_shadow(M, L, L.x, L.w, n_steps);
+                    if (ev == EV_SHADOW_DONE) {
+                        L.R = L.R + L.T * M.env;
+                        L.state = L.d > EPS ? ST_PRIMARY : ST_DEAD;
+                        if (L.state == ST_DEAD) {
+                            if (S.is_camera) {
+                                atomicAdd(out + 3 * L.oidx + 0, L.R.x * scale);
+                                atomicAdd(out + 3 * L.oidx + 1, L.R.y * scale);
+                                atomicAdd(out + 3 * L.oidx + 2, L.R.z * scale);
+                            } else {
+                                out[3 * L.oidx + 0] = L.R.x;
+                                out[3 * L.oidx + 1] = L.R.y;
+                                out[3 * L.oidx + 2] = L.R.z;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if (__all_sync(kFull, L.state == ST_DEAD && exhausted)) break;
+        if (L.state == ST_DEAD) continue;
+
+        // ---- one free-flight step of the current segment
+        const bool prim = L.state == ST_PRIMARY;
+        float3 p = prim ? L.x : L.sx;
+        float3 v = prim ? L.w : L.sw;
+        float md;
+        float mj = majorant(M, p, v, md);
+        float lg = -logf(1.0f - L.rng.uniform());
+        ++n_steps;
+        int ev = EV_NONE;
+        bool need_sigma = false;
+        float m = 0.0f, t = 0.0f;
+        if (prim) {  // vr_path_integrator_NEE.h:20-33
+            m = gmax(EPS, mj);
+            t = lg / m;
+            L.x = L.x + L.w * gmin(t, md);
+            if (t > md) {
+                L.d -= md;
+                if (!(L.d > EPS)) ev = EV_ESCAPE;
+            } else if (t > L.d) {
+                ev = EV_ESCAPE;
+            } else {
+                need_sigma = true;
+            }
+        } else if (M.tr_mode == 0) {  // vr_transmittance_RT.h:15-25
+            m = gmax(0.0000001f, mj);
+            t = lg / m;
+            if (md < L.sd && t > md) {
+                L.sx = L.sx + L.sw * md;
+                L.sd -= md;
+            } else {
+                float dt = gmin(t, gmin(L.sd, md));
+                L.sx = L.sx + L.sw * dt;
+                L.sd -= dt;
+                if (L.sd <= 0.0000001f) ev = EV_SHADOW_DONE;
+                else need_sigma = true;
+            }
+        } else {  // vr_transmittance_DT.h:10-26
+            m = gmax(0.0000001f, mj);
+            float dt = lg / m;
+            float tt = gmin(md, dt);
+            L.sx = L.sx + L.sw * tt;
+            L.sd -= tt;
+            if (!(dt > md)) {
+                if (L.sd <= 0.0000001f) ev = EV_SHADOW_DONE;
+                else need_sigma = true;
+            }
+        }
+        if (need_sigma) {
+            float s = sigma(M, prim ? L.x : L.sx);
+            if (prim) {
+                if (L.rng.uniform() >= s / m) {
+                    L.d -= t;
+                    if (!(L.d > EPS)) ev = EV_ESCAPE;
+                } else {
+                    ev = EV_COLLISION;
+                }
+            } else if (M.tr_mode == 0) {
+                L.T *= (1.0f - s / m);
+                if (L.T < 0.01f) {
+                    if (L.rng.uniform() < 1.0f - L.T) { L.T = 0.0f; ev = EV_SHADOW_DONE; }
+                    else L.T = 1.0f;
+                }
+            } else {
+                if (L.rng.uniform() < s / m) { L.T = 0.0f; ev = EV_SHADOW_DONE; }
+            }
+        }
+        if (++L.steps_path > (uint32_t)kPathStepCap) {
+            raise_status(&sc->status, 4);
+            ev = EV_ESCAPE;
+        }
+
+        // ---- events (divergent, cheap)
+        while (ev != EV_NONE) {
+            if (ev == EV_COLLISION) {  // vr_path_integrator_NEE.h:41-50
+                ++n_verts;
+                float3 sa = albedo(M, L.x);
+                L.R = L.R + L.W * (f3(1.0f) - sa) * M.emission;
+                L.W = L.W * sa;
+                float3 wnee;
+                L.pay = environment_sample(M, L.rng, wnee);
+                L.payph = phase(M, L.w, wnee);
+                L.kind = SH_ENV;
+                ev = start_shadow(M, L, L.x, wnee, n_steps);
+            } else if (ev == EV_SHADOW_DONE) {
+                if (L.kind == SH_DIRECT) {  // vr_path_integrator_NEE.h:13-14
+                    L.R = L.R + L.T * M.env;
+                    L.state = ST_PRIMARY;
+                    ev = L.d > EPS ? EV_NONE : EV_ESCAPE;
+                } else if (L.kind == SH_ENV) {  // :51-52
+                    L.R = L.R + L.W * L.T * L.pay * L.payph;
+                    if (M.has_sun) {
+                        L.pay = M.sun_L;
+                        L.payph = phase(M, L.w, M.sun_dir);
+                        L.kind = SH_SUN;
+                        ev = start_shadow(M, L, L.x, M.sun_dir, n_steps);
+                    } else {
+                        ev = after_nee(M, L);
+                    }
+                } else {
+                    L.R = L.R + L.W * L.T * L.pay * L.payph;
+                    ev = after_nee(M, L);
+                }
+            } else {  // EV_ESCAPE: the path's estimate is complete
+                if (S.is_camera) {
+                    atomicAdd(out + 3 * L.oidx + 0, L.R.x * scale);
+                    atomicAdd(out + 3 * L.oidx + 1, L.R.y * scale);
+                    atomicAdd(out + 3 * L.oidx + 2, L.R.z * scale);
+                } else {
+                    out[3 * L.oidx + 0] = L.R.x;
+                    out[3 * L.oidx + 1] = L.R.y;
+                    out[3 * L.oidx + 2] = L.R.z;
+                }
+                L.state = ST_DEAD;
+                ev = EV_NONE;
+            }
+        }
+    }
+    warp_add_counters(sc, n_paths_done, n_verts, n_steps);
+}
+
+// ------------------------------------------------------------------------
+// Sequential forms (one path per thread), used by the adjoints.
+// ------------------------------------------------------------------------
+
+// vr_path_integrator_NEE.h:1-66 (+ directional light, bounce cap)
+__device__ float3 path_nee_seq(const DMedium& M, Rng& rng, float3 x, float3 w, bool only_scatters, uint32_t& verts,
+                               uint32_t& steps, uint32_t* status) {
+    float tMin, tMax;
+    boundary(M, x, w, tMin, tMax);
+    x = x + w * tMin;
+    float d = tMax - tMin;
+    float3 R = f3(0.0f), W = f3(1.0f);
+    if (!only_scatters) R = R + transmittance(M, rng, x, w, steps, status) * M.env;
+    const float EPS = 0.00001f;
+    int bounces = 0;
+    for (int it = 0; d > EPS; ++it) {
+        if (it >= kPathStepCap) { raise_status(status, 4); break; }
+        float md;
+        float m = gmax(EPS, majorant(M, x, w, md));
+        float t = -logf(1.0f - rng.uniform()) / m;
+        ++steps;
+        x = x + w * gmin(t, md);
+        if (t > md) { d -= md; continue; }
+        if (t > d) break;
+        float s = sigma(M, x);
+        if (rng.uniform() >= s / m) { d -= t; continue; }
+        ++verts;
+        float3 sa = albedo(M, x);
+        R = R + W * (f3(1.0f) - sa) * M.emission;
+        W = W * sa;
+        float3 wnee;
+        float3 env = environment_sample(M, rng, wnee);
+        float T_nee = transmittance(M, rng, x, wnee, steps, status);
+        R = R + W * T_nee * env * phase(M, w, wnee);
+        if (M.has_sun) {
+            float T_sun = transmittance(M, rng, x, M.sun_dir, steps, status);
+            R = R + W * T_sun * M.sun_L * phase(M, w, M.sun_dir);
+        }
+        if (M.max_bounces > 0 && ++bounces >= M.max_bounces) return R;
+        float3 wo = phase_sample(M, rng, w);
+        if (all_less(W, EPS)) return R;
+        w = wo;
+        boundary(M, x, w, tMin, d);
+    }
+    return R;
+}
+
+// vr_path_integrator_DT.h:7-57
+__device__ float3 path_dt_seq(const DMedium& M, Rng& rng, float3 x, float3 w, uint32_t& verts, uint32_t& steps,
+                              uint32_t* status) {
+    float tMin, tMax;
+    boundary(M, x, w, tMin, tMax);
+    x = x + w * tMin;
+    float d = tMax - tMin;
+    float3 R = f3(0.0f), W = f3(1.0f);
+    int bounces = 0;
+    for (int it = 0; d > 0.00000001f; ++it) {
+        if (it >= kPathStepCap) { raise_status(status, 4); break; }
+        float md;
+        float m = gmax(0.00000001f, majorant(M, x, w, md));
+        float t = -logf(1.0f - rng.uniform()) / m;
+        ++steps;
+        x = x + w * gmin(t, md);
+        if (t > md) { d -= md; continue; }
+        if (t > d) break;
+        float s = sigma(M, x);
+        if (rng.uniform() >= s / m) { d -= t; continue; }
+        ++verts;
+        float3 sa = albedo(M, x);
+        R = R + W * (f3(1.0f) - sa) * M.emission;
+        W = W * sa;
+        float3 wo = phase_sample(M, rng, w);
+        if (all_less(W, 0.0000001f)) return R;
+        if (M.max_bounces > 0 && ++bounces >= M.max_bounces) return R;
+        w = wo;
+        boundary(M, x, w, tMin, d);
+    }
+    return W * M.env + R;
+}
+
+// vr_path_integrator_DT.h:59-235
+__device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float eps, float3 dL_dR, uint32_t* status) {
+    const uint32_t before_path = rng.n;
+    const float3 ini_x = x, ini_w = w;
+    float tMin, tMax;
+    boundary(M, x, w, tMin, tMax);
+    x = x + w * tMin;
+    float d = tMax - tMin;
+    const float EPS = 0.00000001f;
+    float3 W = f3(1.0f);
+    float null_W = 1.0f;
+    int bounces = 0;
+    for (int it = 0; d > EPS; ++it) {
+        if (it >= kPathStepCap) { raise_status(status, 4); return; }
+        float md;
+        float m = gmax(EPS, majorant(M, x, w, md) + 2.0f * eps);
+        float t = -logf(1.0f - rng.uniform()) / m;
+        x = x + w * gmin(t, md);
+        if (t > md) { d -= md; continue; }
+        if (t > d) break;
+        float s = sigma(M, x);
+        float Pc = (s + eps) / m;
+        if (rng.uniform() >= Pc) { d -= t; W = W * ((1.0f - s / m) / (1.0f - Pc)); continue; }
+        if (s == 0.0f) {
+            if (null_W == 0.0f) { W = f3(0.0f); break; }
+            null_W = 0.0f;
+        } else {
+            W = W * ((s / m) / Pc);
+        }
+        float3 sa = albedo(M, x);
+        float3 wo = phase_sample(M, rng, w);
+        W = W * (sa * 1.0f);
+        if (all_less(W, EPS)) { W = f3(0.0f); break; }
+        if (M.max_bounces > 0 && ++bounces >= M.max_bounces) { W = f3(0.0f); break; }
+        w = wo;
+        boundary(M, x, w, tMin, d);
+    }
+    const float3 dL_dW = dL_dR * M.env;
+    rng.seek(before_path);
+    x = ini_x;
+    w = ini_w;
+    boundary(M, x, w, tMin, tMax);
+    x = x + w * tMin;
+    d = tMax - tMin;
+    const float3 W_out = W;
+    W = f3(1.0f);
+    bounces = 0;
+    for (int it = 0; d > EPS; ++it) {
+        if (it >= kPathStepCap) { raise_status(status, 4); return; }
+        float md;
+        float m = gmax(EPS, majorant(M, x, w, md) + 2.0f * eps);
+        float t = -logf(1.0f - rng.uniform()) / m;
+        x = x + w * gmin(t, md);
+        if (t > md) { d -= md; continue; }
+        if (t > d) break;
+        float s = sigma(M, x);
+        float Pc = (s + eps) / m;
+        if (rng.uniform() >= Pc) {
+            sigma_bw(M, x, dot(dL_dW, -W_out * null_W / m / (1.0f - s / m)));
+            W = W * ((1.0f - s / m) / (1.0f - Pc));
+            d -= t;
+            continue;
+        }
+        sigma_bw(M, x, dot(dL_dW, s == 0.0f ? W_out : W_out * null_W / s));
+        W = W * (s / m / Pc);
+        if (s == 0.0f) break;
+        float3 sa = albedo(M, x);
+        float3 wo = phase_sample(M, rng, w);
+        W = W * sa;
+        if (all_less(W, EPS)) return;
+        if (M.max_bounces > 0 && ++bounces >= M.max_bounces) return;
+        w = wo;
+        boundary(M, x, w, tMin, d);
+    }
+}
+
+// vr_path_integrator_NEE_DS.h:6-206.  ds_compat selects the reference's
+// replay majorant (x1.2 + 2 eps, different from its primal + 2 eps + 0.1);
+// otherwise the replay uses the primal majorant and retraces the primal path.
+__device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float eps, float3 dL_dR,
+                               uint32_t* status) {
+    const uint32_t before_path = rng.n;
+    const float3 ini_x = x, ini_w = w;
+    float tMin, tMax;
+    boundary(M, x, w, tMin, tMax);
+    x = x + w * tMin;
+    float d = tMax - tMin;
+    float3 R = f3(0.0f), R_after_sp = f3(0.0f), W = f3(1.0f);
+    float null_W = 1.0f;
+    const float EPS = 0.00000001f;
+    bool scattered = false;
+    int bounces = 0;
+    uint32_t steps = 0;
+    for (int it = 0; d > EPS; ++it) {
+        if (it >= kPathStepCap) { raise_status(status, 4); return; }
+        float md;
+        float m = gmax(EPS, majorant(M, x, w, md) + 2.0f * eps + 0.1f);
+        float t = -logf(1.0f - rng.uniform()) / m;
+        x = x + w * gmin(t, md);
+        if (t > md) { d -= md; continue; }
+        if (t > d) break;
+        float s = sigma(M, x);
+        float Pc = (s + eps) / m;
+        if (rng.uniform() >= Pc) { d -= t; W = W * ((1.0f - s / m) / (1.0f - Pc)); continue; }
+        scattered = true;
+        if (s < EPS) {
+            if (null_W < EPS) { W = f3(0.0f); break; }
+            null_W = 0.0f;
+        } else {
+            W = W * ((s / m) / Pc);
+        }
+        float3 sa = albedo(M, x);
+        float3 added_R = W * (f3(1.0f) - sa) * M.emission;
+        W = W * sa;
+        float3 wnee;
+        float3 env = environment_sample(M, rng, wnee);
+        float T_nee = transmittance(M, rng, x, wnee, steps, status);
+        float ph_nee = phase(M, w, wnee);
+        added_R = added_R + W * T_nee * env * ph_nee;
+        if (M.has_sun) {
+            float T_sun = transmittance(M, rng, x, M.sun_dir, steps, status);
+            added_R = added_R + W * T_sun * M.sun_L * phase(M, w, M.sun_dir);
+        }
+        if (null_W < EPS) R_after_sp = R_after_sp + added_R;
+        else R = R + added_R;
+        if (M.max_bounces > 0 && ++bounces >= M.max_bounces) { W = f3(0.0f); break; }
+        float3 wo = phase_sample(M, rng, w);
+        if (all_less(W, EPS)) { W = f3(0.0f); break; }
+        w = wo;
+        boundary(M, x, w, tMin, d);
+    }
+    if (!scattered) R = R + M.env * W;
+
+    rng.seek(before_path);
+    x = ini_x;
+    w = ini_w;
+    W = f3(1.0f);
+    boundary(M, x, w, tMin, tMax);
+    x = x + w * tMin;
+    d = tMax - tMin;
+    bounces = 0;
+    for (int it = 0; d > EPS; ++it) {
+        if (it >= kPathStepCap) { raise_status(status, 4); return; }
+        float md;
+        float mj = majorant(M, x, w, md);
+        float m = M.ds_compat ? gmax(EPS, mj * 1.2f + 2.0f * eps) : gmax(EPS, mj + 2.0f * eps + 0.1f);
+        float t = -logf(1.0f - rng.uniform()) / m;
+        x = x + w * gmin(t, md);
+        if (t > md) { d -= md; continue; }
+        if (t > d) break;
+        float s = sigma(M, x);
+        float Pc = (s + eps) / m;
+        if (rng.uniform() >= Pc) {
+            sigma_bw(M, x, dot(dL_dR, -R / m / (1.0f - s / m)));
+            W = W * ((1.0f - s / m) / (1.0f - Pc));
+            d -= t;
+            continue;
+        }
+        sigma_bw(M, x, dot(dL_dR, s < EPS ? R_after_sp / eps : R / s));
+        W = W * (s / m / Pc);
+        if (s < EPS) return;
+        float3 sa = albedo(M, x);
+        float3 dL_dsa = dL_dR * W * -1.0f * M.emission;
+        R = R - W * (f3(1.0f) - sa) * M.emission;
+        dL_dsa = dL_dsa + dL_dR * R / make_float3(gmax(EPS, sa.x), gmax(EPS, sa.y), gmax(EPS, sa.z));
+        float3 wnee;
+        float3 env = environment_sample(M, rng, wnee);
+        const uint32_t before_tr = rng.n;
+        float T_nee = transmittance(M, rng, x, wnee, steps, status);
+        float ph_nee = phase(M, w, wnee);
+        const uint32_t before_sun = rng.n;
+        float T_sun = 0.0f, ph_sun = 0.0f;
+        if (M.has_sun) {
+            T_sun = transmittance(M, rng, x, M.sun_dir, steps, status);
+            ph_sun = phase(M, w, M.sun_dir);
+        }
+        float3 wo = phase_sample(M, rng, w);
+        const uint32_t before_next = rng.n;
+        W = W * sa;
+        float dL_dTnee = dot(dL_dR, W * env * ph_nee);
+        R = R - W * T_nee * env * ph_nee;
+        float dL_dTsun = 0.0f;
+        if (M.has_sun) {
+            dL_dTsun = dot(dL_dR, W * M.sun_L * ph_sun);
+            R = R - W * T_sun * M.sun_L * ph_sun;
+        }
+        albedo_bw(M, x, dL_dsa);
+        rng.seek(before_tr);
+        transmittance_bw(M, rng, x, wnee, dL_dTnee, status);
+        if (M.has_sun) {
+            rng.seek(before_sun);
+            transmittance_bw(M, rng, x, M.sun_dir, dL_dTsun, status);
+        }
+        rng.seek(before_next);
+        if (M.max_bounces > 0 && ++bounces >= M.max_bounces) return;
+        if (all_less(W, EPS)) return;
+        w = wo;
+        boundary(M, x, w, tMin, d);
+    }
+}
+
+// vr_path_integrator_NEE_DRT.h:8-60 sample_transmittance_position (majorant
+// queried at the sample point x + w t)
+__device__ float sample_transmittance_position(const DMedium& M, Rng& rng, float3 x, float3 w, float d, float& sample_t,
+                                               float& weight_t, uint32_t* status) {
+    float Tr = 1.0f, t = 0.0f, res_t = 0.0f, res_dt = 0.0f, C = 0.0f;
+    const float EPS = 0.0000001f;
+    int it = 0;
+    for (; it < kStepCap; ++it) {
+        float md;
+        float m = gmax(EPS, majorant(M, x + w * t, w, md));
+        float dt = gmin(-logf(1.0f - rng.uniform()) / m, gmin(md, d - t));
+        float w_step = Tr * dt;
+        C += w_step;
+        if (rng.uniform() < w_step / C) { res_t = t; res_dt = dt; }
+        t += dt;
+        if (dt >= md - EPS) continue;
+        if (t >= d - EPS) break;
+        Tr *= 1.0f - sigma(M, x + w * t) / m;
+    }
+    if (it == kStepCap) raise_status(status, 4);
+    weight_t = C;
+    sample_t = res_t + rng.uniform() * res_dt;
+    return Tr;
+}
+
+// vr_path_integrator_NEE_DRT.h:62-270.  The branch seed is Philox stream 1.
+__device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float3 dL_dR, uint32_t* status) {
+    float tMin, tMax;
+    boundary(M, x, w, tMin, tMax);
+    x = x + w * tMin;
+    float d = tMax - tMin;
+    if (d <= 0.0f) return;
+    Rng sec;
+    sec.k0 = rng.k0; sec.k1 = rng.k1; sec.plo = rng.plo; sec.phi = rng.phi;
+    sec.stream = rng.stream + 1;
+    sec.n = 0;
+    uint32_t steps = 0, verts = 0;
+    (void)transmittance(M, rng, x, w, steps, status);
+    transmittance_bw(M, sec, x, w, dot(dL_dR, M.env), status);
+    float3 R = f3(0.0f), W = f3(1.0f);
+    float3 res_x = x, res_w = w, res_W = W;
+    float res_P = 3.0f, total_weight = 3.0f;
+    const float3 ini_x = x, ini_w = w;
+    const float ini_d = d;
+    const float EPS = 0.00000001f;
+    const uint32_t before_path = rng.n;
+    int bounces = 0;
+    for (int it = 0; d > EPS; ++it) {
+        if (it >= kPathStepCap) { raise_status(status, 4); return; }
+        float md;
+        float m = majorant(M, x, w, md) * 1.05f + 0.1f;
+        float t = -logf(1.0f - rng.uniform()) / m;
+        x = x + w * gmin(t, md);
+        if (t > md) { d -= md; continue; }
+        if (t > d) break;
+        float s = sigma(M, x);
+        if (rng.uniform() >= s / m) { d -= t; continue; }
+        float3 sa = albedo(M, x);
+        W = W * sa;
+        float3 wnee;
+        float3 env = environment_sample(M, rng, wnee);
+        float T_nee = transmittance(M, rng, x, wnee, steps, status);
+        float ph_nee = phase(M, w, wnee);
+        R = R + W * T_nee * env * ph_nee;
+        if (M.has_sun) {
+            float T_sun = transmittance(M, rng, x, M.sun_dir, steps, status);
+            R = R + W * T_sun * M.sun_L * phase(M, w, M.sun_dir);
+        }
+        bool capped = M.max_bounces > 0 && ++bounces >= M.max_bounces;
+        float3 wo = phase_sample(M, rng, w);
+        w = wo;
+        boundary(M, x, w, tMin, d);
+        float current_P = W.x + W.y + W.z;
+        total_weight += current_P;
+        if (rng.uniform() < current_P / total_weight) {
+            res_P = current_P; res_W = W; res_x = x; res_w = w;
+        }
+        if (all_less(W, EPS) || capped) break;
+    }
+    W = f3(1.0f);
+    x = ini_x;
+    w = ini_w;
+    d = ini_d;
+    rng.seek(before_path);
+    bounces = 0;
+    for (int it = 0; d > EPS; ++it) {
+        if (it >= kPathStepCap) { raise_status(status, 4); return; }
+        float md;
+        float m = majorant(M, x, w, md) * 1.05f + 0.1f;
+        float t = -logf(1.0f - rng.uniform()) / m;
+        x = x + w * gmin(t, md);
+        if (t > md) { d -= md; continue; }
+        if (t > d) break;
+        float s = sigma(M, x);
+        if (rng.uniform() >= s / m) {
+            sigma_bw(M, x, dot(dL_dR, -R / m / (1.0f - s / m)));
+            d -= t;
+            continue;
+        }
+        float mis_Ts = s * s / (1.0f + s * s);
+        float dL_dsigma = dot(dL_dR, mis_Ts * R / s);
+        float3 sa = albedo(M, x);
+        W = W * sa;
+        float3 wnee;
+        float3 env = environment_sample(M, rng, wnee);
+        float T_nee = transmittance(M, rng, x, wnee, steps, status);
+        float ph_nee = phase(M, w, wnee);
+        float T_sun = 0.0f, ph_sun = 0.0f;
+        if (M.has_sun) {
+            T_sun = transmittance(M, rng, x, M.sun_dir, steps, status);
+            ph_sun = phase(M, w, M.sun_dir);
+        }
+        bool capped = M.max_bounces > 0 && ++bounces >= M.max_bounces;
+        float3 wo = phase_sample(M, rng, w);
+        float dL_dTnee = dot(dL_dR, W * env * ph_nee);
+        R = R - W * T_nee * env * ph_nee;
+        float dL_dTsun = 0.0f;
+        if (M.has_sun) {
+            dL_dTsun = dot(dL_dR, W * M.sun_L * ph_sun);
+            R = R - W * T_sun * M.sun_L * ph_sun;
+        }
+        sigma_bw(M, x, dL_dsigma);
+        transmittance_bw(M, sec, x, wnee, dL_dTnee, status);
+        if (M.has_sun) transmittance_bw(M, sec, x, M.sun_dir, dL_dTsun, status);
+        w = wo;
+        boundary(M, x, w, tMin, d);
+        rng.advance();
+        if (all_less(W, EPS) || capped) break;
+    }
+    boundary(M, res_x, res_w, tMin, d);
+    float s_t, weight_t;
+    sample_transmittance_position(M, rng, res_x, res_w, d, s_t, weight_t, status);
+    float3 xs = res_x + res_w * s_t;
+    float3 ls_dir;
+    float3 Ls_env = environment_sample(M, rng, ls_dir);
+    float3 Ls = transmittance(M, rng, xs, ls_dir, steps, status) * Ls_env * phase(M, res_w, ls_dir);
+    if (M.has_sun) Ls = Ls + transmittance(M, rng, xs, M.sun_dir, steps, status) * M.sun_L * phase(M, res_w, M.sun_dir);
+    float3 ws = phase_sample(M, rng, res_w);
+    Ls = Ls + 1.0f * path_nee_seq(M, rng, xs, ws, true, verts, steps, status);
+    Ls = Ls * res_W * weight_t * albedo(M, xs);
+    float sigma_xs = sigma(M, xs);
+    float mis_T = 1.0f / (1.0f + sigma_xs * sigma_xs);
+    sigma_bw(M, xs, dot(dL_dR, Ls) * mis_T * total_weight / res_P);
+}
+
+// ------------------------------------------------------------------------
+// Kernels over paths (grid-stride, one path per thread at a time)
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_dt_fw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, float* out,
+                                                float scale, DScratch* sc) {
+    uint32_t paths = 0, verts = 0, steps = 0;
+    for (uint64_t pid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; pid < n_paths;
+         pid += (uint64_t)gridDim.x * blockDim.x) {
+        Rng rng;
+        rng.init(seed, pid, 0);
+        float3 x, w;
+        long long oidx;
+        primary_ray(S, pid, rng, x, w, oidx);
+        float3 R = path_dt_seq(M, rng, x, w, verts, steps, &sc->status);
+        ++paths;
+        if (S.is_camera) {
+            atomicAdd(out + 3 * oidx + 0, R.x * scale);
+            atomicAdd(out + 3 * oidx + 1, R.y * scale);
+            atomicAdd(out + 3 * oidx + 2, R.z * scale);
+        } else {
+            out[3 * oidx + 0] = R.x;
+            out[3 * oidx + 1] = R.y;
+            out[3 * oidx + 2] = R.z;
+        }
+    }
+    warp_add_counters(sc, paths, verts, steps);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_path_bw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, const float* dL,
+                                                  float div, DScratch* sc) {
+    uint32_t paths = 0;
+    for (uint64_t pid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; pid < n_paths;
+         pid += (uint64_t)gridDim.x * blockDim.x) {
+        Rng rng;
+        rng.init(seed, pid, 0);
+        float3 x, w;
+        long long oidx;
+        primary_ray(S, pid, rng, x, w, oidx);
+        float3 g = ld3(dL + 3 * oidx) / div;
+        ++paths;
+        if (MODE == 0) path_nee_ds_bw(M, rng, x, w, M.ds_eps, g, &sc->status);
+        else if (MODE == 1) path_dt_bw(M, rng, x, w, M.ds_eps, g, &sc->status);
+        else path_nee_drt_bw(M, rng, x, w, g, &sc->status);
+    }
+    warp_add_counters(sc, paths, 0, 0);
+}
+
+// ------------------------------------------------------------------------
+// Host launchers
+// ------------------------------------------------------------------------
+int launch_radiance_fw(const DMedium& M, int integrator, const PathSrc& src, uint64_t n_paths, uint64_t seed,
+                       float* out, float scale, DScratch* scratch, int num_sms, cudaStream_t stream) {
+    if (n_paths == 0) return 0;
+    if (integrator == 0) {
+        cudaError_t e = cudaMemsetAsync(&scratch->next_path, 0, sizeof(unsigned long long), stream);
+        if (e != cudaSuccess) return launch_status(e);
+        int blocks = persistent_blocks((const void*)k_nee_fw, 256, num_sms);
+        uint64_t need = (n_paths + 255) / 256;
+        if ((uint64_t)blocks > need) blocks = (int)need;
+        k_nee_fw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, scratch);
+    } else {
+        uint64_t need = (n_paths + 255) / 256;
+        int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
+        k_dt_fw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, scratch);
+    }
+    return launch_status(cudaGetLastError());
+}
+
+int launch_radiance_bw(const DMedium& M, int bw_mode, const PathSrc& src, uint64_t n_paths, uint64_t seed,
+                       const float* dL, float div, DScratch* scratch, int num_sms, cudaStream_t stream) {
+    if (n_paths == 0) return 0;
+    uint64_t need = (n_paths + 255) / 256;
+    int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
+    if (bw_mode == 0) k_path_bw<0><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
+    else if (bw_mode == 1) k_path_bw<1><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
+    else k_path_bw<2><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
+    return launch_status(cudaGetLastError());
+}
+
+}  // namespace vrt

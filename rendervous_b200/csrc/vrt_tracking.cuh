@@ -1,0 +1,417 @@
+// vrt_tracking.cuh -- transmittance estimators along one ray (sm_100a).
+//
+//   DDA   include/vr_transmittance_DDA.h:1-156 (midpoint rule of the reference,
+//         or the exact per-cell integral: two-point Gauss-Legendre is exact for
+//         the cubic a trilinear field becomes on a segment)
+//   RT    include/vr_transmittance_RT.h:1-141 (ratio tracking, RR at 0.01 / 0.1)
+//   DT    include/vr_transmittance_DT.h:1-90  (delta tracking)
+//
+// The DDA keeps the 8 corner values of the current cell in registers: a step
+// along axis a keeps the face the ray crosses into and loads only the 4 new
+// corners (the reference reloads all 8; the values are identical because the
+// clamped node indices coincide).  Its adjoint likewise carries the gradient
+// of the shared face and issues 4 atomic adds per cell instead of 8.
+#pragma once
+#include "vrt_device.cuh"
+
+namespace vrt {
+
+constexpr int kStepCap = 1 << 24;  // per-segment iteration bound (error VRT_E_ITER_CAP)
+
+struct DDA {
+    float3 x, w, alpha, alpha_inc, vn, vm;
+    int cx, cy, cz, sx, sy, sz, dimx, dimy, dimz;
+    float d;
+    float s[8];  // corner values, index dz*4 + dy*2 + dx
+
+    // vr_transmittance_DDA.h:3-36.  false when the ray misses (T = 1).
+    __device__ __forceinline__ bool init(const DMedium& M, float3 x0, float3 w0) {
+        float tMin, tMax;
+        if (!boundary(M, x0, w0, tMin, tMax)) return false;
+        float gMin, gMax;
+        if (!intersect_ray_box(x0, w0, M.bmin, M.bmax, gMin, gMax)) return false;
+        tMin = gmax(tMin, gMin);
+        tMax = gmin(tMax, gMax);
+        if (tMax <= tMin) return false;
+        w = w0;
+        x = x0 + w0 * tMin;
+        d = tMax - tMin;
+        dimx = M.sigma.W - 1; dimy = M.sigma.H - 1; dimz = M.sigma.D - 1;
+        float3 fdim = make_float3((float)dimx, (float)dimy, (float)dimz);
+        float3 box_size = M.bmax - M.bmin;
+        float3 cell_size = box_size / fdim;
+        float3 den = make_float3(gmax(0.000001f, fabsf(w.x)), gmax(0.000001f, fabsf(w.y)), gmax(0.000001f, fabsf(w.z)));
+        alpha_inc = cell_size / den;
+        sx = w.x > 0.0f ? 1 : (w.x < 0.0f ? -1 : 0);
+        sy = w.y > 0.0f ? 1 : (w.y < 0.0f ? -1 : 0);
+        sz = w.z > 0.0f ? 1 : (w.z < 0.0f ? -1 : 0);
+        vn = (x - M.bmin) * fdim / box_size;
+        vm = w * fdim / box_size;
+        reset(M);
+        return true;
+    }
+    // cell and alpha at the start of the segment (also used to replay it)
+    __device__ __forceinline__ void reset(const DMedium& M) {
+        float3 fdim = make_float3((float)dimx, (float)dimy, (float)dimz);
+        float3 box_size = M.bmax - M.bmin;
+        float3 cell_size = box_size / fdim;
+        cx = min(max((int)vn.x, 0), dimx - 1);
+        cy = min(max((int)vn.y, 0), dimy - 1);
+        cz = min(max((int)vn.z, 0), dimz - 1);
+        float3 corner = (make_float3((float)cx, (float)cy, (float)cz) + make_float3((float)sx, (float)sy, (float)sz) * 0.5f +
+                         f3(0.5f)) * cell_size + M.bmin;
+        float3 den = make_float3(gmax(0.000001f, fabsf(w.x)), gmax(0.000001f, fabsf(w.y)), gmax(0.000001f, fabsf(w.z)));
+        float3 cd = corner - x;
+        alpha = make_float3(fabsf(cd.x), fabsf(cd.y), fabsf(cd.z)) / den;
+    }
+    // vr_sigma_grid.h:1-7 sigma_at: node clamped to [0, dim]
+    __device__ __forceinline__ int node(const DGrid& g, int x_, int y_, int z_) const {
+        x_ = min(max(x_, 0), dimx); y_ = min(max(y_, 0), dimy); z_ = min(max(z_, 0), dimz);
+        return z_ * g.sD + y_ * g.sH + x_ * g.sW;
+    }
+    __device__ __forceinline__ void load_all(const DGrid& g) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s[k] = ldg(g.data + node(g, cx + (k & 1), cy + ((k >> 1) & 1), cz + (k >> 2)));
+    }
+    // vr_sigma_grid.h:18-27 interpolated_sigma
+    __device__ __forceinline__ float interp(float3 a) const {
+        return mixf(mixf(mixf(s[0], s[1], a.x), mixf(s[2], s[3], a.x), a.y),
+                    mixf(mixf(s[4], s[5], a.x), mixf(s[6], s[7], a.x), a.y), a.z);
+    }
+    __device__ __forceinline__ float3 ialpha(float t) const {
+        return (vm * t + vn) - make_float3((float)cx, (float)cy, (float)cz);
+    }
+    // vr_transmittance_DDA.h:48-55; returns the axis stepped (0,1,2)
+    __device__ __forceinline__ int advance_cell() {
+        if (alpha.x <= alpha.y && alpha.x <= alpha.z) { alpha.x += alpha_inc.x; cx += sx; return 0; }
+        if (alpha.x > alpha.y && alpha.y <= alpha.z) { alpha.y += alpha_inc.y; cy += sy; return 1; }
+        alpha.z += alpha_inc.z; cz += sz; return 2;
+    }
+    // After a step along `axis`, keep the face crossed into and load the other.
+    // Corner slots are compile-time constants in every branch so s[] stays in
+    // registers.  KEEP is the slot offset of the face the ray crossed into.
+    template <int KEEP>
+    __device__ __forceinline__ void shift_x(const DGrid& g) {
+#pragma unroll
+        for (int k = 0; k < 8; k += 2) {
+            s[k + 1 - KEEP] = s[k + KEEP];
+            s[k + KEEP] = ldg(g.data + node(g, cx + KEEP, cy + ((k >> 1) & 1), cz + (k >> 2)));
+        }
+    }
+    template <int KEEP>  // 0 or 2
+    __device__ __forceinline__ void shift_y(const DGrid& g) {
+#pragma unroll
+        for (int z = 0; z < 2; ++z)
+#pragma unroll
+            for (int xx = 0; xx < 2; ++xx) {
+                s[z * 4 + (2 - KEEP) + xx] = s[z * 4 + KEEP + xx];
+                s[z * 4 + KEEP + xx] = ldg(g.data + node(g, cx + xx, cy + (KEEP >> 1), cz + z));
+            }
+    }
+    template <int KEEP>  // 0 or 4
+    __device__ __forceinline__ void shift_z(const DGrid& g) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            s[(4 - KEEP) + k] = s[KEEP + k];
+            s[KEEP + k] = ldg(g.data + node(g, cx + (k & 1), cy + (k >> 1), cz + (KEEP >> 2)));
+        }
+    }
+    __device__ __forceinline__ void shift_load(const DGrid& g, int axis) {
+        if (axis == 0) {
+            if (sx > 0) shift_x<1>(g); else if (sx < 0) shift_x<0>(g);
+        } else if (axis == 1) {
+            if (sy > 0) shift_y<2>(g); else if (sy < 0) shift_y<0>(g);
+        } else {
+            if (sz > 0) shift_z<4>(g); else if (sz < 0) shift_z<0>(g);
+        }
+    }
+
+    static constexpr float kGL = 0.28867513459481288225f;  // 1 / (2 sqrt 3)
+
+    // tau over the segment; counts cells in *cells
+    template <bool EXACT>
+    __device__ __forceinline__ float tau(const DGrid& g, uint32_t& cells) {
+        float acc = 0.0f, ct = 0.0f;
+        load_all(g);
+        int it = 0;
+        while (ct < d - 0.0001f && it < kStepCap) {
+            float nt = gmin(d, gmin(alpha.x, gmin(alpha.y, alpha.z)));
+            float dt = nt - ct;
+            if (!EXACT) {
+                acc += interp(ialpha(mixf(ct, nt, 0.5f))) * dt;
+            } else {
+                float mid = mixf(ct, nt, 0.5f), h = dt * kGL;
+                acc += (interp(ialpha(mid - h)) + interp(ialpha(mid + h))) * (dt * 0.5f);
+            }
+            ct = nt;
+            int axis = advance_cell();
+            shift_load(g, axis);
+            ++cells;
+            ++it;
+        }
+        return acc;
+    }
+
+    // vr_sigma_grid.h:29-39 interpolated_sigma_bw, added into acc[8]
+    __device__ __forceinline__ static void add_weights(float3 a, float dL, float* acc) {
+        acc[0] += dL * (1.0f - a.x) * (1.0f - a.y) * (1.0f - a.z);
+        acc[1] += dL * (a.x) * (1.0f - a.y) * (1.0f - a.z);
+        acc[2] += dL * (1.0f - a.x) * (a.y) * (1.0f - a.z);
+        acc[3] += dL * (a.x) * (a.y) * (1.0f - a.z);
+        acc[4] += dL * (1.0f - a.x) * (1.0f - a.y) * (a.z);
+        acc[5] += dL * (a.x) * (1.0f - a.y) * (a.z);
+        acc[6] += dL * (1.0f - a.x) * (a.y) * (a.z);
+        acc[7] += dL * (a.x) * (a.y) * (a.z);
+    }
+    __device__ __forceinline__ void flush(const DGrid& g, float* acc, int k) const {
+        if (acc[k] != 0.0f) red_add(g.grad + node(g, cx + (k & 1), cy + ((k >> 1) & 1), cz + (k >> 2)), acc[k]);
+        acc[k] = 0.0f;
+    }
+    template <int KEEP>
+    __device__ __forceinline__ void carry_x(const DGrid& g, float* acc) const {
+#pragma unroll
+        for (int k = 0; k < 8; k += 2) { flush(g, acc, k + 1 - KEEP); acc[k + 1 - KEEP] = acc[k + KEEP]; acc[k + KEEP] = 0.0f; }
+    }
+    template <int KEEP>
+    __device__ __forceinline__ void carry_y(const DGrid& g, float* acc) const {
+#pragma unroll
+        for (int z = 0; z < 2; ++z)
+#pragma unroll
+            for (int xx = 0; xx < 2; ++xx) {
+                const int kf = z * 4 + (2 - KEEP) + xx, kk = z * 4 + KEEP + xx;
+                flush(g, acc, kf); acc[kf] = acc[kk]; acc[kk] = 0.0f;
+            }
+    }
+    template <int KEEP>
+    __device__ __forceinline__ void carry_z(const DGrid& g, float* acc) const {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { flush(g, acc, (4 - KEEP) + k); acc[(4 - KEEP) + k] = acc[KEEP + k]; acc[KEEP + k] = 0.0f; }
+    }
+    // vr_transmittance_DDA.h:121-153 second march: dL/dsigma per corner; the
+    // face shared with the next cell stays in registers.
+    template <bool EXACT>
+    __device__ __forceinline__ void scatter(const DGrid& g, float dL_dtau) {
+        float acc[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = 0.0f;
+        float ct = 0.0f;
+        int it = 0;
+        while (ct < d - 0.0001f && it < kStepCap) {
+            float nt = gmin(d, gmin(alpha.x, gmin(alpha.y, alpha.z)));
+            float dt = nt - ct;
+            if (!EXACT) {
+                add_weights(ialpha(mixf(ct, nt, 0.5f)), dL_dtau * dt, acc);
+            } else {
+                float mid = mixf(ct, nt, 0.5f), h = dt * kGL;
+                add_weights(ialpha(mid - h), dL_dtau * dt * 0.5f, acc);
+                add_weights(ialpha(mid + h), dL_dtau * dt * 0.5f, acc);
+            }
+            ct = nt;
+            // flush the face left behind, move the crossed face to its new slot
+            if (alpha.x <= alpha.y && alpha.x <= alpha.z) {
+                if (sx > 0) carry_x<1>(g, acc); else if (sx < 0) carry_x<0>(g, acc);
+                alpha.x += alpha_inc.x; cx += sx;
+            } else if (alpha.x > alpha.y && alpha.y <= alpha.z) {
+                if (sy > 0) carry_y<2>(g, acc); else if (sy < 0) carry_y<0>(g, acc);
+                alpha.y += alpha_inc.y; cy += sy;
+            } else {
+                if (sz > 0) carry_z<4>(g, acc); else if (sz < 0) carry_z<0>(g, acc);
+                alpha.z += alpha_inc.z; cz += sz;
+            }
+            ++it;
+        }
+        // acc now holds the corners of the cell the march stopped in (the face
+        // carried over from the last cell plus zeros): flush at these indices.
+#pragma unroll
+        for (int k = 0; k < 8; ++k) flush(g, acc, k);
+    }
+};
+
+template <bool EXACT>
+__device__ __forceinline__ float transmittance_dda(const DMedium& M, float3 x, float3 w, uint32_t& cells) {
+    DDA q;
+    if (!q.init(M, x, w)) return 1.0f;
+    return expf(-q.tau<EXACT>(M.sigma, cells));
+}
+template <bool EXACT>
+__device__ __forceinline__ void transmittance_dda_bw(const DMedium& M, float3 x, float3 w, float dL_dT) {
+    if (dL_dT == 0.0f || !M.sigma.grad) return;
+    DDA q;
+    if (!q.init(M, x, w)) return;
+    uint32_t cells = 0;
+    float tau = q.tau<EXACT>(M.sigma, cells);
+    float T = expf(-tau);
+    q.reset(M);
+    q.scatter<EXACT>(M.sigma, -dL_dT * T);
+}
+
+// vr_transmittance_RT.h:1-49.  The "grid crossing" branch restarts at a
+// majorant-brick face without a collision; it cannot trigger with the
+// constant majorant (distance 1e6).
+__device__ __forceinline__ float transmittance_rt(const DMedium& M, Rng& rng, float3 x, float3 w, uint32_t& steps,
+                                                  uint32_t* status) {
+    float T = 1.0f;
+    float tMin, tMax;
+    if (!boundary(M, x, w, tMin, tMax)) return T;
+    x = x + w * tMin;
+    float d = tMax - tMin;
+    for (int it = 0; it < kStepCap; ++it) {
+        float md;
+        float maj = gmax(0.0000001f, majorant(M, x, w, md));
+        float t = -logf(1.0f - rng.uniform()) / maj;
+        ++steps;
+        if (md < d && t > md) { x = x + w * md; d -= md; continue; }
+        float dt = gmin(t, gmin(d, md));
+        x = x + w * dt;
+        d -= dt;
+        if (d <= 0.0000001f) return T;
+        T *= (1.0f - sigma(M, x) / maj);
+        if (T < 0.01f) {
+            if (rng.uniform() < 1.0f - T) return 0.0f;
+            T = 1.0f;
+        }
+    }
+    raise_status(status, 4);
+    return T;
+}
+
+// vr_transmittance_RT.h:51-141
+__device__ __forceinline__ void transmittance_rt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float dL_dT,
+                                                    uint32_t* status) {
+    if (dL_dT == 0.0f) return;
+    float tMin, tMax;
+    if (!boundary(M, x, w, tMin, tMax)) return;
+    const float EPS = 0.0000001f;
+    float T = 1.0f;
+    x = x + w * tMin;
+    float d = tMax - tMin;
+    const float3 ini_x = x;
+    const float ini_d = d;
+    const uint32_t before = rng.n;
+    int it = 0;
+    for (; it < kStepCap; ++it) {
+        float md;
+        float maj = gmax(EPS, majorant(M, x, w, md) + 0.1f);
+        float t = -logf(1.0f - rng.uniform()) / maj;
+        if (md < d && t > md) { x = x + w * md; d -= md; continue; }
+        float dt = gmin(t, gmin(d, md));
+        x = x + w * dt;
+        d -= dt;
+        if (d <= EPS) break;
+        T *= (1.0f - sigma(M, x) / maj);
+        if (T < 0.1f) {
+            if (rng.uniform() < 1.0f - T) return;
+            T = 1.0f;
+        }
+    }
+    if (it == kStepCap) { raise_status(status, 4); return; }
+    const float out_T = T;
+    T = 1.0f;
+    rng.seek(before);
+    x = ini_x;
+    d = ini_d;
+    for (it = 0; it < kStepCap; ++it) {
+        float md;
+        float maj = gmax(EPS, majorant(M, x, w, md) + 0.1f);
+        float t = -logf(1.0f - rng.uniform()) / maj;
+        if (md < d && t > md) { x = x + w * md; d -= md; continue; }
+        float dt = gmin(t, gmin(d, md));
+        x = x + w * dt;
+        d -= dt;
+        if (d <= EPS) break;
+        float r = (1.0f - sigma(M, x) / maj);
+        T *= r;
+        sigma_bw(M, x, -out_T * dL_dT / maj / r);
+        if (T < 0.1f) {
+            rng.advance();
+            T = 1.0f;
+        }
+    }
+}
+
+// vr_transmittance_DT.h:1-28
+__device__ __forceinline__ float transmittance_dt(const DMedium& M, Rng& rng, float3 x, float3 w, uint32_t& steps,
+                                                  uint32_t* status) {
+    float tMin, tMax;
+    if (!boundary(M, x, w, tMin, tMax)) return 1.0f;
+    x = x + w * tMin;
+    float d = tMax - tMin;
+    for (int it = 0; it < kStepCap; ++it) {
+        float md;
+        float maj = gmax(0.0000001f, majorant(M, x, w, md));
+        float dt = -logf(1.0f - rng.uniform()) / maj;
+        float t = gmin(md, dt);
+        ++steps;
+        x = x + w * t;
+        d -= t;
+        if (dt > md) continue;
+        if (d <= 0.0000001f) return 1.0f;
+        if (rng.uniform() < sigma(M, x) / maj) return 0.0f;
+    }
+    raise_status(status, 4);
+    return 1.0f;
+}
+
+// vr_transmittance_DT.h:30-90
+__device__ __forceinline__ void transmittance_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float dL_dT,
+                                                    uint32_t* status) {
+    if (dL_dT == 0.0f) return;
+    float tMin, tMax;
+    if (!boundary(M, x, w, tMin, tMax)) return;
+    x = x + w * tMin;
+    float d = tMax - tMin;
+    const float3 ini_x = x;
+    const float ini_d = d;
+    const uint32_t before = rng.n;
+    int it = 0;
+    for (; it < kStepCap; ++it) {
+        float md;
+        float maj = gmax(0.0000001f, majorant(M, x, w, md) + 0.1f);
+        float dt = -logf(1.0f - rng.uniform()) / maj;
+        float t = gmin(md, dt);
+        x = x + w * t;
+        d -= t;
+        if (dt > md) continue;
+        if (d <= 0.0000001f) break;
+        if (rng.uniform() < sigma(M, x) / maj) return;
+    }
+    if (it == kStepCap) { raise_status(status, 4); return; }
+    x = ini_x;
+    d = ini_d;
+    rng.seek(before);
+    for (it = 0; it < kStepCap; ++it) {
+        float md;
+        float maj = gmax(0.0000001f, majorant(M, x, w, md) + 0.1f);
+        float dt = -logf(1.0f - rng.uniform()) / maj;
+        float t = gmin(md, dt);
+        x = x + w * t;
+        d -= t;
+        if (dt > md) continue;
+        if (d <= 0.0000001f) break;
+        rng.advance();
+        float Pc = sigma(M, x) / maj;
+        sigma_bw(M, x, -dL_dT / maj / (1.0f - Pc));
+    }
+}
+
+// include/vr_transmittance.h dispatch over the medium's transmittance map
+__device__ __forceinline__ float transmittance(const DMedium& M, Rng& rng, float3 x, float3 w, uint32_t& steps,
+                                               uint32_t* status) {
+    switch (M.tr_mode) {
+        case 0: return transmittance_rt(M, rng, x, w, steps, status);
+        case 1: return transmittance_dt(M, rng, x, w, steps, status);
+        case 2: return transmittance_dda<false>(M, x, w, steps);
+        default: return transmittance_dda<true>(M, x, w, steps);
+    }
+}
+__device__ __forceinline__ void transmittance_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float dL_dT,
+                                                 uint32_t* status) {
+    switch (M.tr_mode) {
+        case 0: transmittance_rt_bw(M, rng, x, w, dL_dT, status); break;
+        case 1: transmittance_dt_bw(M, rng, x, w, dL_dT, status); break;
+        case 2: transmittance_dda_bw<false>(M, x, w, dL_dT); break;
+        default: transmittance_dda_bw<true>(M, x, w, dL_dT); break;
+    }
+}
+
+}  // namespace vrt

@@ -1,0 +1,294 @@
+"""Lowering of a map graph to the plain medium description the C ABI consumes.
+
+The reference code-generates one GLSL super-kernel per map graph
+(rendervous _maps.py:211-291, 509-633).  Here the graph is recognised and
+reduced to the fixed forms the CUDA kernels implement (a vrt_medium struct):
+
+  sigma                Grid3D (C == 1)
+  scattering_albedo    const[...] or Grid3D (C 1 or 3, same box as sigma)
+  emission             const[...]
+  environment          const[...]
+  environment_sampler  _functionsampler(UniformDirectionSampler, const)
+  phase / sampler      HGPhase + VHGPhaseSampler (reference mixture),
+                       HenyeyGreensteinPhase + HenyeyGreensteinPhaseSampler,
+                       or const[1/4pi] with an isotropic sampler
+  boundary             RayBoxIntersection
+  majorant             const[[m, 1e6]] (reference) or MajorantGrid
+  transmittance        Ratiotracking / Deltatracking / GridDDA transmittance
+
+Anything else raises NotImplementedError -- there is no generic fallback.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import typing
+
+import numpy as np
+import torch
+
+from . import _lib
+
+TR_MODES = {"rt": 0, "dt": 1, "dda": 2, "dda_exact": 3}
+
+
+@dataclasses.dataclass
+class MediumDesc:
+    sigma: torch.Tensor                      # [D,H,W,1]
+    bmin: torch.Tensor
+    bmax: torch.Tensor
+    box_min: torch.Tensor
+    box_max: torch.Tensor
+    albedo_grid: typing.Optional[torch.Tensor] = None
+    albedo_const: tuple = (0.0, 0.0, 0.0)
+    emission: tuple = (0.0, 0.0, 0.0)
+    env: tuple = (0.0, 0.0, 0.0)
+    sun_dir: typing.Optional[tuple] = None
+    sun_radiance: tuple = (0.0, 0.0, 0.0)
+    phase_mode: int = 0
+    phase_g: float = 0.0
+    majorant_mode: int = 0
+    global_majorant: float = 0.0
+    maj_grid: typing.Optional[torch.Tensor] = None
+    maj_brick: int = 8
+    transmittance_mode: int = 0
+    max_bounces: int = 0
+    ds_epsilon: float = 0.1
+    ds_compat: int = 0
+
+    # -- derived quantities, computed in float32 exactly as the kernels read them
+    def inv_bsize(self) -> np.ndarray:
+        bmin = self.bmin.detach().cpu().to(torch.float32)
+        bmax = self.bmax.detach().cpu().to(torch.float32)
+        return (1.0 / (bmax - bmin)).numpy().astype(np.float32)
+
+    def maj_dims(self) -> tuple:
+        if self.maj_grid is None:
+            return (0, 0, 0)
+        d, h, w = self.maj_grid.shape
+        return (int(w), int(h), int(d))
+
+    def maj_scale(self) -> np.ndarray:
+        D, H, W = self.sigma.shape[:3]
+        ib = torch.from_numpy(self.inv_bsize())
+        dim = torch.tensor([W - 1, H - 1, D - 1], dtype=torch.float32)
+        return (ib * dim / float(self.maj_brick)).numpy().astype(np.float32)
+
+    def to_numpy(self) -> dict:
+        """Host copy for the CPU oracle (identical bytes)."""
+        f = lambda t: None if t is None else np.ascontiguousarray(t.detach().cpu().numpy().astype(np.float32))
+        v3 = lambda v: np.asarray(v, np.float32).reshape(3)
+        return dict(
+            sigma=f(self.sigma), bmin=v3(f(self.bmin)), bmax=v3(f(self.bmax)), inv_bsize=self.inv_bsize(),
+            box_min=v3(f(self.box_min)), box_max=v3(f(self.box_max)), albedo=f(self.albedo_grid),
+            albedo_const=v3(self.albedo_const), emission=v3(self.emission), env=v3(self.env),
+            has_sun=self.sun_dir is not None, sun_dir=v3(self.sun_dir if self.sun_dir is not None else (0, 0, 0)),
+            sun_radiance=v3(self.sun_radiance), phase_mode=self.phase_mode, phase_g=self.phase_g,
+            majorant_mode=self.majorant_mode, global_majorant=self.global_majorant,
+            maj_grid=f(self.maj_grid), maj_dims=self.maj_dims(), maj_scale=self.maj_scale(),
+            transmittance_mode=self.transmittance_mode, max_bounces=self.max_bounces,
+            ds_epsilon=self.ds_epsilon, ds_compat=self.ds_compat)
+
+    # -- the C struct (device pointers); keep the returned object alive during the call
+    def to_struct(self, sigma_grad: torch.Tensor | None = None, albedo_grad: torch.Tensor | None = None):
+        ffi, _ = _lib.ffi_lib()
+        m = ffi.new("vrt_medium *")
+        _fill_grid(m.sigma, self.sigma, sigma_grad)
+        for name, val in (("bmin", self.bmin), ("bmax", self.bmax), ("box_min", self.box_min),
+                          ("box_max", self.box_max)):
+            v = val.detach().cpu().to(torch.float32).reshape(3).tolist()
+            for i in range(3):
+                getattr(m, name)[i] = v[i]
+        ib = self.inv_bsize()
+        for i in range(3):
+            m.inv_bsize[i] = float(ib[i])
+            m.albedo_const[i] = float(self.albedo_const[i])
+            m.emission[i] = float(self.emission[i])
+            m.env[i] = float(self.env[i])
+            m.sun_radiance[i] = float(self.sun_radiance[i])
+            m.sun_dir[i] = float(self.sun_dir[i]) if self.sun_dir is not None else 0.0
+        m.has_sun = 1 if self.sun_dir is not None else 0
+        if self.albedo_grid is not None:
+            m.albedo_is_grid = 1
+            _fill_grid(m.albedo, self.albedo_grid, albedo_grad)
+        m.phase_mode = self.phase_mode
+        m.phase_g = float(self.phase_g)
+        m.majorant_mode = self.majorant_mode
+        m.global_majorant = float(self.global_majorant)
+        if self.maj_grid is not None:
+            m.maj_grid = _lib.fptr(self.maj_grid)
+            dims = self.maj_dims()
+            sc = self.maj_scale()
+            for i in range(3):
+                m.maj_dims[i] = dims[i]
+                m.maj_scale[i] = float(sc[i])
+        m.transmittance_mode = self.transmittance_mode
+        m.max_bounces = int(self.max_bounces)
+        m.ds_epsilon = float(self.ds_epsilon)
+        m.ds_compat = int(self.ds_compat)
+        return m
+
+
+def _fill_grid(g, t: torch.Tensor, grad: torch.Tensor | None):
+    if t.dim() != 4:
+        raise ValueError("grids are [D, H, W, C] tensors")
+    if t.dtype != torch.float32:
+        raise TypeError("grids are float32")
+    if not t.is_cuda:
+        raise ValueError("grid tensors must be CUDA tensors (there is no CPU path)")
+    if t.stride(3) != 1:
+        raise ValueError("grid channel stride must be 1")
+    g.data = _lib.fptr(t)
+    if grad is not None:
+        if grad.shape != t.shape or grad.stride() != t.stride():
+            raise ValueError("grad must match the grid's shape and strides")
+        g.grad = _lib.fptr(grad)
+    for i in range(4):
+        g.shape[i] = int(t.shape[i])
+        g.strides[i] = int(t.stride(i))
+
+
+def _const_values(m, n: int) -> tuple:
+    from . import maps
+    if not isinstance(m, maps.ConstantMap):
+        raise NotImplementedError(f"expected a constant map, got {type(m).__name__}")
+    v = m.value.detach().reshape(-1).cpu().tolist()
+    if len(v) == 1:
+        v = v * n
+    if len(v) != n:
+        raise NotImplementedError(f"constant of {len(v)} values where {n} are needed")
+    return tuple(float(a) for a in v)
+
+
+def _check_same_grid(a, b, what: str):
+    if a is not b and not (a.grid is b.grid):
+        raise NotImplementedError(f"{what} must use the integrator's sigma Grid3D")
+
+
+def lower_sigma(sigma, desc_kwargs: dict):
+    from . import maps
+    if not isinstance(sigma, maps.Grid3D):
+        raise NotImplementedError("sigma must be a Grid3D")
+    if sigma.grid.shape[-1] != 1:
+        raise NotImplementedError("sigma Grid3D must have one channel")
+    desc_kwargs.update(sigma=sigma.grid, bmin=sigma.bmin, bmax=sigma.bmax)
+
+
+def lower_boundary(boundary, desc_kwargs: dict):
+    from . import maps
+    if not isinstance(boundary, maps.RayBoxIntersection):
+        raise NotImplementedError("boundary must be a RayBoxIntersection")
+    desc_kwargs.update(box_min=boundary.box_min, box_max=boundary.box_max)
+
+
+def lower_majorant(majorant, sigma, desc_kwargs: dict):
+    from . import maps
+    if isinstance(majorant, maps.MajorantGrid):
+        _check_same_grid(majorant.sigma, sigma, "MajorantGrid")
+        desc_kwargs.update(majorant_mode=1, maj_grid=majorant.tensor(), maj_brick=majorant.brick,
+                           global_majorant=0.0)
+        return
+    v = _const_values(majorant, 2)
+    if v[1] < 1e5:
+        raise NotImplementedError("a constant majorant must have distance >= 1e5 (the reference uses 1e6)")
+    desc_kwargs.update(majorant_mode=0, global_majorant=v[0])
+
+
+def lower_transmittance(tr, sigma, desc_kwargs: dict):
+    from . import maps
+    if isinstance(tr, maps.GridDDATransmittance):
+        _check_same_grid(tr.grid_model, sigma, "GridDDATransmittance")
+        desc_kwargs["transmittance_mode"] = 3 if tr.exact else 2
+    elif isinstance(tr, maps.RatiotrackingTransmittance):
+        _check_same_grid(tr.sigma, sigma, "RatiotrackingTransmittance")
+        desc_kwargs["transmittance_mode"] = 0
+    elif isinstance(tr, maps.DeltatrackingTransmittance):
+        _check_same_grid(tr.sigma, sigma, "DeltatrackingTransmittance")
+        desc_kwargs["transmittance_mode"] = 1
+    else:
+        raise NotImplementedError(f"transmittance map {type(tr).__name__} is not supported")
+
+
+def lower_phase(phase, sampler, desc_kwargs: dict):
+    """Returns (phase_mode, g)."""
+    from . import maps
+    if isinstance(sampler, maps.VHGPhaseSampler):
+        g = _const_values(sampler.phase_g, 1)[0]
+        if isinstance(phase, maps.HGPhase):
+            gp = _const_values(phase.phase_g, 1)[0]
+            if gp != g:
+                raise NotImplementedError("phase and phase sampler disagree on g")
+            mode = 1
+        elif phase is None or isinstance(phase, maps.ConstantMap):
+            if phase is not None:
+                pv = _const_values(phase, 1)[0]
+                if abs(pv - 1.0 / (4 * math.pi)) > 1e-6:
+                    raise NotImplementedError("a constant phase must be isotropic (1/4pi)")
+            if abs(g) >= 0.001:
+                raise NotImplementedError("an isotropic phase needs g == 0 in its sampler")
+            mode = 0
+        else:
+            raise NotImplementedError(f"phase {type(phase).__name__} with VHGPhaseSampler")
+    elif isinstance(sampler, maps.HenyeyGreensteinPhaseSampler):
+        g = _const_values(sampler.phase_g, 1)[0]
+        if phase is not None and not isinstance(phase, maps.HenyeyGreensteinPhase):
+            raise NotImplementedError("HenyeyGreensteinPhaseSampler pairs with HenyeyGreensteinPhase")
+        if phase is not None and _const_values(phase.phase_g, 1)[0] != g:
+            raise NotImplementedError("phase and phase sampler disagree on g")
+        mode = 0
+    else:
+        raise NotImplementedError(f"phase sampler {type(sampler).__name__} is not supported")
+    desc_kwargs.update(phase_mode=mode, phase_g=g)
+
+
+def lower_integrator(pi) -> MediumDesc:
+    """MediumDesc of a path-integrator map (DeltatrackingPathIntegrator, ...)."""
+    from . import maps
+    kw: dict = {}
+    lower_sigma(pi.sigma, kw)
+    alb = pi.scattering_albedo
+    if isinstance(alb, maps.Grid3D):
+        if alb.grid.shape[-1] not in (1, 3):
+            raise NotImplementedError("albedo Grid3D must have 1 or 3 channels")
+        if not (torch.equal(alb.bmin.cpu(), pi.sigma.bmin.cpu()) and torch.equal(alb.bmax.cpu(), pi.sigma.bmax.cpu())):
+            raise NotImplementedError("albedo Grid3D must share sigma's box")
+        kw["albedo_grid"] = alb.grid
+    else:
+        kw["albedo_const"] = _const_values(alb, 3)
+    kw["emission"] = _const_values(pi.emission, 3)
+    kw["env"] = _const_values(pi.environment, 3)
+    es = getattr(pi, "environment_sampler", None)
+    if es is not None:
+        if not (isinstance(es, maps._functionsampler) and isinstance(es.point_sampler, maps.UniformDirectionSampler)):
+            raise NotImplementedError("environment sampler must be _functionsampler(UniformDirectionSampler, const)")
+        if _const_values(es.function_map, 3) != kw["env"]:
+            raise NotImplementedError("environment sampler and environment must be the same constant")
+    lower_phase(getattr(pi, "phase", None), pi.phase_sampler, kw)
+    lower_boundary(pi.boundary, kw)
+    lower_majorant(pi.majorant, pi.sigma, kw)
+    tr = getattr(pi, "transmittance", None)
+    if tr is not None:
+        lower_transmittance(tr, pi.sigma, kw)
+    light = getattr(pi, "directional_light", None)
+    if light is not None:
+        kw["sun_dir"] = tuple(float(v) for v in light.direction.reshape(3).tolist())
+        kw["sun_radiance"] = tuple(float(v) for v in light.radiance.reshape(3).tolist())
+    kw["max_bounces"] = int(getattr(pi, "max_bounces", 0))
+    kw["ds_epsilon"] = float(getattr(pi, "ds_epsilon", 0.1) or 0.0)
+    kw["ds_compat"] = 1 if getattr(pi, "ds_compat", False) else 0
+    return MediumDesc(**kw)
+
+
+def lower_transmittance_map(tr) -> MediumDesc:
+    """MediumDesc of a transmittance map evaluated on rays."""
+    from . import maps
+    kw: dict = {}
+    if isinstance(tr, maps.GridDDATransmittance):
+        lower_sigma(tr.grid_model, kw)
+        kw["transmittance_mode"] = 3 if tr.exact else 2
+    else:
+        lower_sigma(tr.sigma, kw)
+        lower_majorant(tr.majorant, tr.sigma, kw)
+        kw["transmittance_mode"] = 0 if isinstance(tr, maps.RatiotrackingTransmittance) else 1
+    lower_boundary(tr.boundary, kw)
+    return MediumDesc(**kw)

@@ -1,0 +1,336 @@
+"""CUDA path vs the CPU oracle, through the C ABI (needs a B200).
+
+Same inputs and the same Philox keys on both sides, so most paths agree draw
+for draw; float rounding (FMA contraction, libm vs CUDA transcendentals) lets a
+tiny fraction of stochastic paths take a different branch, which the tests
+bound explicitly.  Deterministic quantities (DDA, grids, majorants) are
+compared element-wise.  Tolerances are written in each test.
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from rendervous_b200 import _lib, maps, synthetic
+from tests.helpers import build_field, front_camera, homogeneous
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _setup(cuda):
+    maps.set_sync_checks(True)
+    yield
+
+
+def _scene(field):
+    d = field.lower()
+    return d, oracle.OracleScene(d.to_numpy())
+
+
+def _grad_scene(field):
+    d = field.lower()
+    return d, oracle.OracleScene(d.to_numpy(), with_grads=True)
+
+
+# ------------------------------------------------------------------- grids --
+def test_grid3d_fw_bw(cuda):
+    g = torch.rand(9, 10, 11, 3, device=cuda)
+    bmin, bmax = maps.vec3(-0.7, -0.5, -0.4), maps.vec3(0.6, 0.5, 0.45)
+    grid = maps.Grid3D(torch.nn.Parameter(g), bmin, bmax)
+    x = (torch.rand(20000, 3, device=cuda) * 1.6 - 0.8)
+    y = grid(x)
+    ib = (1.0 / (bmax - bmin)).numpy()
+    ref = oracle.grid3d_fw(g.cpu().numpy(), bmin.numpy(), ib, x.cpu().numpy())
+    assert torch.allclose(y.cpu(), torch.from_numpy(ref), rtol=1e-6, atol=1e-6)
+    dout = torch.rand_like(y)
+    (y * dout).sum().backward()
+    gref = oracle.grid3d_bw(g.cpu().numpy(), bmin.numpy(), ib, x.cpu().numpy(), dout.cpu().numpy())
+    assert torch.allclose(grid.grid.grad.cpu(), torch.from_numpy(gref), rtol=1e-5, atol=1e-5)
+
+
+def test_ray_box(cuda):
+    rays = torch.from_numpy(synthetic.sphere_rays(5000, 1)).to(cuda)
+    rb = maps.ray_box_intersection[maps.vec3(-0.5, -0.4, -0.3), maps.vec3(0.5, 0.4, 0.3)]
+    out = rb(rays).cpu().numpy()
+    ref = oracle.ray_box(rays.cpu().numpy(), [-0.5, -0.4, -0.3], [0.5, 0.4, 0.3])
+    assert np.allclose(out, ref, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("brick", [4, 8])
+def test_majorant_grid_build(cuda, brick):
+    sig = synthetic.gaussian_blobs(37, 6, 9.0, seed=2)
+    grid = maps.Grid3D(torch.from_numpy(sig).to(cuda), *maps.normalized_box(list(sig.shape)))
+    mg = maps.MajorantGrid(grid, brick=brick)
+    assert np.array_equal(mg.tensor().cpu().numpy(), oracle.majorant_build(sig, brick))
+
+
+# --------------------------------------------------------------------- DDA --
+def _dda_map(sig_np, cuda, exact, requires_grad=False):
+    t = torch.from_numpy(sig_np).to(cuda)
+    bmin, bmax = maps.normalized_box(t)
+    g = maps.Grid3D(torch.nn.Parameter(t, requires_grad=requires_grad), bmin, bmax)
+    return maps.GridDDATransmittance(g, maps.ray_box_intersection[bmin, bmax], exact=exact)
+
+
+@pytest.mark.parametrize("exact", [False, True])
+def test_dda_transmittance_matches_oracle(cuda, exact):
+    sig = synthetic.value_noise(65, 4, 50.0, seed=3)
+    tr = _dda_map(sig, cuda, exact, requires_grad=True)
+    rays_np = synthetic.sphere_rays(1 << 15, seed=4)
+    rays = torch.from_numpy(rays_np).to(cuda)
+    T = tr(rays)
+    d, sc = _grad_scene_from_dda(tr)
+    Tref = oracle.transmittance_fw(sc, "dda_exact" if exact else "dda", rays_np, 0)
+    # 1e-5 relative (plus an absolute floor for T ~ 0)
+    assert np.allclose(T.cpu().numpy()[:, 0], Tref, rtol=1e-5, atol=1e-7)
+    w = torch.from_numpy(synthetic.uniform_weights(rays.shape[0], 5)).to(cuda)
+    (T[:, 0] * w).sum().backward()
+    oracle.transmittance_bw(sc, "dda_exact" if exact else "dda", rays_np, 0, w.cpu().numpy())
+    g = tr.grid.grad.cpu().numpy()
+    scale = np.abs(sc.sigma_grad).max()
+    assert np.abs(g - sc.sigma_grad).max() <= 1e-4 * scale
+
+
+def _grad_scene_from_dda(tr):
+    from rendervous_b200.lowering import lower_transmittance_map
+    d = lower_transmittance_map(tr)
+    return d, oracle.OracleScene(d.to_numpy(), with_grads=True)
+
+
+def test_dda_exact_vs_fp64_raymarch(cuda):
+    sig = synthetic.value_noise(65, 4, 50.0, seed=3)
+    tr = _dda_map(sig, cuda, True)
+    rays_np = synthetic.sphere_rays(2048, seed=8)
+    T = tr(torch.from_numpy(rays_np).to(cuda)).cpu().numpy()[:, 0].astype(np.float64)
+    d, sc = _grad_scene_from_dda(tr)
+    tau = oracle.tau_raymarch_fp64(sc, rays_np, 64)
+    assert np.allclose(T, np.exp(-tau), rtol=1e-5, atol=1e-7)
+
+
+def test_dda_full_size_properties(cuda):
+    """256^3, 2^20 rays: T in [0,1]; exact against the FP64 march on a sample;
+    Euler identity of the adjoint (tau is linear in sigma):
+    sum_k sigma_k dL/dsigma_k = -sum_i w_i T_i tau_i."""
+    sig = synthetic.value_noise(256, 4, 50.0, seed=3)
+    tr = _dda_map(sig, cuda, True, requires_grad=True)
+    rays_np = synthetic.sphere_rays(1 << 20, seed=4)
+    rays = torch.from_numpy(rays_np).to(cuda)
+    w = torch.from_numpy(synthetic.uniform_weights(1 << 20, 5)).to(cuda)
+    T = tr(rays)[:, 0]
+    assert float(T.min()) >= 0.0 and float(T.max()) <= 1.0
+    d, sc = _grad_scene_from_dda(tr)
+    idx = np.arange(0, 1 << 20, 512)
+    tau = oracle.tau_raymarch_fp64(sc, rays_np[idx], 16)
+    assert np.allclose(T.cpu().numpy()[idx], np.exp(-tau), rtol=2e-5, atol=1e-7)
+    (T * w).sum().backward()
+    lhs = float((tr.grid.grad.double() * tr.grid.double()).sum())
+    Td = T.double().clamp_min(1e-30)
+    rhs = float(-(w.double() * Td * (-torch.log(Td))).sum())
+    assert abs(lhs - rhs) <= 1e-3 * abs(rhs)
+
+
+# ---------------------------------------------------- ratio / delta tracking --
+def _tracking_map(sig_np, cuda, mode, majorant, brick=8, requires_grad=False):
+    t = torch.from_numpy(sig_np).to(cuda)
+    bmin, bmax = maps.normalized_box(t)
+    g = maps.Grid3D(torch.nn.Parameter(t, requires_grad=requires_grad), bmin, bmax)
+    maj = maps.const[[float(sig_np.max()), 1e6]] if majorant == "global" else maps.MajorantGrid(g, brick=brick)
+    cls = maps.RatiotrackingTransmittance if mode == "rt" else maps.DeltatrackingTransmittance
+    return cls(g, maps.ray_box_intersection[bmin, bmax], maj)
+
+
+@pytest.mark.parametrize("majorant", ["global", "grid"])
+@pytest.mark.parametrize("mode", ["rt", "dt"])
+def test_tracking_transmittance_matches_oracle(cuda, mode, majorant):
+    sig = synthetic.gaussian_blobs(33, 6, 20.0, seed=1)
+    tr = _tracking_map(sig, cuda, mode, majorant, brick=4, requires_grad=True)
+    rays_np = synthetic.sphere_rays(1 << 14, seed=2)
+    T = tr(torch.from_numpy(rays_np).to(cuda), seed=77)
+    from rendervous_b200.lowering import lower_transmittance_map
+    d = lower_transmittance_map(tr)
+    sc = oracle.OracleScene(d.to_numpy(), with_grads=True)
+    Tref = oracle.transmittance_fw(sc, mode, rays_np, 77)
+    Tg = T.detach().cpu().numpy()[:, 0]
+    same = np.isclose(Tg, Tref, rtol=1e-4, atol=1e-6)
+    assert same.mean() >= 0.999, same.mean()      # <= 0.1% of rays may branch differently
+    w = np.ones(rays_np.shape[0], np.float32)
+    T.sum().backward()
+    oracle.transmittance_bw(sc, mode, rays_np, 77, w)
+    g = tr.sigma.grid.grad.cpu().numpy()
+    rel = np.abs(g - sc.sigma_grad).sum() / np.abs(sc.sigma_grad).sum()
+    assert rel < 5e-3, rel
+
+
+# ------------------------------------------------------------ path tracing --
+def _c1_field(cuda, **kw):
+    wl = synthetic.WORKLOADS["plain_forward_64"]
+    sig = torch.from_numpy(synthetic.make_sigma(wl["sigma"])).to(cuda)
+    sun = tuple(float(v) for v in synthetic.gaussian_direction(wl["sun_seed"]))
+    args = dict(albedo=wl["albedo"], env=wl["env"], sun_dir=sun, sun_radiance=wl["sun_intensity"], g=0.0,
+                max_bounces=wl["max_bounces"])
+    args.update(kw)
+    return build_field(sig, **args)
+
+
+def _capture(field, cuda, H, W, spp, seed, jittered=True, views=1):
+    cam = maps.PerspectiveCameraSensor(W, H, front_camera(views).to(cuda), jittered=jittered)
+    return cam, cam.capture(field, fw_samples=spp, bw_samples=spp, seed=seed)
+
+
+def _oracle_capture(sc, integ, H, W, spp, seed, views=1, jittered=True):
+    return oracle.capture_fw(sc, integ, front_camera(views).numpy(), W, H, math.pi / 4, jittered, spp, seed)
+
+
+@pytest.mark.parametrize("variant", [
+    dict(),                                           # C1: RT shadows, global majorant
+    dict(majorant="grid", brick=8),
+    dict(tr="dt"),
+    dict(tr="dda_exact"),
+    dict(phase="reference", g=0.6),
+    dict(g=0.6, max_bounces=0),
+])
+def test_capture_forward_matches_oracle(cuda, variant):
+    field = _c1_field(cuda, **variant)
+    H = W = 64
+    spp = 8
+    _, img = _capture(field, cuda, H, W, spp, seed=123)
+    d, sc = _scene(field)
+    ref, cnt = _oracle_capture(sc, "nee", H, W, spp, 123)
+    a, b = img.cpu().numpy(), ref
+    close = np.isclose(a, b, rtol=1e-3, atol=1e-5).all(axis=-1)
+    assert close.mean() >= 0.99, close.mean()         # >= 99% of pixels agree path for path
+    assert abs(a.mean() - b.mean()) <= 1e-3 * abs(b.mean()) + 1e-5
+    counters = maps.check()
+    assert counters["status"] == 0
+
+
+def test_capture_forward_statistics_independent_seeds(cuda):
+    """8x8 blocks of GPU and oracle images from independent seeds agree within
+    3 standard errors (4 allowed on a few blocks)."""
+    field = _c1_field(cuda)
+    H = W = 64
+    spp = 16
+    gpu = np.stack([_capture(field, cuda, H, W, spp, seed=1000 + s)[1].cpu().numpy() for s in range(4)])
+    d, sc = _scene(field)
+    cpu = np.stack([_oracle_capture(sc, "nee", H, W, spp, 5000 + s)[0] for s in range(4)])
+    def blocks(x):  # (k, 1, H, W, 3) -> (k, nblocks)
+        return x.reshape(x.shape[0], H // 8, 8, W // 8, 8, 3).mean(axis=(2, 4, 5)).reshape(x.shape[0], -1)
+    bg, bc = blocks(gpu), blocks(cpu)
+    se = np.sqrt(bg.var(0, ddof=1) / 4 + bc.var(0, ddof=1) / 4) + 1e-6
+    z = np.abs(bg.mean(0) - bc.mean(0)) / se
+    assert (z < 3).mean() >= 0.9 and z.max() < 6, z
+
+
+def test_dt_integrator_matches_oracle(cuda):
+    field = _c1_field(cuda, integrator="dt", sun_dir=None)
+    H = W = 48
+    _, img = _capture(field, cuda, H, W, 8, seed=9)
+    d, sc = _scene(field)
+    ref, _ = _oracle_capture(sc, "dt", H, W, 8, 9)
+    close = np.isclose(img.cpu().numpy(), ref, rtol=1e-3, atol=1e-5).all(axis=-1)
+    assert close.mean() >= 0.99
+
+
+@pytest.mark.parametrize("bw, kw", [
+    ("ds", dict()),
+    ("ds", dict(majorant="grid", brick=8)),
+    ("ds", dict(ds_compat=True)),
+    ("dt", dict(integrator="dt", sun_dir=None)),
+    ("drt", dict(integrator="drt")),
+])
+def test_capture_backward_matches_oracle(cuda, bw, kw):
+    wl = synthetic.WORKLOADS["plain_forward_64"]
+    sig = torch.from_numpy(synthetic.make_sigma(wl["sigma"])).to(cuda)
+    alb = torch.from_numpy(synthetic.uniform_grid(64, 0.6, 0.95, seed=8)).to(cuda)
+    args = dict(albedo_grid=torch.nn.Parameter(alb), env=1.0, sun_dir=(0.3, 0.8, 0.5), sun_radiance=3.0, g=0.4,
+                max_bounces=16, sigma_requires_grad=True, integrator="nee_ds")
+    args.update(kw)
+    field = build_field(sig, **args)
+    H = W = 32
+    spp = 4
+    cam, img = _capture(field, cuda, H, W, spp, seed=31)
+    dimg = torch.from_numpy(np.random.default_rng(0).random(img.shape).astype(np.float32)).to(cuda)
+    (img * dimg).sum().backward()
+    d, sc = _grad_scene(field)
+    oracle.capture_bw(sc, bw, front_camera(1).numpy(), W, H, math.pi / 4, True, spp, 31, dimg.cpu().numpy())
+    gs = field.sigma.grid.grad.cpu().numpy()
+    rel = np.abs(gs - sc.sigma_grad).sum() / max(np.abs(sc.sigma_grad).sum(), 1e-30)
+    assert rel < 1e-2, rel
+    if bw == "ds":
+        ga = field.scattering_albedo.grid.grad.cpu().numpy()
+        rela = np.abs(ga - sc.albedo_grad).sum() / max(np.abs(sc.albedo_grad).sum(), 1e-30)
+        assert rela < 1e-2, rela
+
+
+def test_ds_adjoint_matches_finite_difference(cuda):
+    """E[dL/ds] along sigma -> s*sigma from the replay adjoint vs a central
+    difference of the GPU forward with common random numbers."""
+    wl = synthetic.WORKLOADS["plain_forward_64"]
+    sig0 = torch.from_numpy(synthetic.make_sigma(wl["sigma"])).to(cuda)
+    H = W = 32
+    spp = 256
+    wimg = torch.from_numpy(np.random.default_rng(1).random((1, H, W, 3)).astype(np.float32)).to(cuda)
+    grads, fds = [], []
+    for rep in range(6):
+        f = build_field(sig0.clone(), albedo=0.8, env=1.0, sun_dir=(0.2, 1, 0.3), g=0.3, sigma_requires_grad=True)
+        f.majorant = maps.const[[25.0, 1e6]]
+        f.transmittance.majorant = f.majorant
+        cam, img = _capture(f, cuda, H, W, spp, seed=100 + rep)
+        (img * wimg).sum().backward()
+        grads.append(float((f.sigma.grid.grad.double() * sig0.double()).sum()))
+        vals = []
+        for s in (1.05, 0.95):
+            f2 = build_field(sig0 * s, albedo=0.8, env=1.0, sun_dir=(0.2, 1, 0.3), g=0.3)
+            f2.majorant = maps.const[[25.0, 1e6]]
+            f2.transmittance.majorant = f2.majorant
+            _, im2 = _capture(f2, cuda, H, W, spp, seed=200 + rep)
+            vals.append(float((im2 * wimg).sum()))
+        fds.append((vals[0] - vals[1]) / 0.1)
+    g, f = np.array(grads), np.array(fds)
+    err = math.sqrt(g.var(ddof=1) / len(g) + f.var(ddof=1) / len(f))
+    assert abs(g.mean() - f.mean()) < 4 * err + 0.03 * abs(f.mean()), (g, f)
+
+
+# ------------------------------------------------------------ error paths --
+def test_iteration_cap_reports_and_recovers(cuda):
+    """A majorant of 1e12 makes ratio tracking take ~1e12 steps; the kernel stops
+    at its iteration bound, records VRT_E_ITER_CAP, and the context stays usable."""
+    sig = homogeneous(5, 1.0)
+    t = torch.from_numpy(sig).to(cuda)
+    bmin, bmax = maps.normalized_box(t)
+    g = maps.Grid3D(t, bmin, bmax)
+    tr = maps.RatiotrackingTransmittance(g, maps.ray_box_intersection[bmin, bmax], maps.const[[1e12, 1e6]])
+    rays = torch.tensor([[-2.0, 0.0, 0.0, 1.0, 0.0, 0.0]], device=cuda)
+    maps.set_sync_checks(False)
+    try:
+        tr(rays)
+        with pytest.raises(_lib.VrtError) as e:
+            maps.check()
+        assert e.value.status == 4
+        ok = maps.RatiotrackingTransmittance(g, maps.ray_box_intersection[bmin, bmax], maps.const[[1.0, 1e6]])(rays)
+        maps.check()
+        assert 0.0 < float(ok) < 1.0
+    finally:
+        maps.set_sync_checks(True)
+
+
+def test_nonfinite_rays_are_misses(cuda):
+    field = _c1_field(cuda)
+    rays = torch.tensor([[float("nan"), 0, -2, 0, 0, 1], [0, 0, -2, 0, 0, 1]], device=cuda)
+    R = field(rays, seed=3)
+    assert torch.isfinite(R).all()
+
+
+def test_invalid_arguments_raise(cuda):
+    field = _c1_field(cuda)
+    d = field.lower()
+    d.phase_mode = 7
+    ffi, lib = _lib.ffi_lib()
+    m = d.to_struct()
+    rays = torch.zeros(4, 6, device=cuda)
+    R = torch.empty(4, 3, device=cuda)
+    st = lib.vrt_radiance_fw(_lib.context().ptr, m, 0, _lib.fptr(rays), 4, 0, _lib.fptr(R), _lib.stream_handle(cuda))
+    assert st == 1

@@ -1,0 +1,381 @@
+"""Analytic pins of the CPU oracle (CPU only).
+
+The reference ships no tests or golden vectors and cannot run here (Vulkan),
+so the oracle's restatement is pinned by known answers instead: published
+Philox vectors, closed-form trilinear integrals, exp(-sigma d) in homogeneous
+media, sampling moments, the furnace identity (a non-absorbing medium under a
+uniform environment radiates exactly the environment) and finite differences.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.helpers import homogeneous, oracle_desc
+from rendervous_b200 import synthetic
+
+
+# ----------------------------------------------------------------- Philox --
+def test_philox_known_answers():
+    # Random123 known-answer vectors for philox4x32-10
+    assert list(oracle.philox(0, 0, [0, 0, 0, 0])) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    assert list(oracle.philox(0xFFFFFFFF, 0xFFFFFFFF, [0xFFFFFFFF] * 4)) == [0x408F276D, 0x41C83B0E, 0xA20BC7C6,
+                                                                              0x6D5451FD]
+    assert list(oracle.philox(0xA4093822, 0x299F31D0, [0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344])) == [
+        0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
+
+
+def test_random_stream_layout():
+    seed, path, stream = 0x1234567890ABCDEF, (5 << 32) + 17, 1
+    u = oracle.random_sequence(seed, path, stream, 0, 12)
+    for k in range(12):
+        word = oracle.philox(seed & 0xFFFFFFFF, seed >> 32, [k >> 2, path & 0xFFFFFFFF, stream, path >> 32])[k & 3]
+        expect = np.frombuffer(np.uint32((int(word) & 0x7FFFFF) | 0x3F800000).tobytes(), np.float32)[0] - 1.0
+        assert u[k] == np.float32(expect)
+    v = oracle.random_sequence(7, 0, 0, 0, 200000)
+    assert v.min() >= 0.0 and v.max() < 1.0
+    assert abs(v.mean() - 0.5) < 4 * math.sqrt(1 / 12 / v.size)
+    # a restart at draw 5 reproduces the tail
+    assert np.array_equal(oracle.random_sequence(7, 0, 0, 5, 10), v[5:15])
+
+
+# ------------------------------------------------------------------ boxes --
+def test_ray_box():
+    rays = np.array([[-2, 0, 0, 1, 0, 0], [0, 0, 0, 0, 0, 1], [-2, 3, 0, 1, 0, 0]], np.float32)
+    out = oracle.ray_box(rays, [-0.5] * 3, [0.5] * 3)
+    assert np.allclose(out[0], [1.5, 2.5])
+    assert np.allclose(out[1], [-0.5, 0.5])
+    assert out[2, 1] < out[2, 0]  # miss
+
+
+# ------------------------------------------------------------------ grids --
+def _numpy_trilinear(grid, bmin, inv_bsize, x):
+    D, H, W, C = grid.shape
+    nc = (x - bmin) * inv_bsize
+    out = np.zeros((x.shape[0], C), np.float64)
+    inside = np.all((nc >= 0) & (nc < 1), axis=1)
+    dim = np.array([W - 1, H - 1, D - 1], np.float64)
+    gc = nc * dim
+    p = np.clip(np.floor(gc).astype(np.int64), 0, (dim - 1).astype(np.int64))
+    a = gc - np.floor(gc)
+    for dz in (0, 1):
+        for dy in (0, 1):
+            for dx in (0, 1):
+                w = (a[:, 0] if dx else 1 - a[:, 0]) * (a[:, 1] if dy else 1 - a[:, 1]) * (a[:, 2] if dz else 1 - a[:, 2])
+                out += w[:, None] * grid[p[:, 2] + dz, p[:, 1] + dy, p[:, 0] + dx].astype(np.float64)
+    out[~inside] = 0
+    return out
+
+
+def test_grid3d_forward_and_backward():
+    rng = np.random.default_rng(0)
+    grid = rng.random((5, 6, 7, 3)).astype(np.float32)
+    bmin = np.array([-1, -0.5, -0.25], np.float32)
+    bmax = np.array([1, 0.5, 0.75], np.float32)
+    ib = (1.0 / (bmax - bmin)).astype(np.float32)
+    x = rng.uniform(-1.2, 1.2, size=(4000, 3)).astype(np.float32)
+    out = oracle.grid3d_fw(grid, bmin, ib, x)
+    ref = _numpy_trilinear(grid, bmin, ib, x)
+    assert np.allclose(out, ref, atol=2e-6)
+    dout = rng.random((4000, 3)).astype(np.float32)
+    g = oracle.grid3d_bw(grid, bmin, ib, x, dout)
+    inside = np.all(((x - bmin) * ib >= 0) & ((x - bmin) * ib < 1), axis=1)
+    # the 8 weights sum to one: total gradient == total upstream gradient of inside points
+    assert np.allclose(g.sum(axis=(0, 1, 2)), dout[inside].sum(axis=0), rtol=1e-5)
+    # linearity: <grad, grid> == <dout, out>
+    assert np.isclose(float((g.astype(np.float64) * grid).sum()), float((dout.astype(np.float64) * out).sum()), rtol=1e-5)
+
+
+# -------------------------------------------------------------------- DDA --
+def _axis_rays(n, seed=0):
+    rng = np.random.default_rng(seed)
+    o = rng.normal(size=(n, 3))
+    o *= 1.5 / np.linalg.norm(o, axis=1, keepdims=True)
+    t = rng.uniform(-0.45, 0.45, size=(n, 3))
+    w = t - o
+    w /= np.linalg.norm(w, axis=1, keepdims=True)
+    return np.concatenate([o, w], 1).astype(np.float32)
+
+
+def _clip(rays, lo=-0.5, hi=0.5):
+    out = oracle.ray_box(rays, [lo] * 3, [hi] * 3)
+    return np.maximum(out[:, 0], 0), out[:, 1]
+
+
+def test_dda_exact_and_midpoint_on_bilinear_field():
+    """sigma = c + x*y is reproduced exactly by trilinear interpolation; along a ray
+    it is quadratic in t, so the exact mode must match the closed form, while the
+    reference's midpoint rule does not (its TODO at vr_transmittance_DDA.h:41)."""
+    res = 9
+    u = np.linspace(-0.5, 0.5, res)
+    z, y, x = np.meshgrid(u, u, u, indexing="ij")
+    sig = (2.0 + 4.0 * x * y)[..., None].astype(np.float32)
+    sc = oracle.OracleScene(oracle_desc(sig))
+    rays = _axis_rays(500)
+    t0, t1 = _clip(rays)
+    o, w = rays[:, :3].astype(np.float64), rays[:, 3:].astype(np.float64)
+
+    def prim(t):  # integral of 2 + 4 (ox + wx t)(oy + wy t)
+        return 2 * t + 4 * (o[:, 0] * o[:, 1] * t + (o[:, 0] * w[:, 1] + o[:, 1] * w[:, 0]) * t ** 2 / 2
+                            + w[:, 0] * w[:, 1] * t ** 3 / 3)
+
+    tau = prim(t1) - prim(t0)
+    T_exact = oracle.transmittance_fw(sc, "dda_exact", rays, 0)
+    assert np.allclose(T_exact, np.exp(-tau), rtol=1e-5, atol=1e-7)
+    T_mid = oracle.transmittance_fw(sc, "dda", rays, 0)
+    assert np.abs(T_mid - np.exp(-tau)).max() > 1e-5  # the midpoint rule is not exact here
+    assert np.allclose(T_mid, np.exp(-tau), rtol=2e-2)
+
+
+def test_dda_linear_field_both_modes_exact():
+    res = 7
+    u = np.linspace(-0.5, 0.5, res)
+    z, y, x = np.meshgrid(u, u, u, indexing="ij")
+    sig = (3.0 + 2.0 * x - 1.0 * y + 0.5 * z)[..., None].astype(np.float32)
+    sc = oracle.OracleScene(oracle_desc(sig))
+    rays = _axis_rays(300, 1)
+    t0, t1 = _clip(rays)
+    o, w = rays[:, :3].astype(np.float64), rays[:, 3:].astype(np.float64)
+    c = np.array([2.0, -1.0, 0.5])
+    tau = 3 * (t1 - t0) + (o @ c) * (t1 - t0) + (w @ c) * (t1 ** 2 - t0 ** 2) / 2
+    for mode in ("dda", "dda_exact"):
+        T = oracle.transmittance_fw(sc, mode, rays, 0)
+        assert np.allclose(T, np.exp(-tau), rtol=2e-5, atol=1e-7), mode
+
+
+def test_dda_exact_matches_fp64_raymarch_on_noise():
+    sig = synthetic.value_noise(33, 3, 8.0, seed=3)
+    sc = oracle.OracleScene(oracle_desc(sig))
+    rays = synthetic.sphere_rays(400, seed=4)
+    tau = oracle.tau_raymarch_fp64(sc, rays, 64)
+    T = oracle.transmittance_fw(sc, "dda_exact", rays, 0, fp64=True)
+    assert np.allclose(T, np.exp(-tau), rtol=1e-6, atol=1e-9)
+    T32 = oracle.transmittance_fw(sc, "dda_exact", rays, 0)
+    assert np.allclose(T32, np.exp(-tau), rtol=3e-5, atol=1e-7)
+
+
+@pytest.mark.parametrize("mode", ["dda", "dda_exact"])
+def test_dda_backward_is_the_derivative(mode):
+    """tau is linear in the node values, so d tau / d sigma_k is exact by a
+    finite difference of any size; check dL/dsigma for L = sum w_i T_i."""
+    sig = synthetic.value_noise(9, 2, 3.0, seed=5)
+    rays = synthetic.sphere_rays(64, seed=6)
+    wts = synthetic.uniform_weights(64, seed=7)
+    sc = oracle.OracleScene(oracle_desc(sig), with_grads=True)
+    oracle.transmittance_bw(sc, mode, rays, 0, wts)
+    grad = sc.sigma_grad.reshape(-1)
+    rng = np.random.default_rng(0)
+    for k in rng.choice(grad.size, 12, replace=False):
+        def loss(delta):
+            s2 = sig.copy().reshape(-1)
+            s2[k] += delta
+            sc2 = oracle.OracleScene(oracle_desc(s2.reshape(sig.shape)))
+            sc2.s.global_majorant = sc.s.global_majorant
+            T = oracle.transmittance_fw(sc2, mode, rays, 0, fp64=True).astype(np.float64)
+            return float((wts * T).sum())
+        h = 1e-2
+        fd = (loss(h) - loss(-h)) / (2 * h)
+        assert abs(fd - grad[k]) <= 2e-4 * max(1.0, abs(fd)) + 2e-4, (k, fd, grad[k])
+
+
+# ------------------------------------------------------- stochastic tracking --
+def _through_centre(n):
+    rays = np.zeros((n, 6), np.float32)
+    rays[:, 0] = -2.0
+    rays[:, 3] = 1.0
+    return rays
+
+
+@pytest.mark.parametrize("majorant", ["global", "grid"])
+@pytest.mark.parametrize("mode", ["rt", "dt"])
+def test_tracking_transmittance_homogeneous(mode, majorant):
+    s = 1.7
+    sc = oracle.OracleScene(oracle_desc(homogeneous(17, s), majorant=majorant, brick=4))
+    if majorant == "global":
+        sc.s.global_majorant = 2.5  # a loose bound exercises null collisions
+    T = oracle.transmittance_fw(sc, mode, _through_centre(40000), 11).astype(np.float64)
+    expect = math.exp(-s * 1.0)
+    se = T.std() / math.sqrt(T.size)
+    assert abs(T.mean() - expect) < 4 * se + 1e-4
+
+
+@pytest.mark.parametrize("mode", ["rt", "dt"])
+def test_tracking_transmittance_gradient_homogeneous(mode):
+    """E[sum_k dT/dsigma_k] = d/ds exp(-s d) = -d exp(-s d) for a uniform grid."""
+    s = 1.2
+    n = 40000
+    sc = oracle.OracleScene(oracle_desc(homogeneous(9, s)), with_grads=True)
+    sc.s.global_majorant = 2.0
+    rays = _through_centre(n)
+    # per-ray totals via separate calls would be slow: split into batches for the error bar
+    totals = []
+    for b in range(8):
+        sc.sigma_grad[...] = 0
+        oracle.transmittance_bw(sc, mode, rays[: n // 8], 100 + b, np.ones(n // 8, np.float32))
+        totals.append(sc.sigma_grad.sum() / (n // 8))
+    totals = np.array(totals)
+    expect = -1.0 * math.exp(-s)
+    assert abs(totals.mean() - expect) < 4 * totals.std(ddof=1) / math.sqrt(len(totals)) + 2e-3
+
+
+# -------------------------------------------------------------- directions --
+@pytest.mark.parametrize("g", [0.0, 0.3, -0.6, 0.8])
+def test_hg_sampling_moments(g):
+    n = 100000
+    w_in = np.tile(np.array([[0.0, 0.6, 0.8]], np.float32), (n, 1))
+    sc = oracle.OracleScene(oracle_desc(homogeneous(3, 1.0), g=g, phase_mode=0))
+    out = oracle.phase_sample(sc, w_in, 3)
+    assert np.all(out[:, 0] == 1.0)
+    wo = out[:, 1:].astype(np.float64)
+    assert np.allclose(np.linalg.norm(wo, axis=1), 1.0, atol=1e-5)
+    c = wo @ w_in[0].astype(np.float64)
+    assert abs(c.mean() - g) < 4 * c.std() / math.sqrt(n) + 1e-3
+    # second moment of HG: E[cos^2] = (1 + 2 g^2) / 3
+    assert abs((c ** 2).mean() - (1 + 2 * g * g) / 3) < 5 * (c ** 2).std() / math.sqrt(n) + 1e-3
+
+
+def test_reference_vhg_mixture_moment():
+    g, n = 0.6, 100000
+    w_in = np.tile(np.array([[1.0, 0.0, 0.0]], np.float32), (n, 1))
+    sc = oracle.OracleScene(oracle_desc(homogeneous(3, 1.0), g=g, phase_mode=1))
+    c = oracle.phase_sample(sc, w_in, 4)[:, 1].astype(np.float64)
+    expect = 0.8 * (g / 5) + 0.2 * g  # VHGPhaseSampler draws g/5 with probability 0.8
+    assert abs(c.mean() - expect) < 4 * c.std() / math.sqrt(n) + 1e-3
+
+
+def test_environment_sampler_uniform_sphere():
+    n = 100000
+    sc = oracle.OracleScene(oracle_desc(homogeneous(3, 1.0), env=(1.0, 2.0, 0.5)))
+    out = oracle.env_sample(sc, n, 9)
+    assert np.allclose(out[:, :3], np.array([1.0, 2.0, 0.5]) * 4 * math.pi, rtol=1e-6)
+    w = out[:, 3:].astype(np.float64)
+    assert np.allclose(np.linalg.norm(w, axis=1), 1.0, atol=1e-5)
+    assert np.all(np.abs(w.mean(0)) < 4 * math.sqrt(1 / 3 / n))
+    assert np.allclose((w ** 2).mean(0), 1 / 3, atol=5e-3)
+
+
+def test_camera_rays():
+    poses = synthetic.ring_poses(2)
+    rays = oracle.camera_rays(poses, 5, 5, math.pi / 4, False, 1, 0)[0]
+    for v in range(2):
+        centre = rays[v * 25 + 12]
+        assert np.allclose(centre[3:], poses[v, 3:6], atol=1e-6)
+        assert np.allclose(centre[:3], poses[v, :3] + poses[v, 3:6] * (0.001 / math.tan(math.pi / 8)), atol=1e-6)
+    jit = oracle.camera_rays(poses, 5, 5, math.pi / 4, True, 2, 0)
+    assert not np.allclose(jit[0], jit[1])
+
+
+# --------------------------------------------------------------- majorant --
+def test_majorant_grid_bounds_every_lookup():
+    sig = synthetic.gaussian_blobs(33, 5, 10.0, seed=2)
+    brick = 4
+    maj = oracle.majorant_build(sig, brick)
+    dim = 32
+    assert maj.shape == (8, 8, 8)
+    # brute force: max over each brick's node window with one-node apron
+    for mz in range(8):
+        for my in range(8):
+            for mx in range(8):
+                lo = [max(m * brick - 1, 0) for m in (mz, my, mx)]
+                hi = [min((m + 1) * brick + 1, dim) for m in (mz, my, mx)]
+                expect = sig[lo[0]:hi[0] + 1, lo[1]:hi[1] + 1, lo[2]:hi[2] + 1, 0].max()
+                assert maj[mz, my, mx] == expect
+    # every trilinear lookup inside a brick is bounded by its majorant
+    rng = np.random.default_rng(1)
+    x = rng.uniform(-0.5, 0.5, size=(20000, 3)).astype(np.float32)
+    sc = oracle.OracleScene(oracle_desc(sig, majorant="grid", brick=brick))
+    s = oracle.grid3d_fw(sig, [sc.s.bmin[i] for i in range(3)], [sc.s.inv_bsize[i] for i in range(3)], x)[:, 0]
+    q = oracle.majorant_query(sc, np.concatenate([x, np.tile([[0.0, 0.0, 1.0]], (x.shape[0], 1))], 1).astype(np.float32))
+    assert np.all(s <= q[:, 0] + 1e-6)
+    assert np.all(q[:, 1] > 0)
+
+
+def test_majorant_query_distance():
+    sig = homogeneous(17, 1.0)
+    sc = oracle.OracleScene(oracle_desc(sig, majorant="grid", brick=4))  # 4 bricks of 0.25 per axis
+    rays = np.array([[-0.49, 0.01, 0.02, 1, 0, 0],      # brick 0 along +x: 0.24 to the face at -0.25
+                     [0.30, 0.01, 0.02, -1, 0, 0],      # brick 3 going -x: 0.05 to 0.25
+                     [-0.25, 0.01, 0.02, 1, 0, 0]],     # on a face: assigned to the brick ahead
+                    np.float32)
+    q = oracle.majorant_query(sc, rays)
+    assert np.allclose(q[:, 1], [0.24, 0.05, 0.25], atol=1e-5)
+
+
+# -------------------------------------------------------- path integrators --
+def _furnace_desc(**kw):
+    sig = synthetic.gaussian_blobs(17, 4, 6.0, seed=3)
+    return oracle_desc(sig, albedo=1.0, env=1.0, **kw)
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(majorant="grid", brick=4), dict(tr="dt"), dict(g=0.6),
+                                dict(phase_mode=1, g=0.6), dict(tr="dda_exact")])
+def test_nee_furnace(kw):
+    """Albedo 1 under a uniform unit environment: the radiance is 1 everywhere."""
+    sc = oracle.OracleScene(_furnace_desc(**kw))
+    rays = np.tile(np.array([[0.1, -0.05, -2.0, 0.0, 0.05, 1.0]], np.float32), (20000, 1))
+    rays[:, 3:] /= np.linalg.norm(rays[:, 3:], axis=1, keepdims=True)
+    R, cnt = oracle.radiance_fw(sc, "nee", rays, 5)
+    assert cnt["vertices"] > 0
+    m = R.astype(np.float64).mean(0)
+    se = R.std(0) / math.sqrt(R.shape[0])
+    assert np.all(np.abs(m - 1.0) < 4 * se + 2e-3), (m, se)
+
+
+def test_dt_integrator_furnace_is_exact_per_path():
+    sc = oracle.OracleScene(_furnace_desc())
+    rays = np.tile(np.array([[0.0, 0.0, -2.0, 0.0, 0.0, 1.0]], np.float32), (2000, 1))
+    R, _ = oracle.radiance_fw(sc, "dt", rays, 6)
+    assert np.allclose(R, 1.0)
+
+
+def test_nee_without_scattering_is_direct_transmittance():
+    sig = synthetic.gaussian_blobs(17, 4, 3.0, seed=4)
+    sc = oracle.OracleScene(oracle_desc(sig, albedo=0.0, env=1.0))
+    ray = np.array([[0.05, 0.02, -2.0, 0.0, 0.0, 1.0]], np.float32)
+    R, _ = oracle.radiance_fw(sc, "nee", np.tile(ray, (30000, 1)), 7)
+    tau = oracle.tau_raymarch_fp64(oracle.OracleScene(oracle_desc(sig)), ray, 64)[0]
+    m, se = R[:, 0].mean(), R[:, 0].std() / math.sqrt(R.shape[0])
+    assert abs(m - math.exp(-tau)) < 4 * se + 1e-3
+
+
+def test_sun_single_scatter_adds_light():
+    sig = synthetic.gaussian_blobs(17, 4, 3.0, seed=4)
+    base = oracle.OracleScene(oracle_desc(sig, albedo=0.8, env=0.0))
+    sun = oracle.OracleScene(oracle_desc(sig, albedo=0.8, env=0.0, sun_dir=(0.3, 1.0, 0.2), sun_radiance=3.0))
+    rays = np.tile(np.array([[0.0, 0.0, -2.0, 0.0, 0.0, 1.0]], np.float32), (4000, 1))
+    assert np.all(oracle.radiance_fw(base, "nee", rays, 1)[0] == 0)
+    assert oracle.radiance_fw(sun, "nee", rays, 1)[0].mean() > 0
+
+
+@pytest.mark.parametrize("bw", ["ds", "dt"])
+def test_adjoint_matches_finite_difference_of_expectation(bw):
+    """dE[L]/ds along sigma -> s*sigma: the replay adjoint (consistent majorant)
+    against a central difference of the forward with common random numbers."""
+    sig = synthetic.gaussian_blobs(9, 3, 4.0, seed=8)
+    kw = dict(albedo=0.7, env=1.0, sun_dir=(0.2, 1.0, 0.1), sun_radiance=2.0, g=0.3)
+    integ = "nee" if bw == "ds" else "dt"
+    poses = synthetic.ring_poses(1)
+    H = W = 8
+    spp = 512
+    wimg = np.random.default_rng(3).random((1, H, W, 3)).astype(np.float32)
+
+    def loss(scale, seed):
+        sc = oracle.OracleScene(oracle_desc(sig * scale, **kw))
+        sc.s.global_majorant = 6.0
+        img, _ = oracle.capture_fw(sc, integ, poses, W, H, math.pi / 4, True, spp, seed)
+        return float((img.astype(np.float64) * wimg).sum())
+
+    sc = oracle.OracleScene(oracle_desc(sig, **kw), with_grads=True)
+    sc.s.global_majorant = 6.0
+    grads = []
+    fds = []
+    h = 0.05
+    for seed in range(4):
+        sc.sigma_grad[...] = 0
+        oracle.capture_bw(sc, bw, poses, W, H, math.pi / 4, True, spp, 1000 + seed, wimg)
+        grads.append(float((sc.sigma_grad.astype(np.float64) * sig).sum()))
+        fds.append((loss(1 + h, 2000 + seed) - loss(1 - h, 2000 + seed)) / (2 * h))
+    g, f = np.array(grads), np.array(fds)
+    err = math.sqrt(g.var(ddof=1) / len(g) + f.var(ddof=1) / len(f))
+    assert abs(g.mean() - f.mean()) < 4 * err + 0.05 * abs(f.mean()), (g, f)
