@@ -1,0 +1,421 @@
+"""Benchmark of the volumetric path-integration hot path on B200.
+
+Workload (one "step"): the differentiable path tracer on the seeded 256^3
+blob medium -- 64 Gaussian blobs with max sigma 40, a 256^3 albedo grid
+U[0.6, 0.95], HG g = 0.6, constant environment 1 plus a directional light of
+intensity 3, one 512x512 camera, 64 spp, at most 64 bounces, NEE with ratio
+tracking over an 8^3-brick majorant grid -- rendered forward, compared with an
+L2 loss against a target rendered from the perturbed grid sigma*(1 + 0.1 u),
+u ~ U(-1, 1), and differentiated by the path-replay adjoint (NEE_DS) into
+dL/dsigma and dL/dalbedo.
+
+Metric: path vertices (real scattering collisions of the forward paths) per
+second of the whole forward + backward step.  With N GPUs every rank renders
+the full image with its own seed (weak scaling) and the gradients are summed
+with one NCCL all-reduce per step, the data-parallel inverse-rendering step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "differentiable_pt_256"
+METRIC = "vertices/s fwd+bwd"
+UNIT = "path vertices/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--small", action="store_true", help="a 128x128, 8 spp image of the same medium (profiling)")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- workload --
+_ARRAYS = {}
+
+
+def workload_arrays():
+    if "v" not in _ARRAYS:
+        _ARRAYS["v"] = _workload_arrays()
+    return _ARRAYS["v"]
+
+
+def _workload_arrays():
+    from rendervous_b200 import synthetic
+    wl = synthetic.WORKLOADS[WORKLOAD]
+    sigma = synthetic.make_sigma(wl["sigma"])
+    kind, a = wl["albedo"]
+    albedo = synthetic.uniform_grid(a["res"], a["lo"], a["hi"], a["seed"])
+    noise = synthetic.uniform_grid(sigma.shape[0], -1.0, 1.0, wl["target_seed"])
+    target_sigma = np.ascontiguousarray(sigma * (1.0 + 0.1 * noise))
+    sun = synthetic.gaussian_direction(wl["sun_seed"])
+    poses = synthetic.ring_poses(wl["views"])
+    return wl, sigma, albedo, target_sigma, sun, poses
+
+
+def build_field(sigma_t, albedo_t, wl, sun):
+    from rendervous_b200 import maps
+    bmin, bmax = maps.normalized_box(sigma_t)
+    sg = maps.Grid3D(sigma_t, bmin, bmax)
+    ag = maps.Grid3D(albedo_t, bmin, bmax)
+    env = maps.const[1.0, 1.0, 1.0]
+    boundary = maps.ray_box_intersection[bmin, bmax]
+    maj = maps.MajorantGrid(sg, brick=8)
+    g = maps.const[wl["phase_g"]]
+    tr = maps.RatiotrackingTransmittance(sg, boundary, maj)
+    return maps.DeltatrackingNEEPathIntegrator(
+        sg, ag, maps.ZERO, env, maps._functionsampler(maps.UniformDirectionSampler(6), env),
+        maps.HenyeyGreensteinPhase(g), maps.HenyeyGreensteinPhaseSampler(g), boundary, maj, tr, 0.1,
+        max_bounces=wl["max_bounces"],
+        directional_light=maps.DirectionalLight(sun, wl["sun_intensity"]))
+
+
+# ----------------------------------------------------------------- clocks --
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        under_load = [s for s in sm if mx and s > 0.3 * mx] or sm
+        return {"sm_mhz": statistics.median(under_load) if under_load else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profiled_traffic(kernel: str):
+    """dram read+write bytes per launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{WORKLOAD}.txt")
+    if not os.path.exists(p):
+        return None
+    for ln in open(p):
+        if ln.startswith("traffic_bytes_per_launch:"):
+            return float(ln.split(":", 1)[1])
+    return None
+
+
+# ------------------------------------------------------------ CPU baseline --
+def cpu_sample(seconds_hint: float = 10.0, threads: int | None = None):
+    """The oracle (the reference's algorithm restated in C++, constant majorant
+    as the reference builds it) on a bounded sample of the workload: the same
+    medium and camera at 256x256 pixels, 16 spp, forward NEE + NEE_DS adjoint.
+    Returns (vertices/s, sample description, threads)."""
+    import oracle
+    from rendervous_b200.lowering import MediumDesc
+    import torch
+    wl, sigma, albedo, target_sigma, sun, poses = workload_arrays()
+    threads = threads or os.cpu_count() or 1
+    oracle.set_threads(threads)
+    bmin = torch.tensor([-0.5, -0.5, -0.5])
+    d = MediumDesc(sigma=torch.from_numpy(sigma), bmin=bmin, bmax=-bmin, box_min=bmin, box_max=-bmin,
+                   albedo_grid=torch.from_numpy(albedo), env=(1.0, 1.0, 1.0), sun_dir=tuple(float(v) for v in sun),
+                   sun_radiance=(wl["sun_intensity"],) * 3, phase_mode=0, phase_g=wl["phase_g"], majorant_mode=0,
+                   global_majorant=float(sigma.max()), transmittance_mode=0, max_bounces=wl["max_bounces"],
+                   ds_epsilon=0.1)
+    sc = oracle.OracleScene(d.to_numpy(), with_grads=True)
+    H = W = 256
+    spp = 16
+    t0 = time.perf_counter()
+    img, cnt = oracle.capture_fw(sc, "nee", poses, W, H, math.pi / 4, True, spp, 12345)
+    dimg = np.ones_like(img)
+    oracle.capture_bw(sc, "ds", poses, W, H, math.pi / 4, True, spp, 12345, dimg)
+    dt = time.perf_counter() - t0
+    return cnt["vertices"] / dt, f"{W}x{H} px x {spp} spp ({W * H * spp} paths) fw+bw of the same medium", threads, dt
+
+
+# --------------------------------------------------------------- our arm --
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from rendervous_b200 import build as vbuild, maps
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    vbuild.build()
+    maps.set_sync_checks(False)
+
+    wl, sigma, albedo, target_sigma, sun, poses_np = workload_arrays()
+    H = W = 128 if args.small else wl["width"]
+    spp = 8 if args.small else wl["spp"]
+    sigma_t = torch.nn.Parameter(torch.from_numpy(sigma).to(dev))
+    albedo_t = torch.nn.Parameter(torch.from_numpy(albedo).to(dev))
+    field = build_field(sigma_t, albedo_t, wl, sun)
+    cam = maps.PerspectiveCameraSensor(W, H, torch.from_numpy(poses_np).to(dev), jittered=True)
+    with torch.no_grad():
+        tfield = build_field(torch.from_numpy(target_sigma).to(dev), albedo_t.detach(), wl, sun)
+        target = cam.capture(tfield, fw_samples=spp, seed=777)
+    maps.check()
+
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+
+    def step(k):
+        sigma_t.grad = None
+        albedo_t.grad = None
+        img = cam.capture(field, fw_samples=spp, bw_samples=spp, seed=1000 * (rank + 1) + k)
+        loss = ((img - target) ** 2).sum()
+        loss.backward()
+        if world > 1:
+            dist.all_reduce(sigma_t.grad)
+            dist.all_reduce(albedo_t.grad)
+        return loss
+
+    for k in range(args.warmup):
+        step(k)
+    counters0 = maps.check()
+    if counters0["status"]:
+        raise RuntimeError(f"device error during warm-up: {counters0}")
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    times = []
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step(args.warmup + k)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    counters = maps.check()
+    total_ms = sum(times)
+    ms_t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+    vt = torch.tensor([float(counters["vertices"])], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(vt)
+    total_ms = float(ms_t.item())
+    vertices = float(vt.item())
+    value = vertices / (total_ms / 1e3)
+
+    # ---- per-kernel split for the roofline (forward kernel and adjoint kernel)
+    roof = {}
+    with torch.no_grad():
+        pass
+    for name in ("fw", "bw"):
+        reps = 2
+        ms_l, cnt_l = [], []
+        for r in range(reps):
+            sigma_t.grad = None
+            albedo_t.grad = None
+            flush.zero_()
+            maps.check()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            if name == "fw":
+                e0.record(stream)
+                img = cam.capture(field, fw_samples=spp, bw_samples=spp, seed=5000 + r)
+                e1.record(stream)
+                e1.synchronize()
+                c = maps.check()
+            else:
+                img = cam.capture(field, fw_samples=spp, bw_samples=spp, seed=5000 + r)
+                loss = ((img - target) ** 2).sum()
+                torch.cuda.synchronize(dev)
+                maps.check()
+                flush.zero_()
+                e0.record(stream)
+                loss.backward()
+                e1.record(stream)
+                e1.synchronize()
+                c = maps.check()
+            ms_l.append(e0.elapsed_time(e1))
+            cnt_l.append(c)
+        ms = statistics.mean(ms_l)
+        c = cnt_l[-1]
+        bytes_alg = 32.0 * c["lookups"] + 32.0 * c["albedo_lookups"] + 4.0 * c["reds"] + 12.0 * c["paths"]
+        roof[name] = dict(ms=ms, bytes=bytes_alg, counters=c)
+    dom = max(roof, key=lambda k: roof[k]["ms"])
+    kern = {"fw": "k_nee_fw", "bw": "k_path_bw"}[dom]
+    peaks = measured_peaks()
+    achieved = roof[dom]["bytes"] / (roof[dom]["ms"] / 1e3) / 1e9
+    traffic = profiled_traffic(kern)
+
+    # ---- end to end: host grids in, loss and gradients out, through the public API
+    e2e = None
+    if not args.no_e2e:
+        h_sigma = torch.from_numpy(sigma).pin_memory()
+        h_albedo = torch.from_numpy(albedo).pin_memory()
+        h_gs = torch.empty_like(h_sigma).pin_memory()
+        h_ga = torch.empty_like(h_albedo).pin_memory()
+        h_loss = torch.empty(1).pin_memory()
+        e2e_ms = []
+        maps.check()
+        for k in range(max(1, args.steps)):
+            flush.zero_()
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            with torch.no_grad():
+                sigma_t.copy_(h_sigma, non_blocking=True)
+                albedo_t.copy_(h_albedo, non_blocking=True)
+            loss = step(100 + k)
+            h_loss.copy_(loss.detach().reshape(1), non_blocking=True)
+            h_gs.copy_(sigma_t.grad, non_blocking=True)
+            h_ga.copy_(albedo_t.grad, non_blocking=True)
+            e1.record(stream)
+            e1.synchronize()
+            e2e_ms.append(e0.elapsed_time(e1))
+        c = maps.check()
+        et = torch.tensor([sum(e2e_ms)], device=dev, dtype=torch.float64)
+        ev = torch.tensor([float(c["vertices"])], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+            dist.all_reduce(ev)
+        e2e = {"value": float(ev.item()) / (float(et.item()) / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h_sigma.numel() * 4 + h_albedo.numel() * 4),
+               "d2h_bytes_per_step": int(h_gs.numel() * 4 + h_ga.numel() * 4 + 4),
+               "ms_per_step": float(et.item()) / max(1, args.steps)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, sample, thr, secs = cpu_sample()
+        cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
+               "sample": sample + f", {secs:.1f} s on {thr} host threads"}
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        c = counters
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+            "config": {"workload": WORKLOAD + ("_small128" if args.small else ""), "grid": list(sigma.shape[:3]),
+                       "image": [H, W], "spp": spp, "max_bounces": wl["max_bounces"], "phase_g": wl["phase_g"],
+                       "transmittance": "ratio tracking", "majorant": "8^3-brick grid", "adjoint": "NEE_DS",
+                       "l2": "flushed between steps (512 MB write)", "parallelism": f"dp{world}"},
+            "e2e": e2e,
+            "gpu_launches": 3 * args.steps,
+            "counters_per_step": {k: v / args.steps for k, v in c.items() if k != "status"},
+            "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                         "peak_source": peaks["source"], "algorithmic_bytes_per_launch": roof[dom]["bytes"],
+                         "launch_ms": roof[dom]["ms"],
+                         "split_ms": {k: roof[k]["ms"] for k in roof}},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------- reference arm --
+def run_reference(args):
+    """The reference's algorithm on the host cores: the oracle (a C++
+    restatement of rendervous's volume GLSL, whose Vulkan runtime cannot run
+    on this machine) on a bounded sample of the same workload per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    oracle.build()
+    for _ in range(args.warmup):
+        cpu_sample()
+    vals, secs = [], 0.0
+    for _ in range(args.steps):
+        v, sample, thr, s = cpu_sample()
+        vals.append(v)
+        secs += s
+    value = statistics.mean(vals)
+    wl = __import__("rendervous_b200.synthetic", fromlist=["x"]).WORKLOADS[WORKLOAD]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(1, args.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generators)",
+        "config": {"workload": WORKLOAD, "grid": [256, 256, 256], "image": [wl["height"], wl["width"]],
+                   "spp": wl["spp"], "max_bounces": wl["max_bounces"], "majorant": "constant (reference)",
+                   "adjoint": "NEE_DS", "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

@@ -99,7 +99,10 @@ typedef struct vrt_camera {
 typedef struct vrt_counters {
     int64_t paths;                   /* paths started */
     int64_t vertices;                /* real scattering collisions */
-    int64_t steps;                   /* tracking steps (free-flight samples), primary and shadow */
+    int64_t steps;                   /* tracking steps (free-flight samples, DDA cells), primary and shadow */
+    int64_t lookups;                 /* sigma lookups (8 node gathers each; DDA: cells) */
+    int64_t reds;                    /* gradient atomic adds issued */
+    int64_t albedo_lookups;          /* albedo grid lookups */
     int64_t status;                  /* device error bits (VRT_E_* as 1 << code) */
 } vrt_counters;
 

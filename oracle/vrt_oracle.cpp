@@ -37,11 +37,25 @@ inline void philox(uint32_t k0, uint32_t k1, const uint32_t c[4], uint32_t o[4])
 }
 
 // Draw k of stream s of path p = word (k & 3) of philox(seed, {k>>2, p_lo, s, p_hi}).
+// Every transmittance estimate draws from a stream of its own, forked from the
+// stream that requests it: the j-th fork of stream s is stream s + 2(j+1)
+// (stream 0 is the path, stream 1 the branch stream of the DRT adjoint, so the
+// two families never meet).  Draws stay i.i.d. uniforms, as in the reference's
+// single Tausworthe stream, and re-forking from a saved state replays a shadow
+// ray exactly (the reference's SAVE_SEED(before_transmittance)).
 struct Rng {
-    uint32_t k0, k1, plo, phi, stream, n;
+    uint32_t k0, k1, plo, phi, stream, n, ntr;
     Rng(uint64_t seed, uint64_t path, uint32_t s)
         : k0((uint32_t)seed), k1((uint32_t)(seed >> 32)), plo((uint32_t)path),
-          phi((uint32_t)(path >> 32)), stream(s), n(0) {}
+          phi((uint32_t)(path >> 32)), stream(s), n(0), ntr(0) {}
+    Rng fork() {
+        Rng r = *this;
+        r.stream = stream + 2u * (1u + ntr);
+        r.n = 0;
+        r.ntr = 0;
+        ++ntr;
+        return r;
+    }
     uint32_t u32() {
         uint32_t c[4] = {n >> 2, plo, stream, phi}, o[4];
         philox(k0, k1, c, o);
@@ -215,10 +229,34 @@ template <typename T> struct Scene {
     // include/vr_majorant.h:1-7.  Mode 0: const[[max sigma, 1e6]] (_objects.py:96-101).
     // Mode 1 (extension): majorant grid of bricks; returns the brick's bound and
     // the distance to leave the brick along w.
+    // Outside the grid's box the bound is 0 (Grid3D is zero there) and the
+    // distance is the one to (re-)enter the box, or 1e6 when w leaves it.
     T majorant(V3<T> x, V3<T> w, T& md) const {
         if (s.majorant_mode == 0) { md = T(1000000.0); return (T)s.global_majorant; }
+        const T inf = std::numeric_limits<T>::infinity();
+        bool inside = true;
+        for (int i = 0; i < 3; ++i) {
+            T q = (x[i] - (T)s.bmin[i]) * (T)s.maj_scale[i];
+            if (!(q >= T(0) && q <= T(s.maj_dims[i]))) inside = false;
+        }
+        if (!inside) {
+            T tn = -inf, tf = inf;
+            for (int i = 0; i < 3; ++i) {
+                T q = (x[i] - (T)s.bmin[i]) * (T)s.maj_scale[i];
+                T v = w[i] * (T)s.maj_scale[i];
+                if (v != T(0)) {
+                    T a = (T(0) - q) / v, b = (T(s.maj_dims[i]) - q) / v;
+                    tn = vmax(tn, vmin(a, b));
+                    tf = vmin(tf, vmax(a, b));
+                } else if (!(q >= T(0) && q <= T(s.maj_dims[i]))) {
+                    tn = inf;
+                }
+            }
+            md = (tn < tf && tn > T(0)) ? vmax(tn, T(1e-6)) : T(1000000.0);
+            return T(0);
+        }
         int c[3];
-        T dist = std::numeric_limits<T>::infinity();
+        T dist = inf;
         for (int i = 0; i < 3; ++i) {
             T q = (x[i] - (T)s.bmin[i]) * (T)s.maj_scale[i];
             T nudge = w[i] > T(0) ? T(1e-4) : (w[i] < T(0) ? T(-1e-4) : T(0));
@@ -340,10 +378,13 @@ template <typename T> struct DDA {
 
     static constexpr double GL = 0.28867513459481288225;  // 1/(2 sqrt 3)
 
+    // The reference stops 1e-4 short of the exit (vr_transmittance_DDA.h:38);
+    // the exact mode (an extension) integrates the whole segment.
     T tau(bool exact, int64_t* steps) {
         T acc = 0, ct = 0;
         T s[2][2][2];
-        while (ct < d - T(0.0001)) {
+        const T stop = exact ? d : d - T(0.0001);
+        while (ct < stop) {
             T nt = vmin(d, vmin(alpha.x, vmin(alpha.y, alpha.z)));
             load_cell(s);
             T dt = nt - ct;
@@ -363,7 +404,8 @@ template <typename T> struct DDA {
     void tau_bw(bool exact, T dL_dtau) {
         T ct = 0;
         T g[2][2][2], g2[2][2][2];
-        while (ct < d - T(0.0001)) {
+        const T stop = exact ? d : d - T(0.0001);
+        while (ct < stop) {
             T nt = vmin(d, vmin(alpha.x, vmin(alpha.y, alpha.z)));
             T dt = nt - ct;
             if (!exact) {
@@ -501,8 +543,10 @@ template <typename T> T transmittance_DT(const Scene<T>& S, Rng& rng, V3<T> x, V
         if (steps) ++*steps;
         x += w * t;
         d -= t;
-        if (dt > md) continue;
+        // the end test precedes the brick-crossing restart (the reference's
+        // order, which the constant majorant never distinguishes)
         if (d <= T(0.0000001)) return T(1);
+        if (dt > md) continue;
         if ((T)rng.uniform() < S.sigma(x) / maj) return T(0);
     }
     return T(1);
@@ -525,8 +569,8 @@ template <typename T> void transmittance_DT_bw(const Scene<T>& S, Rng& rng, V3<T
         T t = vmin(md, dt);
         x += w * t;
         d -= t;
-        if (dt > md) continue;
         if (d <= T(0.0000001)) break;
+        if (dt > md) continue;
         if ((T)rng.uniform() < S.sigma(x) / maj) return;
     }
     x = ini_x;
@@ -539,8 +583,8 @@ template <typename T> void transmittance_DT_bw(const Scene<T>& S, Rng& rng, V3<T
         T t = vmin(md, dt);
         x += w * t;
         d -= t;
-        if (dt > md) continue;
         if (d <= T(0.0000001)) break;
+        if (dt > md) continue;
         rng.advance();
         T Pc = S.sigma(x) / maj;
         T dL_dsigma = -dL_dT / maj / (T(1) - Pc);
@@ -550,17 +594,19 @@ template <typename T> void transmittance_DT_bw(const Scene<T>& S, Rng& rng, V3<T
 
 // include/vr_transmittance.h dispatch over the lowered transmittance map
 template <typename T> T transmittance(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, int64_t* steps) {
+    Rng sr = rng.fork();
     switch (S.s.transmittance_mode) {
-        case 0: return transmittance_RT(S, rng, x, w, steps);
-        case 1: return transmittance_DT(S, rng, x, w, steps);
+        case 0: return transmittance_RT(S, sr, x, w, steps);
+        case 1: return transmittance_DT(S, sr, x, w, steps);
         case 2: return transmittance_DDA(S, x, w, false, steps);
         default: return transmittance_DDA(S, x, w, true, steps);
     }
 }
 template <typename T> void transmittance_bw(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, T dL_dT) {
+    Rng sr = rng.fork();
     switch (S.s.transmittance_mode) {
-        case 0: transmittance_RT_bw(S, rng, x, w, dL_dT); break;
-        case 1: transmittance_DT_bw(S, rng, x, w, dL_dT); break;
+        case 0: transmittance_RT_bw(S, sr, x, w, dL_dT); break;
+        case 1: transmittance_DT_bw(S, sr, x, w, dL_dT); break;
         case 2: transmittance_DDA_bw(S, x, w, false, dL_dT); break;
         default: transmittance_DDA_bw(S, x, w, true, dL_dT); break;
     }
@@ -962,9 +1008,10 @@ template <typename T> void path_integrator_NEE_DRT_bw(const Scene<T>& S, Rng& rn
     x += w * tMin;
     T d = tMax - tMin;
     if (d <= T(0)) return;
-    Rng sec = rng;
+    Rng sec = rng;  // the branch seed (BRANCH_SEED(secondary_seed)) is stream 1
     sec.stream = rng.stream + 1;
     sec.n = 0;
+    sec.ntr = 0;
     Counters dummy;
     T direct_T = transmittance(S, rng, x, w, nullptr);
     V3<T> direct_env = S.environment();

@@ -34,11 +34,26 @@ def _inputs():
     return paths
 
 
+STAMP = LIB + ".stamp"
+
+
+def _digest() -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for p in _inputs():
+        with open(p, "rb") as f:
+            h.update(f.read())
+    h.update(" ".join(NVCC_FLAGS).encode())
+    return h.hexdigest()
+
+
 def up_to_date() -> bool:
-    if not os.path.exists(LIB):
+    """True when libvrt.so was built from exactly the current sources (content
+    hash, so copies of the tree with fresh timestamps do not rebuild)."""
+    if not (os.path.exists(LIB) and os.path.exists(STAMP)):
         return False
-    t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(p) <= t for p in _inputs())
+    with open(STAMP) as f:
+        return f.read().strip() == _digest()
 
 
 def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
@@ -51,6 +66,9 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
     out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("libvrt build failed:\n" + out.stdout + out.stderr)
+    if not extra_flags:
+        with open(STAMP, "w") as f:
+            f.write(_digest())
     if verbose and out.stderr:
         print(out.stderr, file=sys.stderr)
     return LIB

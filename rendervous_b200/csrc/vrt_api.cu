@@ -114,7 +114,7 @@ static int to_dgrid(const vrt_grid& g, int need_c, DGrid& out) {
     for (int i = 0; i < 3; ++i)
         if (g.shape[i] < 2) return VRT_E_BAD_SHAPE;
     if (g.shape[3] < 1 || (need_c > 0 && g.shape[3] != need_c)) return VRT_E_BAD_SHAPE;
-    if (g.strides[3] != 1) return VRT_E_BAD_SHAPE;
+    if (g.shape[3] > 1 && g.strides[3] != 1) return VRT_E_BAD_SHAPE;
     int64_t max_off = 0;
     for (int i = 0; i < 3; ++i) {
         if (g.strides[i] < 0) return VRT_E_BAD_SHAPE;
@@ -256,6 +256,9 @@ int vrt_context_sync(vrt_context* ctx, void* stream, vrt_counters* out) {
         out->paths = (int64_t)h.paths;
         out->vertices = (int64_t)h.vertices;
         out->steps = (int64_t)h.steps;
+        out->lookups = (int64_t)h.lookups;
+        out->reds = (int64_t)h.reds;
+        out->albedo_lookups = (int64_t)h.albedo;
         out->status = (int64_t)h.status;
     }
     for (int code = 1; code < 8; ++code)

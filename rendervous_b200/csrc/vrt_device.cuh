@@ -28,14 +28,27 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1
     return c;
 }
 
+// Each transmittance estimate draws from its own stream: the j-th fork of
+// stream s is stream s + 2(j+1) (stream 0 is the path, stream 1 the DRT
+// adjoint's branch stream).  Re-forking from a saved state replays a shadow
+// ray exactly, which is what the reference's SAVE_SEED(before_transmittance)
+// achieves with its single stream.
 struct Rng {
-    uint32_t k0, k1, plo, phi, stream, n;
+    uint32_t k0, k1, plo, phi, stream, n, ntr;
     uint4 buf;
 
     __device__ __forceinline__ void init(uint64_t seed, uint64_t path, uint32_t s) {
         k0 = (uint32_t)seed; k1 = (uint32_t)(seed >> 32);
         plo = (uint32_t)path; phi = (uint32_t)(path >> 32);
-        stream = s; n = 0;
+        stream = s; n = 0; ntr = 0;
+    }
+    __device__ __forceinline__ Rng fork() {
+        Rng r = *this;
+        r.stream = stream + 2u * (1u + ntr);
+        r.n = 0;
+        r.ntr = 0;
+        ++ntr;
+        return r;
     }
     __device__ __forceinline__ void refill() { buf = philox4x32_10(make_uint4(n >> 2, plo, stream, phi), k0, k1); }
     __device__ __forceinline__ uint32_t u32() {
@@ -49,10 +62,13 @@ struct Rng {
     __device__ __forceinline__ float uniform() {
         return __uint_as_float((u32() & 0x007FFFFFu) | 0x3F800000u) - 1.0f;
     }
-    __device__ __forceinline__ void advance() { ++n; }
-    // restore a saved position (n) of this stream
-    __device__ __forceinline__ void seek(uint32_t pos) {
-        n = pos;
+    __device__ __forceinline__ void advance() { (void)u32(); }  // randoms.h:35-41 advance_random
+    // Position of the stream (draw index and forks taken) for replays.
+    struct Pos { uint32_t n, ntr; };
+    __device__ __forceinline__ Pos pos() const { return Pos{n, ntr}; }
+    __device__ __forceinline__ void seek(Pos p) {
+        n = p.n;
+        ntr = p.ntr;
         if (n & 3u) refill();
     }
 };
@@ -135,7 +151,16 @@ __device__ __forceinline__ float grid_sigma(const DGrid& g, float3 nc) {
 __device__ __forceinline__ float3 normalized(const DMedium& M, float3 x) {
     return make_float3((x.x - M.bmin.x) * M.inv_bsize.x, (x.y - M.bmin.y) * M.inv_bsize.y, (x.z - M.bmin.z) * M.inv_bsize.z);
 }
-__device__ __forceinline__ float sigma(const DMedium& M, float3 x) { return grid_sigma(M.sigma, normalized(M, x)); }
+// Per-thread work tally: free-flight steps, sigma lookups (8 node gathers
+// each), atomic adds and albedo lookups.  Kept in registers, summed per warp.
+struct Tally {
+    uint32_t steps = 0, lookups = 0, reds = 0, albedo = 0;
+};
+
+__device__ __forceinline__ float sigma(const DMedium& M, float3 x, Tally& tl) {
+    ++tl.lookups;
+    return grid_sigma(M.sigma, normalized(M, x));
+}
 
 // Grid3D BACKWARD (include/maps/grid3d.h:39-75): 8 atomic adds per channel.
 __device__ __forceinline__ void red_add(float* p, float v) { atomicAdd(p, v); }
@@ -161,14 +186,16 @@ __device__ __forceinline__ void grid_scatter(const DGrid& g, float3 nc, const fl
         red_add(b + g.sD + g.sH + g.sW + i, d * ax * ay * az);
     }
 }
-__device__ __forceinline__ void sigma_bw(const DMedium& M, float3 x, float dL) {
+__device__ __forceinline__ void sigma_bw(const DMedium& M, float3 x, float dL, Tally& tl) {
     if (dL == 0.0f) return;
+    tl.reds += 8;
     grid_scatter(M.sigma, normalized(M, x), &dL, 1);
 }
 
 // Albedo: const or Grid3D with C 1 (promoted to 3) or 3 (include/vr_scattering_albedo.h).
-__device__ __forceinline__ float3 albedo(const DMedium& M, float3 x) {
+__device__ __forceinline__ float3 albedo(const DMedium& M, float3 x, Tally& tl) {
     if (!M.albedo_is_grid) return M.albedo_const;
+    ++tl.albedo;
     const DGrid& g = M.albedo;
     float3 nc = normalized(M, x);
     if (nc.x < 0.0f || nc.y < 0.0f || nc.z < 0.0f || nc.x >= 1.0f || nc.y >= 1.0f || nc.z >= 1.0f) return f3(0.0f);
@@ -197,8 +224,9 @@ __device__ __forceinline__ float3 albedo(const DMedium& M, float3 x) {
     }
     return o;
 }
-__device__ __forceinline__ void albedo_bw(const DMedium& M, float3 x, float3 dL) {
+__device__ __forceinline__ void albedo_bw(const DMedium& M, float3 x, float3 dL, Tally& tl) {
     if (!M.albedo_is_grid || !M.albedo.grad) return;
+    tl.reds += 8 * M.albedo.C;
     if (M.albedo.C == 1) {
         float g = dL.x + dL.y + dL.z;
         grid_scatter(M.albedo, normalized(M, x), &g, 1);
@@ -214,11 +242,37 @@ __device__ __forceinline__ void albedo_bw(const DMedium& M, float3 x, float3 dL)
 // query returns the brick's bound and the distance to leave the brick.  A
 // point within 1e-4 brick widths of a face is assigned to the brick that w
 // enters, so a ray parked on a face always makes progress.
+// Outside the grid's box the bound is 0 (Grid3D is zero there) and the
+// distance is the one to (re-)enter the box, or 1e6 when w leaves it.
 __device__ __forceinline__ float majorant(const DMedium& M, float3 x, float3 w, float& md) {
     if (M.maj_mode == 0) { md = 1000000.0f; return M.gmaj; }
-    int c[3];
-    float dist = __int_as_float(0x7f800000);
+    const float inf = __int_as_float(0x7f800000);
     const int Md[3] = {M.Mx, M.My, M.Mz};
+    bool inside = true;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float q = (comp(x, i) - comp(M.bmin, i)) * comp(M.maj_scale, i);
+        if (!(q >= 0.0f && q <= (float)Md[i])) inside = false;
+    }
+    if (!inside) {
+        float tn = -inf, tf = inf;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            float q = (comp(x, i) - comp(M.bmin, i)) * comp(M.maj_scale, i);
+            float v = comp(w, i) * comp(M.maj_scale, i);
+            if (v != 0.0f) {
+                float a = (0.0f - q) / v, b = ((float)Md[i] - q) / v;
+                tn = gmax(tn, gmin(a, b));
+                tf = gmin(tf, gmax(a, b));
+            } else if (!(q >= 0.0f && q <= (float)Md[i])) {
+                tn = inf;
+            }
+        }
+        md = (tn < tf && tn > 0.0f) ? gmax(tn, 1e-6f) : 1000000.0f;
+        return 0.0f;
+    }
+    int c[3];
+    float dist = inf;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         float xi = comp(x, i), wi = comp(w, i);

@@ -51,6 +51,9 @@ struct DScratch {
     unsigned long long paths;
     unsigned long long vertices;
     unsigned long long steps;
+    unsigned long long lookups;
+    unsigned long long reds;
+    unsigned long long albedo;
     unsigned int status;           // 1 << VRT_E_* bits
     unsigned int pad;
 };

@@ -42,18 +42,24 @@ __device__ __forceinline__ void primary_ray(const PathSrc& S, uint64_t pid, Rng&
     }
 }
 
-__device__ __forceinline__ void warp_add_counters(DScratch* sc, uint32_t paths, uint32_t verts, uint32_t steps) {
-    unsigned long long p = paths, v = verts, s = steps;
+__device__ __forceinline__ void warp_add_counters(DScratch* sc, uint32_t paths, uint32_t verts, const Tally& tl) {
+    unsigned long long p = paths, v = verts, s = tl.steps, l = tl.lookups, r = tl.reds, a = tl.albedo;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         p += __shfl_down_sync(kFull, p, o);
         v += __shfl_down_sync(kFull, v, o);
         s += __shfl_down_sync(kFull, s, o);
+        l += __shfl_down_sync(kFull, l, o);
+        r += __shfl_down_sync(kFull, r, o);
+        a += __shfl_down_sync(kFull, a, o);
     }
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(&sc->paths, p);
         atomicAdd(&sc->vertices, v);
         atomicAdd(&sc->steps, s);
+        atomicAdd(&sc->lookups, l);
+        atomicAdd(&sc->reds, r);
+        atomicAdd(&sc->albedo, a);
     }
 }
 
@@ -65,7 +71,9 @@ enum : int { SH_DIRECT = 0, SH_ENV = 1, SH_SUN = 2 };
 enum : int { EV_NONE = 0, EV_COLLISION = 1, EV_ESCAPE = 2, EV_SHADOW_DONE = 3 };
 
 struct NeeLane {
-    Rng rng;
+    Rng rng;        // the active stream: the path's, or a shadow ray's fork
+    Rng park;       // the path's stream while a shadow ray runs
+    bool parked;
     float3 x, w, W, R;
     float d;
     int bounces;
@@ -82,11 +90,12 @@ struct NeeLane {
 // Begin a transmittance segment from x0 along dir (the transmittance map's own
 // boundary test, vr_transmittance_RT.h:5-10 / _DT.h:3-8).  DDA segments are
 // deterministic and evaluated inline.
-__device__ __forceinline__ int start_shadow(const DMedium& M, NeeLane& L, float3 x0, float3 dir, uint32_t& steps) {
+__device__ __forceinline__ int start_shadow(const DMedium& M, NeeLane& L, float3 x0, float3 dir, Tally& tl) {
     L.state = ST_SHADOW;
     L.T = 1.0f;
+    Rng child = L.rng.fork();
     if (M.tr_mode >= 2) {
-        L.T = M.tr_mode == 2 ? transmittance_dda<false>(M, x0, dir, steps) : transmittance_dda<true>(M, x0, dir, steps);
+        L.T = M.tr_mode == 2 ? transmittance_dda<false>(M, x0, dir, tl) : transmittance_dda<true>(M, x0, dir, tl);
         return EV_SHADOW_DONE;
     }
     float tMin, tMax;
@@ -94,6 +103,9 @@ __device__ __forceinline__ int start_shadow(const DMedium& M, NeeLane& L, float3
     L.sx = x0 + dir * tMin;
     L.sw = dir;
     L.sd = tMax - tMin;
+    L.park = L.rng;
+    L.rng = child;
+    L.parked = true;
     return EV_NONE;
 }
 
@@ -117,7 +129,8 @@ __global__ void __launch_bounds__(256) k_nee_fw(DMedium M, PathSrc S, uint64_t n
     NeeLane L;
     L.state = ST_DEAD;
     bool exhausted = false;
-    uint32_t n_paths_done = 0, n_verts = 0, n_steps = 0;
+    uint32_t n_paths_done = 0, n_verts = 0;
+    Tally tl;
 
     while (true) {
         // ---- refill dead lanes from the global queue (one atomic per warp)
@@ -146,8 +159,9 @@ __global__ void __launch_bounds__(256) k_nee_fw(DMedium M, PathSrc S, uint64_t n
                     L.bounces = 0;
                     L.steps_path = 0;
                     L.kind = SH_DIRECT;
+                    L.parked = false;
                     ++n_paths_done;
-                    int ev = start_shadow(M, L, L.x, L.w, n_steps);
+                    int ev = start_shadow(M, L, L.x, L.w, tl);
                     if (ev == EV_SHADOW_DONE) {
                         L.R = L.R + L.T * M.env;
                         L.state = L.d > EPS ? ST_PRIMARY : ST_DEAD;
@@ -176,7 +190,7 @@ __global__ void __launch_bounds__(256) k_nee_fw(DMedium M, PathSrc S, uint64_t n
         float md;
         float mj = majorant(M, p, v, md);
         float lg = -logf(1.0f - L.rng.uniform());
-        ++n_steps;
+        ++tl.steps;
         int ev = EV_NONE;
         bool need_sigma = false;
         float m = 0.0f, t = 0.0f;
@@ -217,7 +231,7 @@ __global__ void __launch_bounds__(256) k_nee_fw(DMedium M, PathSrc S, uint64_t n
             }
         }
         if (need_sigma) {
-            float s = sigma(M, prim ? L.x : L.sx);
+            float s = sigma(M, prim ? L.x : L.sx, tl);
             if (prim) {
                 if (L.rng.uniform() >= s / m) {
                     L.d -= t;
@@ -244,15 +258,19 @@ __global__ void __launch_bounds__(256) k_nee_fw(DMedium M, PathSrc S, uint64_t n
         while (ev != EV_NONE) {
             if (ev == EV_COLLISION) {  // vr_path_integrator_NEE.h:41-50
                 ++n_verts;
-                float3 sa = albedo(M, L.x);
+                float3 sa = albedo(M, L.x, tl);
                 L.R = L.R + L.W * (f3(1.0f) - sa) * M.emission;
                 L.W = L.W * sa;
                 float3 wnee;
                 L.pay = environment_sample(M, L.rng, wnee);
                 L.payph = phase(M, L.w, wnee);
                 L.kind = SH_ENV;
-                ev = start_shadow(M, L, L.x, wnee, n_steps);
+                ev = start_shadow(M, L, L.x, wnee, tl);
             } else if (ev == EV_SHADOW_DONE) {
+                if (L.parked) {  // back to the path's stream
+                    L.rng = L.park;
+                    L.parked = false;
+                }
                 if (L.kind == SH_DIRECT) {  // vr_path_integrator_NEE.h:13-14
                     L.R = L.R + L.T * M.env;
                     L.state = ST_PRIMARY;
@@ -263,7 +281,7 @@ __global__ void __launch_bounds__(256) k_nee_fw(DMedium M, PathSrc S, uint64_t n
                         L.pay = M.sun_L;
                         L.payph = phase(M, L.w, M.sun_dir);
                         L.kind = SH_SUN;
-                        ev = start_shadow(M, L, L.x, M.sun_dir, n_steps);
+                        ev = start_shadow(M, L, L.x, M.sun_dir, tl);
                     } else {
                         ev = after_nee(M, L);
                     }
@@ -286,7 +304,7 @@ __global__ void __launch_bounds__(256) k_nee_fw(DMedium M, PathSrc S, uint64_t n
             }
         }
     }
-    warp_add_counters(sc, n_paths_done, n_verts, n_steps);
+    warp_add_counters(sc, n_paths_done, n_verts, tl);
 }
 
 // ------------------------------------------------------------------------
@@ -295,13 +313,13 @@ __global__ void __launch_bounds__(256) k_nee_fw(DMedium M, PathSrc S, uint64_t n
 
 // vr_path_integrator_NEE.h:1-66 (+ directional light, bounce cap)
 __device__ float3 path_nee_seq(const DMedium& M, Rng& rng, float3 x, float3 w, bool only_scatters, uint32_t& verts,
-                               uint32_t& steps, uint32_t* status) {
+                               Tally& tl, uint32_t* status) {
     float tMin, tMax;
     boundary(M, x, w, tMin, tMax);
     x = x + w * tMin;
     float d = tMax - tMin;
     float3 R = f3(0.0f), W = f3(1.0f);
-    if (!only_scatters) R = R + transmittance(M, rng, x, w, steps, status) * M.env;
+    if (!only_scatters) R = R + transmittance(M, rng, x, w, tl, status) * M.env;
     const float EPS = 0.00001f;
     int bounces = 0;
     for (int it = 0; d > EPS; ++it) {
@@ -309,22 +327,22 @@ __device__ float3 path_nee_seq(const DMedium& M, Rng& rng, float3 x, float3 w, b
         float md;
         float m = gmax(EPS, majorant(M, x, w, md));
         float t = -logf(1.0f - rng.uniform()) / m;
-        ++steps;
+        ++tl.steps;
         x = x + w * gmin(t, md);
         if (t > md) { d -= md; continue; }
         if (t > d) break;
-        float s = sigma(M, x);
+        float s = sigma(M, x, tl);
         if (rng.uniform() >= s / m) { d -= t; continue; }
         ++verts;
-        float3 sa = albedo(M, x);
+        float3 sa = albedo(M, x, tl);
         R = R + W * (f3(1.0f) - sa) * M.emission;
         W = W * sa;
         float3 wnee;
         float3 env = environment_sample(M, rng, wnee);
-        float T_nee = transmittance(M, rng, x, wnee, steps, status);
+        float T_nee = transmittance(M, rng, x, wnee, tl, status);
         R = R + W * T_nee * env * phase(M, w, wnee);
         if (M.has_sun) {
-            float T_sun = transmittance(M, rng, x, M.sun_dir, steps, status);
+            float T_sun = transmittance(M, rng, x, M.sun_dir, tl, status);
             R = R + W * T_sun * M.sun_L * phase(M, w, M.sun_dir);
         }
         if (M.max_bounces > 0 && ++bounces >= M.max_bounces) return R;
@@ -337,7 +355,7 @@ __device__ float3 path_nee_seq(const DMedium& M, Rng& rng, float3 x, float3 w, b
 }
 
 // vr_path_integrator_DT.h:7-57
-__device__ float3 path_dt_seq(const DMedium& M, Rng& rng, float3 x, float3 w, uint32_t& verts, uint32_t& steps,
+__device__ float3 path_dt_seq(const DMedium& M, Rng& rng, float3 x, float3 w, uint32_t& verts, Tally& tl,
                               uint32_t* status) {
     float tMin, tMax;
     boundary(M, x, w, tMin, tMax);
@@ -350,14 +368,14 @@ __device__ float3 path_dt_seq(const DMedium& M, Rng& rng, float3 x, float3 w, ui
         float md;
         float m = gmax(0.00000001f, majorant(M, x, w, md));
         float t = -logf(1.0f - rng.uniform()) / m;
-        ++steps;
+        ++tl.steps;
         x = x + w * gmin(t, md);
         if (t > md) { d -= md; continue; }
         if (t > d) break;
-        float s = sigma(M, x);
+        float s = sigma(M, x, tl);
         if (rng.uniform() >= s / m) { d -= t; continue; }
         ++verts;
-        float3 sa = albedo(M, x);
+        float3 sa = albedo(M, x, tl);
         R = R + W * (f3(1.0f) - sa) * M.emission;
         W = W * sa;
         float3 wo = phase_sample(M, rng, w);
@@ -370,8 +388,9 @@ __device__ float3 path_dt_seq(const DMedium& M, Rng& rng, float3 x, float3 w, ui
 }
 
 // vr_path_integrator_DT.h:59-235
-__device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float eps, float3 dL_dR, uint32_t* status) {
-    const uint32_t before_path = rng.n;
+__device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float eps, float3 dL_dR, Tally& tl,
+                           uint32_t* status) {
+    const Rng::Pos before_path = rng.pos();
     const float3 ini_x = x, ini_w = w;
     float tMin, tMax;
     boundary(M, x, w, tMin, tMax);
@@ -389,7 +408,7 @@ __device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float
         x = x + w * gmin(t, md);
         if (t > md) { d -= md; continue; }
         if (t > d) break;
-        float s = sigma(M, x);
+        float s = sigma(M, x, tl);
         float Pc = (s + eps) / m;
         if (rng.uniform() >= Pc) { d -= t; W = W * ((1.0f - s / m) / (1.0f - Pc)); continue; }
         if (s == 0.0f) {
@@ -398,7 +417,7 @@ __device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float
         } else {
             W = W * ((s / m) / Pc);
         }
-        float3 sa = albedo(M, x);
+        float3 sa = albedo(M, x, tl);
         float3 wo = phase_sample(M, rng, w);
         W = W * (sa * 1.0f);
         if (all_less(W, EPS)) { W = f3(0.0f); break; }
@@ -424,18 +443,18 @@ __device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float
         x = x + w * gmin(t, md);
         if (t > md) { d -= md; continue; }
         if (t > d) break;
-        float s = sigma(M, x);
+        float s = sigma(M, x, tl);
         float Pc = (s + eps) / m;
         if (rng.uniform() >= Pc) {
-            sigma_bw(M, x, dot(dL_dW, -W_out * null_W / m / (1.0f - s / m)));
+            sigma_bw(M, x, dot(dL_dW, -W_out * null_W / m / (1.0f - s / m)), tl);
             W = W * ((1.0f - s / m) / (1.0f - Pc));
             d -= t;
             continue;
         }
-        sigma_bw(M, x, dot(dL_dW, s == 0.0f ? W_out : W_out * null_W / s));
+        sigma_bw(M, x, dot(dL_dW, s == 0.0f ? W_out : W_out * null_W / s), tl);
         W = W * (s / m / Pc);
         if (s == 0.0f) break;
-        float3 sa = albedo(M, x);
+        float3 sa = albedo(M, x, tl);
         float3 wo = phase_sample(M, rng, w);
         W = W * sa;
         if (all_less(W, EPS)) return;
@@ -449,8 +468,8 @@ __device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float
 // replay majorant (x1.2 + 2 eps, different from its primal + 2 eps + 0.1);
 // otherwise the replay uses the primal majorant and retraces the primal path.
 __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float eps, float3 dL_dR,
-                               uint32_t* status) {
-    const uint32_t before_path = rng.n;
+                               Tally& tl, uint32_t* status) {
+    const Rng::Pos before_path = rng.pos();
     const float3 ini_x = x, ini_w = w;
     float tMin, tMax;
     boundary(M, x, w, tMin, tMax);
@@ -461,7 +480,6 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
     const float EPS = 0.00000001f;
     bool scattered = false;
     int bounces = 0;
-    uint32_t steps = 0;
     for (int it = 0; d > EPS; ++it) {
         if (it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
@@ -470,7 +488,7 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
         x = x + w * gmin(t, md);
         if (t > md) { d -= md; continue; }
         if (t > d) break;
-        float s = sigma(M, x);
+        float s = sigma(M, x, tl);
         float Pc = (s + eps) / m;
         if (rng.uniform() >= Pc) { d -= t; W = W * ((1.0f - s / m) / (1.0f - Pc)); continue; }
         scattered = true;
@@ -480,16 +498,16 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
         } else {
             W = W * ((s / m) / Pc);
         }
-        float3 sa = albedo(M, x);
+        float3 sa = albedo(M, x, tl);
         float3 added_R = W * (f3(1.0f) - sa) * M.emission;
         W = W * sa;
         float3 wnee;
         float3 env = environment_sample(M, rng, wnee);
-        float T_nee = transmittance(M, rng, x, wnee, steps, status);
+        float T_nee = transmittance(M, rng, x, wnee, tl, status);
         float ph_nee = phase(M, w, wnee);
         added_R = added_R + W * T_nee * env * ph_nee;
         if (M.has_sun) {
-            float T_sun = transmittance(M, rng, x, M.sun_dir, steps, status);
+            float T_sun = transmittance(M, rng, x, M.sun_dir, tl, status);
             added_R = added_R + W * T_sun * M.sun_L * phase(M, w, M.sun_dir);
         }
         if (null_W < EPS) R_after_sp = R_after_sp + added_R;
@@ -519,34 +537,34 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
         x = x + w * gmin(t, md);
         if (t > md) { d -= md; continue; }
         if (t > d) break;
-        float s = sigma(M, x);
+        float s = sigma(M, x, tl);
         float Pc = (s + eps) / m;
         if (rng.uniform() >= Pc) {
-            sigma_bw(M, x, dot(dL_dR, -R / m / (1.0f - s / m)));
+            sigma_bw(M, x, dot(dL_dR, -R / m / (1.0f - s / m)), tl);
             W = W * ((1.0f - s / m) / (1.0f - Pc));
             d -= t;
             continue;
         }
-        sigma_bw(M, x, dot(dL_dR, s < EPS ? R_after_sp / eps : R / s));
+        sigma_bw(M, x, dot(dL_dR, s < EPS ? R_after_sp / eps : R / s), tl);
         W = W * (s / m / Pc);
         if (s < EPS) return;
-        float3 sa = albedo(M, x);
+        float3 sa = albedo(M, x, tl);
         float3 dL_dsa = dL_dR * W * -1.0f * M.emission;
         R = R - W * (f3(1.0f) - sa) * M.emission;
         dL_dsa = dL_dsa + dL_dR * R / make_float3(gmax(EPS, sa.x), gmax(EPS, sa.y), gmax(EPS, sa.z));
         float3 wnee;
         float3 env = environment_sample(M, rng, wnee);
-        const uint32_t before_tr = rng.n;
-        float T_nee = transmittance(M, rng, x, wnee, steps, status);
+        const Rng::Pos before_tr = rng.pos();
+        float T_nee = transmittance(M, rng, x, wnee, tl, status);
         float ph_nee = phase(M, w, wnee);
-        const uint32_t before_sun = rng.n;
+        const Rng::Pos before_sun = rng.pos();
         float T_sun = 0.0f, ph_sun = 0.0f;
         if (M.has_sun) {
-            T_sun = transmittance(M, rng, x, M.sun_dir, steps, status);
+            T_sun = transmittance(M, rng, x, M.sun_dir, tl, status);
             ph_sun = phase(M, w, M.sun_dir);
         }
         float3 wo = phase_sample(M, rng, w);
-        const uint32_t before_next = rng.n;
+        const Rng::Pos before_next = rng.pos();
         W = W * sa;
         float dL_dTnee = dot(dL_dR, W * env * ph_nee);
         R = R - W * T_nee * env * ph_nee;
@@ -555,12 +573,12 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
             dL_dTsun = dot(dL_dR, W * M.sun_L * ph_sun);
             R = R - W * T_sun * M.sun_L * ph_sun;
         }
-        albedo_bw(M, x, dL_dsa);
+        albedo_bw(M, x, dL_dsa, tl);
         rng.seek(before_tr);
-        transmittance_bw(M, rng, x, wnee, dL_dTnee, status);
+        transmittance_bw(M, rng, x, wnee, dL_dTnee, tl, status);
         if (M.has_sun) {
             rng.seek(before_sun);
-            transmittance_bw(M, rng, x, M.sun_dir, dL_dTsun, status);
+            transmittance_bw(M, rng, x, M.sun_dir, dL_dTsun, tl, status);
         }
         rng.seek(before_next);
         if (M.max_bounces > 0 && ++bounces >= M.max_bounces) return;
@@ -573,7 +591,7 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
 // vr_path_integrator_NEE_DRT.h:8-60 sample_transmittance_position (majorant
 // queried at the sample point x + w t)
 __device__ float sample_transmittance_position(const DMedium& M, Rng& rng, float3 x, float3 w, float d, float& sample_t,
-                                               float& weight_t, uint32_t* status) {
+                                               float& weight_t, Tally& tl, uint32_t* status) {
     float Tr = 1.0f, t = 0.0f, res_t = 0.0f, res_dt = 0.0f, C = 0.0f;
     const float EPS = 0.0000001f;
     int it = 0;
@@ -587,7 +605,7 @@ __device__ float sample_transmittance_position(const DMedium& M, Rng& rng, float
         t += dt;
         if (dt >= md - EPS) continue;
         if (t >= d - EPS) break;
-        Tr *= 1.0f - sigma(M, x + w * t) / m;
+        Tr *= 1.0f - sigma(M, x + w * t, tl) / m;
     }
     if (it == kStepCap) raise_status(status, 4);
     weight_t = C;
@@ -596,7 +614,8 @@ __device__ float sample_transmittance_position(const DMedium& M, Rng& rng, float
 }
 
 // vr_path_integrator_NEE_DRT.h:62-270.  The branch seed is Philox stream 1.
-__device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float3 dL_dR, uint32_t* status) {
+__device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float3 dL_dR, Tally& tl,
+                                uint32_t* status) {
     float tMin, tMax;
     boundary(M, x, w, tMin, tMax);
     x = x + w * tMin;
@@ -606,16 +625,17 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
     sec.k0 = rng.k0; sec.k1 = rng.k1; sec.plo = rng.plo; sec.phi = rng.phi;
     sec.stream = rng.stream + 1;
     sec.n = 0;
-    uint32_t steps = 0, verts = 0;
-    (void)transmittance(M, rng, x, w, steps, status);
-    transmittance_bw(M, sec, x, w, dot(dL_dR, M.env), status);
+    sec.ntr = 0;
+    uint32_t verts = 0;
+    (void)transmittance(M, rng, x, w, tl, status);
+    transmittance_bw(M, sec, x, w, dot(dL_dR, M.env), tl, status);
     float3 R = f3(0.0f), W = f3(1.0f);
     float3 res_x = x, res_w = w, res_W = W;
     float res_P = 3.0f, total_weight = 3.0f;
     const float3 ini_x = x, ini_w = w;
     const float ini_d = d;
     const float EPS = 0.00000001f;
-    const uint32_t before_path = rng.n;
+    const Rng::Pos before_path = rng.pos();
     int bounces = 0;
     for (int it = 0; d > EPS; ++it) {
         if (it >= kPathStepCap) { raise_status(status, 4); return; }
@@ -625,17 +645,17 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
         x = x + w * gmin(t, md);
         if (t > md) { d -= md; continue; }
         if (t > d) break;
-        float s = sigma(M, x);
+        float s = sigma(M, x, tl);
         if (rng.uniform() >= s / m) { d -= t; continue; }
-        float3 sa = albedo(M, x);
+        float3 sa = albedo(M, x, tl);
         W = W * sa;
         float3 wnee;
         float3 env = environment_sample(M, rng, wnee);
-        float T_nee = transmittance(M, rng, x, wnee, steps, status);
+        float T_nee = transmittance(M, rng, x, wnee, tl, status);
         float ph_nee = phase(M, w, wnee);
         R = R + W * T_nee * env * ph_nee;
         if (M.has_sun) {
-            float T_sun = transmittance(M, rng, x, M.sun_dir, steps, status);
+            float T_sun = transmittance(M, rng, x, M.sun_dir, tl, status);
             R = R + W * T_sun * M.sun_L * phase(M, w, M.sun_dir);
         }
         bool capped = M.max_bounces > 0 && ++bounces >= M.max_bounces;
@@ -663,23 +683,23 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
         x = x + w * gmin(t, md);
         if (t > md) { d -= md; continue; }
         if (t > d) break;
-        float s = sigma(M, x);
+        float s = sigma(M, x, tl);
         if (rng.uniform() >= s / m) {
-            sigma_bw(M, x, dot(dL_dR, -R / m / (1.0f - s / m)));
+            sigma_bw(M, x, dot(dL_dR, -R / m / (1.0f - s / m)), tl);
             d -= t;
             continue;
         }
         float mis_Ts = s * s / (1.0f + s * s);
         float dL_dsigma = dot(dL_dR, mis_Ts * R / s);
-        float3 sa = albedo(M, x);
+        float3 sa = albedo(M, x, tl);
         W = W * sa;
         float3 wnee;
         float3 env = environment_sample(M, rng, wnee);
-        float T_nee = transmittance(M, rng, x, wnee, steps, status);
+        float T_nee = transmittance(M, rng, x, wnee, tl, status);
         float ph_nee = phase(M, w, wnee);
         float T_sun = 0.0f, ph_sun = 0.0f;
         if (M.has_sun) {
-            T_sun = transmittance(M, rng, x, M.sun_dir, steps, status);
+            T_sun = transmittance(M, rng, x, M.sun_dir, tl, status);
             ph_sun = phase(M, w, M.sun_dir);
         }
         bool capped = M.max_bounces > 0 && ++bounces >= M.max_bounces;
@@ -691,9 +711,9 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
             dL_dTsun = dot(dL_dR, W * M.sun_L * ph_sun);
             R = R - W * T_sun * M.sun_L * ph_sun;
         }
-        sigma_bw(M, x, dL_dsigma);
-        transmittance_bw(M, sec, x, wnee, dL_dTnee, status);
-        if (M.has_sun) transmittance_bw(M, sec, x, M.sun_dir, dL_dTsun, status);
+        sigma_bw(M, x, dL_dsigma, tl);
+        transmittance_bw(M, sec, x, wnee, dL_dTnee, tl, status);
+        if (M.has_sun) transmittance_bw(M, sec, x, M.sun_dir, dL_dTsun, tl, status);
         w = wo;
         boundary(M, x, w, tMin, d);
         rng.advance();
@@ -701,18 +721,18 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
     }
     boundary(M, res_x, res_w, tMin, d);
     float s_t, weight_t;
-    sample_transmittance_position(M, rng, res_x, res_w, d, s_t, weight_t, status);
+    sample_transmittance_position(M, rng, res_x, res_w, d, s_t, weight_t, tl, status);
     float3 xs = res_x + res_w * s_t;
     float3 ls_dir;
     float3 Ls_env = environment_sample(M, rng, ls_dir);
-    float3 Ls = transmittance(M, rng, xs, ls_dir, steps, status) * Ls_env * phase(M, res_w, ls_dir);
-    if (M.has_sun) Ls = Ls + transmittance(M, rng, xs, M.sun_dir, steps, status) * M.sun_L * phase(M, res_w, M.sun_dir);
+    float3 Ls = transmittance(M, rng, xs, ls_dir, tl, status) * Ls_env * phase(M, res_w, ls_dir);
+    if (M.has_sun) Ls = Ls + transmittance(M, rng, xs, M.sun_dir, tl, status) * M.sun_L * phase(M, res_w, M.sun_dir);
     float3 ws = phase_sample(M, rng, res_w);
-    Ls = Ls + 1.0f * path_nee_seq(M, rng, xs, ws, true, verts, steps, status);
-    Ls = Ls * res_W * weight_t * albedo(M, xs);
-    float sigma_xs = sigma(M, xs);
+    Ls = Ls + 1.0f * path_nee_seq(M, rng, xs, ws, true, verts, tl, status);
+    Ls = Ls * res_W * weight_t * albedo(M, xs, tl);
+    float sigma_xs = sigma(M, xs, tl);
     float mis_T = 1.0f / (1.0f + sigma_xs * sigma_xs);
-    sigma_bw(M, xs, dot(dL_dR, Ls) * mis_T * total_weight / res_P);
+    sigma_bw(M, xs, dot(dL_dR, Ls) * mis_T * total_weight / res_P, tl);
 }
 
 // ------------------------------------------------------------------------
@@ -720,7 +740,8 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
 // ------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_dt_fw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, float* out,
                                                 float scale, DScratch* sc) {
-    uint32_t paths = 0, verts = 0, steps = 0;
+    uint32_t paths = 0, verts = 0;
+    Tally tl;
     for (uint64_t pid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; pid < n_paths;
          pid += (uint64_t)gridDim.x * blockDim.x) {
         Rng rng;
@@ -728,7 +749,7 @@ __global__ void __launch_bounds__(256) k_dt_fw(DMedium M, PathSrc S, uint64_t n_
         float3 x, w;
         long long oidx;
         primary_ray(S, pid, rng, x, w, oidx);
-        float3 R = path_dt_seq(M, rng, x, w, verts, steps, &sc->status);
+        float3 R = path_dt_seq(M, rng, x, w, verts, tl, &sc->status);
         ++paths;
         if (S.is_camera) {
             atomicAdd(out + 3 * oidx + 0, R.x * scale);
@@ -740,13 +761,14 @@ __global__ void __launch_bounds__(256) k_dt_fw(DMedium M, PathSrc S, uint64_t n_
             out[3 * oidx + 2] = R.z;
         }
     }
-    warp_add_counters(sc, paths, verts, steps);
+    warp_add_counters(sc, paths, verts, tl);
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_path_bw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, const float* dL,
                                                   float div, DScratch* sc) {
     uint32_t paths = 0;
+    Tally tl;
     for (uint64_t pid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; pid < n_paths;
          pid += (uint64_t)gridDim.x * blockDim.x) {
         Rng rng;
@@ -756,11 +778,11 @@ __global__ void __launch_bounds__(256) k_path_bw(DMedium M, PathSrc S, uint64_t 
         primary_ray(S, pid, rng, x, w, oidx);
         float3 g = ld3(dL + 3 * oidx) / div;
         ++paths;
-        if (MODE == 0) path_nee_ds_bw(M, rng, x, w, M.ds_eps, g, &sc->status);
-        else if (MODE == 1) path_dt_bw(M, rng, x, w, M.ds_eps, g, &sc->status);
-        else path_nee_drt_bw(M, rng, x, w, g, &sc->status);
+        if (MODE == 0) path_nee_ds_bw(M, rng, x, w, M.ds_eps, g, tl, &sc->status);
+        else if (MODE == 1) path_dt_bw(M, rng, x, w, M.ds_eps, g, tl, &sc->status);
+        else path_nee_drt_bw(M, rng, x, w, g, tl, &sc->status);
     }
-    warp_add_counters(sc, paths, 0, 0);
+    warp_add_counters(sc, paths, 0, tl);
 }
 
 // ------------------------------------------------------------------------

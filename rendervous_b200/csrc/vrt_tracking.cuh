@@ -128,25 +128,35 @@ struct DDA {
 
     static constexpr float kGL = 0.28867513459481288225f;  // 1 / (2 sqrt 3)
 
-    // tau over the segment; counts cells in *cells
+    // tau over the segment; one step and one (8-corner) lookup per cell
     template <bool EXACT>
-    __device__ __forceinline__ float tau(const DGrid& g, uint32_t& cells) {
-        float acc = 0.0f, ct = 0.0f;
+    __device__ __forceinline__ float tau(const DGrid& g, Tally& tl) {
+        // compensated (Kahan) sum of the per-cell integrals
+        float acc = 0.0f, comp_err = 0.0f, ct = 0.0f;
         load_all(g);
         int it = 0;
-        while (ct < d - 0.0001f && it < kStepCap) {
+        // the reference stops 1e-4 short of the exit (vr_transmittance_DDA.h:38);
+        // the exact mode integrates the whole segment
+        const float stop = EXACT ? d : d - 0.0001f;
+        while (ct < stop && it < kStepCap) {
             float nt = gmin(d, gmin(alpha.x, gmin(alpha.y, alpha.z)));
             float dt = nt - ct;
+            float term;
             if (!EXACT) {
-                acc += interp(ialpha(mixf(ct, nt, 0.5f))) * dt;
+                term = interp(ialpha(mixf(ct, nt, 0.5f))) * dt;
             } else {
                 float mid = mixf(ct, nt, 0.5f), h = dt * kGL;
-                acc += (interp(ialpha(mid - h)) + interp(ialpha(mid + h))) * (dt * 0.5f);
+                term = (interp(ialpha(mid - h)) + interp(ialpha(mid + h))) * (dt * 0.5f);
             }
+            float yk = term - comp_err;
+            float tk = acc + yk;
+            comp_err = (tk - acc) - yk;
+            acc = tk;
             ct = nt;
             int axis = advance_cell();
             shift_load(g, axis);
-            ++cells;
+            ++tl.steps;
+            ++tl.lookups;
             ++it;
         }
         return acc;
@@ -190,13 +200,14 @@ struct DDA {
     // vr_transmittance_DDA.h:121-153 second march: dL/dsigma per corner; the
     // face shared with the next cell stays in registers.
     template <bool EXACT>
-    __device__ __forceinline__ void scatter(const DGrid& g, float dL_dtau) {
+    __device__ __forceinline__ void scatter(const DGrid& g, float dL_dtau, Tally& tl) {
         float acc[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) acc[k] = 0.0f;
         float ct = 0.0f;
         int it = 0;
-        while (ct < d - 0.0001f && it < kStepCap) {
+        const float stop = EXACT ? d : d - 0.0001f;
+        while (ct < stop && it < kStepCap) {
             float nt = gmin(d, gmin(alpha.x, gmin(alpha.y, alpha.z)));
             float dt = nt - ct;
             if (!EXACT) {
@@ -218,8 +229,10 @@ struct DDA {
                 if (sz > 0) carry_z<4>(g, acc); else if (sz < 0) carry_z<0>(g, acc);
                 alpha.z += alpha_inc.z; cz += sz;
             }
+            tl.reds += 4;
             ++it;
         }
+        tl.reds += 4;
         // acc now holds the corners of the cell the march stopped in (the face
         // carried over from the last cell plus zeros): flush at these indices.
 #pragma unroll
@@ -228,27 +241,26 @@ struct DDA {
 };
 
 template <bool EXACT>
-__device__ __forceinline__ float transmittance_dda(const DMedium& M, float3 x, float3 w, uint32_t& cells) {
+__device__ __forceinline__ float transmittance_dda(const DMedium& M, float3 x, float3 w, Tally& tl) {
     DDA q;
     if (!q.init(M, x, w)) return 1.0f;
-    return expf(-q.tau<EXACT>(M.sigma, cells));
+    return expf(-q.tau<EXACT>(M.sigma, tl));
 }
 template <bool EXACT>
-__device__ __forceinline__ void transmittance_dda_bw(const DMedium& M, float3 x, float3 w, float dL_dT) {
+__device__ __forceinline__ void transmittance_dda_bw(const DMedium& M, float3 x, float3 w, float dL_dT, Tally& tl) {
     if (dL_dT == 0.0f || !M.sigma.grad) return;
     DDA q;
     if (!q.init(M, x, w)) return;
-    uint32_t cells = 0;
-    float tau = q.tau<EXACT>(M.sigma, cells);
+    float tau = q.tau<EXACT>(M.sigma, tl);
     float T = expf(-tau);
     q.reset(M);
-    q.scatter<EXACT>(M.sigma, -dL_dT * T);
+    q.scatter<EXACT>(M.sigma, -dL_dT * T, tl);
 }
 
 // vr_transmittance_RT.h:1-49.  The "grid crossing" branch restarts at a
 // majorant-brick face without a collision; it cannot trigger with the
 // constant majorant (distance 1e6).
-__device__ __forceinline__ float transmittance_rt(const DMedium& M, Rng& rng, float3 x, float3 w, uint32_t& steps,
+__device__ __forceinline__ float transmittance_rt(const DMedium& M, Rng& rng, float3 x, float3 w, Tally& tl,
                                                   uint32_t* status) {
     float T = 1.0f;
     float tMin, tMax;
@@ -259,13 +271,13 @@ __device__ __forceinline__ float transmittance_rt(const DMedium& M, Rng& rng, fl
         float md;
         float maj = gmax(0.0000001f, majorant(M, x, w, md));
         float t = -logf(1.0f - rng.uniform()) / maj;
-        ++steps;
+        ++tl.steps;
         if (md < d && t > md) { x = x + w * md; d -= md; continue; }
         float dt = gmin(t, gmin(d, md));
         x = x + w * dt;
         d -= dt;
         if (d <= 0.0000001f) return T;
-        T *= (1.0f - sigma(M, x) / maj);
+        T *= (1.0f - sigma(M, x, tl) / maj);
         if (T < 0.01f) {
             if (rng.uniform() < 1.0f - T) return 0.0f;
             T = 1.0f;
@@ -277,7 +289,7 @@ __device__ __forceinline__ float transmittance_rt(const DMedium& M, Rng& rng, fl
 
 // vr_transmittance_RT.h:51-141
 __device__ __forceinline__ void transmittance_rt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float dL_dT,
-                                                    uint32_t* status) {
+                                                    Tally& tl, uint32_t* status) {
     if (dL_dT == 0.0f) return;
     float tMin, tMax;
     if (!boundary(M, x, w, tMin, tMax)) return;
@@ -287,7 +299,7 @@ __device__ __forceinline__ void transmittance_rt_bw(const DMedium& M, Rng& rng, 
     float d = tMax - tMin;
     const float3 ini_x = x;
     const float ini_d = d;
-    const uint32_t before = rng.n;
+    const Rng::Pos before = rng.pos();
     int it = 0;
     for (; it < kStepCap; ++it) {
         float md;
@@ -298,7 +310,7 @@ __device__ __forceinline__ void transmittance_rt_bw(const DMedium& M, Rng& rng, 
         x = x + w * dt;
         d -= dt;
         if (d <= EPS) break;
-        T *= (1.0f - sigma(M, x) / maj);
+        T *= (1.0f - sigma(M, x, tl) / maj);
         if (T < 0.1f) {
             if (rng.uniform() < 1.0f - T) return;
             T = 1.0f;
@@ -319,9 +331,9 @@ __device__ __forceinline__ void transmittance_rt_bw(const DMedium& M, Rng& rng, 
         x = x + w * dt;
         d -= dt;
         if (d <= EPS) break;
-        float r = (1.0f - sigma(M, x) / maj);
+        float r = (1.0f - sigma(M, x, tl) / maj);
         T *= r;
-        sigma_bw(M, x, -out_T * dL_dT / maj / r);
+        sigma_bw(M, x, -out_T * dL_dT / maj / r, tl);
         if (T < 0.1f) {
             rng.advance();
             T = 1.0f;
@@ -330,7 +342,7 @@ __device__ __forceinline__ void transmittance_rt_bw(const DMedium& M, Rng& rng, 
 }
 
 // vr_transmittance_DT.h:1-28
-__device__ __forceinline__ float transmittance_dt(const DMedium& M, Rng& rng, float3 x, float3 w, uint32_t& steps,
+__device__ __forceinline__ float transmittance_dt(const DMedium& M, Rng& rng, float3 x, float3 w, Tally& tl,
                                                   uint32_t* status) {
     float tMin, tMax;
     if (!boundary(M, x, w, tMin, tMax)) return 1.0f;
@@ -341,12 +353,14 @@ __device__ __forceinline__ float transmittance_dt(const DMedium& M, Rng& rng, fl
         float maj = gmax(0.0000001f, majorant(M, x, w, md));
         float dt = -logf(1.0f - rng.uniform()) / maj;
         float t = gmin(md, dt);
-        ++steps;
+        ++tl.steps;
         x = x + w * t;
         d -= t;
-        if (dt > md) continue;
+        // the end test precedes the brick-crossing restart (the reference's
+        // order, which the constant majorant never distinguishes)
         if (d <= 0.0000001f) return 1.0f;
-        if (rng.uniform() < sigma(M, x) / maj) return 0.0f;
+        if (dt > md) continue;
+        if (rng.uniform() < sigma(M, x, tl) / maj) return 0.0f;
     }
     raise_status(status, 4);
     return 1.0f;
@@ -354,7 +368,7 @@ __device__ __forceinline__ float transmittance_dt(const DMedium& M, Rng& rng, fl
 
 // vr_transmittance_DT.h:30-90
 __device__ __forceinline__ void transmittance_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float dL_dT,
-                                                    uint32_t* status) {
+                                                    Tally& tl, uint32_t* status) {
     if (dL_dT == 0.0f) return;
     float tMin, tMax;
     if (!boundary(M, x, w, tMin, tMax)) return;
@@ -362,7 +376,7 @@ __device__ __forceinline__ void transmittance_dt_bw(const DMedium& M, Rng& rng, 
     float d = tMax - tMin;
     const float3 ini_x = x;
     const float ini_d = d;
-    const uint32_t before = rng.n;
+    const Rng::Pos before = rng.pos();
     int it = 0;
     for (; it < kStepCap; ++it) {
         float md;
@@ -371,9 +385,9 @@ __device__ __forceinline__ void transmittance_dt_bw(const DMedium& M, Rng& rng, 
         float t = gmin(md, dt);
         x = x + w * t;
         d -= t;
-        if (dt > md) continue;
         if (d <= 0.0000001f) break;
-        if (rng.uniform() < sigma(M, x) / maj) return;
+        if (dt > md) continue;
+        if (rng.uniform() < sigma(M, x, tl) / maj) return;
     }
     if (it == kStepCap) { raise_status(status, 4); return; }
     x = ini_x;
@@ -386,31 +400,34 @@ __device__ __forceinline__ void transmittance_dt_bw(const DMedium& M, Rng& rng, 
         float t = gmin(md, dt);
         x = x + w * t;
         d -= t;
-        if (dt > md) continue;
         if (d <= 0.0000001f) break;
+        if (dt > md) continue;
         rng.advance();
-        float Pc = sigma(M, x) / maj;
-        sigma_bw(M, x, -dL_dT / maj / (1.0f - Pc));
+        float Pc = sigma(M, x, tl) / maj;
+        sigma_bw(M, x, -dL_dT / maj / (1.0f - Pc), tl);
     }
 }
 
-// include/vr_transmittance.h dispatch over the medium's transmittance map
-__device__ __forceinline__ float transmittance(const DMedium& M, Rng& rng, float3 x, float3 w, uint32_t& steps,
+// include/vr_transmittance.h dispatch over the medium's transmittance map; each
+// call draws from a fork of the caller's stream
+__device__ __forceinline__ float transmittance(const DMedium& M, Rng& rng, float3 x, float3 w, Tally& tl,
                                                uint32_t* status) {
+    Rng sr = rng.fork();
     switch (M.tr_mode) {
-        case 0: return transmittance_rt(M, rng, x, w, steps, status);
-        case 1: return transmittance_dt(M, rng, x, w, steps, status);
-        case 2: return transmittance_dda<false>(M, x, w, steps);
-        default: return transmittance_dda<true>(M, x, w, steps);
+        case 0: return transmittance_rt(M, sr, x, w, tl, status);
+        case 1: return transmittance_dt(M, sr, x, w, tl, status);
+        case 2: return transmittance_dda<false>(M, x, w, tl);
+        default: return transmittance_dda<true>(M, x, w, tl);
     }
 }
 __device__ __forceinline__ void transmittance_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float dL_dT,
-                                                 uint32_t* status) {
+                                                 Tally& tl, uint32_t* status) {
+    Rng sr = rng.fork();
     switch (M.tr_mode) {
-        case 0: transmittance_rt_bw(M, rng, x, w, dL_dT, status); break;
-        case 1: transmittance_dt_bw(M, rng, x, w, dL_dT, status); break;
-        case 2: transmittance_dda_bw<false>(M, x, w, dL_dT); break;
-        default: transmittance_dda_bw<true>(M, x, w, dL_dT); break;
+        case 0: transmittance_rt_bw(M, sr, x, w, dL_dT, tl, status); break;
+        case 1: transmittance_dt_bw(M, sr, x, w, dL_dT, tl, status); break;
+        case 2: transmittance_dda_bw<false>(M, x, w, dL_dT, tl); break;
+        default: transmittance_dda_bw<true>(M, x, w, dL_dT, tl); break;
     }
 }
 

@@ -10,56 +10,71 @@
 
 namespace vrt {
 
+__device__ __forceinline__ void warp_tally(DScratch* sc, uint32_t count, const Tally& tl) {
+    unsigned long long p = count, s = tl.steps, l = tl.lookups, r = tl.reds;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        p += __shfl_down_sync(0xffffffffu, p, o);
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        l += __shfl_down_sync(0xffffffffu, l, o);
+        r += __shfl_down_sync(0xffffffffu, r, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&sc->paths, p);
+        atomicAdd(&sc->steps, s);
+        atomicAdd(&sc->lookups, l);
+        atomicAdd(&sc->reds, r);
+    }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(256) k_transmittance_fw(DMedium M, const float* __restrict__ rays, int64_t n,
                                                            uint64_t seed, float* __restrict__ T, DScratch* sc) {
-    uint32_t steps = 0, count = 0;
+    uint32_t count = 0;
+    Tally tl;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const float2* r2 = reinterpret_cast<const float2*>(rays + 6 * i);  // rows are 8-byte aligned
         float2 a = __ldg(r2), b = __ldg(r2 + 1), c = __ldg(r2 + 2);
         float3 x = make_float3(a.x, a.y, b.x), w = make_float3(b.y, c.x, c.y);
         float v;
-        if (MODE == 2) v = transmittance_dda<false>(M, x, w, steps);
-        else if (MODE == 3) v = transmittance_dda<true>(M, x, w, steps);
+        if (MODE == 2) v = transmittance_dda<false>(M, x, w, tl);
+        else if (MODE == 3) v = transmittance_dda<true>(M, x, w, tl);
         else {
-            Rng rng;
-            rng.init(seed, (uint64_t)i, 0);
-            v = MODE == 0 ? transmittance_rt(M, rng, x, w, steps, &sc->status)
-                          : transmittance_dt(M, rng, x, w, steps, &sc->status);
+            Rng path;
+            path.init(seed, (uint64_t)i, 0);
+            Rng rng = path.fork();  // as the dispatch of a path integrator would
+            v = MODE == 0 ? transmittance_rt(M, rng, x, w, tl, &sc->status)
+                          : transmittance_dt(M, rng, x, w, tl, &sc->status);
         }
         T[i] = v;
         ++count;
     }
-    unsigned long long s = steps, p = count;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        s += __shfl_down_sync(0xffffffffu, s, o);
-        p += __shfl_down_sync(0xffffffffu, p, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&sc->steps, s);
-        atomicAdd(&sc->paths, p);
-    }
+    warp_tally(sc, count, tl);
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_transmittance_bw(DMedium M, const float* __restrict__ rays, int64_t n,
                                                            uint64_t seed, const float* __restrict__ dL_dT,
                                                            DScratch* sc) {
+    uint32_t count = 0;
+    Tally tl;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const float2* r2 = reinterpret_cast<const float2*>(rays + 6 * i);
         float2 a = __ldg(r2), b = __ldg(r2 + 1), c = __ldg(r2 + 2);
         float3 x = make_float3(a.x, a.y, b.x), w = make_float3(b.y, c.x, c.y);
         float g = __ldg(dL_dT + i);
-        if (MODE == 2) transmittance_dda_bw<false>(M, x, w, g);
-        else if (MODE == 3) transmittance_dda_bw<true>(M, x, w, g);
+        if (MODE == 2) transmittance_dda_bw<false>(M, x, w, g, tl);
+        else if (MODE == 3) transmittance_dda_bw<true>(M, x, w, g, tl);
         else {
-            Rng rng;
-            rng.init(seed, (uint64_t)i, 0);
-            if (MODE == 0) transmittance_rt_bw(M, rng, x, w, g, &sc->status);
-            else transmittance_dt_bw(M, rng, x, w, g, &sc->status);
+            Rng path;
+            path.init(seed, (uint64_t)i, 0);
+            Rng rng = path.fork();
+            if (MODE == 0) transmittance_rt_bw(M, rng, x, w, g, tl, &sc->status);
+            else transmittance_dt_bw(M, rng, x, w, g, tl, &sc->status);
         }
+        ++count;
     }
+    warp_tally(sc, count, tl);
 }
 
 static int grid_for(int64_t n) {

@@ -136,16 +136,16 @@ def _fill_grid(g, t: torch.Tensor, grad: torch.Tensor | None):
         raise TypeError("grids are float32")
     if not t.is_cuda:
         raise ValueError("grid tensors must be CUDA tensors (there is no CPU path)")
-    if t.stride(3) != 1:
+    if t.shape[3] > 1 and t.stride(3) != 1:
         raise ValueError("grid channel stride must be 1")
     g.data = _lib.fptr(t)
     if grad is not None:
-        if grad.shape != t.shape or grad.stride() != t.stride():
+        if grad.shape != t.shape or grad.stride()[:3] != t.stride()[:3]:
             raise ValueError("grad must match the grid's shape and strides")
         g.grad = _lib.fptr(grad)
     for i in range(4):
         g.shape[i] = int(t.shape[i])
-        g.strides[i] = int(t.stride(i))
+        g.strides[i] = int(t.stride(i)) if i < 3 else 1
 
 
 def _const_values(m, n: int) -> tuple:
