@@ -143,6 +143,20 @@ int vrt_transmittance_fw(vrt_context* ctx, const vrt_medium* m, int32_t mode, co
 int vrt_transmittance_bw(vrt_context* ctx, const vrt_medium* m, int32_t mode, const float* rays, int64_t n,
                          uint64_t seed, const float* dL_dT, void* stream);
 
+/* Transmittance forward for callers that cannot allocate device memory (no
+   counterpart in the reference).  Same result as vrt_transmittance_fw, but it
+   needs no vrt_context: with brick > 0 and a tracking mode (RT, DT) it builds
+   the brick^3 majorant grid of m->sigma into a fixed array inside libvrt.so
+   and tracks against it; with brick == 0 it uses m's own majorant.  The array
+   holds at most 64^3 bricks (1 MiB, kept on every device that loads the
+   library until exit); larger grids return VRT_E_BAD_SHAPE.  All calls share
+   the array, so calls that overlap on the GPU race.  The first call on a
+   device looks up the array's address; make it before any stream capture.
+   Device-side counters and the error word are cleared per call and not
+   reported. */
+int vrt_transmittance_fw_noalloc(const vrt_medium* m, int32_t mode, int32_t brick, const float* rays, int64_t n,
+                                 uint64_t seed, float* T, void* stream);
+
 /* Path integrator as a map on rays [n,6] -> R [n,3] (DeltatrackingPathIntegrator,
    DeltatrackingNEEPathIntegrator, DRTPathIntegrator, _maps.py:2886-3022; path i
    uses Philox path id i).  Backward accumulates into sigma.grad and albedo.grad. */
