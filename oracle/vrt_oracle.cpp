@@ -117,6 +117,23 @@ struct Counters {
     int64_t paths = 0, vertices = 0, steps = 0;
 };
 
+// Optical distance of the current free flight.  With a piecewise-constant
+// majorant the flight continues across a majorant-brick face with the optical
+// depth it has left (exponential lengths are memoryless), so a new draw is
+// taken only after the previous one ended at a candidate collision or at the
+// end of the segment.  With the reference's constant majorant (distance 1e6)
+// no flight ever crosses a face and every step draws, as in the reference.
+template <typename T> struct Flight {
+    T tau = T(-1);
+    int it = 0;
+    T sample(Rng& rng) {
+        if (tau < T(0)) tau = -std::log(T(1) - (T)rng.uniform());
+        return tau;
+    }
+    void cross(T m, T md) { tau -= m * md; }
+    void used() { tau = T(-1); }
+};
+
 // ---------------------------------------------------------------------------
 // include/maths.h:11-26 intersect_ray_box and :28-38 ray_box_intersection
 // ---------------------------------------------------------------------------
@@ -245,7 +262,8 @@ template <typename T> struct Scene {
                 T q = (x[i] - (T)s.bmin[i]) * (T)s.maj_scale[i];
                 T v = w[i] * (T)s.maj_scale[i];
                 if (v != T(0)) {
-                    T a = (T(0) - q) / v, b = (T(s.maj_dims[i]) - q) / v;
+                    T rv = T(1) / v;
+                    T a = (T(0) - q) * rv, b = (T(s.maj_dims[i]) - q) * rv;
                     tn = vmax(tn, vmin(a, b));
                     tf = vmin(tf, vmax(a, b));
                 } else if (!(q >= T(0) && q <= T(s.maj_dims[i]))) {
@@ -264,7 +282,8 @@ template <typename T> struct Scene {
             ci = std::min(std::max(ci, 0), s.maj_dims[i] - 1);
             c[i] = ci;
             T v = w[i] * (T)s.maj_scale[i];
-            T di = v > T(0) ? (T(ci + 1) - q) / v : (v < T(0) ? (T(ci) - q) / v : std::numeric_limits<T>::infinity());
+            T rv = T(1) / v;  // face distances use a correctly rounded reciprocal
+            T di = v > T(0) ? (T(ci + 1) - q) * rv : (v < T(0) ? (T(ci) - q) * rv : std::numeric_limits<T>::infinity());
             dist = vmin(dist, di);
         }
         md = vmax(dist, T(1e-6));
@@ -458,12 +477,13 @@ template <typename T> T transmittance_RT(const Scene<T>& S, Rng& rng, V3<T> x, V
     if (!S.boundary(x, w, tMin, tMax)) return Tr;
     x += w * tMin;
     T d = tMax - tMin;
-    for (int it = 0; it < (1 << 24); ++it) {
+    for (Flight<T> ff; ff.it < (1 << 24); ++ff.it) {
         T md;
         T maj = vmax(T(0.0000001), S.majorant(x, w, md));
-        T t = -std::log(T(1) - (T)rng.uniform()) / maj;
+        T t = ff.sample(rng) / maj;
         if (steps) ++*steps;
-        if (md < d && t > md) { x += w * md; d -= md; continue; }  // grid crossing
+        if (md < d && t > md) { x += w * md; d -= md; ff.cross(maj, md); continue; }  // grid crossing
+        ff.used();
         T dt = vmin(t, vmin(d, md));
         x += w * dt;
         d -= dt;
@@ -489,11 +509,12 @@ template <typename T> void transmittance_RT_bw(const Scene<T>& S, Rng& rng, V3<T
     V3<T> ini_x = x;
     T ini_d = d;
     Rng before = rng;
-    for (int it = 0; it < (1 << 24); ++it) {
+    for (Flight<T> ff; ff.it < (1 << 24); ++ff.it) {
         T md;
         T maj = vmax(EPS, S.majorant(x, w, md) + T(0.1));
-        T t = -std::log(T(1) - (T)rng.uniform()) / maj;
-        if (md < d && t > md) { x += w * md; d -= md; continue; }  // grid crossing
+        T t = ff.sample(rng) / maj;
+        if (md < d && t > md) { x += w * md; d -= md; ff.cross(maj, md); continue; }  // grid crossing
+        ff.used();
         T dt = vmin(t, vmin(d, md));
         x += w * dt;
         d -= dt;
@@ -509,11 +530,12 @@ template <typename T> void transmittance_RT_bw(const Scene<T>& S, Rng& rng, V3<T
     rng = before;
     x = ini_x;
     d = ini_d;
-    for (int it = 0; it < (1 << 24); ++it) {
+    for (Flight<T> ff; ff.it < (1 << 24); ++ff.it) {
         T md;
         T maj = vmax(EPS, S.majorant(x, w, md) + T(0.1));
-        T t = -std::log(T(1) - (T)rng.uniform()) / maj;
-        if (md < d && t > md) { x += w * md; d -= md; continue; }  // grid crossing
+        T t = ff.sample(rng) / maj;
+        if (md < d && t > md) { x += w * md; d -= md; ff.cross(maj, md); continue; }  // grid crossing
+        ff.used();
         T dt = vmin(t, vmin(d, md));
         x += w * dt;
         d -= dt;
@@ -535,10 +557,10 @@ template <typename T> T transmittance_DT(const Scene<T>& S, Rng& rng, V3<T> x, V
     if (!S.boundary(x, w, tMin, tMax)) return T(1);
     x += w * tMin;
     T d = tMax - tMin;
-    for (int it = 0; it < (1 << 24); ++it) {
+    for (Flight<T> ff; ff.it < (1 << 24); ++ff.it) {
         T md;
         T maj = vmax(T(0.0000001), S.majorant(x, w, md));
-        T dt = -std::log(T(1) - (T)rng.uniform()) / maj;
+        T dt = ff.sample(rng) / maj;
         T t = vmin(md, dt);
         if (steps) ++*steps;
         x += w * t;
@@ -546,7 +568,8 @@ template <typename T> T transmittance_DT(const Scene<T>& S, Rng& rng, V3<T> x, V
         // the end test precedes the brick-crossing restart (the reference's
         // order, which the constant majorant never distinguishes)
         if (d <= T(0.0000001)) return T(1);
-        if (dt > md) continue;
+        if (dt > md) { ff.cross(maj, md); continue; }
+        ff.used();
         if ((T)rng.uniform() < S.sigma(x) / maj) return T(0);
     }
     return T(1);
@@ -562,29 +585,31 @@ template <typename T> void transmittance_DT_bw(const Scene<T>& S, Rng& rng, V3<T
     V3<T> ini_x = x;
     T ini_d = d;
     Rng before = rng;
-    for (int it = 0; it < (1 << 24); ++it) {
+    for (Flight<T> ff; ff.it < (1 << 24); ++ff.it) {
         T md;
         T maj = vmax(T(0.0000001), S.majorant(x, w, md) + T(0.1));
-        T dt = -std::log(T(1) - (T)rng.uniform()) / maj;
+        T dt = ff.sample(rng) / maj;
         T t = vmin(md, dt);
         x += w * t;
         d -= t;
         if (d <= T(0.0000001)) break;
-        if (dt > md) continue;
+        if (dt > md) { ff.cross(maj, md); continue; }
+        ff.used();
         if ((T)rng.uniform() < S.sigma(x) / maj) return;
     }
     x = ini_x;
     d = ini_d;
     rng = before;
-    for (int it = 0; it < (1 << 24); ++it) {
+    for (Flight<T> ff; ff.it < (1 << 24); ++ff.it) {
         T md;
         T maj = vmax(T(0.0000001), S.majorant(x, w, md) + T(0.1));
-        T dt = -std::log(T(1) - (T)rng.uniform()) / maj;
+        T dt = ff.sample(rng) / maj;
         T t = vmin(md, dt);
         x += w * t;
         d -= t;
         if (d <= T(0.0000001)) break;
-        if (dt > md) continue;
+        if (dt > md) { ff.cross(maj, md); continue; }
+        ff.used();
         rng.advance();
         T Pc = S.sigma(x) / maj;
         T dL_dsigma = -dL_dT / maj / (T(1) - Pc);
@@ -694,13 +719,14 @@ V3<T> path_integrator_NEE(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, bool on
     const T EPS = T(0.00001);
     int bounces = 0;
     const V3<T> sun_dir = V3<T>::load(S.s.sun_dir), sun_L = V3<T>::load(S.s.sun_radiance);
-    while (d > EPS) {
+    for (Flight<T> ff; d > EPS;) {
         T md;
         T m = vmax(EPS, S.majorant(x, w, md));
-        T t = -std::log(T(1) - (T)rng.uniform()) / m;
+        T t = ff.sample(rng) / m;
         ++cnt.steps;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         T s = S.sigma(x);
         T Pc = s / m;
@@ -737,13 +763,14 @@ template <typename T> V3<T> path_integrator_DT(const Scene<T>& S, Rng& rng, V3<T
     T d = tMax - tMin;
     V3<T> R(T(0)), W(T(1));
     int bounces = 0;
-    while (d > T(0.00000001)) {
+    for (Flight<T> ff; d > T(0.00000001);) {
         T md;
         T m = vmax(T(0.00000001), S.majorant(x, w, md));
-        T t = -std::log(T(1) - (T)rng.uniform()) / m;
+        T t = ff.sample(rng) / m;
         ++cnt.steps;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         T s = S.sigma(x);
         T Pc = s / m;
@@ -776,12 +803,13 @@ template <typename T> void path_integrator_DT_bw(const Scene<T>& S, Rng& rng, V3
     V3<T> W(T(1));
     T null_W = 1;
     int bounces = 0;
-    while (d > EPS) {
+    for (Flight<T> ff; d > EPS;) {
         T md;
         T m = vmax(EPS, S.majorant(x, w, md) + T(2) * eps);
-        T t = -std::log(T(1) - (T)rng.uniform()) / m;
+        T t = ff.sample(rng) / m;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         T s = S.sigma(x);
         T Pc = (s + eps) / m;
@@ -811,12 +839,13 @@ template <typename T> void path_integrator_DT_bw(const Scene<T>& S, Rng& rng, V3
     V3<T> W_out = W;
     W = V3<T>(T(1));
     bounces = 0;
-    while (d > EPS) {
+    for (Flight<T> ff; d > EPS;) {
         T md;
         T m = vmax(EPS, S.majorant(x, w, md) + T(2) * eps);
-        T t = -std::log(T(1) - (T)rng.uniform()) / m;
+        T t = ff.sample(rng) / m;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         T s = S.sigma(x);
         T Pc = (s + eps) / m;
@@ -862,12 +891,13 @@ template <typename T> void path_integrator_NEE_DS_bw(const Scene<T>& S, Rng& rng
     bool scattered = false;
     int bounces = 0;
     const V3<T> sun_dir = V3<T>::load(S.s.sun_dir), sun_L = V3<T>::load(S.s.sun_radiance);
-    while (d > EPS) {
+    for (Flight<T> ff; d > EPS;) {
         T md;
         T m = vmax(EPS, S.majorant(x, w, md) + T(2) * eps + T(0.1));
-        T t = -std::log(T(1) - (T)rng.uniform()) / m;
+        T t = ff.sample(rng) / m;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         T s = S.sigma(x);
         T Pc = (s + eps) / m;
@@ -911,13 +941,14 @@ template <typename T> void path_integrator_NEE_DS_bw(const Scene<T>& S, Rng& rng
     x += w * tMin;
     d = tMax - tMin;
     bounces = 0;
-    while (d > EPS) {
+    for (Flight<T> ff; d > EPS;) {
         T md;
         T mj = S.majorant(x, w, md);
         T m = S.s.ds_compat ? vmax(EPS, mj * T(1.2) + T(2) * eps) : vmax(EPS, mj + T(2) * eps + T(0.1));
-        T t = -std::log(T(1) - (T)rng.uniform()) / m;
+        T t = ff.sample(rng) / m;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         T s = S.sigma(x);
         T Pc = (s + eps) / m;
@@ -983,7 +1014,7 @@ template <typename T>
 T sample_transmittance_position(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, T d, T& sample_t, T& weight_t) {
     T Tr = 1, t = 0, res_t = 0, res_dt = 0, C = 0;
     const T EPS = T(0.0000001);
-    for (int it = 0; it < (1 << 24); ++it) {
+    for (Flight<T> ff; ff.it < (1 << 24); ++ff.it) {
         T md;
         T m = vmax(EPS, S.majorant(x + w * t, w, md));
         T dt = vmin(-std::log(T(1) - (T)rng.uniform()) / m, vmin(md, d - t));
@@ -1027,12 +1058,13 @@ template <typename T> void path_integrator_NEE_DRT_bw(const Scene<T>& S, Rng& rn
     Rng before_path = rng;
     int bounces = 0;
     (void)direct_T;
-    while (d > EPS) {
+    for (Flight<T> ff; d > EPS;) {
         T md;
         T m = S.majorant(x, w, md) * T(1.05) + T(0.1);
-        T t = -std::log(T(1) - (T)rng.uniform()) / m;
+        T t = ff.sample(rng) / m;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         T s = S.sigma(x);
         T Pc = s / m;
@@ -1067,12 +1099,13 @@ template <typename T> void path_integrator_NEE_DRT_bw(const Scene<T>& S, Rng& rn
     d = ini_d;
     rng = before_path;
     bounces = 0;
-    while (d > EPS) {
+    for (Flight<T> ff; d > EPS;) {
         T md;
         T m = S.majorant(x, w, md) * T(1.05) + T(0.1);
-        T t = -std::log(T(1) - (T)rng.uniform()) / m;
+        T t = ff.sample(rng) / m;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         T s = S.sigma(x);
         T Pc = s / m;

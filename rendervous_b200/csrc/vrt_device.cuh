@@ -261,7 +261,8 @@ __device__ __forceinline__ float majorant(const DMedium& M, float3 x, float3 w, 
             float q = (comp(x, i) - comp(M.bmin, i)) * comp(M.maj_scale, i);
             float v = comp(w, i) * comp(M.maj_scale, i);
             if (v != 0.0f) {
-                float a = (0.0f - q) / v, b = ((float)Md[i] - q) / v;
+                float rv = __frcp_rn(v);
+                float a = (0.0f - q) * rv, b = ((float)Md[i] - q) * rv;
                 tn = gmax(tn, gmin(a, b));
                 tf = gmin(tf, gmax(a, b));
             } else if (!(q >= 0.0f && q <= (float)Md[i])) {
@@ -282,7 +283,8 @@ __device__ __forceinline__ float majorant(const DMedium& M, float3 x, float3 w, 
         ci = min(max(ci, 0), Md[i] - 1);
         c[i] = ci;
         float v = wi * comp(M.maj_scale, i);
-        float di = v > 0.0f ? ((float)(ci + 1) - q) / v : (v < 0.0f ? ((float)ci - q) / v : __int_as_float(0x7f800000));
+        float rv = __frcp_rn(v);  // face distances use a correctly rounded reciprocal
+        float di = v > 0.0f ? ((float)(ci + 1) - q) * rv : (v < 0.0f ? ((float)ci - q) * rv : __int_as_float(0x7f800000));
         dist = gmin(dist, di);
     }
     md = gmax(dist, 1e-6f);

@@ -31,4 +31,8 @@ int launch_radiance_fw(const DMedium& M, int integrator, const PathSrc& src, uin
 int launch_radiance_bw(const DMedium& M, int bw_mode, const PathSrc& src, uint64_t n_paths, uint64_t seed,
                        const float* dL, float div, DScratch* scratch, int num_sms, cudaStream_t stream);
 
+// The NEE_DS adjoint as a persistent state machine (vrt_adjoint.cu).
+int launch_nee_ds_bw(const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed, const float* dL,
+                     float div, DScratch* scratch, int num_sms, cudaStream_t stream);
+
 }  // namespace vrt

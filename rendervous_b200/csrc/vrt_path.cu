@@ -71,6 +71,7 @@ enum : int { SH_DIRECT = 0, SH_ENV = 1, SH_SUN = 2 };
 enum : int { EV_NONE = 0, EV_COLLISION = 1, EV_ESCAPE = 2, EV_SHADOW_DONE = 3 };
 
 struct NeeLane {
+    Flight ff;      // the current free flight (residual optical depth)
     Rng rng;        // the active stream: the path's, or a shadow ray's fork
     Rng park;       // the path's stream while a shadow ray runs
     bool parked;
@@ -93,6 +94,7 @@ struct NeeLane {
 __device__ __forceinline__ int start_shadow(const DMedium& M, NeeLane& L, float3 x0, float3 dir, Tally& tl) {
     L.state = ST_SHADOW;
     L.T = 1.0f;
+    L.ff = Flight();
     Rng child = L.rng.fork();
     if (M.tr_mode >= 2) {
         L.T = M.tr_mode == 2 ? transmittance_dda<false>(M, x0, dir, tl) : transmittance_dda<true>(M, x0, dir, tl);
@@ -183,51 +185,62 @@ __global__ void __launch_bounds__(256) k_nee_fw(DMedium M, PathSrc S, uint64_t n
         if (__all_sync(kFull, L.state == ST_DEAD && exhausted)) break;
         if (L.state == ST_DEAD) continue;
 
-        // ---- one free-flight step of the current segment
+        // ---- one free flight of the current segment; majorant-brick faces it
+        // crosses are handled in the inner loop without new draws
         const bool prim = L.state == ST_PRIMARY;
-        float3 p = prim ? L.x : L.sx;
-        float3 v = prim ? L.w : L.sw;
-        float md;
-        float mj = majorant(M, p, v, md);
-        float lg = -logf(1.0f - L.rng.uniform());
-        ++tl.steps;
         int ev = EV_NONE;
         bool need_sigma = false;
         float m = 0.0f, t = 0.0f;
-        if (prim) {  // vr_path_integrator_NEE.h:20-33
-            m = gmax(EPS, mj);
-            t = lg / m;
-            L.x = L.x + L.w * gmin(t, md);
-            if (t > md) {
-                L.d -= md;
-                if (!(L.d > EPS)) ev = EV_ESCAPE;
-            } else if (t > L.d) {
+        if (L.ff.tau < 0.0f) ++tl.steps;
+        L.ff.sample(L.rng);
+        for (int k = 0;; ++k) {
+            if (k >= kStepCap) {
+                raise_status(&sc->status, 4);
                 ev = EV_ESCAPE;
-            } else {
-                need_sigma = true;
+                break;
             }
-        } else if (M.tr_mode == 0) {  // vr_transmittance_RT.h:15-25
-            m = gmax(0.0000001f, mj);
-            t = lg / m;
-            if (md < L.sd && t > md) {
-                L.sx = L.sx + L.sw * md;
-                L.sd -= md;
-            } else {
+            float md;
+            if (prim) {  // vr_path_integrator_NEE.h:20-33
+                m = gmax(EPS, majorant(M, L.x, L.w, md));
+                t = L.ff.tau / m;
+                L.x = L.x + L.w * gmin(t, md);
+                if (t > md) {
+                    L.d -= md;
+                    L.ff.cross(m, md);
+                    if (!(L.d > EPS)) { ev = EV_ESCAPE; break; }
+                    continue;
+                }
+                L.ff.used();
+                if (t > L.d) ev = EV_ESCAPE;
+                else need_sigma = true;
+                break;
+            } else if (M.tr_mode == 0) {  // vr_transmittance_RT.h:15-25
+                m = gmax(0.0000001f, majorant(M, L.sx, L.sw, md));
+                t = L.ff.tau / m;
+                if (md < L.sd && t > md) {
+                    L.sx = L.sx + L.sw * md;
+                    L.sd -= md;
+                    L.ff.cross(m, md);
+                    continue;
+                }
+                L.ff.used();
                 float dt = gmin(t, gmin(L.sd, md));
                 L.sx = L.sx + L.sw * dt;
                 L.sd -= dt;
                 if (L.sd <= 0.0000001f) ev = EV_SHADOW_DONE;
                 else need_sigma = true;
-            }
-        } else {  // vr_transmittance_DT.h:10-26
-            m = gmax(0.0000001f, mj);
-            float dt = lg / m;
-            float tt = gmin(md, dt);
-            L.sx = L.sx + L.sw * tt;
-            L.sd -= tt;
-            if (!(dt > md)) {
-                if (L.sd <= 0.0000001f) ev = EV_SHADOW_DONE;
-                else need_sigma = true;
+                break;
+            } else {  // vr_transmittance_DT.h:10-26
+                m = gmax(0.0000001f, majorant(M, L.sx, L.sw, md));
+                float dt = L.ff.tau / m;
+                float tt = gmin(md, dt);
+                L.sx = L.sx + L.sw * tt;
+                L.sd -= tt;
+                if (L.sd <= 0.0000001f) { L.ff.used(); ev = EV_SHADOW_DONE; break; }
+                if (dt > md) { L.ff.cross(m, md); continue; }
+                L.ff.used();
+                need_sigma = true;
+                break;
             }
         }
         if (need_sigma) {
@@ -271,6 +284,7 @@ __global__ void __launch_bounds__(256) k_nee_fw(DMedium M, PathSrc S, uint64_t n
                     L.rng = L.park;
                     L.parked = false;
                 }
+                L.ff = Flight();
                 if (L.kind == SH_DIRECT) {  // vr_path_integrator_NEE.h:13-14
                     L.R = L.R + L.T * M.env;
                     L.state = ST_PRIMARY;
@@ -322,14 +336,15 @@ __device__ float3 path_nee_seq(const DMedium& M, Rng& rng, float3 x, float3 w, b
     if (!only_scatters) R = R + transmittance(M, rng, x, w, tl, status) * M.env;
     const float EPS = 0.00001f;
     int bounces = 0;
-    for (int it = 0; d > EPS; ++it) {
-        if (it >= kPathStepCap) { raise_status(status, 4); break; }
+    for (Flight ff; d > EPS; ++ff.it) {
+        if (ff.it >= kPathStepCap) { raise_status(status, 4); break; }
         float md;
         float m = gmax(EPS, majorant(M, x, w, md));
-        float t = -logf(1.0f - rng.uniform()) / m;
-        ++tl.steps;
+        if (ff.tau < 0.0f) ++tl.steps;
+        float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         float s = sigma(M, x, tl);
         if (rng.uniform() >= s / m) { d -= t; continue; }
@@ -363,14 +378,15 @@ __device__ float3 path_dt_seq(const DMedium& M, Rng& rng, float3 x, float3 w, ui
     float d = tMax - tMin;
     float3 R = f3(0.0f), W = f3(1.0f);
     int bounces = 0;
-    for (int it = 0; d > 0.00000001f; ++it) {
-        if (it >= kPathStepCap) { raise_status(status, 4); break; }
+    for (Flight ff; d > 0.00000001f; ++ff.it) {
+        if (ff.it >= kPathStepCap) { raise_status(status, 4); break; }
         float md;
         float m = gmax(0.00000001f, majorant(M, x, w, md));
-        float t = -logf(1.0f - rng.uniform()) / m;
-        ++tl.steps;
+        if (ff.tau < 0.0f) ++tl.steps;
+        float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         float s = sigma(M, x, tl);
         if (rng.uniform() >= s / m) { d -= t; continue; }
@@ -400,13 +416,14 @@ __device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float
     float3 W = f3(1.0f);
     float null_W = 1.0f;
     int bounces = 0;
-    for (int it = 0; d > EPS; ++it) {
-        if (it >= kPathStepCap) { raise_status(status, 4); return; }
+    for (Flight ff; d > EPS; ++ff.it) {
+        if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
         float m = gmax(EPS, majorant(M, x, w, md) + 2.0f * eps);
-        float t = -logf(1.0f - rng.uniform()) / m;
+        float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         float s = sigma(M, x, tl);
         float Pc = (s + eps) / m;
@@ -435,13 +452,14 @@ __device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float
     const float3 W_out = W;
     W = f3(1.0f);
     bounces = 0;
-    for (int it = 0; d > EPS; ++it) {
-        if (it >= kPathStepCap) { raise_status(status, 4); return; }
+    for (Flight ff; d > EPS; ++ff.it) {
+        if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
         float m = gmax(EPS, majorant(M, x, w, md) + 2.0f * eps);
-        float t = -logf(1.0f - rng.uniform()) / m;
+        float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         float s = sigma(M, x, tl);
         float Pc = (s + eps) / m;
@@ -480,13 +498,14 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
     const float EPS = 0.00000001f;
     bool scattered = false;
     int bounces = 0;
-    for (int it = 0; d > EPS; ++it) {
-        if (it >= kPathStepCap) { raise_status(status, 4); return; }
+    for (Flight ff; d > EPS; ++ff.it) {
+        if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
         float m = gmax(EPS, majorant(M, x, w, md) + 2.0f * eps + 0.1f);
-        float t = -logf(1.0f - rng.uniform()) / m;
+        float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         float s = sigma(M, x, tl);
         float Pc = (s + eps) / m;
@@ -528,14 +547,15 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
     x = x + w * tMin;
     d = tMax - tMin;
     bounces = 0;
-    for (int it = 0; d > EPS; ++it) {
-        if (it >= kPathStepCap) { raise_status(status, 4); return; }
+    for (Flight ff; d > EPS; ++ff.it) {
+        if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
         float mj = majorant(M, x, w, md);
         float m = M.ds_compat ? gmax(EPS, mj * 1.2f + 2.0f * eps) : gmax(EPS, mj + 2.0f * eps + 0.1f);
-        float t = -logf(1.0f - rng.uniform()) / m;
+        float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         float s = sigma(M, x, tl);
         float Pc = (s + eps) / m;
@@ -637,13 +657,14 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
     const float EPS = 0.00000001f;
     const Rng::Pos before_path = rng.pos();
     int bounces = 0;
-    for (int it = 0; d > EPS; ++it) {
-        if (it >= kPathStepCap) { raise_status(status, 4); return; }
+    for (Flight ff; d > EPS; ++ff.it) {
+        if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
         float m = majorant(M, x, w, md) * 1.05f + 0.1f;
-        float t = -logf(1.0f - rng.uniform()) / m;
+        float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         float s = sigma(M, x, tl);
         if (rng.uniform() >= s / m) { d -= t; continue; }
@@ -675,13 +696,14 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
     d = ini_d;
     rng.seek(before_path);
     bounces = 0;
-    for (int it = 0; d > EPS; ++it) {
-        if (it >= kPathStepCap) { raise_status(status, 4); return; }
+    for (Flight ff; d > EPS; ++ff.it) {
+        if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
         float m = majorant(M, x, w, md) * 1.05f + 0.1f;
-        float t = -logf(1.0f - rng.uniform()) / m;
+        float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; continue; }
+        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        ff.used();
         if (t > d) break;
         float s = sigma(M, x, tl);
         if (rng.uniform() >= s / m) {
@@ -809,6 +831,7 @@ int launch_radiance_fw(const DMedium& M, int integrator, const PathSrc& src, uin
 int launch_radiance_bw(const DMedium& M, int bw_mode, const PathSrc& src, uint64_t n_paths, uint64_t seed,
                        const float* dL, float div, DScratch* scratch, int num_sms, cudaStream_t stream) {
     if (n_paths == 0) return 0;
+    if (bw_mode == 0) return launch_nee_ds_bw(M, src, n_paths, seed, dL, div, scratch, num_sms, stream);
     uint64_t need = (n_paths + 255) / 256;
     int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
     if (bw_mode == 0) k_path_bw<0><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);

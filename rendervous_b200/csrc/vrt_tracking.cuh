@@ -18,6 +18,23 @@ namespace vrt {
 
 constexpr int kStepCap = 1 << 24;  // per-segment iteration bound (error VRT_E_ITER_CAP)
 
+// Optical distance of the current free flight.  With a piecewise-constant
+// majorant a flight continues across a majorant-brick face with the optical
+// depth it has left (exponential lengths are memoryless), so a draw is taken
+// only after the previous flight ended at a candidate collision or at the end
+// of the segment.  The constant majorant (distance 1e6) never crosses a face,
+// so then every step draws, as the reference does.
+struct Flight {
+    float tau = -1.0f;
+    int it = 0;
+    __device__ __forceinline__ float sample(Rng& rng) {
+        if (tau < 0.0f) tau = -logf(1.0f - rng.uniform());
+        return tau;
+    }
+    __device__ __forceinline__ void cross(float m, float md) { tau -= __fmul_rn(m, md); }
+    __device__ __forceinline__ void used() { tau = -1.0f; }
+};
+
 struct DDA {
     float3 x, w, alpha, alpha_inc, vn, vm;
     int cx, cy, cz, sx, sy, sz, dimx, dimy, dimz;
@@ -267,12 +284,14 @@ __device__ __forceinline__ float transmittance_rt(const DMedium& M, Rng& rng, fl
     if (!boundary(M, x, w, tMin, tMax)) return T;
     x = x + w * tMin;
     float d = tMax - tMin;
+    Flight ff;
     for (int it = 0; it < kStepCap; ++it) {
         float md;
         float maj = gmax(0.0000001f, majorant(M, x, w, md));
-        float t = -logf(1.0f - rng.uniform()) / maj;
-        ++tl.steps;
-        if (md < d && t > md) { x = x + w * md; d -= md; continue; }
+        if (ff.tau < 0.0f) ++tl.steps;
+        float t = ff.sample(rng) / maj;
+        if (md < d && t > md) { x = x + w * md; d -= md; ff.cross(maj, md); continue; }
+        ff.used();
         float dt = gmin(t, gmin(d, md));
         x = x + w * dt;
         d -= dt;
@@ -301,11 +320,13 @@ __device__ __forceinline__ void transmittance_rt_bw(const DMedium& M, Rng& rng, 
     const float ini_d = d;
     const Rng::Pos before = rng.pos();
     int it = 0;
+    Flight ff;
     for (; it < kStepCap; ++it) {
         float md;
         float maj = gmax(EPS, majorant(M, x, w, md) + 0.1f);
-        float t = -logf(1.0f - rng.uniform()) / maj;
-        if (md < d && t > md) { x = x + w * md; d -= md; continue; }
+        float t = ff.sample(rng) / maj;
+        if (md < d && t > md) { x = x + w * md; d -= md; ff.cross(maj, md); continue; }
+        ff.used();
         float dt = gmin(t, gmin(d, md));
         x = x + w * dt;
         d -= dt;
@@ -322,11 +343,13 @@ __device__ __forceinline__ void transmittance_rt_bw(const DMedium& M, Rng& rng, 
     rng.seek(before);
     x = ini_x;
     d = ini_d;
+    ff = Flight();
     for (it = 0; it < kStepCap; ++it) {
         float md;
         float maj = gmax(EPS, majorant(M, x, w, md) + 0.1f);
-        float t = -logf(1.0f - rng.uniform()) / maj;
-        if (md < d && t > md) { x = x + w * md; d -= md; continue; }
+        float t = ff.sample(rng) / maj;
+        if (md < d && t > md) { x = x + w * md; d -= md; ff.cross(maj, md); continue; }
+        ff.used();
         float dt = gmin(t, gmin(d, md));
         x = x + w * dt;
         d -= dt;
@@ -348,18 +371,20 @@ __device__ __forceinline__ float transmittance_dt(const DMedium& M, Rng& rng, fl
     if (!boundary(M, x, w, tMin, tMax)) return 1.0f;
     x = x + w * tMin;
     float d = tMax - tMin;
+    Flight ff;
     for (int it = 0; it < kStepCap; ++it) {
         float md;
         float maj = gmax(0.0000001f, majorant(M, x, w, md));
-        float dt = -logf(1.0f - rng.uniform()) / maj;
+        if (ff.tau < 0.0f) ++tl.steps;
+        float dt = ff.sample(rng) / maj;
         float t = gmin(md, dt);
-        ++tl.steps;
         x = x + w * t;
         d -= t;
         // the end test precedes the brick-crossing restart (the reference's
         // order, which the constant majorant never distinguishes)
         if (d <= 0.0000001f) return 1.0f;
-        if (dt > md) continue;
+        if (dt > md) { ff.cross(maj, md); continue; }
+        ff.used();
         if (rng.uniform() < sigma(M, x, tl) / maj) return 0.0f;
     }
     raise_status(status, 4);
@@ -378,30 +403,34 @@ __device__ __forceinline__ void transmittance_dt_bw(const DMedium& M, Rng& rng, 
     const float ini_d = d;
     const Rng::Pos before = rng.pos();
     int it = 0;
+    Flight ff;
     for (; it < kStepCap; ++it) {
         float md;
         float maj = gmax(0.0000001f, majorant(M, x, w, md) + 0.1f);
-        float dt = -logf(1.0f - rng.uniform()) / maj;
+        float dt = ff.sample(rng) / maj;
         float t = gmin(md, dt);
         x = x + w * t;
         d -= t;
         if (d <= 0.0000001f) break;
-        if (dt > md) continue;
+        if (dt > md) { ff.cross(maj, md); continue; }
+        ff.used();
         if (rng.uniform() < sigma(M, x, tl) / maj) return;
     }
     if (it == kStepCap) { raise_status(status, 4); return; }
     x = ini_x;
     d = ini_d;
     rng.seek(before);
+    ff = Flight();
     for (it = 0; it < kStepCap; ++it) {
         float md;
         float maj = gmax(0.0000001f, majorant(M, x, w, md) + 0.1f);
-        float dt = -logf(1.0f - rng.uniform()) / maj;
+        float dt = ff.sample(rng) / maj;
         float t = gmin(md, dt);
         x = x + w * t;
         d -= t;
         if (d <= 0.0000001f) break;
-        if (dt > md) continue;
+        if (dt > md) { ff.cross(maj, md); continue; }
+        ff.used();
         rng.advance();
         float Pc = sigma(M, x, tl) / maj;
         sigma_bw(M, x, -dL_dT / maj / (1.0f - Pc), tl);
