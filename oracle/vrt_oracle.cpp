@@ -123,9 +123,72 @@ struct Counters {
 // taken only after the previous one ended at a candidate collision or at the
 // end of the segment.  With the reference's constant majorant (distance 1e6)
 // no flight ever crosses a face and every step draws, as in the reference.
+template <typename T> struct Scene;
+
+// Majorant bricks along one straight segment (majorant-grid mode): a 3D DDA
+// over the brick grid started at the segment's first query.  The brick of the
+// start point is chosen with the 1e-4-brick nudge of Scene::majorant, the face
+// distances use correctly rounded reciprocals, and outside the grid's box the
+// bound is 0.  With the constant majorant it is inert.
+template <typename T> struct BrickWalk {
+    bool live = false;
+    int c[3] = {0, 0, 0}, st[3] = {0, 0, 0};
+    T tn[3] = {0, 0, 0}, dt[3] = {0, 0, 0}, t = 0, m = 0;
+    void reset() { live = false; }
+    T lookup(const orc_scene& s) const {
+        for (int i = 0; i < 3; ++i)
+            if (c[i] < 0 || c[i] >= s.maj_dims[i]) return T(0);
+        return (T)s.maj_grid[((int64_t)c[2] * s.maj_dims[1] + c[1]) * s.maj_dims[0] + c[0]];
+    }
+    void init(const orc_scene& s, V3<T> x, V3<T> w) {
+        live = true;
+        t = T(0);
+        const T inf = std::numeric_limits<T>::infinity();
+        for (int i = 0; i < 3; ++i) {
+            T q = (x[i] - (T)s.bmin[i]) * (T)s.maj_scale[i];
+            T dq = w[i] * (T)s.maj_scale[i];
+            if (dq > T(0)) {
+                c[i] = (int)std::floor(q + T(1e-4)); st[i] = 1;
+                T rv = T(1) / dq;
+                tn[i] = (T(c[i] + 1) - q) * rv; dt[i] = rv;
+            } else if (dq < T(0)) {
+                c[i] = (int)std::floor(q - T(1e-4)); st[i] = -1;
+                T rv = T(1) / dq;
+                tn[i] = (T(c[i]) - q) * rv; dt[i] = -rv;
+            } else {
+                c[i] = (int)std::floor(q); st[i] = 0; tn[i] = inf; dt[i] = inf;
+            }
+        }
+        m = lookup(s);
+    }
+    int axis() const { return (tn[0] <= tn[1] && tn[0] <= tn[2]) ? 0 : (tn[1] <= tn[2] ? 1 : 2); }
+    bool never_enters(const orc_scene& s) const {
+        for (int i = 0; i < 3; ++i)
+            if ((c[i] < 0 && st[i] <= 0) || (c[i] >= s.maj_dims[i] && st[i] >= 0)) return true;
+        return false;
+    }
+    T query(const orc_scene& s, V3<T> x, V3<T> w, T& md) {
+        if (s.majorant_mode == 0) { md = T(1000000.0); return (T)s.global_majorant; }
+        if (!live) init(s, x, w);
+        if (never_enters(s)) { md = T(1000000.0); return T(0); }
+        md = tn[axis()] - t;
+        return m;
+    }
+    void advance(const orc_scene& s) {
+        if (!live) return;
+        int a = axis();
+        t = tn[a];
+        tn[a] += dt[a];
+        c[a] += st[a];
+        m = lookup(s);
+    }
+    void move(T dist) { t += dist; }
+};
+
 template <typename T> struct Flight {
     T tau = T(-1);
     int it = 0;
+    BrickWalk<T> bk;  // majorant bricks of the current segment
     T sample(Rng& rng) {
         if (tau < T(0)) tau = -std::log(T(1) - (T)rng.uniform());
         return tau;
@@ -479,12 +542,13 @@ template <typename T> T transmittance_RT(const Scene<T>& S, Rng& rng, V3<T> x, V
     T d = tMax - tMin;
     for (Flight<T> ff; ff.it < (1 << 24); ++ff.it) {
         T md;
-        T maj = vmax(T(0.0000001), S.majorant(x, w, md));
+        T maj = vmax(T(0.0000001), ff.bk.query(S.s, x, w, md));
         T t = ff.sample(rng) / maj;
         if (steps) ++*steps;
-        if (md < d && t > md) { x += w * md; d -= md; ff.cross(maj, md); continue; }  // grid crossing
+        if (md < d && t > md) { x += w * md; d -= md; ff.cross(maj, md); ff.bk.advance(S.s); continue; }  // grid crossing
         ff.used();
         T dt = vmin(t, vmin(d, md));
+        ff.bk.move(dt);
         x += w * dt;
         d -= dt;
         if (d <= T(0.0000001)) return Tr;
@@ -511,11 +575,12 @@ template <typename T> void transmittance_RT_bw(const Scene<T>& S, Rng& rng, V3<T
     Rng before = rng;
     for (Flight<T> ff; ff.it < (1 << 24); ++ff.it) {
         T md;
-        T maj = vmax(EPS, S.majorant(x, w, md) + T(0.1));
+        T maj = vmax(EPS, ff.bk.query(S.s, x, w, md) + T(0.1));
         T t = ff.sample(rng) / maj;
-        if (md < d && t > md) { x += w * md; d -= md; ff.cross(maj, md); continue; }  // grid crossing
+        if (md < d && t > md) { x += w * md; d -= md; ff.cross(maj, md); ff.bk.advance(S.s); continue; }  // grid crossing
         ff.used();
         T dt = vmin(t, vmin(d, md));
+        ff.bk.move(dt);
         x += w * dt;
         d -= dt;
         if (d <= EPS) break;
@@ -532,11 +597,12 @@ template <typename T> void transmittance_RT_bw(const Scene<T>& S, Rng& rng, V3<T
     d = ini_d;
     for (Flight<T> ff; ff.it < (1 << 24); ++ff.it) {
         T md;
-        T maj = vmax(EPS, S.majorant(x, w, md) + T(0.1));
+        T maj = vmax(EPS, ff.bk.query(S.s, x, w, md) + T(0.1));
         T t = ff.sample(rng) / maj;
-        if (md < d && t > md) { x += w * md; d -= md; ff.cross(maj, md); continue; }  // grid crossing
+        if (md < d && t > md) { x += w * md; d -= md; ff.cross(maj, md); ff.bk.advance(S.s); continue; }  // grid crossing
         ff.used();
         T dt = vmin(t, vmin(d, md));
+        ff.bk.move(dt);
         x += w * dt;
         d -= dt;
         if (d <= EPS) break;
@@ -559,7 +625,7 @@ template <typename T> T transmittance_DT(const Scene<T>& S, Rng& rng, V3<T> x, V
     T d = tMax - tMin;
     for (Flight<T> ff; ff.it < (1 << 24); ++ff.it) {
         T md;
-        T maj = vmax(T(0.0000001), S.majorant(x, w, md));
+        T maj = vmax(T(0.0000001), ff.bk.query(S.s, x, w, md));
         T dt = ff.sample(rng) / maj;
         T t = vmin(md, dt);
         if (steps) ++*steps;
@@ -568,8 +634,9 @@ template <typename T> T transmittance_DT(const Scene<T>& S, Rng& rng, V3<T> x, V
         // the end test precedes the brick-crossing restart (the reference's
         // order, which the constant majorant never distinguishes)
         if (d <= T(0.0000001)) return T(1);
-        if (dt > md) { ff.cross(maj, md); continue; }
+        if (dt > md) { ff.cross(maj, md); ff.bk.advance(S.s); continue; }
         ff.used();
+        ff.bk.move(t);
         if ((T)rng.uniform() < S.sigma(x) / maj) return T(0);
     }
     return T(1);
@@ -587,14 +654,15 @@ template <typename T> void transmittance_DT_bw(const Scene<T>& S, Rng& rng, V3<T
     Rng before = rng;
     for (Flight<T> ff; ff.it < (1 << 24); ++ff.it) {
         T md;
-        T maj = vmax(T(0.0000001), S.majorant(x, w, md) + T(0.1));
+        T maj = vmax(T(0.0000001), ff.bk.query(S.s, x, w, md) + T(0.1));
         T dt = ff.sample(rng) / maj;
         T t = vmin(md, dt);
         x += w * t;
         d -= t;
         if (d <= T(0.0000001)) break;
-        if (dt > md) { ff.cross(maj, md); continue; }
+        if (dt > md) { ff.cross(maj, md); ff.bk.advance(S.s); continue; }
         ff.used();
+        ff.bk.move(t);
         if ((T)rng.uniform() < S.sigma(x) / maj) return;
     }
     x = ini_x;
@@ -602,14 +670,15 @@ template <typename T> void transmittance_DT_bw(const Scene<T>& S, Rng& rng, V3<T
     rng = before;
     for (Flight<T> ff; ff.it < (1 << 24); ++ff.it) {
         T md;
-        T maj = vmax(T(0.0000001), S.majorant(x, w, md) + T(0.1));
+        T maj = vmax(T(0.0000001), ff.bk.query(S.s, x, w, md) + T(0.1));
         T dt = ff.sample(rng) / maj;
         T t = vmin(md, dt);
         x += w * t;
         d -= t;
         if (d <= T(0.0000001)) break;
-        if (dt > md) { ff.cross(maj, md); continue; }
+        if (dt > md) { ff.cross(maj, md); ff.bk.advance(S.s); continue; }
         ff.used();
+        ff.bk.move(t);
         rng.advance();
         T Pc = S.sigma(x) / maj;
         T dL_dsigma = -dL_dT / maj / (T(1) - Pc);
@@ -721,13 +790,14 @@ V3<T> path_integrator_NEE(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, bool on
     const V3<T> sun_dir = V3<T>::load(S.s.sun_dir), sun_L = V3<T>::load(S.s.sun_radiance);
     for (Flight<T> ff; d > EPS;) {
         T md;
-        T m = vmax(EPS, S.majorant(x, w, md));
+        T m = vmax(EPS, ff.bk.query(S.s, x, w, md));
         T t = ff.sample(rng) / m;
         ++cnt.steps;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(S.s); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         T s = S.sigma(x);
         T Pc = s / m;
         if ((T)rng.uniform() >= Pc) { d -= t; continue; }
@@ -751,6 +821,7 @@ V3<T> path_integrator_NEE(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, bool on
         if (all_less(W, EPS)) return R;
         w = wo;
         S.boundary(x, w, tMin, d);
+        ff.bk.reset();
     }
     return R;
 }
@@ -765,13 +836,14 @@ template <typename T> V3<T> path_integrator_DT(const Scene<T>& S, Rng& rng, V3<T
     int bounces = 0;
     for (Flight<T> ff; d > T(0.00000001);) {
         T md;
-        T m = vmax(T(0.00000001), S.majorant(x, w, md));
+        T m = vmax(T(0.00000001), ff.bk.query(S.s, x, w, md));
         T t = ff.sample(rng) / m;
         ++cnt.steps;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(S.s); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         T s = S.sigma(x);
         T Pc = s / m;
         if ((T)rng.uniform() >= Pc) { d -= t; continue; }
@@ -787,6 +859,7 @@ template <typename T> V3<T> path_integrator_DT(const Scene<T>& S, Rng& rng, V3<T
         if (S.s.max_bounces > 0 && ++bounces >= S.s.max_bounces) return R;
         w = wo;
         S.boundary(x, w, tMin, d);
+        ff.bk.reset();
     }
     return W * S.environment() + R;
 }
@@ -805,12 +878,13 @@ template <typename T> void path_integrator_DT_bw(const Scene<T>& S, Rng& rng, V3
     int bounces = 0;
     for (Flight<T> ff; d > EPS;) {
         T md;
-        T m = vmax(EPS, S.majorant(x, w, md) + T(2) * eps);
+        T m = vmax(EPS, ff.bk.query(S.s, x, w, md) + T(2) * eps);
         T t = ff.sample(rng) / m;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(S.s); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         T s = S.sigma(x);
         T Pc = (s + eps) / m;
         if ((T)rng.uniform() >= Pc) { d -= t; W *= (T(1) - s / m) / (T(1) - Pc); continue; }
@@ -827,6 +901,7 @@ template <typename T> void path_integrator_DT_bw(const Scene<T>& S, Rng& rng, V3
         if (S.s.max_bounces > 0 && ++bounces >= S.s.max_bounces) { W = V3<T>(T(0)); break; }
         w = wo;
         S.boundary(x, w, tMin, d);
+        ff.bk.reset();
     }
     V3<T> env = S.environment();
     V3<T> dL_dW = dL_dR * env;
@@ -841,12 +916,13 @@ template <typename T> void path_integrator_DT_bw(const Scene<T>& S, Rng& rng, V3
     bounces = 0;
     for (Flight<T> ff; d > EPS;) {
         T md;
-        T m = vmax(EPS, S.majorant(x, w, md) + T(2) * eps);
+        T m = vmax(EPS, ff.bk.query(S.s, x, w, md) + T(2) * eps);
         T t = ff.sample(rng) / m;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(S.s); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         T s = S.sigma(x);
         T Pc = (s + eps) / m;
         if ((T)rng.uniform() >= Pc) {
@@ -871,6 +947,7 @@ template <typename T> void path_integrator_DT_bw(const Scene<T>& S, Rng& rng, V3
         if (S.s.max_bounces > 0 && ++bounces >= S.s.max_bounces) return;
         w = wo;
         S.boundary(x, w, tMin, d);
+        ff.bk.reset();
     }
 }
 
@@ -893,12 +970,13 @@ template <typename T> void path_integrator_NEE_DS_bw(const Scene<T>& S, Rng& rng
     const V3<T> sun_dir = V3<T>::load(S.s.sun_dir), sun_L = V3<T>::load(S.s.sun_radiance);
     for (Flight<T> ff; d > EPS;) {
         T md;
-        T m = vmax(EPS, S.majorant(x, w, md) + T(2) * eps + T(0.1));
+        T m = vmax(EPS, ff.bk.query(S.s, x, w, md) + T(2) * eps + T(0.1));
         T t = ff.sample(rng) / m;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(S.s); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         T s = S.sigma(x);
         T Pc = (s + eps) / m;
         if ((T)rng.uniform() >= Pc) { d -= t; W *= (T(1) - s / m) / (T(1) - Pc); continue; }
@@ -930,6 +1008,7 @@ template <typename T> void path_integrator_NEE_DS_bw(const Scene<T>& S, Rng& rng
         if (all_less(W, EPS)) { W = V3<T>(T(0)); break; }
         w = wo;
         S.boundary(x, w, tMin, d);
+        ff.bk.reset();
     }
     if (!scattered) R += S.environment() * W;
 
@@ -943,13 +1022,14 @@ template <typename T> void path_integrator_NEE_DS_bw(const Scene<T>& S, Rng& rng
     bounces = 0;
     for (Flight<T> ff; d > EPS;) {
         T md;
-        T mj = S.majorant(x, w, md);
+        T mj = ff.bk.query(S.s, x, w, md);
         T m = S.s.ds_compat ? vmax(EPS, mj * T(1.2) + T(2) * eps) : vmax(EPS, mj + T(2) * eps + T(0.1));
         T t = ff.sample(rng) / m;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(S.s); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         T s = S.sigma(x);
         T Pc = (s + eps) / m;
         T dL_dsigma;
@@ -1004,6 +1084,7 @@ template <typename T> void path_integrator_NEE_DS_bw(const Scene<T>& S, Rng& rng
         if (all_less(W, EPS)) return;
         w = wo;
         S.boundary(x, w, tMin, d);
+        ff.bk.reset();
     }
 }
 
@@ -1060,12 +1141,13 @@ template <typename T> void path_integrator_NEE_DRT_bw(const Scene<T>& S, Rng& rn
     (void)direct_T;
     for (Flight<T> ff; d > EPS;) {
         T md;
-        T m = S.majorant(x, w, md) * T(1.05) + T(0.1);
+        T m = ff.bk.query(S.s, x, w, md) * T(1.05) + T(0.1);
         T t = ff.sample(rng) / m;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(S.s); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         T s = S.sigma(x);
         T Pc = s / m;
         if ((T)rng.uniform() >= Pc) { d -= t; continue; }
@@ -1086,6 +1168,7 @@ template <typename T> void path_integrator_NEE_DRT_bw(const Scene<T>& S, Rng& rn
         W *= rho;
         w = wo;
         S.boundary(x, w, tMin, d);
+        ff.bk.reset();
         T current_P = W.x + W.y + W.z;
         total_weight += current_P;
         if ((T)rng.uniform() < current_P / total_weight) {
@@ -1101,12 +1184,13 @@ template <typename T> void path_integrator_NEE_DRT_bw(const Scene<T>& S, Rng& rn
     bounces = 0;
     for (Flight<T> ff; d > EPS;) {
         T md;
-        T m = S.majorant(x, w, md) * T(1.05) + T(0.1);
+        T m = ff.bk.query(S.s, x, w, md) * T(1.05) + T(0.1);
         T t = ff.sample(rng) / m;
         x += w * vmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(S.s); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         T s = S.sigma(x);
         T Pc = s / m;
         T dL_dsigma;
@@ -1145,6 +1229,7 @@ template <typename T> void path_integrator_NEE_DRT_bw(const Scene<T>& S, Rng& rn
         W *= rho;
         w = wo;
         S.boundary(x, w, tMin, d);
+        ff.bk.reset();
         rng.advance();
         if (all_less(W, EPS) || capped) break;
     }

@@ -54,6 +54,7 @@ struct Lane {
     float ph_nee, ph_sun, T_nee, T_sun, dTnee, dTsun;
     float s_hit, m_hit, Pc_hit;
     uint32_t jfork;
+    float bt0[2], bt1[2];  // shadow-ray box interval per light (tMax < tMin: miss)
     // segment
     int state, light;
     float3 sx;
@@ -100,8 +101,10 @@ __device__ __forceinline__ int begin_segment(const DMedium& M, Lane& L, int st, 
         return E_SEG_ABORT;  // nothing more to run for this light
     }
     if (st != S_TRFW && L.dLdT == 0.0f) return E_SEG_ABORT;  // _RT.h:53 / _DT.h:32
-    float tMin, tMax;
-    if (!boundary(M, L.x, dir, tMin, tMax)) {
+    // the vertex's box interval for this light, computed once per vertex
+    const float tMin = L.light == L_ENV ? L.bt0[0] : L.bt0[1];
+    const float tMax = L.light == L_ENV ? L.bt1[0] : L.bt1[1];
+    if (!(tMax >= tMin)) {
         L.T = 1.0f;
         return st == S_TRFW ? E_SEG_DONE : E_SEG_ABORT;
     }
@@ -116,6 +119,16 @@ __device__ __forceinline__ int begin_segment(const DMedium& M, Lane& L, int st, 
     return E_NONE;
 }
 
+// The transmittance maps' boundary test (vr_transmittance_RT.h:5-10) for both
+// shadow directions of the current vertex; a miss is stored as tMax < tMin.
+__device__ __forceinline__ void shadow_intervals(const DMedium& M, Lane& L) {
+    float a, b;
+    if (boundary(M, L.x, L.wnee, a, b)) { L.bt0[0] = a; L.bt1[0] = b; }
+    else { L.bt0[0] = 1.0f; L.bt1[0] = 0.0f; }
+    if (M.has_sun && boundary(M, L.x, M.sun_dir, a, b)) { L.bt0[1] = a; L.bt1[1] = b; }
+    else { L.bt0[1] = 1.0f; L.bt1[1] = 0.0f; }
+}
+
 // After the path's own draws of a replayed vertex: decide what runs next.
 // Sequence per light: TRFW env, TRFW sun, (R update), TRBW1/2 env, TRBW1/2 sun.
 __device__ __forceinline__ void path_resume(Lane& L) {
@@ -126,7 +139,7 @@ __device__ __forceinline__ void path_resume(Lane& L) {
 
 }  // namespace
 
-__global__ void __launch_bounds__(256) k_nee_ds_bw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
+__global__ void __launch_bounds__(256, 2) k_nee_ds_bw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
                                                     const float* __restrict__ dL, float div, DScratch* sc) {
     const unsigned lane = threadIdx.x & 31u;
     const float EPS = 0.00000001f;
@@ -210,33 +223,37 @@ __global__ void __launch_bounds__(256) k_nee_ds_bw(DMedium M, PathSrc S, uint64_
                 if (prim) {
                     // primal: + 2 eps + 0.1 (_NEE_DS.h:36); replay: the same, or the
                     // reference's x1.2 + 2 eps (_NEE_DS.h:120) under ds_compat
-                    const float mj = majorant(M, L.x, v, md);
+                    const float mj = L.ff.bk.query(M, L.x, v, md);
                     m = (L.replay && M.ds_compat) ? gmax(EPS, mj * 1.2f + 2.0f * eps) : gmax(EPS, mj + 2.0f * eps + 0.1f);
                     t = L.ff.tau / m;
                     L.x = L.x + v * gmin(t, md);
                     if (t > md) {
                         L.d -= md;
                         L.ff.cross(m, md);
+                        L.ff.bk.advance(M);
                         if (!(L.d > EPS)) { ev = E_END; break; }
                         continue;
                     }
                     L.ff.used();
                     if (t > L.d) ev = E_END;
                     else need = true;
+                    L.ff.bk.move(t);
                     break;
                 }
                 const float add = L.state == S_TRFW ? 0.0f : 0.1f;  // adjoint majorant +0.1 (_RT.h:75, _DT.h:48)
-                m = gmax(0.0000001f, majorant(M, L.sx, v, md) + add);
+                m = gmax(0.0000001f, L.ff.bk.query(M, L.sx, v, md) + add);
                 if (M.tr_mode == 0) {
                     t = L.ff.tau / m;
                     if (md < L.sd && t > md) {
                         L.sx = L.sx + v * md;
                         L.sd -= md;
                         L.ff.cross(m, md);
+                        L.ff.bk.advance(M);
                         continue;
                     }
                     L.ff.used();
                     float dt = gmin(t, gmin(L.sd, md));
+                    L.ff.bk.move(dt);
                     L.sx = L.sx + v * dt;
                     L.sd -= dt;
                     if (L.sd <= 0.0000001f) ev = E_SEG_DONE;
@@ -248,8 +265,9 @@ __global__ void __launch_bounds__(256) k_nee_ds_bw(DMedium M, PathSrc S, uint64_
                 L.sx = L.sx + v * tt;
                 L.sd -= tt;
                 if (L.sd <= 0.0000001f) { L.ff.used(); ev = E_SEG_DONE; break; }
-                if (dt > md) { L.ff.cross(m, md); continue; }
+                if (dt > md) { L.ff.cross(m, md); L.ff.bk.advance(M); continue; }
                 L.ff.used();
+                L.ff.bk.move(tt);
                 need = true;
                 break;
             }
@@ -322,6 +340,7 @@ __global__ void __launch_bounds__(256) k_nee_ds_bw(DMedium M, PathSrc S, uint64_
                     L.env = environment_sample(M, L.rng, L.wnee);
                     L.ph_nee = phase(M, L.w, L.wnee);
                     L.ph_sun = M.has_sun ? phase(M, L.w, M.sun_dir) : 0.0f;
+                    shadow_intervals(M, L);
                     L.jfork = L.rng.ntr;
                     L.rng.ntr += M.has_sun ? 2u : 1u;
                     const bool capped = M.max_bounces > 0 && L.bounces + 1 >= M.max_bounces;
@@ -341,6 +360,7 @@ __global__ void __launch_bounds__(256) k_nee_ds_bw(DMedium M, PathSrc S, uint64_
                     L.env = environment_sample(M, L.rng, L.wnee);
                     L.ph_nee = phase(M, L.w, L.wnee);
                     L.ph_sun = M.has_sun ? phase(M, L.w, M.sun_dir) : 0.0f;
+                    shadow_intervals(M, L);
                     L.jfork = L.rng.ntr;
                     L.rng.ntr += M.has_sun ? 2u : 1u;
                     L.wo = phase_sample(M, L.rng, L.w);
@@ -395,6 +415,7 @@ __global__ void __launch_bounds__(256) k_nee_ds_bw(DMedium M, PathSrc S, uint64_
                     L.w = L.wo;
                     float tMin;
                     boundary(M, L.x, L.w, tMin, L.d);
+                    L.ff = Flight();
                     ev = E_NONE;
                     continue;
                 }
@@ -423,6 +444,7 @@ __global__ void __launch_bounds__(256) k_nee_ds_bw(DMedium M, PathSrc S, uint64_
             L.w = L.wo;
             float tMin;
             boundary(M, L.x, L.w, tMin, L.d);
+            L.ff = Flight();
             ev = E_NONE;
         }
     }

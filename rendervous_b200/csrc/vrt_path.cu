@@ -120,11 +120,12 @@ __device__ __forceinline__ int after_nee(const DMedium& M, NeeLane& L) {
     L.w = wo;
     float tMin;
     boundary(M, L.x, L.w, tMin, L.d);
+    L.ff = Flight();
     L.state = ST_PRIMARY;
     return L.d > 0.00001f ? EV_NONE : EV_ESCAPE;
 }
 
-__global__ void __launch_bounds__(256) k_nee_fw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, float* out,
+__global__ void __launch_bounds__(256, 3) k_nee_fw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, float* out,
                                                  float scale, DScratch* sc) {
     const unsigned lane = threadIdx.x & 31u;
     const float EPS = 0.00001f;
@@ -201,44 +202,49 @@ __global__ void __launch_bounds__(256) k_nee_fw(DMedium M, PathSrc S, uint64_t n
             }
             float md;
             if (prim) {  // vr_path_integrator_NEE.h:20-33
-                m = gmax(EPS, majorant(M, L.x, L.w, md));
+                m = gmax(EPS, L.ff.bk.query(M, L.x, L.w, md));
                 t = L.ff.tau / m;
                 L.x = L.x + L.w * gmin(t, md);
                 if (t > md) {
                     L.d -= md;
                     L.ff.cross(m, md);
+                    L.ff.bk.advance(M);
                     if (!(L.d > EPS)) { ev = EV_ESCAPE; break; }
                     continue;
                 }
                 L.ff.used();
                 if (t > L.d) ev = EV_ESCAPE;
                 else need_sigma = true;
+                L.ff.bk.move(t);
                 break;
             } else if (M.tr_mode == 0) {  // vr_transmittance_RT.h:15-25
-                m = gmax(0.0000001f, majorant(M, L.sx, L.sw, md));
+                m = gmax(0.0000001f, L.ff.bk.query(M, L.sx, L.sw, md));
                 t = L.ff.tau / m;
                 if (md < L.sd && t > md) {
                     L.sx = L.sx + L.sw * md;
                     L.sd -= md;
                     L.ff.cross(m, md);
+                    L.ff.bk.advance(M);
                     continue;
                 }
                 L.ff.used();
                 float dt = gmin(t, gmin(L.sd, md));
+                L.ff.bk.move(dt);
                 L.sx = L.sx + L.sw * dt;
                 L.sd -= dt;
                 if (L.sd <= 0.0000001f) ev = EV_SHADOW_DONE;
                 else need_sigma = true;
                 break;
             } else {  // vr_transmittance_DT.h:10-26
-                m = gmax(0.0000001f, majorant(M, L.sx, L.sw, md));
+                m = gmax(0.0000001f, L.ff.bk.query(M, L.sx, L.sw, md));
                 float dt = L.ff.tau / m;
                 float tt = gmin(md, dt);
                 L.sx = L.sx + L.sw * tt;
                 L.sd -= tt;
                 if (L.sd <= 0.0000001f) { L.ff.used(); ev = EV_SHADOW_DONE; break; }
-                if (dt > md) { L.ff.cross(m, md); continue; }
+                if (dt > md) { L.ff.cross(m, md); L.ff.bk.advance(M); continue; }
                 L.ff.used();
+                L.ff.bk.move(tt);
                 need_sigma = true;
                 break;
             }
@@ -339,13 +345,14 @@ __device__ float3 path_nee_seq(const DMedium& M, Rng& rng, float3 x, float3 w, b
     for (Flight ff; d > EPS; ++ff.it) {
         if (ff.it >= kPathStepCap) { raise_status(status, 4); break; }
         float md;
-        float m = gmax(EPS, majorant(M, x, w, md));
+        float m = gmax(EPS, ff.bk.query(M, x, w, md));
         if (ff.tau < 0.0f) ++tl.steps;
         float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(M); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         float s = sigma(M, x, tl);
         if (rng.uniform() >= s / m) { d -= t; continue; }
         ++verts;
@@ -365,6 +372,7 @@ __device__ float3 path_nee_seq(const DMedium& M, Rng& rng, float3 x, float3 w, b
         if (all_less(W, EPS)) return R;
         w = wo;
         boundary(M, x, w, tMin, d);
+        ff.bk.reset();
     }
     return R;
 }
@@ -381,13 +389,14 @@ __device__ float3 path_dt_seq(const DMedium& M, Rng& rng, float3 x, float3 w, ui
     for (Flight ff; d > 0.00000001f; ++ff.it) {
         if (ff.it >= kPathStepCap) { raise_status(status, 4); break; }
         float md;
-        float m = gmax(0.00000001f, majorant(M, x, w, md));
+        float m = gmax(0.00000001f, ff.bk.query(M, x, w, md));
         if (ff.tau < 0.0f) ++tl.steps;
         float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(M); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         float s = sigma(M, x, tl);
         if (rng.uniform() >= s / m) { d -= t; continue; }
         ++verts;
@@ -399,6 +408,7 @@ __device__ float3 path_dt_seq(const DMedium& M, Rng& rng, float3 x, float3 w, ui
         if (M.max_bounces > 0 && ++bounces >= M.max_bounces) return R;
         w = wo;
         boundary(M, x, w, tMin, d);
+        ff.bk.reset();
     }
     return W * M.env + R;
 }
@@ -419,12 +429,13 @@ __device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float
     for (Flight ff; d > EPS; ++ff.it) {
         if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
-        float m = gmax(EPS, majorant(M, x, w, md) + 2.0f * eps);
+        float m = gmax(EPS, ff.bk.query(M, x, w, md) + 2.0f * eps);
         float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(M); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         float s = sigma(M, x, tl);
         float Pc = (s + eps) / m;
         if (rng.uniform() >= Pc) { d -= t; W = W * ((1.0f - s / m) / (1.0f - Pc)); continue; }
@@ -441,6 +452,7 @@ __device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float
         if (M.max_bounces > 0 && ++bounces >= M.max_bounces) { W = f3(0.0f); break; }
         w = wo;
         boundary(M, x, w, tMin, d);
+        ff.bk.reset();
     }
     const float3 dL_dW = dL_dR * M.env;
     rng.seek(before_path);
@@ -455,12 +467,13 @@ __device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float
     for (Flight ff; d > EPS; ++ff.it) {
         if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
-        float m = gmax(EPS, majorant(M, x, w, md) + 2.0f * eps);
+        float m = gmax(EPS, ff.bk.query(M, x, w, md) + 2.0f * eps);
         float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(M); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         float s = sigma(M, x, tl);
         float Pc = (s + eps) / m;
         if (rng.uniform() >= Pc) {
@@ -479,6 +492,7 @@ __device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float
         if (M.max_bounces > 0 && ++bounces >= M.max_bounces) return;
         w = wo;
         boundary(M, x, w, tMin, d);
+        ff.bk.reset();
     }
 }
 
@@ -501,12 +515,13 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
     for (Flight ff; d > EPS; ++ff.it) {
         if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
-        float m = gmax(EPS, majorant(M, x, w, md) + 2.0f * eps + 0.1f);
+        float m = gmax(EPS, ff.bk.query(M, x, w, md) + 2.0f * eps + 0.1f);
         float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(M); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         float s = sigma(M, x, tl);
         float Pc = (s + eps) / m;
         if (rng.uniform() >= Pc) { d -= t; W = W * ((1.0f - s / m) / (1.0f - Pc)); continue; }
@@ -536,6 +551,7 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
         if (all_less(W, EPS)) { W = f3(0.0f); break; }
         w = wo;
         boundary(M, x, w, tMin, d);
+        ff.bk.reset();
     }
     if (!scattered) R = R + M.env * W;
 
@@ -550,13 +566,14 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
     for (Flight ff; d > EPS; ++ff.it) {
         if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
-        float mj = majorant(M, x, w, md);
+        float mj = ff.bk.query(M, x, w, md);
         float m = M.ds_compat ? gmax(EPS, mj * 1.2f + 2.0f * eps) : gmax(EPS, mj + 2.0f * eps + 0.1f);
         float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(M); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         float s = sigma(M, x, tl);
         float Pc = (s + eps) / m;
         if (rng.uniform() >= Pc) {
@@ -605,6 +622,7 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
         if (all_less(W, EPS)) return;
         w = wo;
         boundary(M, x, w, tMin, d);
+        ff.bk.reset();
     }
 }
 
@@ -660,12 +678,13 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
     for (Flight ff; d > EPS; ++ff.it) {
         if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
-        float m = majorant(M, x, w, md) * 1.05f + 0.1f;
+        float m = ff.bk.query(M, x, w, md) * 1.05f + 0.1f;
         float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(M); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         float s = sigma(M, x, tl);
         if (rng.uniform() >= s / m) { d -= t; continue; }
         float3 sa = albedo(M, x, tl);
@@ -683,6 +702,7 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
         float3 wo = phase_sample(M, rng, w);
         w = wo;
         boundary(M, x, w, tMin, d);
+        ff.bk.reset();
         float current_P = W.x + W.y + W.z;
         total_weight += current_P;
         if (rng.uniform() < current_P / total_weight) {
@@ -699,12 +719,13 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
     for (Flight ff; d > EPS; ++ff.it) {
         if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
-        float m = majorant(M, x, w, md) * 1.05f + 0.1f;
+        float m = ff.bk.query(M, x, w, md) * 1.05f + 0.1f;
         float t = ff.sample(rng) / m;
         x = x + w * gmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); continue; }
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(M); continue; }
         ff.used();
         if (t > d) break;
+        ff.bk.move(t);
         float s = sigma(M, x, tl);
         if (rng.uniform() >= s / m) {
             sigma_bw(M, x, dot(dL_dR, -R / m / (1.0f - s / m)), tl);
@@ -738,6 +759,7 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
         if (M.has_sun) transmittance_bw(M, sec, x, M.sun_dir, dL_dTsun, tl, status);
         w = wo;
         boundary(M, x, w, tMin, d);
+        ff.bk.reset();
         rng.advance();
         if (all_less(W, EPS) || capped) break;
     }

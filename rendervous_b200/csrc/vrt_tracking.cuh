@@ -24,9 +24,74 @@ constexpr int kStepCap = 1 << 24;  // per-segment iteration bound (error VRT_E_I
 // only after the previous flight ended at a candidate collision or at the end
 // of the segment.  The constant majorant (distance 1e6) never crosses a face,
 // so then every step draws, as the reference does.
+// Majorant bricks along one straight segment (majorant-grid mode): a 3D DDA
+// over the brick grid, started at the segment's first query.  The brick of the
+// start point gets the 1e-4-brick nudge of majorant(), face distances use
+// correctly rounded reciprocals, and outside the grid's box the bound is 0.
+// Inert with the constant majorant.  Axis selection is by branches so the
+// state stays in registers.
+struct BrickWalk {
+    bool live = false;
+    int c0, c1, c2, s0, s1, s2;
+    float n0, n1, n2, d0, d1, d2, t, m;
+
+    __device__ __forceinline__ void reset() { live = false; }
+    __device__ __forceinline__ float lookup(const DMedium& M) const {
+        if (c0 < 0 || c0 >= M.Mx || c1 < 0 || c1 >= M.My || c2 < 0 || c2 >= M.Mz) return 0.0f;
+        return __ldg(M.maj + ((c2 * M.My + c1) * M.Mx + c0));
+    }
+    __device__ __forceinline__ static void axis_init(float x, float bmin, float scale, float w, int& c, int& st, float& n,
+                                                     float& dd) {
+        const float inf = __int_as_float(0x7f800000);
+        float q = (x - bmin) * scale;
+        float dq = w * scale;
+        if (dq > 0.0f) {
+            c = (int)floorf(q + 1e-4f); st = 1;
+            float rv = __frcp_rn(dq);
+            n = ((float)(c + 1) - q) * rv; dd = rv;
+        } else if (dq < 0.0f) {
+            c = (int)floorf(q - 1e-4f); st = -1;
+            float rv = __frcp_rn(dq);
+            n = ((float)c - q) * rv; dd = -rv;
+        } else {
+            c = (int)floorf(q); st = 0; n = inf; dd = inf;
+        }
+    }
+    __device__ __forceinline__ void init(const DMedium& M, float3 x, float3 w) {
+        live = true;
+        t = 0.0f;
+        axis_init(x.x, M.bmin.x, M.maj_scale.x, w.x, c0, s0, n0, d0);
+        axis_init(x.y, M.bmin.y, M.maj_scale.y, w.y, c1, s1, n1, d1);
+        axis_init(x.z, M.bmin.z, M.maj_scale.z, w.z, c2, s2, n2, d2);
+        m = lookup(M);
+    }
+    __device__ __forceinline__ bool never_enters(const DMedium& M) const {
+        return (c0 < 0 && s0 <= 0) || (c0 >= M.Mx && s0 >= 0) || (c1 < 0 && s1 <= 0) || (c1 >= M.My && s1 >= 0) ||
+               (c2 < 0 && s2 <= 0) || (c2 >= M.Mz && s2 >= 0);
+    }
+    // (majorant, distance to the next brick face) at the walk's position
+    __device__ __forceinline__ float query(const DMedium& M, float3 x, float3 w, float& md) {
+        if (M.maj_mode == 0) { md = 1000000.0f; return M.gmaj; }
+        if (!live) init(M, x, w);
+        if (never_enters(M)) { md = 1000000.0f; return 0.0f; }
+        float nt = (n0 <= n1 && n0 <= n2) ? n0 : (n1 <= n2 ? n1 : n2);
+        md = nt - t;
+        return m;
+    }
+    __device__ __forceinline__ void advance(const DMedium& M) {
+        if (!live) return;
+        if (n0 <= n1 && n0 <= n2) { t = n0; n0 += d0; c0 += s0; }
+        else if (n1 <= n2) { t = n1; n1 += d1; c1 += s1; }
+        else { t = n2; n2 += d2; c2 += s2; }
+        m = lookup(M);
+    }
+    __device__ __forceinline__ void move(float dist) { t += dist; }
+};
+
 struct Flight {
     float tau = -1.0f;
     int it = 0;
+    BrickWalk bk;  // majorant bricks of the current segment
     __device__ __forceinline__ float sample(Rng& rng) {
         if (tau < 0.0f) tau = -logf(1.0f - rng.uniform());
         return tau;
@@ -287,12 +352,13 @@ __device__ __forceinline__ float transmittance_rt(const DMedium& M, Rng& rng, fl
     Flight ff;
     for (int it = 0; it < kStepCap; ++it) {
         float md;
-        float maj = gmax(0.0000001f, majorant(M, x, w, md));
+        float maj = gmax(0.0000001f, ff.bk.query(M, x, w, md));
         if (ff.tau < 0.0f) ++tl.steps;
         float t = ff.sample(rng) / maj;
-        if (md < d && t > md) { x = x + w * md; d -= md; ff.cross(maj, md); continue; }
+        if (md < d && t > md) { x = x + w * md; d -= md; ff.cross(maj, md); ff.bk.advance(M); continue; }
         ff.used();
         float dt = gmin(t, gmin(d, md));
+        ff.bk.move(dt);
         x = x + w * dt;
         d -= dt;
         if (d <= 0.0000001f) return T;
@@ -323,11 +389,12 @@ __device__ __forceinline__ void transmittance_rt_bw(const DMedium& M, Rng& rng, 
     Flight ff;
     for (; it < kStepCap; ++it) {
         float md;
-        float maj = gmax(EPS, majorant(M, x, w, md) + 0.1f);
+        float maj = gmax(EPS, ff.bk.query(M, x, w, md) + 0.1f);
         float t = ff.sample(rng) / maj;
-        if (md < d && t > md) { x = x + w * md; d -= md; ff.cross(maj, md); continue; }
+        if (md < d && t > md) { x = x + w * md; d -= md; ff.cross(maj, md); ff.bk.advance(M); continue; }
         ff.used();
         float dt = gmin(t, gmin(d, md));
+        ff.bk.move(dt);
         x = x + w * dt;
         d -= dt;
         if (d <= EPS) break;
@@ -346,11 +413,12 @@ __device__ __forceinline__ void transmittance_rt_bw(const DMedium& M, Rng& rng, 
     ff = Flight();
     for (it = 0; it < kStepCap; ++it) {
         float md;
-        float maj = gmax(EPS, majorant(M, x, w, md) + 0.1f);
+        float maj = gmax(EPS, ff.bk.query(M, x, w, md) + 0.1f);
         float t = ff.sample(rng) / maj;
-        if (md < d && t > md) { x = x + w * md; d -= md; ff.cross(maj, md); continue; }
+        if (md < d && t > md) { x = x + w * md; d -= md; ff.cross(maj, md); ff.bk.advance(M); continue; }
         ff.used();
         float dt = gmin(t, gmin(d, md));
+        ff.bk.move(dt);
         x = x + w * dt;
         d -= dt;
         if (d <= EPS) break;
@@ -374,7 +442,7 @@ __device__ __forceinline__ float transmittance_dt(const DMedium& M, Rng& rng, fl
     Flight ff;
     for (int it = 0; it < kStepCap; ++it) {
         float md;
-        float maj = gmax(0.0000001f, majorant(M, x, w, md));
+        float maj = gmax(0.0000001f, ff.bk.query(M, x, w, md));
         if (ff.tau < 0.0f) ++tl.steps;
         float dt = ff.sample(rng) / maj;
         float t = gmin(md, dt);
@@ -383,8 +451,9 @@ __device__ __forceinline__ float transmittance_dt(const DMedium& M, Rng& rng, fl
         // the end test precedes the brick-crossing restart (the reference's
         // order, which the constant majorant never distinguishes)
         if (d <= 0.0000001f) return 1.0f;
-        if (dt > md) { ff.cross(maj, md); continue; }
+        if (dt > md) { ff.cross(maj, md); ff.bk.advance(M); continue; }
         ff.used();
+        ff.bk.move(t);
         if (rng.uniform() < sigma(M, x, tl) / maj) return 0.0f;
     }
     raise_status(status, 4);
@@ -406,14 +475,15 @@ __device__ __forceinline__ void transmittance_dt_bw(const DMedium& M, Rng& rng, 
     Flight ff;
     for (; it < kStepCap; ++it) {
         float md;
-        float maj = gmax(0.0000001f, majorant(M, x, w, md) + 0.1f);
+        float maj = gmax(0.0000001f, ff.bk.query(M, x, w, md) + 0.1f);
         float dt = ff.sample(rng) / maj;
         float t = gmin(md, dt);
         x = x + w * t;
         d -= t;
         if (d <= 0.0000001f) break;
-        if (dt > md) { ff.cross(maj, md); continue; }
+        if (dt > md) { ff.cross(maj, md); ff.bk.advance(M); continue; }
         ff.used();
+        ff.bk.move(t);
         if (rng.uniform() < sigma(M, x, tl) / maj) return;
     }
     if (it == kStepCap) { raise_status(status, 4); return; }
@@ -423,14 +493,15 @@ __device__ __forceinline__ void transmittance_dt_bw(const DMedium& M, Rng& rng, 
     ff = Flight();
     for (it = 0; it < kStepCap; ++it) {
         float md;
-        float maj = gmax(0.0000001f, majorant(M, x, w, md) + 0.1f);
+        float maj = gmax(0.0000001f, ff.bk.query(M, x, w, md) + 0.1f);
         float dt = ff.sample(rng) / maj;
         float t = gmin(md, dt);
         x = x + w * t;
         d -= t;
         if (d <= 0.0000001f) break;
-        if (dt > md) { ff.cross(maj, md); continue; }
+        if (dt > md) { ff.cross(maj, md); ff.bk.advance(M); continue; }
         ff.used();
+        ff.bk.move(t);
         rng.advance();
         float Pc = sigma(M, x, tl) / maj;
         sigma_bw(M, x, -dL_dT / maj / (1.0f - Pc), tl);
