@@ -51,8 +51,8 @@ enum { VRT_PI_NEE = 0, VRT_PI_DT = 1 };
 enum { VRT_BW_NEE_DS = 0, VRT_BW_DT = 1, VRT_BW_NEE_DRT = 2 };
 
 /* A node-centred FP32 grid, the Grid3D parameter (rendervous _maps.py:2319-2365).
-   Element (z,y,x,c) is data[z*strides[0] + y*strides[1] + x*strides[2] + c]; the
-   channel stride must be 1.  grad uses the same strides and may be NULL. */
+   Element (z,y,x,c) is data[z*strides[0] + y*strides[1] + x*strides[2] + c]; with
+   C > 1 the channel stride must be 1.  grad uses the same strides and may be NULL. */
 typedef struct vrt_grid {
     const float* data;
     float* grad;
@@ -164,6 +164,38 @@ int vrt_radiance_fw(vrt_context* ctx, const vrt_medium* m, int32_t integrator, c
                     uint64_t seed, float* R, void* stream);
 int vrt_radiance_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const float* rays, int64_t n,
                     uint64_t seed, const float* dL_dR, void* stream);
+
+/* Radiance cache (no reference counterpart): a 16-level dense grid encoding
+   (2 features per level, FP32 parameters) plus degree-3 real spherical
+   harmonics of the direction feed an MLP 64 -> 4 x 64 (ReLU) -> 16 (RGB in
+   the first 3), run on the tensor cores with BF16 operands and FP32
+   accumulation.  weights: W1..W4 [64][64] then W5 [16][64], row-major FP32.
+   Level l of the grid is a (res[l]+1)^3 x 2 node array at the running offset
+   of the previous levels; positions map to the grid through [bmin, bmax]. */
+typedef struct vrt_cache {
+    float* grid;
+    float* grid_grad;
+    float* weights;
+    float* weights_grad;
+    int32_t levels;                  /* must be 16 */
+    int32_t res[16];
+    float bmin[3], bmax[3];
+} vrt_cache;
+int64_t vrt_cache_grid_size(const int32_t res[16]);
+/* MLP alone on given inputs [n,64] -> out [n,16] (tensor cores). */
+int vrt_cache_mlp_fw(const float* weights, const float* inputs, int64_t n, float* out, void* stream);
+/* Encoding + MLP: pos [n,3], dir [n,3] -> rgb [n,3]. */
+int vrt_cache_infer(const vrt_cache* c, const float* pos, const float* dir, int64_t n, float* rgb, void* stream);
+/* One pass of the relative-L2 loss against target [n,3]; adds sum(loss)/n into *loss
+   and accumulates the gradients into grid_grad and weights_grad. */
+int vrt_cache_train(const vrt_cache* c, const float* pos, const float* dir, const float* target, int64_t n,
+                    float* loss, void* stream);
+/* Adam step over n parameters (bias-corrected, step >= 1); clears grads. */
+int vrt_cache_adam(float* params, float* grads, float* m, float* v, int64_t n, float lr, float beta1, float beta2,
+                   float eps, int32_t step, void* stream);
+/* Waits for `stream`; returns VRT_OK, or VRT_E_ITER_CAP when a cache kernel
+   gave up waiting for the tensor cores since the last call (and clears it). */
+int vrt_cache_status(void* stream);
 
 /* Camera capture (SensorsBase.capture, _maps.py:1741-1749, capture kernels
    _maps.py:509-746): rgb [views,H,W,3] = mean over spp paths; sample s of pixel p
