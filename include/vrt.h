@@ -186,13 +186,19 @@ int64_t vrt_cache_grid_size(const int32_t res[16]);
 int vrt_cache_mlp_fw(const float* weights, const float* inputs, int64_t n, float* out, void* stream);
 /* Encoding + MLP: pos [n,3], dir [n,3] -> rgb [n,3]. */
 int vrt_cache_infer(const vrt_cache* c, const float* pos, const float* dir, int64_t n, float* rgb, void* stream);
-/* One pass of the relative-L2 loss against target [n,3]; adds sum(loss)/n into *loss
-   and accumulates the gradients into grid_grad and weights_grad. */
+/* One pass of the relative-L2 loss sum_c (y_c - t_c)^2 / (y_c^2 + 0.01) (y held
+   constant in the denominator) against target [n,3]; adds the sum over rows / n
+   into *loss and accumulates the gradients into grid_grad and weights_grad.
+   Rows with a non-finite target are skipped. */
 int vrt_cache_train(const vrt_cache* c, const float* pos, const float* dir, const float* target, int64_t n,
                     float* loss, void* stream);
 /* Adam step over n parameters (bias-corrected, step >= 1); clears grads. */
 int vrt_cache_adam(float* params, float* grads, float* m, float* v, int64_t n, float lr, float beta1, float beta2,
                    float eps, int32_t step, void* stream);
+/* Adds the cache's estimate for path-prefix queries (the planes written by
+   vrt_capture_prefix_fw): rgb[row % npix] += scale * W[row] * cache(pos, dir). */
+int vrt_cache_resolve(const vrt_cache* c, const float* queries, int64_t n, int64_t npix, float scale, float* rgb,
+                      void* stream);
 /* Waits for `stream`; returns VRT_OK, or VRT_E_ITER_CAP when a cache kernel
    gave up waiting for the tensor cores since the last call (and clears it). */
 int vrt_cache_status(void* stream);
@@ -205,6 +211,25 @@ int vrt_capture_fw(vrt_context* ctx, const vrt_medium* m, int32_t integrator, co
                    uint64_t seed, float* rgb, void* stream);
 int vrt_capture_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const vrt_camera* cam, int32_t spp,
                    uint64_t seed, const float* dL_drgb, void* stream);
+/* Radiance-cache forms of the NEE capture (no reference counterpart).
+   Prefix: the integrator of vrt_capture_fw, but a path stops at its (cut+1)-th
+   real collision and records a query there; rgb ACCUMULATES prefix / spp (not
+   cleared) and queries is 3 planes [n,3] (position, arrival direction,
+   throughput; 0 throughput where the path ended before the cut), n = spp *
+   pixels, row = Philox path id.  vrt_cache_resolve then adds the cache's part.
+   Training samples: n_paths paths from pixels drawn by each path's first draw;
+   with c == NULL they run to the end (the medium's bounce cap applies), else
+   they stop into the cache c at their (cut+1)-th collision (cut >= rec), as
+   the rendered paths do at theirs.  The first rec <= 8 collisions of path i
+   fill rows i*rec.. of samples = 4 planes [n_paths*rec, 3]: position, arrival
+   direction, in-scattered radiance target (R_final - R_k) / W_k and W_k.
+   Rows of collisions the path never reached hold NaN targets, which
+   vrt_cache_train skips.  work: 12 * n_paths floats of device scratch. */
+int vrt_capture_prefix_fw(vrt_context* ctx, const vrt_medium* m, const vrt_camera* cam, int32_t spp, uint64_t seed,
+                          int32_t cut, float* rgb, float* queries, void* stream);
+int vrt_capture_train_samples(vrt_context* ctx, const vrt_medium* m, const vrt_camera* cam, const vrt_cache* c,
+                              int32_t cut, int64_t n_paths, uint64_t seed, int32_t rec, float* samples, float* work,
+                              void* stream);
 /* CDEF-END */
 
 #ifdef __cplusplus

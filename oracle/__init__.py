@@ -287,6 +287,27 @@ def capture_bw(scene: OracleScene, bw_mode: str, poses, width, height, fov, jitt
     L.orc_capture_bw(scene.s, BW_MODES[bw_mode], cam, spp, seed, ptr(ffi, g))
 
 
+def capture_prefix(scene: OracleScene, poses, width, height, fov, jittered, spp, seed, cut):
+    """Radiance-cache prefix: (rgb of the prefixes, queries [3, n, 3])."""
+    ffi, L = lib()
+    cam, keep = make_camera(poses, width, height, fov, jittered)
+    rgb = np.zeros((keep.shape[0], height, width, 3), np.float32)
+    n = keep.shape[0] * height * width * spp
+    q = np.empty((3, n, 3), np.float32)
+    L.orc_capture_prefix(scene.s, cam, spp, seed, cut, ptr(ffi, rgb), ptr(ffi, q))
+    return rgb, q
+
+
+def train_samples(scene: OracleScene, poses, width, height, fov, jittered, n_paths, seed, rec, cut=-1):
+    """Radiance-cache training samples [4, n_paths*rec, 3]: position, direction, target, W.
+    cut >= 0: paths stop at their (cut+1)-th collision (a cache returning 0)."""
+    ffi, L = lib()
+    cam, keep = make_camera(poses, width, height, fov, jittered)
+    out = np.empty((4, n_paths * rec, 3), np.float32)
+    L.orc_train_samples(scene.s, cam, n_paths, seed, rec, cut, ptr(ffi, out))
+    return out
+
+
 def set_threads(n: int) -> None:
     _, L = lib()
     L.orc_set_threads(n)

@@ -106,6 +106,18 @@ void orc_radiance_bw(const orc_scene* s, int32_t bw_mode, const float* rays, int
 
 void orc_capture_fw(const orc_scene* s, int32_t integrator, const orc_camera* cam, int32_t spp, uint64_t seed, float* rgb, orc_counters* c);
 void orc_capture_bw(const orc_scene* s, int32_t bw_mode, const orc_camera* cam, int32_t spp, uint64_t seed, const float* dL_drgb);
+/* Radiance-cache forms of the NEE capture.  prefix: paths stop at their
+   (cut+1)-th real collision; rgb += prefix / spp; queries = 3 planes [n,3]
+   (position, direction, throughput W; W = 0 where the path ended earlier),
+   n = spp * pixels, row = Philox path id.  train: n_paths paths from pixels
+   drawn by each path's first u32; samples = 4 planes [n_paths*rec, 3]
+   (position, direction, target (R_final - R_k)/W_k, W_k); unused rows have
+   NaN targets; rec <= 8.  cut >= 0 stops training paths at their (cut+1)-th
+   collision with nothing added for the rest (a cache that returns 0). */
+void orc_capture_prefix(const orc_scene* s, const orc_camera* cam, int32_t spp, uint64_t seed, int32_t cut, float* rgb,
+                        float* queries);
+void orc_train_samples(const orc_scene* s, const orc_camera* cam, int64_t n_paths, uint64_t seed, int32_t rec,
+                       int32_t cut, float* samples);
 /* CDEF-END */
 #ifdef __cplusplus
 }

@@ -777,8 +777,22 @@ template <typename T> V3<T> environment_sampler(const Scene<T>& S, Rng& rng, V3<
 // light sampled after the environment at every real collision, and an
 // optional bounce cap (0 keeps the reference's uncapped loop).
 // ---------------------------------------------------------------------------
+// Hooks of the radiance-cache forms (no reference counterpart).  cut >= 0: a
+// path reaching its (cut+1)-th real collision records (x, w, W) there and stops
+// (the cache adds W * L(x, w) later).  rec > 0: the first rec collisions record
+// (x, w, W, R so far) so the caller can form the in-scattered radiance targets
+// (R_final - R_k) / W_k.
+template <typename T> struct PathHooks {
+    int cut = -1, rec = 0;
+    bool queried = false;
+    V3<T> qx, qw, qW;
+    int nrec = 0;
+    V3<T> rx[8], rw[8], rW[8], rR[8];
+};
+
 template <typename T>
-V3<T> path_integrator_NEE(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, bool only_scatters, Counters& cnt) {
+V3<T> path_integrator_NEE(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, bool only_scatters, Counters& cnt,
+                          PathHooks<T>* hk = nullptr) {
     T tMin, tMax;
     S.boundary(x, w, tMin, tMax);
     x += w * tMin;
@@ -802,6 +816,15 @@ V3<T> path_integrator_NEE(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, bool on
         T Pc = s / m;
         if ((T)rng.uniform() >= Pc) { d -= t; continue; }
         ++cnt.vertices;
+        if (hk && hk->cut >= 0 && bounces == hk->cut) {
+            hk->queried = true;
+            hk->qx = x; hk->qw = w; hk->qW = W;
+            return R;
+        }
+        if (hk && bounces < hk->rec) {
+            hk->rx[bounces] = x; hk->rw[bounces] = w; hk->rW[bounces] = W; hk->rR[bounces] = R;
+            hk->nrec = bounces + 1;
+        }
         V3<T> sa = S.albedo(x);
         V3<T> em = S.emission();
         R += W * (V3<T>(T(1)) - sa) * em;
@@ -814,7 +837,8 @@ V3<T> path_integrator_NEE(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, bool on
             T T_sun = transmittance(S, rng, x, sun_dir, &cnt.steps);
             R += W * T_sun * sun_L * phase(S, w, sun_dir);
         }
-        if (S.s.max_bounces > 0 && ++bounces >= S.s.max_bounces) return R;
+        ++bounces;
+        if (S.s.max_bounces > 0 && bounces >= S.s.max_bounces) return R;
         V3<T> wo;
         T rho = phase_sampler(S, rng, w, wo);
         W *= rho;
@@ -1272,6 +1296,9 @@ void camera_ray(const orc_camera& cam, int view, int row, int col, Rng& rng, V3<
 
 inline uint64_t capture_path_id(int64_t pixel, int s, int64_t npix) { return (uint64_t)s * (uint64_t)npix + (uint64_t)pixel; }
 
+// pixel of a radiance-cache training path: the path's first draw, scaled to npix
+inline int64_t random_pixel(Rng& rng, int64_t npix) { return (int64_t)(((uint64_t)rng.u32() * (uint64_t)npix) >> 32); }
+
 template <typename T> V3<T> radiance(const Scene<T>& S, int integrator, Rng& rng, V3<T> x, V3<T> w, Counters& c) {
     return integrator == 0 ? path_integrator_NEE(S, rng, x, w, false, c) : path_integrator_DT(S, rng, x, w, c);
 }
@@ -1511,6 +1538,73 @@ void orc_capture_fw(const orc_scene* s, int32_t integrator, const orc_camera* ca
         steps += cnt.steps;
     }
     if (c) { c->paths = npix * spp; c->vertices = verts; c->steps = steps; }
+}
+
+void orc_capture_prefix(const orc_scene* s, const orc_camera* cam, int32_t spp, uint64_t seed, int32_t cut, float* rgb,
+                        float* queries) {
+    Scene<float> S(*s);
+    int64_t npix = (int64_t)cam->views * cam->height * cam->width;
+    int64_t n = npix * spp;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t p = 0; p < npix; ++p) {
+        int view = (int)(p / ((int64_t)cam->height * cam->width));
+        int rem = (int)(p % ((int64_t)cam->height * cam->width));
+        V3<float> acc(0.0f);
+        Counters cnt;
+        for (int sidx = 0; sidx < spp; ++sidx) {
+            uint64_t pid = capture_path_id(p, sidx, npix);
+            Rng rng(seed, pid, 0);
+            V3<float> x, w;
+            camera_ray(*cam, view, rem / cam->width, rem % cam->width, rng, x, w);
+            PathHooks<float> hk;
+            hk.cut = cut;
+            acc += path_integrator_NEE(S, rng, x, w, false, cnt, &hk);
+            V3<float> qx(0.0f), qw(0.0f, 0.0f, 1.0f), qW(0.0f);
+            if (hk.queried) { qx = hk.qx; qw = hk.qw; qW = hk.qW; }
+            float* q = queries + 3 * pid;
+            q[0] = qx.x; q[1] = qx.y; q[2] = qx.z;
+            q[3 * n + 0] = qw.x; q[3 * n + 1] = qw.y; q[3 * n + 2] = qw.z;
+            q[6 * n + 0] = qW.x; q[6 * n + 1] = qW.y; q[6 * n + 2] = qW.z;
+        }
+        rgb[3 * p] += acc.x / (float)spp;
+        rgb[3 * p + 1] += acc.y / (float)spp;
+        rgb[3 * p + 2] += acc.z / (float)spp;
+    }
+}
+
+void orc_train_samples(const orc_scene* s, const orc_camera* cam, int64_t n_paths, uint64_t seed, int32_t rec,
+                       int32_t cut, float* samples) {
+    Scene<float> S(*s);
+    int64_t npix = (int64_t)cam->views * cam->height * cam->width;
+    int64_t n = n_paths * rec;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t i = 0; i < n_paths; ++i) {
+        Rng rng(seed, (uint64_t)i, 0);
+        int64_t p = random_pixel(rng, npix);
+        int view = (int)(p / ((int64_t)cam->height * cam->width));
+        int rem = (int)(p % ((int64_t)cam->height * cam->width));
+        V3<float> x, w;
+        camera_ray(*cam, view, rem / cam->width, rem % cam->width, rng, x, w);
+        PathHooks<float> hk;
+        hk.rec = rec < 8 ? rec : 8;
+        hk.cut = cut;
+        Counters cnt;
+        V3<float> R = path_integrator_NEE(S, rng, x, w, false, cnt, &hk);
+        for (int k = 0; k < rec; ++k) {
+            int64_t slot = i * rec + k;
+            float* o = samples + 3 * slot;
+            V3<float> px(0.0f), pw(0.0f, 0.0f, 1.0f), tg(NAN), wt(0.0f);
+            if (k < hk.nrec) {
+                px = hk.rx[k]; pw = hk.rw[k]; wt = hk.rW[k];
+                V3<float> num = R - hk.rR[k];
+                tg = V3<float>(num.x / wt.x, num.y / wt.y, num.z / wt.z);
+            }
+            o[0] = px.x; o[1] = px.y; o[2] = px.z;
+            o[3 * n + 0] = pw.x; o[3 * n + 1] = pw.y; o[3 * n + 2] = pw.z;
+            o[6 * n + 0] = tg.x; o[6 * n + 1] = tg.y; o[6 * n + 2] = tg.z;
+            o[9 * n + 0] = wt.x; o[9 * n + 1] = wt.y; o[9 * n + 2] = wt.z;
+        }
+    }
 }
 
 void orc_capture_bw(const orc_scene* s, int32_t bw_mode, const orc_camera* cam, int32_t spp, uint64_t seed, const float* dL_drgb) {

@@ -113,3 +113,82 @@ def mlp_forward(weights: torch.Tensor, inputs: torch.Tensor) -> torch.Tensor:
     _lib.check(lib.vrt_cache_mlp_fw(_lib.fptr(weights.contiguous()), _lib.fptr(x), x.shape[0], _lib.fptr(out),
                                     _lib.stream_handle(x.device)), "vrt_cache_mlp_fw")
     return out
+
+
+class CachedRenderer:
+    """Renders an NEE path-integrator field through a camera with the radiance
+    cache: every path is traced without bias for its first `cut` collisions
+    (next-event estimation at each) and at its (cut+1)-th collision adds
+    W * cache(x, w) instead of continuing.  Each frame first trains the cache on
+    `train_paths` full paths from random pixels (their first `rec` collisions
+    give 2^16 samples at the defaults), then renders `spp` paths per pixel with
+    it.  Training paths stop into the cache themselves at their
+    (train_cut+1)-th collision (self-training; train_cut < 0 traces them to
+    the end).  `render()` returns the mean of its frames.
+    """
+
+    def __init__(self, field, camera, cache: RadianceCache = None, *, cut: int = 2, train_paths: int = 1 << 14,
+                 rec: int = 4, train_cut: int = 16, lr: float = 1e-2, seed: int = 0):
+        field = field.cast(input_dim=6)
+        if getattr(field, "FW", None) != 0:
+            raise NotImplementedError("the radiance cache terminates NEE path-integrator paths")
+        self.desc = field.lower()
+        self.dev = self.desc.sigma.device
+        self.m = self.desc.to_struct()
+        self.cam, self._poses = camera.to_struct(self.dev)
+        self.shape = (camera.views, camera.height, camera.width, 3)
+        self.npix = camera.views * camera.height * camera.width
+        bmin = self.desc.box_min.detach().float().cpu()
+        bmax = self.desc.box_max.detach().float().cpu()
+        self.cache = cache if cache is not None else RadianceCache(bmin, bmax, self.dev, seed=seed)
+        self.cut, self.train_paths, self.rec, self.lr = int(cut), int(train_paths), int(rec), float(lr)
+        self.train_cut = int(train_cut)
+        self.samples = torch.empty(4, self.train_paths * self.rec, 3, device=self.dev)
+        self.work = torch.empty(12 * self.train_paths, device=self.dev)
+        self._queries = None
+        self._seed = (int(seed) * 0x9E3779B1 + 0x1234567) & 0xFFFFFFFF
+        self.frames = 0
+        self.last_loss = None
+
+    def _next_seed(self) -> int:
+        self._seed = (self._seed * 6364136223846793005 + 1442695040888963407) & 0xFFFFFFFFFFFFFFFF
+        return self._seed >> 16
+
+    def train_frame(self) -> torch.Tensor:
+        ffi, lib = _lib.ffi_lib()
+        vctx = _lib.context(self.dev)
+        c = self.cache.struct() if self.train_cut >= 0 else ffi.NULL
+        _lib.check(lib.vrt_capture_train_samples(vctx.ptr, self.m, self.cam, c, self.train_cut, self.train_paths,
+                                                 self._next_seed(), self.rec, _lib.fptr(self.samples),
+                                                 _lib.fptr(self.work), _lib.stream_handle(self.dev)),
+                   "vrt_capture_train_samples")
+        self.last_loss = self.cache.train_step(self.samples[0], self.samples[1], self.samples[2], lr=self.lr)
+        return self.last_loss
+
+    def render_frame(self, rgb: torch.Tensor, spp: int = 1) -> None:
+        """Adds one spp-sample estimate into rgb [views, H, W, 3]."""
+        ffi, lib = _lib.ffi_lib()
+        n = self.npix * spp
+        if self._queries is None or self._queries.shape[1] != n:
+            self._queries = torch.empty(3, n, 3, device=self.dev)
+        vctx = _lib.context(self.dev)
+        stream = _lib.stream_handle(self.dev)
+        _lib.check(lib.vrt_capture_prefix_fw(vctx.ptr, self.m, self.cam, spp, self._next_seed(), self.cut,
+                                             _lib.fptr(rgb), _lib.fptr(self._queries), stream), "vrt_capture_prefix_fw")
+        _lib.check(lib.vrt_cache_resolve(self.cache.struct(), _lib.fptr(self._queries), n, self.npix, 1.0 / spp,
+                                         _lib.fptr(rgb), stream), "vrt_cache_resolve")
+        self.frames += 1
+
+    def render(self, frames: int, spp: int = 1, train: bool = True) -> torch.Tensor:
+        rgb = torch.zeros(self.shape, device=self.dev)
+        for _ in range(frames):
+            if train:
+                self.train_frame()
+            self.render_frame(rgb, spp)
+        return rgb / frames
+
+    def check(self) -> None:
+        """Raises if a kernel of the renderer or the cache reported a device error."""
+        ffi, lib = _lib.ffi_lib()
+        _lib.context(self.dev).sync()
+        _lib.check(lib.vrt_cache_status(_lib.stream_handle(self.dev)), "radiance cache")

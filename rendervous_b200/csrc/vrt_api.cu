@@ -416,4 +416,51 @@ int vrt_capture_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const
                               ctx->scratch, ctx->num_sms, (cudaStream_t)stream);
 }
 
+int vrt_capture_prefix_fw(vrt_context* ctx, const vrt_medium* m, const vrt_camera* cam, int32_t spp, uint64_t seed,
+                          int32_t cut, float* rgb, float* queries, void* stream) {
+    int st = check_ctx(ctx);
+    if (st) return st;
+    if (spp < 1 || cut < 0) return VRT_E_INVALID_ARGUMENT;
+    DMedium M;
+    if ((st = to_dmedium(m, M))) return st;
+    PathSrc S;
+    std::memset(&S, 0, sizeof(S));
+    if ((st = to_dcamera(cam, S.cam))) return st;
+    if (!rgb || !queries) return VRT_E_NULL_POINTER;
+    S.is_camera = 1;
+    S.npix = (long long)S.cam.views * S.cam.height * S.cam.width;
+    const uint64_t n = (uint64_t)S.npix * (uint64_t)spp;
+    CacheIO io = {cut, 0, queries, nullptr, nullptr, (long long)n};
+    return launch_cache_paths(M, FW_CUT, S, n, seed, rgb, 1.0f / (float)spp, io, ctx->scratch, ctx->num_sms,
+                              (cudaStream_t)stream);
+}
+
+int vrt_capture_train_samples(vrt_context* ctx, const vrt_medium* m, const vrt_camera* cam, const vrt_cache* c,
+                              int32_t cut, int64_t n_paths, uint64_t seed, int32_t rec, float* samples, float* work,
+                              void* stream) {
+    int st = check_ctx(ctx);
+    if (st) return st;
+    if (n_paths < 0 || rec < 1 || rec > 8) return VRT_E_INVALID_ARGUMENT;
+    if (c && cut < rec) return VRT_E_INVALID_ARGUMENT;
+    DMedium M;
+    if ((st = to_dmedium(m, M))) return st;
+    PathSrc S;
+    std::memset(&S, 0, sizeof(S));
+    if ((st = to_dcamera(cam, S.cam))) return st;
+    if (!samples || !work) return VRT_E_NULL_POINTER;
+    S.is_camera = 1;
+    S.npix = (long long)S.cam.views * S.cam.height * S.cam.width;
+    if (S.npix >= (1ll << 32)) return VRT_E_BAD_SHAPE;
+    if (n_paths == 0) return VRT_OK;
+    float* pR = work;
+    float* q = work + 3 * n_paths;
+    CacheIO io = {c ? cut : -1, rec, q, samples, pR, (long long)n_paths};
+    cudaStream_t s = (cudaStream_t)stream;
+    if ((st = launch_cache_paths(M, FW_TRAIN, S, (uint64_t)n_paths, seed, nullptr, 0.0f, io, ctx->scratch,
+                                 ctx->num_sms, s)))
+        return st;
+    if (c && (st = vrt_cache_resolve(c, q, n_paths, n_paths, 1.0f, pR, stream))) return st;
+    return launch_cache_targets(samples, pR, n_paths, rec, s);
+}
+
 }  // extern "C"

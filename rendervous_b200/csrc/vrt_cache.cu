@@ -261,11 +261,17 @@ struct InferSmem {
     int fail;
 };
 
-// rows: n samples; inputs either given (X [n,64]) or encoded from (pos, dir)
-template <bool ENCODE>
+enum : int { IN_GIVEN = 0, IN_ENCODE = 1, IN_RESOLVE = 2 };
+
+// rows: n samples.  IN_GIVEN: inputs X [n,64], out [n,16].  IN_ENCODE: inputs
+// encoded from (pos, dir), out = rgb [n,3].  IN_RESOLVE: as IN_ENCODE with a
+// throughput W per row: out[row % npix] += scale * W * rgb (rows with W == 0
+// are skipped).
+template <int IN>
 __global__ void __launch_bounds__(128) k_mlp_infer(Enc E, const float* __restrict__ w, const float* __restrict__ X,
                                                     const float* __restrict__ pos, const float* __restrict__ dir,
-                                                    int64_t n, float* __restrict__ out, int out_stride) {
+                                                    const float* __restrict__ thr, int64_t n, float* __restrict__ out,
+                                                    int out_stride, int64_t npix, float scale) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     InferSmem& S = *reinterpret_cast<InferSmem*>(smem_align128(smem_raw));
     const int t = threadIdx.x;
@@ -287,8 +293,14 @@ __global__ void __launch_bounds__(128) k_mlp_infer(Enc E, const float* __restric
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int64_t row = tile * kTile + t;
         float x[64];
-        if (row < n) {
-            if (ENCODE) encode(E, ld3(pos + 3 * row), ld3(dir + 3 * row), x);
+        float3 Wr = f3(0.0f);
+        bool live = row < n;
+        if (IN == IN_RESOLVE && live) {
+            Wr = ld3(thr + 3 * row);
+            live = Wr.x != 0.0f || Wr.y != 0.0f || Wr.z != 0.0f;
+        }
+        if (live) {
+            if (IN != IN_GIVEN) encode(E, ld3(pos + 3 * row), ld3(dir + 3 * row), x);
             else {
 #pragma unroll
                 for (int i = 0; i < 64; i += 4) {
@@ -317,7 +329,14 @@ __global__ void __launch_bounds__(128) k_mlp_infer(Enc E, const float* __restric
             __syncthreads();  // every row is read before the tile is rewritten
         }
         if (S.fail) break;
-        if (row < n) {
+        if (IN == IN_RESOLVE) {
+            if (live) {
+                float* o = out + 3 * (row % npix);
+                atomicAdd(o + 0, scale * Wr.x * x[0]);
+                atomicAdd(o + 1, scale * Wr.y * x[1]);
+                atomicAdd(o + 2, scale * Wr.z * x[2]);
+            }
+        } else if (live) {
             for (int c = 0; c < out_stride; ++c) out[row * out_stride + c] = x[c];
         }
     }
@@ -393,7 +412,12 @@ __global__ void __launch_bounds__(128) k_mlp_train(Enc E, const float* __restric
     const int64_t tiles = (n + kTile - 1) / kTile;
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int64_t row = tile * kTile + t;
-        const bool valid = row < n;
+        bool valid = row < n;
+        float3 tg3 = f3(0.0f);
+        if (valid) {  // rows without a finite target (a path that ended before the vertex) are skipped
+            tg3 = ld3(target + 3 * row);
+            valid = isfinite(tg3.x) && isfinite(tg3.y) && isfinite(tg3.z);
+        }
         float3 p = f3(0.0f), d = make_float3(0.0f, 0.0f, 1.0f);
         float x[64];
         if (valid) {
@@ -426,7 +450,7 @@ __global__ void __launch_bounds__(128) k_mlp_train(Enc E, const float* __restric
         for (int i = 0; i < 16; ++i) g16[i] = 0.0f;
         if (valid) {
             for (int c = 0; c < 3; ++c) {
-                const float y = x[c], tg = __ldg(target + 3 * row + c);
+                const float y = x[c], tg = c == 0 ? tg3.x : (c == 1 ? tg3.y : tg3.z);
                 const float den = y * y + 0.01f;
                 const float r = y - tg;
                 lsum += r * r / den * inv_batch;
@@ -571,9 +595,10 @@ extern "C" int vrt_cache_mlp_fw(const float* weights, const float* inputs, int64
     if (((uintptr_t)inputs & 15u) != 0) return VRT_E_INVALID_ARGUMENT;
     Enc E = {};
     size_t smem = sizeof(InferSmem) + 128;
-    int blocks = mlp_blocks(k_mlp_infer<false>, smem, n, 4);
+    int blocks = mlp_blocks(k_mlp_infer<IN_GIVEN>, smem, n, 4);
     if (blocks <= 0) return VRT_E_CUDA;
-    k_mlp_infer<false><<<blocks, kTile, smem, (cudaStream_t)stream>>>(E, weights, inputs, nullptr, nullptr, n, out, kOut);
+    k_mlp_infer<IN_GIVEN><<<blocks, kTile, smem, (cudaStream_t)stream>>>(E, weights, inputs, nullptr, nullptr, nullptr,
+                                                                         n, out, kOut, 0, 0.0f);
     return launch_status(cudaGetLastError());
 }
 
@@ -586,9 +611,26 @@ extern "C" int vrt_cache_infer(const vrt_cache* c, const float* pos, const float
     if (n == 0) return VRT_OK;
     if (!pos || !dir || !rgb || !c->weights) return VRT_E_NULL_POINTER;
     size_t smem = sizeof(InferSmem) + 128;
-    int blocks = mlp_blocks(k_mlp_infer<true>, smem, n, 4);
+    int blocks = mlp_blocks(k_mlp_infer<IN_ENCODE>, smem, n, 4);
     if (blocks <= 0) return VRT_E_CUDA;
-    k_mlp_infer<true><<<blocks, kTile, smem, (cudaStream_t)stream>>>(E, c->weights, nullptr, pos, dir, n, rgb, 3);
+    k_mlp_infer<IN_ENCODE><<<blocks, kTile, smem, (cudaStream_t)stream>>>(E, c->weights, nullptr, pos, dir, nullptr, n,
+                                                                          rgb, 3, 0, 0.0f);
+    return launch_status(cudaGetLastError());
+}
+
+extern "C" int vrt_cache_resolve(const vrt_cache* c, const float* queries, int64_t n, int64_t npix, float scale,
+                                 float* rgb, void* stream) {
+    Enc E;
+    int st = to_enc(c, E);
+    if (st) return st;
+    if (n < 0 || npix < 1) return VRT_E_BAD_SHAPE;
+    if (n == 0) return VRT_OK;
+    if (!queries || !rgb || !c->weights) return VRT_E_NULL_POINTER;
+    size_t smem = sizeof(InferSmem) + 128;
+    int blocks = mlp_blocks(k_mlp_infer<IN_RESOLVE>, smem, n, 4);
+    if (blocks <= 0) return VRT_E_CUDA;
+    k_mlp_infer<IN_RESOLVE><<<blocks, kTile, smem, (cudaStream_t)stream>>>(
+        E, c->weights, nullptr, queries, queries + 3 * n, queries + 6 * n, n, rgb, 3, npix, scale);
     return launch_status(cudaGetLastError());
 }
 

@@ -31,6 +31,12 @@ int launch_radiance_fw(const DMedium& M, int integrator, const PathSrc& src, uin
 int launch_radiance_bw(const DMedium& M, int bw_mode, const PathSrc& src, uint64_t n_paths, uint64_t seed,
                        const float* dL, float div, DScratch* scratch, int num_sms, cudaStream_t stream);
 
+// Radiance-cache forms of the forward NEE kernel (mode FW_CUT or FW_TRAIN).
+int launch_cache_paths(const DMedium& M, int mode, const PathSrc& src, uint64_t n_paths, uint64_t seed, float* out,
+                       float scale, const CacheIO& io, DScratch* scratch, int num_sms, cudaStream_t stream);
+// Training targets from the recorded collisions and the per-path estimates.
+int launch_cache_targets(float* smp, const float* pR, long long n_paths, int rec, cudaStream_t stream);
+
 // The NEE_DS adjoint as a persistent state machine (vrt_adjoint.cu).
 int launch_nee_ds_bw(const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed, const float* dL,
                      float div, DScratch* scratch, int num_sms, cudaStream_t stream);

@@ -86,7 +86,44 @@ struct NeeLane {
     int state;
     long long oidx;
     uint32_t steps_path;
+    long long pid;  // cache forms: the path's row
+    int nrec;       // FW_TRAIN: collisions recorded so far
 };
+
+__device__ __forceinline__ void st3(float* p, float3 v) {
+    p[0] = v.x;
+    p[1] = v.y;
+    p[2] = v.z;
+}
+
+// A finished path: its estimate goes to the image / ray output.  A training
+// path stores its estimate (the cache query, if any, is added later) and marks
+// the collisions it never reached (NaN target, zero throughput).
+template <int MODE>
+__device__ __forceinline__ void end_path(const PathSrc& S, const NeeLane& L, float* out, float scale,
+                                         const CacheIO& io) {
+    if (MODE == FW_TRAIN) {
+        const long long n = io.rows * io.rec;
+        st3(io.pR + 3 * L.pid, L.R);
+        for (int k = L.nrec; k < io.rec; ++k) {
+            float* o = io.smp + 3 * (L.pid * io.rec + k);
+            st3(o, f3(0.0f));
+            st3(o + 3 * n, make_float3(0.0f, 0.0f, 1.0f));
+            st3(o + 6 * n, f3(__int_as_float(0x7fc00000)));
+            st3(o + 9 * n, f3(0.0f));
+        }
+        return;
+    }
+    if (S.is_camera) {
+        atomicAdd(out + 3 * L.oidx + 0, L.R.x * scale);
+        atomicAdd(out + 3 * L.oidx + 1, L.R.y * scale);
+        atomicAdd(out + 3 * L.oidx + 2, L.R.z * scale);
+    } else {
+        out[3 * L.oidx + 0] = L.R.x;
+        out[3 * L.oidx + 1] = L.R.y;
+        out[3 * L.oidx + 2] = L.R.z;
+    }
+}
 
 // Begin a transmittance segment from x0 along dir (the transmittance map's own
 // boundary test, vr_transmittance_RT.h:5-10 / _DT.h:3-8).  DDA segments are
@@ -113,7 +150,8 @@ __device__ __forceinline__ int start_shadow(const DMedium& M, NeeLane& L, float3
 
 // vr_path_integrator_NEE.h:57-62 plus the optional bounce cap
 __device__ __forceinline__ int after_nee(const DMedium& M, NeeLane& L) {
-    if (M.max_bounces > 0 && ++L.bounces >= M.max_bounces) return EV_ESCAPE;
+    ++L.bounces;
+    if (M.max_bounces > 0 && L.bounces >= M.max_bounces) return EV_ESCAPE;
     float3 wo = phase_sample(M, L.rng, L.w);
     L.W = L.W * 1.0f;
     if (all_less(L.W, 0.00001f)) return EV_ESCAPE;
@@ -125,8 +163,12 @@ __device__ __forceinline__ int after_nee(const DMedium& M, NeeLane& L) {
     return L.d > 0.00001f ? EV_NONE : EV_ESCAPE;
 }
 
+// MODE: FW_PLAIN (the integrator), FW_CUT (unbiased prefix that stops into the
+// radiance cache), FW_TRAIN (full paths from random pixels that record
+// in-scattered radiance samples for the cache).
+template <int MODE>
 __global__ void __launch_bounds__(256, 3) k_nee_fw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, float* out,
-                                                 float scale, DScratch* sc) {
+                                                 float scale, DScratch* sc, CacheIO io) {
     const unsigned lane = threadIdx.x & 31u;
     const float EPS = 0.00001f;
     NeeLane L;
@@ -151,7 +193,20 @@ __global__ void __launch_bounds__(256, 3) k_nee_fw(DMedium M, PathSrc S, uint64_
                     // path_integrator_NEE prologue (vr_path_integrator_NEE.h:3-14)
                     L.rng.init(seed, pid, 0);
                     float3 x0, w0;
-                    primary_ray(S, pid, L.rng, x0, w0, L.oidx);
+                    if (MODE == FW_TRAIN && S.is_camera) {  // a random pixel: the path's first draw
+                        const uint64_t px = ((uint64_t)L.rng.u32() * (uint64_t)S.npix) >> 32;
+                        primary_ray(S, px, L.rng, x0, w0, L.oidx);
+                    } else {
+                        primary_ray(S, pid, L.rng, x0, w0, L.oidx);
+                    }
+                    L.pid = (long long)pid;
+                    L.nrec = 0;
+                    if (MODE == FW_CUT || (MODE == FW_TRAIN && io.cut >= 0)) {  // no query unless the path reaches the cut
+                        float* q = io.q + 3 * L.pid;
+                        st3(q, f3(0.0f));
+                        st3(q + 3 * io.rows, make_float3(0.0f, 0.0f, 1.0f));
+                        st3(q + 6 * io.rows, f3(0.0f));
+                    }
                     float tMin, tMax;
                     boundary(M, x0, w0, tMin, tMax);
                     L.x = x0 + w0 * tMin;
@@ -168,17 +223,7 @@ __global__ void __launch_bounds__(256, 3) k_nee_fw(DMedium M, PathSrc S, uint64_
                     if (ev == EV_SHADOW_DONE) {
                         L.R = L.R + L.T * M.env;
                         L.state = L.d > EPS ? ST_PRIMARY : ST_DEAD;
-                        if (L.state == ST_DEAD) {
-                            if (S.is_camera) {
-                                atomicAdd(out + 3 * L.oidx + 0, L.R.x * scale);
-                                atomicAdd(out + 3 * L.oidx + 1, L.R.y * scale);
-                                atomicAdd(out + 3 * L.oidx + 2, L.R.z * scale);
-                            } else {
-                                out[3 * L.oidx + 0] = L.R.x;
-                                out[3 * L.oidx + 1] = L.R.y;
-                                out[3 * L.oidx + 2] = L.R.z;
-                            }
-                        }
+                        if (L.state == ST_DEAD) end_path<MODE>(S, L, out, scale, io);
                     }
                 }
             }
@@ -277,6 +322,24 @@ __global__ void __launch_bounds__(256, 3) k_nee_fw(DMedium M, PathSrc S, uint64_
         while (ev != EV_NONE) {
             if (ev == EV_COLLISION) {  // vr_path_integrator_NEE.h:41-50
                 ++n_verts;
+                if ((MODE == FW_CUT || (MODE == FW_TRAIN && io.cut >= 0)) && L.bounces == io.cut) {
+                    // the rest of the path comes from the cache
+                    float* q = io.q + 3 * L.pid;
+                    st3(q, L.x);
+                    st3(q + 3 * io.rows, L.w);
+                    st3(q + 6 * io.rows, L.W);
+                    ev = EV_ESCAPE;
+                    continue;
+                }
+                if (MODE == FW_TRAIN && L.bounces < io.rec) {  // R and W at arrival; targets at the end
+                    const long long n = io.rows * io.rec;
+                    float* o = io.smp + 3 * (L.pid * io.rec + L.bounces);
+                    st3(o, L.x);
+                    st3(o + 3 * n, L.w);
+                    st3(o + 6 * n, L.R);
+                    st3(o + 9 * n, L.W);
+                    L.nrec = L.bounces + 1;
+                }
                 float3 sa = albedo(M, L.x, tl);
                 L.R = L.R + L.W * (f3(1.0f) - sa) * M.emission;
                 L.W = L.W * sa;
@@ -310,15 +373,7 @@ __global__ void __launch_bounds__(256, 3) k_nee_fw(DMedium M, PathSrc S, uint64_
                     ev = after_nee(M, L);
                 }
             } else {  // EV_ESCAPE: the path's estimate is complete
-                if (S.is_camera) {
-                    atomicAdd(out + 3 * L.oidx + 0, L.R.x * scale);
-                    atomicAdd(out + 3 * L.oidx + 1, L.R.y * scale);
-                    atomicAdd(out + 3 * L.oidx + 2, L.R.z * scale);
-                } else {
-                    out[3 * L.oidx + 0] = L.R.x;
-                    out[3 * L.oidx + 1] = L.R.y;
-                    out[3 * L.oidx + 2] = L.R.z;
-                }
+                end_path<MODE>(S, L, out, scale, io);
                 L.state = ST_DEAD;
                 ev = EV_NONE;
             }
@@ -838,15 +893,50 @@ int launch_radiance_fw(const DMedium& M, int integrator, const PathSrc& src, uin
     if (integrator == 0) {
         cudaError_t e = cudaMemsetAsync(&scratch->next_path, 0, sizeof(unsigned long long), stream);
         if (e != cudaSuccess) return launch_status(e);
-        int blocks = persistent_blocks((const void*)k_nee_fw, 256, num_sms);
+        int blocks = persistent_blocks((const void*)k_nee_fw<FW_PLAIN>, 256, num_sms);
         uint64_t need = (n_paths + 255) / 256;
         if ((uint64_t)blocks > need) blocks = (int)need;
-        k_nee_fw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, scratch);
+        CacheIO io = {};
+        k_nee_fw<FW_PLAIN><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, scratch, io);
     } else {
         uint64_t need = (n_paths + 255) / 256;
         int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
         k_dt_fw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, scratch);
     }
+    return launch_status(cudaGetLastError());
+}
+
+int launch_cache_paths(const DMedium& M, int mode, const PathSrc& src, uint64_t n_paths, uint64_t seed, float* out,
+                       float scale, const CacheIO& io, DScratch* scratch, int num_sms, cudaStream_t stream) {
+    if (n_paths == 0) return 0;
+    cudaError_t e = cudaMemsetAsync(&scratch->next_path, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return launch_status(e);
+    const void* kern = mode == FW_CUT ? (const void*)k_nee_fw<FW_CUT> : (const void*)k_nee_fw<FW_TRAIN>;
+    int blocks = persistent_blocks(kern, 256, num_sms);
+    uint64_t need = (n_paths + 255) / 256;
+    if ((uint64_t)blocks > need) blocks = (int)need;
+    if (mode == FW_CUT) k_nee_fw<FW_CUT><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, scratch, io);
+    else k_nee_fw<FW_TRAIN><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, scratch, io);
+    return launch_status(cudaGetLastError());
+}
+
+// targets of the recorded collisions: (R_final - R_k) / W_k, R_final per path
+__global__ void k_cache_targets(float* __restrict__ smp, const float* __restrict__ pR, long long n_paths, int rec) {
+    const long long n = n_paths * rec;
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
+        float* o = smp + 3 * r;
+        const float3 Wk = ld3(o + 9 * n);
+        if (Wk.x == 0.0f && Wk.y == 0.0f && Wk.z == 0.0f) continue;  // not reached: NaN target already
+        const float3 num = ld3(pR + 3 * (r / rec)) - ld3(o + 6 * n);
+        st3(o + 6 * n, make_float3(num.x / Wk.x, num.y / Wk.y, num.z / Wk.z));
+    }
+}
+
+int launch_cache_targets(float* smp, const float* pR, long long n_paths, int rec, cudaStream_t stream) {
+    const long long n = n_paths * rec;
+    if (n == 0) return 0;
+    long long b = (n + 255) / 256;
+    k_cache_targets<<<(int)(b < 4096 ? b : 4096), 256, 0, stream>>>(smp, pR, n_paths, rec);
     return launch_status(cudaGetLastError());
 }
 

@@ -53,12 +53,16 @@ def _interp_matrix(res: int, freq: int) -> np.ndarray:
     return m
 
 
-def value_noise(res: int, octaves: int, max_sigma: float, seed: int, base_freq: int = 4) -> np.ndarray:
+def value_noise(res: int, octaves: int, max_sigma: float, seed: int, base_freq: int = 4, device=None):
     """Multi-octave value noise: octave o is the trilinear interpolation of a
     (f+1)^3 lattice of U[0,1) values with f = base_freq * 2^o, weighted 0.5^o.
     The sum is centred on its expected value, clamped at 0 and scaled to
-    ``max_sigma``, which leaves roughly half of the box empty.
+    ``max_sigma``, which leaves roughly half of the box empty.  With a torch
+    ``device`` the same lattices are interpolated there (float64) and a
+    [res,res,res,1] float32 tensor is returned.
     """
+    if device is not None:
+        return _value_noise_torch(res, octaves, max_sigma, seed, base_freq, device)
     g = _rng(seed)
     vol = np.zeros((res, res, res), np.float64)
     amp_total = 0.0
@@ -77,6 +81,27 @@ def value_noise(res: int, octaves: int, max_sigma: float, seed: int, base_freq: 
     np.maximum(vol, 0.0, out=vol)
     vol *= max_sigma / vol.max()
     return np.ascontiguousarray(vol.astype(np.float32)[..., None])
+
+
+def _value_noise_torch(res, octaves, max_sigma, seed, base_freq, device):
+    import torch
+    g = _rng(seed)
+    vol = torch.zeros(res, res, res, dtype=torch.float64, device=device)
+    amp_total = 0.0
+    for o in range(octaves):
+        f = base_freq * (2 ** o)
+        amp = 0.5 ** o
+        lat = torch.from_numpy(g.uniform(0.0, 1.0, size=(f + 1, f + 1, f + 1))).to(device)
+        m = torch.from_numpy(_interp_matrix(res, f)).to(device)
+        t = torch.einsum("abc,xc->abx", lat, m)
+        t = torch.einsum("abx,yb->ayx", t, m)
+        vol += amp * torch.einsum("ayx,za->zyx", t, m)
+        amp_total += amp
+        del t
+    vol -= 0.5 * amp_total
+    vol.clamp_(min=0.0)
+    vol *= max_sigma / vol.max()
+    return vol.to(torch.float32).unsqueeze(-1).contiguous()
 
 
 def uniform_grid(res: int, lo: float, hi: float, seed: int, channels: int = 1) -> np.ndarray:
