@@ -194,7 +194,7 @@ def cpu_sample(seconds_hint: float = 10.0, threads: int | None = None):
 def run_ours(args):
     import torch
     import torch.distributed as dist
-    from rendervous_b200 import build as vbuild, maps
+    from rendervous_b200 import _lib, build as vbuild, maps
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -242,6 +242,8 @@ def run_ours(args):
         dist.barrier()
     torch.cuda.synchronize(dev)
     times = []
+    _, vlib = _lib.ffi_lib()
+    launches0 = int(vlib.vrt_launch_count())
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             flush.zero_()
@@ -253,6 +255,7 @@ def run_ours(args):
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
     torch.cuda.synchronize(dev)
+    launches = int(vlib.vrt_launch_count()) - launches0
     if world > 1:
         dist.barrier()
     counters = maps.check()
@@ -304,7 +307,7 @@ def run_ours(args):
         bytes_alg = 32.0 * c["lookups"] + 32.0 * c["albedo_lookups"] + 4.0 * c["reds"] + 12.0 * c["paths"]
         roof[name] = dict(ms=ms, bytes=bytes_alg, counters=c)
     dom = max(roof, key=lambda k: roof[k]["ms"])
-    kern = {"fw": "k_nee_fw", "bw": "k_path_bw"}[dom]
+    kern = {"fw": "k_walk_fw+k_shadow_fw", "bw": "k_nee_ds_bw"}[dom]
     peaks = measured_peaks()
     achieved = roof[dom]["bytes"] / (roof[dom]["ms"] / 1e3) / 1e9
     traffic = profiled_traffic(kern)
@@ -365,7 +368,7 @@ def run_ours(args):
                        "transmittance": "ratio tracking", "majorant": "8^3-brick grid", "adjoint": "NEE_DS",
                        "l2": "flushed between steps (512 MB write)", "parallelism": f"dp{world}"},
             "e2e": e2e,
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": launches,
             "counters_per_step": {k: v / args.steps for k, v in c.items() if k != "status"},
             "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peaks["hbm_gbs"],
                          "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,

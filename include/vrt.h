@@ -116,6 +116,8 @@ int vrt_context_destroy(vrt_context* ctx);
    Returns VRT_OK or the first device-side error. */
 int vrt_context_sync(vrt_context* ctx, void* stream, vrt_counters* out);
 const char* vrt_status_string(int32_t status);
+/* Number of kernels this library has launched in the process (for launch accounting). */
+int64_t vrt_launch_count(void);
 int32_t vrt_version(void);
 
 /* RayBoxIntersection forward (rendervous _maps.py:4128-4154, include/maths.h:28-38):

@@ -12,7 +12,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvrt.so")
-SOURCES = ["vrt_api.cu", "vrt_transmittance.cu", "vrt_path.cu", "vrt_adjoint.cu", "vrt_cache.cu", "vrt_noalloc.cu"]
+SOURCES = ["vrt_api.cu", "vrt_transmittance.cu", "vrt_path.cu", "vrt_adjoint.cu", "vrt_wave.cu", "vrt_cache.cu",
+           "vrt_noalloc.cu"]
 HEADERS = ["vrt_device.cuh", "vrt_tracking.cuh", "vrt_params.h", "vrt_internal.h"]
 
 NVCC_FLAGS = [

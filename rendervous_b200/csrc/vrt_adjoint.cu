@@ -475,6 +475,7 @@ int launch_nee_ds_bw(const DMedium& M, const PathSrc& src, uint64_t n_paths, uin
     uint64_t need = (n_paths + 255) / 256;
     if ((uint64_t)blocks > need) blocks = (int)need;
     k_nee_ds_bw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 

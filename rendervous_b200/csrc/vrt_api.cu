@@ -4,6 +4,7 @@
 // strides, modes, alignment) before any launch, converts the C structs into the
 // kernel-parameter forms of vrt_params.h and launches on the caller's stream.
 // There is no CPU fallback: every computation is a CUDA kernel.
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -20,6 +21,31 @@ int launch_status(cudaError_t e) {
     if (e == cudaSuccess) return VRT_OK;
     std::fprintf(stderr, "[vrt] CUDA error: %s\n", cudaGetErrorString(e));
     return VRT_E_CUDA;
+}
+
+static std::atomic<long long> g_launches{0};
+void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// The wavefront serves the NEE forward of capped paths (its job buffer is sized
+// from the bounce cap); uncapped paths run the persistent state machine.
+static bool use_wave(const DMedium& M, int integrator) {
+    return integrator == VRT_PI_NEE && M.max_bounces > 0 && M.max_bounces <= 4096;
+}
+
+int ensure_wave_buffer(vrt_context* ctx, size_t bytes) {
+    if (ctx->wave && ctx->wave_bytes >= bytes) return VRT_OK;
+    if (ctx->wave) {
+        cudaFree(ctx->wave);
+        ctx->wave = nullptr;
+        ctx->wave_bytes = 0;
+    }
+    if (cudaMalloc(&ctx->wave, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->wave = nullptr;
+        return VRT_E_CUDA;
+    }
+    ctx->wave_bytes = bytes;
+    return VRT_OK;
 }
 
 int persistent_blocks(const void* kernel, int block, int num_sms) {
@@ -204,6 +230,8 @@ extern "C" {
 
 int32_t vrt_version(void) { return 1; }
 
+int64_t vrt_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
 const char* vrt_status_string(int32_t s) {
     switch (s) {
         case VRT_OK: return "ok";
@@ -230,6 +258,8 @@ int vrt_context_create(int32_t device, vrt_context** out) {
     ctx->device = device;
     ctx->num_sms = prop.multiProcessorCount;
     ctx->scratch = nullptr;
+    ctx->wave = nullptr;
+    ctx->wave_bytes = 0;
     if (cudaMalloc(&ctx->scratch, sizeof(DScratch)) != cudaSuccess) { delete ctx; return VRT_E_CUDA; }
     if (cudaMemset(ctx->scratch, 0, sizeof(DScratch)) != cudaSuccess) { cudaFree(ctx->scratch); delete ctx; return VRT_E_CUDA; }
     *out = ctx;
@@ -239,6 +269,7 @@ int vrt_context_create(int32_t device, vrt_context** out) {
 int vrt_context_destroy(vrt_context* ctx) {
     if (!ctx) return VRT_E_NULL_POINTER;
     cudaError_t e = cudaFree(ctx->scratch);
+    if (ctx->wave) cudaFree(ctx->wave);
     delete ctx;
     return e == cudaSuccess ? VRT_OK : VRT_E_CUDA;
 }
@@ -271,6 +302,7 @@ int vrt_ray_box(const float* rays, int64_t n, const float bmin[3], const float b
     if (n == 0) return VRT_OK;
     if (!rays || !bmin || !bmax || !out) return VRT_E_NULL_POINTER;
     k_ray_box<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(rays, n, mk3(bmin), mk3(bmax), out);
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 
@@ -284,6 +316,7 @@ int vrt_grid3d_fw(const vrt_grid* g, const float bmin[3], const float inv_bsize[
     int st = to_dgrid(*g, 0, G);
     if (st) return st;
     k_grid_fw<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(G, mk3(bmin), mk3(inv_bsize), x, n, out);
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 
@@ -297,6 +330,7 @@ int vrt_grid3d_bw(const vrt_grid* g, const float bmin[3], const float inv_bsize[
     int st = to_dgrid(*g, 0, G);
     if (st) return st;
     k_grid_bw<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(G, mk3(bmin), mk3(inv_bsize), x, dout, n);
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 
@@ -311,6 +345,7 @@ int vrt_majorant_build(const vrt_grid* sigma, int32_t brick, float* out, int32_t
     if (!out) return VRT_OK;
     int64_t total = (int64_t)M[0] * M[1] * M[2];
     k_majorant_build<<<blocks_for(total * 32), 256, 0, (cudaStream_t)stream>>>(G, brick, M[0], M[1], M[2], out);
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 
@@ -356,6 +391,11 @@ int vrt_radiance_fw(vrt_context* ctx, const vrt_medium* m, int32_t integrator, c
     std::memset(&S, 0, sizeof(S));
     S.is_camera = 0;
     S.rays = rays;
+    if (use_wave(M, integrator)) {  // the wavefront accumulates: clear R first
+        cudaError_t e = cudaMemsetAsync(R, 0, sizeof(float) * 3 * (size_t)n, (cudaStream_t)stream);
+        if (e != cudaSuccess) return launch_status(e);
+        return launch_wave_fw(ctx, M, S, (uint64_t)n, seed, R, 1.0f, (cudaStream_t)stream);
+    }
     return launch_radiance_fw(M, integrator, S, (uint64_t)n, seed, R, 1.0f, ctx->scratch, ctx->num_sms,
                               (cudaStream_t)stream);
 }
@@ -394,6 +434,9 @@ int vrt_capture_fw(vrt_context* ctx, const vrt_medium* m, int32_t integrator, co
     S.npix = (long long)S.cam.views * S.cam.height * S.cam.width;
     cudaError_t e = cudaMemsetAsync(rgb, 0, sizeof(float) * 3 * S.npix, (cudaStream_t)stream);
     if (e != cudaSuccess) return launch_status(e);
+    if (use_wave(M, integrator))
+        return launch_wave_fw(ctx, M, S, (uint64_t)S.npix * (uint64_t)spp, seed, rgb, 1.0f / (float)spp,
+                              (cudaStream_t)stream);
     return launch_radiance_fw(M, integrator, S, (uint64_t)S.npix * (uint64_t)spp, seed, rgb, 1.0f / (float)spp,
                               ctx->scratch, ctx->num_sms, (cudaStream_t)stream);
 }

@@ -599,6 +599,7 @@ extern "C" int vrt_cache_mlp_fw(const float* weights, const float* inputs, int64
     if (blocks <= 0) return VRT_E_CUDA;
     k_mlp_infer<IN_GIVEN><<<blocks, kTile, smem, (cudaStream_t)stream>>>(E, weights, inputs, nullptr, nullptr, nullptr,
                                                                          n, out, kOut, 0, 0.0f);
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 
@@ -615,6 +616,7 @@ extern "C" int vrt_cache_infer(const vrt_cache* c, const float* pos, const float
     if (blocks <= 0) return VRT_E_CUDA;
     k_mlp_infer<IN_ENCODE><<<blocks, kTile, smem, (cudaStream_t)stream>>>(E, c->weights, nullptr, pos, dir, nullptr, n,
                                                                           rgb, 3, 0, 0.0f);
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 
@@ -631,6 +633,7 @@ extern "C" int vrt_cache_resolve(const vrt_cache* c, const float* queries, int64
     if (blocks <= 0) return VRT_E_CUDA;
     k_mlp_infer<IN_RESOLVE><<<blocks, kTile, smem, (cudaStream_t)stream>>>(
         E, c->weights, nullptr, queries, queries + 3 * n, queries + 6 * n, n, rgb, 3, npix, scale);
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 
@@ -647,6 +650,7 @@ extern "C" int vrt_cache_train(const vrt_cache* c, const float* pos, const float
     if (blocks <= 0) return VRT_E_CUDA;
     k_mlp_train<<<blocks, kTile, smem, (cudaStream_t)stream>>>(E, c->weights, c->weights_grad, pos, dir, target, n,
                                                                1.0f / (float)n, loss);
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 
@@ -659,6 +663,7 @@ extern "C" int vrt_cache_adam(float* params, float* grads, float* m, float* v, i
     int64_t b = (n + 255) / 256;
     int blocks = (int)(b < 4096 ? b : 4096);
     k_adam<<<blocks, 256, 0, (cudaStream_t)stream>>>(params, grads, m, v, n, lr, beta1, beta2, eps, c1, c2);
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 

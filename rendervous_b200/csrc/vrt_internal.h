@@ -9,12 +9,24 @@ struct vrt_context {
     int device;
     int num_sms;
     vrt::DScratch* scratch;  // device memory
+    void* wave;              // wavefront job buffer (grown on demand)
+    size_t wave_bytes;
 };
 
 namespace vrt {
 
 // Returns VRT_OK or VRT_E_CUDA after checking the launch.
 int launch_status(cudaError_t e);
+
+// Grows the context's wavefront buffer to at least `bytes` (contents undefined).
+int ensure_wave_buffer(vrt_context* ctx, size_t bytes);
+
+// Host-side count of the kernels this library launched (vrt_launch_count).
+void count_launches(int n);
+
+// Wavefront NEE forward (vrt_wave.cu), capped paths only.
+int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed, float* out,
+                   float scale, cudaStream_t stream);
 
 int persistent_blocks(const void* kernel, int block, int num_sms);
 

@@ -903,6 +903,7 @@ int launch_radiance_fw(const DMedium& M, int integrator, const PathSrc& src, uin
         int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
         k_dt_fw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, scratch);
     }
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 
@@ -917,6 +918,7 @@ int launch_cache_paths(const DMedium& M, int mode, const PathSrc& src, uint64_t 
     if ((uint64_t)blocks > need) blocks = (int)need;
     if (mode == FW_CUT) k_nee_fw<FW_CUT><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, scratch, io);
     else k_nee_fw<FW_TRAIN><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, scratch, io);
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 
@@ -937,6 +939,7 @@ int launch_cache_targets(float* smp, const float* pR, long long n_paths, int rec
     if (n == 0) return 0;
     long long b = (n + 255) / 256;
     k_cache_targets<<<(int)(b < 4096 ? b : 4096), 256, 0, stream>>>(smp, pR, n_paths, rec);
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 
@@ -949,6 +952,7 @@ int launch_radiance_bw(const DMedium& M, int bw_mode, const PathSrc& src, uint64
     if (bw_mode == 0) k_path_bw<0><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
     else if (bw_mode == 1) k_path_bw<1><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
     else k_path_bw<2><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 

@@ -92,6 +92,7 @@ int launch_transmittance_fw(const DMedium& M, int mode, const float* rays, int64
         case 2: k_transmittance_fw<2><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
         default: k_transmittance_fw<3><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
     }
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 
@@ -105,6 +106,7 @@ int launch_transmittance_bw(const DMedium& M, int mode, const float* rays, int64
         case 2: k_transmittance_bw<2><<<g, 256, 0, stream>>>(M, rays, n, seed, dL_dT, scratch); break;
         default: k_transmittance_bw<3><<<g, 256, 0, stream>>>(M, rays, n, seed, dL_dT, scratch); break;
     }
+    count_launches(1);
     return launch_status(cudaGetLastError());
 }
 
