@@ -104,6 +104,7 @@ typedef struct vrt_counters {
     int64_t reds;                    /* gradient atomic adds issued */
     int64_t albedo_lookups;          /* albedo grid lookups */
     int64_t status;                  /* device error bits (VRT_E_* as 1 << code) */
+    int64_t detail;                  /* which device guard raised it (bit per site; diagnostics) */
 } vrt_counters;
 
 typedef struct vrt_context vrt_context;

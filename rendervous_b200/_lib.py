@@ -91,7 +91,8 @@ class Context:
         with torch.cuda.device(self.device):
             st = lib.vrt_context_sync(self.ptr, stream_handle(torch.device("cuda", self.device)), c)
         counters = dict(paths=int(c.paths), vertices=int(c.vertices), steps=int(c.steps), lookups=int(c.lookups),
-                        reds=int(c.reds), albedo_lookups=int(c.albedo_lookups), status=int(c.status))
+                        reds=int(c.reds), albedo_lookups=int(c.albedo_lookups), status=int(c.status),
+                        detail=int(c.detail))
         check(st, "device-side error recorded by a kernel")
         return counters
 

@@ -45,6 +45,7 @@ def _digest() -> str:
         with open(p, "rb") as f:
             h.update(f.read())
     h.update(" ".join(NVCC_FLAGS).encode())
+    h.update(repr(sorted(PER_FILE_FLAGS.items())).encode())
     return h.hexdigest()
 
 
@@ -57,21 +58,43 @@ def up_to_date() -> bool:
         return f.read().strip() == _digest()
 
 
+# Files whose kernels must round every operation on its own: the wavefront
+# primal and replay walks are separate kernels that have to retrace the same
+# path bit for bit, so no a*b+c may be contracted differently in the two.
+PER_FILE_FLAGS = {"vrt_wave.cu": ["-fmad=false"]}
+OBJ_DIR = os.path.join(HERE, "_build")
+
+
 def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
-    """Compile every .cu of csrc/ into one shared library with nvcc."""
+    """Compile every .cu of csrc/ (in parallel, one object each) and link them
+    into one shared library with nvcc."""
     if not force and up_to_date():
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, *(extra_flags or []), "-shared", "-o", LIB] + [os.path.join(CSRC, s) for s in SOURCES]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    procs = []
+    for src in SOURCES:
+        obj = os.path.join(OBJ_DIR, src[:-3] + ".o")
+        cmd = [nvcc(), *NVCC_FLAGS, *PER_FILE_FLAGS.get(src, []), *(extra_flags or []), "-c",
+               os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((src, obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    errors = []
+    for src, obj, proc in procs:
+        out, err = proc.communicate()
+        if proc.returncode != 0:
+            errors.append(f"{src}:\n{out}{err}")
+        elif verbose and err:
+            print(err, file=sys.stderr)
+    if errors:
+        raise RuntimeError("libvrt build failed:\n" + "\n".join(errors))
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB] + [o for _, o, _ in procs]
     out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
-        raise RuntimeError("libvrt build failed:\n" + out.stdout + out.stderr)
+        raise RuntimeError("libvrt link failed:\n" + out.stdout + out.stderr)
     if not extra_flags:
         with open(STAMP, "w") as f:
             f.write(_digest())
-    if verbose and out.stderr:
-        print(out.stderr, file=sys.stderr)
     return LIB
 
 

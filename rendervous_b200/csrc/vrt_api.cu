@@ -31,6 +31,11 @@ void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed);
 static bool use_wave(const DMedium& M, int integrator) {
     return integrator == VRT_PI_NEE && M.max_bounces > 0 && M.max_bounces <= 4096;
 }
+// The NEE_DS adjoint wavefront reuses the primal's shadow transmittances in the
+// replay, which retraces the primal only with the default replay majorant.
+static bool use_wave_bw(const DMedium& M, int bw_mode) {
+    return bw_mode == VRT_BW_NEE_DS && M.max_bounces > 0 && M.max_bounces <= 4096 && !M.ds_compat;
+}
 
 int ensure_wave_buffer(vrt_context* ctx, size_t bytes) {
     if (ctx->wave && ctx->wave_bytes >= bytes) return VRT_OK;
@@ -291,6 +296,7 @@ int vrt_context_sync(vrt_context* ctx, void* stream, vrt_counters* out) {
         out->reds = (int64_t)h.reds;
         out->albedo_lookups = (int64_t)h.albedo;
         out->status = (int64_t)h.status;
+        out->detail = (int64_t)h.detail;
     }
     for (int code = 1; code < 8; ++code)
         if (h.status & (1u << code)) return code;
@@ -414,6 +420,7 @@ int vrt_radiance_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, cons
     std::memset(&S, 0, sizeof(S));
     S.is_camera = 0;
     S.rays = rays;
+    if (use_wave_bw(M, bw_mode)) return launch_wave_ds_bw(ctx, M, S, (uint64_t)n, seed, dL_dR, 1.0f, (cudaStream_t)stream);
     return launch_radiance_bw(M, bw_mode, S, (uint64_t)n, seed, dL_dR, 1.0f, ctx->scratch, ctx->num_sms,
                               (cudaStream_t)stream);
 }
@@ -455,6 +462,9 @@ int vrt_capture_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const
     if (!dL_drgb) return VRT_E_NULL_POINTER;
     S.is_camera = 1;
     S.npix = (long long)S.cam.views * S.cam.height * S.cam.width;
+    if (use_wave_bw(M, bw_mode))
+        return launch_wave_ds_bw(ctx, M, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
+                                 (cudaStream_t)stream);
     return launch_radiance_bw(M, bw_mode, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
                               ctx->scratch, ctx->num_sms, (cudaStream_t)stream);
 }

@@ -24,6 +24,10 @@ int ensure_wave_buffer(vrt_context* ctx, size_t bytes);
 // Host-side count of the kernels this library launched (vrt_launch_count).
 void count_launches(int n);
 
+// Wavefront NEE_DS adjoint (vrt_wave.cu): capped paths, default replay majorant.
+int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed,
+                      const float* dL, float div, cudaStream_t stream);
+
 // Wavefront NEE forward (vrt_wave.cu), capped paths only.
 int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed, float* out,
                    float scale, cudaStream_t stream);

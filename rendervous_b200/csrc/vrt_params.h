@@ -55,7 +55,7 @@ struct DScratch {
     unsigned long long reds;
     unsigned long long albedo;
     unsigned int status;           // 1 << VRT_E_* bits
-    unsigned int pad;
+    unsigned int detail;           // which guard raised a device error (bit per site)
 };
 
 }  // namespace vrt

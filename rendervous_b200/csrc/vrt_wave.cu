@@ -45,11 +45,30 @@ struct ShadowJob {
 };
 
 __device__ __forceinline__ void put_job(ShadowJob* J, unsigned long long slot, float3 x, float3 d, float3 wt,
-                                        unsigned long long key) {
+                                        unsigned long long key, uint32_t tgt = 0u) {
     float4* p = reinterpret_cast<float4*>(J + slot);
     p[0] = make_float4(x.x, x.y, x.z, d.x);
     p[1] = make_float4(d.y, d.z, wt.x, wt.y);
-    p[2] = make_float4(wt.z, 0.0f, __uint_as_float((uint32_t)key), __uint_as_float((uint32_t)(key >> 32)));
+    p[2] = make_float4(wt.z, __uint_as_float(tgt), __uint_as_float((uint32_t)key), __uint_as_float((uint32_t)(key >> 32)));
+}
+
+struct JobView {
+    float3 x, dir, wt;
+    uint64_t pid;
+    uint32_t fork, tgt;
+};
+__device__ __forceinline__ JobView get_job(const ShadowJob* J, unsigned long long i) {
+    const float4* p = reinterpret_cast<const float4*>(J + i);
+    const float4 a = __ldcs(p), b = __ldcs(p + 1), c = __ldcs(p + 2);
+    JobView v;
+    v.x = make_float3(a.x, a.y, a.z);
+    v.dir = make_float3(a.w, b.x, b.y);
+    v.wt = make_float3(b.z, b.w, c.x);
+    v.tgt = __float_as_uint(c.y);
+    const unsigned long long key = (unsigned long long)__float_as_uint(c.z) | ((unsigned long long)__float_as_uint(c.w) << 32);
+    v.pid = key >> 16;
+    v.fork = (uint32_t)(key & 0xffffu);
+    return v;
 }
 
 __device__ __forceinline__ unsigned long long job_key(uint64_t pid, uint32_t fork) {
@@ -75,8 +94,10 @@ __device__ __forceinline__ unsigned long long reserve_slots(unsigned long long* 
     return base + (unsigned long long)(incl - n);
 }
 
+// Per-warp sums of the lanes' tallies into the context counters.  `verts`
+// counts forward path vertices only (the metric's unit); adjoint kernels pass 0.
 __device__ __forceinline__ void flush_counters(DScratch* sc, uint32_t paths, uint32_t verts, const Tally& tl) {
-    unsigned long long p = paths, v = verts, s = tl.steps, l = tl.lookups, a = tl.albedo;
+    unsigned long long p = paths, v = verts, s = tl.steps, l = tl.lookups, a = tl.albedo, r = tl.reds;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         p += __shfl_down_sync(kAll, p, o);
@@ -84,6 +105,7 @@ __device__ __forceinline__ void flush_counters(DScratch* sc, uint32_t paths, uin
         s += __shfl_down_sync(kAll, s, o);
         l += __shfl_down_sync(kAll, l, o);
         a += __shfl_down_sync(kAll, a, o);
+        r += __shfl_down_sync(kAll, r, o);
     }
     if ((threadIdx.x & 31u) == 0) {
         if (p) atomicAdd(&sc->paths, p);
@@ -91,11 +113,40 @@ __device__ __forceinline__ void flush_counters(DScratch* sc, uint32_t paths, uin
         if (s) atomicAdd(&sc->steps, s);
         if (l) atomicAdd(&sc->lookups, l);
         if (a) atomicAdd(&sc->albedo, a);
+        if (r) atomicAdd(&sc->reds, r);
     }
+}
+
+// a device guard fired: the error code plus the site (VRT_E_ITER_CAP in both)
+__device__ __forceinline__ void guard(DScratch* sc, int site) {
+    atomicOr(&sc->status, 1u << 4);
+    atomicOr(&sc->detail, 1u << site);
 }
 
 __device__ __forceinline__ long long out_index(const PathSrc& S, uint64_t pid) {
     return S.is_camera ? (long long)(pid % (uint64_t)S.npix) : (long long)pid;
+}
+
+template <int TR>
+__device__ __forceinline__ float shadow_T(const DMedium& M, Rng& r, float3 x, float3 dir, Tally& tl, uint32_t* status) {
+    if (TR == 0) return transmittance_rt(M, r, x, dir, tl, status);
+    if (TR == 1) return transmittance_dt(M, r, x, dir, tl, status);
+    if (TR == 2) return transmittance_dda<false>(M, x, dir, tl);
+    return transmittance_dda<true>(M, x, dir, tl);
+}
+
+// The primary ray of path pid (camera or ray input), with the camera's draws.
+__device__ __forceinline__ void start_ray(const PathSrc& S, uint64_t pid, Rng& rng, float3& x0, float3& w0) {
+    if (S.is_camera) {
+        const long long px = (long long)(pid % (uint64_t)S.npix);
+        const long long hw = (long long)S.cam.height * S.cam.width;
+        const int view = (int)(px / hw);
+        const int rem = (int)(px - (long long)view * hw);
+        camera_ray(S.cam, view, rem / S.cam.width, rem % S.cam.width, rng, x0, w0);
+    } else {
+        x0 = ld3(S.rays + 6 * pid);
+        w0 = ld3(S.rays + 6 * pid + 3);
+    }
 }
 
 }  // namespace
@@ -195,7 +246,7 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
             ff.sample(rng);
             for (int k = 0;; ++k) {
                 if (k >= kStepCap) {
-                    raise_status(&sc->status, 4);
+                    guard(sc, 0);
                     ev = 2;
                     break;
                 }
@@ -226,7 +277,7 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                 }
             }
             if (++steps_path > (uint32_t)kPathCap) {
-                raise_status(&sc->status, 4);
+                guard(sc, 1);
                 ev = 2;
             }
             if (ev == 1) {  // real collision (vr_path_integrator_NEE.h:41-62)
@@ -288,23 +339,13 @@ __global__ void __launch_bounds__(256, 4) k_shadow_fw(DMedium M, PathSrc S, cons
     Tally tl;
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
          i += (unsigned long long)gridDim.x * blockDim.x) {
-        const float4* p = reinterpret_cast<const float4*>(jobs + i);
-        const float4 a = __ldcs(p), b = __ldcs(p + 1), c = __ldcs(p + 2);
-        const float3 x = make_float3(a.x, a.y, a.z), dir = make_float3(a.w, b.x, b.y);
-        const float3 wt = make_float3(b.z, b.w, c.x);
-        const unsigned long long key = (unsigned long long)__float_as_uint(c.z) |
-                                       ((unsigned long long)__float_as_uint(c.w) << 32);
-        const uint64_t pid = key >> 16;
+        const JobView jv = get_job(jobs, i);
         Rng r;
-        r.init(seed, pid, 2u * (1u + (uint32_t)(key & 0xffffu)));  // fork j of the path's stream 0
-        float T;
-        if (TR == 0) T = transmittance_rt(M, r, x, dir, tl, &sc->status);
-        else if (TR == 1) T = transmittance_dt(M, r, x, dir, tl, &sc->status);
-        else if (TR == 2) T = transmittance_dda<false>(M, x, dir, tl);
-        else T = transmittance_dda<true>(M, x, dir, tl);
-        const float3 c3 = wt * T;
+        r.init(seed, jv.pid, 2u * (1u + jv.fork));  // fork j of the path's stream 0
+        const float T = shadow_T<TR>(M, r, jv.x, jv.dir, tl, &sc->status);
+        const float3 c3 = jv.wt * T;
         if (c3.x != 0.0f || c3.y != 0.0f || c3.z != 0.0f) {
-            const long long o = out_index(S, pid);
+            const long long o = out_index(S, jv.pid);
             atomicAdd(out + 3 * o + 0, c3.x * scale);
             atomicAdd(out + 3 * o + 1, c3.y * scale);
             atomicAdd(out + 3 * o + 2, c3.z * scale);
@@ -357,6 +398,514 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
             return launch_status(e);
         if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return launch_status(e);
         if (taken >= n_paths) break;
+        if (round > (1 << 20)) return VRT_E_ITER_CAP;
+    }
+    return 0;
+}
+
+// ------------------------------------------------------------------------
+// NEE_DS adjoint (include/vr_path_integrator_NEE_DS.h:6-206) as a wavefront.
+//
+// With the default replay majorant (the primal's) the replay retraces the
+// primal's vertices exactly -- same draws, same throughputs, and shadow j of
+// the path draws from fork j in both passes -- so a vertex's shadow
+// transmittances are computed once and stored, and the transmittance adjoints
+// (which feed nothing back into the path) run as independent jobs:
+//
+//   A k_ds_primal   the primal walk: per real collision a vertex record (linked
+//                   per path) and a T job per light; per path the emission and
+//                   escape terms of R and Rsp
+//   B k_shadow_T    T of each job into its record, weight * T into its path's
+//                   R (or Rsp after a zero-density collision)
+//   C k_ds_replay   the replay walk: dL/dsigma at every collision, dL/dalbedo
+//                   at real ones, the R bookkeeping from the stored T, and a
+//                   transmittance-adjoint job per light with dL/dT != 0
+//   D k_shadow_bw   the two-pass ratio / delta tracking adjoint or the DDA
+//                   adjoint of each job
+//
+// Rounds bound the buffers as in the forward wavefront.
+// ------------------------------------------------------------------------
+namespace {
+constexpr uint32_t kNone = 0xffffffffu;
+struct VertexRec {
+    float Te, Ts;
+    uint32_t next, pad;
+};
+}  // namespace
+
+struct WaveBw {
+    ShadowJob* jobs;
+    VertexRec* recs;
+    float* info;               // per path: R (3), Rsp (3), first record, pad
+    unsigned long long* hdr;   // [0] jobs, [1] records, [2] replay queue
+    unsigned long long cap_jobs, cap_recs, cap_paths;
+    unsigned long long res_jobs, res_recs, lanes;
+    uint64_t p_begin;
+};
+
+__global__ void __launch_bounds__(256, 4) k_ds_primal(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
+                                                    DScratch* sc, WaveBw wv) {
+    const unsigned lane = threadIdx.x & 31u;
+    const float EPS = 0.00000001f;
+    const float eps = M.ds_eps;
+    const int lights = M.has_sun ? 2 : 1;
+    Flight ff;
+    Rng rng;
+    float3 x = f3(0.0f), w = f3(0.0f), W = f3(0.0f), Racc = f3(0.0f), Rspacc = f3(0.0f);
+    float d = 0.0f, null_W = 1.0f;
+    bool scattered = false, alive = false, exhausted = false;
+    int bounces = 0;
+    uint64_t pid = 0;
+    uint32_t steps_path = 0, first = kNone, prev = kNone;
+    uint32_t n_paths_done = 0;
+    Tally tl;
+
+    while (true) {
+        unsigned want = __ballot_sync(kAll, !alive && !exhausted);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) {
+                const unsigned long long uj = *((volatile unsigned long long*)&wv.hdr[0]);
+                const unsigned long long ur = *((volatile unsigned long long*)&wv.hdr[1]);
+                const unsigned long long up = *((volatile unsigned long long*)&sc->next_path) - wv.p_begin;
+                const bool room = uj + wv.res_jobs <= wv.cap_jobs && ur + wv.res_recs <= wv.cap_recs &&
+                                  up + wv.lanes <= wv.cap_paths;
+                base = room ? atomicAdd(&sc->next_path, (unsigned long long)__popc(want)) : ~0ull;
+            }
+            base = __shfl_sync(kAll, base, leader);
+            if (base == ~0ull) {
+                exhausted = true;
+            } else if (!alive && !exhausted) {
+                const uint64_t p = base + __popc(want & ((1u << lane) - 1u));
+                if (p >= n_paths) {
+                    exhausted = true;
+                } else {
+                    pid = p;
+                    rng.init(seed, pid, 0);
+                    float3 x0, w0;
+                    start_ray(S, pid, rng, x0, w0);
+                    float tMin, tMax;
+                    boundary(M, x0, w0, tMin, tMax);
+                    x = x0 + w0 * tMin;
+                    w = w0;
+                    d = tMax - tMin;
+                    W = f3(1.0f);
+                    Racc = f3(0.0f);
+                    Rspacc = f3(0.0f);
+                    null_W = 1.0f;
+                    scattered = false;
+                    bounces = 0;
+                    steps_path = 0;
+                    first = kNone;
+                    prev = kNone;
+                    ff = Flight();
+                    alive = true;
+                    ++n_paths_done;
+                }
+            }
+        }
+        if (__all_sync(kAll, !alive && exhausted)) break;
+
+        int nrec = 0, nj = 0;
+        bool finish = false, rsp = false;
+        float3 wnee = f3(0.0f), we = f3(0.0f), ws = f3(0.0f);
+        uint32_t jfork = 0;
+        if (alive) {
+            int ev = 0;  // 0 none, 1 collision, 2 end
+            if (!(d > EPS)) {
+                ev = 2;  // the while (d > EPS) test (_NEE_DS.h:31)
+            } else {
+                bool need = false;
+                float m = 0.0f, t = 0.0f;
+                if (ff.tau < 0.0f) ++tl.steps;
+                ff.sample(rng);
+                for (int k = 0;; ++k) {
+                    if (k >= kStepCap) {
+                        guard(sc, 2);
+                        ev = 2;
+                        break;
+                    }
+                    float md;
+                    m = gmax(EPS, ff.bk.query(M, x, w, md) + 2.0f * eps + 0.1f);  // _NEE_DS.h:36
+                    t = ff.tau / m;
+                    x = x + w * gmin(t, md);
+                    if (t > md) {
+                        d -= md;
+                        ff.cross(m, md);
+                        ff.bk.advance(M);
+                        if (!(d > EPS)) { ev = 2; break; }
+                        continue;
+                    }
+                    ff.used();
+                    if (t > d) ev = 2;
+                    else need = true;
+                    ff.bk.move(t);
+                    break;
+                }
+                if (need) {
+                    const float s = sigma(M, x, tl);
+                    const float Pc = (s + eps) / m;
+                    if (rng.uniform() >= Pc) {  // null collision (_NEE_DS.h:41-45)
+                        W = W * ((1.0f - s / m) / (1.0f - Pc));
+                        d -= t;
+                    } else {  // real collision (_NEE_DS.h:48-99)
+                        scattered = true;
+                        bool dead = false;
+                        if (s < EPS) {
+                            if (null_W < EPS) { W = f3(0.0f); dead = true; }
+                            else null_W = 0.0f;
+                        } else {
+                            W = W * ((s / m) / Pc);
+                        }
+                        if (dead) {
+                            ev = 2;
+                        } else {
+                            const float3 sa = albedo(M, x, tl);
+                            const float3 acc = W * (f3(1.0f) - sa) * M.emission;
+                            W = W * sa;
+                            const float3 Le = environment_sample(M, rng, wnee);
+                            we = W * Le * phase(M, w, wnee);
+                            if (M.has_sun) ws = W * M.sun_L * phase(M, w, M.sun_dir);
+                            jfork = rng.ntr;
+                            rng.ntr += (uint32_t)lights;
+                            const bool capped = M.max_bounces > 0 && bounces + 1 >= M.max_bounces;
+                            float3 wo = w;
+                            if (!capped) wo = phase_sample(M, rng, w);
+                            rsp = null_W < EPS;
+                            if (rsp) Rspacc = Rspacc + acc;
+                            else Racc = Racc + acc;
+                            nrec = 1;
+                            nj = lights;
+                            ++bounces;
+                            if (capped || all_less(W, EPS)) {
+                                W = f3(0.0f);
+                                ev = 2;
+                            } else {
+                                w = wo;
+                                float tMin;
+                                boundary(M, x, w, tMin, d);
+                                ff = Flight();
+                            }
+                        }
+                    }
+                }
+            }
+            if (++steps_path > (uint32_t)kPathCap) {
+                guard(sc, 3);
+                ev = 2;
+            }
+            finish = ev == 2;
+        }
+        // ---- the vertex record (linked to the path's previous one) and its T jobs
+        const unsigned long long r = reserve_slots(&wv.hdr[1], nrec);
+        if (nrec) {
+            VertexRec* rp = wv.recs + r;
+            rp->Te = 1.0f;
+            rp->Ts = 1.0f;
+            rp->next = kNone;
+            if (first == kNone) first = (uint32_t)r;
+            else wv.recs[prev].next = (uint32_t)r;
+            prev = (uint32_t)r;
+        }
+        const unsigned long long j = reserve_slots(&wv.hdr[0], nj);
+        if (nj) {
+            const uint32_t tgt = ((uint32_t)r << 2) | (rsp ? 2u : 0u);
+            put_job(wv.jobs, j, x, wnee, we, job_key(pid, jfork), tgt);
+            if (nj == 2) put_job(wv.jobs, j + 1, x, M.sun_dir, ws, job_key(pid, jfork + 1), tgt | 1u);
+        }
+        if (finish) {  // end of the primal (_NEE_DS.h:106-110): escape term, then the path's totals
+            if (!scattered) Racc = Racc + M.env * W;
+            float* io = wv.info + 8 * (pid - wv.p_begin);
+            reinterpret_cast<float4*>(io)[0] = make_float4(Racc.x, Racc.y, Racc.z, Rspacc.x);
+            reinterpret_cast<float4*>(io)[1] = make_float4(Rspacc.y, Rspacc.z, __uint_as_float(first), 0.0f);
+            alive = false;
+        }
+    }
+    flush_counters(sc, n_paths_done, 0, tl);  // the forward counts the vertices
+}
+
+template <int TR>
+__global__ void __launch_bounds__(256, 4) k_shadow_T(DMedium M, WaveBw wv, uint64_t seed, DScratch* sc) {
+    const unsigned long long n = wv.hdr[0];
+    Tally tl;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const JobView jv = get_job(wv.jobs, i);
+        Rng r;
+        r.init(seed, jv.pid, 2u * (1u + jv.fork));
+        const float T = shadow_T<TR>(M, r, jv.x, jv.dir, tl, &sc->status);
+        VertexRec* rp = wv.recs + (jv.tgt >> 2);
+        if (jv.tgt & 1u) rp->Ts = T;
+        else rp->Te = T;
+        const float3 c3 = jv.wt * T;
+        if (c3.x != 0.0f || c3.y != 0.0f || c3.z != 0.0f) {
+            float* io = wv.info + 8 * (jv.pid - wv.p_begin) + ((jv.tgt & 2u) ? 3 : 0);
+            atomicAdd(io + 0, c3.x);
+            atomicAdd(io + 1, c3.y);
+            atomicAdd(io + 2, c3.z);
+        }
+    }
+    flush_counters(sc, 0, 0, tl);
+}
+
+__global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
+                                                    const float* __restrict__ dL, float div, DScratch* sc, WaveBw wv) {
+    const unsigned lane = threadIdx.x & 31u;
+    const float EPS = 0.00000001f;
+    const float eps = M.ds_eps;
+    const int lights = M.has_sun ? 2 : 1;
+    unsigned long long p_end = *((volatile unsigned long long*)&sc->next_path);
+    if (p_end > n_paths) p_end = n_paths;
+    const unsigned long long n_round = p_end - wv.p_begin;
+    Flight ff;
+    Rng rng;
+    float3 x = f3(0.0f), w = f3(0.0f), W = f3(0.0f), R = f3(0.0f), Rsp = f3(0.0f), dLdR = f3(0.0f);
+    float d = 0.0f;
+    bool alive = false, exhausted = false;
+    int bounces = 0;
+    uint64_t pid = 0;
+    uint32_t steps_path = 0, cur = kNone;
+    Tally tl;
+
+    while (true) {
+        unsigned want = __ballot_sync(kAll, !alive && !exhausted);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(&wv.hdr[2], (unsigned long long)__popc(want));
+            base = __shfl_sync(kAll, base, leader);
+            if (!alive && !exhausted) {
+                const unsigned long long k = base + __popc(want & ((1u << lane) - 1u));
+                if (k >= n_round) {
+                    exhausted = true;
+                } else {
+                    pid = wv.p_begin + k;
+                    rng.init(seed, pid, 0);
+                    float3 x0, w0;
+                    start_ray(S, pid, rng, x0, w0);
+                    dLdR = ld3(dL + 3 * out_index(S, pid)) / div;
+                    float tMin, tMax;
+                    boundary(M, x0, w0, tMin, tMax);
+                    x = x0 + w0 * tMin;
+                    w = w0;
+                    d = tMax - tMin;
+                    W = f3(1.0f);
+                    bounces = 0;
+                    steps_path = 0;
+                    const float4* io = reinterpret_cast<const float4*>(wv.info + 8 * k);
+                    const float4 a = io[0], b = io[1];
+                    R = make_float3(a.x, a.y, a.z);
+                    Rsp = make_float3(a.w, b.x, b.y);
+                    cur = __float_as_uint(b.z);
+                    ff = Flight();
+                    alive = true;
+                }
+            }
+        }
+        if (__all_sync(kAll, !alive && exhausted)) break;
+
+        int nj = 0;
+        float3 jd0 = f3(0.0f), jd1 = f3(0.0f);
+        float dT0 = 0.0f, dT1 = 0.0f;
+        uint32_t f0 = 0, f1 = 0;
+        if (alive) {
+            int ev = 0;
+            if (!(d > EPS)) {
+                ev = 2;
+            } else {
+                bool need = false;
+                float m = 0.0f, t = 0.0f;
+                if (ff.tau < 0.0f) ++tl.steps;
+                ff.sample(rng);
+                for (int k = 0;; ++k) {
+                    if (k >= kStepCap) {
+                        guard(sc, 4);
+                        ev = 2;
+                        break;
+                    }
+                    float md;
+                    m = gmax(EPS, ff.bk.query(M, x, w, md) + 2.0f * eps + 0.1f);
+                    t = ff.tau / m;
+                    x = x + w * gmin(t, md);
+                    if (t > md) {
+                        d -= md;
+                        ff.cross(m, md);
+                        ff.bk.advance(M);
+                        if (!(d > EPS)) { ev = 2; break; }
+                        continue;
+                    }
+                    ff.used();
+                    if (t > d) ev = 2;
+                    else need = true;
+                    ff.bk.move(t);
+                    break;
+                }
+                if (need) {
+                    const float s = sigma(M, x, tl);
+                    const float Pc = (s + eps) / m;
+                    float gsc;
+                    const bool real = !(rng.uniform() >= Pc);
+                    if (!real) {  // _NEE_DS.h:130-140
+                        gsc = dot(dLdR, -R / m / (1.0f - s / m));
+                        W = W * ((1.0f - s / m) / (1.0f - Pc));
+                        d -= t;
+                    } else {      // _NEE_DS.h:142-150
+                        gsc = dot(dLdR, s < EPS ? Rsp / eps : R / s);
+                    }
+                    if (gsc != 0.0f) sigma_bw(M, x, gsc, tl);
+                    if (real) {   // replayed vertex (_NEE_DS.h:151-203)
+                        W = W * (s / m / Pc);
+                        if (s < EPS) {
+                            ev = 2;
+                        } else {
+                            const float3 sa = albedo(M, x, tl);
+                            float3 dL_dsa = dLdR * W * -1.0f * M.emission;
+                            R = R - W * (f3(1.0f) - sa) * M.emission;
+                            dL_dsa = dL_dsa + dLdR * R / make_float3(gmax(EPS, sa.x), gmax(EPS, sa.y), gmax(EPS, sa.z));
+                            albedo_bw(M, x, dL_dsa, tl);
+                            float3 wnee;
+                            const float3 Le = environment_sample(M, rng, wnee);
+                            const float ph_nee = phase(M, w, wnee);
+                            const float ph_sun = M.has_sun ? phase(M, w, M.sun_dir) : 0.0f;
+                            const uint32_t jf = rng.ntr;
+                            rng.ntr += (uint32_t)lights;
+                            const float3 wo = phase_sample(M, rng, w);
+                            W = W * sa;
+                            float Te = 1.0f, Ts = 1.0f;
+                            if (cur == kNone) {
+                                guard(sc, 5);  // the replay left the primal's path
+                                ev = 2;
+                            } else {
+                                const VertexRec rec = wv.recs[cur];
+                                Te = rec.Te;
+                                Ts = rec.Ts;
+                                cur = rec.next;
+                            }
+                            if (ev != 2) {
+                                const float dTe = dot(dLdR, W * Le * ph_nee);
+                                R = R - W * Te * Le * ph_nee;
+                                if (dTe != 0.0f) { jd0 = wnee; dT0 = dTe; f0 = jf; nj = 1; }
+                                if (M.has_sun) {
+                                    const float dTs = dot(dLdR, W * M.sun_L * ph_sun);
+                                    R = R - W * Ts * M.sun_L * ph_sun;
+                                    if (dTs != 0.0f) {
+                                        if (nj == 0) { jd0 = M.sun_dir; dT0 = dTs; f0 = jf + 1; nj = 1; }
+                                        else { jd1 = M.sun_dir; dT1 = dTs; f1 = jf + 1; nj = 2; }
+                                    }
+                                }
+                                ++bounces;
+                                if ((M.max_bounces > 0 && bounces >= M.max_bounces) || all_less(W, EPS)) {
+                                    ev = 2;
+                                } else {
+                                    w = wo;
+                                    float tMin;
+                                    boundary(M, x, w, tMin, d);
+                                    ff = Flight();
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            if (++steps_path > (uint32_t)kPathCap) {
+                guard(sc, 6);
+                ev = 2;
+            }
+            if (ev == 2) alive = false;
+        }
+        const unsigned long long j = reserve_slots(&wv.hdr[0], nj);
+        if (nj) {
+            if (j + (unsigned long long)nj > wv.cap_jobs) {
+                guard(sc, 7);
+            } else {
+                put_job(wv.jobs, j, x, jd0, make_float3(dT0, 0.0f, 0.0f), job_key(pid, f0));
+                if (nj == 2) put_job(wv.jobs, j + 1, x, jd1, make_float3(dT1, 0.0f, 0.0f), job_key(pid, f1));
+            }
+        }
+    }
+    flush_counters(sc, 0, 0, tl);
+}
+
+template <int TR>
+__global__ void __launch_bounds__(256, 4) k_shadow_bw(DMedium M, WaveBw wv, uint64_t seed, DScratch* sc) {
+    unsigned long long n = wv.hdr[0];
+    if (n > wv.cap_jobs) n = wv.cap_jobs;
+    Tally tl;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const JobView jv = get_job(wv.jobs, i);
+        Rng r;
+        r.init(seed, jv.pid, 2u * (1u + jv.fork));
+        if (TR == 0) transmittance_rt_bw(M, r, jv.x, jv.dir, jv.wt.x, tl, &sc->status);
+        else if (TR == 1) transmittance_dt_bw(M, r, jv.x, jv.dir, jv.wt.x, tl, &sc->status);
+        else if (TR == 2) transmittance_dda_bw<false>(M, jv.x, jv.dir, jv.wt.x, tl);
+        else transmittance_dda_bw<true>(M, jv.x, jv.dir, jv.wt.x, tl);
+    }
+    flush_counters(sc, 0, 0, tl);
+}
+
+int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed,
+                      const float* dL, float div, cudaStream_t stream) {
+    if (n_paths == 0) return 0;
+    if (M.max_bounces <= 0 || M.ds_compat) return VRT_E_UNSUPPORTED;
+    const unsigned long long lights = M.has_sun ? 2ull : 1ull, B = (unsigned long long)M.max_bounces;
+    int blocksA = persistent_blocks((const void*)k_ds_primal, 256, ctx->num_sms);
+    int blocksC = persistent_blocks((const void*)k_ds_replay, 256, ctx->num_sms);
+    const uint64_t need = (n_paths + 255) / 256;
+    if ((uint64_t)blocksA > need) blocksA = (int)need;
+    if ((uint64_t)blocksC > need) blocksC = (int)need;
+    WaveBw wv;
+    wv.lanes = (unsigned long long)blocksA * 256ull;
+    wv.res_jobs = wv.lanes * lights * B;
+    wv.res_recs = wv.lanes * B;
+    wv.cap_jobs = 3ull * wv.res_jobs;
+    wv.cap_recs = 3ull * wv.res_recs;
+    if (wv.cap_jobs < (1ull << 24)) wv.cap_jobs = 1ull << 24;
+    if (wv.cap_recs < (1ull << 23)) wv.cap_recs = 1ull << 23;
+    if (wv.cap_recs > (1ull << 30)) return VRT_E_UNSUPPORTED;  // record indices are 30-bit in a job
+    wv.cap_paths = 1ull << 24;
+    if (wv.cap_paths < 4ull * wv.lanes) wv.cap_paths = 4ull * wv.lanes;
+    const size_t bytes = 256 + wv.cap_jobs * sizeof(ShadowJob) + wv.cap_recs * sizeof(VertexRec) + wv.cap_paths * 32;
+    int st = ensure_wave_buffer(ctx, bytes);
+    if (st) return st;
+    char* base = static_cast<char*>(ctx->wave);
+    wv.hdr = reinterpret_cast<unsigned long long*>(base);
+    wv.jobs = reinterpret_cast<ShadowJob*>(base + 256);
+    wv.recs = reinterpret_cast<VertexRec*>(base + 256 + wv.cap_jobs * sizeof(ShadowJob));
+    wv.info = reinterpret_cast<float*>(base + 256 + wv.cap_jobs * sizeof(ShadowJob) + wv.cap_recs * sizeof(VertexRec));
+    wv.p_begin = 0;
+    cudaError_t e = cudaMemsetAsync(&ctx->scratch->next_path, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return launch_status(e);
+    const int sblocks = ctx->num_sms * 8;
+    for (int round = 0;; ++round) {
+        if ((e = cudaMemsetAsync(wv.hdr, 0, 3 * sizeof(unsigned long long), stream)) != cudaSuccess)
+            return launch_status(e);
+        k_ds_primal<<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
+        switch (M.tr_mode) {
+            case 0: k_shadow_T<0><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
+            case 1: k_shadow_T<1><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
+            case 2: k_shadow_T<2><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
+            default: k_shadow_T<3><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
+        }
+        if ((e = cudaMemsetAsync(wv.hdr, 0, sizeof(unsigned long long), stream)) != cudaSuccess)
+            return launch_status(e);
+        k_ds_replay<<<blocksC, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, ctx->scratch, wv);
+        switch (M.tr_mode) {
+            case 0: k_shadow_bw<0><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
+            case 1: k_shadow_bw<1><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
+            case 2: k_shadow_bw<2><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
+            default: k_shadow_bw<3><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
+        }
+        count_launches(4);
+        if ((st = launch_status(cudaGetLastError()))) return st;
+        unsigned long long taken = 0;
+        if ((e = cudaMemcpyAsync(&taken, &ctx->scratch->next_path, sizeof(taken), cudaMemcpyDeviceToHost, stream)) !=
+            cudaSuccess)
+            return launch_status(e);
+        if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return launch_status(e);
+        if (taken >= n_paths) break;
+        wv.p_begin = taken;
         if (round > (1 << 20)) return VRT_E_ITER_CAP;
     }
     return 0;
