@@ -149,6 +149,124 @@ __device__ __forceinline__ void start_ray(const PathSrc& S, uint64_t pid, Rng& r
     }
 }
 
+// Jobs a round aims to hold beyond the reserve: twice the expected count of
+// the launch (two per path and light), at least 2^20 and at most 2^25.
+inline unsigned long long batch_jobs(uint64_t n_paths, unsigned long long per_path) {
+    unsigned long long c = (unsigned long long)n_paths * per_path * 2ull;
+    if (c < (1ull << 20)) c = 1ull << 20;
+    if (c > (1ull << 25)) c = 1ull << 25;
+    return c;
+}
+
+// ---------------------------------------------------------------------------
+// A shadow ray advanced one event per call: a majorant-brick crossing or a
+// tracking collision.  The draws and arithmetic are those of transmittance_rt
+// / transmittance_dt (vr_transmittance_RT.h:1-49, _DT.h:1-28) and of the first
+// pass of their adjoints (_RT.h:51-98, _DT.h:30-62, majorant + 0.1); kernels
+// that run one event per loop iteration for every lane keep the warp in one
+// code path while rays of different lengths finish and are replaced.
+// ---------------------------------------------------------------------------
+struct ShadowRay {
+    float3 x, dir;
+    float d, T;
+    Flight ff;
+    Rng r;
+    int it;
+};
+
+// Starts the ray (x, dir) on fork `fork` of path pid; false when it misses the
+// medium (T = 1).
+__device__ __forceinline__ bool shadow_begin(const DMedium& M, ShadowRay& s, float3 x, float3 dir, uint64_t seed,
+                                             uint64_t pid, uint32_t fork) {
+    s.r.init(seed, pid, 2u * (1u + fork));
+    s.T = 1.0f;
+    s.it = 0;
+    s.ff = Flight();
+    s.dir = dir;
+    float tMin, tMax;
+    if (!boundary(M, x, dir, tMin, tMax)) return false;
+    s.x = x + dir * tMin;
+    s.d = tMax - tMin;
+    return true;
+}
+
+// One event.  TR 0 ratio tracking, 1 delta tracking; BW: the adjoint's first
+// pass (majorant + 0.1, ratio-tracking roulette below 0.1).  Returns true when
+// the estimate is complete (s.T).  On a tracking collision that continues the
+// ray, hit is set with the majorant and the factor the adjoint's second pass
+// scatters with (RT: r = 1 - sigma/maj; DT: Pc = sigma/maj).
+template <int TR, bool BW>
+__device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tally& tl, DScratch* sc, bool& hit,
+                                             float& hmaj, float& hf) {
+    hit = false;
+    if (++s.it > kStepCap) {
+        raise_status(&sc->status, 4);
+        return true;
+    }
+    float md;
+    const float EPS = 0.0000001f;
+    if (TR == 0) {
+        const float q = s.ff.bk.query(M, s.x, s.dir, md);
+        const float maj = BW ? gmax(EPS, q + 0.1f) : gmax(EPS, q);
+        if (!BW && s.ff.tau < 0.0f) ++tl.steps;
+        const float t = s.ff.sample(s.r) / maj;
+        if (md < s.d && t > md) {
+            s.x = s.x + s.dir * md;
+            s.d -= md;
+            s.ff.cross(maj, md);
+            s.ff.bk.advance(M);
+            return false;
+        }
+        s.ff.used();
+        const float dt = gmin(t, gmin(s.d, md));
+        s.ff.bk.move(dt);
+        s.x = s.x + s.dir * dt;
+        s.d -= dt;
+        if (s.d <= EPS) return true;
+        const float r = 1.0f - sigma(M, s.x, tl) / maj;
+        s.T *= r;
+        if (s.T < (BW ? 0.1f : 0.01f)) {
+            if (s.r.uniform() < 1.0f - s.T) {
+                s.T = 0.0f;
+                return true;
+            }
+            s.T = 1.0f;
+        }
+        hit = true;
+        hmaj = maj;
+        hf = r;
+        return false;
+    } else {
+        const float q = s.ff.bk.query(M, s.x, s.dir, md);
+        const float maj = BW ? gmax(EPS, q + 0.1f) : gmax(EPS, q);
+        if (!BW && s.ff.tau < 0.0f) ++tl.steps;
+        const float dt = s.ff.sample(s.r) / maj;
+        const float t = gmin(md, dt);
+        s.x = s.x + s.dir * t;
+        s.d -= t;
+        if (s.d <= EPS) {
+            s.T = 1.0f;
+            return true;
+        }
+        if (dt > md) {
+            s.ff.cross(maj, md);
+            s.ff.bk.advance(M);
+            return false;
+        }
+        s.ff.used();
+        s.ff.bk.move(t);
+        const float Pc = sigma(M, s.x, tl) / maj;
+        if (s.r.uniform() < Pc) {
+            s.T = 0.0f;
+            return true;
+        }
+        hit = true;
+        hmaj = maj;
+        hf = Pc;
+        return false;
+    }
+}
+
 }  // namespace
 
 struct WaveFw {
@@ -354,24 +472,198 @@ __global__ void __launch_bounds__(256, 4) k_shadow_fw(DMedium M, PathSrc S, cons
     flush_counters(sc, 0, 0, tl);
 }
 
+namespace {
+constexpr uint32_t kNone = 0xffffffffu;
+// A primal vertex of the NEE_DS adjoint wavefront: its two shadow
+// transmittances and the next vertex of the same path.
+struct VertexRec {
+    float Te, Ts;
+    uint32_t next, pad;
+};
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Persistent shadow kernels for ratio / delta tracking: one event per lane per
+// iteration, finished lanes refilled from the job buffer with one atomic per
+// warp (ranks from a ballot).
+// ---------------------------------------------------------------------------
+struct ShadowOut {
+    float* out;        // OUT_IMAGE: image / ray radiance
+    float scale;
+    VertexRec* recs;   // OUT_RECORD: vertex records and per-path R / Rsp
+    float* info;
+    uint64_t p_begin;
+};
+enum : int { OUT_IMAGE = 0, OUT_RECORD = 1 };
+
+template <int OUT>
+__device__ __forceinline__ void shadow_finish(const PathSrc& S, const ShadowOut& so, const JobView& jv, float T) {
+    if (OUT == OUT_RECORD) {
+        VertexRec* rp = so.recs + (jv.tgt >> 2);
+        if (jv.tgt & 1u) rp->Ts = T;
+        else rp->Te = T;
+    }
+    const float3 c3 = jv.wt * T;
+    if (c3.x != 0.0f || c3.y != 0.0f || c3.z != 0.0f) {
+        if (OUT == OUT_IMAGE) {
+            float* o = so.out + 3 * out_index(S, jv.pid);
+            atomicAdd(o + 0, c3.x * so.scale);
+            atomicAdd(o + 1, c3.y * so.scale);
+            atomicAdd(o + 2, c3.z * so.scale);
+        } else {
+            float* o = so.info + 8 * (jv.pid - so.p_begin) + ((jv.tgt & 2u) ? 3 : 0);
+            atomicAdd(o + 0, c3.x);
+            atomicAdd(o + 1, c3.y);
+            atomicAdd(o + 2, c3.z);
+        }
+    }
+}
+
+template <int TR, int OUT>
+__global__ void __launch_bounds__(256, 4) k_shadow_run(DMedium M, PathSrc S, const ShadowJob* __restrict__ jobs,
+                                                     const unsigned long long* __restrict__ count,
+                                                     unsigned long long cap, unsigned long long* head, uint64_t seed,
+                                                     ShadowOut so, DScratch* sc) {
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned long long n = *count;
+    if (n > cap) n = cap;
+    ShadowRay s;
+    JobView jv;
+    bool alive = false, exhausted = false;
+    Tally tl;
+    while (true) {
+        const unsigned want = __ballot_sync(kAll, !alive && !exhausted);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(head, (unsigned long long)__popc(want));
+            base = __shfl_sync(kAll, base, leader);
+            if (!alive && !exhausted) {
+                const unsigned long long i = base + __popc(want & ((1u << lane) - 1u));
+                if (i >= n) {
+                    exhausted = true;
+                } else {
+                    jv = get_job(jobs, i);
+                    alive = shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork);
+                    if (!alive) shadow_finish<OUT>(S, so, jv, 1.0f);
+                }
+            }
+        }
+        if (__all_sync(kAll, !alive && exhausted)) break;
+        if (alive) {
+            bool hit;
+            float hm, hf;
+            if (shadow_event<TR, false>(M, s, tl, sc, hit, hm, hf)) {
+                shadow_finish<OUT>(S, so, jv, s.T);
+                alive = false;
+            }
+        }
+    }
+    flush_counters(sc, 0, 0, tl);
+}
+
+// The transmittance adjoint (vr_transmittance_RT.h:51-141 / _DT.h:30-90): the
+// first pass runs as events and keeps its tracking collisions; the second pass
+// of the reference replays the same draws and scatters at exactly those
+// points, so the scatter is done from the kept list once the first pass's
+// estimate is known.  A ray with more than kKeep collisions replays its
+// second pass as events instead.
+constexpr int kKeep = 16;
+
+template <int TR>
+__global__ void __launch_bounds__(256, 3) k_shadow_adj(DMedium M, const ShadowJob* __restrict__ jobs,
+                                                     const unsigned long long* __restrict__ count,
+                                                     unsigned long long cap, unsigned long long* head, uint64_t seed,
+                                                     DScratch* sc) {
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned long long n = *count;
+    if (n > cap) n = cap;
+    ShadowRay s;
+    JobView jv;
+    float4 keep[kKeep];  // position, majorant
+    float keepf[kKeep];  // RT: r; DT: Pc
+    int nkeep = 0, phase = 0;  // 0 idle, 1 first pass, 2 second pass (more than kKeep collisions)
+    float outT = 0.0f;
+    bool exhausted = false;
+    Tally tl;
+    while (true) {
+        const unsigned want = __ballot_sync(kAll, phase == 0 && !exhausted);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(head, (unsigned long long)__popc(want));
+            base = __shfl_sync(kAll, base, leader);
+            if (phase == 0 && !exhausted) {
+                const unsigned long long i = base + __popc(want & ((1u << lane) - 1u));
+                if (i >= n) {
+                    exhausted = true;
+                } else {
+                    jv = get_job(jobs, i);
+                    nkeep = 0;
+                    if (jv.wt.x != 0.0f && shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork)) phase = 1;
+                }
+            }
+        }
+        if (__all_sync(kAll, phase == 0 && exhausted)) break;
+        if (phase != 0) {
+            bool hit;
+            float hm, hf;
+            const bool done = shadow_event<TR, true>(M, s, tl, sc, hit, hm, hf);
+            const float dLdT = jv.wt.x;
+            if (phase == 1) {
+                if (hit) {
+                    if (nkeep < kKeep) {
+                        keep[nkeep] = make_float4(s.x.x, s.x.y, s.x.z, hm);
+                        keepf[nkeep] = hf;
+                    }
+                    ++nkeep;
+                }
+                if (done) {
+                    outT = s.T;
+                    if (outT == 0.0f || s.it > kStepCap) {
+                        phase = 0;  // ended by the roulette, a collision or the step cap: no gradient
+                    } else if (nkeep <= kKeep) {
+                        for (int k = 0; k < nkeep; ++k) {
+                            const float3 px = make_float3(keep[k].x, keep[k].y, keep[k].z);
+                            const float g = TR == 0 ? -outT * dLdT / keep[k].w / keepf[k]
+                                                    : -dLdT / keep[k].w / (1.0f - keepf[k]);
+                            sigma_bw(M, px, g, tl);
+                        }
+                        phase = 0;
+                    } else {  // replay the second pass
+                        shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork);
+                        phase = 2;
+                    }
+                }
+            } else {
+                if (hit) {
+                    const float g = TR == 0 ? -outT * dLdT / hm / hf : -dLdT / hm / (1.0f - hf);
+                    sigma_bw(M, s.x, g, tl);
+                }
+                if (done) phase = 0;
+            }
+        }
+    }
+    flush_counters(sc, 0, 0, tl);
+}
+
 // Host: rounds of walk + shadow until every path has been taken.
 int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed, float* out,
                    float scale, cudaStream_t stream) {
     if (n_paths == 0) return 0;
     if (M.max_bounces <= 0) return VRT_E_UNSUPPORTED;
-    const int lights = M.has_sun ? 2 : 1;
-    const unsigned long long per_path = 1ull + (unsigned long long)lights * (unsigned long long)M.max_bounces;
+    const unsigned long long lights = M.has_sun ? 2ull : 1ull;
+    const unsigned long long per_path = 1ull + lights * (unsigned long long)M.max_bounces;
     int blocks = persistent_blocks((const void*)k_walk_fw, 256, ctx->num_sms);
     const uint64_t need = (n_paths + 255) / 256;
     if ((uint64_t)blocks > need) blocks = (int)need;
-    const unsigned long long reserve = (unsigned long long)blocks * 256ull * per_path;
-    unsigned long long cap = 3ull * reserve;
-    if (cap < (1ull << 24)) cap = 1ull << 24;
+    // the worst case of every path in flight, plus room for a round's expected jobs
+    unsigned long long inflight = (unsigned long long)blocks * 256ull;
+    if (inflight > n_paths) inflight = n_paths;
+    const unsigned long long reserve = inflight * per_path;
+    const unsigned long long cap = reserve + batch_jobs(n_paths, 1ull + lights);
     int st = ensure_wave_buffer(ctx, 256 + cap * sizeof(ShadowJob));
-    if (st) {  // fall back to a smaller buffer (still > reserve)
-        cap = reserve + reserve / 2;
-        if ((st = ensure_wave_buffer(ctx, 256 + cap * sizeof(ShadowJob)))) return st;
-    }
+    if (st) return st;
     WaveFw wv;
     wv.count = reinterpret_cast<unsigned long long*>(ctx->wave);
     wv.jobs = reinterpret_cast<ShadowJob*>(static_cast<char*>(ctx->wave) + 256);
@@ -380,13 +672,17 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
     cudaError_t e = cudaMemsetAsync(&ctx->scratch->next_path, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return launch_status(e);
     const int sblocks = ctx->num_sms * 8;
+    const int rblocks = persistent_blocks(M.tr_mode == 0 ? (const void*)k_shadow_run<0, OUT_IMAGE>
+                                                         : (const void*)k_shadow_run<1, OUT_IMAGE>, 256, ctx->num_sms);
+    const ShadowOut so = {out, scale, nullptr, nullptr, 0};
     for (int round = 0;; ++round) {
-        if ((e = cudaMemsetAsync(wv.count, 0, sizeof(unsigned long long), stream)) != cudaSuccess)
+        // count of the jobs written, and the head the persistent shadow kernel takes them from
+        if ((e = cudaMemsetAsync(wv.count, 0, 2 * sizeof(unsigned long long), stream)) != cudaSuccess)
             return launch_status(e);
         k_walk_fw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, ctx->scratch, wv);
         switch (M.tr_mode) {
-            case 0: k_shadow_fw<0><<<sblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, seed, out, scale, ctx->scratch); break;
-            case 1: k_shadow_fw<1><<<sblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, seed, out, scale, ctx->scratch); break;
+            case 0: k_shadow_run<0, OUT_IMAGE><<<rblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, wv.cap, wv.count + 1, seed, so, ctx->scratch); break;
+            case 1: k_shadow_run<1, OUT_IMAGE><<<rblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, wv.cap, wv.count + 1, seed, so, ctx->scratch); break;
             case 2: k_shadow_fw<2><<<sblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, seed, out, scale, ctx->scratch); break;
             default: k_shadow_fw<3><<<sblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, seed, out, scale, ctx->scratch); break;
         }
@@ -425,13 +721,6 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
 //
 // Rounds bound the buffers as in the forward wavefront.
 // ------------------------------------------------------------------------
-namespace {
-constexpr uint32_t kNone = 0xffffffffu;
-struct VertexRec {
-    float Te, Ts;
-    uint32_t next, pad;
-};
-}  // namespace
 
 struct WaveBw {
     ShadowJob* jobs;
@@ -857,15 +1146,13 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     if ((uint64_t)blocksC > need) blocksC = (int)need;
     WaveBw wv;
     wv.lanes = (unsigned long long)blocksA * 256ull;
-    wv.res_jobs = wv.lanes * lights * B;
-    wv.res_recs = wv.lanes * B;
-    wv.cap_jobs = 3ull * wv.res_jobs;
-    wv.cap_recs = 3ull * wv.res_recs;
-    if (wv.cap_jobs < (1ull << 24)) wv.cap_jobs = 1ull << 24;
-    if (wv.cap_recs < (1ull << 23)) wv.cap_recs = 1ull << 23;
+    const unsigned long long inflight = wv.lanes < n_paths ? wv.lanes : n_paths;
+    wv.res_jobs = inflight * lights * B;
+    wv.res_recs = inflight * B;
+    wv.cap_jobs = wv.res_jobs + batch_jobs(n_paths, lights);
+    wv.cap_recs = wv.res_recs + batch_jobs(n_paths, 1);
     if (wv.cap_recs > (1ull << 30)) return VRT_E_UNSUPPORTED;  // record indices are 30-bit in a job
-    wv.cap_paths = 1ull << 24;
-    if (wv.cap_paths < 4ull * wv.lanes) wv.cap_paths = 4ull * wv.lanes;
+    wv.cap_paths = (n_paths < (1ull << 24) ? n_paths : (1ull << 24)) + wv.lanes;
     const size_t bytes = 256 + wv.cap_jobs * sizeof(ShadowJob) + wv.cap_recs * sizeof(VertexRec) + wv.cap_paths * 32;
     int st = ensure_wave_buffer(ctx, bytes);
     if (st) return st;
@@ -878,13 +1165,20 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     cudaError_t e = cudaMemsetAsync(&ctx->scratch->next_path, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return launch_status(e);
     const int sblocks = ctx->num_sms * 8;
+    const int tblocks = persistent_blocks(M.tr_mode == 0 ? (const void*)k_shadow_run<0, OUT_RECORD>
+                                                         : (const void*)k_shadow_run<1, OUT_RECORD>, 256, ctx->num_sms);
+    const int ablocks = persistent_blocks(M.tr_mode == 0 ? (const void*)k_shadow_adj<0> : (const void*)k_shadow_adj<1>,
+                                          256, ctx->num_sms);
+    ShadowOut sor = {nullptr, 0.0f, wv.recs, wv.info, 0};
     for (int round = 0;; ++round) {
-        if ((e = cudaMemsetAsync(wv.hdr, 0, 3 * sizeof(unsigned long long), stream)) != cudaSuccess)
+        // [0] jobs, [1] records, [2] replay queue, [3] / [4] heads of the shadow kernels
+        if ((e = cudaMemsetAsync(wv.hdr, 0, 5 * sizeof(unsigned long long), stream)) != cudaSuccess)
             return launch_status(e);
+        sor.p_begin = wv.p_begin;
         k_ds_primal<<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
         switch (M.tr_mode) {
-            case 0: k_shadow_T<0><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
-            case 1: k_shadow_T<1><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
+            case 0: k_shadow_run<0, OUT_RECORD><<<tblocks, 256, 0, stream>>>(M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[3], seed, sor, ctx->scratch); break;
+            case 1: k_shadow_run<1, OUT_RECORD><<<tblocks, 256, 0, stream>>>(M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[3], seed, sor, ctx->scratch); break;
             case 2: k_shadow_T<2><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
             default: k_shadow_T<3><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
         }
@@ -892,8 +1186,8 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
             return launch_status(e);
         k_ds_replay<<<blocksC, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, ctx->scratch, wv);
         switch (M.tr_mode) {
-            case 0: k_shadow_bw<0><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
-            case 1: k_shadow_bw<1><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
+            case 0: k_shadow_adj<0><<<ablocks, 256, 0, stream>>>(M, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, ctx->scratch); break;
+            case 1: k_shadow_adj<1><<<ablocks, 256, 0, stream>>>(M, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, ctx->scratch); break;
             case 2: k_shadow_bw<2><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
             default: k_shadow_bw<3><<<sblocks, 256, 0, stream>>>(M, wv, seed, ctx->scratch); break;
         }
