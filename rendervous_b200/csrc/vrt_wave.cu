@@ -190,33 +190,60 @@ __device__ __forceinline__ bool shadow_begin(const DMedium& M, ShadowRay& s, flo
     return true;
 }
 
-// One event.  TR 0 ratio tracking, 1 delta tracking; BW: the adjoint's first
-// pass (majorant + 0.1, ratio-tracking roulette below 0.1).  Returns true when
-// the estimate is complete (s.T).  On a tracking collision that continues the
-// ray, hit is set with the majorant and the factor the adjoint's second pass
-// scatters with (RT: r = 1 - sigma/maj; DT: Pc = sigma/maj).
+// One step: brick crossings (at most kCross) up to the next tracking
+// collision, then that collision.  TR 0 ratio tracking, 1 delta tracking; BW:
+// the adjoint's first pass (majorant + 0.1, ratio-tracking roulette below
+// 0.1).  The lanes of a warp cross bricks in the inner loop and meet for the
+// expensive part (sigma gather, draws), which thus runs with most lanes
+// active.  Returns true when the estimate is complete (s.T).  On a tracking
+// collision that continues the ray, hit is set with the majorant and the
+// factor the adjoint's second pass scatters with (RT: r = 1 - sigma/maj; DT:
+// Pc = sigma/maj).
+constexpr int kCross = 16;
+
 template <int TR, bool BW>
 __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tally& tl, DScratch* sc, bool& hit,
                                              float& hmaj, float& hf) {
     hit = false;
-    if (++s.it > kStepCap) {
-        raise_status(&sc->status, 4);
-        return true;
-    }
-    float md;
     const float EPS = 0.0000001f;
-    if (TR == 0) {
-        const float q = s.ff.bk.query(M, s.x, s.dir, md);
-        const float maj = BW ? gmax(EPS, q + 0.1f) : gmax(EPS, q);
-        if (!BW && s.ff.tau < 0.0f) ++tl.steps;
-        const float t = s.ff.sample(s.r) / maj;
-        if (md < s.d && t > md) {
-            s.x = s.x + s.dir * md;
-            s.d -= md;
-            s.ff.cross(maj, md);
-            s.ff.bk.advance(M);
-            return false;
+    float md, maj, t;
+    for (int c = 0;; ++c) {
+        if (++s.it > kStepCap) {
+            raise_status(&sc->status, 4);
+            return true;
         }
+        const float q = s.ff.bk.query(M, s.x, s.dir, md);
+        maj = BW ? gmax(EPS, q + 0.1f) : gmax(EPS, q);
+        if (!BW && s.ff.tau < 0.0f) ++tl.steps;
+        if (TR == 0) {
+            t = s.ff.sample(s.r) / maj;
+            if (md < s.d && t > md) {
+                s.x = s.x + s.dir * md;
+                s.d -= md;
+                s.ff.cross(maj, md);
+                s.ff.bk.advance(M);
+                if (c + 1 >= kCross) return false;
+                continue;
+            }
+        } else {
+            const float dt = s.ff.sample(s.r) / maj;
+            t = gmin(md, dt);
+            s.x = s.x + s.dir * t;
+            s.d -= t;
+            if (s.d <= EPS) {
+                s.T = 1.0f;
+                return true;
+            }
+            if (dt > md) {
+                s.ff.cross(maj, md);
+                s.ff.bk.advance(M);
+                if (c + 1 >= kCross) return false;
+                continue;
+            }
+        }
+        break;
+    }
+    if (TR == 0) {
         s.ff.used();
         const float dt = gmin(t, gmin(s.d, md));
         s.ff.bk.move(dt);
@@ -237,22 +264,6 @@ __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tal
         hf = r;
         return false;
     } else {
-        const float q = s.ff.bk.query(M, s.x, s.dir, md);
-        const float maj = BW ? gmax(EPS, q + 0.1f) : gmax(EPS, q);
-        if (!BW && s.ff.tau < 0.0f) ++tl.steps;
-        const float dt = s.ff.sample(s.r) / maj;
-        const float t = gmin(md, dt);
-        s.x = s.x + s.dir * t;
-        s.d -= t;
-        if (s.d <= EPS) {
-            s.T = 1.0f;
-            return true;
-        }
-        if (dt > md) {
-            s.ff.cross(maj, md);
-            s.ff.bk.advance(M);
-            return false;
-        }
         s.ff.used();
         s.ff.bk.move(t);
         const float Pc = sigma(M, s.x, tl) / maj;
