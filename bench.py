@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--small", action="store_true", help="a 128x128, 8 spp image of the same medium (profiling)")
+    ap.add_argument("--width", type=int, default=None, help="square image size of the same medium (profiling)")
+    ap.add_argument("--spp", type=int, default=None, help="samples per pixel (profiling)")
     return ap.parse_args()
 
 
@@ -207,8 +209,8 @@ def run_ours(args):
     maps.set_sync_checks(False)
 
     wl, sigma, albedo, target_sigma, sun, poses_np = workload_arrays()
-    H = W = 128 if args.small else wl["width"]
-    spp = 8 if args.small else wl["spp"]
+    H = W = args.width or (128 if args.small else wl["width"])
+    spp = args.spp or (8 if args.small else wl["spp"])
     sigma_t = torch.nn.Parameter(torch.from_numpy(sigma).to(dev))
     albedo_t = torch.nn.Parameter(torch.from_numpy(albedo).to(dev))
     field = build_field(sigma_t, albedo_t, wl, sun)
@@ -363,7 +365,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
-            "config": {"workload": WORKLOAD + ("_small128" if args.small else ""), "grid": list(sigma.shape[:3]),
+            "config": {"workload": WORKLOAD + ("" if (H, spp) == (wl["width"], wl["spp"]) else f"_{W}px_{spp}spp"), "grid": list(sigma.shape[:3]),
                        "image": [H, W], "spp": spp, "max_bounces": wl["max_bounces"], "phase_g": wl["phase_g"],
                        "transmittance": "ratio tracking", "majorant": "8^3-brick grid", "adjoint": "NEE_DS",
                        "l2": "flushed between steps (512 MB write)", "parallelism": f"dp{world}"},

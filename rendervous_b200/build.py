@@ -12,9 +12,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvrt.so")
-SOURCES = ["vrt_api.cu", "vrt_transmittance.cu", "vrt_path.cu", "vrt_adjoint.cu", "vrt_wave.cu", "vrt_cache.cu",
-           "vrt_noalloc.cu"]
-HEADERS = ["vrt_device.cuh", "vrt_tracking.cuh", "vrt_params.h", "vrt_internal.h"]
+SOURCES = ["vrt_api.cu", "vrt_transmittance.cu", "vrt_path.cu", "vrt_adjoint.cu", "vrt_wave.cu", "vrt_wave_ds.cu",
+           "vrt_cache.cu", "vrt_noalloc.cu"]
+HEADERS = ["vrt_device.cuh", "vrt_tracking.cuh", "vrt_params.h", "vrt_internal.h", "vrt_wave.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -61,7 +61,7 @@ def up_to_date() -> bool:
 # Files whose kernels must round every operation on its own: the wavefront
 # primal and replay walks are separate kernels that have to retrace the same
 # path bit for bit, so no a*b+c may be contracted differently in the two.
-PER_FILE_FLAGS = {"vrt_wave.cu": ["-fmad=false"]}
+PER_FILE_FLAGS = {"vrt_wave_ds.cu": ["-fmad=false"]}
 OBJ_DIR = os.path.join(HERE, "_build")
 
 

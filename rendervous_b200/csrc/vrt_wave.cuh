@@ -1,0 +1,289 @@
+// vrt_wave.cuh -- pieces shared by the wavefront kernels: the shadow-job
+// buffer, warp-aggregated slot reservation, counter flushes, and a shadow ray
+// advanced one step at a time (vrt_wave.cu: forward walk and every shadow
+// kernel; vrt_wave_ds.cu: the NEE_DS primal and replay walks).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/vrt.h"
+#include "vrt_device.cuh"
+#include "vrt_internal.h"
+#include "vrt_tracking.cuh"
+
+namespace vrt {
+namespace wave {
+
+constexpr unsigned kAll = 0xffffffffu;
+constexpr int kPathCap = 1 << 26;  // free-flight steps of one path before VRT_E_ITER_CAP
+
+// 48 bytes: position, direction, weight, key = pid << 16 | fork
+struct ShadowJob {
+    float4 a, b, c;
+};
+
+__device__ __forceinline__ void put_job(ShadowJob* J, unsigned long long slot, float3 x, float3 d, float3 wt,
+                                        unsigned long long key, uint32_t tgt = 0u) {
+    float4* p = reinterpret_cast<float4*>(J + slot);
+    p[0] = make_float4(x.x, x.y, x.z, d.x);
+    p[1] = make_float4(d.y, d.z, wt.x, wt.y);
+    p[2] = make_float4(wt.z, __uint_as_float(tgt), __uint_as_float((uint32_t)key), __uint_as_float((uint32_t)(key >> 32)));
+}
+
+struct JobView {
+    float3 x, dir, wt;
+    uint64_t pid;
+    uint32_t fork, tgt;
+};
+__device__ __forceinline__ JobView get_job(const ShadowJob* J, unsigned long long i) {
+    const float4* p = reinterpret_cast<const float4*>(J + i);
+    const float4 a = __ldcs(p), b = __ldcs(p + 1), c = __ldcs(p + 2);
+    JobView v;
+    v.x = make_float3(a.x, a.y, a.z);
+    v.dir = make_float3(a.w, b.x, b.y);
+    v.wt = make_float3(b.z, b.w, c.x);
+    v.tgt = __float_as_uint(c.y);
+    const unsigned long long key = (unsigned long long)__float_as_uint(c.z) | ((unsigned long long)__float_as_uint(c.w) << 32);
+    v.pid = key >> 16;
+    v.fork = (uint32_t)(key & 0xffffu);
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long job_key(uint64_t pid, uint32_t fork) {
+    return ((unsigned long long)pid << 16) | (unsigned long long)(fork & 0xffffu);
+}
+
+// Reserves n slots for this lane (all 32 lanes call it): an inclusive warp scan
+// of n, one atomicAdd by the last lane, the base broadcast.
+__device__ __forceinline__ unsigned long long reserve_slots(unsigned long long* count, int n) {
+    const unsigned lane = threadIdx.x & 31u;
+    int incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(kAll, incl, o);
+        if ((int)lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(kAll, incl, 31);
+    unsigned long long base = 0;
+    if (total > 0) {
+        if (lane == 31u) base = atomicAdd(count, (unsigned long long)total);
+        base = __shfl_sync(kAll, base, 31);
+    }
+    return base + (unsigned long long)(incl - n);
+}
+
+// Per-warp sums of the lanes' tallies into the context counters.  `verts`
+// counts forward path vertices only (the metric's unit); adjoint kernels pass 0.
+__device__ __forceinline__ void flush_counters(DScratch* sc, uint32_t paths, uint32_t verts, const Tally& tl) {
+    unsigned long long p = paths, v = verts, s = tl.steps, l = tl.lookups, a = tl.albedo, r = tl.reds;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        p += __shfl_down_sync(kAll, p, o);
+        v += __shfl_down_sync(kAll, v, o);
+        s += __shfl_down_sync(kAll, s, o);
+        l += __shfl_down_sync(kAll, l, o);
+        a += __shfl_down_sync(kAll, a, o);
+        r += __shfl_down_sync(kAll, r, o);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        if (p) atomicAdd(&sc->paths, p);
+        if (v) atomicAdd(&sc->vertices, v);
+        if (s) atomicAdd(&sc->steps, s);
+        if (l) atomicAdd(&sc->lookups, l);
+        if (a) atomicAdd(&sc->albedo, a);
+        if (r) atomicAdd(&sc->reds, r);
+    }
+}
+
+// a device guard fired: the error code plus the site (VRT_E_ITER_CAP in both)
+__device__ __forceinline__ void guard(DScratch* sc, int site) {
+    atomicOr(&sc->status, 1u << 4);
+    atomicOr(&sc->detail, 1u << site);
+}
+
+__device__ __forceinline__ long long out_index(const PathSrc& S, uint64_t pid) {
+    return S.is_camera ? (long long)(pid % (uint64_t)S.npix) : (long long)pid;
+}
+
+template <int TR>
+__device__ __forceinline__ float shadow_T(const DMedium& M, Rng& r, float3 x, float3 dir, Tally& tl, uint32_t* status) {
+    if (TR == 0) return transmittance_rt(M, r, x, dir, tl, status);
+    if (TR == 1) return transmittance_dt(M, r, x, dir, tl, status);
+    if (TR == 2) return transmittance_dda<false>(M, x, dir, tl);
+    return transmittance_dda<true>(M, x, dir, tl);
+}
+
+// The primary ray of path pid (camera or ray input), with the camera's draws.
+__device__ __forceinline__ void start_ray(const PathSrc& S, uint64_t pid, Rng& rng, float3& x0, float3& w0) {
+    if (S.is_camera) {
+        const long long px = (long long)(pid % (uint64_t)S.npix);
+        const long long hw = (long long)S.cam.height * S.cam.width;
+        const int view = (int)(px / hw);
+        const int rem = (int)(px - (long long)view * hw);
+        camera_ray(S.cam, view, rem / S.cam.width, rem % S.cam.width, rng, x0, w0);
+    } else {
+        x0 = ld3(S.rays + 6 * pid);
+        w0 = ld3(S.rays + 6 * pid + 3);
+    }
+}
+
+// Jobs a round aims to hold beyond the reserve: twice the expected count of
+// the launch (two per path and light), at least 2^20 and at most 2^25.
+inline unsigned long long batch_jobs(uint64_t n_paths, unsigned long long per_path) {
+    unsigned long long c = (unsigned long long)n_paths * per_path * 2ull;
+    if (c < (1ull << 20)) c = 1ull << 20;
+    if (c > (1ull << 25)) c = 1ull << 25;
+    return c;
+}
+
+// ---------------------------------------------------------------------------
+// A shadow ray advanced one event per call: a majorant-brick crossing or a
+// tracking collision.  The draws and arithmetic are those of transmittance_rt
+// / transmittance_dt (vr_transmittance_RT.h:1-49, _DT.h:1-28) and of the first
+// pass of their adjoints (_RT.h:51-98, _DT.h:30-62, majorant + 0.1); kernels
+// that run one event per loop iteration for every lane keep the warp in one
+// code path while rays of different lengths finish and are replaced.
+// ---------------------------------------------------------------------------
+struct ShadowRay {
+    float3 x, dir;
+    float d, T;
+    Flight ff;
+    Rng r;
+    int it;
+};
+
+// Starts the ray (x, dir) on fork `fork` of path pid; false when it misses the
+// medium (T = 1).
+__device__ __forceinline__ bool shadow_begin(const DMedium& M, ShadowRay& s, float3 x, float3 dir, uint64_t seed,
+                                             uint64_t pid, uint32_t fork) {
+    s.r.init(seed, pid, 2u * (1u + fork));
+    s.T = 1.0f;
+    s.it = 0;
+    s.ff = Flight();
+    s.dir = dir;
+    float tMin, tMax;
+    if (!boundary(M, x, dir, tMin, tMax)) return false;
+    s.x = x + dir * tMin;
+    s.d = tMax - tMin;
+    return true;
+}
+
+// One step: brick crossings (at most kCross) up to the next tracking
+// collision, then that collision.  TR 0 ratio tracking, 1 delta tracking; BW:
+// the adjoint's first pass (majorant + 0.1, ratio-tracking roulette below
+// 0.1).  The lanes of a warp cross bricks in the inner loop and meet for the
+// expensive part (sigma gather, draws), which thus runs with most lanes
+// active.  Returns true when the estimate is complete (s.T).  On a tracking
+// collision that continues the ray, hit is set with the majorant and the
+// factor the adjoint's second pass scatters with (RT: r = 1 - sigma/maj; DT:
+// Pc = sigma/maj).
+constexpr int kCross = 16;
+
+template <int TR, bool BW>
+__device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tally& tl, DScratch* sc, bool& hit,
+                                             float& hmaj, float& hf) {
+    hit = false;
+    const float EPS = 0.0000001f;
+    float md, maj, t;
+    for (int c = 0;; ++c) {
+        if (++s.it > kStepCap) {
+            raise_status(&sc->status, 4);
+            return true;
+        }
+        const float q = s.ff.bk.query(M, s.x, s.dir, md);
+        maj = BW ? gmax(EPS, q + 0.1f) : gmax(EPS, q);
+        if (!BW && s.ff.tau < 0.0f) ++tl.steps;
+        if (TR == 0) {
+            t = s.ff.sample(s.r) / maj;
+            if (md < s.d && t > md) {
+                s.x = s.x + s.dir * md;
+                s.d -= md;
+                s.ff.cross(maj, md);
+                s.ff.bk.advance(M);
+                if (c + 1 >= kCross) return false;
+                continue;
+            }
+        } else {
+            const float dt = s.ff.sample(s.r) / maj;
+            t = gmin(md, dt);
+            s.x = s.x + s.dir * t;
+            s.d -= t;
+            if (s.d <= EPS) {
+                s.T = 1.0f;
+                return true;
+            }
+            if (dt > md) {
+                s.ff.cross(maj, md);
+                s.ff.bk.advance(M);
+                if (c + 1 >= kCross) return false;
+                continue;
+            }
+        }
+        break;
+    }
+    if (TR == 0) {
+        s.ff.used();
+        const float dt = gmin(t, gmin(s.d, md));
+        s.ff.bk.move(dt);
+        s.x = s.x + s.dir * dt;
+        s.d -= dt;
+        if (s.d <= EPS) return true;
+        const float r = 1.0f - sigma(M, s.x, tl) / maj;
+        s.T *= r;
+        if (s.T < (BW ? 0.1f : 0.01f)) {
+            if (s.r.uniform() < 1.0f - s.T) {
+                s.T = 0.0f;
+                return true;
+            }
+            s.T = 1.0f;
+        }
+        hit = true;
+        hmaj = maj;
+        hf = r;
+        return false;
+    } else {
+        s.ff.used();
+        s.ff.bk.move(t);
+        const float Pc = sigma(M, s.x, tl) / maj;
+        if (s.r.uniform() < Pc) {
+            s.T = 0.0f;
+            return true;
+        }
+        hit = true;
+        hmaj = maj;
+        hf = Pc;
+        return false;
+    }
+}
+
+
+constexpr uint32_t kNone = 0xffffffffu;
+// A primal vertex of the NEE_DS adjoint wavefront: its two shadow
+// transmittances and the next vertex of the same path.
+struct VertexRec {
+    float Te, Ts;
+    uint32_t next, pad;
+};
+
+// Buffers of one round of the NEE_DS adjoint wavefront (vrt_wave_ds.cu).
+struct WaveBw {
+    ShadowJob* jobs;
+    VertexRec* recs;
+    float* info;               // per path: R (3), Rsp (3), first record, pad
+    unsigned long long* hdr;   // [0] jobs, [1] records, [2] replay queue
+    unsigned long long cap_jobs, cap_recs, cap_paths;
+    unsigned long long res_jobs, res_recs, lanes;
+    uint64_t p_begin;
+};
+
+}  // namespace wave
+
+// Shadow kernels of the NEE_DS adjoint rounds (defined in vrt_wave.cu, so they
+// are compiled with the forward's floating-point contraction): T of the
+// primal's jobs into their vertex records and paths (head: hdr[3]), and the
+// transmittance adjoints of the replay's jobs (head: hdr[4]).
+int launch_shadow_record(const DMedium& M, const PathSrc& src, const wave::WaveBw& wv, uint64_t seed, DScratch* sc,
+                         int num_sms, cudaStream_t stream);
+int launch_shadow_adjoint(const DMedium& M, const wave::WaveBw& wv, uint64_t seed, DScratch* sc, int num_sms,
+                          cudaStream_t stream);
+
+}  // namespace vrt

@@ -1,0 +1,451 @@
+// vrt_wave_ds.cu -- the NEE_DS adjoint as a wavefront (sm_100a).
+//
+// Compiled with -fmad=false: the primal walk (k_ds_primal) and the replay walk
+// (k_ds_replay) are separate kernels that must retrace the same path bit for
+// bit, so every operation is rounded on its own and no a*b+c can be
+// contracted differently in the two.  The shadow kernels of the rounds live in
+// vrt_wave.cu.
+#include "vrt_wave.cuh"
+
+namespace vrt {
+
+using namespace wave;
+
+// ------------------------------------------------------------------------
+// NEE_DS adjoint (include/vr_path_integrator_NEE_DS.h:6-206) as a wavefront.
+//
+// With the default replay majorant (the primal's) the replay retraces the
+// primal's vertices exactly -- same draws, same throughputs, and shadow j of
+// the path draws from fork j in both passes -- so a vertex's shadow
+// transmittances are computed once and stored, and the transmittance adjoints
+// (which feed nothing back into the path) run as independent jobs:
+//
+//   A k_ds_primal   the primal walk: per real collision a vertex record (linked
+//                   per path) and a T job per light; per path the emission and
+//                   escape terms of R and Rsp
+//   B (vrt_wave.cu) T of each job into its record, weight * T into its
+//                   path's R (or Rsp after a zero-density collision)
+//   C k_ds_replay   the replay walk: dL/dsigma at every collision, dL/dalbedo
+//                   at real ones, the R bookkeeping from the stored T, and a
+//                   transmittance-adjoint job per light with dL/dT != 0
+//   D (vrt_wave.cu) the ratio / delta tracking adjoint or the DDA adjoint of
+//                   each job
+//
+// Rounds bound the buffers as in the forward wavefront.
+// ------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256, 4) k_ds_primal(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
+                                                    DScratch* sc, WaveBw wv) {
+    const unsigned lane = threadIdx.x & 31u;
+    const float EPS = 0.00000001f;
+    const float eps = M.ds_eps;
+    const int lights = M.has_sun ? 2 : 1;
+    Flight ff;
+    Rng rng;
+    float3 x = f3(0.0f), w = f3(0.0f), W = f3(0.0f), Racc = f3(0.0f), Rspacc = f3(0.0f);
+    float d = 0.0f, null_W = 1.0f;
+    bool scattered = false, alive = false, exhausted = false;
+    int bounces = 0;
+    uint64_t pid = 0;
+    uint32_t steps_path = 0, first = kNone, prev = kNone;
+    uint32_t n_paths_done = 0;
+    Tally tl;
+
+    while (true) {
+        unsigned want = __ballot_sync(kAll, !alive && !exhausted);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) {
+                const unsigned long long uj = *((volatile unsigned long long*)&wv.hdr[0]);
+                const unsigned long long ur = *((volatile unsigned long long*)&wv.hdr[1]);
+                const unsigned long long up = *((volatile unsigned long long*)&sc->next_path) - wv.p_begin;
+                const bool room = uj + wv.res_jobs <= wv.cap_jobs && ur + wv.res_recs <= wv.cap_recs &&
+                                  up + wv.lanes <= wv.cap_paths;
+                base = room ? atomicAdd(&sc->next_path, (unsigned long long)__popc(want)) : ~0ull;
+            }
+            base = __shfl_sync(kAll, base, leader);
+            if (base == ~0ull) {
+                exhausted = true;
+            } else if (!alive && !exhausted) {
+                const uint64_t p = base + __popc(want & ((1u << lane) - 1u));
+                if (p >= n_paths) {
+                    exhausted = true;
+                } else {
+                    pid = p;
+                    rng.init(seed, pid, 0);
+                    float3 x0, w0;
+                    start_ray(S, pid, rng, x0, w0);
+                    float tMin, tMax;
+                    boundary(M, x0, w0, tMin, tMax);
+                    x = x0 + w0 * tMin;
+                    w = w0;
+                    d = tMax - tMin;
+                    W = f3(1.0f);
+                    Racc = f3(0.0f);
+                    Rspacc = f3(0.0f);
+                    null_W = 1.0f;
+                    scattered = false;
+                    bounces = 0;
+                    steps_path = 0;
+                    first = kNone;
+                    prev = kNone;
+                    ff = Flight();
+                    alive = true;
+                    ++n_paths_done;
+                }
+            }
+        }
+        if (__all_sync(kAll, !alive && exhausted)) break;
+
+        int nrec = 0, nj = 0;
+        bool finish = false, rsp = false;
+        float3 wnee = f3(0.0f), we = f3(0.0f), ws = f3(0.0f);
+        uint32_t jfork = 0;
+        if (alive) {
+            int ev = 0;  // 0 none, 1 collision, 2 end
+            if (!(d > EPS)) {
+                ev = 2;  // the while (d > EPS) test (_NEE_DS.h:31)
+            } else {
+                bool need = false;
+                float m = 0.0f, t = 0.0f;
+                if (ff.tau < 0.0f) ++tl.steps;
+                ff.sample(rng);
+                for (int k = 0;; ++k) {
+                    if (k >= kStepCap) {
+                        guard(sc, 2);
+                        ev = 2;
+                        break;
+                    }
+                    float md;
+                    m = gmax(EPS, ff.bk.query(M, x, w, md) + 2.0f * eps + 0.1f);  // _NEE_DS.h:36
+                    t = ff.tau / m;
+                    x = x + w * gmin(t, md);
+                    if (t > md) {
+                        d -= md;
+                        ff.cross(m, md);
+                        ff.bk.advance(M);
+                        if (!(d > EPS)) { ev = 2; break; }
+                        continue;
+                    }
+                    ff.used();
+                    if (t > d) ev = 2;
+                    else need = true;
+                    ff.bk.move(t);
+                    break;
+                }
+                if (need) {
+                    const float s = sigma(M, x, tl);
+                    const float Pc = (s + eps) / m;
+                    if (rng.uniform() >= Pc) {  // null collision (_NEE_DS.h:41-45)
+                        W = W * ((1.0f - s / m) / (1.0f - Pc));
+                        d -= t;
+                    } else {  // real collision (_NEE_DS.h:48-99)
+                        scattered = true;
+                        bool dead = false;
+                        if (s < EPS) {
+                            if (null_W < EPS) { W = f3(0.0f); dead = true; }
+                            else null_W = 0.0f;
+                        } else {
+                            W = W * ((s / m) / Pc);
+                        }
+                        if (dead) {
+                            ev = 2;
+                        } else {
+                            const float3 sa = albedo(M, x, tl);
+                            const float3 acc = W * (f3(1.0f) - sa) * M.emission;
+                            W = W * sa;
+                            const float3 Le = environment_sample(M, rng, wnee);
+                            we = W * Le * phase(M, w, wnee);
+                            if (M.has_sun) ws = W * M.sun_L * phase(M, w, M.sun_dir);
+                            jfork = rng.ntr;
+                            rng.ntr += (uint32_t)lights;
+                            const bool capped = M.max_bounces > 0 && bounces + 1 >= M.max_bounces;
+                            float3 wo = w;
+                            if (!capped) wo = phase_sample(M, rng, w);
+                            rsp = null_W < EPS;
+                            if (rsp) Rspacc = Rspacc + acc;
+                            else Racc = Racc + acc;
+                            nrec = 1;
+                            nj = lights;
+                            ++bounces;
+                            if (capped || all_less(W, EPS)) {
+                                W = f3(0.0f);
+                                ev = 2;
+                            } else {
+                                w = wo;
+                                float tMin;
+                                boundary(M, x, w, tMin, d);
+                                ff = Flight();
+                            }
+                        }
+                    }
+                }
+            }
+            if (++steps_path > (uint32_t)kPathCap) {
+                guard(sc, 3);
+                ev = 2;
+            }
+            finish = ev == 2;
+        }
+        // ---- the vertex record (linked to the path's previous one) and its T jobs
+        const unsigned long long r = reserve_slots(&wv.hdr[1], nrec);
+        if (nrec) {
+            VertexRec* rp = wv.recs + r;
+            rp->Te = 1.0f;
+            rp->Ts = 1.0f;
+            rp->next = kNone;
+            if (first == kNone) first = (uint32_t)r;
+            else wv.recs[prev].next = (uint32_t)r;
+            prev = (uint32_t)r;
+        }
+        const unsigned long long j = reserve_slots(&wv.hdr[0], nj);
+        if (nj) {
+            const uint32_t tgt = ((uint32_t)r << 2) | (rsp ? 2u : 0u);
+            put_job(wv.jobs, j, x, wnee, we, job_key(pid, jfork), tgt);
+            if (nj == 2) put_job(wv.jobs, j + 1, x, M.sun_dir, ws, job_key(pid, jfork + 1), tgt | 1u);
+        }
+        if (finish) {  // end of the primal (_NEE_DS.h:106-110): escape term, then the path's totals
+            if (!scattered) Racc = Racc + M.env * W;
+            float* io = wv.info + 8 * (pid - wv.p_begin);
+            reinterpret_cast<float4*>(io)[0] = make_float4(Racc.x, Racc.y, Racc.z, Rspacc.x);
+            reinterpret_cast<float4*>(io)[1] = make_float4(Rspacc.y, Rspacc.z, __uint_as_float(first), 0.0f);
+            alive = false;
+        }
+    }
+    flush_counters(sc, n_paths_done, 0, tl);  // the forward counts the vertices
+}
+
+__global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
+                                                    const float* __restrict__ dL, float div, DScratch* sc, WaveBw wv) {
+    const unsigned lane = threadIdx.x & 31u;
+    const float EPS = 0.00000001f;
+    const float eps = M.ds_eps;
+    const int lights = M.has_sun ? 2 : 1;
+    unsigned long long p_end = *((volatile unsigned long long*)&sc->next_path);
+    if (p_end > n_paths) p_end = n_paths;
+    const unsigned long long n_round = p_end - wv.p_begin;
+    Flight ff;
+    Rng rng;
+    float3 x = f3(0.0f), w = f3(0.0f), W = f3(0.0f), R = f3(0.0f), Rsp = f3(0.0f), dLdR = f3(0.0f);
+    float d = 0.0f;
+    bool alive = false, exhausted = false;
+    int bounces = 0;
+    uint64_t pid = 0;
+    uint32_t steps_path = 0, cur = kNone;
+    Tally tl;
+
+    while (true) {
+        unsigned want = __ballot_sync(kAll, !alive && !exhausted);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(&wv.hdr[2], (unsigned long long)__popc(want));
+            base = __shfl_sync(kAll, base, leader);
+            if (!alive && !exhausted) {
+                const unsigned long long k = base + __popc(want & ((1u << lane) - 1u));
+                if (k >= n_round) {
+                    exhausted = true;
+                } else {
+                    pid = wv.p_begin + k;
+                    rng.init(seed, pid, 0);
+                    float3 x0, w0;
+                    start_ray(S, pid, rng, x0, w0);
+                    dLdR = ld3(dL + 3 * out_index(S, pid)) / div;
+                    float tMin, tMax;
+                    boundary(M, x0, w0, tMin, tMax);
+                    x = x0 + w0 * tMin;
+                    w = w0;
+                    d = tMax - tMin;
+                    W = f3(1.0f);
+                    bounces = 0;
+                    steps_path = 0;
+                    const float4* io = reinterpret_cast<const float4*>(wv.info + 8 * k);
+                    const float4 a = io[0], b = io[1];
+                    R = make_float3(a.x, a.y, a.z);
+                    Rsp = make_float3(a.w, b.x, b.y);
+                    cur = __float_as_uint(b.z);
+                    ff = Flight();
+                    alive = true;
+                }
+            }
+        }
+        if (__all_sync(kAll, !alive && exhausted)) break;
+
+        int nj = 0;
+        float3 jd0 = f3(0.0f), jd1 = f3(0.0f);
+        float dT0 = 0.0f, dT1 = 0.0f;
+        uint32_t f0 = 0, f1 = 0;
+        if (alive) {
+            int ev = 0;
+            if (!(d > EPS)) {
+                ev = 2;
+            } else {
+                bool need = false;
+                float m = 0.0f, t = 0.0f;
+                if (ff.tau < 0.0f) ++tl.steps;
+                ff.sample(rng);
+                for (int k = 0;; ++k) {
+                    if (k >= kStepCap) {
+                        guard(sc, 4);
+                        ev = 2;
+                        break;
+                    }
+                    float md;
+                    m = gmax(EPS, ff.bk.query(M, x, w, md) + 2.0f * eps + 0.1f);
+                    t = ff.tau / m;
+                    x = x + w * gmin(t, md);
+                    if (t > md) {
+                        d -= md;
+                        ff.cross(m, md);
+                        ff.bk.advance(M);
+                        if (!(d > EPS)) { ev = 2; break; }
+                        continue;
+                    }
+                    ff.used();
+                    if (t > d) ev = 2;
+                    else need = true;
+                    ff.bk.move(t);
+                    break;
+                }
+                if (need) {
+                    const float s = sigma(M, x, tl);
+                    const float Pc = (s + eps) / m;
+                    float gsc;
+                    const bool real = !(rng.uniform() >= Pc);
+                    if (!real) {  // _NEE_DS.h:130-140
+                        gsc = dot(dLdR, -R / m / (1.0f - s / m));
+                        W = W * ((1.0f - s / m) / (1.0f - Pc));
+                        d -= t;
+                    } else {      // _NEE_DS.h:142-150
+                        gsc = dot(dLdR, s < EPS ? Rsp / eps : R / s);
+                    }
+                    if (gsc != 0.0f) sigma_bw(M, x, gsc, tl);
+                    if (real) {   // replayed vertex (_NEE_DS.h:151-203)
+                        W = W * (s / m / Pc);
+                        if (s < EPS) {
+                            ev = 2;
+                        } else {
+                            const float3 sa = albedo(M, x, tl);
+                            float3 dL_dsa = dLdR * W * -1.0f * M.emission;
+                            R = R - W * (f3(1.0f) - sa) * M.emission;
+                            dL_dsa = dL_dsa + dLdR * R / make_float3(gmax(EPS, sa.x), gmax(EPS, sa.y), gmax(EPS, sa.z));
+                            albedo_bw(M, x, dL_dsa, tl);
+                            float3 wnee;
+                            const float3 Le = environment_sample(M, rng, wnee);
+                            const float ph_nee = phase(M, w, wnee);
+                            const float ph_sun = M.has_sun ? phase(M, w, M.sun_dir) : 0.0f;
+                            const uint32_t jf = rng.ntr;
+                            rng.ntr += (uint32_t)lights;
+                            const float3 wo = phase_sample(M, rng, w);
+                            W = W * sa;
+                            float Te = 1.0f, Ts = 1.0f;
+                            if (cur == kNone) {
+                                guard(sc, 5);  // the replay left the primal's path
+                                ev = 2;
+                            } else {
+                                const VertexRec rec = wv.recs[cur];
+                                Te = rec.Te;
+                                Ts = rec.Ts;
+                                cur = rec.next;
+                            }
+                            if (ev != 2) {
+                                const float dTe = dot(dLdR, W * Le * ph_nee);
+                                R = R - W * Te * Le * ph_nee;
+                                if (dTe != 0.0f) { jd0 = wnee; dT0 = dTe; f0 = jf; nj = 1; }
+                                if (M.has_sun) {
+                                    const float dTs = dot(dLdR, W * M.sun_L * ph_sun);
+                                    R = R - W * Ts * M.sun_L * ph_sun;
+                                    if (dTs != 0.0f) {
+                                        if (nj == 0) { jd0 = M.sun_dir; dT0 = dTs; f0 = jf + 1; nj = 1; }
+                                        else { jd1 = M.sun_dir; dT1 = dTs; f1 = jf + 1; nj = 2; }
+                                    }
+                                }
+                                ++bounces;
+                                if ((M.max_bounces > 0 && bounces >= M.max_bounces) || all_less(W, EPS)) {
+                                    ev = 2;
+                                } else {
+                                    w = wo;
+                                    float tMin;
+                                    boundary(M, x, w, tMin, d);
+                                    ff = Flight();
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            if (++steps_path > (uint32_t)kPathCap) {
+                guard(sc, 6);
+                ev = 2;
+            }
+            if (ev == 2) alive = false;
+        }
+        const unsigned long long j = reserve_slots(&wv.hdr[0], nj);
+        if (nj) {
+            if (j + (unsigned long long)nj > wv.cap_jobs) {
+                guard(sc, 7);
+            } else {
+                put_job(wv.jobs, j, x, jd0, make_float3(dT0, 0.0f, 0.0f), job_key(pid, f0));
+                if (nj == 2) put_job(wv.jobs, j + 1, x, jd1, make_float3(dT1, 0.0f, 0.0f), job_key(pid, f1));
+            }
+        }
+    }
+    flush_counters(sc, 0, 0, tl);
+}
+
+int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed,
+                      const float* dL, float div, cudaStream_t stream) {
+    if (n_paths == 0) return 0;
+    if (M.max_bounces <= 0 || M.ds_compat) return VRT_E_UNSUPPORTED;
+    const unsigned long long lights = M.has_sun ? 2ull : 1ull, B = (unsigned long long)M.max_bounces;
+    int blocksA = persistent_blocks((const void*)k_ds_primal, 256, ctx->num_sms);
+    int blocksC = persistent_blocks((const void*)k_ds_replay, 256, ctx->num_sms);
+    const uint64_t need = (n_paths + 255) / 256;
+    if ((uint64_t)blocksA > need) blocksA = (int)need;
+    if ((uint64_t)blocksC > need) blocksC = (int)need;
+    WaveBw wv;
+    wv.lanes = (unsigned long long)blocksA * 256ull;
+    const unsigned long long inflight = wv.lanes < n_paths ? wv.lanes : n_paths;
+    wv.res_jobs = inflight * lights * B;
+    wv.res_recs = inflight * B;
+    wv.cap_jobs = wv.res_jobs + batch_jobs(n_paths, lights);
+    wv.cap_recs = wv.res_recs + batch_jobs(n_paths, 1);
+    if (wv.cap_recs > (1ull << 30)) return VRT_E_UNSUPPORTED;  // record indices are 30-bit in a job
+    wv.cap_paths = (n_paths < (1ull << 24) ? n_paths : (1ull << 24)) + wv.lanes;
+    const size_t bytes = 256 + wv.cap_jobs * sizeof(ShadowJob) + wv.cap_recs * sizeof(VertexRec) + wv.cap_paths * 32;
+    int st = ensure_wave_buffer(ctx, bytes);
+    if (st) return st;
+    char* base = static_cast<char*>(ctx->wave);
+    wv.hdr = reinterpret_cast<unsigned long long*>(base);
+    wv.jobs = reinterpret_cast<ShadowJob*>(base + 256);
+    wv.recs = reinterpret_cast<VertexRec*>(base + 256 + wv.cap_jobs * sizeof(ShadowJob));
+    wv.info = reinterpret_cast<float*>(base + 256 + wv.cap_jobs * sizeof(ShadowJob) + wv.cap_recs * sizeof(VertexRec));
+    wv.p_begin = 0;
+    cudaError_t e = cudaMemsetAsync(&ctx->scratch->next_path, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return launch_status(e);
+    for (int round = 0;; ++round) {
+        // [0] jobs, [1] records, [2] replay queue, [3] / [4] heads of the shadow kernels
+        if ((e = cudaMemsetAsync(wv.hdr, 0, 5 * sizeof(unsigned long long), stream)) != cudaSuccess)
+            return launch_status(e);
+        k_ds_primal<<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
+        if ((st = launch_shadow_record(M, src, wv, seed, ctx->scratch, ctx->num_sms, stream))) return st;
+        if ((e = cudaMemsetAsync(wv.hdr, 0, sizeof(unsigned long long), stream)) != cudaSuccess)
+            return launch_status(e);
+        k_ds_replay<<<blocksC, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, ctx->scratch, wv);
+        if ((st = launch_shadow_adjoint(M, wv, seed, ctx->scratch, ctx->num_sms, stream))) return st;
+        count_launches(2);
+        if ((st = launch_status(cudaGetLastError()))) return st;
+        unsigned long long taken = 0;
+        if ((e = cudaMemcpyAsync(&taken, &ctx->scratch->next_path, sizeof(taken), cudaMemcpyDeviceToHost, stream)) !=
+            cudaSuccess)
+            return launch_status(e);
+        if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return launch_status(e);
+        if (taken >= n_paths) break;
+        wv.p_begin = taken;
+        if (round > (1 << 20)) return VRT_E_ITER_CAP;
+    }
+    return 0;
+}
+
+}  // namespace vrt
