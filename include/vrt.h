@@ -47,8 +47,17 @@ enum {
 };
 /* Path-integrator forward passes. */
 enum { VRT_PI_NEE = 0, VRT_PI_DT = 1 };
-/* Path-replay adjoints. */
-enum { VRT_BW_NEE_DS = 0, VRT_BW_DT = 1, VRT_BW_NEE_DRT = 2 };
+/* Path-replay adjoints (DeltatrackingNEEPathIntegrator, DeltatrackingPathIntegrator,
+   DRTPathIntegrator, DRTQPathIntegrator, DRTDSPathIntegrator, SPSPathIntegrator;
+   include/vr_path_integrator_NEE_DS.h, _DT.h, _NEE_DRT.h, _NEE_DRTQ.h, _NEE_DRTDS.h, _NEE_SPS.h). */
+enum {
+    VRT_BW_NEE_DS = 0,
+    VRT_BW_DT = 1,
+    VRT_BW_NEE_DRT = 2,
+    VRT_BW_NEE_DRTQ = 3,
+    VRT_BW_NEE_DRTDS = 4,
+    VRT_BW_NEE_SPS = 5
+};
 
 /* A node-centred FP32 grid, the Grid3D parameter (rendervous _maps.py:2319-2365).
    Element (z,y,x,c) is data[z*strides[0] + y*strides[1] + x*strides[2] + c]; with

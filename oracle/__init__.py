@@ -58,7 +58,7 @@ def ptr(ffi, arr: np.ndarray | None, ctype: str = "float *"):
 
 
 TRANSMITTANCE_MODES = {"rt": 0, "dt": 1, "dda": 2, "dda_midpoint": 2, "dda_exact": 3}
-BW_MODES = {"ds": 0, "dt": 1, "drt": 2}
+BW_MODES = {"ds": 0, "dt": 1, "drt": 2, "drtq": 3, "drtds": 4, "sps": 5}
 INTEGRATORS = {"nee": 0, "dt": 1}
 
 

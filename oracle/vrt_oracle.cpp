@@ -1275,6 +1275,448 @@ template <typename T> void path_integrator_NEE_DRT_bw(const Scene<T>& S, Rng& rn
     S.sigma_bw(xs, dL_dsc);
 }
 
+// include/vr_path_integrator_NEE_DRTQ.h:45-55 in_scattering, plus the
+// directional light after the environment (as every NEE here).
+template <typename T> V3<T> in_scattering(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w) {
+    const V3<T> sun_dir = V3<T>::load(S.s.sun_dir), sun_L = V3<T>::load(S.s.sun_radiance);
+    V3<T> ls_dir;
+    V3<T> Ls_env = environment_sampler(S, rng, ls_dir);
+    V3<T> Ls = transmittance(S, rng, x, ls_dir, nullptr) * Ls_env * phase(S, w, ls_dir);
+    if (S.s.has_sun) Ls += transmittance(S, rng, x, sun_dir, nullptr) * sun_L * phase(S, w, sun_dir);
+    V3<T> ws;
+    T rho_s = phase_sampler(S, rng, w, ws);
+    Counters dummy;
+    Ls += rho_s * path_integrator_NEE(S, rng, x, ws, true, dummy);
+    return S.albedo(x) * Ls;
+}
+
+// Shared by the DRT family: the scatter-gradient term at a transmittance-
+// sampled position of the segment (x, w, d) on the branch stream
+// (vr_path_integrator_NEE_DRTQ.h:156-165 and :249-259).
+template <typename T>
+void drtq_scatter_term(const Scene<T>& S, Rng& sec, V3<T> x, V3<T> w, T d, V3<T> W, V3<T> dL_dR) {
+    T s_t, weight_t;
+    sample_transmittance_position(S, sec, x, w, d, s_t, weight_t);
+    V3<T> xs = x + w * s_t;
+    V3<T> Ls = in_scattering(S, sec, xs, w);
+    T sigma_t = S.sigma(xs);
+    T mis_T = T(1) / (T(1) + sigma_t * sigma_t);
+    S.sigma_bw(xs, mis_T * weight_t * dot(dL_dR, W * Ls));
+}
+
+// include/vr_path_integrator_NEE_DRTQ.h:58-260 path_integrator_NEE_DRTQ_bw:
+// the DRT primal without a reservoir, and a scatter-gradient term on every
+// segment of the replay.  Branch seed = Philox stream 1.
+template <typename T> void path_integrator_NEE_DRTQ_bw(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, V3<T> dL_dR) {
+    T tMin, tMax;
+    S.boundary(x, w, tMin, tMax);
+    x += w * tMin;
+    T d = tMax - tMin;
+    if (d <= T(0)) return;
+    Rng sec = rng;
+    sec.stream = rng.stream + 1;
+    sec.n = 0;
+    sec.ntr = 0;
+    (void)transmittance(S, rng, x, w, nullptr);
+    transmittance_bw(S, sec, x, w, dot(dL_dR, S.environment()));
+    V3<T> R(T(0)), W(T(1));
+    const V3<T> ini_x = x, ini_w = w;
+    const T ini_d = d;
+    const T EPS = T(0.00000001);
+    const V3<T> sun_dir = V3<T>::load(S.s.sun_dir), sun_L = V3<T>::load(S.s.sun_radiance);
+    Rng before_path = rng;
+    int bounces = 0;
+    for (Flight<T> ff; d > EPS;) {
+        T md;
+        T m = ff.bk.query(S.s, x, w, md) * T(1.05) + T(0.1);
+        T t = ff.sample(rng) / m;
+        x += w * vmin(t, md);
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(S.s); continue; }
+        ff.used();
+        if (t > d) break;
+        ff.bk.move(t);
+        T s = S.sigma(x);
+        if ((T)rng.uniform() >= s / m) { d -= t; continue; }
+        W *= S.albedo(x);
+        V3<T> wnee;
+        V3<T> env = environment_sampler(S, rng, wnee);
+        T T_nee = transmittance(S, rng, x, wnee, nullptr);
+        R += W * T_nee * env * phase(S, w, wnee);
+        if (S.s.has_sun) R += W * transmittance(S, rng, x, sun_dir, nullptr) * sun_L * phase(S, w, sun_dir);
+        bool capped = S.s.max_bounces > 0 && ++bounces >= S.s.max_bounces;
+        V3<T> wo;
+        W *= phase_sampler(S, rng, w, wo);
+        w = wo;
+        S.boundary(x, w, tMin, d);
+        ff.bk.reset();
+        if (all_less(W, EPS) || capped) break;
+    }
+    W = V3<T>(T(1));
+    x = ini_x;
+    w = ini_w;
+    d = ini_d;
+    rng = before_path;
+    bounces = 0;
+    drtq_scatter_term(S, sec, x, w, d, W, dL_dR);
+    for (Flight<T> ff; d > EPS;) {
+        T md;
+        T m = ff.bk.query(S.s, x, w, md) * T(1.05) + T(0.1);
+        T t = ff.sample(rng) / m;
+        x += w * vmin(t, md);
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(S.s); continue; }
+        ff.used();
+        if (t > d) break;
+        ff.bk.move(t);
+        T s = S.sigma(x);
+        T Pc = s / m;
+        if ((T)rng.uniform() >= Pc) {
+            S.sigma_bw(x, dot(dL_dR, -R / m / (T(1) - s / m)));
+            d -= t;
+            continue;
+        }
+        T dL_dsigma = dot(dL_dR, s * s / (T(1) + s * s) * R / s);
+        W *= S.albedo(x);
+        V3<T> wnee;
+        V3<T> env = environment_sampler(S, rng, wnee);
+        T T_nee = transmittance(S, rng, x, wnee, nullptr);
+        T ph_nee = phase(S, w, wnee);
+        T T_sun = 0, ph_sun = 0;
+        if (S.s.has_sun) {
+            T_sun = transmittance(S, rng, x, sun_dir, nullptr);
+            ph_sun = phase(S, w, sun_dir);
+        }
+        bool capped = S.s.max_bounces > 0 && ++bounces >= S.s.max_bounces;
+        V3<T> wo;
+        T rho = phase_sampler(S, rng, w, wo);
+        T dL_dTnee = dot(dL_dR, W * env * ph_nee);
+        R -= W * T_nee * env * ph_nee;
+        T dL_dTsun = 0;
+        if (S.s.has_sun) {
+            dL_dTsun = dot(dL_dR, W * sun_L * ph_sun);
+            R -= W * T_sun * sun_L * ph_sun;
+        }
+        S.sigma_bw(x, dL_dsigma);
+        transmittance_bw(S, sec, x, wnee, dL_dTnee);
+        if (S.s.has_sun) transmittance_bw(S, sec, x, sun_dir, dL_dTsun);
+        W *= rho;
+        w = wo;
+        S.boundary(x, w, tMin, d);
+        ff.bk.reset();
+        if (all_less(W, EPS) || capped) break;
+        drtq_scatter_term(S, sec, x, w, d, W, dL_dR);
+    }
+}
+
+// include/vr_path_integrator_NEE_DRTDS.h:8-38 sample_collision_position_ds
+// (majorant queried at the sample point, as in sample_transmittance_position).
+template <typename T>
+void sample_collision_position_ds(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, T d, T epsilon, T& t, T& weight_t) {
+    const T EPS = T(0.0000001);
+    t = 0;
+    weight_t = 1;
+    for (int it = 0; it < (1 << 24); ++it) {
+        T md;
+        T m = vmax(EPS, S.majorant(x + w * t, w, md) + T(2) * epsilon + T(0.1));
+        T dt = vmin(-std::log(T(1) - (T)rng.uniform()) / m, vmin(md, d - t));
+        t += dt;
+        if (dt >= md - EPS) continue;
+        if (t >= d - EPS) break;
+        T s = S.sigma(x + w * t);
+        T Pc = (s + epsilon) / m;
+        if ((T)rng.uniform() < Pc) {
+            weight_t *= T(1) / (s + epsilon);
+            return;
+        }
+        weight_t *= (T(1) - s / m) / (T(1) - Pc);
+    }
+    weight_t = 0;
+}
+
+// include/vr_path_integrator_NEE_DRTDS.h:40-253 path_integrator_NEE_DRTDS_bw:
+// the DRT primal and reservoir; the replay scatters no MIS term at real
+// collisions, and the reservoir term samples a defensive collision position.
+template <typename T>
+void path_integrator_NEE_DRTDS_bw(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, T epsilon, V3<T> dL_dR) {
+    T tMin, tMax;
+    S.boundary(x, w, tMin, tMax);
+    x += w * tMin;
+    T d = tMax - tMin;
+    if (d <= T(0)) return;
+    Rng sec = rng;
+    sec.stream = rng.stream + 1;
+    sec.n = 0;
+    sec.ntr = 0;
+    (void)transmittance(S, rng, x, w, nullptr);
+    transmittance_bw(S, sec, x, w, dot(dL_dR, S.environment()));
+    V3<T> R(T(0)), W(T(1));
+    V3<T> res_x = x, res_w = w, res_W = W;
+    T res_P = 3, total_weight = 3;
+    const V3<T> ini_x = x, ini_w = w;
+    const T ini_d = d;
+    const T EPS = T(0.00000001);
+    const V3<T> sun_dir = V3<T>::load(S.s.sun_dir), sun_L = V3<T>::load(S.s.sun_radiance);
+    Rng before_path = rng;
+    int bounces = 0;
+    for (Flight<T> ff; d > EPS;) {
+        T md;
+        T m = ff.bk.query(S.s, x, w, md) * T(1.05) + T(0.1);
+        T t = ff.sample(rng) / m;
+        x += w * vmin(t, md);
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(S.s); continue; }
+        ff.used();
+        if (t > d) break;
+        ff.bk.move(t);
+        T s = S.sigma(x);
+        if ((T)rng.uniform() >= s / m) { d -= t; continue; }
+        W *= S.albedo(x);
+        V3<T> wnee;
+        V3<T> env = environment_sampler(S, rng, wnee);
+        T T_nee = transmittance(S, rng, x, wnee, nullptr);
+        R += W * T_nee * env * phase(S, w, wnee);
+        if (S.s.has_sun) R += W * transmittance(S, rng, x, sun_dir, nullptr) * sun_L * phase(S, w, sun_dir);
+        bool capped = S.s.max_bounces > 0 && ++bounces >= S.s.max_bounces;
+        V3<T> wo;
+        W *= phase_sampler(S, rng, w, wo);
+        w = wo;
+        S.boundary(x, w, tMin, d);
+        ff.bk.reset();
+        T current_P = W.x + W.y + W.z;
+        total_weight += current_P;
+        if ((T)rng.uniform() < current_P / total_weight) {
+            res_P = current_P; res_W = W; res_x = x; res_w = w;
+        }
+        if (all_less(W, EPS) || capped) break;
+    }
+    W = V3<T>(T(1));
+    x = ini_x;
+    w = ini_w;
+    d = ini_d;
+    rng = before_path;
+    bounces = 0;
+    for (Flight<T> ff; d > EPS;) {
+        T md;
+        T m = ff.bk.query(S.s, x, w, md) * T(1.05) + T(0.1);
+        T t = ff.sample(rng) / m;
+        x += w * vmin(t, md);
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(S.s); continue; }
+        ff.used();
+        if (t > d) break;
+        ff.bk.move(t);
+        T s = S.sigma(x);
+        if ((T)rng.uniform() >= s / m) {
+            S.sigma_bw(x, dot(dL_dR, -R / m / (T(1) - s / m)));
+            d -= t;
+            continue;
+        }
+        V3<T> sa = S.albedo(x);
+        V3<T> wnee;
+        V3<T> env = environment_sampler(S, rng, wnee);
+        T T_nee = transmittance(S, rng, x, wnee, nullptr);
+        T ph_nee = phase(S, w, wnee);
+        T T_sun = 0, ph_sun = 0;
+        if (S.s.has_sun) {
+            T_sun = transmittance(S, rng, x, sun_dir, nullptr);
+            ph_sun = phase(S, w, sun_dir);
+        }
+        bool capped = S.s.max_bounces > 0 && ++bounces >= S.s.max_bounces;
+        V3<T> wo;
+        T rho = phase_sampler(S, rng, w, wo);
+        W *= sa;
+        T dL_dTnee = dot(dL_dR, W * env * ph_nee);
+        R -= W * T_nee * env * ph_nee;
+        T dL_dTsun = 0;
+        if (S.s.has_sun) {
+            dL_dTsun = dot(dL_dR, W * sun_L * ph_sun);
+            R -= W * T_sun * sun_L * ph_sun;
+        }
+        transmittance_bw(S, sec, x, wnee, dL_dTnee);
+        if (S.s.has_sun) transmittance_bw(S, sec, x, sun_dir, dL_dTsun);
+        W *= rho;
+        w = wo;
+        S.boundary(x, w, tMin, d);
+        ff.bk.reset();
+        rng.advance();
+        if (all_less(W, EPS) || capped) break;
+    }
+    S.boundary(res_x, res_w, tMin, d);
+    T s_t, weight_t;
+    sample_collision_position_ds(S, rng, res_x, res_w, d, epsilon, s_t, weight_t);
+    if (weight_t > T(0)) {
+        V3<T> xs = res_x + res_w * s_t;
+        V3<T> ls_dir;
+        V3<T> Ls_env = environment_sampler(S, rng, ls_dir);
+        V3<T> Ls = transmittance(S, rng, xs, ls_dir, nullptr) * Ls_env * phase(S, res_w, ls_dir);
+        if (S.s.has_sun) Ls += transmittance(S, rng, xs, sun_dir, nullptr) * sun_L * phase(S, res_w, sun_dir);
+        V3<T> ws;
+        T rho_s = phase_sampler(S, rng, res_w, ws);
+        Counters dummy;
+        Ls += rho_s * path_integrator_NEE(S, rng, xs, ws, true, dummy);
+        Ls *= res_W * weight_t * S.albedo(xs);
+        S.sigma_bw(xs, dot(dL_dR, Ls) * total_weight / res_P);
+    }
+}
+
+// include/vr_path_integrator_NEE_SPS.h:1-59 sample_collision_position: delta
+// tracking to a collision (majorant + 1e-6, queried at the current sample
+// point: the reference queries it at the not yet written output point, which
+// its constant majorant ignores), then, while MIS is allowed, a choice with
+// MIS (beta 3) between that collision and a uniform point of the segment up to
+// it; picking the uniform point makes it the path's singular vertex.
+template <typename T>
+bool sample_collision_position(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, T d, V3<T>& xc, T& weight_xc,
+                               T& sigma_xc, int& samples, bool& mis_allowed) {
+    T t = 0;
+    weight_xc = 0;
+    sigma_xc = 0;
+    samples = 0;
+    xc = x;
+    for (int it = 0; it < (1 << 24); ++it) {
+        T md;
+        T m = S.majorant(xc, w, md) + T(0.000001);
+        T dt = vmin(-std::log(T(1) - (T)rng.uniform()) / m, vmin(md, d - t));
+        t += dt;
+        xc = w * t + x;
+        if (dt >= md - T(0.0000001)) continue;
+        if (t >= d - T(0.0000001)) break;
+        T s = S.sigma(xc);
+        samples++;
+        if ((T)rng.uniform() < s / m) {
+            weight_xc = 1;
+            sigma_xc = s;
+            break;
+        }
+    }
+    if (!mis_allowed) return false;
+    T powered_c = sigma_xc * sigma_xc * sigma_xc;  // pow(sigma, MIS_BETA) with MIS_BETA = 3
+    T mis_wc = weight_xc * powered_c / (T(1) + powered_c);
+    T u = (T)rng.uniform();
+    V3<T> xf = xc * (T(1) - u) + x * u;
+    T sigma_f = S.sigma(xf);
+    T powered_f = sigma_f * sigma_f * sigma_f;
+    T mis_wf = t / (T(1) + powered_f);
+    weight_xc = mis_wc + mis_wf;
+    if ((T)rng.uniform() * weight_xc < mis_wf) {
+        xc = xf;
+        sigma_xc = sigma_f;
+        mis_allowed = false;
+        return true;
+    }
+    return false;
+}
+
+// include/vr_path_integrator_NEE_SPS.h:88-101 st_tau_bw (stratified bins)
+template <typename T> void st_tau_bw(const Scene<T>& S, Rng& rng, V3<T> a, V3<T> b, int bins, T dL_dtau) {
+    if (dL_dtau == T(0) || bins == 0) return;
+    T d = std::sqrt(dot(a - b, a - b));
+    T g = dL_dtau * d / T(bins);
+    for (int i = 0; i < bins; ++i) {
+        T f = (T(i) + (T)rng.uniform()) / T(bins);
+        S.sigma_bw(b * (T(1) - f) + a * f, g);
+    }
+}
+
+// include/vr_path_integrator_NEE_SPS.h:104-263 path_integrator_NEE_SPS_bw
+// (emission ignored, as in the reference; directional light and bounce cap as
+// in the other adjoints).
+template <typename T> void path_integrator_NEE_SPS_bw(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, V3<T> dL_dR) {
+    T tMin, tMax;
+    S.boundary(x, w, tMin, tMax);
+    x += w * tMin;
+    T d = tMax - tMin;
+    if (d <= T(0)) return;
+    Rng sec = rng;
+    sec.stream = rng.stream + 1;
+    sec.n = 0;
+    sec.ntr = 0;
+    (void)transmittance(S, rng, x, w, nullptr);
+    transmittance_bw(S, sec, x, w, dot(dL_dR, S.environment()));
+    const V3<T> sun_dir = V3<T>::load(S.s.sun_dir), sun_L = V3<T>::load(S.s.sun_radiance);
+    V3<T> R(T(0)), Rf(T(0)), W(T(1));
+    T W_singular = 1;
+    bool mis_allowed = true;
+    const V3<T> ini_x = x, ini_w = w;
+    const T ini_d = d;
+    const T EPS = T(0.00001);
+    Rng before_path = rng;
+    int bounces = 0;
+    for (int it = 0; it < (1 << 24); ++it) {
+        T weight_xc, sigma_xc;
+        V3<T> xc;
+        int samples;
+        if (sample_collision_position(S, rng, x, w, d, xc, weight_xc, sigma_xc, samples, mis_allowed))
+            W_singular = sigma_xc;
+        if (weight_xc == T(0)) break;
+        x = xc;
+        W *= weight_xc * S.albedo(x);
+        V3<T> wnee;
+        V3<T> nee_env = environment_sampler(S, rng, wnee);
+        T nee_T = transmittance(S, rng, x, wnee, nullptr);
+        V3<T> added_R = W * nee_T * phase(S, w, wnee) * nee_env;
+        if (S.s.has_sun) added_R += W * transmittance(S, rng, x, sun_dir, nullptr) * phase(S, w, sun_dir) * sun_L;
+        if (mis_allowed) R += added_R;
+        else Rf += added_R;
+        bool capped = S.s.max_bounces > 0 && ++bounces >= S.s.max_bounces;
+        V3<T> wo;
+        W *= phase_sampler(S, rng, w, wo);
+        w = wo;
+        S.boundary(x, w, tMin, d);
+        if (all_less(W, EPS) || capped) break;
+    }
+    W = V3<T>(T(1));
+    mis_allowed = true;
+    x = ini_x;
+    w = ini_w;
+    d = ini_d;
+    V3<T> prev_x = x;
+    rng = before_path;
+    bounces = 0;
+    for (int it = 0; it < (1 << 24); ++it) {
+        T weight_xc, sigma_xc;
+        V3<T> xc;
+        int samples;
+        bool singular = sample_collision_position(S, rng, x, w, d, xc, weight_xc, sigma_xc, samples, mis_allowed);
+        if (weight_xc == T(0)) break;
+        V3<T> further_R = R + W_singular * Rf;
+        T k = dot(dL_dR, further_R);
+        T dL_dtau = -k;
+        T dL_dsigma = singular ? dot(dL_dR, Rf) : k / vmax(T(0.001), sigma_xc);
+        x = xc;
+        W *= weight_xc;
+        W *= S.albedo(x);
+        V3<T> wnee;
+        V3<T> env = environment_sampler(S, rng, wnee);
+        T T_nee = transmittance(S, rng, x, wnee, nullptr);
+        T ph_nee = phase(S, w, wnee);
+        T T_sun = 0, ph_sun = 0;
+        if (S.s.has_sun) {
+            T_sun = transmittance(S, rng, x, sun_dir, nullptr);
+            ph_sun = phase(S, w, sun_dir);
+        }
+        bool capped = S.s.max_bounces > 0 && ++bounces >= S.s.max_bounces;
+        V3<T> wo;
+        T rho = phase_sampler(S, rng, w, wo);
+        const T fs = mis_allowed ? T(1) : W_singular;
+        T dL_dTnee = dot(dL_dR, W * fs * env * ph_nee);
+        V3<T> added_R = W * T_nee * ph_nee * env;
+        T dL_dTsun = 0;
+        if (S.s.has_sun) {
+            dL_dTsun = dot(dL_dR, W * fs * sun_L * ph_sun);
+            added_R += W * T_sun * ph_sun * sun_L;
+        }
+        if (mis_allowed) R -= added_R;
+        else Rf -= added_R;
+        S.sigma_bw(x, dL_dsigma);
+        st_tau_bw(S, sec, x, prev_x, samples > 1 ? samples : 1, dL_dtau);
+        transmittance_bw(S, sec, x, wnee, dL_dTnee);
+        if (S.s.has_sun) transmittance_bw(S, sec, x, sun_dir, dL_dTsun);
+        W *= rho;
+        w = wo;
+        S.boundary(x, w, tMin, d);
+        if (all_less(W, EPS) || capped) break;
+        prev_x = x;
+    }
+}
+
 // include/maps/sensor_perspective_camera.h:1-27
 template <typename T>
 void camera_ray(const orc_camera& cam, int view, int row, int col, Rng& rng, V3<T>& x, V3<T>& w) {
@@ -1305,7 +1747,10 @@ template <typename T> V3<T> radiance(const Scene<T>& S, int integrator, Rng& rng
 template <typename T> void radiance_bw(const Scene<T>& S, int bw_mode, Rng& rng, V3<T> x, V3<T> w, V3<T> dL) {
     if (bw_mode == 0) path_integrator_NEE_DS_bw(S, rng, x, w, (T)S.s.ds_epsilon, dL);
     else if (bw_mode == 1) path_integrator_DT_bw(S, rng, x, w, (T)S.s.ds_epsilon, dL);
-    else path_integrator_NEE_DRT_bw(S, rng, x, w, dL);
+    else if (bw_mode == 2) path_integrator_NEE_DRT_bw(S, rng, x, w, dL);
+    else if (bw_mode == 3) path_integrator_NEE_DRTQ_bw(S, rng, x, w, dL);
+    else if (bw_mode == 4) path_integrator_NEE_DRTDS_bw(S, rng, x, w, (T)S.s.ds_epsilon, dL);
+    else path_integrator_NEE_SPS_bw(S, rng, x, w, dL);
 }
 
 template <typename T> void transmittance_fw_impl(const orc_scene* s, int32_t mode, const float* rays, int64_t n, uint64_t seed, float* Tout) {

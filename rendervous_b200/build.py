@@ -58,10 +58,14 @@ def up_to_date() -> bool:
         return f.read().strip() == _digest()
 
 
-# Files whose kernels must round every operation on its own: the wavefront
-# primal and replay walks are separate kernels that have to retrace the same
-# path bit for bit, so no a*b+c may be contracted differently in the two.
-PER_FILE_FLAGS = {"vrt_wave_ds.cu": ["-fmad=false"]}
+# Files whose kernels round every operation on its own (no a*b+c contracted
+# into an FMA).  vrt_wave_ds.cu: the NEE_DS primal and replay walks are
+# separate kernels that must retrace the same path bit for bit.  vrt_path.cu:
+# the position samplers of the DRT / DRTQ / SPS adjoints draw once per
+# majorant-brick crossing, so a face distance one ulp off changes how many
+# draws a sample takes; rounding as the CPU restatement does keeps them on the
+# same paths.
+PER_FILE_FLAGS = {"vrt_wave_ds.cu": ["-fmad=false"], "vrt_path.cu": ["-fmad=false"]}
 OBJ_DIR = os.path.join(HERE, "_build")
 
 

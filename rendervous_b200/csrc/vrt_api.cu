@@ -410,7 +410,7 @@ int vrt_radiance_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, cons
                     uint64_t seed, const float* dL_dR, void* stream) {
     int st = check_ctx(ctx);
     if (st) return st;
-    if (bw_mode < 0 || bw_mode > 2) return VRT_E_INVALID_ARGUMENT;
+    if (bw_mode < 0 || bw_mode > VRT_BW_NEE_SPS) return VRT_E_INVALID_ARGUMENT;
     if (n < 0) return VRT_E_BAD_SHAPE;
     DMedium M;
     if ((st = to_dmedium(m, M))) return st;
@@ -452,7 +452,7 @@ int vrt_capture_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const
                    uint64_t seed, const float* dL_drgb, void* stream) {
     int st = check_ctx(ctx);
     if (st) return st;
-    if (bw_mode < 0 || bw_mode > 2) return VRT_E_INVALID_ARGUMENT;
+    if (bw_mode < 0 || bw_mode > VRT_BW_NEE_SPS) return VRT_E_INVALID_ARGUMENT;
     if (spp < 1) return VRT_E_INVALID_ARGUMENT;
     DMedium M;
     if ((st = to_dmedium(m, M))) return st;

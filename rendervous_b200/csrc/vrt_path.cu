@@ -681,6 +681,14 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
     }
 }
 
+// x + w t with the product and the sum each rounded (no contraction into an
+// FMA): sample points of the position samplers land exactly on majorant-brick
+// faces, where the brick chosen depends on the last bit.
+__device__ __forceinline__ float3 ray_at(float3 x, float3 w, float t) {
+    return make_float3(__fadd_rn(x.x, __fmul_rn(w.x, t)), __fadd_rn(x.y, __fmul_rn(w.y, t)),
+                       __fadd_rn(x.z, __fmul_rn(w.z, t)));
+}
+
 // vr_path_integrator_NEE_DRT.h:8-60 sample_transmittance_position (majorant
 // queried at the sample point x + w t)
 __device__ float sample_transmittance_position(const DMedium& M, Rng& rng, float3 x, float3 w, float d, float& sample_t,
@@ -690,7 +698,7 @@ __device__ float sample_transmittance_position(const DMedium& M, Rng& rng, float
     int it = 0;
     for (; it < kStepCap; ++it) {
         float md;
-        float m = gmax(EPS, majorant(M, x + w * t, w, md));
+        float m = gmax(EPS, majorant(M, ray_at(x, w, t), w, md));
         float dt = gmin(-logf(1.0f - rng.uniform()) / m, gmin(md, d - t));
         float w_step = Tr * dt;
         C += w_step;
@@ -698,7 +706,7 @@ __device__ float sample_transmittance_position(const DMedium& M, Rng& rng, float
         t += dt;
         if (dt >= md - EPS) continue;
         if (t >= d - EPS) break;
-        Tr *= 1.0f - sigma(M, x + w * t, tl) / m;
+        Tr *= 1.0f - sigma(M, ray_at(x, w, t), tl) / m;
     }
     if (it == kStepCap) raise_status(status, 4);
     weight_t = C;
@@ -834,6 +842,425 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
     sigma_bw(M, xs, dot(dL_dR, Ls) * mis_T * total_weight / res_P, tl);
 }
 
+__device__ __forceinline__ Rng branch_stream(const Rng& rng) {
+    Rng sec;
+    sec.k0 = rng.k0; sec.k1 = rng.k1; sec.plo = rng.plo; sec.phi = rng.phi;
+    sec.stream = rng.stream + 1;
+    sec.n = 0;
+    sec.ntr = 0;
+    return sec;
+}
+
+// vr_path_integrator_NEE_DRTQ.h:45-55 in_scattering (+ directional light)
+__device__ float3 in_scattering(const DMedium& M, Rng& rng, float3 x, float3 w, Tally& tl, uint32_t* status) {
+    float3 ls_dir;
+    float3 Ls_env = environment_sample(M, rng, ls_dir);
+    float3 Ls = transmittance(M, rng, x, ls_dir, tl, status) * Ls_env * phase(M, w, ls_dir);
+    if (M.has_sun) Ls = Ls + transmittance(M, rng, x, M.sun_dir, tl, status) * M.sun_L * phase(M, w, M.sun_dir);
+    float3 ws = phase_sample(M, rng, w);
+    uint32_t verts = 0;
+    Ls = Ls + 1.0f * path_nee_seq(M, rng, x, ws, true, verts, tl, status);
+    return albedo(M, x, tl) * Ls;
+}
+
+// scatter-gradient term of a segment on the branch stream (_DRTQ.h:156-165, :249-259)
+__device__ void drtq_scatter_term(const DMedium& M, Rng& sec, float3 x, float3 w, float d, float3 W, float3 dL_dR,
+                                  Tally& tl, uint32_t* status) {
+    float s_t, weight_t;
+    sample_transmittance_position(M, sec, x, w, d, s_t, weight_t, tl, status);
+    float3 xs = x + w * s_t;
+    float3 Ls = in_scattering(M, sec, xs, w, tl, status);
+    float sigma_t = sigma(M, xs, tl);
+    float mis_T = 1.0f / (1.0f + sigma_t * sigma_t);
+    sigma_bw(M, xs, mis_T * weight_t * dot(dL_dR, W * Ls), tl);
+}
+
+// vr_path_integrator_NEE_DRTQ.h:58-260 (branch seed = Philox stream 1)
+__device__ void path_nee_drtq_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float3 dL_dR, Tally& tl,
+                                 uint32_t* status) {
+    float tMin, tMax;
+    boundary(M, x, w, tMin, tMax);
+    x = x + w * tMin;
+    float d = tMax - tMin;
+    if (d <= 0.0f) return;
+    Rng sec = branch_stream(rng);
+    (void)transmittance(M, rng, x, w, tl, status);
+    transmittance_bw(M, sec, x, w, dot(dL_dR, M.env), tl, status);
+    float3 R = f3(0.0f), W = f3(1.0f);
+    const float3 ini_x = x, ini_w = w;
+    const float ini_d = d;
+    const float EPS = 0.00000001f;
+    const Rng::Pos before_path = rng.pos();
+    int bounces = 0;
+    for (Flight ff; d > EPS; ++ff.it) {
+        if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
+        float md;
+        float m = ff.bk.query(M, x, w, md) * 1.05f + 0.1f;
+        float t = ff.sample(rng) / m;
+        x = x + w * gmin(t, md);
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(M); continue; }
+        ff.used();
+        if (t > d) break;
+        ff.bk.move(t);
+        float s = sigma(M, x, tl);
+        if (rng.uniform() >= s / m) { d -= t; continue; }
+        W = W * albedo(M, x, tl);
+        float3 wnee;
+        float3 env = environment_sample(M, rng, wnee);
+        float T_nee = transmittance(M, rng, x, wnee, tl, status);
+        R = R + W * T_nee * env * phase(M, w, wnee);
+        if (M.has_sun) R = R + W * transmittance(M, rng, x, M.sun_dir, tl, status) * M.sun_L * phase(M, w, M.sun_dir);
+        bool capped = M.max_bounces > 0 && ++bounces >= M.max_bounces;
+        w = phase_sample(M, rng, w);
+        boundary(M, x, w, tMin, d);
+        ff.bk.reset();
+        if (all_less(W, EPS) || capped) break;
+    }
+    W = f3(1.0f);
+    x = ini_x;
+    w = ini_w;
+    d = ini_d;
+    rng.seek(before_path);
+    bounces = 0;
+    drtq_scatter_term(M, sec, x, w, d, W, dL_dR, tl, status);
+    for (Flight ff; d > EPS; ++ff.it) {
+        if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
+        float md;
+        float m = ff.bk.query(M, x, w, md) * 1.05f + 0.1f;
+        float t = ff.sample(rng) / m;
+        x = x + w * gmin(t, md);
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(M); continue; }
+        ff.used();
+        if (t > d) break;
+        ff.bk.move(t);
+        float s = sigma(M, x, tl);
+        if (rng.uniform() >= s / m) {
+            sigma_bw(M, x, dot(dL_dR, -R / m / (1.0f - s / m)), tl);
+            d -= t;
+            continue;
+        }
+        float dL_dsigma = dot(dL_dR, s * s / (1.0f + s * s) * R / s);
+        W = W * albedo(M, x, tl);
+        float3 wnee;
+        float3 env = environment_sample(M, rng, wnee);
+        float T_nee = transmittance(M, rng, x, wnee, tl, status);
+        float ph_nee = phase(M, w, wnee);
+        float T_sun = 0.0f, ph_sun = 0.0f;
+        if (M.has_sun) {
+            T_sun = transmittance(M, rng, x, M.sun_dir, tl, status);
+            ph_sun = phase(M, w, M.sun_dir);
+        }
+        bool capped = M.max_bounces > 0 && ++bounces >= M.max_bounces;
+        float3 wo = phase_sample(M, rng, w);
+        float dL_dTnee = dot(dL_dR, W * env * ph_nee);
+        R = R - W * T_nee * env * ph_nee;
+        float dL_dTsun = 0.0f;
+        if (M.has_sun) {
+            dL_dTsun = dot(dL_dR, W * M.sun_L * ph_sun);
+            R = R - W * T_sun * M.sun_L * ph_sun;
+        }
+        sigma_bw(M, x, dL_dsigma, tl);
+        transmittance_bw(M, sec, x, wnee, dL_dTnee, tl, status);
+        if (M.has_sun) transmittance_bw(M, sec, x, M.sun_dir, dL_dTsun, tl, status);
+        w = wo;
+        boundary(M, x, w, tMin, d);
+        ff.bk.reset();
+        if (all_less(W, EPS) || capped) break;
+        drtq_scatter_term(M, sec, x, w, d, W, dL_dR, tl, status);
+    }
+}
+
+// vr_path_integrator_NEE_DRTDS.h:8-38 (majorant at the sample point)
+__device__ void sample_collision_position_ds(const DMedium& M, Rng& rng, float3 x, float3 w, float d, float epsilon,
+                                             float& t, float& weight_t, Tally& tl, uint32_t* status) {
+    const float EPS = 0.0000001f;
+    t = 0.0f;
+    weight_t = 1.0f;
+    for (int it = 0; it < kStepCap; ++it) {
+        float md;
+        float m = gmax(EPS, majorant(M, ray_at(x, w, t), w, md) + 2.0f * epsilon + 0.1f);
+        float dt = gmin(-logf(1.0f - rng.uniform()) / m, gmin(md, d - t));
+        t += dt;
+        if (dt >= md - EPS) continue;
+        if (t >= d - EPS) { weight_t = 0.0f; return; }
+        float s = sigma(M, ray_at(x, w, t), tl);
+        float Pc = (s + epsilon) / m;
+        if (rng.uniform() < Pc) {
+            weight_t *= 1.0f / (s + epsilon);
+            return;
+        }
+        weight_t *= (1.0f - s / m) / (1.0f - Pc);
+    }
+    raise_status(status, 4);
+    weight_t = 0.0f;
+}
+
+// vr_path_integrator_NEE_DRTDS.h:40-253 (branch seed = Philox stream 1)
+__device__ void path_nee_drtds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float epsilon, float3 dL_dR,
+                                  Tally& tl, uint32_t* status) {
+    float tMin, tMax;
+    boundary(M, x, w, tMin, tMax);
+    x = x + w * tMin;
+    float d = tMax - tMin;
+    if (d <= 0.0f) return;
+    Rng sec = branch_stream(rng);
+    uint32_t verts = 0;
+    (void)transmittance(M, rng, x, w, tl, status);
+    transmittance_bw(M, sec, x, w, dot(dL_dR, M.env), tl, status);
+    float3 R = f3(0.0f), W = f3(1.0f);
+    float3 res_x = x, res_w = w, res_W = W;
+    float res_P = 3.0f, total_weight = 3.0f;
+    const float3 ini_x = x, ini_w = w;
+    const float ini_d = d;
+    const float EPS = 0.00000001f;
+    const Rng::Pos before_path = rng.pos();
+    int bounces = 0;
+    for (Flight ff; d > EPS; ++ff.it) {
+        if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
+        float md;
+        float m = ff.bk.query(M, x, w, md) * 1.05f + 0.1f;
+        float t = ff.sample(rng) / m;
+        x = x + w * gmin(t, md);
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(M); continue; }
+        ff.used();
+        if (t > d) break;
+        ff.bk.move(t);
+        float s = sigma(M, x, tl);
+        if (rng.uniform() >= s / m) { d -= t; continue; }
+        W = W * albedo(M, x, tl);
+        float3 wnee;
+        float3 env = environment_sample(M, rng, wnee);
+        float T_nee = transmittance(M, rng, x, wnee, tl, status);
+        R = R + W * T_nee * env * phase(M, w, wnee);
+        if (M.has_sun) R = R + W * transmittance(M, rng, x, M.sun_dir, tl, status) * M.sun_L * phase(M, w, M.sun_dir);
+        bool capped = M.max_bounces > 0 && ++bounces >= M.max_bounces;
+        w = phase_sample(M, rng, w);
+        boundary(M, x, w, tMin, d);
+        ff.bk.reset();
+        float current_P = W.x + W.y + W.z;
+        total_weight += current_P;
+        if (rng.uniform() < current_P / total_weight) {
+            res_P = current_P; res_W = W; res_x = x; res_w = w;
+        }
+        if (all_less(W, EPS) || capped) break;
+    }
+    W = f3(1.0f);
+    x = ini_x;
+    w = ini_w;
+    d = ini_d;
+    rng.seek(before_path);
+    bounces = 0;
+    for (Flight ff; d > EPS; ++ff.it) {
+        if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
+        float md;
+        float m = ff.bk.query(M, x, w, md) * 1.05f + 0.1f;
+        float t = ff.sample(rng) / m;
+        x = x + w * gmin(t, md);
+        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(M); continue; }
+        ff.used();
+        if (t > d) break;
+        ff.bk.move(t);
+        float s = sigma(M, x, tl);
+        if (rng.uniform() >= s / m) {
+            sigma_bw(M, x, dot(dL_dR, -R / m / (1.0f - s / m)), tl);
+            d -= t;
+            continue;
+        }
+        float3 sa = albedo(M, x, tl);
+        float3 wnee;
+        float3 env = environment_sample(M, rng, wnee);
+        float T_nee = transmittance(M, rng, x, wnee, tl, status);
+        float ph_nee = phase(M, w, wnee);
+        float T_sun = 0.0f, ph_sun = 0.0f;
+        if (M.has_sun) {
+            T_sun = transmittance(M, rng, x, M.sun_dir, tl, status);
+            ph_sun = phase(M, w, M.sun_dir);
+        }
+        bool capped = M.max_bounces > 0 && ++bounces >= M.max_bounces;
+        float3 wo = phase_sample(M, rng, w);
+        W = W * sa;
+        float dL_dTnee = dot(dL_dR, W * env * ph_nee);
+        R = R - W * T_nee * env * ph_nee;
+        float dL_dTsun = 0.0f;
+        if (M.has_sun) {
+            dL_dTsun = dot(dL_dR, W * M.sun_L * ph_sun);
+            R = R - W * T_sun * M.sun_L * ph_sun;
+        }
+        transmittance_bw(M, sec, x, wnee, dL_dTnee, tl, status);
+        if (M.has_sun) transmittance_bw(M, sec, x, M.sun_dir, dL_dTsun, tl, status);
+        w = wo;
+        boundary(M, x, w, tMin, d);
+        ff.bk.reset();
+        rng.advance();
+        if (all_less(W, EPS) || capped) break;
+    }
+    boundary(M, res_x, res_w, tMin, d);
+    float s_t, weight_t;
+    sample_collision_position_ds(M, rng, res_x, res_w, d, epsilon, s_t, weight_t, tl, status);
+    if (weight_t > 0.0f) {
+        float3 xs = res_x + res_w * s_t;
+        float3 ls_dir;
+        float3 Ls_env = environment_sample(M, rng, ls_dir);
+        float3 Ls = transmittance(M, rng, xs, ls_dir, tl, status) * Ls_env * phase(M, res_w, ls_dir);
+        if (M.has_sun) Ls = Ls + transmittance(M, rng, xs, M.sun_dir, tl, status) * M.sun_L * phase(M, res_w, M.sun_dir);
+        float3 ws = phase_sample(M, rng, res_w);
+        Ls = Ls + 1.0f * path_nee_seq(M, rng, xs, ws, true, verts, tl, status);
+        Ls = Ls * res_W * weight_t * albedo(M, xs, tl);
+        sigma_bw(M, xs, dot(dL_dR, Ls) * total_weight / res_P, tl);
+    }
+}
+
+// vr_path_integrator_NEE_SPS.h:1-59 (majorant at the current sample point;
+// pow(sigma, 3) as sigma * sigma * sigma)
+__device__ bool sample_collision_position(const DMedium& M, Rng& rng, float3 x, float3 w, float d, float3& xc,
+                                          float& weight_xc, float& sigma_xc, int& samples, bool& mis_allowed,
+                                          Tally& tl, uint32_t* status) {
+    float t = 0.0f;
+    weight_xc = 0.0f;
+    sigma_xc = 0.0f;
+    samples = 0;
+    xc = x;
+    int it = 0;
+    for (; it < kStepCap; ++it) {
+        float md;
+        float m = majorant(M, xc, w, md) + 0.000001f;
+        float dt = gmin(-logf(1.0f - rng.uniform()) / m, gmin(md, d - t));
+        t += dt;
+        xc = ray_at(x, w, t);
+        if (dt >= md - 0.0000001f) continue;
+        if (t >= d - 0.0000001f) break;
+        float s = sigma(M, xc, tl);
+        samples++;
+        if (rng.uniform() < s / m) {
+            weight_xc = 1.0f;
+            sigma_xc = s;
+            break;
+        }
+    }
+    if (it == kStepCap) raise_status(status, 4);
+    if (!mis_allowed) return false;
+    float powered_c = sigma_xc * sigma_xc * sigma_xc;
+    float mis_wc = weight_xc * powered_c / (1.0f + powered_c);
+    float u = rng.uniform();
+    float3 xf = xc * (1.0f - u) + x * u;
+    float sigma_f = sigma(M, xf, tl);
+    float powered_f = sigma_f * sigma_f * sigma_f;
+    float mis_wf = t / (1.0f + powered_f);
+    weight_xc = mis_wc + mis_wf;
+    if (rng.uniform() * weight_xc < mis_wf) {
+        xc = xf;
+        sigma_xc = sigma_f;
+        mis_allowed = false;
+        return true;
+    }
+    return false;
+}
+
+// vr_path_integrator_NEE_SPS.h:88-101 st_tau_bw (stratified bins)
+__device__ void st_tau_bw(const DMedium& M, Rng& rng, float3 a, float3 b, int bins, float dL_dtau, Tally& tl) {
+    if (dL_dtau == 0.0f || bins == 0) return;
+    float d = sqrtf(dot(a - b, a - b));
+    float g = dL_dtau * d / (float)bins;
+    for (int i = 0; i < bins; ++i) {
+        float f = ((float)i + rng.uniform()) / (float)bins;
+        sigma_bw(M, b * (1.0f - f) + a * f, g, tl);
+    }
+}
+
+// vr_path_integrator_NEE_SPS.h:104-263 (emission ignored, as in the reference)
+__device__ void path_nee_sps_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float3 dL_dR, Tally& tl,
+                                uint32_t* status) {
+    float tMin, tMax;
+    boundary(M, x, w, tMin, tMax);
+    x = x + w * tMin;
+    float d = tMax - tMin;
+    if (d <= 0.0f) return;
+    Rng sec = branch_stream(rng);
+    (void)transmittance(M, rng, x, w, tl, status);
+    transmittance_bw(M, sec, x, w, dot(dL_dR, M.env), tl, status);
+    float3 R = f3(0.0f), Rf = f3(0.0f), W = f3(1.0f);
+    float W_singular = 1.0f;
+    bool mis_allowed = true;
+    const float3 ini_x = x, ini_w = w;
+    const float ini_d = d;
+    const float EPS = 0.00001f;
+    const Rng::Pos before_path = rng.pos();
+    int bounces = 0;
+    for (int it = 0; it < kStepCap; ++it) {
+        float weight_xc, sigma_xc;
+        float3 xc;
+        int samples;
+        if (sample_collision_position(M, rng, x, w, d, xc, weight_xc, sigma_xc, samples, mis_allowed, tl, status))
+            W_singular = sigma_xc;
+        if (weight_xc == 0.0f) break;
+        x = xc;
+        W = W * (weight_xc * albedo(M, x, tl));
+        float3 wnee;
+        float3 nee_env = environment_sample(M, rng, wnee);
+        float nee_T = transmittance(M, rng, x, wnee, tl, status);
+        float3 added_R = W * nee_T * phase(M, w, wnee) * nee_env;
+        if (M.has_sun) added_R = added_R + W * transmittance(M, rng, x, M.sun_dir, tl, status) * phase(M, w, M.sun_dir) * M.sun_L;
+        if (mis_allowed) R = R + added_R;
+        else Rf = Rf + added_R;
+        bool capped = M.max_bounces > 0 && ++bounces >= M.max_bounces;
+        w = phase_sample(M, rng, w);
+        boundary(M, x, w, tMin, d);
+        if (all_less(W, EPS) || capped) break;
+    }
+    W = f3(1.0f);
+    mis_allowed = true;
+    x = ini_x;
+    w = ini_w;
+    d = ini_d;
+    float3 prev_x = x;
+    rng.seek(before_path);
+    bounces = 0;
+    for (int it = 0; it < kStepCap; ++it) {
+        float weight_xc, sigma_xc;
+        float3 xc;
+        int samples;
+        bool singular = sample_collision_position(M, rng, x, w, d, xc, weight_xc, sigma_xc, samples, mis_allowed, tl,
+                                                  status);
+        if (weight_xc == 0.0f) break;
+        float3 further_R = R + W_singular * Rf;
+        float k = dot(dL_dR, further_R);
+        float dL_dtau = -k;
+        float dL_dsigma = singular ? dot(dL_dR, Rf) : k / gmax(0.001f, sigma_xc);
+        x = xc;
+        W = W * weight_xc;
+        W = W * albedo(M, x, tl);
+        float3 wnee;
+        float3 env = environment_sample(M, rng, wnee);
+        float T_nee = transmittance(M, rng, x, wnee, tl, status);
+        float ph_nee = phase(M, w, wnee);
+        float T_sun = 0.0f, ph_sun = 0.0f;
+        if (M.has_sun) {
+            T_sun = transmittance(M, rng, x, M.sun_dir, tl, status);
+            ph_sun = phase(M, w, M.sun_dir);
+        }
+        bool capped = M.max_bounces > 0 && ++bounces >= M.max_bounces;
+        float3 wo = phase_sample(M, rng, w);
+        const float fs = mis_allowed ? 1.0f : W_singular;
+        float dL_dTnee = dot(dL_dR, W * fs * env * ph_nee);
+        float3 added_R = W * T_nee * ph_nee * env;
+        float dL_dTsun = 0.0f;
+        if (M.has_sun) {
+            dL_dTsun = dot(dL_dR, W * fs * M.sun_L * ph_sun);
+            added_R = added_R + W * T_sun * ph_sun * M.sun_L;
+        }
+        if (mis_allowed) R = R - added_R;
+        else Rf = Rf - added_R;
+        sigma_bw(M, x, dL_dsigma, tl);
+        st_tau_bw(M, sec, x, prev_x, samples > 1 ? samples : 1, dL_dtau, tl);
+        transmittance_bw(M, sec, x, wnee, dL_dTnee, tl, status);
+        if (M.has_sun) transmittance_bw(M, sec, x, M.sun_dir, dL_dTsun, tl, status);
+        w = wo;
+        boundary(M, x, w, tMin, d);
+        if (all_less(W, EPS) || capped) break;
+        prev_x = x;
+    }
+}
+
 // ------------------------------------------------------------------------
 // Kernels over paths (grid-stride, one path per thread at a time)
 // ------------------------------------------------------------------------
@@ -879,7 +1306,10 @@ __global__ void __launch_bounds__(256) k_path_bw(DMedium M, PathSrc S, uint64_t 
         ++paths;
         if (MODE == 0) path_nee_ds_bw(M, rng, x, w, M.ds_eps, g, tl, &sc->status);
         else if (MODE == 1) path_dt_bw(M, rng, x, w, M.ds_eps, g, tl, &sc->status);
-        else path_nee_drt_bw(M, rng, x, w, g, tl, &sc->status);
+        else if (MODE == 2) path_nee_drt_bw(M, rng, x, w, g, tl, &sc->status);
+        else if (MODE == 3) path_nee_drtq_bw(M, rng, x, w, g, tl, &sc->status);
+        else if (MODE == 4) path_nee_drtds_bw(M, rng, x, w, M.ds_eps, g, tl, &sc->status);
+        else path_nee_sps_bw(M, rng, x, w, g, tl, &sc->status);
     }
     warp_add_counters(sc, paths, 0, tl);
 }
@@ -951,7 +1381,10 @@ int launch_radiance_bw(const DMedium& M, int bw_mode, const PathSrc& src, uint64
     int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
     if (bw_mode == 0) k_path_bw<0><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
     else if (bw_mode == 1) k_path_bw<1><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
-    else k_path_bw<2><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
+    else if (bw_mode == 2) k_path_bw<2><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
+    else if (bw_mode == 3) k_path_bw<3><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
+    else if (bw_mode == 4) k_path_bw<4><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
+    else k_path_bw<5><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
     count_launches(1);
     return launch_status(cudaGetLastError());
 }

@@ -579,14 +579,17 @@ class DRTPathIntegrator(_PathIntegrator):
 
 
 class DRTQPathIntegrator(DRTPathIntegrator):
-    """DRTQPathIntegrator (_maps.py:3025-3066): shares the NEE forward; its
-    quadratic adjoint (vr_path_integrator_NEE_DRTQ.h) is not built yet."""
-    BW = None
+    """DRTQPathIntegrator (_maps.py:3025-3066): NEE forward; differential ratio
+    tracking adjoint with a scatter-gradient term on every path segment
+    (vr_path_integrator_NEE_DRTQ.h)."""
+    BW = 3
 
 
 class DRTDSPathIntegrator(_PathIntegrator):
-    """DRTDSPathIntegrator (_maps.py:3070-3114): NEE forward; adjoint not built yet."""
-    FW, BW = 0, None
+    """DRTDSPathIntegrator (_maps.py:3070-3114): NEE forward; differential ratio
+    tracking adjoint whose reservoir term samples a defensive collision position
+    (vr_path_integrator_NEE_DRTDS.h)."""
+    FW, BW = 0, 4
 
     def __init__(self, sigma, scattering_albedo, emission, environment, environment_sampler, phase, phase_sampler,
                  boundary, majorant, transmittance, ds_epsilon: float, **ext):
@@ -595,8 +598,10 @@ class DRTDSPathIntegrator(_PathIntegrator):
 
 
 class SPSPathIntegrator(DRTPathIntegrator):
-    """SPSPathIntegrator (_maps.py:3118-3159): NEE forward; adjoint not built yet."""
-    BW = None
+    """SPSPathIntegrator (_maps.py:3118-3159): NEE forward; singular-path sampling
+    adjoint with MIS between collision and uniform segment vertices
+    (vr_path_integrator_NEE_SPS.h)."""
+    BW = 5
 
 
 # ------------------------------------------------------------------ sensors --

@@ -90,6 +90,13 @@ def build_field(sigma: torch.Tensor, *, albedo=0.9, albedo_grid: torch.Tensor | 
     if integrator == "nee_ds":
         return maps.DeltatrackingNEEPathIntegrator(sg, alb, maps.ZERO, envm, env_sampler, ph, ps, boundary, maj, trm,
                                                    ds_epsilon, ds_compat=ds_compat, **ext)
+    if integrator == "drtq":
+        return maps.DRTQPathIntegrator(sg, alb, maps.ZERO, envm, env_sampler, ph, ps, boundary, maj, trm, **ext)
+    if integrator == "drtds":
+        return maps.DRTDSPathIntegrator(sg, alb, maps.ZERO, envm, env_sampler, ph, ps, boundary, maj, trm, ds_epsilon,
+                                        **ext)
+    if integrator == "sps":
+        return maps.SPSPathIntegrator(sg, alb, maps.ZERO, envm, env_sampler, ph, ps, boundary, maj, trm, **ext)
     return maps.DRTPathIntegrator(sg, alb, maps.ZERO, envm, env_sampler, ph, ps, boundary, maj, trm, **ext)
 
 

@@ -262,6 +262,10 @@ def test_dt_integrator_matches_oracle(cuda):
     ("ds", dict(ds_compat=True)),
     ("dt", dict(integrator="dt", sun_dir=None)),
     ("drt", dict(integrator="drt")),
+    ("drtq", dict(integrator="drtq")),
+    ("drtds", dict(integrator="drtds")),
+    ("sps", dict(integrator="sps")),
+    ("sps", dict(integrator="sps", majorant="grid", brick=8)),
 ])
 def test_capture_backward_matches_oracle(cuda, bw, kw):
     wl = synthetic.WORKLOADS["plain_forward_64"]

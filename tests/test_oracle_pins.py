@@ -348,7 +348,7 @@ def test_sun_single_scatter_adds_light():
     assert oracle.radiance_fw(sun, "nee", rays, 1)[0].mean() > 0
 
 
-@pytest.mark.parametrize("bw", ["ds", "dt"])
+@pytest.mark.parametrize("bw", ["ds", "dt", "drt", "drtq", "drtds", "sps"])
 def test_adjoint_matches_finite_difference_of_expectation(bw):
     """dE[L]/ds along sigma -> s*sigma: the replay adjoint (consistent majorant)
     against a central difference of the forward with common random numbers."""
