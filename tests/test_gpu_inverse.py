@@ -1,0 +1,18 @@
+"""The inverse-rendering loop (multi-view capture, NEE_DS adjoint, Adam) on a
+small version of workload inverse_rendering_128: the loss on the training
+views falls, and so does the loss on held-out views (cameras between the
+training ones), so the reconstruction is not only fitted to the images it saw.
+Needs a B200."""
+import pytest
+
+from rendervous_b200 import inverse_eval
+
+pytestmark = pytest.mark.gpu
+
+
+def test_inverse_rendering_reduces_training_and_heldout_loss(cuda):
+    # a larger Adam step than the workload's 0.01 so a short run moves sigma far enough
+    r = inverse_eval.run(iterations=80, width=48, spp=8, target_spp=64, views=4, res=32, target_res=64, seed=1,
+                         device=cuda, lr=0.3)
+    assert r["loss_final_mean10"] < 0.5 * r["loss_first"], r
+    assert r["heldout_loss_final"] < 0.7 * r["heldout_loss_initial"], r
