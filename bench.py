@@ -163,6 +163,58 @@ def profiled_traffic(kernel: str):
     return None
 
 
+KERNELS = ["k_walk_fw", "k_shadow_fw", "k_ds_primal", "k_shadow_T", "k_ds_replay", "k_shadow_adj"]
+# the kernel functions each slot covers (ratio-tracking shadows run k_shadow_run / k_shadow_adj)
+KERNEL_FUNCS = {"k_walk_fw": "k_walk_fw", "k_shadow_fw": "k_shadow_run<0, 0>", "k_ds_primal": "k_ds_primal",
+                "k_shadow_T": "k_shadow_run<0, 1>", "k_ds_replay": "k_ds_replay", "k_shadow_adj": "k_shadow_adj<0>"}
+
+
+def gather_peaks(dev, reps: int = 5) -> dict:
+    """Random 32-byte gather bandwidth (GB/s of sectors) over an L2-resident
+    64 MB buffer and a 4 GB buffer, CUDA events around `reps` launches."""
+    import torch
+    from rendervous_b200 import _lib
+    ffi, lib = _lib.ffi_lib()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    threads, per_thread = sms * 2048, 256
+    sink = torch.zeros(1, dtype=torch.int32, device=dev)
+    stream = _lib.stream_handle(dev)
+    out = {}
+    for name, nbytes in (("l2", 64 << 20), ("hbm", 4 << 30)):
+        buf = torch.ones(nbytes // 4, dtype=torch.float32, device=dev)
+        args = (ffi.cast("void *", buf.data_ptr()), nbytes, threads, per_thread)
+        _lib.check(lib.vrt_gather_peak(*args, 1, ffi.cast("uint32_t *", sink.data_ptr()), stream))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for r in range(reps):
+            _lib.check(lib.vrt_gather_peak(*args, 2 + r, ffi.cast("uint32_t *", sink.data_ptr()), stream))
+        e1.record()
+        e1.synchronize()
+        out[name] = 32.0 * threads * per_thread * reps / (e0.elapsed_time(e1) / 1e3) / 1e9
+        del buf
+    return out
+
+
+def kernel_table(stats, steps: int) -> dict:
+    """Per wavefront kernel over the timed steps: launches, event time, and
+    algorithmic bytes (32 B per sigma / albedo lookup, 4 B per atomic add)."""
+    table = {}
+    for name, st in zip(KERNELS, stats):
+        if st.launches == 0:
+            continue
+        alg = 32.0 * st.lookups + 32.0 * st.albedo_lookups + 4.0 * st.reds
+        ms_launch = st.ms / st.launches
+        table[name] = {"function": KERNEL_FUNCS[name], "launches_per_step": st.launches / steps,
+                       "ms_per_step": st.ms / steps, "ms_per_launch": ms_launch,
+                       "bytes_per_launch": alg / st.launches,
+                       "gbs": (alg / st.launches) / (ms_launch / 1e3) / 1e9 if ms_launch > 0 else None,
+                       "lookups_per_step": st.lookups / steps, "reds_per_step": st.reds / steps}
+    tot = sum(v["ms_per_step"] for v in table.values()) or 1.0
+    for v in table.values():
+        v["share"] = v["ms_per_step"] / tot
+    return table
+
+
 # ------------------------------------------------------------ CPU baseline --
 def cpu_sample(seconds_hint: float = 10.0, threads: int | None = None):
     """The oracle (the reference's algorithm restated in C++, constant majorant
@@ -244,8 +296,11 @@ def run_ours(args):
         dist.barrier()
     torch.cuda.synchronize(dev)
     times = []
-    _, vlib = _lib.ffi_lib()
+    vffi, vlib = _lib.ffi_lib()
     launches0 = int(vlib.vrt_launch_count())
+    kstats = vffi.new("vrt_kernel_stat[]", len(KERNELS))
+    _lib.check(vlib.vrt_kernel_stats(_lib.context(dev).ptr, _lib.stream_handle(dev), kstats))  # clear
+    vlib.vrt_set_kernel_timing(1)
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             flush.zero_()
@@ -258,6 +313,9 @@ def run_ours(args):
             times.append(e0.elapsed_time(e1))
     torch.cuda.synchronize(dev)
     launches = int(vlib.vrt_launch_count()) - launches0
+    _lib.check(vlib.vrt_kernel_stats(_lib.context(dev).ptr, _lib.stream_handle(dev), kstats))
+    vlib.vrt_set_kernel_timing(0)
+    ktable = kernel_table(kstats, args.steps)
     if world > 1:
         dist.barrier()
     counters = maps.check()
@@ -308,10 +366,12 @@ def run_ours(args):
         c = cnt_l[-1]
         bytes_alg = 32.0 * c["lookups"] + 32.0 * c["albedo_lookups"] + 4.0 * c["reds"] + 12.0 * c["paths"]
         roof[name] = dict(ms=ms, bytes=bytes_alg, counters=c)
-    dom = max(roof, key=lambda k: roof[k]["ms"])
-    kern = {"fw": "k_walk_fw+k_shadow_fw", "bw": "k_nee_ds_bw"}[dom]
+    # the dominant kernel of the timed steps (by event time) sets the roofline line
+    kern = max(ktable, key=lambda k: ktable[k]["ms_per_step"])
+    kd = ktable[kern]
     peaks = measured_peaks()
-    achieved = roof[dom]["bytes"] / (roof[dom]["ms"] / 1e3) / 1e9
+    gpeaks = gather_peaks(dev)
+    achieved = kd["gbs"]
     traffic = profiled_traffic(kern)
 
     # ---- end to end: host grids in, loss and gradients out, through the public API
@@ -372,11 +432,14 @@ def run_ours(args):
             "e2e": e2e,
             "gpu_launches": launches,
             "counters_per_step": {k: v / args.steps for k, v in c.items() if k != "status"},
-            "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peaks["hbm_gbs"],
-                         "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                         "peak_source": peaks["source"], "algorithmic_bytes_per_launch": roof[dom]["bytes"],
-                         "launch_ms": roof[dom]["ms"],
+            "roofline": {"bound": "hbm", "kernel": kern, "function": kd["function"], "achieved": achieved,
+                         "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                         "traffic": traffic, "peak_source": peaks["source"],
+                         "algorithmic_bytes_per_launch": kd["bytes_per_launch"], "launch_ms": kd["ms_per_launch"],
+                         "gather_peak_gbs": gpeaks, "frac_of_l2_gather": achieved / gpeaks["l2"],
+                         "frac_of_hbm_gather": achieved / gpeaks["hbm"],
                          "split_ms": {k: roof[k]["ms"] for k in roof}},
+            "kernels": ktable,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }

@@ -128,6 +128,34 @@ int vrt_context_sync(vrt_context* ctx, void* stream, vrt_counters* out);
 const char* vrt_status_string(int32_t status);
 /* Number of kernels this library has launched in the process (for launch accounting). */
 int64_t vrt_launch_count(void);
+
+/* Per-kernel measurement of the wavefront kernels (no reference counterpart).
+   Each kernel adds its own tallies (tracking steps, sigma lookups, atomic adds,
+   albedo lookups) to a slot of the context; with timing on, the library also
+   brackets every launch with CUDA events on its stream.  vrt_kernel_stats
+   waits for `stream`, fills VRT_K_COUNT entries (launches, event time summed in
+   ms, tallies) accumulated since its last call, and clears them. */
+enum {
+    VRT_K_WALK_FW = 0,     /* forward walk (primary paths, shadow jobs) */
+    VRT_K_SHADOW_FW = 1,   /* forward shadow transmittances */
+    VRT_K_DS_PRIMAL = 2,   /* NEE_DS adjoint: primal walk */
+    VRT_K_SHADOW_T = 3,    /* NEE_DS adjoint: the primal's shadow transmittances */
+    VRT_K_DS_REPLAY = 4,   /* NEE_DS adjoint: replay walk (sigma / albedo scatters) */
+    VRT_K_SHADOW_ADJ = 5,  /* NEE_DS adjoint: transmittance adjoints */
+    VRT_K_COUNT = 6
+};
+typedef struct vrt_kernel_stat {
+    int64_t launches;
+    double ms;                       /* 0 unless timing was on */
+    int64_t steps, lookups, reds, albedo_lookups;
+} vrt_kernel_stat;
+void vrt_set_kernel_timing(int32_t on);
+/* Gather microbenchmark (the roofline of the lookups): threads x per_thread
+   random 32-byte loads (L1 bypassed) from `buffer` (bytes long, 32-byte
+   aligned); the caller times it.  sink: one device uint32 the kernel may write. */
+int vrt_gather_peak(const void* buffer, int64_t bytes, int64_t threads, int32_t per_thread, uint32_t seed,
+                    uint32_t* sink, void* stream);
+int vrt_kernel_stats(vrt_context* ctx, void* stream, vrt_kernel_stat* out);
 int32_t vrt_version(void);
 
 /* RayBoxIntersection forward (rendervous _maps.py:4128-4154, include/maths.h:28-38):

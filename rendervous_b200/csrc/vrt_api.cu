@@ -5,7 +5,10 @@
 // kernel-parameter forms of vrt_params.h and launches on the caller's stream.
 // There is no CPU fallback: every computation is a CUDA kernel.
 #include <atomic>
+#include <mutex>
+#include <vector>
 #include <cmath>
+#include <cstddef>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -25,6 +28,56 @@ int launch_status(cudaError_t e) {
 
 static std::atomic<long long> g_launches{0};
 void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Per-kernel launch counts and (optional) event timing of the wavefront kernels.
+namespace {
+struct KernelTiming {
+    std::mutex mu;
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    struct Pending {
+        int kid;
+        cudaEvent_t e0, e1;
+    };
+    std::vector<Pending> pending;
+    long long launches[VRT_K_COUNT] = {};
+};
+KernelTiming& timing() {
+    static KernelTiming t;
+    return t;
+}
+cudaEvent_t take_event(KernelTiming& t) {
+    if (!t.pool.empty()) {
+        cudaEvent_t e = t.pool.back();
+        t.pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return e;
+}
+}  // namespace
+
+KernelScope::KernelScope(int k, cudaStream_t s) : kid(k), stream(s), e0(nullptr), e1(nullptr) {
+    KernelTiming& t = timing();
+    std::lock_guard<std::mutex> lock(t.mu);
+    ++t.launches[kid];
+    if (!t.on) return;
+    e0 = take_event(t);
+    e1 = take_event(t);
+    if (e0) cudaEventRecord(e0, stream);
+}
+
+KernelScope::~KernelScope() {
+    if (!e0 || !e1) return;
+    KernelTiming& t = timing();
+    std::lock_guard<std::mutex> lock(t.mu);
+    cudaEventRecord(e1, stream);
+    t.pending.push_back({kid, e0, e1});
+}
 
 // The wavefront serves the NEE forward of capped paths (its job buffer is sized
 // from the bounce cap); uncapped paths run the persistent state machine.
@@ -60,6 +113,28 @@ int persistent_blocks(const void* kernel, int block, int num_sms) {
 }
 
 // ---------------------------------------------------------------- kernels --
+// Random 32-byte gathers (one L2 sector each, L1 bypassed) over `sectors`
+// sectors: four independent address chains per thread keep loads in flight;
+// every loaded word feeds the result, so no load can be dropped.
+__global__ void __launch_bounds__(256) k_gather_peak(const uint4* __restrict__ buf, unsigned long long sectors,
+                                                     int per_thread, uint32_t seed, unsigned int* sink) {
+    uint32_t h[4];
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) h[c] = (t * 4u + (uint32_t)c) * 2654435761u ^ seed;
+    uint32_t acc = 0;
+    for (int i = 0; i < per_thread; i += 4) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            h[c] = h[c] * 1664525u + 1013904223u;  // LCG (Numerical Recipes constants)
+            const unsigned long long s = ((unsigned long long)(h[c] ^ (h[c] >> 15)) * sectors) >> 32;
+            const uint4 a = __ldcg(buf + 2 * s), b = __ldcg(buf + 2 * s + 1);
+            acc ^= a.x ^ a.y ^ a.z ^ a.w ^ b.x ^ b.y ^ b.z ^ b.w;  // every loaded byte is used
+        }
+    }
+    if (acc == 0x9e3779b9u) atomicAdd(sink, 1u);
+}
+
 __global__ void k_ray_box(const float* __restrict__ rays, int64_t n, float3 bmin, float3 bmax, float* __restrict__ out) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         float tMin, tMax;
@@ -237,6 +312,60 @@ int32_t vrt_version(void) { return 1; }
 
 int64_t vrt_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
+int vrt_gather_peak(const void* buffer, int64_t bytes, int64_t threads, int32_t per_thread, uint32_t seed,
+                    uint32_t* sink, void* stream) {
+    if (!buffer || !sink) return VRT_E_NULL_POINTER;
+    if (bytes < 64 || threads < 256 || per_thread < 4 || (per_thread & 3) || ((uintptr_t)buffer & 31u))
+        return VRT_E_INVALID_ARGUMENT;
+    const unsigned long long sectors = (unsigned long long)bytes / 32ull;
+    if (sectors > (1ull << 32)) return VRT_E_BAD_SHAPE;
+    const int blocks = (int)(threads / 256);
+    k_gather_peak<<<blocks, 256, 0, (cudaStream_t)stream>>>(static_cast<const uint4*>(buffer), sectors, per_thread,
+                                                            seed, sink);
+    count_launches(1);
+    return launch_status(cudaGetLastError());
+}
+
+void vrt_set_kernel_timing(int32_t on) {
+    KernelTiming& t = timing();
+    std::lock_guard<std::mutex> lock(t.mu);
+    t.on = on != 0;
+}
+
+int vrt_kernel_stats(vrt_context* ctx, void* stream, vrt_kernel_stat* out) {
+    int st = check_ctx(ctx);
+    if (st) return st;
+    if (!out) return VRT_E_NULL_POINTER;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return launch_status(cudaGetLastError());
+    unsigned long long k[8][4];
+    if (cudaMemcpy(k, ctx->scratch->kstat, sizeof(k), cudaMemcpyDeviceToHost) != cudaSuccess) return VRT_E_CUDA;
+    if (cudaMemset(ctx->scratch->kstat, 0, sizeof(k)) != cudaSuccess) return VRT_E_CUDA;
+    KernelTiming& t = timing();
+    std::lock_guard<std::mutex> lock(t.mu);
+    double ms[VRT_K_COUNT] = {};
+    for (const auto& p : t.pending) {
+        float e = 0.0f;
+        if (cudaEventSynchronize(p.e1) == cudaSuccess && cudaEventElapsedTime(&e, p.e0, p.e1) == cudaSuccess)
+            ms[p.kid] += e;
+        else
+            cudaGetLastError();
+        t.pool.push_back(p.e0);
+        t.pool.push_back(p.e1);
+    }
+    t.pending.clear();
+    for (int i = 0; i < VRT_K_COUNT; ++i) {
+        out[i].launches = t.launches[i];
+        out[i].ms = ms[i];
+        out[i].steps = (int64_t)k[i][0];
+        out[i].lookups = (int64_t)k[i][1];
+        out[i].reds = (int64_t)k[i][2];
+        out[i].albedo_lookups = (int64_t)k[i][3];
+        t.launches[i] = 0;
+    }
+    return VRT_OK;
+}
+
 const char* vrt_status_string(int32_t s) {
     switch (s) {
         case VRT_OK: return "ok";
@@ -286,7 +415,8 @@ int vrt_context_sync(vrt_context* ctx, void* stream, vrt_counters* out) {
     if (cudaStreamSynchronize(s) != cudaSuccess) return launch_status(cudaGetLastError());
     DScratch h;
     if (cudaMemcpyAsync(&h, ctx->scratch, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess) return VRT_E_CUDA;
-    if (cudaMemsetAsync(ctx->scratch, 0, sizeof(h), s) != cudaSuccess) return VRT_E_CUDA;
+    // the per-kernel slots (kstat) stay: vrt_kernel_stats reads and clears them
+    if (cudaMemsetAsync(ctx->scratch, 0, offsetof(DScratch, kstat), s) != cudaSuccess) return VRT_E_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return VRT_E_CUDA;
     if (out) {
         out->paths = (int64_t)h.paths;

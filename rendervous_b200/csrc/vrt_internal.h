@@ -24,6 +24,16 @@ int ensure_wave_buffer(vrt_context* ctx, size_t bytes);
 // Host-side count of the kernels this library launched (vrt_launch_count).
 void count_launches(int n);
 
+// Brackets one launch of wavefront kernel `kid` (VRT_K_*): counts it and, with
+// kernel timing on, records CUDA events before and after it on `stream`.
+struct KernelScope {
+    int kid;
+    cudaStream_t stream;
+    cudaEvent_t e0, e1;
+    KernelScope(int kid, cudaStream_t stream);
+    ~KernelScope();
+};
+
 // Wavefront NEE_DS adjoint (vrt_wave.cu): capped paths, default replay majorant.
 int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed,
                       const float* dL, float div, cudaStream_t stream);

@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
             }
         }
     }
-    flush_counters(sc, n_paths_done, n_verts, tl);
+    flush_counters(sc, VRT_K_WALK_FW, n_paths_done, n_verts, tl);
 }
 
 template <int TR>
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow_fw(DMedium M, PathSrc S, cons
             atomicAdd(out + 3 * o + 2, c3.z * scale);
         }
     }
-    flush_counters(sc, 0, 0, tl);
+    flush_counters(sc, VRT_K_SHADOW_FW, 0, 0, tl);
 }
 
 // ---------------------------------------------------------------------------
@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow_run(DMedium M, PathSrc S, con
             }
         }
     }
-    flush_counters(sc, 0, 0, tl);
+    flush_counters(sc, OUT == OUT_IMAGE ? VRT_K_SHADOW_FW : VRT_K_SHADOW_T, 0, 0, tl);
 }
 
 // The transmittance adjoint (vr_transmittance_RT.h:51-141 / _DT.h:30-90): the
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(256, 3) k_shadow_adj(DMedium M, const ShadowJo
             }
         }
     }
-    flush_counters(sc, 0, 0, tl);
+    flush_counters(sc, VRT_K_SHADOW_ADJ, 0, 0, tl);
 }
 
 // Host: rounds of walk + shadow until every path has been taken.
@@ -437,12 +437,18 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
         // count of the jobs written, and the head the persistent shadow kernel takes them from
         if ((e = cudaMemsetAsync(wv.count, 0, 2 * sizeof(unsigned long long), stream)) != cudaSuccess)
             return launch_status(e);
-        k_walk_fw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, ctx->scratch, wv);
-        switch (M.tr_mode) {
-            case 0: k_shadow_run<0, OUT_IMAGE><<<rblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, wv.cap, wv.count + 1, seed, so, ctx->scratch); break;
-            case 1: k_shadow_run<1, OUT_IMAGE><<<rblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, wv.cap, wv.count + 1, seed, so, ctx->scratch); break;
-            case 2: k_shadow_fw<2><<<sblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, seed, out, scale, ctx->scratch); break;
-            default: k_shadow_fw<3><<<sblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, seed, out, scale, ctx->scratch); break;
+        {
+            KernelScope ks(VRT_K_WALK_FW, stream);
+            k_walk_fw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, ctx->scratch, wv);
+        }
+        {
+            KernelScope ks(VRT_K_SHADOW_FW, stream);
+            switch (M.tr_mode) {
+                case 0: k_shadow_run<0, OUT_IMAGE><<<rblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, wv.cap, wv.count + 1, seed, so, ctx->scratch); break;
+                case 1: k_shadow_run<1, OUT_IMAGE><<<rblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, wv.cap, wv.count + 1, seed, so, ctx->scratch); break;
+                case 2: k_shadow_fw<2><<<sblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, seed, out, scale, ctx->scratch); break;
+                default: k_shadow_fw<3><<<sblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, seed, out, scale, ctx->scratch); break;
+            }
         }
         count_launches(2);
         if ((st = launch_status(cudaGetLastError()))) return st;
@@ -478,7 +484,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow_T(DMedium M, WaveBw wv, uint6
             atomicAdd(io + 2, c3.z);
         }
     }
-    flush_counters(sc, 0, 0, tl);
+    flush_counters(sc, VRT_K_SHADOW_T, 0, 0, tl);
 }
 
 template <int TR>
@@ -496,12 +502,13 @@ __global__ void __launch_bounds__(256, 4) k_shadow_bw(DMedium M, WaveBw wv, uint
         else if (TR == 2) transmittance_dda_bw<false>(M, jv.x, jv.dir, jv.wt.x, tl);
         else transmittance_dda_bw<true>(M, jv.x, jv.dir, jv.wt.x, tl);
     }
-    flush_counters(sc, 0, 0, tl);
+    flush_counters(sc, VRT_K_SHADOW_ADJ, 0, 0, tl);
 }
 
 int launch_shadow_record(const DMedium& M, const PathSrc& src, const WaveBw& wv, uint64_t seed, DScratch* sc,
                          int num_sms, cudaStream_t stream) {
     const ShadowOut so = {nullptr, 0.0f, wv.recs, wv.info, wv.p_begin};
+    KernelScope ks(VRT_K_SHADOW_T, stream);
     switch (M.tr_mode) {
         case 0:
             k_shadow_run<0, OUT_RECORD><<<persistent_blocks((const void*)k_shadow_run<0, OUT_RECORD>, 256, num_sms), 256,
@@ -520,6 +527,7 @@ int launch_shadow_record(const DMedium& M, const PathSrc& src, const WaveBw& wv,
 
 int launch_shadow_adjoint(const DMedium& M, const WaveBw& wv, uint64_t seed, DScratch* sc, int num_sms,
                           cudaStream_t stream) {
+    KernelScope ks(VRT_K_SHADOW_ADJ, stream);
     switch (M.tr_mode) {
         case 0:
             k_shadow_adj<0><<<persistent_blocks((const void*)k_shadow_adj<0>, 256, num_sms), 256, 0, stream>>>(

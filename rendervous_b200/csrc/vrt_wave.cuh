@@ -73,7 +73,7 @@ __device__ __forceinline__ unsigned long long reserve_slots(unsigned long long* 
 
 // Per-warp sums of the lanes' tallies into the context counters.  `verts`
 // counts forward path vertices only (the metric's unit); adjoint kernels pass 0.
-__device__ __forceinline__ void flush_counters(DScratch* sc, uint32_t paths, uint32_t verts, const Tally& tl) {
+__device__ __forceinline__ void flush_counters(DScratch* sc, int kid, uint32_t paths, uint32_t verts, const Tally& tl) {
     unsigned long long p = paths, v = verts, s = tl.steps, l = tl.lookups, a = tl.albedo, r = tl.reds;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -91,6 +91,10 @@ __device__ __forceinline__ void flush_counters(DScratch* sc, uint32_t paths, uin
         if (l) atomicAdd(&sc->lookups, l);
         if (a) atomicAdd(&sc->albedo, a);
         if (r) atomicAdd(&sc->reds, r);
+        if (s) atomicAdd(&sc->kstat[kid][0], s);
+        if (l) atomicAdd(&sc->kstat[kid][1], l);
+        if (r) atomicAdd(&sc->kstat[kid][2], r);
+        if (a) atomicAdd(&sc->kstat[kid][3], a);
     }
 }
 

@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(256, 4) k_ds_primal(DMedium M, PathSrc S, uint
             alive = false;
         }
     }
-    flush_counters(sc, n_paths_done, 0, tl);  // the forward counts the vertices
+    flush_counters(sc, VRT_K_DS_PRIMAL, n_paths_done, 0, tl);  // the forward counts the vertices
 }
 
 __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, uint
             }
         }
     }
-    flush_counters(sc, 0, 0, tl);
+    flush_counters(sc, VRT_K_DS_REPLAY, 0, 0, tl);
 }
 
 int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed,
@@ -428,11 +428,17 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
         // [0] jobs, [1] records, [2] replay queue, [3] / [4] heads of the shadow kernels
         if ((e = cudaMemsetAsync(wv.hdr, 0, 5 * sizeof(unsigned long long), stream)) != cudaSuccess)
             return launch_status(e);
-        k_ds_primal<<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
+        {
+            KernelScope ks(VRT_K_DS_PRIMAL, stream);
+            k_ds_primal<<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
+        }
         if ((st = launch_shadow_record(M, src, wv, seed, ctx->scratch, ctx->num_sms, stream))) return st;
         if ((e = cudaMemsetAsync(wv.hdr, 0, sizeof(unsigned long long), stream)) != cudaSuccess)
             return launch_status(e);
-        k_ds_replay<<<blocksC, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, ctx->scratch, wv);
+        {
+            KernelScope ks(VRT_K_DS_REPLAY, stream);
+            k_ds_replay<<<blocksC, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, ctx->scratch, wv);
+        }
         if ((st = launch_shadow_adjoint(M, wv, seed, ctx->scratch, ctx->num_sms, stream))) return st;
         count_launches(2);
         if ((st = launch_status(cudaGetLastError()))) return st;
