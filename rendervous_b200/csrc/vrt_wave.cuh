@@ -24,9 +24,12 @@ struct ShadowJob {
 __device__ __forceinline__ void put_job(ShadowJob* J, unsigned long long slot, float3 x, float3 d, float3 wt,
                                         unsigned long long key, uint32_t tgt = 0u) {
     float4* p = reinterpret_cast<float4*>(J + slot);
-    p[0] = make_float4(x.x, x.y, x.z, d.x);
-    p[1] = make_float4(d.y, d.z, wt.x, wt.y);
-    p[2] = make_float4(wt.z, __uint_as_float(tgt), __uint_as_float((uint32_t)key), __uint_as_float((uint32_t)(key >> 32)));
+    // streaming stores: jobs are read once, by the next kernel; keep them from
+    // evicting the grids' lines in L2
+    __stcs(p, make_float4(x.x, x.y, x.z, d.x));
+    __stcs(p + 1, make_float4(d.y, d.z, wt.x, wt.y));
+    __stcs(p + 2, make_float4(wt.z, __uint_as_float(tgt), __uint_as_float((uint32_t)key),
+                              __uint_as_float((uint32_t)(key >> 32))));
 }
 
 struct JobView {

@@ -192,9 +192,7 @@ __global__ void __launch_bounds__(256, 4) k_ds_primal(DMedium M, PathSrc S, uint
         const unsigned long long r = reserve_slots(&wv.hdr[1], nrec);
         if (nrec) {
             VertexRec* rp = wv.recs + r;
-            rp->Te = 1.0f;
-            rp->Ts = 1.0f;
-            rp->next = kNone;
+            __stcs(reinterpret_cast<uint4*>(rp), make_uint4(__float_as_uint(1.0f), __float_as_uint(1.0f), kNone, 0u));
             if (first == kNone) first = (uint32_t)r;
             else wv.recs[prev].next = (uint32_t)r;
             prev = (uint32_t)r;
@@ -208,8 +206,8 @@ __global__ void __launch_bounds__(256, 4) k_ds_primal(DMedium M, PathSrc S, uint
         if (finish) {  // end of the primal (_NEE_DS.h:106-110): escape term, then the path's totals
             if (!scattered) Racc = Racc + M.env * W;
             float* io = wv.info + 8 * (pid - wv.p_begin);
-            reinterpret_cast<float4*>(io)[0] = make_float4(Racc.x, Racc.y, Racc.z, Rspacc.x);
-            reinterpret_cast<float4*>(io)[1] = make_float4(Rspacc.y, Rspacc.z, __uint_as_float(first), 0.0f);
+            __stcs(reinterpret_cast<float4*>(io), make_float4(Racc.x, Racc.y, Racc.z, Rspacc.x));
+            __stcs(reinterpret_cast<float4*>(io) + 1, make_float4(Rspacc.y, Rspacc.z, __uint_as_float(first), 0.0f));
             alive = false;
         }
     }
