@@ -360,3 +360,63 @@ def test_invalid_arguments_raise(cuda):
     R = torch.empty(4, 3, device=cuda)
     st = lib.vrt_radiance_fw(_lib.context().ptr, m, 0, _lib.fptr(rays), 4, 0, _lib.fptr(R), _lib.stream_handle(cuda))
     assert st == 1
+
+
+def test_ds_gradient_statistics_independent_seeds(cuda):
+    """NEE_DS sigma gradients of the GPU and the oracle from independent seeds:
+    sums over 8^3-voxel blocks agree within 3 standard errors (6 estimates a
+    side; 90 % of the blocks under 3, none above 8 -- the per-block estimates
+    are heavy-tailed and the variances come from 6 samples)."""
+    wl = synthetic.WORKLOADS["plain_forward_64"]
+    sig = torch.from_numpy(synthetic.make_sigma(wl["sigma"])).to(cuda)
+    H = W = 32
+    spp = 8
+    dimg = torch.from_numpy(np.random.default_rng(5).random((1, H, W, 3)).astype(np.float32)).to(cuda)
+
+    def blocks(g):
+        g = np.asarray(g, np.float64).reshape(64, 64, 64)[:64, :64, :64]
+        return g.reshape(8, 8, 8, 8, 8, 8).sum(axis=(1, 3, 5)).ravel()
+
+    gpu, cpu = [], []
+    for k in range(6):
+        field = build_field(sig.clone(), albedo=0.8, env=1.0, sun_dir=(0.3, 0.8, 0.5), g=0.4, max_bounces=16,
+                            sigma_requires_grad=True)
+        cam, img = _capture(field, cuda, H, W, spp, seed=400 + k)
+        (img * dimg).sum().backward()
+        gpu.append(blocks(field.sigma.grid.grad.cpu().numpy()))
+        d, sc = _grad_scene(field)
+        oracle.capture_bw(sc, "ds", front_camera(1).numpy(), W, H, math.pi / 4, True, spp, 900 + k,
+                          dimg.cpu().numpy())
+        cpu.append(blocks(sc.sigma_grad))
+    bg, bc = np.stack(gpu), np.stack(cpu)
+    live = (np.abs(bg).mean(0) + np.abs(bc).mean(0)) > 1e-6 * np.abs(bc).mean(0).max()
+    se = np.sqrt(bg.var(0, ddof=1) / 6 + bc.var(0, ddof=1) / 6) + 1e-12
+    z = np.abs(bg.mean(0) - bc.mean(0))[live] / se[live]
+    assert live.sum() > 50
+    assert (z < 3).mean() >= 0.9 and z.max() < 8, (np.sort(z)[-5:], live.sum())
+
+
+def test_kernel_stats_add_up(cuda):
+    """vrt_kernel_stats: with timing on, the wavefront kernels of a capture and
+    its adjoint report launches, event time and tallies; the per-kernel lookups
+    add up to the context's total."""
+    ffi, lib = _lib.ffi_lib()
+    stream = _lib.stream_handle(cuda)
+    ctx = _lib.context(cuda)
+    ks = ffi.new("vrt_kernel_stat[]", 6)
+    maps.check()
+    _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
+    lib.vrt_set_kernel_timing(1)
+    maps.set_sync_checks(False)  # keep the context totals of both calls
+    try:
+        field = _c1_field(cuda, majorant="grid", brick=8, sigma_requires_grad=True)
+        cam, img = _capture(field, cuda, 32, 32, 4, seed=3)
+        img.sum().backward()
+        _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
+        totals = maps.check()
+    finally:
+        lib.vrt_set_kernel_timing(0)
+        maps.set_sync_checks(True)
+    assert all(ks[i].launches > 0 and ks[i].ms > 0 for i in range(6))
+    assert sum(ks[i].lookups for i in range(6)) == totals["lookups"]
+    assert ks[1].steps > 0 and ks[4].reds > 0
