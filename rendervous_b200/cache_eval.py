@@ -128,7 +128,7 @@ def plain_curve(field, cam, pixels, ref, budget_s, spp_chunk, seed):
     t = Timer()
     curve = []
     n = 0
-    while t.total < budget_s:
+    while n == 0 or t.total < budget_s:
         img = {}
         t.run(lambda: img.setdefault("x", cam.capture(field, fw_samples=spp_chunk, seed=seed + n)))
         acc += img["x"]
@@ -151,7 +151,7 @@ def cached_curve(field, cam, pixels, ref, budget_s, spp, warmup, seed, **kw):
     acc = torch.zeros(cam.views, cam.height, cam.width, 3, device=dev)
     curve = []
     n = 0
-    while t.total < budget_s:
+    while n == 0 or t.total < budget_s:  # at least one frame, even when the warm-up used the budget
         def frame():
             r.train_frame()
             r.render_frame(acc, spp)
