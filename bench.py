@@ -248,7 +248,7 @@ def cpu_sample(seconds_hint: float = 10.0, threads: int | None = None):
 def run_ours(args):
     import torch
     import torch.distributed as dist
-    from rendervous_b200 import _lib, build as vbuild, maps
+    from rendervous_b200 import _lib, build as vbuild, distributed as vdist, maps
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -278,12 +278,10 @@ def run_ours(args):
     def step(k):
         sigma_t.grad = None
         albedo_t.grad = None
-        img = cam.capture(field, fw_samples=spp, bw_samples=spp, seed=1000 * (rank + 1) + k)
+        img = cam.capture(field, fw_samples=spp, bw_samples=spp, seed=vdist.rank_seed(k, rank))
         loss = ((img - target) ** 2).sum()
         loss.backward()
-        if world > 1:
-            dist.all_reduce(sigma_t.grad)
-            dist.all_reduce(albedo_t.grad)
+        vdist.allreduce_grads([sigma_t, albedo_t])
         return loss
 
     for k in range(args.warmup):
@@ -320,13 +318,8 @@ def run_ours(args):
         dist.barrier()
     counters = maps.check()
     total_ms = sum(times)
-    ms_t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-    vt = torch.tensor([float(counters["vertices"])], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(vt)
-    total_ms = float(ms_t.item())
-    vertices = float(vt.item())
+    total_ms = vdist.max_over_ranks(total_ms, dev)        # the job ends with its slowest rank
+    vertices = vdist.sum_over_ranks(float(counters["vertices"]), dev)
     value = vertices / (total_ms / 1e3)
 
     # ---- per-kernel split for the roofline (forward kernel and adjoint kernel)
@@ -401,15 +394,12 @@ def run_ours(args):
             e1.synchronize()
             e2e_ms.append(e0.elapsed_time(e1))
         c = maps.check()
-        et = torch.tensor([sum(e2e_ms)], device=dev, dtype=torch.float64)
-        ev = torch.tensor([float(c["vertices"])], device=dev, dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(et, op=dist.ReduceOp.MAX)
-            dist.all_reduce(ev)
-        e2e = {"value": float(ev.item()) / (float(et.item()) / 1e3), "unit": UNIT,
+        e2e_total = vdist.max_over_ranks(sum(e2e_ms), dev)
+        e2e_vertices = vdist.sum_over_ranks(float(c["vertices"]), dev)
+        e2e = {"value": e2e_vertices / (e2e_total / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": int(h_sigma.numel() * 4 + h_albedo.numel() * 4),
                "d2h_bytes_per_step": int(h_gs.numel() * 4 + h_ga.numel() * 4 + 4),
-               "ms_per_step": float(et.item()) / max(1, args.steps)}
+               "ms_per_step": e2e_total / max(1, args.steps)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -58,6 +58,7 @@ __device__ __forceinline__ unsigned long long job_key(uint64_t pid, uint32_t for
 // Reserves n slots for this lane (all 32 lanes call it): an inclusive warp scan
 // of n, one atomicAdd by the last lane, the base broadcast.
 __device__ __forceinline__ unsigned long long reserve_slots(unsigned long long* count, int n) {
+    if (!__any_sync(kAll, n != 0)) return 0;  // most iterations emit nothing: skip the scan
     const unsigned lane = threadIdx.x & 31u;
     int incl = n;
 #pragma unroll
