@@ -163,10 +163,11 @@ def profiled_traffic(kernel: str):
     return None
 
 
-KERNELS = ["k_walk_fw", "k_shadow_fw", "k_ds_primal", "k_shadow_T", "k_ds_replay", "k_shadow_adj"]
+KERNELS = ["k_walk_fw", "k_shadow_fw", "k_ds_primal", "k_shadow_T", "k_ds_replay", "k_shadow_adj", "k_ds_rewalk"]
 # the kernel functions each slot covers (ratio-tracking shadows run k_shadow_run / k_shadow_adj)
 KERNEL_FUNCS = {"k_walk_fw": "k_walk_fw", "k_shadow_fw": "k_shadow_run<0, 0>", "k_ds_primal": "k_ds_primal",
-                "k_shadow_T": "k_shadow_run<0, 1>", "k_ds_replay": "k_ds_replay", "k_shadow_adj": "k_shadow_adj<0>"}
+                "k_shadow_T": "k_shadow_run<0, 1>", "k_ds_replay": "k_ds_replay", "k_shadow_adj": "k_shadow_adj<0>",
+                "k_ds_rewalk": "k_ds_rewalk"}
 
 
 def gather_peaks(dev, reps: int = 5) -> dict:
@@ -197,18 +198,20 @@ def gather_peaks(dev, reps: int = 5) -> dict:
 
 def kernel_table(stats, steps: int) -> dict:
     """Per wavefront kernel over the timed steps: launches, event time, and
-    algorithmic bytes (32 B per sigma / albedo lookup, 4 B per atomic add)."""
+    algorithmic bytes (32 B per sigma / albedo lookup, 4 B per atomic add, and
+    the NEE_DS collision-log bytes the kernel writes or reads)."""
     table = {}
     for name, st in zip(KERNELS, stats):
         if st.launches == 0:
             continue
-        alg = 32.0 * st.lookups + 32.0 * st.albedo_lookups + 4.0 * st.reds
+        alg = 32.0 * st.lookups + 32.0 * st.albedo_lookups + 4.0 * st.reds + float(st.log_bytes)
         ms_launch = st.ms / st.launches
         table[name] = {"function": KERNEL_FUNCS[name], "launches_per_step": st.launches / steps,
                        "ms_per_step": st.ms / steps, "ms_per_launch": ms_launch,
                        "bytes_per_launch": alg / st.launches,
                        "gbs": (alg / st.launches) / (ms_launch / 1e3) / 1e9 if ms_launch > 0 else None,
-                       "lookups_per_step": st.lookups / steps, "reds_per_step": st.reds / steps}
+                       "lookups_per_step": st.lookups / steps, "reds_per_step": st.reds / steps,
+                       "log_bytes_per_step": st.log_bytes / steps}
     tot = sum(v["ms_per_step"] for v in table.values()) or 1.0
     for v in table.values():
         v["share"] = v["ms_per_step"] / tot

@@ -131,24 +131,32 @@ int64_t vrt_launch_count(void);
 
 /* Per-kernel measurement of the wavefront kernels (no reference counterpart).
    Each kernel adds its own tallies (tracking steps, sigma lookups, atomic adds,
-   albedo lookups) to a slot of the context; with timing on, the library also
-   brackets every launch with CUDA events on its stream.  vrt_kernel_stats
-   waits for `stream`, fills VRT_K_COUNT entries (launches, event time summed in
-   ms, tallies) accumulated since its last call, and clears them. */
+   albedo lookups, bytes of the NEE_DS collision log written or read) to a slot
+   of the context; with timing on, the library also brackets every launch with
+   CUDA events on its stream.  vrt_kernel_stats waits for `stream`, fills
+   VRT_K_COUNT entries (launches, event time summed in ms, tallies) accumulated
+   since its last call, and clears them.  The replay's `steps` are the logged
+   collisions it replayed. */
 enum {
     VRT_K_WALK_FW = 0,     /* forward walk (primary paths, shadow jobs) */
     VRT_K_SHADOW_FW = 1,   /* forward shadow transmittances */
-    VRT_K_DS_PRIMAL = 2,   /* NEE_DS adjoint: primal walk */
+    VRT_K_DS_PRIMAL = 2,   /* NEE_DS adjoint: primal walk (writes the collision log) */
     VRT_K_SHADOW_T = 3,    /* NEE_DS adjoint: the primal's shadow transmittances */
-    VRT_K_DS_REPLAY = 4,   /* NEE_DS adjoint: replay walk (sigma / albedo scatters) */
+    VRT_K_DS_REPLAY = 4,   /* NEE_DS adjoint: replay of the logged collisions (sigma / albedo scatters) */
     VRT_K_SHADOW_ADJ = 5,  /* NEE_DS adjoint: transmittance adjoints */
-    VRT_K_COUNT = 6
+    VRT_K_DS_REWALK = 6,   /* NEE_DS adjoint: replay walk of the paths the log could not hold */
+    VRT_K_COUNT = 7
 };
 typedef struct vrt_kernel_stat {
     int64_t launches;
     double ms;                       /* 0 unless timing was on */
-    int64_t steps, lookups, reds, albedo_lookups;
+    int64_t steps, lookups, reds, albedo_lookups, log_bytes;
 } vrt_kernel_stat;
+/* Caps the NEE_DS collision log of a context at `events` collision records
+   (32 bytes each) per round; 0 restores the automatic size.  Paths whose
+   collisions do not fit are replayed by walking them again (same gradients,
+   more time). */
+int vrt_set_collision_log_limit(vrt_context* ctx, int64_t events);
 void vrt_set_kernel_timing(int32_t on);
 /* Gather microbenchmark (the roofline of the lookups): threads x per_thread
    random 32-byte loads (L1 bypassed) from `buffer` (bytes long, 32-byte

@@ -326,6 +326,14 @@ int vrt_gather_peak(const void* buffer, int64_t bytes, int64_t threads, int32_t 
     return launch_status(cudaGetLastError());
 }
 
+int vrt_set_collision_log_limit(vrt_context* ctx, int64_t events) {
+    int st = check_ctx(ctx);
+    if (st) return st;
+    if (events < 0) return VRT_E_BAD_SHAPE;
+    ctx->log_limit = (unsigned long long)events;
+    return VRT_OK;
+}
+
 void vrt_set_kernel_timing(int32_t on) {
     KernelTiming& t = timing();
     std::lock_guard<std::mutex> lock(t.mu);
@@ -338,7 +346,7 @@ int vrt_kernel_stats(vrt_context* ctx, void* stream, vrt_kernel_stat* out) {
     if (!out) return VRT_E_NULL_POINTER;
     cudaStream_t s = (cudaStream_t)stream;
     if (cudaStreamSynchronize(s) != cudaSuccess) return launch_status(cudaGetLastError());
-    unsigned long long k[8][4];
+    unsigned long long k[8][5];
     if (cudaMemcpy(k, ctx->scratch->kstat, sizeof(k), cudaMemcpyDeviceToHost) != cudaSuccess) return VRT_E_CUDA;
     if (cudaMemset(ctx->scratch->kstat, 0, sizeof(k)) != cudaSuccess) return VRT_E_CUDA;
     KernelTiming& t = timing();
@@ -361,6 +369,7 @@ int vrt_kernel_stats(vrt_context* ctx, void* stream, vrt_kernel_stat* out) {
         out[i].lookups = (int64_t)k[i][1];
         out[i].reds = (int64_t)k[i][2];
         out[i].albedo_lookups = (int64_t)k[i][3];
+        out[i].log_bytes = (int64_t)k[i][4];
         t.launches[i] = 0;
     }
     return VRT_OK;
@@ -394,6 +403,7 @@ int vrt_context_create(int32_t device, vrt_context** out) {
     ctx->scratch = nullptr;
     ctx->wave = nullptr;
     ctx->wave_bytes = 0;
+    ctx->log_limit = 0;
     if (cudaMalloc(&ctx->scratch, sizeof(DScratch)) != cudaSuccess) { delete ctx; return VRT_E_CUDA; }
     if (cudaMemset(ctx->scratch, 0, sizeof(DScratch)) != cudaSuccess) { cudaFree(ctx->scratch); delete ctx; return VRT_E_CUDA; }
     *out = ctx;

@@ -152,9 +152,10 @@ __device__ __forceinline__ float3 normalized(const DMedium& M, float3 x) {
     return make_float3((x.x - M.bmin.x) * M.inv_bsize.x, (x.y - M.bmin.y) * M.inv_bsize.y, (x.z - M.bmin.z) * M.inv_bsize.z);
 }
 // Per-thread work tally: free-flight steps, sigma lookups (8 node gathers
-// each), atomic adds and albedo lookups.  Kept in registers, summed per warp.
+// each), atomic adds, albedo lookups and bytes of the NEE_DS collision log
+// written or read.  Kept in registers, summed per warp.
 struct Tally {
-    uint32_t steps = 0, lookups = 0, reds = 0, albedo = 0;
+    uint32_t steps = 0, lookups = 0, reds = 0, albedo = 0, logb = 0;
 };
 
 __device__ __forceinline__ float sigma(const DMedium& M, float3 x, Tally& tl) {

@@ -11,6 +11,7 @@ struct vrt_context {
     vrt::DScratch* scratch;  // device memory
     void* wave;              // wavefront job buffer (grown on demand)
     size_t wave_bytes;
+    unsigned long long log_limit;  // NEE_DS collision-log cap in records (0: automatic)
 };
 
 namespace vrt {

@@ -56,9 +56,9 @@ struct DScratch {
     unsigned long long albedo;
     unsigned int status;           // 1 << VRT_E_* bits
     unsigned int detail;           // which guard raised a device error (bit per site)
-    // per-kernel tallies of the wavefront kernels (VRT_K_*): steps, lookups, atomics, albedo lookups;
-    // not cleared by vrt_context_sync, read and cleared by vrt_kernel_stats
-    unsigned long long kstat[8][4];
+    // per-kernel tallies of the wavefront kernels (VRT_K_*): steps, lookups, atomics, albedo lookups,
+    // collision-log bytes; not cleared by vrt_context_sync, read and cleared by vrt_kernel_stats
+    unsigned long long kstat[8][5];
 };
 
 }  // namespace vrt

@@ -75,12 +75,47 @@ __device__ __forceinline__ unsigned long long reserve_slots(unsigned long long* 
     return base + (unsigned long long)(incl - n);
 }
 
+// Warp-aggregated reservation on four counters at once: the lanes' counts are
+// packed a byte apiece (each warp total stays below 256), one shuffle scan
+// gives every lane its offsets, and lanes 31, 30, 29 and 28 add the totals to
+// counters 0..3.  Returns each lane's first slot per counter.
+struct Slots4 {
+    unsigned long long s0, s1, s2, s3;
+};
+__device__ __forceinline__ Slots4 reserve_slots4(unsigned long long* c0, unsigned long long* c1,
+                                                 unsigned long long* c2, unsigned long long* c3, uint32_t packed) {
+    Slots4 out = {0ull, 0ull, 0ull, 0ull};
+    if (!__any_sync(kAll, packed != 0u)) return out;
+    const unsigned lane = threadIdx.x & 31u;
+    uint32_t incl = packed;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(kAll, incl, o);
+        if ((int)lane >= o) incl += v;
+    }
+    const uint32_t total = __shfl_sync(kAll, incl, 31);
+    unsigned long long b = 0;
+    const unsigned f = 31u - lane;
+    if (f < 4u) {
+        const uint32_t t = (total >> (8u * f)) & 0xffu;
+        unsigned long long* c = f == 0u ? c0 : (f == 1u ? c1 : (f == 2u ? c2 : c3));
+        if (t) b = atomicAdd(c, (unsigned long long)t);
+    }
+    const uint32_t excl = incl - packed;
+    out.s0 = __shfl_sync(kAll, b, 31) + (excl & 0xffu);
+    out.s1 = __shfl_sync(kAll, b, 30) + ((excl >> 8) & 0xffu);
+    out.s2 = __shfl_sync(kAll, b, 29) + ((excl >> 16) & 0xffu);
+    out.s3 = __shfl_sync(kAll, b, 28) + (excl >> 24);
+    return out;
+}
+
 // Per-warp sums of the lanes' tallies into the context counters.  `verts`
 // counts forward path vertices only (the metric's unit); adjoint kernels pass 0.
 __device__ __forceinline__ void flush_counters(DScratch* sc, int kid, uint32_t paths, uint32_t verts, const Tally& tl) {
-    unsigned long long p = paths, v = verts, s = tl.steps, l = tl.lookups, a = tl.albedo, r = tl.reds;
+    unsigned long long p = paths, v = verts, s = tl.steps, l = tl.lookups, a = tl.albedo, r = tl.reds, b = tl.logb;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
+        b += __shfl_down_sync(kAll, b, o);
         p += __shfl_down_sync(kAll, p, o);
         v += __shfl_down_sync(kAll, v, o);
         s += __shfl_down_sync(kAll, s, o);
@@ -99,6 +134,7 @@ __device__ __forceinline__ void flush_counters(DScratch* sc, int kid, uint32_t p
         if (l) atomicAdd(&sc->kstat[kid][1], l);
         if (r) atomicAdd(&sc->kstat[kid][2], r);
         if (a) atomicAdd(&sc->kstat[kid][3], a);
+        if (b) atomicAdd(&sc->kstat[kid][4], b);
     }
 }
 
@@ -265,21 +301,44 @@ __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tal
 
 
 constexpr uint32_t kNone = 0xffffffffu;
-// A primal vertex of the NEE_DS adjoint wavefront: its two shadow
-// transmittances and the next vertex of the same path.
+constexpr uint32_t kUnlogged = 0xfffffffeu;  // a path whose collisions did not fit the log
+// A real-collision vertex of the NEE_DS primal (64 bytes): its two shadow
+// transmittances (filled by the shadow kernel), the next vertex of the same
+// path, the fork of its light rays, and what the replay needs to redo the
+// vertex without walking to it: the albedo, the environment direction,
+// radiance and the two phase values.
 struct VertexRec {
     float Te, Ts;
-    uint32_t next, pad;
+    uint32_t next, fork;
+    float sa[3], ph_env;
+    float wnee[3], ph_sun;
+    float Le[3], pad;
 };
+static_assert(sizeof(VertexRec) == 64, "vertex records are four 16-byte words");
+
+// One tracking collision of the NEE_DS primal (32 bytes, two 16-byte words):
+// position and sigma there; majorant, next collision of the path, the vertex
+// record (real collisions that scatter) and bit 0 = real collision.
+struct CollisionRec {
+    float4 xs;   // x, y, z, sigma
+    uint4 link;  // majorant bits, next, record, flags
+};
+static_assert(sizeof(CollisionRec) == 32, "collision records are two 16-byte words");
 
 // Buffers of one round of the NEE_DS adjoint wavefront (vrt_wave_ds.cu).
 struct WaveBw {
     ShadowJob* jobs;
     VertexRec* recs;
-    float* info;               // per path: R (3), Rsp (3), first record, pad
-    unsigned long long* hdr;   // [0] jobs, [1] records, [2] replay queue
-    unsigned long long cap_jobs, cap_recs, cap_paths;
-    unsigned long long res_jobs, res_recs, lanes;
+    CollisionRec* evs;         // the collision log
+    float* info;               // per path: R (3), Rsp (3), first record, first collision (or kUnlogged)
+    uint32_t* over;            // round-local indices of the paths left out of the log
+    uint2* list;               // paths with logged collisions: round-local index, first collision
+    // [0] jobs, [1] records, [2] re-walk queue, [3] / [4] heads of the shadow
+    // kernels, [5] collisions, [6] paths left out of the log, [7] replay queue,
+    // [8] replay list
+    unsigned long long* hdr;
+    unsigned long long cap_jobs, cap_recs, cap_paths, cap_evs;
+    unsigned long long res_jobs, res_recs, res_evs, lanes;
     uint64_t p_begin;
 };
 

@@ -1,10 +1,11 @@
 // vrt_wave_ds.cu -- the NEE_DS adjoint as a wavefront (sm_100a).
 //
 // Compiled with -fmad=false: the primal walk (k_ds_primal) and the replay walk
-// (k_ds_replay) are separate kernels that must retrace the same path bit for
-// bit, so every operation is rounded on its own and no a*b+c can be
-// contracted differently in the two.  The shadow kernels of the rounds live in
-// vrt_wave.cu.
+// of the paths the collision log could not hold (k_ds_rewalk) are separate
+// kernels that must retrace the same path bit for bit, and the log replay
+// (k_ds_replay) must redo the primal's throughput arithmetic exactly, so every
+// operation is rounded on its own and no a*b+c can be contracted differently
+// in them.  The shadow kernels of the rounds live in vrt_wave.cu.
 #include "vrt_wave.cuh"
 
 namespace vrt {
@@ -14,27 +15,33 @@ using namespace wave;
 // ------------------------------------------------------------------------
 // NEE_DS adjoint (include/vr_path_integrator_NEE_DS.h:6-206) as a wavefront.
 //
-// With the default replay majorant (the primal's) the replay retraces the
-// primal's vertices exactly -- same draws, same throughputs, and shadow j of
-// the path draws from fork j in both passes -- so a vertex's shadow
-// transmittances are computed once and stored, and the transmittance adjoints
-// (which feed nothing back into the path) run as independent jobs:
+// With the default replay majorant (the primal's) the reference's replay
+// retraces the primal's vertices exactly -- same draws, same throughputs, and
+// shadow j of the path draws from fork j in both passes.  So the primal logs
+// what the replay would recompute: a 32-byte collision record per tracking
+// collision and a 64-byte vertex record per scattering vertex; a vertex's
+// shadow transmittances are computed once into its record, and the
+// transmittance adjoints (which feed nothing back into the path) run as
+// independent jobs:
 //
-//   A k_ds_primal   the primal walk: per real collision a vertex record (linked
-//                   per path) and a T job per light; per path the emission and
-//                   escape terms of R and Rsp
+//   A k_ds_primal   the primal walk: per tracking collision a collision record,
+//                   per real collision a vertex record (both linked per path)
+//                   and a T job per light; per path the emission and escape
+//                   terms of R and Rsp
 //   B (vrt_wave.cu) T of each job into its record, weight * T into its
 //                   path's R (or Rsp after a zero-density collision)
-//   C k_ds_replay   the replay walk: dL/dsigma at every collision, dL/dalbedo
-//                   at real ones, the R bookkeeping from the stored T, and a
-//                   transmittance-adjoint job per light with dL/dT != 0
+//   C k_ds_replay   the replay from the log: dL/dsigma at every collision,
+//                   dL/dalbedo at real ones, the R bookkeeping from the stored
+//                   T, and a transmittance-adjoint job per light with dL/dT != 0
+//     k_ds_rewalk   the same for the paths the log had no room for, by walking
+//                   them again with the primal's draws
 //   D (vrt_wave.cu) the ratio / delta tracking adjoint or the DDA adjoint of
 //                   each job
 //
 // Rounds bound the buffers as in the forward wavefront.
 // ------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(256, 4) k_ds_primal(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
+__global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
                                                     DScratch* sc, WaveBw wv) {
     const unsigned lane = threadIdx.x & 31u;
     const float EPS = 0.00000001f;
@@ -47,8 +54,9 @@ __global__ void __launch_bounds__(256, 4) k_ds_primal(DMedium M, PathSrc S, uint
     bool scattered = false, alive = false, exhausted = false;
     int bounces = 0;
     uint64_t pid = 0;
-    uint32_t steps_path = 0, first = kNone, prev = kNone;
+    uint32_t steps_path = 0, first = kNone, prev = kNone, first_ev = kNone, prev_ev = kNone;
     uint32_t n_paths_done = 0;
+    bool logged = false;
     Tally tl;
 
     while (true) {
@@ -59,9 +67,10 @@ __global__ void __launch_bounds__(256, 4) k_ds_primal(DMedium M, PathSrc S, uint
             if ((int)lane == leader) {
                 const unsigned long long uj = *((volatile unsigned long long*)&wv.hdr[0]);
                 const unsigned long long ur = *((volatile unsigned long long*)&wv.hdr[1]);
+                const unsigned long long ue = *((volatile unsigned long long*)&wv.hdr[5]);
                 const unsigned long long up = *((volatile unsigned long long*)&sc->next_path) - wv.p_begin;
                 const bool room = uj + wv.res_jobs <= wv.cap_jobs && ur + wv.res_recs <= wv.cap_recs &&
-                                  up + wv.lanes <= wv.cap_paths;
+                                  ue + wv.res_evs <= wv.cap_evs && up + wv.lanes <= wv.cap_paths;
                 base = room ? atomicAdd(&sc->next_path, (unsigned long long)__popc(want)) : ~0ull;
             }
             base = __shfl_sync(kAll, base, leader);
@@ -90,6 +99,9 @@ __global__ void __launch_bounds__(256, 4) k_ds_primal(DMedium M, PathSrc S, uint
                     steps_path = 0;
                     first = kNone;
                     prev = kNone;
+                    first_ev = kNone;
+                    prev_ev = kNone;
+                    logged = true;
                     ff = Flight();
                     alive = true;
                     ++n_paths_done;
@@ -98,10 +110,11 @@ __global__ void __launch_bounds__(256, 4) k_ds_primal(DMedium M, PathSrc S, uint
         }
         if (__all_sync(kAll, !alive && exhausted)) break;
 
-        int nrec = 0, nj = 0;
+        int nrec = 0, nj = 0, nev = 0;
         bool finish = false, rsp = false;
-        float3 wnee = f3(0.0f), we = f3(0.0f), ws = f3(0.0f);
-        uint32_t jfork = 0;
+        float3 wnee = f3(0.0f), we = f3(0.0f), ws = f3(0.0f), sa = f3(0.0f), Le = f3(0.0f);
+        float ev_s = 0.0f, ev_m = 0.0f, ph_env = 0.0f, ph_sun = 0.0f;
+        uint32_t jfork = 0, ev_real = 0;
         if (alive) {
             int ev = 0;  // 0 none, 1 collision, 2 end
             if (!(d > EPS)) {
@@ -137,10 +150,14 @@ __global__ void __launch_bounds__(256, 4) k_ds_primal(DMedium M, PathSrc S, uint
                 if (need) {
                     const float s = sigma(M, x, tl);
                     const float Pc = (s + eps) / m;
+                    nev = logged ? 1 : 0;
+                    ev_s = s;
+                    ev_m = m;
                     if (rng.uniform() >= Pc) {  // null collision (_NEE_DS.h:41-45)
                         W = W * ((1.0f - s / m) / (1.0f - Pc));
                         d -= t;
                     } else {  // real collision (_NEE_DS.h:48-99)
+                        ev_real = 1u;
                         scattered = true;
                         bool dead = false;
                         if (s < EPS) {
@@ -152,12 +169,16 @@ __global__ void __launch_bounds__(256, 4) k_ds_primal(DMedium M, PathSrc S, uint
                         if (dead) {
                             ev = 2;
                         } else {
-                            const float3 sa = albedo(M, x, tl);
+                            sa = albedo(M, x, tl);
                             const float3 acc = W * (f3(1.0f) - sa) * M.emission;
                             W = W * sa;
-                            const float3 Le = environment_sample(M, rng, wnee);
-                            we = W * Le * phase(M, w, wnee);
-                            if (M.has_sun) ws = W * M.sun_L * phase(M, w, M.sun_dir);
+                            Le = environment_sample(M, rng, wnee);
+                            ph_env = phase(M, w, wnee);
+                            we = W * Le * ph_env;
+                            if (M.has_sun) {
+                                ph_sun = phase(M, w, M.sun_dir);
+                                ws = W * M.sun_L * ph_sun;
+                            }
                             jfork = rng.ntr;
                             rng.ntr += (uint32_t)lights;
                             const bool capped = M.max_bounces > 0 && bounces + 1 >= M.max_bounces;
@@ -188,41 +209,72 @@ __global__ void __launch_bounds__(256, 4) k_ds_primal(DMedium M, PathSrc S, uint
             }
             finish = ev == 2;
         }
-        // ---- the vertex record (linked to the path's previous one) and its T jobs
-        const unsigned long long r = reserve_slots(&wv.hdr[1], nrec);
-        if (nrec) {
-            VertexRec* rp = wv.recs + r;
-            __stcs(reinterpret_cast<uint4*>(rp), make_uint4(__float_as_uint(1.0f), __float_as_uint(1.0f), kNone, 0u));
+        // ---- one reservation for the T jobs, the vertex record, the collision
+        // record and (at the end of a path with logged collisions) its replay-list entry
+        const int nl = (finish && logged && (first_ev != kNone || nev)) ? 1 : 0;
+        const Slots4 sl = reserve_slots4(&wv.hdr[0], &wv.hdr[1], &wv.hdr[5], &wv.hdr[8],
+                                         (uint32_t)nj | ((uint32_t)nrec << 8) | ((uint32_t)nev << 16) |
+                                             ((uint32_t)nl << 24));
+        const unsigned long long r = sl.s1;
+        if (nrec) {  // the vertex record, linked to the path's previous one
+            uint4* rp = reinterpret_cast<uint4*>(wv.recs + r);
+            __stcs(rp, make_uint4(__float_as_uint(1.0f), __float_as_uint(1.0f), kNone, jfork));
+            __stcs(reinterpret_cast<float4*>(rp + 1), make_float4(sa.x, sa.y, sa.z, ph_env));
+            __stcs(reinterpret_cast<float4*>(rp + 2), make_float4(wnee.x, wnee.y, wnee.z, ph_sun));
+            __stcs(reinterpret_cast<float4*>(rp + 3), make_float4(Le.x, Le.y, Le.z, 0.0f));
+            tl.logb += (uint32_t)sizeof(VertexRec);
             if (first == kNone) first = (uint32_t)r;
             else wv.recs[prev].next = (uint32_t)r;
             prev = (uint32_t)r;
         }
-        const unsigned long long j = reserve_slots(&wv.hdr[0], nj);
+        if (nev) {  // the collision record (null and real), linked to the path's previous one
+            const unsigned long long je = sl.s2;
+            if (je >= wv.cap_evs) {
+                logged = false;  // the log is full: this path is replayed by walking it again
+            } else {
+                CollisionRec* ep = wv.evs + je;
+                __stcs(&ep->xs, make_float4(x.x, x.y, x.z, ev_s));
+                __stcs(&ep->link, make_uint4(__float_as_uint(ev_m), kNone, nrec ? (uint32_t)r : kNone, ev_real));
+                tl.logb += (uint32_t)sizeof(CollisionRec);
+                if (first_ev == kNone) first_ev = (uint32_t)je;
+                else wv.evs[prev_ev].link.y = (uint32_t)je;
+                prev_ev = (uint32_t)je;
+            }
+        }
         if (nj) {
+            const unsigned long long j = sl.s0;
             const uint32_t tgt = ((uint32_t)r << 2) | (rsp ? 2u : 0u);
             put_job(wv.jobs, j, x, wnee, we, job_key(pid, jfork), tgt);
             if (nj == 2) put_job(wv.jobs, j + 1, x, M.sun_dir, ws, job_key(pid, jfork + 1), tgt | 1u);
         }
         if (finish) {  // end of the primal (_NEE_DS.h:106-110): escape term, then the path's totals
             if (!scattered) Racc = Racc + M.env * W;
-            float* io = wv.info + 8 * (pid - wv.p_begin);
+            const uint64_t k = pid - wv.p_begin;
+            float* io = wv.info + 8 * k;
             __stcs(reinterpret_cast<float4*>(io), make_float4(Racc.x, Racc.y, Racc.z, Rspacc.x));
-            __stcs(reinterpret_cast<float4*>(io) + 1, make_float4(Rspacc.y, Rspacc.z, __uint_as_float(first), 0.0f));
+            __stcs(reinterpret_cast<float4*>(io) + 1, make_float4(Rspacc.y, Rspacc.z, __uint_as_float(first),
+                                                                  __uint_as_float(logged ? first_ev : kUnlogged)));
+            // an entry whose last collision found the log full is skipped by the replay
+            if (nl) __stcs(wv.list + sl.s3, make_uint2((uint32_t)k, logged ? first_ev : kUnlogged));
+            if (!logged) {
+                const unsigned long long o = atomicAdd(&wv.hdr[6], 1ull);
+                if (o < wv.cap_paths) wv.over[o] = (uint32_t)k;
+                else guard(sc, 8);
+            }
             alive = false;
         }
     }
     flush_counters(sc, VRT_K_DS_PRIMAL, n_paths_done, 0, tl);  // the forward counts the vertices
 }
 
-__global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
+__global__ void __launch_bounds__(256, 3) k_ds_rewalk(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
                                                     const float* __restrict__ dL, float div, DScratch* sc, WaveBw wv) {
     const unsigned lane = threadIdx.x & 31u;
     const float EPS = 0.00000001f;
     const float eps = M.ds_eps;
     const int lights = M.has_sun ? 2 : 1;
-    unsigned long long p_end = *((volatile unsigned long long*)&sc->next_path);
-    if (p_end > n_paths) p_end = n_paths;
-    const unsigned long long n_round = p_end - wv.p_begin;
+    unsigned long long n_over = *((volatile unsigned long long*)&wv.hdr[6]);
+    if (n_over > wv.cap_paths) n_over = wv.cap_paths;
     Flight ff;
     Rng rng;
     float3 x = f3(0.0f), w = f3(0.0f), W = f3(0.0f), R = f3(0.0f), Rsp = f3(0.0f), dLdR = f3(0.0f);
@@ -241,10 +293,11 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, uint
             if ((int)lane == leader) base = atomicAdd(&wv.hdr[2], (unsigned long long)__popc(want));
             base = __shfl_sync(kAll, base, leader);
             if (!alive && !exhausted) {
-                const unsigned long long k = base + __popc(want & ((1u << lane) - 1u));
-                if (k >= n_round) {
+                const unsigned long long q = base + __popc(want & ((1u << lane) - 1u));
+                if (q >= n_over) {
                     exhausted = true;
                 } else {
+                    const unsigned long long k = wv.over[q];
                     pid = wv.p_begin + k;
                     rng.init(seed, pid, 0);
                     float3 x0, w0;
@@ -389,6 +442,156 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, uint
             }
         }
     }
+    flush_counters(sc, VRT_K_DS_REWALK, 0, 0, tl);
+}
+
+// Replay of the logged collisions (_NEE_DS.h:112-206 without the walk): the
+// primal logged every tracking collision (position, sigma, majorant) and every
+// scattering vertex (albedo, light directions, radiance, phases, fork), so the
+// replay redoes the estimator's bookkeeping -- W, R and the scatter weights --
+// from the log with the same arithmetic, and no majorant walk, sigma or albedo
+// lookup, or random draw.  Lanes take paths from the primal's list of paths
+// with logged collisions; each iteration replays one collision per lane while
+// the loads of the path's next collision and of the vertex record are in
+// flight.
+__global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, const float* __restrict__ dL, float div,
+                                                    DScratch* sc, WaveBw wv) {
+    const unsigned lane = threadIdx.x & 31u;
+    const float EPS = 0.00000001f;
+    const float eps = M.ds_eps;
+    unsigned long long n_list = *((volatile unsigned long long*)&wv.hdr[8]);
+    if (n_list > wv.cap_paths) n_list = wv.cap_paths;
+    float3 W = f3(0.0f), R = f3(0.0f), Rsp = f3(0.0f), dLdR = f3(0.0f);
+    bool alive = false, exhausted = false;
+    int bounces = 0;
+    uint64_t pid = 0;
+    uint32_t steps_path = 0;
+    float4 xs = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // the collision to replay
+    uint4 ln = make_uint4(0u, kNone, kNone, 0u);
+    Tally tl;
+
+    while (true) {
+        unsigned want = __ballot_sync(kAll, !alive && !exhausted);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(&wv.hdr[7], (unsigned long long)__popc(want));
+            base = __shfl_sync(kAll, base, leader);
+            if (!alive && !exhausted) {
+                const unsigned long long q = base + __popc(want & ((1u << lane) - 1u));
+                if (q >= n_list) {
+                    exhausted = true;
+                } else {
+                    const uint2 e = __ldcs(wv.list + q);
+                    if (e.y != kUnlogged) {  // (a path whose last collision found the log full: k_ds_rewalk)
+                        const CollisionRec* ep = wv.evs + e.y;
+                        xs = __ldcs(&ep->xs);
+                        ln = __ldcs(&ep->link);
+                        const float4* io = reinterpret_cast<const float4*>(wv.info + 8 * (uint64_t)e.x);
+                        const float4 a = io[0], b = io[1];
+                        pid = wv.p_begin + e.x;
+                        dLdR = ld3(dL + 3 * out_index(S, pid)) / div;
+                        R = make_float3(a.x, a.y, a.z);
+                        Rsp = make_float3(a.w, b.x, b.y);
+                        W = f3(1.0f);
+                        bounces = 0;
+                        steps_path = 0;
+                        alive = true;
+                    }
+                }
+            }
+        }
+        if (__all_sync(kAll, !alive && exhausted)) break;
+
+        int nj = 0;
+        float3 xj = f3(0.0f), jd0 = f3(0.0f), jd1 = f3(0.0f);
+        float dT0 = 0.0f, dT1 = 0.0f;
+        uint32_t f0 = 0, f1 = 0;
+        if (alive) {
+            bool end = false;
+            // the next collision of the path and this one's vertex record, loaded ahead
+            const uint32_t nx = ln.y;
+            const bool real = (ln.w & 1u) != 0u;
+            float4 nxs = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            uint4 nln = make_uint4(0u, kNone, kNone, 0u);
+            if (nx != kNone) {
+                const CollisionRec* np = wv.evs + nx;
+                nxs = __ldcs(&np->xs);
+                nln = __ldcs(&np->link);
+            }
+            uint4 r0 = make_uint4(0u, 0u, 0u, 0u);
+            float4 r1 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), r2 = r1, r3 = r1;
+            if (real && ln.z != kNone) {
+                const uint4* rp = reinterpret_cast<const uint4*>(wv.recs + ln.z);
+                r0 = __ldcs(rp);
+                r1 = __ldcs(reinterpret_cast<const float4*>(rp + 1));
+                r2 = __ldcs(reinterpret_cast<const float4*>(rp + 2));
+                r3 = __ldcs(reinterpret_cast<const float4*>(rp + 3));
+            }
+            tl.logb += (uint32_t)sizeof(CollisionRec);
+            ++tl.steps;
+            const float3 x = make_float3(xs.x, xs.y, xs.z);
+            const float s = xs.w, m = __uint_as_float(ln.x);
+            const float Pc = (s + eps) / m;
+            float gsc;
+            if (!real) {  // _NEE_DS.h:130-140
+                gsc = dot(dLdR, -R / m / (1.0f - s / m));
+                W = W * ((1.0f - s / m) / (1.0f - Pc));
+            } else {      // _NEE_DS.h:142-150
+                gsc = dot(dLdR, s < EPS ? Rsp / eps : R / s);
+            }
+            if (gsc != 0.0f) sigma_bw(M, x, gsc, tl);
+            if (real) {   // the scattering vertex (_NEE_DS.h:151-203)
+                W = W * (s / m / Pc);
+                if (s < EPS || ln.z == kNone) {
+                    if (s >= EPS) guard(sc, 9);  // a scattering collision without its vertex record
+                    end = true;
+                } else {
+                    tl.logb += (uint32_t)sizeof(VertexRec);
+                    const float Te = __uint_as_float(r0.x), Ts = __uint_as_float(r0.y);
+                    const float3 sa = make_float3(r1.x, r1.y, r1.z);
+                    const float ph_nee = r1.w, ph_sun = r2.w;
+                    const float3 wnee = make_float3(r2.x, r2.y, r2.z), Le = make_float3(r3.x, r3.y, r3.z);
+                    float3 dL_dsa = dLdR * W * -1.0f * M.emission;
+                    R = R - W * (f3(1.0f) - sa) * M.emission;
+                    dL_dsa = dL_dsa + dLdR * R / make_float3(gmax(EPS, sa.x), gmax(EPS, sa.y), gmax(EPS, sa.z));
+                    albedo_bw(M, x, dL_dsa, tl);
+                    W = W * sa;
+                    const float dTe = dot(dLdR, W * Le * ph_nee);
+                    R = R - W * Te * Le * ph_nee;
+                    xj = x;
+                    if (dTe != 0.0f) { jd0 = wnee; dT0 = dTe; f0 = r0.w; nj = 1; }
+                    if (M.has_sun) {
+                        const float dTs = dot(dLdR, W * M.sun_L * ph_sun);
+                        R = R - W * Ts * M.sun_L * ph_sun;
+                        if (dTs != 0.0f) {
+                            if (nj == 0) { jd0 = M.sun_dir; dT0 = dTs; f0 = r0.w + 1u; nj = 1; }
+                            else { jd1 = M.sun_dir; dT1 = dTs; f1 = r0.w + 1u; nj = 2; }
+                        }
+                    }
+                    ++bounces;
+                    if ((M.max_bounces > 0 && bounces >= M.max_bounces) || all_less(W, EPS)) end = true;
+                }
+            }
+            xs = nxs;
+            ln = nln;
+            if (nx == kNone) end = true;
+            if (++steps_path > (uint32_t)kPathCap) {
+                guard(sc, 6);
+                end = true;
+            }
+            if (end) alive = false;
+        }
+        const unsigned long long j = reserve_slots(&wv.hdr[0], nj);
+        if (nj) {
+            if (j + (unsigned long long)nj > wv.cap_jobs) {
+                guard(sc, 7);
+            } else {
+                put_job(wv.jobs, j, xj, jd0, make_float3(dT0, 0.0f, 0.0f), job_key(pid, f0));
+                if (nj == 2) put_job(wv.jobs, j + 1, xj, jd1, make_float3(dT1, 0.0f, 0.0f), job_key(pid, f1));
+            }
+        }
+    }
     flush_counters(sc, VRT_K_DS_REPLAY, 0, 0, tl);
 }
 
@@ -399,9 +602,11 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     const unsigned long long lights = M.has_sun ? 2ull : 1ull, B = (unsigned long long)M.max_bounces;
     int blocksA = persistent_blocks((const void*)k_ds_primal, 256, ctx->num_sms);
     int blocksC = persistent_blocks((const void*)k_ds_replay, 256, ctx->num_sms);
+    int blocksW = persistent_blocks((const void*)k_ds_rewalk, 256, ctx->num_sms);
     const uint64_t need = (n_paths + 255) / 256;
     if ((uint64_t)blocksA > need) blocksA = (int)need;
     if ((uint64_t)blocksC > need) blocksC = (int)need;
+    if ((uint64_t)blocksW > need) blocksW = (int)need;
     WaveBw wv;
     wv.lanes = (unsigned long long)blocksA * 256ull;
     const unsigned long long inflight = wv.lanes < n_paths ? wv.lanes : n_paths;
@@ -411,20 +616,33 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     wv.cap_recs = wv.res_recs + batch_jobs(n_paths, 1);
     if (wv.cap_recs > (1ull << 30)) return VRT_E_UNSUPPORTED;  // record indices are 30-bit in a job
     wv.cap_paths = (n_paths < (1ull << 24) ? n_paths : (1ull << 24)) + wv.lanes;
-    const size_t bytes = 256 + wv.cap_jobs * sizeof(ShadowJob) + wv.cap_recs * sizeof(VertexRec) + wv.cap_paths * 32;
+    // the collision log: room for about four collisions per vertex record of a
+    // round, and admission of new paths stops while less than 16 collisions per
+    // lane in flight are left; a path that still finds it full is re-walked
+    wv.cap_evs = ctx->log_limit ? ctx->log_limit : 4ull * batch_jobs(n_paths, 1) + inflight * 16ull;
+    if (wv.cap_evs > 0xfff00000ull) wv.cap_evs = 0xfff00000ull;  // 32-bit links, kNone / kUnlogged reserved
+    wv.res_evs = inflight * 16ull < wv.cap_evs / 2 ? inflight * 16ull : wv.cap_evs / 2;
+    const size_t o_jobs = 256, o_recs = o_jobs + wv.cap_jobs * sizeof(ShadowJob);
+    const size_t o_info = o_recs + wv.cap_recs * sizeof(VertexRec), o_over = o_info + wv.cap_paths * 32;
+    const size_t o_list = o_over + ((wv.cap_paths * 4 + 255) & ~(size_t)255);
+    const size_t o_evs = o_list + ((wv.cap_paths * 8 + 255) & ~(size_t)255), bytes = o_evs + wv.cap_evs * 32;
     int st = ensure_wave_buffer(ctx, bytes);
     if (st) return st;
     char* base = static_cast<char*>(ctx->wave);
     wv.hdr = reinterpret_cast<unsigned long long*>(base);
-    wv.jobs = reinterpret_cast<ShadowJob*>(base + 256);
-    wv.recs = reinterpret_cast<VertexRec*>(base + 256 + wv.cap_jobs * sizeof(ShadowJob));
-    wv.info = reinterpret_cast<float*>(base + 256 + wv.cap_jobs * sizeof(ShadowJob) + wv.cap_recs * sizeof(VertexRec));
+    wv.jobs = reinterpret_cast<ShadowJob*>(base + o_jobs);
+    wv.recs = reinterpret_cast<VertexRec*>(base + o_recs);
+    wv.info = reinterpret_cast<float*>(base + o_info);
+    wv.over = reinterpret_cast<uint32_t*>(base + o_over);
+    wv.list = reinterpret_cast<uint2*>(base + o_list);
+    wv.evs = reinterpret_cast<CollisionRec*>(base + o_evs);
     wv.p_begin = 0;
     cudaError_t e = cudaMemsetAsync(&ctx->scratch->next_path, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return launch_status(e);
     for (int round = 0;; ++round) {
-        // [0] jobs, [1] records, [2] replay queue, [3] / [4] heads of the shadow kernels
-        if ((e = cudaMemsetAsync(wv.hdr, 0, 5 * sizeof(unsigned long long), stream)) != cudaSuccess)
+        // [0] jobs, [1] records, [2] re-walk queue, [3] / [4] heads of the shadow kernels,
+        // [5] collisions, [6] paths left out of the log, [7] replay queue, [8] replay list
+        if ((e = cudaMemsetAsync(wv.hdr, 0, 9 * sizeof(unsigned long long), stream)) != cudaSuccess)
             return launch_status(e);
         {
             KernelScope ks(VRT_K_DS_PRIMAL, stream);
@@ -435,10 +653,15 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
             return launch_status(e);
         {
             KernelScope ks(VRT_K_DS_REPLAY, stream);
-            k_ds_replay<<<blocksC, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, ctx->scratch, wv);
+            k_ds_replay<<<blocksC, 256, 0, stream>>>(M, src, dL, div, ctx->scratch, wv);
+        }
+        {
+            // exits at once when every path of the round fit the log
+            KernelScope ks(VRT_K_DS_REWALK, stream);
+            k_ds_rewalk<<<blocksW, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, ctx->scratch, wv);
         }
         if ((st = launch_shadow_adjoint(M, wv, seed, ctx->scratch, ctx->num_sms, stream))) return st;
-        count_launches(2);
+        count_launches(3);
         if ((st = launch_status(cudaGetLastError()))) return st;
         unsigned long long taken = 0;
         if ((e = cudaMemcpyAsync(&taken, &ctx->scratch->next_path, sizeof(taken), cudaMemcpyDeviceToHost, stream)) !=

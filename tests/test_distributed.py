@@ -66,6 +66,7 @@ def test_two_rank_gradient_allreduce(tmp_path):
     assert np.abs(_grad(0, 5) - _grad(1, 5)).sum() > 0          # the ranks' paths differ
     for r in range(2):
         g = np.load(f"{out}_{r}.npy")
-        assert np.allclose(g, expect, rtol=1e-6, atol=1e-9)
+        # the oracle's threads add into the gradient in any order: float rounding only
+        assert np.allclose(g, expect, rtol=1e-5, atol=1e-6 * np.abs(expect).max())
         slowest, total = np.load(f"{out}_{r}_red.npy")
         assert slowest == 20.0 and total == 3.0

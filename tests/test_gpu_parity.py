@@ -291,6 +291,45 @@ def test_capture_backward_matches_oracle(cuda, bw, kw):
         assert rela < 1e-2, rela
 
 
+@pytest.mark.parametrize("limit", [1, 3000])
+def test_ds_collision_log_overflow_rewalks(cuda, limit):
+    """Paths whose collisions do not fit the NEE_DS collision log (capped here
+    at `limit` records: none or part of the paths fit) are replayed by walking
+    them again; the gradients equal those of the fully logged replay up to the
+    order of the float atomics."""
+    ffi, lib = _lib.ffi_lib()
+    stream = _lib.stream_handle(cuda)
+    ctx = _lib.context(cuda)
+    wl = synthetic.WORKLOADS["plain_forward_64"]
+    sig = torch.from_numpy(synthetic.make_sigma(wl["sigma"])).to(cuda)
+    alb = torch.from_numpy(synthetic.uniform_grid(64, 0.6, 0.95, seed=8)).to(cuda)
+    dimg = None
+    grads, stats = [], []
+    ks = ffi.new("vrt_kernel_stat[]", lib.VRT_K_COUNT)
+    for lim in (0, limit):
+        field = build_field(sig, albedo_grid=torch.nn.Parameter(alb.clone()), env=1.0, sun_dir=(0.3, 0.8, 0.5),
+                            sun_radiance=3.0, g=0.4, max_bounces=16, sigma_requires_grad=True, integrator="nee_ds",
+                            majorant="grid", brick=8)
+        _lib.check(lib.vrt_set_collision_log_limit(ctx.ptr, lim))
+        try:
+            maps.check()
+            _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
+            cam, img = _capture(field, cuda, 32, 32, 4, seed=31)
+            if dimg is None:
+                dimg = torch.from_numpy(np.random.default_rng(0).random(img.shape).astype(np.float32)).to(cuda)
+            (img * dimg).sum().backward()
+            maps.check()
+            _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
+        finally:
+            _lib.check(lib.vrt_set_collision_log_limit(ctx.ptr, 0))
+        grads.append((field.sigma.grid.grad.cpu().numpy(), field.scattering_albedo.grid.grad.cpu().numpy()))
+        stats.append({k: getattr(ks[lib.VRT_K_DS_REWALK], k) for k in ("steps", "lookups", "reds")})
+    assert stats[0]["reds"] == 0 and stats[1]["reds"] > 0 and stats[1]["lookups"] > 0, stats
+    for a, b in zip(grads[0], grads[1]):
+        rel = np.abs(a - b).sum() / max(np.abs(a).sum(), 1e-30)
+        assert np.abs(a).sum() > 0 and rel < 1e-4, rel
+
+
 def test_ds_adjoint_matches_finite_difference(cuda):
     """E[dL/ds] along sigma -> s*sigma from the replay adjoint vs a central
     difference of the GPU forward with common random numbers."""
@@ -403,7 +442,8 @@ def test_kernel_stats_add_up(cuda):
     ffi, lib = _lib.ffi_lib()
     stream = _lib.stream_handle(cuda)
     ctx = _lib.context(cuda)
-    ks = ffi.new("vrt_kernel_stat[]", 6)
+    nk = lib.VRT_K_COUNT
+    ks = ffi.new("vrt_kernel_stat[]", nk)
     maps.check()
     _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
     lib.vrt_set_kernel_timing(1)
@@ -417,6 +457,12 @@ def test_kernel_stats_add_up(cuda):
     finally:
         lib.vrt_set_kernel_timing(0)
         maps.set_sync_checks(True)
-    assert all(ks[i].launches > 0 and ks[i].ms > 0 for i in range(6))
-    assert sum(ks[i].lookups for i in range(6)) == totals["lookups"]
+    assert all(ks[i].launches > 0 and ks[i].ms > 0 for i in range(nk))
+    assert sum(ks[i].lookups for i in range(nk)) == totals["lookups"]
     assert ks[1].steps > 0 and ks[4].reds > 0
+    # the replay reads the primal's collision log (no lookups of its own); with
+    # the automatic log size no path is left to the re-walk
+    assert ks[lib.VRT_K_DS_PRIMAL].log_bytes > 0
+    assert 0 < ks[lib.VRT_K_DS_REPLAY].log_bytes <= ks[lib.VRT_K_DS_PRIMAL].log_bytes
+    assert ks[lib.VRT_K_DS_REPLAY].lookups == 0 and ks[lib.VRT_K_DS_REPLAY].steps > 0
+    assert ks[lib.VRT_K_DS_REWALK].steps == 0 and ks[lib.VRT_K_DS_REWALK].reds == 0
