@@ -220,7 +220,7 @@ __device__ __forceinline__ bool shadow_begin(const DMedium& M, ShadowRay& s, flo
 // collision that continues the ray, hit is set with the majorant and the
 // factor the adjoint's second pass scatters with (RT: r = 1 - sigma/maj; DT:
 // Pc = sigma/maj).
-constexpr int kCross = 16;
+constexpr int kCross = 8;
 
 template <int TR, bool BW>
 __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tally& tl, DScratch* sc, bool& hit,
