@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                     ff.cross(m, md);
                     ff.bk.advance(M);
                     if (!(d > EPS)) { ev = 2; break; }
+                    if (k + 1 >= kWalkCross) break;  // the flight resumes in the next iteration
                     continue;
                 }
                 ff.used();

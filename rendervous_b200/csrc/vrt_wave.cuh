@@ -221,6 +221,11 @@ __device__ __forceinline__ bool shadow_begin(const DMedium& M, ShadowRay& s, flo
 // factor the adjoint's second pass scatters with (RT: r = 1 - sigma/maj; DT:
 // Pc = sigma/maj).
 constexpr int kCross = 8;
+// The same bound for the path walks (measured per kernel): a flight that needs
+// more brick crossings leaves the crossing loop without an event and resumes
+// in the next iteration, so the warp's long flights do not hold the others.
+constexpr int kWalkCross = 12;  // k_walk_fw
+constexpr int kDsCross = 8;     // k_ds_primal, k_ds_rewalk
 
 template <int TR, bool BW>
 __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tally& tl, DScratch* sc, bool& hit,

@@ -139,6 +139,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                         ff.cross(m, md);
                         ff.bk.advance(M);
                         if (!(d > EPS)) { ev = 2; break; }
+                        if (k + 1 >= kDsCross) break;  // the flight resumes in the next iteration
                         continue;
                     }
                     ff.used();
@@ -351,6 +352,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_rewalk(DMedium M, PathSrc S, uint
                         ff.cross(m, md);
                         ff.bk.advance(M);
                         if (!(d > EPS)) { ev = 2; break; }
+                        if (k + 1 >= kDsCross) break;  // the flight resumes in the next iteration
                         continue;
                     }
                     ff.used();
