@@ -243,8 +243,8 @@ __global__ void __launch_bounds__(256, 4) k_shadow_fw(DMedium M, PathSrc S, cons
 
 // ---------------------------------------------------------------------------
 // Persistent shadow kernels for ratio / delta tracking: one event per lane per
-// iteration, finished lanes refilled from the job buffer with one atomic per
-// warp (ranks from a ballot).
+// iteration, finished lanes refilled from the job buffer (a warp claims 64
+// jobs per atomic and hands them out by ballot rank).
 // ---------------------------------------------------------------------------
 struct ShadowOut {
     float* out;        // OUT_IMAGE: image / ray radiance
@@ -283,24 +283,21 @@ __global__ void __launch_bounds__(256, 4) k_shadow_run(DMedium M, PathSrc S, con
                                                      const unsigned long long* __restrict__ count,
                                                      unsigned long long cap, unsigned long long* head, uint64_t seed,
                                                      ShadowOut so, DScratch* sc) {
-    const unsigned lane = threadIdx.x & 31u;
     unsigned long long n = *count;
     if (n > cap) n = cap;
     ShadowRay s;
     JobView jv;
     bool alive = false, exhausted = false;
+    WarpQueue wq;
     Tally tl;
     while (true) {
         const unsigned want = __ballot_sync(kAll, !alive && !exhausted);
         if (want) {
-            const int leader = __ffs(want) - 1;
-            unsigned long long base = 0;
-            if ((int)lane == leader) base = atomicAdd(head, (unsigned long long)__popc(want));
-            base = __shfl_sync(kAll, base, leader);
+            unsigned long long i;
+            const bool got = wq.take(head, n, 64, want, i);  // 64 jobs per warp and atomic
             if (!alive && !exhausted) {
-                const unsigned long long i = base + __popc(want & ((1u << lane) - 1u));
-                if (i >= n) {
-                    exhausted = true;
+                if (!got) {
+                    exhausted = wq.drained;
                 } else {
                     jv = get_job(jobs, i);
                     alive = shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork);
@@ -331,10 +328,10 @@ constexpr int kKeep = 16;
 
 template <int TR>
 __global__ void __launch_bounds__(256, 3) k_shadow_adj(DMedium M, const ShadowJob* __restrict__ jobs,
+                                                     const float* __restrict__ dldt,
                                                      const unsigned long long* __restrict__ count,
                                                      unsigned long long cap, unsigned long long* head, uint64_t seed,
                                                      DScratch* sc) {
-    const unsigned lane = threadIdx.x & 31u;
     unsigned long long n = *count;
     if (n > cap) n = cap;
     ShadowRay s;
@@ -344,20 +341,19 @@ __global__ void __launch_bounds__(256, 3) k_shadow_adj(DMedium M, const ShadowJo
     int nkeep = 0, phase = 0;  // 0 idle, 1 first pass, 2 second pass (more than kKeep collisions)
     float outT = 0.0f;
     bool exhausted = false;
+    WarpQueue wq;
     Tally tl;
     while (true) {
         const unsigned want = __ballot_sync(kAll, phase == 0 && !exhausted);
         if (want) {
-            const int leader = __ffs(want) - 1;
-            unsigned long long base = 0;
-            if ((int)lane == leader) base = atomicAdd(head, (unsigned long long)__popc(want));
-            base = __shfl_sync(kAll, base, leader);
+            unsigned long long i;
+            const bool got = wq.take(head, n, 64, want, i);  // 64 jobs per warp and atomic
             if (phase == 0 && !exhausted) {
-                const unsigned long long i = base + __popc(want & ((1u << lane) - 1u));
-                if (i >= n) {
-                    exhausted = true;
+                if (!got) {
+                    exhausted = wq.drained;
                 } else {
                     jv = get_job(jobs, i);
+                    jv.wt.x = dldt[i];  // the replay's dL/dT (0: no adjoint for this ray)
                     nkeep = 0;
                     if (jv.wt.x != 0.0f && shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork)) phase = 1;
                 }
@@ -495,7 +491,9 @@ __global__ void __launch_bounds__(256, 4) k_shadow_bw(DMedium M, WaveBw wv, uint
     Tally tl;
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
          i += (unsigned long long)gridDim.x * blockDim.x) {
-        const JobView jv = get_job(wv.jobs, i);
+        JobView jv = get_job(wv.jobs, i);
+        jv.wt.x = wv.dldt[i];  // the replay's dL/dT (0: no adjoint for this ray)
+        if (jv.wt.x == 0.0f) continue;
         Rng r;
         r.init(seed, jv.pid, 2u * (1u + jv.fork));
         if (TR == 0) transmittance_rt_bw(M, r, jv.x, jv.dir, jv.wt.x, tl, &sc->status);
@@ -532,11 +530,11 @@ int launch_shadow_adjoint(const DMedium& M, const WaveBw& wv, uint64_t seed, DSc
     switch (M.tr_mode) {
         case 0:
             k_shadow_adj<0><<<persistent_blocks((const void*)k_shadow_adj<0>, 256, num_sms), 256, 0, stream>>>(
-                M, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, sc);
+                M, wv.jobs, wv.dldt, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, sc);
             break;
         case 1:
             k_shadow_adj<1><<<persistent_blocks((const void*)k_shadow_adj<1>, 256, num_sms), 256, 0, stream>>>(
-                M, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, sc);
+                M, wv.jobs, wv.dldt, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, sc);
             break;
         case 2: k_shadow_bw<2><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
         default: k_shadow_bw<3><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;

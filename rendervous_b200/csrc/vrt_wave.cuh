@@ -109,6 +109,39 @@ __device__ __forceinline__ Slots4 reserve_slots4(unsigned long long* c0, unsigne
     return out;
 }
 
+// Work items [0, n) claimed from a global counter a chunk per warp: one atomic
+// per `chunk` items instead of one per refill.  All lanes call take()
+// together with the ballot of the lanes that want an item; a lane gets one
+// (returns true, item set) while the warp's chunk lasts.  Lanes left over wait
+// for the next call, which claims a new chunk; `drained` turns true when a
+// claim finds the counter past n.
+struct WarpQueue {
+    unsigned long long next = 0, end = 0;
+    bool drained = false;
+    __device__ __forceinline__ bool take(unsigned long long* head, unsigned long long n, unsigned long long chunk,
+                                         unsigned want, unsigned long long& item) {
+        const unsigned lane = threadIdx.x & 31u;
+        if (next >= end && !drained) {
+            unsigned long long b = 0;
+            if (lane == 0u) b = atomicAdd(head, chunk);
+            b = __shfl_sync(kAll, b, 0);
+            if (b >= n) {
+                drained = true;
+            } else {
+                next = b;
+                end = b + chunk < n ? b + chunk : n;
+            }
+        }
+        const unsigned long long avail = next < end ? end - next : 0ull;
+        const unsigned rank = __popc(want & ((1u << lane) - 1u));
+        const bool got = ((want >> lane) & 1u) != 0u && (unsigned long long)rank < avail;
+        item = next + rank;
+        const unsigned long long used = (unsigned long long)__popc(want);
+        next += used < avail ? used : avail;
+        return got;
+    }
+};
+
 // Per-warp sums of the lanes' tallies into the context counters.  `verts`
 // counts forward path vertices only (the metric's unit); adjoint kernels pass 0.
 __device__ __forceinline__ void flush_counters(DScratch* sc, int kid, uint32_t paths, uint32_t verts, const Tally& tl) {
@@ -307,19 +340,20 @@ __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tal
 
 constexpr uint32_t kNone = 0xffffffffu;
 constexpr uint32_t kUnlogged = 0xfffffffeu;  // a path whose collisions did not fit the log
-// A real-collision vertex of the NEE_DS primal (64 bytes): its two shadow
+// A real-collision vertex of the NEE_DS primal (48 bytes): its two shadow
 // transmittances (filled by the shadow kernel), the next vertex of the same
-// path, the fork of its light rays, and what the replay needs to redo the
-// vertex without walking to it: the albedo, the environment direction,
-// radiance and the two phase values.
+// path, the slot of its environment job (the sun job follows it), and what the
+// replay needs to redo the vertex without walking to it: the albedo, the
+// environment radiance and the two phase values.  The transmittance adjoint
+// of the vertex reuses the primal's jobs (same ray, same Philox fork), so the
+// replay only stores dL/dT per job slot.
 struct VertexRec {
     float Te, Ts;
-    uint32_t next, fork;
+    uint32_t next, job;
     float sa[3], ph_env;
-    float wnee[3], ph_sun;
-    float Le[3], pad;
+    float Le[3], ph_sun;
 };
-static_assert(sizeof(VertexRec) == 64, "vertex records are four 16-byte words");
+static_assert(sizeof(VertexRec) == 48, "vertex records are three 16-byte words");
 
 // One tracking collision of the NEE_DS primal (32 bytes, two 16-byte words):
 // position and sigma there; majorant, next collision of the path, the vertex
@@ -333,6 +367,7 @@ static_assert(sizeof(CollisionRec) == 32, "collision records are two 16-byte wor
 // Buffers of one round of the NEE_DS adjoint wavefront (vrt_wave_ds.cu).
 struct WaveBw {
     ShadowJob* jobs;
+    float* dldt;               // per job slot: dL/dT from the replay (0: no transmittance adjoint)
     VertexRec* recs;
     CollisionRec* evs;         // the collision log
     float* info;               // per path: R (3), Rsp (3), first record, first collision (or kUnlogged)

@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
 
         int nrec = 0, nj = 0, nev = 0;
         bool finish = false, rsp = false;
-        float3 wnee = f3(0.0f), we = f3(0.0f), ws = f3(0.0f), sa = f3(0.0f), Le = f3(0.0f);
+        float3 wnee = f3(0.0f), sa = f3(0.0f), Le = f3(0.0f);
         float ev_s = 0.0f, ev_m = 0.0f, ph_env = 0.0f, ph_sun = 0.0f;
         uint32_t jfork = 0, ev_real = 0;
         if (alive) {
@@ -175,11 +175,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                             W = W * sa;
                             Le = environment_sample(M, rng, wnee);
                             ph_env = phase(M, w, wnee);
-                            we = W * Le * ph_env;
-                            if (M.has_sun) {
-                                ph_sun = phase(M, w, M.sun_dir);
-                                ws = W * M.sun_L * ph_sun;
-                            }
+                            if (M.has_sun) ph_sun = phase(M, w, M.sun_dir);
                             jfork = rng.ntr;
                             rng.ntr += (uint32_t)lights;
                             const bool capped = M.max_bounces > 0 && bounces + 1 >= M.max_bounces;
@@ -192,8 +188,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                             nj = lights;
                             ++bounces;
                             if (capped || all_less(W, EPS)) {
-                                W = f3(0.0f);
-                                ev = 2;
+                                ev = 2;  // W stays: the light jobs below weigh with it
                             } else {
                                 w = wo;
                                 float tMin;
@@ -219,10 +214,9 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
         const unsigned long long r = sl.s1;
         if (nrec) {  // the vertex record, linked to the path's previous one
             uint4* rp = reinterpret_cast<uint4*>(wv.recs + r);
-            __stcs(rp, make_uint4(__float_as_uint(1.0f), __float_as_uint(1.0f), kNone, jfork));
+            __stcs(rp, make_uint4(__float_as_uint(1.0f), __float_as_uint(1.0f), kNone, (uint32_t)sl.s0));
             __stcs(reinterpret_cast<float4*>(rp + 1), make_float4(sa.x, sa.y, sa.z, ph_env));
-            __stcs(reinterpret_cast<float4*>(rp + 2), make_float4(wnee.x, wnee.y, wnee.z, ph_sun));
-            __stcs(reinterpret_cast<float4*>(rp + 3), make_float4(Le.x, Le.y, Le.z, 0.0f));
+            __stcs(reinterpret_cast<float4*>(rp + 2), make_float4(Le.x, Le.y, Le.z, ph_sun));
             tl.logb += (uint32_t)sizeof(VertexRec);
             if (first == kNone) first = (uint32_t)r;
             else wv.recs[prev].next = (uint32_t)r;
@@ -245,8 +239,9 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
         if (nj) {
             const unsigned long long j = sl.s0;
             const uint32_t tgt = ((uint32_t)r << 2) | (rsp ? 2u : 0u);
-            put_job(wv.jobs, j, x, wnee, we, job_key(pid, jfork), tgt);
-            if (nj == 2) put_job(wv.jobs, j + 1, x, M.sun_dir, ws, job_key(pid, jfork + 1), tgt | 1u);
+            // the light rays of the vertex, weighted W * L * phase (W after the albedo)
+            put_job(wv.jobs, j, x, wnee, W * Le * ph_env, job_key(pid, jfork), tgt);
+            if (nj == 2) put_job(wv.jobs, j + 1, x, M.sun_dir, W * M.sun_L * ph_sun, job_key(pid, jfork + 1), tgt | 1u);
         }
         if (finish) {  // end of the primal (_NEE_DS.h:106-110): escape term, then the path's totals
             if (!scattered) Racc = Racc + M.env * W;
@@ -324,10 +319,6 @@ __global__ void __launch_bounds__(256, 3) k_ds_rewalk(DMedium M, PathSrc S, uint
         }
         if (__all_sync(kAll, !alive && exhausted)) break;
 
-        int nj = 0;
-        float3 jd0 = f3(0.0f), jd1 = f3(0.0f);
-        float dT0 = 0.0f, dT1 = 0.0f;
-        uint32_t f0 = 0, f1 = 0;
         if (alive) {
             int ev = 0;
             if (!(d > EPS)) {
@@ -388,11 +379,11 @@ __global__ void __launch_bounds__(256, 3) k_ds_rewalk(DMedium M, PathSrc S, uint
                             const float3 Le = environment_sample(M, rng, wnee);
                             const float ph_nee = phase(M, w, wnee);
                             const float ph_sun = M.has_sun ? phase(M, w, M.sun_dir) : 0.0f;
-                            const uint32_t jf = rng.ntr;
-                            rng.ntr += (uint32_t)lights;
+                            rng.ntr += (uint32_t)lights;  // the forks of the vertex's light rays
                             const float3 wo = phase_sample(M, rng, w);
                             W = W * sa;
                             float Te = 1.0f, Ts = 1.0f;
+                            uint32_t job = 0;
                             if (cur == kNone) {
                                 guard(sc, 5);  // the replay left the primal's path
                                 ev = 2;
@@ -400,19 +391,17 @@ __global__ void __launch_bounds__(256, 3) k_ds_rewalk(DMedium M, PathSrc S, uint
                                 const VertexRec rec = wv.recs[cur];
                                 Te = rec.Te;
                                 Ts = rec.Ts;
+                                job = rec.job;
                                 cur = rec.next;
                             }
                             if (ev != 2) {
                                 const float dTe = dot(dLdR, W * Le * ph_nee);
                                 R = R - W * Te * Le * ph_nee;
-                                if (dTe != 0.0f) { jd0 = wnee; dT0 = dTe; f0 = jf; nj = 1; }
+                                if (dTe != 0.0f) wv.dldt[job] = dTe;  // into the primal's job slots
                                 if (M.has_sun) {
                                     const float dTs = dot(dLdR, W * M.sun_L * ph_sun);
                                     R = R - W * Ts * M.sun_L * ph_sun;
-                                    if (dTs != 0.0f) {
-                                        if (nj == 0) { jd0 = M.sun_dir; dT0 = dTs; f0 = jf + 1; nj = 1; }
-                                        else { jd1 = M.sun_dir; dT1 = dTs; f1 = jf + 1; nj = 2; }
-                                    }
+                                    if (dTs != 0.0f) wv.dldt[job + 1] = dTs;
                                 }
                                 ++bounces;
                                 if ((M.max_bounces > 0 && bounces >= M.max_bounces) || all_less(W, EPS)) {
@@ -434,15 +423,6 @@ __global__ void __launch_bounds__(256, 3) k_ds_rewalk(DMedium M, PathSrc S, uint
             }
             if (ev == 2) alive = false;
         }
-        const unsigned long long j = reserve_slots(&wv.hdr[0], nj);
-        if (nj) {
-            if (j + (unsigned long long)nj > wv.cap_jobs) {
-                guard(sc, 7);
-            } else {
-                put_job(wv.jobs, j, x, jd0, make_float3(dT0, 0.0f, 0.0f), job_key(pid, f0));
-                if (nj == 2) put_job(wv.jobs, j + 1, x, jd1, make_float3(dT1, 0.0f, 0.0f), job_key(pid, f1));
-            }
-        }
     }
     flush_counters(sc, VRT_K_DS_REWALK, 0, 0, tl);
 }
@@ -458,7 +438,6 @@ __global__ void __launch_bounds__(256, 3) k_ds_rewalk(DMedium M, PathSrc S, uint
 // flight.
 __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, const float* __restrict__ dL, float div,
                                                     DScratch* sc, WaveBw wv) {
-    const unsigned lane = threadIdx.x & 31u;
     const float EPS = 0.00000001f;
     const float eps = M.ds_eps;
     unsigned long long n_list = *((volatile unsigned long long*)&wv.hdr[8]);
@@ -470,19 +449,17 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, cons
     uint32_t steps_path = 0;
     float4 xs = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // the collision to replay
     uint4 ln = make_uint4(0u, kNone, kNone, 0u);
+    WarpQueue wq;
     Tally tl;
 
     while (true) {
-        unsigned want = __ballot_sync(kAll, !alive && !exhausted);
+        const unsigned want = __ballot_sync(kAll, !alive && !exhausted);
         if (want) {
-            const int leader = __ffs(want) - 1;
-            unsigned long long base = 0;
-            if ((int)lane == leader) base = atomicAdd(&wv.hdr[7], (unsigned long long)__popc(want));
-            base = __shfl_sync(kAll, base, leader);
+            unsigned long long q;
+            const bool got = wq.take(&wv.hdr[7], n_list, 64, want, q);
             if (!alive && !exhausted) {
-                const unsigned long long q = base + __popc(want & ((1u << lane) - 1u));
-                if (q >= n_list) {
-                    exhausted = true;
+                if (!got) {
+                    exhausted = wq.drained;
                 } else {
                     const uint2 e = __ldcs(wv.list + q);
                     if (e.y != kUnlogged) {  // (a path whose last collision found the log full: k_ds_rewalk)
@@ -505,10 +482,6 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, cons
         }
         if (__all_sync(kAll, !alive && exhausted)) break;
 
-        int nj = 0;
-        float3 xj = f3(0.0f), jd0 = f3(0.0f), jd1 = f3(0.0f);
-        float dT0 = 0.0f, dT1 = 0.0f;
-        uint32_t f0 = 0, f1 = 0;
         if (alive) {
             bool end = false;
             // the next collision of the path and this one's vertex record, loaded ahead
@@ -522,13 +495,12 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, cons
                 nln = __ldcs(&np->link);
             }
             uint4 r0 = make_uint4(0u, 0u, 0u, 0u);
-            float4 r1 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), r2 = r1, r3 = r1;
+            float4 r1 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), r2 = r1;
             if (real && ln.z != kNone) {
                 const uint4* rp = reinterpret_cast<const uint4*>(wv.recs + ln.z);
                 r0 = __ldcs(rp);
                 r1 = __ldcs(reinterpret_cast<const float4*>(rp + 1));
                 r2 = __ldcs(reinterpret_cast<const float4*>(rp + 2));
-                r3 = __ldcs(reinterpret_cast<const float4*>(rp + 3));
             }
             tl.logb += (uint32_t)sizeof(CollisionRec);
             ++tl.steps;
@@ -553,23 +525,21 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, cons
                     const float Te = __uint_as_float(r0.x), Ts = __uint_as_float(r0.y);
                     const float3 sa = make_float3(r1.x, r1.y, r1.z);
                     const float ph_nee = r1.w, ph_sun = r2.w;
-                    const float3 wnee = make_float3(r2.x, r2.y, r2.z), Le = make_float3(r3.x, r3.y, r3.z);
+                    const float3 Le = make_float3(r2.x, r2.y, r2.z);
                     float3 dL_dsa = dLdR * W * -1.0f * M.emission;
                     R = R - W * (f3(1.0f) - sa) * M.emission;
                     dL_dsa = dL_dsa + dLdR * R / make_float3(gmax(EPS, sa.x), gmax(EPS, sa.y), gmax(EPS, sa.z));
                     albedo_bw(M, x, dL_dsa, tl);
                     W = W * sa;
+                    // dL/dT of the vertex's light rays into their primal job slots
+                    const uint32_t job = r0.w;
                     const float dTe = dot(dLdR, W * Le * ph_nee);
                     R = R - W * Te * Le * ph_nee;
-                    xj = x;
-                    if (dTe != 0.0f) { jd0 = wnee; dT0 = dTe; f0 = r0.w; nj = 1; }
+                    if (dTe != 0.0f) wv.dldt[job] = dTe;
                     if (M.has_sun) {
                         const float dTs = dot(dLdR, W * M.sun_L * ph_sun);
                         R = R - W * Ts * M.sun_L * ph_sun;
-                        if (dTs != 0.0f) {
-                            if (nj == 0) { jd0 = M.sun_dir; dT0 = dTs; f0 = r0.w + 1u; nj = 1; }
-                            else { jd1 = M.sun_dir; dT1 = dTs; f1 = r0.w + 1u; nj = 2; }
-                        }
+                        if (dTs != 0.0f) wv.dldt[job + 1] = dTs;
                     }
                     ++bounces;
                     if ((M.max_bounces > 0 && bounces >= M.max_bounces) || all_less(W, EPS)) end = true;
@@ -583,15 +553,6 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, cons
                 end = true;
             }
             if (end) alive = false;
-        }
-        const unsigned long long j = reserve_slots(&wv.hdr[0], nj);
-        if (nj) {
-            if (j + (unsigned long long)nj > wv.cap_jobs) {
-                guard(sc, 7);
-            } else {
-                put_job(wv.jobs, j, xj, jd0, make_float3(dT0, 0.0f, 0.0f), job_key(pid, f0));
-                if (nj == 2) put_job(wv.jobs, j + 1, xj, jd1, make_float3(dT1, 0.0f, 0.0f), job_key(pid, f1));
-            }
         }
     }
     flush_counters(sc, VRT_K_DS_REPLAY, 0, 0, tl);
@@ -624,7 +585,8 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     wv.cap_evs = ctx->log_limit ? ctx->log_limit : 4ull * batch_jobs(n_paths, 1) + inflight * 16ull;
     if (wv.cap_evs > 0xfff00000ull) wv.cap_evs = 0xfff00000ull;  // 32-bit links, kNone / kUnlogged reserved
     wv.res_evs = inflight * 16ull < wv.cap_evs / 2 ? inflight * 16ull : wv.cap_evs / 2;
-    const size_t o_jobs = 256, o_recs = o_jobs + wv.cap_jobs * sizeof(ShadowJob);
+    const size_t o_jobs = 256, o_dldt = o_jobs + wv.cap_jobs * sizeof(ShadowJob);
+    const size_t o_recs = o_dldt + ((wv.cap_jobs * 4 + 255) & ~(size_t)255);
     const size_t o_info = o_recs + wv.cap_recs * sizeof(VertexRec), o_over = o_info + wv.cap_paths * 32;
     const size_t o_list = o_over + ((wv.cap_paths * 4 + 255) & ~(size_t)255);
     const size_t o_evs = o_list + ((wv.cap_paths * 8 + 255) & ~(size_t)255), bytes = o_evs + wv.cap_evs * 32;
@@ -633,6 +595,7 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     char* base = static_cast<char*>(ctx->wave);
     wv.hdr = reinterpret_cast<unsigned long long*>(base);
     wv.jobs = reinterpret_cast<ShadowJob*>(base + o_jobs);
+    wv.dldt = reinterpret_cast<float*>(base + o_dldt);
     wv.recs = reinterpret_cast<VertexRec*>(base + o_recs);
     wv.info = reinterpret_cast<float*>(base + o_info);
     wv.over = reinterpret_cast<uint32_t*>(base + o_over);
@@ -651,7 +614,9 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
             k_ds_primal<<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
         }
         if ((st = launch_shadow_record(M, src, wv, seed, ctx->scratch, ctx->num_sms, stream))) return st;
-        if ((e = cudaMemsetAsync(wv.hdr, 0, sizeof(unsigned long long), stream)) != cudaSuccess)
+        // dL/dT per job slot of the round: the replays fill in the vertices they redo; the
+        // transmittance adjoints then run over the primal's jobs and skip the zeros
+        if ((e = cudaMemsetAsync(wv.dldt, 0, wv.cap_jobs * sizeof(float), stream)) != cudaSuccess)
             return launch_status(e);
         {
             KernelScope ks(VRT_K_DS_REPLAY, stream);
