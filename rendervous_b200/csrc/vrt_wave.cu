@@ -138,9 +138,8 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                 }
                 float md;
                 m = gmax(EPS, ff.bk.query(M, x, w, md));
-                t = ff.tau / m;
-                x = x + w * gmin(t, md);
-                if (t > md) {
+                if (ff.tau > md * m) {  // crosses the brick face (optical depth > majorant x distance)
+                    x = x + w * md;
                     d -= md;
                     ff.cross(m, md);
                     ff.bk.advance(M);
@@ -148,6 +147,8 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                     if (k + 1 >= kWalkCross) break;  // the flight resumes in the next iteration
                     continue;
                 }
+                t = ff.tau / m;
+                x = x + w * gmin(t, md);
                 ff.used();
                 if (t > d) ev = 2;
                 else need_sigma = true;

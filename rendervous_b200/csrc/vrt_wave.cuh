@@ -274,9 +274,12 @@ __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tal
         const float q = s.ff.bk.query(M, s.x, s.dir, md);
         maj = BW ? gmax(EPS, q + 0.1f) : gmax(EPS, q);
         if (!BW && s.ff.tau < 0.0f) ++tl.steps;
+        // the flight crosses the brick face when its optical depth exceeds
+        // majorant x distance to the face: tested without a division, and the
+        // crossing leaves the depth positive
         if (TR == 0) {
-            t = s.ff.sample(s.r) / maj;
-            if (md < s.d && t > md) {
+            const float tau = s.ff.sample(s.r);
+            if (md < s.d && tau > md * maj) {
                 s.x = s.x + s.dir * md;
                 s.d -= md;
                 s.ff.cross(maj, md);
@@ -284,16 +287,19 @@ __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tal
                 if (c + 1 >= kCross) return false;
                 continue;
             }
+            t = tau / maj;
         } else {
-            const float dt = s.ff.sample(s.r) / maj;
-            t = gmin(md, dt);
+            const float tau = s.ff.sample(s.r);
+            const bool crosses = tau > md * maj;
+            t = md;
+            if (!crosses) t = gmin(md, tau / maj);
             s.x = s.x + s.dir * t;
             s.d -= t;
             if (s.d <= EPS) {
                 s.T = 1.0f;
                 return true;
             }
-            if (dt > md) {
+            if (crosses) {
                 s.ff.cross(maj, md);
                 s.ff.bk.advance(M);
                 if (c + 1 >= kCross) return false;

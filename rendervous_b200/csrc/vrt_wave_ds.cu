@@ -132,9 +132,8 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                     }
                     float md;
                     m = gmax(EPS, ff.bk.query(M, x, w, md) + 2.0f * eps + 0.1f);  // _NEE_DS.h:36
-                    t = ff.tau / m;
-                    x = x + w * gmin(t, md);
-                    if (t > md) {
+                    if (ff.tau > md * m) {  // crosses the brick face (optical depth > majorant x distance)
+                        x = x + w * md;
                         d -= md;
                         ff.cross(m, md);
                         ff.bk.advance(M);
@@ -142,6 +141,8 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                         if (k + 1 >= kDsCross) break;  // the flight resumes in the next iteration
                         continue;
                     }
+                    t = ff.tau / m;
+                    x = x + w * gmin(t, md);
                     ff.used();
                     if (t > d) ev = 2;
                     else need = true;
@@ -336,9 +337,8 @@ __global__ void __launch_bounds__(256, 3) k_ds_rewalk(DMedium M, PathSrc S, uint
                     }
                     float md;
                     m = gmax(EPS, ff.bk.query(M, x, w, md) + 2.0f * eps + 0.1f);
-                    t = ff.tau / m;
-                    x = x + w * gmin(t, md);
-                    if (t > md) {
+                    if (ff.tau > md * m) {  // the primal's test (k_ds_primal)
+                        x = x + w * md;
                         d -= md;
                         ff.cross(m, md);
                         ff.bk.advance(M);
@@ -346,6 +346,8 @@ __global__ void __launch_bounds__(256, 3) k_ds_rewalk(DMedium M, PathSrc S, uint
                         if (k + 1 >= kDsCross) break;  // the flight resumes in the next iteration
                         continue;
                     }
+                    t = ff.tau / m;
+                    x = x + w * gmin(t, md);
                     ff.used();
                     if (t > d) ev = 2;
                     else need = true;
