@@ -577,8 +577,11 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     const unsigned long long inflight = wv.lanes < n_paths ? wv.lanes : n_paths;
     wv.res_jobs = inflight * lights * B;
     wv.res_recs = inflight * B;
-    wv.cap_jobs = wv.res_jobs + batch_jobs(n_paths, lights);
-    wv.cap_recs = wv.res_recs + batch_jobs(n_paths, 1);
+    // room for three vertex records per path (the NEE_DS primal's majorant and
+    // epsilon collisions make more vertices than the forward's: 2.3 per path
+    // on the benchmark medium)
+    wv.cap_jobs = wv.res_jobs + batch_jobs(n_paths, 3ull * lights);
+    wv.cap_recs = wv.res_recs + batch_jobs(n_paths, 3);
     if (wv.cap_recs > (1ull << 30)) return VRT_E_UNSUPPORTED;  // record indices are 30-bit in a job
     wv.cap_paths = (n_paths < (1ull << 24) ? n_paths : (1ull << 24)) + wv.lanes;
     // the collision log: room for about four collisions per vertex record of a
