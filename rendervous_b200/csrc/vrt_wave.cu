@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow_run(DMedium M, PathSrc S, con
 constexpr int kKeep = 16;
 
 template <int TR>
-__global__ void __launch_bounds__(256, 3) k_shadow_adj(DMedium M, const ShadowJob* __restrict__ jobs,
+__global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, const ShadowJob* __restrict__ jobs,
                                                      const float* __restrict__ dldt,
                                                      const unsigned long long* __restrict__ count,
                                                      unsigned long long cap, unsigned long long* head, uint64_t seed,
