@@ -623,6 +623,10 @@ int vrt_capture_prefix_fw(vrt_context* ctx, const vrt_medium* m, const vrt_camer
     S.is_camera = 1;
     S.npix = (long long)S.cam.views * S.cam.height * S.cam.width;
     const uint64_t n = (uint64_t)S.npix * (uint64_t)spp;
+    // the wavefront forward with a cut (its job reserve is bounded by the cut,
+    // capped or not); very deep cuts stay on the per-lane state machine
+    if (cut <= 4096 && (M.max_bounces <= 0 || M.max_bounces <= 4096))
+        return launch_wave_fw(ctx, M, S, n, seed, rgb, 1.0f / (float)spp, (cudaStream_t)stream, cut, queries);
     CacheIO io = {cut, 0, queries, nullptr, nullptr, (long long)n};
     return launch_cache_paths(M, FW_CUT, S, n, seed, rgb, 1.0f / (float)spp, io, ctx->scratch, ctx->num_sms,
                               (cudaStream_t)stream);

@@ -40,8 +40,11 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
                       const float* dL, float div, cudaStream_t stream);
 
 // Wavefront NEE forward (vrt_wave.cu), capped paths only.
+// cut >= 0: a path stops at its (cut+1)-th real collision and writes its
+// radiance-cache query there (3 planes of `n_paths` rows in `queries`: position,
+// arrival direction, throughput; zeros when it never gets there).
 int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed, float* out,
-                   float scale, cudaStream_t stream);
+                   float scale, cudaStream_t stream, int cut = -1, float* queries = nullptr);
 
 int persistent_blocks(const void* kernel, int block, int num_sms);
 

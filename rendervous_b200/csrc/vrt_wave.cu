@@ -41,6 +41,9 @@ struct WaveFw {
     ShadowJob* jobs;
     unsigned long long* count;
     unsigned long long cap, reserve;
+    int cut;          // >= 0: paths stop into the radiance cache at their (cut+1)-th real collision
+    float* q;         // the cache queries: 3 planes [rows, 3] (position, direction, throughput)
+    long long rows;
 };
 
 __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, float* out,
@@ -106,6 +109,13 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                     steps_path = 0;
                     ff = Flight();
                     ++n_paths_done;
+                    if (wv.cut >= 0) {  // no query unless the path reaches the cut
+                        float* q = wv.q + 3 * pid;
+                        q[0] = q[1] = q[2] = 0.0f;
+                        q[3 * wv.rows] = q[3 * wv.rows + 1] = 0.0f;
+                        q[3 * wv.rows + 2] = 1.0f;
+                        q[6 * wv.rows] = q[6 * wv.rows + 1] = q[6 * wv.rows + 2] = 0.0f;
+                    }
                     njobs = 1;
                     jx = x;
                     jd = w;
@@ -168,7 +178,14 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                 guard(sc, 1);
                 ev = 2;
             }
-            if (ev == 1) {  // real collision (vr_path_integrator_NEE.h:41-62)
+            if (ev == 1 && wv.cut >= 0 && bounces == wv.cut) {  // the rest of the path comes from the cache
+                ++n_verts;
+                float* q = wv.q + 3 * pid;
+                q[0] = x.x; q[1] = x.y; q[2] = x.z;
+                q[3 * wv.rows] = w.x; q[3 * wv.rows + 1] = w.y; q[3 * wv.rows + 2] = w.z;
+                q[6 * wv.rows] = W.x; q[6 * wv.rows + 1] = W.y; q[6 * wv.rows + 2] = W.z;
+                ev = 2;
+            } else if (ev == 1) {  // real collision (vr_path_integrator_NEE.h:41-62)
                 ++n_verts;
                 const float3 sa = albedo(M, x, tl);
                 Rem = Rem + W * (f3(1.0f) - sa) * M.emission;
@@ -405,11 +422,15 @@ __global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, const ShadowJo
 
 // Host: rounds of walk + shadow until every path has been taken.
 int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed, float* out,
-                   float scale, cudaStream_t stream) {
+                   float scale, cudaStream_t stream, int cut, float* queries) {
     if (n_paths == 0) return 0;
-    if (M.max_bounces <= 0) return VRT_E_UNSUPPORTED;
+    if (M.max_bounces <= 0 && cut < 0) return VRT_E_UNSUPPORTED;  // the reserve needs a bound on vertices
+    if (cut >= 0 && !queries) return VRT_E_NULL_POINTER;
     const unsigned long long lights = M.has_sun ? 2ull : 1ull;
-    const unsigned long long per_path = 1ull + lights * (unsigned long long)M.max_bounces;
+    // light jobs come from the vertices before the cap or the cut
+    unsigned long long verts = M.max_bounces > 0 ? (unsigned long long)M.max_bounces : ~0ull;
+    if (cut >= 0 && (unsigned long long)cut < verts) verts = (unsigned long long)cut;
+    const unsigned long long per_path = 1ull + lights * verts;
     int blocks = persistent_blocks((const void*)k_walk_fw, 256, ctx->num_sms);
     const uint64_t need = (n_paths + 255) / 256;
     if ((uint64_t)blocks > need) blocks = (int)need;
@@ -425,6 +446,9 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
     wv.jobs = reinterpret_cast<ShadowJob*>(static_cast<char*>(ctx->wave) + 256);
     wv.cap = cap;
     wv.reserve = reserve;
+    wv.cut = cut;
+    wv.q = queries;
+    wv.rows = (long long)n_paths;
     cudaError_t e = cudaMemsetAsync(&ctx->scratch->next_path, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return launch_status(e);
     const int sblocks = ctx->num_sms * 8;
