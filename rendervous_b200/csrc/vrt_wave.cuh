@@ -1,7 +1,7 @@
 // vrt_wave.cuh -- pieces shared by the wavefront kernels: the shadow-job
 // buffer, warp-aggregated slot reservation, counter flushes, and a shadow ray
 // advanced one step at a time (vrt_wave.cu: forward walk and every shadow
-// kernel; vrt_wave_ds.cu: the NEE_DS primal and replay walks).
+// kernel; vrt_wave_ds.cu: the NEE_DS primal walk and its collision-log replay).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -381,7 +381,7 @@ struct WaveBw {
     uint32_t* over;            // round-local indices of the paths left out of the log
     uint2* list;               // paths with logged collisions: round-local index, first collision
     // [0] jobs, [1] records, [2] re-walk queue, [3] / [4] heads of the shadow
-    // kernels, [5] collisions, [6] paths left out of the log, [7] replay queue,
+    // kernels, [5] collisions, [6] paths left out of the log, [7] replay-list head,
     // [8] replay list
     unsigned long long* hdr;
     unsigned long long cap_jobs, cap_recs, cap_paths, cap_evs;
@@ -394,7 +394,7 @@ struct WaveBw {
 // Shadow kernels of the NEE_DS adjoint rounds (defined in vrt_wave.cu, so they
 // are compiled with the forward's floating-point contraction): T of the
 // primal's jobs into their vertex records and paths (head: hdr[3]), and the
-// transmittance adjoints of the replay's jobs (head: hdr[4]).
+// transmittance adjoints of the same jobs with the replay's dL/dT (head: hdr[4]).
 int launch_shadow_record(const DMedium& M, const PathSrc& src, const wave::WaveBw& wv, uint64_t seed, DScratch* sc,
                          int num_sms, cudaStream_t stream);
 int launch_shadow_adjoint(const DMedium& M, const wave::WaveBw& wv, uint64_t seed, DScratch* sc, int num_sms,

@@ -19,10 +19,10 @@ using namespace wave;
 // retraces the primal's vertices exactly -- same draws, same throughputs, and
 // shadow j of the path draws from fork j in both passes.  So the primal logs
 // what the replay would recompute: a 32-byte collision record per tracking
-// collision and a 64-byte vertex record per scattering vertex; a vertex's
+// collision and a 48-byte vertex record per scattering vertex; a vertex's
 // shadow transmittances are computed once into its record, and the
-// transmittance adjoints (which feed nothing back into the path) run as
-// independent jobs:
+// transmittance adjoints (which feed nothing back into the path) run over the
+// primal's light jobs (same rays, same forks) with the replay's dL/dT:
 //
 //   A k_ds_primal   the primal walk: per tracking collision a collision record,
 //                   per real collision a vertex record (both linked per path)
@@ -32,11 +32,11 @@ using namespace wave;
 //                   path's R (or Rsp after a zero-density collision)
 //   C k_ds_replay   the replay from the log: dL/dsigma at every collision,
 //                   dL/dalbedo at real ones, the R bookkeeping from the stored
-//                   T, and a transmittance-adjoint job per light with dL/dT != 0
+//                   T, and dL/dT of each light ray into its job slot
 //     k_ds_rewalk   the same for the paths the log had no room for, by walking
 //                   them again with the primal's draws
 //   D (vrt_wave.cu) the ratio / delta tracking adjoint or the DDA adjoint of
-//                   each job
+//                   each job with dL/dT != 0
 //
 // Rounds bound the buffers as in the forward wavefront.
 // ------------------------------------------------------------------------
@@ -611,7 +611,7 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     if (e != cudaSuccess) return launch_status(e);
     for (int round = 0;; ++round) {
         // [0] jobs, [1] records, [2] re-walk queue, [3] / [4] heads of the shadow kernels,
-        // [5] collisions, [6] paths left out of the log, [7] replay queue, [8] replay list
+        // [5] collisions, [6] paths left out of the log, [7] replay-list head, [8] replay list
         if ((e = cudaMemsetAsync(wv.hdr, 0, 9 * sizeof(unsigned long long), stream)) != cudaSuccess)
             return launch_status(e);
         {
