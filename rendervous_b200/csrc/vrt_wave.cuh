@@ -379,7 +379,7 @@ struct WaveBw {
     CollisionRec* evs;         // the collision log
     float* info;               // per path: R (3), Rsp (3), first record, first collision (or kUnlogged)
     uint32_t* over;            // round-local indices of the paths left out of the log
-    uint2* list;               // paths with logged collisions: round-local index, first collision
+    uint4* list;               // paths with logged collisions: round-local index, first collision, count
     // [0] jobs, [1] records, [2] re-walk queue, [3] / [4] heads of the shadow
     // kernels, [5] collisions, [6] paths left out of the log, [7] replay-list head,
     // [8] replay list

@@ -54,7 +54,10 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
     bool scattered = false, alive = false, exhausted = false;
     int bounces = 0;
     uint64_t pid = 0;
-    uint32_t steps_path = 0, first = kNone, prev = kNone, first_ev = kNone, prev_ev = kNone;
+    // a path's records are linked forward without patching: each record is
+    // written with the slot reserved for the path's next one (rec_next,
+    // ev_next), so every path leaves one reserved slot of each kind unused
+    uint32_t steps_path = 0, first = kNone, rec_next = kNone, first_ev = kNone, ev_next = kNone, n_ev = 0;
     uint32_t n_paths_done = 0;
     bool logged = false;
     Tally tl;
@@ -98,9 +101,10 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                     bounces = 0;
                     steps_path = 0;
                     first = kNone;
-                    prev = kNone;
+                    rec_next = kNone;
                     first_ev = kNone;
-                    prev_ev = kNone;
+                    ev_next = kNone;
+                    n_ev = 0;
                     logged = true;
                     ff = Flight();
                     alive = true;
@@ -152,7 +156,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                 if (need) {
                     const float s = sigma(M, x, tl);
                     const float Pc = (s + eps) / m;
-                    nev = logged ? 1 : 0;
+                    nev = logged ? (ev_next == kNone ? 2 : 1) : 0;  // this collision's slot and the next one's
                     ev_s = s;
                     ev_m = m;
                     if (rng.uniform() >= Pc) {  // null collision (_NEE_DS.h:41-45)
@@ -185,7 +189,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                             rsp = null_W < EPS;
                             if (rsp) Rspacc = Rspacc + acc;
                             else Racc = Racc + acc;
-                            nrec = 1;
+                            nrec = rec_next == kNone ? 2 : 1;
                             nj = lights;
                             ++bounces;
                             if (capped || all_less(W, EPS)) {
@@ -212,29 +216,30 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
         const Slots4 sl = reserve_slots4(&wv.hdr[0], &wv.hdr[1], &wv.hdr[5], &wv.hdr[8],
                                          (uint32_t)nj | ((uint32_t)nrec << 8) | ((uint32_t)nev << 16) |
                                              ((uint32_t)nl << 24));
-        const unsigned long long r = sl.s1;
-        if (nrec) {  // the vertex record, linked to the path's previous one
+        const unsigned long long r = rec_next == kNone ? sl.s1 : rec_next;
+        if (nrec) {  // the vertex record, with the slot of the path's next one
+            const uint32_t rn = rec_next == kNone ? (uint32_t)(sl.s1 + 1) : (uint32_t)sl.s1;
             uint4* rp = reinterpret_cast<uint4*>(wv.recs + r);
-            __stcs(rp, make_uint4(__float_as_uint(1.0f), __float_as_uint(1.0f), kNone, (uint32_t)sl.s0));
+            __stcs(rp, make_uint4(__float_as_uint(1.0f), __float_as_uint(1.0f), rn, (uint32_t)sl.s0));
             __stcs(reinterpret_cast<float4*>(rp + 1), make_float4(sa.x, sa.y, sa.z, ph_env));
             __stcs(reinterpret_cast<float4*>(rp + 2), make_float4(Le.x, Le.y, Le.z, ph_sun));
             tl.logb += (uint32_t)sizeof(VertexRec);
             if (first == kNone) first = (uint32_t)r;
-            else wv.recs[prev].next = (uint32_t)r;
-            prev = (uint32_t)r;
+            rec_next = rn;
         }
-        if (nev) {  // the collision record (null and real), linked to the path's previous one
-            const unsigned long long je = sl.s2;
-            if (je >= wv.cap_evs) {
+        if (nev) {  // the collision record (null and real), with the slot of the path's next one
+            const unsigned long long je = ev_next == kNone ? sl.s2 : ev_next;
+            const unsigned long long jn = ev_next == kNone ? sl.s2 + 1 : sl.s2;
+            if (je >= wv.cap_evs || jn >= wv.cap_evs) {
                 logged = false;  // the log is full: this path is replayed by walking it again
             } else {
                 CollisionRec* ep = wv.evs + je;
                 __stcs(&ep->xs, make_float4(x.x, x.y, x.z, ev_s));
-                __stcs(&ep->link, make_uint4(__float_as_uint(ev_m), kNone, nrec ? (uint32_t)r : kNone, ev_real));
+                __stcs(&ep->link, make_uint4(__float_as_uint(ev_m), (uint32_t)jn, nrec ? (uint32_t)r : kNone, ev_real));
                 tl.logb += (uint32_t)sizeof(CollisionRec);
                 if (first_ev == kNone) first_ev = (uint32_t)je;
-                else wv.evs[prev_ev].link.y = (uint32_t)je;
-                prev_ev = (uint32_t)je;
+                ev_next = (uint32_t)jn;
+                ++n_ev;
             }
         }
         if (nj) {
@@ -252,7 +257,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
             __stcs(reinterpret_cast<float4*>(io) + 1, make_float4(Rspacc.y, Rspacc.z, __uint_as_float(first),
                                                                   __uint_as_float(logged ? first_ev : kUnlogged)));
             // an entry whose last collision found the log full is skipped by the replay
-            if (nl) __stcs(wv.list + sl.s3, make_uint2((uint32_t)k, logged ? first_ev : kUnlogged));
+            if (nl) __stcs(wv.list + sl.s3, make_uint4((uint32_t)k, logged ? first_ev : kUnlogged, n_ev, 0u));
             if (!logged) {
                 const unsigned long long o = atomicAdd(&wv.hdr[6], 1ull);
                 if (o < wv.cap_paths) wv.over[o] = (uint32_t)k;
@@ -448,7 +453,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, cons
     bool alive = false, exhausted = false;
     int bounces = 0;
     uint64_t pid = 0;
-    uint32_t steps_path = 0;
+    uint32_t left = 0;  // collisions of the path still to replay
     float4 xs = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // the collision to replay
     uint4 ln = make_uint4(0u, kNone, kNone, 0u);
     WarpQueue wq;
@@ -463,8 +468,8 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, cons
                 if (!got) {
                     exhausted = wq.drained;
                 } else {
-                    const uint2 e = __ldcs(wv.list + q);
-                    if (e.y != kUnlogged) {  // (a path whose last collision found the log full: k_ds_rewalk)
+                    const uint4 e = __ldcs(wv.list + q);
+                    if (e.y != kUnlogged && e.z > 0u) {  // (a path whose last collision found the log full: k_ds_rewalk)
                         const CollisionRec* ep = wv.evs + e.y;
                         xs = __ldcs(&ep->xs);
                         ln = __ldcs(&ep->link);
@@ -476,7 +481,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, cons
                         Rsp = make_float3(a.w, b.x, b.y);
                         W = f3(1.0f);
                         bounces = 0;
-                        steps_path = 0;
+                        left = e.z;
                         alive = true;
                     }
                 }
@@ -491,7 +496,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, cons
             const bool real = (ln.w & 1u) != 0u;
             float4 nxs = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             uint4 nln = make_uint4(0u, kNone, kNone, 0u);
-            if (nx != kNone) {
+            if (left > 1u) {
                 const CollisionRec* np = wv.evs + nx;
                 nxs = __ldcs(&np->xs);
                 nln = __ldcs(&np->link);
@@ -549,11 +554,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, cons
             }
             xs = nxs;
             ln = nln;
-            if (nx == kNone) end = true;
-            if (++steps_path > (uint32_t)kPathCap) {
-                guard(sc, 6);
-                end = true;
-            }
+            if (--left == 0u) end = true;
             if (end) alive = false;
         }
     }
@@ -576,7 +577,7 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     wv.lanes = (unsigned long long)blocksA * 256ull;
     const unsigned long long inflight = wv.lanes < n_paths ? wv.lanes : n_paths;
     wv.res_jobs = inflight * lights * B;
-    wv.res_recs = inflight * B;
+    wv.res_recs = inflight * (B + 1);  // B records and the reserved slot after the last one
     // room for three vertex records per path (the NEE_DS primal's majorant and
     // epsilon collisions make more vertices than the forward's: 2.3 per path
     // on the benchmark medium)
@@ -594,7 +595,7 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     const size_t o_recs = o_dldt + ((wv.cap_jobs * 4 + 255) & ~(size_t)255);
     const size_t o_info = o_recs + wv.cap_recs * sizeof(VertexRec), o_over = o_info + wv.cap_paths * 32;
     const size_t o_list = o_over + ((wv.cap_paths * 4 + 255) & ~(size_t)255);
-    const size_t o_evs = o_list + ((wv.cap_paths * 8 + 255) & ~(size_t)255), bytes = o_evs + wv.cap_evs * 32;
+    const size_t o_evs = o_list + ((wv.cap_paths * 16 + 255) & ~(size_t)255), bytes = o_evs + wv.cap_evs * 32;
     int st = ensure_wave_buffer(ctx, bytes);
     if (st) return st;
     char* base = static_cast<char*>(ctx->wave);
@@ -604,7 +605,7 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     wv.recs = reinterpret_cast<VertexRec*>(base + o_recs);
     wv.info = reinterpret_cast<float*>(base + o_info);
     wv.over = reinterpret_cast<uint32_t*>(base + o_over);
-    wv.list = reinterpret_cast<uint2*>(base + o_list);
+    wv.list = reinterpret_cast<uint4*>(base + o_list);
     wv.evs = reinterpret_cast<CollisionRec*>(base + o_evs);
     wv.p_begin = 0;
     cudaError_t e = cudaMemsetAsync(&ctx->scratch->next_path, 0, sizeof(unsigned long long), stream);
