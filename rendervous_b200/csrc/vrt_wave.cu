@@ -59,6 +59,10 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
     uint32_t steps_path = 0;
     bool alive = false, exhausted = false;
     uint32_t n_paths_done = 0, n_verts = 0;
+    // the job slot reserved for the direct term of the lane's next path (taken
+    // with the collision jobs of an iteration, so a path start needs no scan of
+    // its own; ~0: none yet)
+    unsigned long long dslot = ~0ull;
     Tally tl;
 
     while (true) {
@@ -116,16 +120,22 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                         q[3 * wv.rows + 2] = 1.0f;
                         q[6 * wv.rows] = q[6 * wv.rows + 1] = q[6 * wv.rows + 2] = 0.0f;
                     }
-                    njobs = 1;
-                    jx = x;
-                    jd = w;
-                    jw = M.env;
-                    jfork = rng.ntr++;
+                    const uint32_t f = rng.ntr++;
+                    if (dslot != ~0ull) {
+                        put_job(wv.jobs, dslot, x, w, M.env, job_key(pid, f));
+                        dslot = ~0ull;
+                    } else {
+                        njobs = 1;
+                        jx = x;
+                        jd = w;
+                        jw = M.env;
+                        jfork = f;
+                    }
                     alive = d > EPS;
                 }
             }
         }
-        {  // direct-term jobs of the lanes just started
+        {  // direct-term jobs of the lanes that had no reserved slot (their first path)
             const unsigned long long slot = reserve_slots(wv.count, njobs);
             if (njobs) put_job(wv.jobs, slot, jx, jd, jw, job_key(pid, jfork));
         }
@@ -225,13 +235,19 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                 alive = false;
             }
         }
-        {
-            const unsigned long long slot = reserve_slots(wv.count, njobs);
+        {  // the collision's light jobs, and a direct-term slot for the lane's next path
+            const int nd = (dslot == ~0ull && !exhausted) ? 1 : 0;
+            const unsigned long long slot = reserve_slots(wv.count, njobs + nd);
             if (njobs) {
                 put_job(wv.jobs, slot, jx, jd, jw, job_key(pid, jfork));
                 if (njobs == 2) put_job(wv.jobs, slot + 1, jx, M.sun_dir, jw2, job_key(pid, jfork + 1));
             }
+            if (nd) dslot = slot + (unsigned long long)njobs;
         }
+    }
+    if (dslot != ~0ull) {  // an unused reserved slot: a ray that misses the medium and adds nothing
+        const float nan = __int_as_float(0x7fc00000);
+        put_job(wv.jobs, dslot, f3(nan), f3(nan), f3(0.0f), 0ull);
     }
     flush_counters(sc, VRT_K_WALK_FW, n_paths_done, n_verts, tl);
 }
@@ -437,7 +453,7 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
     // the worst case of every path in flight, plus room for a round's expected jobs
     unsigned long long inflight = (unsigned long long)blocks * 256ull;
     if (inflight > n_paths) inflight = n_paths;
-    const unsigned long long reserve = inflight * per_path;
+    const unsigned long long reserve = inflight * (per_path + 1);  // + the reserved direct-term slot
     const unsigned long long cap = reserve + batch_jobs(n_paths, 1ull + lights);
     int st = ensure_wave_buffer(ctx, 256 + cap * sizeof(ShadowJob));
     if (st) return st;
