@@ -166,6 +166,28 @@ __device__ __forceinline__ float sigma(const DMedium& M, float3 x, Tally& tl) {
 // Grid3D BACKWARD (include/maps/grid3d.h:39-75): 8 atomic adds per channel.
 __device__ __forceinline__ void red_add(float* p, float v) { atomicAdd(p, v); }
 
+// Two adjacent floats added by one vector atomic (sm_90+) when the first is
+// 8-byte aligned, else by two scalar ones; each component is still its own
+// atomic add of the same value.
+__device__ __forceinline__ void red_add2(float* p, float a, float b) {
+    if ((reinterpret_cast<uintptr_t>(p) & 7u) == 0u) {
+        atomicAdd(reinterpret_cast<float2*>(p), make_float2(a, b));
+    } else {
+        atomicAdd(p, a);
+        atomicAdd(p + 1, b);
+    }
+}
+// Three adjacent floats (one node's channels): a vector pair and a scalar.
+__device__ __forceinline__ void red_add3(float* p, float a, float b, float c) {
+    if ((reinterpret_cast<uintptr_t>(p) & 7u) == 0u) {
+        atomicAdd(reinterpret_cast<float2*>(p), make_float2(a, b));
+        atomicAdd(p + 2, c);
+    } else {
+        atomicAdd(p, a);
+        atomicAdd(reinterpret_cast<float2*>(p + 1), make_float2(b, c));
+    }
+}
+
 __device__ __forceinline__ void grid_scatter(const DGrid& g, float3 nc, const float* dout, int C) {
     if (!g.grad) return;
     if (nc.x < 0.0f || nc.y < 0.0f || nc.z < 0.0f || nc.x >= 1.0f || nc.y >= 1.0f || nc.z >= 1.0f) return;
@@ -175,6 +197,29 @@ __device__ __forceinline__ void grid_scatter(const DGrid& g, float3 nc, const fl
     int px = min(max((int)gx, 0), dx - 1), py = min(max((int)gy, 0), dy - 1), pz = min(max((int)gz, 0), dz - 1);
     float* b = g.grad + (pz * g.sD + py * g.sH + px * g.sW);
     float bx = 1.0f - ax, by = 1.0f - ay, bz = 1.0f - az;
+    if (C == 1 && g.sW == 1) {  // x-neighbours adjacent: the four x-pairs as vector pairs where aligned
+        const float d = dout[0];
+        red_add2(b, d * bx * by * bz, d * ax * by * bz);
+        red_add2(b + g.sH, d * bx * ay * bz, d * ax * ay * bz);
+        red_add2(b + g.sD, d * bx * by * az, d * ax * by * az);
+        red_add2(b + g.sD + g.sH, d * bx * ay * az, d * ax * ay * az);
+        return;
+    }
+    if (C == 3) {  // a node's three channels adjacent (channel stride 1)
+        const float d0 = dout[0], d1 = dout[1], d2 = dout[2];
+        // the same products, in the same order, as the per-channel form below
+#define VRT_CORNER(o, fx, fy, fz) red_add3(b + (o), d0 * fx * fy * fz, d1 * fx * fy * fz, d2 * fx * fy * fz)
+        VRT_CORNER(0, bx, by, bz);
+        VRT_CORNER(g.sW, ax, by, bz);
+        VRT_CORNER(g.sH, bx, ay, bz);
+        VRT_CORNER(g.sH + g.sW, ax, ay, bz);
+        VRT_CORNER(g.sD, bx, by, az);
+        VRT_CORNER(g.sD + g.sW, ax, by, az);
+        VRT_CORNER(g.sD + g.sH, bx, ay, az);
+        VRT_CORNER(g.sD + g.sH + g.sW, ax, ay, az);
+#undef VRT_CORNER
+        return;
+    }
     for (int i = 0; i < C; ++i) {
         float d = dout[i];
         red_add(b + i, d * bx * by * bz);
