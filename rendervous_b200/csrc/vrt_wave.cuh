@@ -245,7 +245,8 @@ __device__ __forceinline__ bool shadow_begin(const DMedium& M, ShadowRay& s, flo
     return true;
 }
 
-// One step: brick crossings (at most kCross) up to the next tracking
+// One step: brick crossings (at most kCross, kCrossBw in the adjoint's first
+// pass) up to the next tracking
 // collision, then that collision.  TR 0 ratio tracking, 1 delta tracking; BW:
 // the adjoint's first pass (majorant + 0.1, ratio-tracking roulette below
 // 0.1).  The lanes of a warp cross bricks in the inner loop and meet for the
@@ -254,7 +255,8 @@ __device__ __forceinline__ bool shadow_begin(const DMedium& M, ShadowRay& s, flo
 // collision that continues the ray, hit is set with the majorant and the
 // factor the adjoint's second pass scatters with (RT: r = 1 - sigma/maj; DT:
 // Pc = sigma/maj).
-constexpr int kCross = 8;
+constexpr int kCross = 6;    // forward transmittances (k_shadow_run)
+constexpr int kCrossBw = 8;  // the transmittance adjoint's first pass (k_shadow_adj)
 // The same bound for the path walks (measured per kernel): a flight that needs
 // more brick crossings leaves the crossing loop without an event and resumes
 // in the next iteration, so the warp's long flights do not hold the others.
@@ -285,7 +287,7 @@ __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tal
                 s.d -= md;
                 s.ff.cross(maj, md);
                 s.ff.bk.advance(M);
-                if (c + 1 >= kCross) return false;
+                if (c + 1 >= (BW ? kCrossBw : kCross)) return false;
                 continue;
             }
             t = tau / maj;
@@ -303,7 +305,7 @@ __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tal
             if (crosses) {
                 s.ff.cross(maj, md);
                 s.ff.bk.advance(M);
-                if (c + 1 >= kCross) return false;
+                if (c + 1 >= (BW ? kCrossBw : kCross)) return false;
                 continue;
             }
         }
