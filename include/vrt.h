@@ -97,12 +97,20 @@ typedef struct vrt_medium {
     int32_t ds_compat;               /* 1: reference replay majorant of NEE_DS bw */
 } vrt_medium;
 
-/* PerspectiveCameraSensor (rendervous _maps.py:1765-1802). */
+/* PerspectiveCameraSensor (rendervous _maps.py:1765-1802).  sensors == NULL:
+   every pixel of every view (image [views, H, W, 3]); else a sensors batch of
+   n_sensors (view, row, col) triples (SensorsBase.capture's sensors_batch,
+   _maps.py:1741-1749; image [n_sensors, 3], sample s of sensor k is Philox
+   path id s * n_sensors + k).  A triple outside the camera is recorded as
+   VRT_E_INVALID_ARGUMENT (returned by vrt_context_sync) and its pixel's value
+   is undefined. */
 typedef struct vrt_camera {
     const float* poses;              /* [views, 9]: origin, direction, up */
     int32_t views, height, width;
     float fov, znear;
     int32_t jittered;
+    const int64_t* sensors;          /* device [n_sensors, 3] int64, or NULL */
+    int64_t n_sensors;
 } vrt_camera;
 
 typedef struct vrt_counters {
@@ -192,18 +200,22 @@ int vrt_transmittance_bw(vrt_context* ctx, const vrt_medium* m, int32_t mode, co
                          uint64_t seed, const float* dL_dT, void* stream);
 
 /* Transmittance forward for callers that cannot allocate device memory (no
-   counterpart in the reference).  Same result as vrt_transmittance_fw, but it
-   needs no vrt_context: with brick > 0 and a tracking mode (RT, DT) it builds
-   the brick^3 majorant grid of m->sigma into a fixed array inside libvrt.so
-   and tracks against it; with brick == 0 it uses m's own majorant.  The array
-   holds at most 64^3 bricks (1 MiB, kept on every device that loads the
-   library until exit); larger grids return VRT_E_BAD_SHAPE.  All calls share
-   the array, so calls that overlap on the GPU race.  The first call on a
-   device looks up the array's address; make it before any stream capture.
-   Device-side counters and the error word are cleared per call and not
-   reported. */
+   counterpart in the reference): code running inside another framework's
+   pre-sized memory pool, or plugins that must not grow the device footprint.
+   Same result as vrt_transmittance_fw, but it needs no vrt_context: with
+   brick > 0 and a tracking mode (RT, DT) it builds the brick^3 majorant grid
+   of m->sigma into a fixed array inside libvrt.so and tracks against it; with
+   brick == 0 it uses m's own majorant.  The array holds at most 64^3 bricks
+   (1 MiB, kept on every device that loads the library until exit); larger
+   grids return VRT_E_BAD_SHAPE.  All calls share the array, so calls that
+   overlap on the GPU race.  The first call in a CUDA context looks up the
+   array's address; make it before any stream capture.  Every argument is
+   checked before the first launch.  status_out == NULL: the call stays
+   asynchronous and device-side errors (an iteration cap hit) are not
+   reported.  status_out != NULL: the call waits for `stream`, stores the
+   device error bits (1 << VRT_E_*) there and returns the first of them. */
 int vrt_transmittance_fw_noalloc(const vrt_medium* m, int32_t mode, int32_t brick, const float* rays, int64_t n,
-                                 uint64_t seed, float* T, void* stream);
+                                 uint64_t seed, float* T, int64_t* status_out, void* stream);
 
 /* Path integrator as a map on rays [n,6] -> R [n,3] (DeltatrackingPathIntegrator,
    DeltatrackingNEEPathIntegrator, DRTPathIntegrator, _maps.py:2886-3022; path i

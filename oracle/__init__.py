@@ -115,7 +115,23 @@ class OracleScene:
         g.D, g.H, g.W, g.C = [int(v) for v in arr.shape]
 
 
-def make_camera(poses: np.ndarray, width: int, height: int, fov: float, jittered: bool, znear: float = 0.001):
+class _CameraKeep:
+    """The numpy buffers an orc_camera points into, and the capture's image shape."""
+
+    def __init__(self, poses, sensors, height, width):
+        self.poses = poses
+        self.sensors = sensors
+        self.shape = ((poses.shape[0], height, width) if sensors is None else (sensors.shape[0],))
+
+    @property
+    def npix(self) -> int:
+        return int(np.prod(self.shape))
+
+
+def make_camera(poses: np.ndarray, width: int, height: int, fov: float, jittered: bool, znear: float = 0.001,
+                sensors: np.ndarray | None = None):
+    """orc_camera over every pixel of every view, or over a sensors batch
+    [n, 3] of (view, row, col) (SensorsBase.capture's sensors_batch)."""
     ffi, _ = lib()
     poses = np.ascontiguousarray(poses, dtype=np.float32).reshape(-1, 9)
     cam = ffi.new("orc_camera *")
@@ -126,7 +142,11 @@ def make_camera(poses: np.ndarray, width: int, height: int, fov: float, jittered
     cam.fov = float(fov)
     cam.znear = float(znear)
     cam.jittered = 1 if jittered else 0
-    return cam, poses
+    if sensors is not None:
+        sensors = np.ascontiguousarray(sensors, dtype=np.int64).reshape(-1, 3)
+        cam.sensors = ffi.cast("int64_t *", sensors.ctypes.data)
+        cam.n_sensors = sensors.shape[0]
+    return cam, _CameraKeep(poses, sensors, height, width)
 
 
 # ---------------------------------------------------------------- wrappers --
@@ -224,6 +244,15 @@ def transmittance_bw(scene: OracleScene, mode: str, rays: np.ndarray, seed: int,
     L.orc_transmittance_bw(scene.s, TRANSMITTANCE_MODES[mode], ptr(ffi, rays), rays.shape[0], seed, ptr(ffi, g))
 
 
+def dda_tau_fp64(scene: OracleScene, rays: np.ndarray, exact: bool = False) -> np.ndarray:
+    """The DDA's optical depth along each ray, in FP64 (no exp)."""
+    ffi, L = lib()
+    rays = np.ascontiguousarray(rays, np.float32)
+    out = np.empty(rays.shape[0], np.float64)
+    L.orc_dda_tau_fp64(scene.s, int(exact), ptr(ffi, rays), rays.shape[0], ptr(ffi, out, "double *"))
+    return out
+
+
 def tau_raymarch_fp64(scene: OracleScene, rays: np.ndarray, substeps: int = 32) -> np.ndarray:
     ffi, L = lib()
     rays = np.ascontiguousarray(rays, np.float32)
@@ -271,19 +300,22 @@ def radiance_bw(scene: OracleScene, bw_mode: str, rays: np.ndarray, seed: int, d
     L.orc_radiance_bw(scene.s, BW_MODES[bw_mode], ptr(ffi, rays), rays.shape[0], seed, ptr(ffi, g))
 
 
-def capture_fw(scene: OracleScene, integrator: str, poses, width, height, fov, jittered, spp, seed):
+def capture_fw(scene: OracleScene, integrator: str, poses, width, height, fov, jittered, spp, seed, sensors=None):
+    """[views, H, W, 3], or [n, 3] for a sensors batch [n, 3] of (view, row, col)."""
     ffi, L = lib()
-    cam, keep = make_camera(poses, width, height, fov, jittered)
-    out = np.empty((keep.shape[0], height, width, 3), np.float32)
+    cam, keep = make_camera(poses, width, height, fov, jittered, sensors=sensors)
+    out = np.empty(keep.shape + (3,), np.float32)
     c = ffi.new("orc_counters *")
     L.orc_capture_fw(scene.s, INTEGRATORS[integrator], cam, spp, seed, ptr(ffi, out), c)
     return out, dict(paths=c.paths, vertices=c.vertices, steps=c.steps)
 
 
-def capture_bw(scene: OracleScene, bw_mode: str, poses, width, height, fov, jittered, spp, seed, dL_drgb) -> None:
+def capture_bw(scene: OracleScene, bw_mode: str, poses, width, height, fov, jittered, spp, seed, dL_drgb,
+               sensors=None) -> None:
     ffi, L = lib()
-    cam, keep = make_camera(poses, width, height, fov, jittered)
+    cam, keep = make_camera(poses, width, height, fov, jittered, sensors=sensors)
     g = np.ascontiguousarray(dL_drgb, np.float32)
+    assert g.size == 3 * keep.npix
     L.orc_capture_bw(scene.s, BW_MODES[bw_mode], cam, spp, seed, ptr(ffi, g))
 
 

@@ -69,6 +69,8 @@ typedef struct orc_camera {
     int32_t views, height, width;
     float fov, znear;
     int32_t jittered;
+    const int64_t* sensors;       /* NULL: every pixel; else [n_sensors, 3] (view, row, col) */
+    int64_t n_sensors;
 } orc_camera;
 
 typedef struct orc_counters {
@@ -91,6 +93,8 @@ void orc_majorant_query(const orc_scene* s, const float* rays, int64_t n, float*
 /* mode: 0 RT, 1 DT, 2 DDA midpoint, 3 DDA exact */
 void orc_transmittance_fw(const orc_scene* s, int32_t mode, const float* rays, int64_t n, uint64_t seed, int32_t fp64, float* T);
 void orc_transmittance_bw(const orc_scene* s, int32_t mode, const float* rays, int64_t n, uint64_t seed, const float* dL_dT);
+/* The DDA's optical depth (midpoint or exact rule) in FP64 */
+void orc_dda_tau_fp64(const orc_scene* s, int32_t exact, const float* rays, int64_t n, double* tau);
 /* FP64 fine ray-march of tau = int sigma along the ray, sigma read with the DDA-side clamping lookup */
 void orc_tau_raymarch_fp64(const orc_scene* s, const float* rays, int64_t n, int32_t substeps, double* tau);
 

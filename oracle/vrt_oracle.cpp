@@ -1738,6 +1738,23 @@ void camera_ray(const orc_camera& cam, int view, int row, int col, Rng& rng, V3<
 
 inline uint64_t capture_path_id(int64_t pixel, int s, int64_t npix) { return (uint64_t)s * (uint64_t)npix + (uint64_t)pixel; }
 
+// Sensors of a capture (SensorsBase.capture, _maps.py:1741-1749, and the
+// capture kernel's index decoding, _maps.py:560-577): every pixel of every
+// view in raster order, or the (view, row, col) triples of a sensors batch.
+inline int64_t camera_npix(const orc_camera& cam) {
+    return cam.sensors ? cam.n_sensors : (int64_t)cam.views * cam.height * cam.width;
+}
+inline void camera_pixel(const orc_camera& cam, int64_t p, int& view, int& row, int& col) {
+    if (cam.sensors) {
+        view = (int)cam.sensors[3 * p]; row = (int)cam.sensors[3 * p + 1]; col = (int)cam.sensors[3 * p + 2];
+        return;
+    }
+    view = (int)(p / ((int64_t)cam.height * cam.width));
+    int rem = (int)(p % ((int64_t)cam.height * cam.width));
+    row = rem / cam.width;
+    col = rem % cam.width;
+}
+
 // pixel of a radiance-cache training path: the path's first draw, scaled to npix
 inline int64_t random_pixel(Rng& rng, int64_t npix) { return (int64_t)(((uint64_t)rng.u32() * (uint64_t)npix) >> 32); }
 
@@ -1858,6 +1875,17 @@ void orc_transmittance_bw(const orc_scene* s, int32_t mode, const float* rays, i
     }
 }
 
+// The DDA's optical depth in FP64 (vr_transmittance_DDA.h:1-59 without the
+// final exp): the quantity whose central differences check the DDA adjoint.
+void orc_dda_tau_fp64(const orc_scene* s, int32_t exact, const float* rays, int64_t n, double* tau) {
+    Scene<double> S(*s);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i) {
+        DDA<double> dda(S, V3<double>::load(rays + 6 * i), V3<double>::load(rays + 6 * i + 3));
+        tau[i] = dda.valid ? dda.tau(exact != 0, nullptr) : 0.0;
+    }
+}
+
 // FP64 fine ray-march (extension, reference for the DDA modes): tau over the
 // same clipped segment, split into `substeps` pieces per cell size along the
 // ray, each integrated with two-point Gauss-Legendre of the trilinear field
@@ -1922,14 +1950,14 @@ void orc_env_sample(const orc_scene* s, int64_t n, uint64_t seed, float* out6) {
 }
 
 void orc_camera_rays(const orc_camera* cam, int32_t spp, uint64_t seed, float* out6) {
-    int64_t npix = (int64_t)cam->views * cam->height * cam->width;
+    int64_t npix = camera_npix(*cam);
     for (int s = 0; s < spp; ++s)
         for (int64_t p = 0; p < npix; ++p) {
-            int view = (int)(p / ((int64_t)cam->height * cam->width));
-            int rem = (int)(p % ((int64_t)cam->height * cam->width));
+            int view, row, col;
+            camera_pixel(*cam, p, view, row, col);
             Rng rng(seed, capture_path_id(p, s, npix), 0);
             V3<float> x, w;
-            camera_ray(*cam, view, rem / cam->width, rem % cam->width, rng, x, w);
+            camera_ray(*cam, view, row, col, rng, x, w);
             float* o = out6 + 6 * ((int64_t)s * npix + p);
             o[0] = x.x; o[1] = x.y; o[2] = x.z; o[3] = w.x; o[4] = w.y; o[5] = w.z;
         }
@@ -1962,18 +1990,18 @@ void orc_radiance_bw(const orc_scene* s, int32_t bw_mode, const float* rays, int
 
 void orc_capture_fw(const orc_scene* s, int32_t integrator, const orc_camera* cam, int32_t spp, uint64_t seed, float* rgb, orc_counters* c) {
     Scene<float> S(*s);
-    int64_t npix = (int64_t)cam->views * cam->height * cam->width;
+    int64_t npix = camera_npix(*cam);
     int64_t verts = 0, steps = 0;
 #pragma omp parallel for schedule(dynamic, 16) reduction(+ : verts, steps)
     for (int64_t p = 0; p < npix; ++p) {
-        int view = (int)(p / ((int64_t)cam->height * cam->width));
-        int rem = (int)(p % ((int64_t)cam->height * cam->width));
+        int view, row, col;
+        camera_pixel(*cam, p, view, row, col);
         V3<float> acc(0.0f);
         Counters cnt;
         for (int sidx = 0; sidx < spp; ++sidx) {
             Rng rng(seed, capture_path_id(p, sidx, npix), 0);
             V3<float> x, w;
-            camera_ray(*cam, view, rem / cam->width, rem % cam->width, rng, x, w);
+            camera_ray(*cam, view, row, col, rng, x, w);
             acc += radiance(S, integrator, rng, x, w, cnt);
         }
         rgb[3 * p] = acc.x / (float)spp;
@@ -1988,19 +2016,19 @@ void orc_capture_fw(const orc_scene* s, int32_t integrator, const orc_camera* ca
 void orc_capture_prefix(const orc_scene* s, const orc_camera* cam, int32_t spp, uint64_t seed, int32_t cut, float* rgb,
                         float* queries) {
     Scene<float> S(*s);
-    int64_t npix = (int64_t)cam->views * cam->height * cam->width;
+    int64_t npix = camera_npix(*cam);
     int64_t n = npix * spp;
 #pragma omp parallel for schedule(dynamic, 16)
     for (int64_t p = 0; p < npix; ++p) {
-        int view = (int)(p / ((int64_t)cam->height * cam->width));
-        int rem = (int)(p % ((int64_t)cam->height * cam->width));
+        int view, row, col;
+        camera_pixel(*cam, p, view, row, col);
         V3<float> acc(0.0f);
         Counters cnt;
         for (int sidx = 0; sidx < spp; ++sidx) {
             uint64_t pid = capture_path_id(p, sidx, npix);
             Rng rng(seed, pid, 0);
             V3<float> x, w;
-            camera_ray(*cam, view, rem / cam->width, rem % cam->width, rng, x, w);
+            camera_ray(*cam, view, row, col, rng, x, w);
             PathHooks<float> hk;
             hk.cut = cut;
             acc += path_integrator_NEE(S, rng, x, w, false, cnt, &hk);
@@ -2054,16 +2082,16 @@ void orc_train_samples(const orc_scene* s, const orc_camera* cam, int64_t n_path
 
 void orc_capture_bw(const orc_scene* s, int32_t bw_mode, const orc_camera* cam, int32_t spp, uint64_t seed, const float* dL_drgb) {
     Scene<float> S(*s);
-    int64_t npix = (int64_t)cam->views * cam->height * cam->width;
+    int64_t npix = camera_npix(*cam);
 #pragma omp parallel for schedule(dynamic, 16)
     for (int64_t p = 0; p < npix; ++p) {
-        int view = (int)(p / ((int64_t)cam->height * cam->width));
-        int rem = (int)(p % ((int64_t)cam->height * cam->width));
+        int view, row, col;
+        camera_pixel(*cam, p, view, row, col);
         V3<float> dL = V3<float>::load(dL_drgb + 3 * p) / (float)spp;
         for (int sidx = 0; sidx < spp; ++sidx) {
             Rng rng(seed, capture_path_id(p, sidx, npix), 0);
             V3<float> x, w;
-            camera_ray(*cam, view, rem / cam->width, rem % cam->width, rng, x, w);
+            camera_ray(*cam, view, row, col, rng, x, w);
             radiance_bw(S, bw_mode, rng, x, w, dL);
         }
     }

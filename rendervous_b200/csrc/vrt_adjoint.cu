@@ -166,10 +166,7 @@ __global__ void __launch_bounds__(256, 2) k_nee_ds_bw(DMedium M, PathSrc S, uint
                     L.rng.init(seed, pid, 0);
                     if (S.is_camera) {
                         long long p = (long long)(pid % (uint64_t)S.npix);
-                        long long hw = (long long)S.cam.height * S.cam.width;
-                        int view = (int)(p / hw);
-                        int rem = (int)(p - (long long)view * hw);
-                        camera_ray(S.cam, view, rem / S.cam.width, rem % S.cam.width, L.rng, L.x0, L.w0);
+                        camera_pixel_ray(S.cam, p, L.rng, L.x0, L.w0, &sc->status);
                         L.oidx = p;
                     } else {
                         L.x0 = ld3(S.rays + 6 * pid);

@@ -286,10 +286,17 @@ static int to_dcamera(const vrt_camera* c, DCamera& C) {
     if (!c->poses) return VRT_E_NULL_POINTER;
     if (c->views < 1 || c->height < 1 || c->width < 1) return VRT_E_BAD_SHAPE;
     if (!std::isfinite(c->fov) || !std::isfinite(c->znear) || c->fov <= 0.0f || c->znear <= 0.0f) return VRT_E_INVALID_ARGUMENT;
+    if (c->sensors && c->n_sensors < 1) return VRT_E_BAD_SHAPE;
     C.poses = c->poses;
     C.views = c->views; C.height = c->height; C.width = c->width;
     C.fov = c->fov; C.znear = c->znear; C.jittered = c->jittered ? 1 : 0;
+    C.sensors = reinterpret_cast<const long long*>(c->sensors);
     return VRT_OK;
+}
+
+// pixels of a capture: every pixel of every view, or the sensors batch
+static long long capture_pixels(const vrt_camera* c) {
+    return c->sensors ? (long long)c->n_sensors : (long long)c->views * c->height * c->width;
 }
 
 static int check_ctx(vrt_context* ctx) {
@@ -578,7 +585,7 @@ int vrt_capture_fw(vrt_context* ctx, const vrt_medium* m, int32_t integrator, co
     if ((st = to_dcamera(cam, S.cam))) return st;
     if (!rgb) return VRT_E_NULL_POINTER;
     S.is_camera = 1;
-    S.npix = (long long)S.cam.views * S.cam.height * S.cam.width;
+    S.npix = capture_pixels(cam);
     cudaError_t e = cudaMemsetAsync(rgb, 0, sizeof(float) * 3 * S.npix, (cudaStream_t)stream);
     if (e != cudaSuccess) return launch_status(e);
     if (use_wave(M, integrator))
@@ -601,7 +608,7 @@ int vrt_capture_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const
     if ((st = to_dcamera(cam, S.cam))) return st;
     if (!dL_drgb) return VRT_E_NULL_POINTER;
     S.is_camera = 1;
-    S.npix = (long long)S.cam.views * S.cam.height * S.cam.width;
+    S.npix = capture_pixels(cam);
     if (use_wave_bw(M, bw_mode))
         return launch_wave_ds_bw(ctx, M, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
                                  (cudaStream_t)stream);
@@ -621,7 +628,7 @@ int vrt_capture_prefix_fw(vrt_context* ctx, const vrt_medium* m, const vrt_camer
     if ((st = to_dcamera(cam, S.cam))) return st;
     if (!rgb || !queries) return VRT_E_NULL_POINTER;
     S.is_camera = 1;
-    S.npix = (long long)S.cam.views * S.cam.height * S.cam.width;
+    S.npix = capture_pixels(cam);
     const uint64_t n = (uint64_t)S.npix * (uint64_t)spp;
     // the wavefront forward with a cut (its job reserve is bounded by the cut,
     // capped or not); very deep cuts stay on the per-lane state machine
@@ -646,7 +653,7 @@ int vrt_capture_train_samples(vrt_context* ctx, const vrt_medium* m, const vrt_c
     if ((st = to_dcamera(cam, S.cam))) return st;
     if (!samples || !work) return VRT_E_NULL_POINTER;
     S.is_camera = 1;
-    S.npix = (long long)S.cam.views * S.cam.height * S.cam.width;
+    S.npix = capture_pixels(cam);
     if (S.npix >= (1ll << 32)) return VRT_E_BAD_SHAPE;
     if (n_paths == 0) return VRT_OK;
     float* pR = work;

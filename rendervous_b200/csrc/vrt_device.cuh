@@ -414,6 +414,33 @@ __device__ __forceinline__ void camera_ray(const DCamera& C, int view, int row, 
     w = normalize(w);
 }
 
+// Primary ray of capture pixel px (0 <= px < npix): pixels of all views in
+// raster order, or entry px of a sensors batch (the capture kernel's index
+// decoding, _maps.py:560-577).  A sensors entry outside the camera sets the
+// invalid-argument bit and returns false (the path adds nothing).
+__device__ __forceinline__ bool camera_pixel_ray(const DCamera& C, long long px, Rng& rng, float3& x, float3& w,
+                                                 uint32_t* status) {
+    int view, row, col;
+    if (C.sensors) {
+        const long long v = C.sensors[3 * px], r = C.sensors[3 * px + 1], c = C.sensors[3 * px + 2];
+        if (v < 0 || v >= C.views || r < 0 || r >= C.height || c < 0 || c >= C.width) {
+            if (status) atomicOr(status, 1u << 1);
+            x = make_float3(0.0f, 0.0f, 0.0f);
+            w = make_float3(__int_as_float(0x7fc00000), 0.0f, 0.0f);  // a NaN ray misses the medium
+            return false;
+        }
+        view = (int)v; row = (int)r; col = (int)c;
+    } else {
+        const long long hw = (long long)C.height * C.width;
+        view = (int)(px / hw);
+        const int rem = (int)(px - (long long)view * hw);
+        row = rem / C.width;
+        col = rem % C.width;
+    }
+    camera_ray(C, view, row, col, rng, x, w);
+    return true;
+}
+
 // ------------------------------------------------------------ diagnostics --
 __device__ __forceinline__ void raise_status(uint32_t* status, int code) {
     if (status) atomicOr(status, 1u << code);

@@ -43,6 +43,7 @@ struct DCamera {
     int views, height, width;
     float fov, znear;
     int jittered;
+    const long long* sensors;  // [npix, 3] (view, row, col) of a sensors batch, or null: every pixel
 };
 
 // Device scratch owned by a context.

@@ -30,10 +30,7 @@ __device__ __forceinline__ void primary_ray(const PathSrc& S, uint64_t pid, Rng&
                                             long long& oidx) {
     if (S.is_camera) {
         long long p = (long long)(pid % (uint64_t)S.npix);
-        long long hw = (long long)S.cam.height * S.cam.width;
-        int view = (int)(p / hw);
-        int rem = (int)(p - (long long)view * hw);
-        camera_ray(S.cam, view, rem / S.cam.width, rem % S.cam.width, rng, x, w);
+        camera_pixel_ray(S.cam, p, rng, x, w, nullptr);  // sensor triples are checked on the host
         oidx = p;
     } else {
         x = ld3(S.rays + 6 * pid);

@@ -92,16 +92,7 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                     pid = p;
                     rng.init(seed, pid, 0);
                     float3 x0, w0;
-                    if (S.is_camera) {
-                        const long long px = (long long)(pid % (uint64_t)S.npix);
-                        const long long hw = (long long)S.cam.height * S.cam.width;
-                        const int view = (int)(px / hw);
-                        const int rem = (int)(px - (long long)view * hw);
-                        camera_ray(S.cam, view, rem / S.cam.width, rem % S.cam.width, rng, x0, w0);
-                    } else {
-                        x0 = ld3(S.rays + 6 * pid);
-                        w0 = ld3(S.rays + 6 * pid + 3);
-                    }
+                    start_ray(S, pid, rng, x0, w0, sc);
                     float tMin, tMax;
                     boundary(M, x0, w0, tMin, tMax);
                     x = x0 + w0 * tMin;

@@ -190,13 +190,10 @@ __device__ __forceinline__ float shadow_T(const DMedium& M, Rng& r, float3 x, fl
 }
 
 // The primary ray of path pid (camera or ray input), with the camera's draws.
-__device__ __forceinline__ void start_ray(const PathSrc& S, uint64_t pid, Rng& rng, float3& x0, float3& w0) {
+__device__ __forceinline__ void start_ray(const PathSrc& S, uint64_t pid, Rng& rng, float3& x0, float3& w0,
+                                          DScratch* sc) {
     if (S.is_camera) {
-        const long long px = (long long)(pid % (uint64_t)S.npix);
-        const long long hw = (long long)S.cam.height * S.cam.width;
-        const int view = (int)(px / hw);
-        const int rem = (int)(px - (long long)view * hw);
-        camera_ray(S.cam, view, rem / S.cam.width, rem % S.cam.width, rng, x0, w0);
+        camera_pixel_ray(S.cam, (long long)(pid % (uint64_t)S.npix), rng, x0, w0, &sc->status);
     } else {
         x0 = ld3(S.rays + 6 * pid);
         w0 = ld3(S.rays + 6 * pid + 3);

@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                     pid = p;
                     rng.init(seed, pid, 0);
                     float3 x0, w0;
-                    start_ray(S, pid, rng, x0, w0);
+                    start_ray(S, pid, rng, x0, w0, sc);
                     float tMin, tMax;
                     boundary(M, x0, w0, tMin, tMax);
                     x = x0 + w0 * tMin;
@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_rewalk(DMedium M, PathSrc S, uint
                     pid = wv.p_begin + k;
                     rng.init(seed, pid, 0);
                     float3 x0, w0;
-                    start_ray(S, pid, rng, x0, w0);
+                    start_ray(S, pid, rng, x0, w0, sc);
                     dLdR = ld3(dL + 3 * out_index(S, pid)) / div;
                     float tMin, tMax;
                     boundary(M, x0, w0, tMin, tMax);

@@ -13,8 +13,12 @@ import torch.distributed as dist
 
 
 def rank_seed(step: int, rank: int) -> int:
-    """Philox key of `rank`'s paths at `step` (distinct per rank and step)."""
-    return 1000 * (rank + 1) + step
+    """Philox key of `rank`'s paths at `step`: the rank in the key's high 32-bit
+    word and the step in the low one, so two (rank, step) pairs share a key only
+    if both are equal (steps below 2^32, ranks below 2^31)."""
+    if not (0 <= step < (1 << 32)) or not (0 <= rank < (1 << 31)):
+        raise ValueError(f"rank_seed: step {step} or rank {rank} out of range")
+    return ((rank + 1) << 32) | step
 
 
 def allreduce_grads(params) -> None:

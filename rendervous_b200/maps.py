@@ -607,17 +607,21 @@ class SPSPathIntegrator(DRTPathIntegrator):
 # ------------------------------------------------------------------ sensors --
 class _CaptureFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, sigma_grid, albedo_grid, camera, field, desc, fw_samples, bw_samples, seed):
+    def forward(ctx, sigma_grid, albedo_grid, camera, field, desc, fw_samples, bw_samples, seed, sensors):
         ffi, lib = _lib.ffi_lib()
         dev = sigma_grid.device
-        out = torch.empty(camera.views, camera.height, camera.width, 3, device=dev, dtype=torch.float32)
+        if sensors is None:
+            out = torch.empty(camera.views, camera.height, camera.width, 3, device=dev, dtype=torch.float32)
+        else:
+            out = torch.empty(*sensors.shape[:-1], 3, device=dev, dtype=torch.float32)
         m = desc.to_struct()
-        cam, keep = camera.to_struct(dev)
+        cam, keep = camera.to_struct(dev, sensors)
         vctx = _lib.context(dev)
         _lib.check(lib.vrt_capture_fw(vctx.ptr, m, field.FW, cam, fw_samples, seed, _lib.fptr(out),
                                       _lib.stream_handle(dev)), "vrt_capture_fw")
         _after_call(dev)
         ctx.desc, ctx.camera, ctx.field, ctx.bw_samples, ctx.seed = desc, camera, field, bw_samples, seed
+        ctx.sensors = sensors
         return out
 
     @staticmethod
@@ -631,13 +635,13 @@ class _CaptureFn(torch.autograd.Function):
             ffi, lib = _lib.ffi_lib()
             dev = desc.sigma.device
             m = desc.to_struct(sigma_grad=gs, albedo_grad=ga)
-            cam, keep = ctx.camera.to_struct(dev)
+            cam, keep = ctx.camera.to_struct(dev, ctx.sensors)
             d = dI.contiguous().float()
             vctx = _lib.context(dev)
             _lib.check(lib.vrt_capture_bw(vctx.ptr, m, ctx.field.BW, cam, ctx.bw_samples, ctx.seed, _lib.fptr(d),
                                           _lib.stream_handle(dev)), "vrt_capture_bw")
             _after_call(dev)
-        return gs, ga, None, None, None, None, None, None
+        return gs, ga, None, None, None, None, None, None, None
 
 
 class PerspectiveCameraSensor(MapBase):
@@ -653,7 +657,9 @@ class PerspectiveCameraSensor(MapBase):
         self.views = int(poses.shape[0])
         self.generation_mode = 0 if not jittered else 1
 
-    def to_struct(self, dev):
+    def to_struct(self, dev, sensors: typing.Optional[torch.Tensor] = None):
+        """The vrt_camera of this sensor, over every pixel or over a sensors
+        batch (an int64 [n, 3] tensor of (view, row, col) on `dev`)."""
         ffi, _ = _lib.ffi_lib()
         poses = self.poses.detach().to(device=dev, dtype=torch.float32).reshape(-1, 9).contiguous()
         c = ffi.new("vrt_camera *")
@@ -661,16 +667,49 @@ class PerspectiveCameraSensor(MapBase):
         c.views, c.height, c.width = poses.shape[0], self.height, self.width
         c.fov, c.znear = self.fov, self.znear
         c.jittered = self.generation_mode
-        return c, poses
+        if sensors is not None:
+            c.sensors = ffi.cast("int64_t *", sensors.data_ptr())
+            c.n_sensors = sensors.numel() // 3
+        return c, (poses, sensors)
+
+    @property
+    def index_shape(self) -> typing.Tuple[int, int, int]:
+        """Sensor index ranges (views, height, width) (SensorsBase.index_shape, _maps.py:1695)."""
+        return (self.views, self.height, self.width)
+
+    def random_sensors(self, batch_size: int, out: typing.Optional[torch.Tensor] = None) -> torch.Tensor:
+        """SensorsBase.random_sensors (_maps.py:1756-1765): batch_size uniform
+        (view, row, col) triples, int64 [batch_size, 3] on the current device."""
+        dev = device() if out is None else out.device
+        idx = torch.stack([torch.randint(0, d, (int(batch_size),), device=dev, dtype=torch.int64)
+                           for d in self.index_shape], dim=-1)
+        if out is None:
+            return idx
+        out.copy_(idx)
+        return out
+
+    def _checked_sensors(self, sensors_batch: torch.Tensor, dev) -> torch.Tensor:
+        if sensors_batch.shape[-1] != 3:
+            raise ValueError("sensors_batch must end in 3 indices (view, row, col)")
+        s = sensors_batch.to(device=dev, dtype=torch.int64).reshape(-1, 3).contiguous()
+        if s.shape[0] == 0:
+            raise ValueError("sensors_batch is empty")
+        lo = s.min(dim=0).values
+        hi = s.max(dim=0).values
+        lim = torch.tensor(self.index_shape, device=dev, dtype=torch.int64)
+        if bool((lo < 0).any()) or bool((hi >= lim).any()):
+            raise IndexError(f"sensors_batch indices outside the camera's {self.index_shape}")
+        return s.reshape(*sensors_batch.shape)
 
     def capture(self, field: MapBase, sensors_batch: typing.Optional[torch.Tensor] = None,
                 batch_size: typing.Optional[int] = None, fw_samples: int = 1, bw_samples: int = 1,
                 debug_out: typing.Optional[torch.Tensor] = None, seed: typing.Optional[int] = None) -> torch.Tensor:
         """SensorsBase.capture (_maps.py:1741-1749): [views, H, W, 3] mean of
-        fw_samples paths per pixel; backward replays bw_samples paths per pixel
-        with the same per-path Philox streams."""
-        if sensors_batch is not None:
-            raise NotImplementedError("capture of a sensor subset is not supported; capture all pixels")
+        fw_samples paths per pixel (or sensors_batch.shape[:-1] + [3] for a
+        batch of (view, row, col) sensors, e.g. from random_sensors); backward
+        replays bw_samples paths per pixel with the same per-path Philox
+        streams.  batch_size only splits the reference's dispatches; one
+        launch covers every sensor here, so it does not change the result."""
         if debug_out is not None:
             raise NotImplementedError("debug_out counters are reported by rendervous_b200.check() instead")
         if not isinstance(field, _PathIntegrator):
@@ -678,8 +717,9 @@ class PerspectiveCameraSensor(MapBase):
         field = field.cast(input_dim=6)
         desc = field.lower()
         sg, ag = field.grid_tensors()
+        sensors = None if sensors_batch is None else self._checked_sensors(sensors_batch, sg.device)
         return _CaptureFn.apply(sg, ag, self, field, desc, int(fw_samples), int(bw_samples),
-                                next_seed() if seed is None else int(seed))
+                                next_seed() if seed is None else int(seed), sensors)
 
 
 ZERO = const[0.0]

@@ -53,8 +53,11 @@ def _free_port() -> int:
 
 
 def test_rank_seeds_are_distinct():
-    seeds = {vdist.rank_seed(k, r) for k in range(100) for r in range(8)}
-    assert len(seeds) == 800
+    # past 1000 steps too (an earlier key, 1000 * (rank + 1) + step, repeated there)
+    seeds = {vdist.rank_seed(k, r) for k in range(5000) for r in range(8)}
+    assert len(seeds) == 5000 * 8
+    assert vdist.rank_seed(1000, 0) != vdist.rank_seed(0, 1)
+    assert all(0 < s < (1 << 62) for s in seeds)
 
 
 def test_two_rank_gradient_allreduce(tmp_path):

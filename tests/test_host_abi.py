@@ -75,6 +75,19 @@ def test_argument_validation_before_launch(lib):
     assert L.vrt_capture_fw(ffi.NULL, m, 0, ffi.NULL, 1, 0, ffi.NULL, ffi.NULL) == 2
     assert L.vrt_context_destroy(ffi.NULL) == 2
     assert L.vrt_context_sync(ffi.NULL, ffi.NULL, ffi.NULL) == 2
+    # the no-allocation transmittance checks everything before its first CUDA call
+    NA = L.vrt_transmittance_fw_noalloc
+    rays = ffi.cast("float *", 0x1000)
+    assert NA(ffi.NULL, 0, 0, rays, 1, 0, out, ffi.NULL, ffi.NULL) == 2          # null medium
+    assert NA(m, 9, 0, rays, 1, 0, out, ffi.NULL, ffi.NULL) == 1                 # bad mode
+    assert NA(m, 0, -1, rays, 1, 0, out, ffi.NULL, ffi.NULL) == 1                # bad brick
+    assert NA(m, 0, 0, rays, -1, 0, out, ffi.NULL, ffi.NULL) == 3                # n < 0
+    assert NA(m, 0, 0, ffi.NULL, 0, 0, ffi.NULL, ffi.NULL, ffi.NULL) == 0        # empty input: no-op
+    assert NA(m, 0, 0, ffi.NULL, 1, 0, out, ffi.NULL, ffi.NULL) == 2             # null rays
+    assert NA(m, 0, 0, ffi.cast("float *", 0x1004), 1, 0, out, ffi.NULL, ffi.NULL) == 1  # rays not 8-byte aligned
+    big = ffi.new("vrt_medium *")
+    big.sigma = _grid(ffi, [130, 130, 130, 1], [130 * 130, 130, 1, 1], 0x1000)[0]
+    assert NA(big, 0, 2, rays, 1, 0, out, ffi.NULL, ffi.NULL) == 3               # 65^3 bricks > 64^3
 
 
 def test_lowering_of_reference_style_scene():

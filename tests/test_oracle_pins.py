@@ -379,3 +379,21 @@ def test_adjoint_matches_finite_difference_of_expectation(bw):
     g, f = np.array(grads), np.array(fds)
     err = math.sqrt(g.var(ddof=1) / len(g) + f.var(ddof=1) / len(f))
     assert abs(g.mean() - f.mean()) < 4 * err + 0.05 * abs(f.mean()), (g, f)
+
+
+def test_sensor_batch_capture_runs_the_same_paths(oracle_lib):
+    """A sensors batch listing every pixel in raster order is the full capture
+    (sample s of sensor k is Philox path s * n + k); a shuffled batch gives the
+    shuffled pixels their own paths (ids follow the batch position)."""
+    from tests.helpers import oracle_desc
+    sig = synthetic.gaussian_blobs(17, 4, 8.0, seed=2)
+    sc = oracle_lib.OracleScene(oracle_desc(sig, albedo=0.8, env=1.0, g=0.3, max_bounces=8))
+    poses = synthetic.ring_poses(2)
+    H, W = 6, 5
+    full, _ = oracle_lib.capture_fw(sc, "nee", poses, W, H, math.pi / 4, True, 4, 99)
+    idx = np.stack(np.meshgrid(np.arange(2), np.arange(H), np.arange(W), indexing="ij"), -1).reshape(-1, 3)
+    part, cnt = oracle_lib.capture_fw(sc, "nee", poses, W, H, math.pi / 4, True, 4, 99, sensors=idx)
+    assert np.array_equal(part.reshape(full.shape), full)
+    assert cnt["paths"] == idx.shape[0] * 4
+    sub, _ = oracle_lib.capture_fw(sc, "nee", poses, W, H, math.pi / 4, True, 4, 99, sensors=idx[::7])
+    assert sub.shape == (idx[::7].shape[0], 3) and np.isfinite(sub).all()
