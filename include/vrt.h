@@ -43,7 +43,9 @@ enum {
     VRT_TR_RATIO_TRACKING = 0,  /* RatiotrackingTransmittance, include/vr_transmittance_RT.h */
     VRT_TR_DELTA_TRACKING = 1,  /* DeltatrackingTransmittance, include/vr_transmittance_DT.h */
     VRT_TR_DDA_MIDPOINT = 2,    /* GridDDATransmittance, include/vr_transmittance_DDA.h */
-    VRT_TR_DDA_EXACT = 3        /* DDA with the exact per-cell trilinear integral (no reference) */
+    VRT_TR_DDA_EXACT = 3,       /* DDA with the exact per-cell trilinear integral (no reference) */
+    VRT_TR_GRID_RATIO = 4,      /* GridRatiotrackingTransmittance, include/vr_transmittance_GRT.h (forward only) */
+    VRT_TR_GRID_DELTA = 5       /* GridDeltatrackingTransmittance, include/vr_transmittance_GDT.h (forward only) */
 };
 /* Path-integrator forward passes. */
 enum { VRT_PI_NEE = 0, VRT_PI_DT = 1 };

@@ -57,7 +57,7 @@ def ptr(ffi, arr: np.ndarray | None, ctype: str = "float *"):
     return ffi.cast(ctype, arr.ctypes.data)
 
 
-TRANSMITTANCE_MODES = {"rt": 0, "dt": 1, "dda": 2, "dda_midpoint": 2, "dda_exact": 3}
+TRANSMITTANCE_MODES = {"rt": 0, "dt": 1, "dda": 2, "dda_midpoint": 2, "dda_exact": 3, "grt": 4, "gdt": 5}
 BW_MODES = {"ds": 0, "dt": 1, "drt": 2, "drtq": 3, "drtds": 4, "sps": 5}
 INTEGRATORS = {"nee": 0, "dt": 1}
 
@@ -118,10 +118,10 @@ class OracleScene:
 class _CameraKeep:
     """The numpy buffers an orc_camera points into, and the capture's image shape."""
 
-    def __init__(self, poses, sensors, height, width):
+    def __init__(self, poses, sensors, height, width, batch_shape=None):
         self.poses = poses
         self.sensors = sensors
-        self.shape = ((poses.shape[0], height, width) if sensors is None else (sensors.shape[0],))
+        self.shape = (poses.shape[0], height, width) if sensors is None else tuple(batch_shape)
 
     @property
     def npix(self) -> int:
@@ -142,11 +142,13 @@ def make_camera(poses: np.ndarray, width: int, height: int, fov: float, jittered
     cam.fov = float(fov)
     cam.znear = float(znear)
     cam.jittered = 1 if jittered else 0
+    batch_shape = None
     if sensors is not None:
+        batch_shape = np.shape(sensors)[:-1]
         sensors = np.ascontiguousarray(sensors, dtype=np.int64).reshape(-1, 3)
         cam.sensors = ffi.cast("int64_t *", sensors.ctypes.data)
         cam.n_sensors = sensors.shape[0]
-    return cam, _CameraKeep(poses, sensors, height, width)
+    return cam, _CameraKeep(poses, sensors, height, width, batch_shape)
 
 
 # ---------------------------------------------------------------- wrappers --
@@ -301,7 +303,7 @@ def radiance_bw(scene: OracleScene, bw_mode: str, rays: np.ndarray, seed: int, d
 
 
 def capture_fw(scene: OracleScene, integrator: str, poses, width, height, fov, jittered, spp, seed, sensors=None):
-    """[views, H, W, 3], or [n, 3] for a sensors batch [n, 3] of (view, row, col)."""
+    """[views, H, W, 3], or sensors.shape[:-1] + [3] for a sensors batch of (view, row, col)."""
     ffi, L = lib()
     cam, keep = make_camera(poses, width, height, fov, jittered, sensors=sensors)
     out = np.empty(keep.shape + (3,), np.float32)

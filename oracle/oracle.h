@@ -58,7 +58,7 @@ typedef struct orc_scene {
     const float* maj_grid;        /* [Mz,My,Mx] */
     int32_t maj_dims[3];          /* Mx, My, Mz */
     float maj_scale[3];           /* inv_bsize * dim / brick */
-    int32_t transmittance_mode;   /* 0 RT, 1 DT, 2 DDA midpoint, 3 DDA exact */
+    int32_t transmittance_mode;   /* 0 RT, 1 DT, 2 DDA midpoint, 3 DDA exact, 4 GRT, 5 GDT */
     int32_t max_bounces;          /* 0 = uncapped (reference) */
     float ds_epsilon;
     int32_t ds_compat;            /* 1 = reference replay majorant quirk in NEE_DS bw */
@@ -90,7 +90,7 @@ void orc_grid3d_bw(const orc_grid* g, const float bmin[3], const float inv_bsize
 void orc_majorant_build(const orc_grid* sigma, int32_t brick, float* out, int32_t dims_out[3]);
 void orc_majorant_query(const orc_scene* s, const float* rays, int64_t n, float* out2);
 
-/* mode: 0 RT, 1 DT, 2 DDA midpoint, 3 DDA exact */
+/* mode: 0 RT, 1 DT, 2 DDA midpoint, 3 DDA exact, 4 GRT, 5 GDT (forward only) */
 void orc_transmittance_fw(const orc_scene* s, int32_t mode, const float* rays, int64_t n, uint64_t seed, int32_t fp64, float* T);
 void orc_transmittance_bw(const orc_scene* s, int32_t mode, const float* rays, int64_t n, uint64_t seed, const float* dL_dT);
 /* The DDA's optical depth (midpoint or exact rule) in FP64 */

@@ -511,6 +511,50 @@ template <typename T> struct DDA {
     }
 };
 
+// include/vr_transmittance_GRT.h:1-83 (delta == false) and
+// include/vr_transmittance_GDT.h:1-84 (delta == true): the DDA walk of the
+// grid's cells; per cell the eight corner values give a majorant and a
+// minorant, the minorant part is integrated in closed form and the residual
+// sigma - minorant is tracked against majorant - minorant.  Forward only (the
+// reference's maps have no backward).
+template <typename T>
+T transmittance_grid_tracking(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, bool delta, int64_t* steps) {
+    DDA<T> dda(S, x, w);
+    if (!dda.valid) return T(1);
+    T Tr = T(1), ct = T(0);
+    T s[2][2][2];
+    while (ct < dda.d - T(0.0001)) {
+        T nt = vmin(dda.d, vmin(dda.alpha.x, vmin(dda.alpha.y, dda.alpha.z)));
+        dda.load_cell(s);
+        T mx = s[0][0][0], mn = s[0][0][0];
+        for (int k = 1; k < 8; ++k) {
+            const T v = s[k >> 2][(k >> 1) & 1][k & 1];
+            mx = std::max(mx, v);
+            mn = std::min(mn, v);
+        }
+        if (steps) ++*steps;
+        Tr *= std::exp(-mn * (nt - ct));
+        const T rm = vmax(T(0.000001), mx - mn);
+        T cell_t = ct;
+        while (true) {
+            const T dt = -std::log(T(1) - (T)rng.uniform()) / rm;
+            if (cell_t + dt > nt) break;
+            cell_t += dt;
+            const T sv = interpolated_sigma(dda.ialpha(cell_t), s);
+            const T Pc = (sv - mn) / rm;
+            if (steps) ++*steps;
+            if (delta) {
+                if ((T)rng.uniform() < Pc) return T(0);
+            } else {
+                Tr *= (T(1) - Pc);
+            }
+        }
+        ct = nt;
+        dda.step();
+    }
+    return Tr;
+}
+
 template <typename T> T transmittance_DDA(const Scene<T>& S, V3<T> x, V3<T> w, bool exact, int64_t* steps) {
     DDA<T> dda(S, x, w);
     if (!dda.valid) return T(1);
@@ -693,7 +737,9 @@ template <typename T> T transmittance(const Scene<T>& S, Rng& rng, V3<T> x, V3<T
         case 0: return transmittance_RT(S, sr, x, w, steps);
         case 1: return transmittance_DT(S, sr, x, w, steps);
         case 2: return transmittance_DDA(S, x, w, false, steps);
-        default: return transmittance_DDA(S, x, w, true, steps);
+        case 3: return transmittance_DDA(S, x, w, true, steps);
+        case 4: return transmittance_grid_tracking(S, sr, x, w, false, steps);
+        default: return transmittance_grid_tracking(S, sr, x, w, true, steps);
     }
 }
 template <typename T> void transmittance_bw(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, T dL_dT) {
@@ -702,7 +748,8 @@ template <typename T> void transmittance_bw(const Scene<T>& S, Rng& rng, V3<T> x
         case 0: transmittance_RT_bw(S, sr, x, w, dL_dT); break;
         case 1: transmittance_DT_bw(S, sr, x, w, dL_dT); break;
         case 2: transmittance_DDA_bw(S, x, w, false, dL_dT); break;
-        default: transmittance_DDA_bw(S, x, w, true, dL_dT); break;
+        case 3: transmittance_DDA_bw(S, x, w, true, dL_dT); break;
+        default: break;  // GRT / GDT: no backward (the reference's maps define none)
     }
 }
 

@@ -91,14 +91,20 @@ __device__ __forceinline__ void unpark(Lane& L) {
 __device__ __forceinline__ int begin_segment(const DMedium& M, Lane& L, int st, Tally& tl, uint32_t* status) {
     const float3 dir = shadow_dir(M, L);
     const uint32_t j = L.jfork + (uint32_t)L.light;
-    if (M.tr_mode >= 2) {  // DDA: deterministic, evaluated inline
+    if (M.tr_mode >= 2) {  // DDA, GRT, GDT: evaluated inline
         if (st == S_TRFW) {
-            L.T = M.tr_mode == 2 ? transmittance_dda<false>(M, L.x, dir, tl) : transmittance_dda<true>(M, L.x, dir, tl);
+            if (M.tr_mode == 2) L.T = transmittance_dda<false>(M, L.x, dir, tl);
+            else if (M.tr_mode == 3) L.T = transmittance_dda<true>(M, L.x, dir, tl);
+            else {
+                Rng r = fork_at(L, j);
+                L.T = M.tr_mode == 4 ? transmittance_grid_tracking<false>(M, r, L.x, dir, tl, status)
+                                     : transmittance_grid_tracking<true>(M, r, L.x, dir, tl, status);
+            }
             return E_SEG_DONE;
         }
         if (M.tr_mode == 2) transmittance_dda_bw<false>(M, L.x, dir, L.dLdT, tl);
-        else transmittance_dda_bw<true>(M, L.x, dir, L.dLdT, tl);
-        return E_SEG_ABORT;  // nothing more to run for this light
+        else if (M.tr_mode == 3) transmittance_dda_bw<true>(M, L.x, dir, L.dLdT, tl);
+        return E_SEG_ABORT;  // nothing more to run for this light (GRT / GDT have no backward)
     }
     if (st != S_TRFW && L.dLdT == 0.0f) return E_SEG_ABORT;  // _RT.h:53 / _DT.h:32
     // the vertex's box interval for this light, computed once per vertex

@@ -254,7 +254,7 @@ static int to_dmedium(const vrt_medium* m, DMedium& M) {
     if (!std::isfinite(m->phase_g) || !std::isfinite(m->ds_epsilon) || !std::isfinite(m->global_majorant))
         return VRT_E_NONFINITE;
     if (m->phase_mode < 0 || m->phase_mode > 1) return VRT_E_INVALID_ARGUMENT;
-    if (m->transmittance_mode < 0 || m->transmittance_mode > 3) return VRT_E_INVALID_ARGUMENT;
+    if (m->transmittance_mode < 0 || m->transmittance_mode > 5) return VRT_E_INVALID_ARGUMENT;
     if (m->max_bounces < 0) return VRT_E_INVALID_ARGUMENT;
     if (m->majorant_mode == 1) {
         if (!m->maj_grid) return VRT_E_NULL_POINTER;
@@ -506,7 +506,7 @@ int vrt_transmittance_fw(vrt_context* ctx, const vrt_medium* m, int32_t mode, co
                          uint64_t seed, float* T, void* stream) {
     int st = check_ctx(ctx);
     if (st) return st;
-    if (mode < 0 || mode > 3) return VRT_E_INVALID_ARGUMENT;
+    if (mode < 0 || mode > 5) return VRT_E_INVALID_ARGUMENT;
     if (n < 0) return VRT_E_BAD_SHAPE;
     DMedium M;
     if ((st = to_dmedium(m, M))) return st;
@@ -520,11 +520,12 @@ int vrt_transmittance_bw(vrt_context* ctx, const vrt_medium* m, int32_t mode, co
                          uint64_t seed, const float* dL_dT, void* stream) {
     int st = check_ctx(ctx);
     if (st) return st;
-    if (mode < 0 || mode > 3) return VRT_E_INVALID_ARGUMENT;
+    if (mode < 0 || mode > 5) return VRT_E_INVALID_ARGUMENT;
     if (n < 0) return VRT_E_BAD_SHAPE;
     DMedium M;
     if ((st = to_dmedium(m, M))) return st;
-    if (n == 0 || !M.sigma.grad) return VRT_OK;
+    // GRT / GDT have no backward (the reference's maps define none): no gradient
+    if (n == 0 || !M.sigma.grad || mode >= 4) return VRT_OK;
     if (!rays || !dL_dT) return VRT_E_NULL_POINTER;
     if (!aligned8(rays)) return VRT_E_INVALID_ARGUMENT;
     return launch_transmittance_bw(M, mode, rays, n, seed, dL_dT, ctx->scratch, (cudaStream_t)stream);

@@ -130,8 +130,11 @@ __device__ __forceinline__ int start_shadow(const DMedium& M, NeeLane& L, float3
     L.T = 1.0f;
     L.ff = Flight();
     Rng child = L.rng.fork();
-    if (M.tr_mode >= 2) {
-        L.T = M.tr_mode == 2 ? transmittance_dda<false>(M, x0, dir, tl) : transmittance_dda<true>(M, x0, dir, tl);
+    if (M.tr_mode >= 2) {  // DDA, GRT, GDT: one call
+        if (M.tr_mode == 2) L.T = transmittance_dda<false>(M, x0, dir, tl);
+        else if (M.tr_mode == 3) L.T = transmittance_dda<true>(M, x0, dir, tl);
+        else if (M.tr_mode == 4) L.T = transmittance_grid_tracking<false>(M, child, x0, dir, tl, nullptr);
+        else L.T = transmittance_grid_tracking<true>(M, child, x0, dir, tl, nullptr);
         return EV_SHADOW_DONE;
     }
     float tMin, tMax;

@@ -5,6 +5,8 @@
 //         the cubic a trilinear field becomes on a segment)
 //   RT    include/vr_transmittance_RT.h:1-141 (ratio tracking, RR at 0.01 / 0.1)
 //   DT    include/vr_transmittance_DT.h:1-90  (delta tracking)
+//   GRT / GDT  include/vr_transmittance_GRT.h:1-83, _GDT.h:1-84 (ratio / delta
+//         tracking of the residual over per-cell minorants, on the DDA walk)
 //
 // The DDA keeps the 8 corner values of the current cell in registers: a step
 // along axis a keeps the face the ray crosses into and loads only the 4 new
@@ -339,6 +341,63 @@ __device__ __forceinline__ void transmittance_dda_bw(const DMedium& M, float3 x,
     q.scatter<EXACT>(M.sigma, -dL_dT * T, tl);
 }
 
+// GridRatiotrackingTransmittance / GridDeltatrackingTransmittance
+// (include/vr_transmittance_GRT.h:1-83, _GDT.h:1-84): the DDA walk of the
+// grid's cells (the corner values stay in registers, 4 new loads per cell);
+// per cell the eight corners bound the trilinear field, the minorant part is
+// integrated in closed form (exp(-min * dt)) and the residual sigma - min is
+// tracked against max - min: ratio tracking multiplies T by 1 - Pc, delta
+// tracking ends the ray (T = 0) at a collision.  Forward only: the
+// reference's maps define no backward.
+template <bool DELTA>
+__device__ __forceinline__ float transmittance_grid_tracking(const DMedium& M, Rng& rng, float3 x, float3 w,
+                                                             Tally& tl, uint32_t* status) {
+    DDA q;
+    if (!q.init(M, x, w)) return 1.0f;
+    q.load_all(M.sigma);
+    float T = 1.0f, ct = 0.0f;
+    const float stop = q.d - 0.0001f;
+    int it = 0;
+    while (ct < stop) {
+        if (++it > kStepCap) {
+            raise_status(status, 4);
+            return T;
+        }
+        const float nt = gmin(q.d, gmin(q.alpha.x, gmin(q.alpha.y, q.alpha.z)));
+        float mx = q.s[0], mn = q.s[0];
+#pragma unroll
+        for (int k = 1; k < 8; ++k) {
+            mx = fmaxf(mx, q.s[k]);
+            mn = fminf(mn, q.s[k]);
+        }
+        ++tl.steps;
+        ++tl.lookups;
+        T *= expf(-mn * (nt - ct));
+        const float rm = gmax(0.000001f, mx - mn);
+        float cell_t = ct;
+        while (true) {
+            if (++it > kStepCap) {
+                raise_status(status, 4);
+                return T;
+            }
+            const float dt = -logf(1.0f - rng.uniform()) / rm;
+            if (cell_t + dt > nt) break;
+            cell_t += dt;
+            const float Pc = (q.interp(q.ialpha(cell_t)) - mn) / rm;
+            ++tl.steps;
+            if (DELTA) {
+                if (rng.uniform() < Pc) return 0.0f;
+            } else {
+                T *= (1.0f - Pc);
+            }
+        }
+        ct = nt;
+        const int axis = q.advance_cell();
+        q.shift_load(M.sigma, axis);
+    }
+    return T;
+}
+
 // vr_transmittance_RT.h:1-49.  The "grid crossing" branch restarts at a
 // majorant-brick face without a collision; it cannot trigger with the
 // constant majorant (distance 1e6).
@@ -517,7 +576,9 @@ __device__ __forceinline__ float transmittance(const DMedium& M, Rng& rng, float
         case 0: return transmittance_rt(M, sr, x, w, tl, status);
         case 1: return transmittance_dt(M, sr, x, w, tl, status);
         case 2: return transmittance_dda<false>(M, x, w, tl);
-        default: return transmittance_dda<true>(M, x, w, tl);
+        case 3: return transmittance_dda<true>(M, x, w, tl);
+        case 4: return transmittance_grid_tracking<false>(M, sr, x, w, tl, status);
+        default: return transmittance_grid_tracking<true>(M, sr, x, w, tl, status);
     }
 }
 __device__ __forceinline__ void transmittance_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float dL_dT,
@@ -527,7 +588,8 @@ __device__ __forceinline__ void transmittance_bw(const DMedium& M, Rng& rng, flo
         case 0: transmittance_rt_bw(M, sr, x, w, dL_dT, tl, status); break;
         case 1: transmittance_dt_bw(M, sr, x, w, dL_dT, tl, status); break;
         case 2: transmittance_dda_bw<false>(M, x, w, dL_dT, tl); break;
-        default: transmittance_dda_bw<true>(M, x, w, dL_dT, tl); break;
+        case 3: transmittance_dda_bw<true>(M, x, w, dL_dT, tl); break;
+        default: break;  // GRT / GDT: no backward (the reference's maps define none)
     }
 }
 

@@ -2,7 +2,8 @@
 //
 // One thread per ray; ray i draws from Philox path id i.  These are the
 // operator forms of GridDDATransmittance / RatiotrackingTransmittance /
-// DeltatrackingTransmittance (include/maps/transmittance_{dda,rt,dt}.h).
+// DeltatrackingTransmittance, GridRatiotrackingTransmittance and
+// GridDeltatrackingTransmittance (include/maps/transmittance_{dda,rt,dt,grt,gdt}.h).
 #include <cuda_runtime.h>
 
 #include "vrt_internal.h"
@@ -43,8 +44,9 @@ __global__ void __launch_bounds__(256) k_transmittance_fw(DMedium M, const float
             Rng path;
             path.init(seed, (uint64_t)i, 0);
             Rng rng = path.fork();  // as the dispatch of a path integrator would
-            v = MODE == 0 ? transmittance_rt(M, rng, x, w, tl, &sc->status)
-                          : transmittance_dt(M, rng, x, w, tl, &sc->status);
+            if (MODE == 0) v = transmittance_rt(M, rng, x, w, tl, &sc->status);
+            else if (MODE == 1) v = transmittance_dt(M, rng, x, w, tl, &sc->status);
+            else v = transmittance_grid_tracking<MODE == 5>(M, rng, x, w, tl, &sc->status);
         }
         T[i] = v;
         ++count;
@@ -90,7 +92,9 @@ int launch_transmittance_fw(const DMedium& M, int mode, const float* rays, int64
         case 0: k_transmittance_fw<0><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
         case 1: k_transmittance_fw<1><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
         case 2: k_transmittance_fw<2><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
-        default: k_transmittance_fw<3><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
+        case 3: k_transmittance_fw<3><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
+        case 4: k_transmittance_fw<4><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
+        default: k_transmittance_fw<5><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
     }
     count_launches(1);
     return launch_status(cudaGetLastError());

@@ -476,7 +476,9 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
                 case 0: k_shadow_run<0, OUT_IMAGE><<<rblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, wv.cap, wv.count + 1, seed, so, ctx->scratch); break;
                 case 1: k_shadow_run<1, OUT_IMAGE><<<rblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, wv.cap, wv.count + 1, seed, so, ctx->scratch); break;
                 case 2: k_shadow_fw<2><<<sblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, seed, out, scale, ctx->scratch); break;
-                default: k_shadow_fw<3><<<sblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, seed, out, scale, ctx->scratch); break;
+                case 3: k_shadow_fw<3><<<sblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, seed, out, scale, ctx->scratch); break;
+                case 4: k_shadow_fw<4><<<sblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, seed, out, scale, ctx->scratch); break;
+                default: k_shadow_fw<5><<<sblocks, 256, 0, stream>>>(M, src, wv.jobs, wv.count, seed, out, scale, ctx->scratch); break;
             }
         }
         count_launches(2);
@@ -550,7 +552,9 @@ int launch_shadow_record(const DMedium& M, const PathSrc& src, const WaveBw& wv,
                                           0, stream>>>(M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[3], seed, so, sc);
             break;
         case 2: k_shadow_T<2><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
-        default: k_shadow_T<3><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
+        case 3: k_shadow_T<3><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
+        case 4: k_shadow_T<4><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
+        default: k_shadow_T<5><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
     }
     count_launches(1);
     return launch_status(cudaGetLastError());
@@ -569,7 +573,8 @@ int launch_shadow_adjoint(const DMedium& M, const WaveBw& wv, uint64_t seed, DSc
                 M, wv.jobs, wv.dldt, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, sc);
             break;
         case 2: k_shadow_bw<2><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
-        default: k_shadow_bw<3><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
+        case 3: k_shadow_bw<3><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
+        default: return VRT_OK;  // GRT / GDT shadow rays carry no gradient (no backward in the reference)
     }
     count_launches(1);
     return launch_status(cudaGetLastError());

@@ -186,7 +186,9 @@ __device__ __forceinline__ float shadow_T(const DMedium& M, Rng& r, float3 x, fl
     if (TR == 0) return transmittance_rt(M, r, x, dir, tl, status);
     if (TR == 1) return transmittance_dt(M, r, x, dir, tl, status);
     if (TR == 2) return transmittance_dda<false>(M, x, dir, tl);
-    return transmittance_dda<true>(M, x, dir, tl);
+    if (TR == 3) return transmittance_dda<true>(M, x, dir, tl);
+    if (TR == 4) return transmittance_grid_tracking<false>(M, r, x, dir, tl, status);
+    return transmittance_grid_tracking<true>(M, r, x, dir, tl, status);
 }
 
 // The primary ray of path pid (camera or ray input), with the camera's draws.

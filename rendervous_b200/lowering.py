@@ -29,7 +29,7 @@ import torch
 
 from . import _lib
 
-TR_MODES = {"rt": 0, "dt": 1, "dda": 2, "dda_exact": 3}
+TR_MODES = {"rt": 0, "dt": 1, "dda": 2, "dda_exact": 3, "grt": 4, "gdt": 5}
 
 
 @dataclasses.dataclass
@@ -205,6 +205,9 @@ def lower_transmittance(tr, sigma, desc_kwargs: dict):
     elif isinstance(tr, maps.DeltatrackingTransmittance):
         _check_same_grid(tr.sigma, sigma, "DeltatrackingTransmittance")
         desc_kwargs["transmittance_mode"] = 1
+    elif isinstance(tr, (maps.GridRatiotrackingTransmittance, maps.GridDeltatrackingTransmittance)):
+        _check_same_grid(tr.grid_model, sigma, type(tr).__name__)
+        desc_kwargs["transmittance_mode"] = tr._mode()
     else:
         raise NotImplementedError(f"transmittance map {type(tr).__name__} is not supported")
 
@@ -286,6 +289,9 @@ def lower_transmittance_map(tr) -> MediumDesc:
     if isinstance(tr, maps.GridDDATransmittance):
         lower_sigma(tr.grid_model, kw)
         kw["transmittance_mode"] = 3 if tr.exact else 2
+    elif isinstance(tr, (maps.GridRatiotrackingTransmittance, maps.GridDeltatrackingTransmittance)):
+        lower_sigma(tr.grid_model, kw)
+        kw["transmittance_mode"] = tr._mode()
     else:
         lower_sigma(tr.sigma, kw)
         lower_majorant(tr.majorant, tr.sigma, kw)

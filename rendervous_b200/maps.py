@@ -448,6 +448,46 @@ class GridDDATransmittance(_TransmittanceMap):
         return TR_MODES["dda_exact" if self.exact else "dda"]
 
 
+class _GridTrackingTransmittance(_TransmittanceMap):
+    """Shared constructor of GridRatiotrackingTransmittance and
+    GridDeltatrackingTransmittance (_maps.py:2588-2637): tracking over the
+    grid's own cells with per-cell majorant and minorant, no majorant map.
+    Forward only, as in the reference (its maps define no backward): the
+    gradient through them is zero."""
+
+    def __init__(self, grid: Grid3D, boundary: MapBase):
+        super().__init__()
+        self.grid_model = grid
+        self.grid = grid.grid
+        self.box_min = grid.bmin.clone()
+        self.box_max = grid.bmax.clone()
+        self.boundary = boundary.cast(6, 2)
+
+    def update_grid(self, grid: typing.Optional[Grid3D] = None):
+        if grid is None:
+            assert self.grid_model is not None
+            grid = self.grid_model
+        else:
+            self.grid_model = grid
+        self.grid = grid.grid
+        self.box_min = grid.bmin.clone()
+        self.box_max = grid.bmax.clone()
+
+
+class GridRatiotrackingTransmittance(_GridTrackingTransmittance):
+    """GridRatiotrackingTransmittance (_maps.py:2588-2614, include/vr_transmittance_GRT.h)."""
+
+    def _mode(self) -> int:
+        return TR_MODES["grt"]
+
+
+class GridDeltatrackingTransmittance(_GridTrackingTransmittance):
+    """GridDeltatrackingTransmittance (_maps.py:2617-2637, include/vr_transmittance_GDT.h)."""
+
+    def _mode(self) -> int:
+        return TR_MODES["gdt"]
+
+
 class RatiotrackingTransmittance(_TransmittanceMap):
     """RatiotrackingTransmittance (_maps.py:2670-2682, include/vr_transmittance_RT.h)."""
 

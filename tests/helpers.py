@@ -40,7 +40,7 @@ def oracle_desc(sigma: np.ndarray, *, albedo=0.9, albedo_grid: np.ndarray | None
         desc.majorant_mode = 1
         desc.maj_brick = brick
         desc.maj_grid = torch.from_numpy(oracle.majorant_build(sigma, brick))
-    desc.transmittance_mode = {"rt": 0, "dt": 1, "dda": 2, "dda_exact": 3}[tr]
+    desc.transmittance_mode = {"rt": 0, "dt": 1, "dda": 2, "dda_exact": 3, "grt": 4, "gdt": 5}[tr]
     desc.max_bounces = max_bounces
     desc.ds_epsilon = ds_epsilon
     desc.ds_compat = ds_compat
@@ -80,6 +80,10 @@ def build_field(sigma: torch.Tensor, *, albedo=0.9, albedo_grid: torch.Tensor | 
         trm = maps.RatiotrackingTransmittance(sg, boundary, maj)
     elif tr == "dt":
         trm = maps.DeltatrackingTransmittance(sg, boundary, maj)
+    elif tr == "grt":
+        trm = maps.GridRatiotrackingTransmittance(sg, boundary)
+    elif tr == "gdt":
+        trm = maps.GridDeltatrackingTransmittance(sg, boundary)
     else:
         trm = maps.GridDDATransmittance(sg, boundary, exact=(tr == "dda_exact"))
     light = None if sun_dir is None else maps.DirectionalLight(torch.tensor(sun_dir, dtype=torch.float32), sun_radiance)
