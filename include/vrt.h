@@ -47,8 +47,11 @@ enum {
     VRT_TR_GRID_RATIO = 4,      /* GridRatiotrackingTransmittance, include/vr_transmittance_GRT.h (forward only) */
     VRT_TR_GRID_DELTA = 5       /* GridDeltatrackingTransmittance, include/vr_transmittance_GDT.h (forward only) */
 };
-/* Path-integrator forward passes. */
-enum { VRT_PI_NEE = 0, VRT_PI_DT = 1 };
+/* Integrator forward passes: the path integrators, and the collision
+   integrators MCCollisionIntegrator (include/maps/collision_integrator_mc.h)
+   and GridDDACollisionIntegrator (include/vr_collision_integrator_DDA.h),
+   whose exitance radiance is vrt_medium.exitance_mode. */
+enum { VRT_PI_NEE = 0, VRT_PI_DT = 1, VRT_PI_MC_COLLISION = 2, VRT_PI_DDA_COLLISION = 3 };
 /* Path-replay adjoints (DeltatrackingNEEPathIntegrator, DeltatrackingPathIntegrator,
    DRTPathIntegrator, DRTQPathIntegrator, DRTDSPathIntegrator, SPSPathIntegrator;
    include/vr_path_integrator_NEE_DS.h, _DT.h, _NEE_DRT.h, _NEE_DRTQ.h, _NEE_DRTDS.h, _NEE_SPS.h). */
@@ -58,7 +61,9 @@ enum {
     VRT_BW_NEE_DRT = 2,
     VRT_BW_NEE_DRTQ = 3,
     VRT_BW_NEE_DRTDS = 4,
-    VRT_BW_NEE_SPS = 5
+    VRT_BW_NEE_SPS = 5,
+    VRT_BW_MC_COLLISION = 6,    /* MCCollisionIntegrator BACKWARD (collision_integrator_mc.h:20-41) */
+    VRT_BW_DDA_COLLISION = 7    /* GridDDACollisionIntegrator BACKWARD (vr_collision_integrator_DDA.h:85-207) */
 };
 
 /* A node-centred FP32 grid, the Grid3D parameter (rendervous _maps.py:2319-2365).
@@ -95,8 +100,14 @@ typedef struct vrt_medium {
     float maj_scale[3];              /* inv_bsize * (shape-1) / brick */
     int32_t transmittance_mode;      /* VRT_TR_* used for NEE shadow rays */
     int32_t max_bounces;             /* 0 = uncapped, as the reference */
-    float ds_epsilon;                /* defensive-sampling epsilon of the DS / DT adjoints */
+    float ds_epsilon;                /* defensive-sampling epsilon of the DS / DT adjoints and the collision sampler */
     int32_t ds_compat;               /* 1: reference replay majorant of NEE_DS bw */
+    /* exitance radiance of the collision integrators (VRT_PI_MC_COLLISION, VRT_PI_DDA_COLLISION):
+       0 the emission (ds.exitance_radiance = ds.emission), 1 MCScatteredRadiance,
+       2 MCScatteredEmittedRadiance (_maps.py:2730-2760; radiance = transmittance x environment) */
+    int32_t exitance_mode;
+    int32_t emission_is_grid;        /* 0: emission[3] constant; 1: emission_grid (Grid3D, C 1 or 3, sigma's box) */
+    vrt_grid emission_grid;
 } vrt_medium;
 
 /* PerspectiveCameraSensor (rendervous _maps.py:1765-1802).  sensors == NULL:
@@ -218,6 +229,16 @@ int vrt_transmittance_bw(vrt_context* ctx, const vrt_medium* m, int32_t mode, co
    device error bits (1 << VRT_E_*) there and returns the first of them. */
 int vrt_transmittance_fw_noalloc(const vrt_medium* m, int32_t mode, int32_t brick, const float* rays, int64_t n,
                                  uint64_t seed, float* T, int64_t* status_out, void* stream);
+
+/* DeltatrackingCollisionSampler as a map on rays [n,6] -> out [n,3] = (C, t, T)
+   (include/maps/collision_sampler_dt.h, _maps.py:2714-2727; ray i draws from
+   stream 2 of Philox path i).  Backward takes dL/d(C, t, T) [n,3] (dL/dt is not
+   propagated, as in the reference) and accumulates dL/dsigma into
+   medium->sigma.grad from the defensively sampled walk (ds_epsilon). */
+int vrt_collision_sample_fw(vrt_context* ctx, const vrt_medium* m, const float* rays, int64_t n, uint64_t seed,
+                            float* out, void* stream);
+int vrt_collision_sample_bw(vrt_context* ctx, const vrt_medium* m, const float* rays, int64_t n, uint64_t seed,
+                            const float* dL_dout, void* stream);
 
 /* Path integrator as a map on rays [n,6] -> R [n,3] (DeltatrackingPathIntegrator,
    DeltatrackingNEEPathIntegrator, DRTPathIntegrator, _maps.py:2886-3022; path i

@@ -58,8 +58,8 @@ def ptr(ffi, arr: np.ndarray | None, ctype: str = "float *"):
 
 
 TRANSMITTANCE_MODES = {"rt": 0, "dt": 1, "dda": 2, "dda_midpoint": 2, "dda_exact": 3, "grt": 4, "gdt": 5}
-BW_MODES = {"ds": 0, "dt": 1, "drt": 2, "drtq": 3, "drtds": 4, "sps": 5}
-INTEGRATORS = {"nee": 0, "dt": 1}
+BW_MODES = {"ds": 0, "dt": 1, "drt": 2, "drtq": 3, "drtds": 4, "sps": 5, "mc_collision": 6, "dda_collision": 7}
+INTEGRATORS = {"nee": 0, "dt": 1, "mc_collision": 2, "dda_collision": 3}
 
 
 class OracleScene:
@@ -107,6 +107,14 @@ class OracleScene:
         s.max_bounces = int(desc["max_bounces"])
         s.ds_epsilon = float(desc["ds_epsilon"])
         s.ds_compat = int(desc["ds_compat"])
+        s.exitance_mode = int(desc.get("exitance_mode", 0))
+        em = desc.get("emission_grid")
+        self.emission_grad = None
+        if em is not None:
+            self.emission_grid = np.ascontiguousarray(em, dtype=np.float32)
+            self.emission_grad = np.zeros_like(self.emission_grid) if with_grads else None
+            self._grid(s.emission_grid, self.emission_grid, self.emission_grad)
+            s.emission_is_grid = 1
         self.s = s
 
     def _grid(self, g, arr, grad):
@@ -253,6 +261,23 @@ def dda_tau_fp64(scene: OracleScene, rays: np.ndarray, exact: bool = False) -> n
     out = np.empty(rays.shape[0], np.float64)
     L.orc_dda_tau_fp64(scene.s, int(exact), ptr(ffi, rays), rays.shape[0], ptr(ffi, out, "double *"))
     return out
+
+
+def collision_sample_fw(scene: OracleScene, rays: np.ndarray, seed: int) -> np.ndarray:
+    """DeltatrackingCollisionSampler on rays: [n, 3] = (C, t, T)."""
+    ffi, L = lib()
+    rays = np.ascontiguousarray(rays, np.float32)
+    out = np.empty((rays.shape[0], 3), np.float32)
+    L.orc_collision_sample_fw(scene.s, ptr(ffi, rays), rays.shape[0], seed, ptr(ffi, out))
+    return out
+
+
+def collision_sample_bw(scene: OracleScene, rays: np.ndarray, seed: int, dL_dout: np.ndarray) -> None:
+    """Accumulates into scene.sigma_grad."""
+    ffi, L = lib()
+    rays = np.ascontiguousarray(rays, np.float32)
+    g = np.ascontiguousarray(dL_dout, np.float32).reshape(-1, 3)
+    L.orc_collision_sample_bw(scene.s, ptr(ffi, rays), rays.shape[0], seed, ptr(ffi, g))
 
 
 def tau_raymarch_fp64(scene: OracleScene, rays: np.ndarray, substeps: int = 32) -> np.ndarray:

@@ -62,6 +62,9 @@ typedef struct orc_scene {
     int32_t max_bounces;          /* 0 = uncapped (reference) */
     float ds_epsilon;
     int32_t ds_compat;            /* 1 = reference replay majorant quirk in NEE_DS bw */
+    int32_t exitance_mode;        /* collision integrators: 0 emission, 1 scattered, 2 scattered + emitted */
+    int32_t emission_is_grid;     /* emission: 0 const emission[3], 1 emission_grid (C 1 or 3, sigma's box) */
+    orc_grid emission_grid;
 } orc_scene;
 
 typedef struct orc_camera {
@@ -103,9 +106,12 @@ void orc_env_sample(const orc_scene* s, int64_t n, uint64_t seed, float* out6);
 
 void orc_camera_rays(const orc_camera* cam, int32_t spp, uint64_t seed, float* out6);
 
-/* integrator: 0 NEE (DS/DRT/... forward), 1 DT (no NEE) */
+/* integrator: 0 NEE (DS/DRT/... forward), 1 DT (no NEE), 2 MC collision integrator, 3 DDA collision integrator */
 void orc_radiance_fw(const orc_scene* s, int32_t integrator, const float* rays, int64_t n, uint64_t seed, float* R, orc_counters* c);
-/* bw_mode: 0 NEE_DS, 1 DT, 2 NEE_DRT */
+/* bw_mode: 0 NEE_DS, 1 DT, 2 NEE_DRT, 3 DRTQ, 4 DRTDS, 5 SPS, 6 MC collision integrator, 7 DDA collision integrator */
+/* DeltatrackingCollisionSampler on rays: out3 [n,3] = (C, t, T); bw scatters dL/d(C, T) */
+void orc_collision_sample_fw(const orc_scene* s, const float* rays, int64_t n, uint64_t seed, float* out3);
+void orc_collision_sample_bw(const orc_scene* s, const float* rays, int64_t n, uint64_t seed, const float* dL_dout3);
 void orc_radiance_bw(const orc_scene* s, int32_t bw_mode, const float* rays, int64_t n, uint64_t seed, const float* dL_dR);
 
 void orc_capture_fw(const orc_scene* s, int32_t integrator, const orc_camera* cam, int32_t spp, uint64_t seed, float* rgb, orc_counters* c);

@@ -70,6 +70,15 @@ struct Rng {
         return f - 1.0f;
     }
     void advance() { ++n; }  // randoms.h:35-41 advance_random
+    // stream s of the same path and key (the collision integrators give the
+    // collision sampler, its adjoint and every exitance evaluation a stream)
+    Rng with_stream(uint32_t s) const {
+        Rng r = *this;
+        r.stream = s;
+        r.n = 0;
+        r.ntr = 0;
+        return r;
+    }
 };
 
 template <typename T> struct V3 {
@@ -304,6 +313,19 @@ template <typename T> struct Scene {
         else { T g[3] = {dL.x, dL.y, dL.z}; grid_bw(s.albedo, x, g); }
     }
     V3<T> emission() const { return V3<T>::load(s.emission); }
+    // include/vr_emission.h over const or a Grid3D of emission (C 1 or 3,
+    // sigma's box; the collision integrators' exitance radiance)
+    V3<T> emission_at(V3<T> x) const {
+        if (!s.emission_is_grid) return emission();
+        T v[3];
+        grid_fw(s.emission_grid, x, v);
+        return s.emission_grid.C == 1 ? V3<T>(v[0]) : V3<T>(v[0], v[1], v[2]);
+    }
+    void emission_bw(V3<T> x, V3<T> dL) const {
+        if (!s.emission_is_grid || !s.emission_grid.grad) return;
+        if (s.emission_grid.C == 1) { T g = dL.x + dL.y + dL.z; grid_bw(s.emission_grid, x, &g); }
+        else { T g[3] = {dL.x, dL.y, dL.z}; grid_bw(s.emission_grid, x, g); }
+    }
     V3<T> environment() const { return V3<T>::load(s.env); }
 
     // include/vr_majorant.h:1-7.  Mode 0: const[[max sigma, 1e6]] (_objects.py:96-101).
@@ -1805,7 +1827,273 @@ inline void camera_pixel(const orc_camera& cam, int64_t p, int& view, int& row, 
 // pixel of a radiance-cache training path: the path's first draw, scaled to npix
 inline int64_t random_pixel(Rng& rng, int64_t npix) { return (int64_t)(((uint64_t)rng.u32() * (uint64_t)npix) >> 32); }
 
+// ---------------------------------------------------------------------------
+// Collision sampling and collision integrators (_maps.py:2714-2852).
+// ---------------------------------------------------------------------------
+// include/vr_collision_sampler_DT.h:6-43: a delta-tracking collision along the
+// ray; returns C (1 at a collision, else 0), the collision distance out_t from
+// x and out_T (0 at a collision, else 1).  The free flight carries its residual
+// optical depth across majorant-brick faces, as every tracker here does.
+template <typename T>
+T collision_sampler_DT(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, T& out_t, T& out_T, int64_t* steps) {
+    out_T = T(1);
+    out_t = T(0);
+    T C = T(0);
+    T tMin, tMax;
+    if (!S.boundary(x, w, tMin, tMax)) return C;
+    const T d = tMax - tMin;
+    x += w * tMin;
+    T t = T(0);
+    Flight<T> ff;
+    for (; ff.it < (1 << 24); ++ff.it) {
+        T md;
+        const T maj = ff.bk.query(S.s, x, w, md);
+        const T tau = ff.sample(rng);
+        if (steps) ++*steps;
+        const bool crosses = tau > md * maj;
+        T dt = crosses ? md : tau / maj;
+        dt = vmin(dt, d);
+        x += w * dt;
+        t += dt;
+        if (t >= d - T(0.0000001)) break;
+        if (crosses) { ff.cross(maj, md); ff.bk.advance(S.s); continue; }
+        ff.used();
+        ff.bk.move(dt);
+        if ((T)rng.uniform() < S.sigma(x) / maj) {
+            out_T = T(0);
+            C = T(1);
+            break;
+        }
+    }
+    out_t = tMin + t;
+    return C;
+}
+
+// include/vr_collision_sampler_DT.h:45-134: the defensively sampled walk
+// (majorant + 2 eps, Pc = (sigma + eps) / majorant) for the estimate, then the
+// same draws again scattering dL/dsigma at its collisions.
+template <typename T>
+void collision_sampler_DT_bw(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, T eps, T dL_dC, T dL_dT) {
+    T tMin, tMax;
+    if (!S.boundary(x, w, tMin, tMax)) return;
+    const Rng before = rng;
+    T out_T = T(1), C = T(0), s_t = T(0);
+    const T d = tMax - tMin;
+    x += w * tMin;
+    const V3<T> ini_x = x;
+    for (int pass = 0; pass < 2; ++pass) {
+        T t = T(0);
+        Flight<T> ff;
+        for (; ff.it < (1 << 24); ++ff.it) {
+            T md;
+            const T maj = vmax(T(0.0000000001), ff.bk.query(S.s, x, w, md) + T(2) * eps);
+            const T tau = ff.sample(rng);
+            const bool crosses = tau > md * maj;
+            T dt = crosses ? md : tau / maj;
+            dt = vmin(dt, d);
+            x += w * dt;
+            t += dt;
+            if (t >= d - T(0.0000001)) break;
+            if (crosses) { ff.cross(maj, md); ff.bk.advance(S.s); continue; }
+            ff.used();
+            ff.bk.move(dt);
+            const T s = S.sigma(x);
+            const T Pc = (s + eps) / maj;
+            const bool hit = (T)rng.uniform() < Pc;
+            if (pass == 0) {
+                if (hit) {
+                    out_T = T(0);
+                    C = T(1);
+                    s_t = s / maj / Pc;
+                    break;
+                }
+                out_T *= (T(1) - s / maj) / (T(1) - Pc);
+            } else if (hit) {
+                S.sigma_bw(x, dL_dC * (C / Pc) * (T(1) / maj));
+                break;
+            } else {
+                const T g = (dL_dT * out_T + dL_dC * C * s_t) / ((T(1) - s / maj) / (T(1) - Pc)) / (T(1) - Pc);
+                S.sigma_bw(x, g * (T(-1) / maj));
+            }
+        }
+        rng = before;
+        x = ini_x;
+    }
+}
+
+// Exitance radiance R(x, w_out) of a collision integrator (w_out = -ray
+// direction), by the medium's exitance_mode:
+//   0  the emission map (const or Grid3D): ds.exitance_radiance = ds.emission
+//   1  MCScatteredRadiance (include/maps/scattered_radiance_mc.h):
+//      sa(x) * rho * radiance(x, wo), (rho, wo) = phase_sampler(x, -w_out)
+//   2  MCScatteredEmittedRadiance (include/maps/scattered_emitted_radiance_mc.h):
+//      the same plus (1 - sa) * emission(x)
+// where radiance(x, wo) = transmittance(x, wo) * environment (the
+// ds.transmittance * ds.environment.after(ray_direction) of _objects.py:270).
+// rng is the evaluation's own stream; the transmittance forks from it.
+template <typename T> V3<T> exitance(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> wout) {
+    const int mode = S.s.exitance_mode;
+    if (mode == 0) return S.emission_at(x);
+    V3<T> wo;
+    const T rho = phase_sampler(S, rng, -wout, wo);
+    const V3<T> sa = S.albedo(x);
+    const V3<T> rad = S.environment() * transmittance(S, rng, x, wo, (int64_t*)nullptr);
+    V3<T> R = sa * rho * rad;
+    if (mode == 2) R += (V3<T>(T(1)) - sa) * S.emission_at(x);
+    return R;
+}
+// Adjoint of exitance() on the same draws.  The reference's backward of the
+// scattered maps hands (w, dL/dR) to the radiance map and drops the dL/dR
+// factor of the emission term of dL/dsa; here each factor gets the adjoint of
+// the forward's own expression.
+template <typename T> void exitance_bw(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> wout, V3<T> dL) {
+    const int mode = S.s.exitance_mode;
+    if (mode == 0) { S.emission_bw(x, dL); return; }
+    V3<T> wo;
+    const T rho = phase_sampler(S, rng, -wout, wo);
+    const V3<T> sa = S.albedo(x);
+    Rng tr_rng = rng;
+    const T Tr = transmittance(S, rng, x, wo, (int64_t*)nullptr);
+    const V3<T> env = S.environment();
+    const V3<T> rad = env * Tr;
+    V3<T> dL_dsa = dL * rad * rho;
+    const V3<T> dL_drad = dL * sa * rho;
+    if (mode == 2) {
+        const V3<T> em = S.emission_at(x);
+        dL_dsa -= dL * em;
+        S.emission_bw(x, dL * (V3<T>(T(1)) - sa));
+    }
+    S.albedo_bw(x, dL_dsa);
+    transmittance_bw(S, tr_rng, x, wo, dot(dL_drad, env));
+}
+
+// Streams of one collision-integrator path: the collision sampler on stream 2,
+// its adjoint on stream 4, exitance evaluation k on stream (k + 1) << 16 (its
+// transmittance on the fork after it).
+inline uint32_t exitance_stream(int64_t k) { return (uint32_t)((k + 1) & 0x7fff) << 16; }
+
+// include/maps/collision_integrator_mc.h:8-18 (MCCollisionIntegrator FORWARD)
+template <typename T> V3<T> collision_integrator_MC(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, Counters& c) {
+    Rng cs = rng.with_stream(2);
+    T t, Tt;
+    const T C = collision_sampler_DT(S, cs, x, w, t, Tt, &c.steps);
+    if (C != T(0)) ++c.vertices;
+    const V3<T> xt = w * t + x;
+    Rng xr = rng.with_stream(exitance_stream(0));
+    const V3<T> eR = C != T(0) ? exitance(S, xr, xt, -w) : V3<T>(T(0));
+    return eR * C + S.environment() * Tt;
+}
+// include/maps/collision_integrator_mc.h:20-41 (BACKWARD): the forward's
+// collision (same stream), the sampler's adjoint on its own stream, the
+// exitance's adjoint on the forward's exitance draws.
+template <typename T> void collision_integrator_MC_bw(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, V3<T> dL) {
+    Rng cs = rng.with_stream(2);
+    T t, Tt;
+    const T C = collision_sampler_DT(S, cs, x, w, t, Tt, (int64_t*)nullptr);
+    const V3<T> xt = w * t + x;
+    Rng xr = rng.with_stream(exitance_stream(0));
+    const V3<T> eR = C != T(0) ? exitance(S, xr, xt, -w) : V3<T>(T(0));
+    const V3<T> env = S.environment();
+    Rng cb = rng.with_stream(4);
+    collision_sampler_DT_bw(S, cb, x, w, (T)S.s.ds_epsilon, dot(dL, eR), dot(dL, env));
+    if (C != T(0)) {
+        Rng xb = rng.with_stream(exitance_stream(0));
+        exitance_bw(S, xb, xt, -w, dL * C);
+    }
+}
+
+// include/vr_collision_integrator_DDA.h:1-82: the DDA walk of the grid with
+// one random point per cell (the path stream): per cell the homogeneous
+// transmittance exp(-dt sigma(point)) and the exitance at the point.
+template <typename T> V3<T> collision_integrator_DDA(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, Counters& c) {
+    const V3<T> env = S.environment();
+    DDA<T> dda(S, x, w);
+    if (!dda.valid) return env;
+    T Tr = T(1), ct = T(0);
+    V3<T> R(T(0));
+    T s[2][2][2];
+    int64_t k = 0;
+    while (ct < dda.d - T(0.0001)) {
+        const T nt = vmin(dda.d, vmin(dda.alpha.x, vmin(dda.alpha.y, dda.alpha.z)));
+        dda.load_cell(s);
+        const T cell_t = mix(ct, nt, (T)rng.uniform());
+        const T sv = interpolated_sigma(dda.ialpha(cell_t), s);
+        const T vt = std::exp(-(nt - ct) * sv);
+        Rng xr = rng.with_stream(exitance_stream(k));
+        const V3<T> Le = exitance(S, xr, dda.x + w * cell_t, -w);
+        R += Le * (Tr * (T(1) - vt));
+        Tr *= vt;
+        ++c.steps;
+        ct = nt;
+        dda.step();
+        ++k;
+    }
+    return R + env * Tr;
+}
+// include/vr_collision_integrator_DDA.h:85-207: the same walk for fw_T and the
+// emitted part, then a replay from the same cell draws scattering
+// dL/dsigma = dL/dR . (T Le - fw_T env - R_rest) dt and the exitance adjoint.
+template <typename T> void collision_integrator_DDA_bw(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, V3<T> dL) {
+    if (dL.x == T(0) && dL.y == T(0) && dL.z == T(0)) return;
+    DDA<T> dda(S, x, w);
+    if (!dda.valid) return;
+    const Rng before = rng;
+    T Tr = T(1), ct = T(0);
+    V3<T> R(T(0));
+    T s[2][2][2];
+    int64_t k = 0;
+    while (ct < dda.d - T(0.0001)) {
+        const T nt = vmin(dda.d, vmin(dda.alpha.x, vmin(dda.alpha.y, dda.alpha.z)));
+        dda.load_cell(s);
+        const T cell_t = mix(ct, nt, (T)rng.uniform());
+        const T sv = interpolated_sigma(dda.ialpha(cell_t), s);
+        const T vt = std::exp(-(nt - ct) * sv);
+        Rng xr = rng.with_stream(exitance_stream(k));
+        R += exitance(S, xr, dda.x + w * cell_t, -w) * (Tr * (T(1) - vt));
+        Tr *= vt;
+        ct = nt;
+        dda.step();
+        ++k;
+    }
+    const V3<T> env = S.environment();
+    const T fw_T = Tr;
+    rng = before;
+    dda.reset_march();
+    Tr = T(1);
+    ct = T(0);
+    k = 0;
+    T g[2][2][2];
+    while (ct < dda.d - T(0.0001)) {
+        const T nt = vmin(dda.d, vmin(dda.alpha.x, vmin(dda.alpha.y, dda.alpha.z)));
+        dda.load_cell(s);
+        const T cell_t = mix(ct, nt, (T)rng.uniform());
+        const V3<T> a = dda.ialpha(cell_t);
+        const T sv = interpolated_sigma(a, s);
+        const T dt = nt - ct;
+        const T vt = std::exp(-dt * sv);
+        const V3<T> xp = dda.x + w * cell_t;
+        Rng xr = rng.with_stream(exitance_stream(k));
+        const V3<T> Le = exitance(S, xr, xp, -w);
+        Rng xb = rng.with_stream(exitance_stream(k));
+        exitance_bw(S, xb, xp, -w, dL * (Tr * (T(1) - vt)));
+        R -= Le * (Tr * (T(1) - vt));
+        Tr *= vt;
+        const T dL_dsigma = dot(dL, (Le * Tr - env * fw_T - R) * dt);
+        interpolated_sigma_bw(a, dL_dsigma, g);
+        for (int dz = 0; dz < 2; ++dz)
+            for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx)
+                    S.sigma_at_bw(dda.cell[0] + dx, dda.cell[1] + dy, dda.cell[2] + dz, g[dz][dy][dx]);
+        ct = nt;
+        dda.step();
+        ++k;
+    }
+}
+
+// integrator: 0 NEE, 1 DT, 2 MC collision integrator, 3 DDA collision integrator
 template <typename T> V3<T> radiance(const Scene<T>& S, int integrator, Rng& rng, V3<T> x, V3<T> w, Counters& c) {
+    if (integrator == 2) return collision_integrator_MC(S, rng, x, w, c);
+    if (integrator == 3) return collision_integrator_DDA(S, rng, x, w, c);
     return integrator == 0 ? path_integrator_NEE(S, rng, x, w, false, c) : path_integrator_DT(S, rng, x, w, c);
 }
 template <typename T> void radiance_bw(const Scene<T>& S, int bw_mode, Rng& rng, V3<T> x, V3<T> w, V3<T> dL) {
@@ -1814,7 +2102,9 @@ template <typename T> void radiance_bw(const Scene<T>& S, int bw_mode, Rng& rng,
     else if (bw_mode == 2) path_integrator_NEE_DRT_bw(S, rng, x, w, dL);
     else if (bw_mode == 3) path_integrator_NEE_DRTQ_bw(S, rng, x, w, dL);
     else if (bw_mode == 4) path_integrator_NEE_DRTDS_bw(S, rng, x, w, (T)S.s.ds_epsilon, dL);
-    else path_integrator_NEE_SPS_bw(S, rng, x, w, dL);
+    else if (bw_mode == 5) path_integrator_NEE_SPS_bw(S, rng, x, w, dL);
+    else if (bw_mode == 6) collision_integrator_MC_bw(S, rng, x, w, dL);
+    else collision_integrator_DDA_bw(S, rng, x, w, dL);
 }
 
 template <typename T> void transmittance_fw_impl(const orc_scene* s, int32_t mode, const float* rays, int64_t n, uint64_t seed, float* Tout) {
@@ -2023,6 +2313,32 @@ void orc_radiance_fw(const orc_scene* s, int32_t integrator, const float* rays, 
         steps += cnt.steps;
     }
     if (c) { c->paths = n; c->vertices = verts; c->steps = steps; }
+}
+
+// DeltatrackingCollisionSampler as a map (include/maps/collision_sampler_dt.h):
+// ray i draws from stream 2 of path i (its adjoint from stream 4), as inside
+// the MC collision integrator.
+void orc_collision_sample_fw(const orc_scene* s, const float* rays, int64_t n, uint64_t seed, float* out3) {
+    Scene<float> S(*s);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < n; ++i) {
+        Rng rng(seed, (uint64_t)i, 2);
+        float t, Tt;
+        const float C = collision_sampler_DT(S, rng, V3<float>::load(rays + 6 * i), V3<float>::load(rays + 6 * i + 3), t,
+                                             Tt, (int64_t*)nullptr);
+        out3[3 * i] = C;
+        out3[3 * i + 1] = t;
+        out3[3 * i + 2] = Tt;
+    }
+}
+void orc_collision_sample_bw(const orc_scene* s, const float* rays, int64_t n, uint64_t seed, const float* dL_dout3) {
+    Scene<float> S(*s);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < n; ++i) {
+        Rng rng(seed, (uint64_t)i, 4);
+        collision_sampler_DT_bw(S, rng, V3<float>::load(rays + 6 * i), V3<float>::load(rays + 6 * i + 3),
+                                (float)s->ds_epsilon, dL_dout3[3 * i], dL_dout3[3 * i + 2]);
+    }
 }
 
 void orc_radiance_bw(const orc_scene* s, int32_t bw_mode, const float* rays, int64_t n, uint64_t seed, const float* dL_dR) {

@@ -90,6 +90,13 @@ static bool use_wave_bw(const DMedium& M, int bw_mode) {
     return bw_mode == VRT_BW_NEE_DS && M.max_bounces > 0 && M.max_bounces <= 4096 && !M.ds_compat;
 }
 
+static bool is_collision(int integrator) {
+    return integrator == VRT_PI_MC_COLLISION || integrator == VRT_PI_DDA_COLLISION;
+}
+static int collision_of(int bw_mode) {
+    return bw_mode == VRT_BW_MC_COLLISION ? VRT_PI_MC_COLLISION : VRT_PI_DDA_COLLISION;
+}
+
 int ensure_wave_buffer(vrt_context* ctx, size_t bytes) {
     if (ctx->wave && ctx->wave_bytes >= bytes) return VRT_OK;
     if (ctx->wave) {
@@ -256,6 +263,12 @@ static int to_dmedium(const vrt_medium* m, DMedium& M) {
     if (m->phase_mode < 0 || m->phase_mode > 1) return VRT_E_INVALID_ARGUMENT;
     if (m->transmittance_mode < 0 || m->transmittance_mode > 5) return VRT_E_INVALID_ARGUMENT;
     if (m->max_bounces < 0) return VRT_E_INVALID_ARGUMENT;
+    if (m->exitance_mode < 0 || m->exitance_mode > 2) return VRT_E_INVALID_ARGUMENT;
+    if (m->emission_is_grid) {
+        st = to_dgrid(m->emission_grid, 0, M.emission_grid);
+        if (st) return st;
+        if (M.emission_grid.C != 1 && M.emission_grid.C != 3) return VRT_E_BAD_SHAPE;
+    }
     if (m->majorant_mode == 1) {
         if (!m->maj_grid) return VRT_E_NULL_POINTER;
         if (m->maj_dims[0] < 1 || m->maj_dims[1] < 1 || m->maj_dims[2] < 1) return VRT_E_BAD_SHAPE;
@@ -278,6 +291,8 @@ static int to_dmedium(const vrt_medium* m, DMedium& M) {
     M.max_bounces = m->max_bounces;
     M.ds_eps = m->ds_epsilon;
     M.ds_compat = m->ds_compat;
+    M.exitance_mode = m->exitance_mode;
+    M.emission_is_grid = m->emission_is_grid ? 1 : 0;
     return VRT_OK;
 }
 
@@ -531,11 +546,36 @@ int vrt_transmittance_bw(vrt_context* ctx, const vrt_medium* m, int32_t mode, co
     return launch_transmittance_bw(M, mode, rays, n, seed, dL_dT, ctx->scratch, (cudaStream_t)stream);
 }
 
+int vrt_collision_sample_fw(vrt_context* ctx, const vrt_medium* m, const float* rays, int64_t n, uint64_t seed,
+                            float* out, void* stream) {
+    int st = check_ctx(ctx);
+    if (st) return st;
+    if (n < 0) return VRT_E_BAD_SHAPE;
+    DMedium M;
+    if ((st = to_dmedium(m, M))) return st;
+    if (n == 0) return VRT_OK;
+    if (!rays || !out) return VRT_E_NULL_POINTER;
+    return launch_collision_sample(M, rays, n, seed, out, nullptr, ctx->scratch, ctx->num_sms, (cudaStream_t)stream);
+}
+
+int vrt_collision_sample_bw(vrt_context* ctx, const vrt_medium* m, const float* rays, int64_t n, uint64_t seed,
+                            const float* dL_dout, void* stream) {
+    int st = check_ctx(ctx);
+    if (st) return st;
+    if (n < 0) return VRT_E_BAD_SHAPE;
+    DMedium M;
+    if ((st = to_dmedium(m, M))) return st;
+    if (n == 0 || !M.sigma.grad) return VRT_OK;
+    if (!rays || !dL_dout) return VRT_E_NULL_POINTER;
+    return launch_collision_sample(M, rays, n, seed, nullptr, dL_dout, ctx->scratch, ctx->num_sms,
+                                   (cudaStream_t)stream);
+}
+
 int vrt_radiance_fw(vrt_context* ctx, const vrt_medium* m, int32_t integrator, const float* rays, int64_t n,
                     uint64_t seed, float* R, void* stream) {
     int st = check_ctx(ctx);
     if (st) return st;
-    if (integrator < 0 || integrator > 1) return VRT_E_INVALID_ARGUMENT;
+    if (integrator < 0 || integrator > VRT_PI_DDA_COLLISION) return VRT_E_INVALID_ARGUMENT;
     if (n < 0) return VRT_E_BAD_SHAPE;
     DMedium M;
     if ((st = to_dmedium(m, M))) return st;
@@ -545,6 +585,9 @@ int vrt_radiance_fw(vrt_context* ctx, const vrt_medium* m, int32_t integrator, c
     std::memset(&S, 0, sizeof(S));
     S.is_camera = 0;
     S.rays = rays;
+    if (is_collision(integrator))
+        return launch_collision_fw(M, integrator, S, (uint64_t)n, seed, R, 1.0f, ctx->scratch, ctx->num_sms,
+                                   (cudaStream_t)stream);
     if (use_wave(M, integrator)) {  // the wavefront accumulates: clear R first
         cudaError_t e = cudaMemsetAsync(R, 0, sizeof(float) * 3 * (size_t)n, (cudaStream_t)stream);
         if (e != cudaSuccess) return launch_status(e);
@@ -558,7 +601,7 @@ int vrt_radiance_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, cons
                     uint64_t seed, const float* dL_dR, void* stream) {
     int st = check_ctx(ctx);
     if (st) return st;
-    if (bw_mode < 0 || bw_mode > VRT_BW_NEE_SPS) return VRT_E_INVALID_ARGUMENT;
+    if (bw_mode < 0 || bw_mode > VRT_BW_DDA_COLLISION) return VRT_E_INVALID_ARGUMENT;
     if (n < 0) return VRT_E_BAD_SHAPE;
     DMedium M;
     if ((st = to_dmedium(m, M))) return st;
@@ -568,6 +611,9 @@ int vrt_radiance_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, cons
     std::memset(&S, 0, sizeof(S));
     S.is_camera = 0;
     S.rays = rays;
+    if (bw_mode >= VRT_BW_MC_COLLISION)
+        return launch_collision_bw(M, collision_of(bw_mode), S, (uint64_t)n, seed, dL_dR, 1.0f, ctx->scratch,
+                                   ctx->num_sms, (cudaStream_t)stream);
     if (use_wave_bw(M, bw_mode)) return launch_wave_ds_bw(ctx, M, S, (uint64_t)n, seed, dL_dR, 1.0f, (cudaStream_t)stream);
     return launch_radiance_bw(M, bw_mode, S, (uint64_t)n, seed, dL_dR, 1.0f, ctx->scratch, ctx->num_sms,
                               (cudaStream_t)stream);
@@ -577,7 +623,7 @@ int vrt_capture_fw(vrt_context* ctx, const vrt_medium* m, int32_t integrator, co
                    uint64_t seed, float* rgb, void* stream) {
     int st = check_ctx(ctx);
     if (st) return st;
-    if (integrator < 0 || integrator > 1) return VRT_E_INVALID_ARGUMENT;
+    if (integrator < 0 || integrator > VRT_PI_DDA_COLLISION) return VRT_E_INVALID_ARGUMENT;
     if (spp < 1) return VRT_E_INVALID_ARGUMENT;
     DMedium M;
     if ((st = to_dmedium(m, M))) return st;
@@ -589,6 +635,9 @@ int vrt_capture_fw(vrt_context* ctx, const vrt_medium* m, int32_t integrator, co
     S.npix = capture_pixels(cam);
     cudaError_t e = cudaMemsetAsync(rgb, 0, sizeof(float) * 3 * S.npix, (cudaStream_t)stream);
     if (e != cudaSuccess) return launch_status(e);
+    if (is_collision(integrator))
+        return launch_collision_fw(M, integrator, S, (uint64_t)S.npix * (uint64_t)spp, seed, rgb, 1.0f / (float)spp,
+                                   ctx->scratch, ctx->num_sms, (cudaStream_t)stream);
     if (use_wave(M, integrator))
         return launch_wave_fw(ctx, M, S, (uint64_t)S.npix * (uint64_t)spp, seed, rgb, 1.0f / (float)spp,
                               (cudaStream_t)stream);
@@ -600,7 +649,7 @@ int vrt_capture_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const
                    uint64_t seed, const float* dL_drgb, void* stream) {
     int st = check_ctx(ctx);
     if (st) return st;
-    if (bw_mode < 0 || bw_mode > VRT_BW_NEE_SPS) return VRT_E_INVALID_ARGUMENT;
+    if (bw_mode < 0 || bw_mode > VRT_BW_DDA_COLLISION) return VRT_E_INVALID_ARGUMENT;
     if (spp < 1) return VRT_E_INVALID_ARGUMENT;
     DMedium M;
     if ((st = to_dmedium(m, M))) return st;
@@ -610,6 +659,9 @@ int vrt_capture_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const
     if (!dL_drgb) return VRT_E_NULL_POINTER;
     S.is_camera = 1;
     S.npix = capture_pixels(cam);
+    if (bw_mode >= VRT_BW_MC_COLLISION)
+        return launch_collision_bw(M, collision_of(bw_mode), S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb,
+                                   (float)spp, ctx->scratch, ctx->num_sms, (cudaStream_t)stream);
     if (use_wave_bw(M, bw_mode))
         return launch_wave_ds_bw(ctx, M, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
                                  (cudaStream_t)stream);

@@ -238,12 +238,9 @@ __device__ __forceinline__ void sigma_bw(const DMedium& M, float3 x, float dL, T
     grid_scatter(M.sigma, normalized(M, x), &dL, 1);
 }
 
-// Albedo: const or Grid3D with C 1 (promoted to 3) or 3 (include/vr_scattering_albedo.h).
-__device__ __forceinline__ float3 albedo(const DMedium& M, float3 x, Tally& tl) {
-    if (!M.albedo_is_grid) return M.albedo_const;
-    ++tl.albedo;
-    const DGrid& g = M.albedo;
-    float3 nc = normalized(M, x);
+// Grid3D lookup of a C == 1 (promoted to 3) or C == 3 grid at normalized
+// coordinates nc (include/maps/grid3d.h:6-37): zero outside [0, 1)^3.
+__device__ __forceinline__ float3 grid_rgb(const DGrid& g, float3 nc) {
     if (nc.x < 0.0f || nc.y < 0.0f || nc.z < 0.0f || nc.x >= 1.0f || nc.y >= 1.0f || nc.z >= 1.0f) return f3(0.0f);
     const int dx = g.W - 1, dy = g.H - 1, dz = g.D - 1;
     float gx = nc.x * (float)dx, gy = nc.y * (float)dy, gz = nc.z * (float)dz;
@@ -270,16 +267,39 @@ __device__ __forceinline__ float3 albedo(const DMedium& M, float3 x, Tally& tl) 
     }
     return o;
 }
+// Adjoint of grid_rgb (a C == 1 grid receives the channel sum).
+__device__ __forceinline__ void grid_rgb_bw(const DGrid& g, float3 nc, float3 dL) {
+    if (g.C == 1) {
+        float s = dL.x + dL.y + dL.z;
+        grid_scatter(g, nc, &s, 1);
+    } else {
+        float d[3] = {dL.x, dL.y, dL.z};
+        grid_scatter(g, nc, d, 3);
+    }
+}
+
+// Albedo: const or Grid3D with C 1 (promoted to 3) or 3 (include/vr_scattering_albedo.h).
+__device__ __forceinline__ float3 albedo(const DMedium& M, float3 x, Tally& tl) {
+    if (!M.albedo_is_grid) return M.albedo_const;
+    ++tl.albedo;
+    return grid_rgb(M.albedo, normalized(M, x));
+}
 __device__ __forceinline__ void albedo_bw(const DMedium& M, float3 x, float3 dL, Tally& tl) {
     if (!M.albedo_is_grid || !M.albedo.grad) return;
     tl.reds += 8 * M.albedo.C;
-    if (M.albedo.C == 1) {
-        float g = dL.x + dL.y + dL.z;
-        grid_scatter(M.albedo, normalized(M, x), &g, 1);
-    } else {
-        float g[3] = {dL.x, dL.y, dL.z};
-        grid_scatter(M.albedo, normalized(M, x), g, 3);
-    }
+    grid_rgb_bw(M.albedo, normalized(M, x), dL);
+}
+
+// Emission of the collision integrators' exitance (include/vr_emission.h):
+// const, or a Grid3D (C 1 or 3) over sigma's box.
+__device__ __forceinline__ float3 emission_at(const DMedium& M, float3 x) {
+    if (!M.emission_is_grid) return M.emission;
+    return grid_rgb(M.emission_grid, normalized(M, x));
+}
+__device__ __forceinline__ void emission_bw(const DMedium& M, float3 x, float3 dL, Tally& tl) {
+    if (!M.emission_is_grid || !M.emission_grid.grad) return;
+    tl.reds += 8 * M.emission_grid.C;
+    grid_rgb_bw(M.emission_grid, normalized(M, x), dL);
 }
 
 // ------------------------------------------------------------- majorant --

@@ -67,6 +67,16 @@ int launch_cache_paths(const DMedium& M, int mode, const PathSrc& src, uint64_t 
 // Training targets from the recorded collisions and the per-path estimates.
 int launch_cache_targets(float* smp, const float* pR, long long n_paths, int rec, cudaStream_t stream);
 
+// Collision integrators (vrt_collision.cu): integrator VRT_PI_MC_COLLISION or
+// VRT_PI_DDA_COLLISION; out / dL as in launch_radiance_fw / _bw.
+int launch_collision_fw(const DMedium& M, int integrator, const PathSrc& src, uint64_t n_paths, uint64_t seed,
+                        float* out, float scale, DScratch* scratch, int num_sms, cudaStream_t stream);
+int launch_collision_bw(const DMedium& M, int integrator, const PathSrc& src, uint64_t n_paths, uint64_t seed,
+                        const float* dL, float div, DScratch* scratch, int num_sms, cudaStream_t stream);
+// DeltatrackingCollisionSampler on rays: forward when out3 != null, else backward with dL3.
+int launch_collision_sample(const DMedium& M, const float* rays, int64_t n, uint64_t seed, float* out3,
+                            const float* dL3, DScratch* scratch, int num_sms, cudaStream_t stream);
+
 // The NEE_DS adjoint as a persistent state machine (vrt_adjoint.cu).
 int launch_nee_ds_bw(const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed, const float* dL,
                      float div, DScratch* scratch, int num_sms, cudaStream_t stream);

@@ -36,6 +36,9 @@ struct DMedium {
     int max_bounces;
     float ds_eps;
     int ds_compat;
+    int exitance_mode;     // collision integrators: 0 emission, 1 scattered, 2 scattered + emitted
+    int emission_is_grid;  // emission: 0 const, 1 emission_grid
+    DGrid emission_grid;
 };
 
 struct DCamera {

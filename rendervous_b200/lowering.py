@@ -55,6 +55,8 @@ class MediumDesc:
     max_bounces: int = 0
     ds_epsilon: float = 0.1
     ds_compat: int = 0
+    exitance_mode: int = 0                   # collision integrators: 0 emission, 1 scattered, 2 scattered+emitted
+    emission_grid: typing.Optional[torch.Tensor] = None  # [D,H,W,C], C 1 or 3, sigma's box
 
     # -- derived quantities, computed in float32 exactly as the kernels read them
     def inv_bsize(self) -> np.ndarray:
@@ -87,10 +89,12 @@ class MediumDesc:
             majorant_mode=self.majorant_mode, global_majorant=self.global_majorant,
             maj_grid=f(self.maj_grid), maj_dims=self.maj_dims(), maj_scale=self.maj_scale(),
             transmittance_mode=self.transmittance_mode, max_bounces=self.max_bounces,
-            ds_epsilon=self.ds_epsilon, ds_compat=self.ds_compat)
+            ds_epsilon=self.ds_epsilon, ds_compat=self.ds_compat, exitance_mode=self.exitance_mode,
+            emission_grid=f(self.emission_grid))
 
     # -- the C struct (device pointers); keep the returned object alive during the call
-    def to_struct(self, sigma_grad: torch.Tensor | None = None, albedo_grad: torch.Tensor | None = None):
+    def to_struct(self, sigma_grad: torch.Tensor | None = None, albedo_grad: torch.Tensor | None = None,
+                  emission_grad: torch.Tensor | None = None):
         ffi, _ = _lib.ffi_lib()
         m = ffi.new("vrt_medium *")
         _fill_grid(m.sigma, self.sigma, sigma_grad)
@@ -126,6 +130,10 @@ class MediumDesc:
         m.max_bounces = int(self.max_bounces)
         m.ds_epsilon = float(self.ds_epsilon)
         m.ds_compat = int(self.ds_compat)
+        m.exitance_mode = int(self.exitance_mode)
+        if self.emission_grid is not None:
+            m.emission_is_grid = 1
+            _fill_grid(m.emission_grid, self.emission_grid, emission_grad)
         return m
 
 
@@ -279,6 +287,104 @@ def lower_integrator(pi) -> MediumDesc:
     kw["max_bounces"] = int(getattr(pi, "max_bounces", 0))
     kw["ds_epsilon"] = float(getattr(pi, "ds_epsilon", 0.1) or 0.0)
     kw["ds_compat"] = 1 if getattr(pi, "ds_compat", False) else 0
+    return MediumDesc(**kw)
+
+
+def _lower_albedo(alb, sigma, kw: dict):
+    from . import maps
+    if isinstance(alb, maps.Grid3D):
+        if alb.grid.shape[-1] not in (1, 3):
+            raise NotImplementedError("albedo Grid3D must have 1 or 3 channels")
+        if not (torch.equal(alb.bmin.cpu(), sigma.bmin.cpu()) and torch.equal(alb.bmax.cpu(), sigma.bmax.cpu())):
+            raise NotImplementedError("albedo Grid3D must share sigma's box")
+        kw["albedo_grid"] = alb.grid
+    else:
+        kw["albedo_const"] = _const_values(alb, 3)
+
+
+def _lower_emission(em, sigma, kw: dict):
+    """The emission map of an exitance radiance: a constant, or a Grid3D of 1 or
+    3 channels over sigma's box (read at the position; it ignores the direction)."""
+    from . import maps
+    if isinstance(em, maps.Grid3D):
+        if em.grid.shape[-1] not in (1, 3):
+            raise NotImplementedError("an emission Grid3D must have 1 or 3 channels")
+        if not (torch.equal(em.bmin.cpu(), sigma.bmin.cpu()) and torch.equal(em.bmax.cpu(), sigma.bmax.cpu())):
+            raise NotImplementedError("an emission Grid3D must share sigma's box")
+        kw["emission_grid"] = em.grid
+    else:
+        kw["emission"] = _const_values(em, 3)
+
+
+def _lower_phase_sampler(sampler, kw: dict):
+    """A phase sampler used alone (no phase map is evaluated): VHGPhaseSampler
+    draws the reference's mixture (phase_mode 1), HenyeyGreensteinPhaseSampler
+    pure HG (phase_mode 0); both report weight 1."""
+    from . import maps
+    if isinstance(sampler, maps.VHGPhaseSampler):
+        kw["phase_mode"] = 1
+    elif isinstance(sampler, maps.HenyeyGreensteinPhaseSampler):
+        kw["phase_mode"] = 0
+    else:
+        raise NotImplementedError(f"phase sampler {type(sampler).__name__} is not supported")
+    kw["phase_g"] = _const_values(sampler.phase_g, 1)[0]
+
+
+def _transmitted_environment(radiance):
+    """(transmittance map, environment constant) of a radiance map of the form
+    transmittance * environment.after(ray_direction) (_objects.py:262-265)."""
+    from . import maps
+    if not isinstance(radiance, maps.MultiplicationMap):
+        raise NotImplementedError("the radiance of a scattered exitance must be transmittance * environment")
+    a, b = radiance.map_a, radiance.map_b
+    if isinstance(a, maps.CompositionMap):
+        a, b = b, a
+    if not (isinstance(b, maps.CompositionMap) and isinstance(b.map_a, maps.RayDirection)):
+        raise NotImplementedError("the radiance of a scattered exitance must be transmittance * environment")
+    return a, _const_values(b.map_b, 3)
+
+
+def lower_collision_integrator(ci) -> MediumDesc:
+    """MediumDesc of MCCollisionIntegrator (_maps.py:2792-2808) or
+    GridDDACollisionIntegrator (_maps.py:2811-2852): sigma, boundary (and the
+    collision sampler's majorant and epsilon), the environment constant, and
+    the exitance radiance -- an emission map, MCScatteredRadiance or
+    MCScatteredEmittedRadiance over transmittance * environment."""
+    from . import maps
+    kw: dict = {}
+    if isinstance(ci, maps.MCCollisionIntegrator):
+        cs = ci.collision_sampler
+        if not isinstance(cs, maps.DeltatrackingCollisionSampler):
+            raise NotImplementedError("the collision sampler must be a DeltatrackingCollisionSampler")
+        sigma = cs.sigma
+        lower_sigma(sigma, kw)
+        lower_boundary(cs.boundary, kw)
+        lower_majorant(cs.majorant, sigma, kw)
+        kw["ds_epsilon"] = float(cs.ds_epsilon)
+    else:
+        sigma = ci.sigma_grid
+        lower_sigma(sigma, kw)
+        lower_boundary(ci.boundary, kw)
+    kw["env"] = _const_values(ci.environment, 3)
+    ex = ci.exitance_radiance
+    if isinstance(ex, (maps.MCScatteredRadiance, maps.MCScatteredEmittedRadiance)):
+        kw["exitance_mode"] = 1 if isinstance(ex, maps.MCScatteredRadiance) else 2
+        _lower_albedo(ex.scattering_albedo, sigma, kw)
+        _lower_phase_sampler(ex.phase_sampler, kw)
+        tr, env = _transmitted_environment(ex.radiance)
+        if env != kw["env"]:
+            raise NotImplementedError("the scattered radiance's environment must be the integrator's environment")
+        lower_transmittance(tr, sigma, kw)
+        tmaj = getattr(tr, "majorant", None)
+        if tmaj is not None:
+            if isinstance(ci, maps.MCCollisionIntegrator) and tmaj is not ci.collision_sampler.majorant:
+                raise NotImplementedError("the transmittance and the collision sampler must share the majorant")
+            lower_majorant(tmaj, sigma, kw)
+        if isinstance(ex, maps.MCScatteredEmittedRadiance):
+            _lower_emission(ex.emission, sigma, kw)
+    else:
+        kw["exitance_mode"] = 0
+        _lower_emission(ex, sigma, kw)
     return MediumDesc(**kw)
 
 

@@ -18,7 +18,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .lowering import TR_MODES, lower_integrator, lower_transmittance_map
+from .lowering import TR_MODES, lower_collision_integrator, lower_integrator, lower_transmittance_map
 
 # ----------------------------------------------------------------- seeds --
 _MANUAL_SEED: dict = {"value": None}
@@ -101,6 +101,46 @@ class MapBase(torch.nn.Module):
 
     def forward(self, *args):
         raise NotImplementedError(f"{type(self).__name__} is evaluated only inside a path integrator here")
+
+    # map algebra (_maps.py:1347-1415): the forms the lowering recognises
+    def after(self, prev_map: "MapBase") -> "MapBase":
+        """CompositionMap(prev_map, self): self applied to prev_map's output."""
+        return CompositionMap(prev_map, self)
+
+    def __mul__(self, other):
+        return MultiplicationMap(self, other if isinstance(other, MapBase) else const[other])
+
+    def __rmul__(self, other):
+        return MultiplicationMap(self, other if isinstance(other, MapBase) else const[other])
+
+
+class CompositionMap(MapBase):
+    """CompositionMap (_maps.py:1804): map_b(map_a(x))."""
+
+    def __init__(self, map_a: MapBase, map_b: MapBase):
+        super().__init__(map_a.input_dim, map_b.output_dim)
+        self.map_a = map_a
+        self.map_b = map_b
+
+
+class MultiplicationMap(MapBase):
+    """MultiplicationMap (_maps.py:1918): map_a(x) * map_b(x) (a scalar side promoted)."""
+
+    def __init__(self, map_a: MapBase, map_b: MapBase):
+        dims = [d for d in (map_a.output_dim, map_b.output_dim) if d is not None]
+        super().__init__(map_a.input_dim or map_b.input_dim, max(dims) if dims else None)
+        self.map_a = map_a
+        self.map_b = map_b
+
+
+class RayDirection(MapBase):
+    """RayDirection (_maps.py:3164-3185): (x, w) -> w."""
+
+    def __init__(self):
+        super().__init__(6, 3)
+
+
+ray_direction = RayDirection()
 
 
 class ConstantMap(MapBase):
@@ -517,7 +557,7 @@ class DeltatrackingTransmittance(_TransmittanceMap):
 # -------------------------------------------------------- path integrators --
 class _RadianceFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, rays, sigma_grid, albedo_grid, integrator, desc, fw_mode, bw_mode, seed):
+    def forward(ctx, rays, sigma_grid, albedo_grid, emission_grid, integrator, desc, fw_mode, bw_mode, seed):
         ffi, lib = _lib.ffi_lib()
         r = rays.detach().reshape(-1, 6).contiguous()
         R = torch.empty(r.shape[0], 3, device=rays.device, dtype=torch.float32)
@@ -538,16 +578,18 @@ class _RadianceFn(torch.autograd.Function):
             raise NotImplementedError("this integrator's adjoint is not available")
         gs = torch.zeros_like(desc.sigma) if ctx.needs_input_grad[1] else None
         ga = torch.zeros_like(desc.albedo_grid) if (ctx.needs_input_grad[2] and desc.albedo_grid is not None) else None
-        if gs is not None or ga is not None:
+        ge = (torch.zeros_like(desc.emission_grid)
+              if (ctx.needs_input_grad[3] and desc.emission_grid is not None) else None)
+        if gs is not None or ga is not None or ge is not None:
             ffi, lib = _lib.ffi_lib()
-            m = desc.to_struct(sigma_grad=gs, albedo_grad=ga)
+            m = desc.to_struct(sigma_grad=gs, albedo_grad=ga, emission_grad=ge)
             d = dR.reshape(-1, 3).contiguous().float()
             vctx = _lib.context(r.device)
             _lib.check(lib.vrt_radiance_bw(vctx.ptr, m, ctx.bw_mode, _lib.fptr(r), r.shape[0], ctx.seed, _lib.fptr(d),
                                            _lib.stream_handle(r.device)), "vrt_radiance_bw")
             _after_call(r.device)
         dr = torch.zeros(ctx.rshape, device=r.device) if ctx.needs_input_grad[0] else None
-        return dr, gs, ga, None, None, None, None, None
+        return dr, gs, ga, ge, None, None, None, None, None
 
 
 class _PathIntegrator(MapBase):
@@ -566,14 +608,15 @@ class _PathIntegrator(MapBase):
         return lower_integrator(self)
 
     def grid_tensors(self):
+        """(sigma, albedo, emission) grid parameters the adjoint may write (None where constant)."""
         sg = self.sigma.grid
         ag = self.scattering_albedo.grid if isinstance(self.scattering_albedo, Grid3D) else None
-        return sg, ag
+        return sg, ag, None
 
     def forward(self, rays: torch.Tensor, seed: typing.Optional[int] = None) -> torch.Tensor:
         desc = self.lower()
-        sg, ag = self.grid_tensors()
-        return _RadianceFn.apply(rays, sg, ag, self, desc, self.FW, self.BW, next_seed() if seed is None else seed)
+        sg, ag, eg = self.grid_tensors()
+        return _RadianceFn.apply(rays, sg, ag, eg, self, desc, self.FW, self.BW, next_seed() if seed is None else seed)
 
 
 def _nee_subs(sigma, scattering_albedo, emission, environment, environment_sampler, phase, phase_sampler, boundary,
@@ -644,10 +687,149 @@ class SPSPathIntegrator(DRTPathIntegrator):
     BW = 5
 
 
+# ---------------------------------------------------- collision integrators --
+class _CollisionSampleFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, rays, sigma_grid, desc, seed):
+        ffi, lib = _lib.ffi_lib()
+        r = rays.detach().reshape(-1, 6).contiguous()
+        out = torch.empty(r.shape[0], 3, device=rays.device, dtype=torch.float32)
+        _lib.check(lib.vrt_collision_sample_fw(_lib.context(rays.device).ptr, desc.to_struct(), _lib.fptr(r),
+                                               r.shape[0], seed, _lib.fptr(out), _lib.stream_handle(rays.device)),
+                   "vrt_collision_sample_fw")
+        _after_call(rays.device)
+        ctx.save_for_backward(r)
+        ctx.desc, ctx.seed, ctx.rshape = desc, seed, rays.shape
+        return out.reshape(*rays.shape[:-1], 3)
+
+    @staticmethod
+    def backward(ctx, dout):
+        r, = ctx.saved_tensors
+        gs = None
+        if ctx.needs_input_grad[1]:
+            ffi, lib = _lib.ffi_lib()
+            gs = torch.zeros_like(ctx.desc.sigma)
+            d = dout.reshape(-1, 3).contiguous().float()
+            _lib.check(lib.vrt_collision_sample_bw(_lib.context(r.device).ptr, ctx.desc.to_struct(sigma_grad=gs),
+                                                   _lib.fptr(r), r.shape[0], ctx.seed, _lib.fptr(d),
+                                                   _lib.stream_handle(r.device)), "vrt_collision_sample_bw")
+            _after_call(r.device)
+        dr = torch.zeros(ctx.rshape, device=r.device) if ctx.needs_input_grad[0] else None
+        return dr, gs, None, None
+
+
+class DeltatrackingCollisionSampler(MapBase):
+    """DeltatrackingCollisionSampler (_maps.py:2714-2727, include/vr_collision_sampler_DT.h):
+    (x, w) -> (C, t, T): a delta-tracking collision (C = 1, T = 0) at distance t,
+    or none (C = 0, T = 1, t at the exit).  Backward: the defensively sampled
+    adjoint of dL/dC and dL/dT (ds_epsilon); dL/dt is not propagated."""
+
+    def __init__(self, sigma: MapBase, boundary: MapBase, majorant: MapBase, ds_epsilon: float):
+        super().__init__(6, 3)
+        self.sigma = sigma
+        self.boundary = boundary
+        self.majorant = majorant
+        self.ds_epsilon = float(ds_epsilon)
+
+    def lower(self):
+        from .lowering import MediumDesc, lower_boundary, lower_majorant, lower_sigma
+        kw: dict = {}
+        lower_sigma(self.sigma, kw)
+        lower_boundary(self.boundary, kw)
+        lower_majorant(self.majorant, self.sigma, kw)
+        kw["ds_epsilon"] = self.ds_epsilon
+        return MediumDesc(**kw)
+
+    def forward(self, rays: torch.Tensor, seed: typing.Optional[int] = None) -> torch.Tensor:
+        desc = self.lower()
+        return _CollisionSampleFn.apply(rays, desc.sigma, desc, next_seed() if seed is None else seed)
+
+
+class MCScatteredRadiance(MapBase):
+    """MCScatteredRadiance (_maps.py:2730-2743, include/maps/scattered_radiance_mc.h):
+    exitance sa(x) * rho * radiance(x, wo), (rho, wo) from the phase sampler;
+    an exitance radiance of the collision integrators (radiance =
+    transmittance * environment.after(ray_direction))."""
+
+    def __init__(self, scattering_albedo: MapBase, phase_sampler: MapBase, radiance: MapBase):
+        super().__init__(6, 3)
+        self.scattering_albedo = scattering_albedo
+        self.phase_sampler = phase_sampler
+        self.radiance = radiance
+
+
+class MCScatteredEmittedRadiance(MapBase):
+    """MCScatteredEmittedRadiance (_maps.py:2746-2760, include/maps/scattered_emitted_radiance_mc.h):
+    MCScatteredRadiance plus (1 - sa) * emission(x)."""
+
+    def __init__(self, scattering_albedo: MapBase, emission: MapBase, phase_sampler: MapBase, radiance: MapBase):
+        super().__init__(6, 3)
+        self.scattering_albedo = scattering_albedo
+        self.emission = emission
+        self.phase_sampler = phase_sampler
+        self.radiance = radiance
+
+
+class _CollisionIntegrator(_PathIntegrator):
+    def lower(self):
+        return lower_collision_integrator(self)
+
+    def _sigma_grid3d(self) -> Grid3D:
+        raise NotImplementedError
+
+    def grid_tensors(self):
+        ex = self.exitance_radiance
+        ag = eg = None
+        if isinstance(ex, (MCScatteredRadiance, MCScatteredEmittedRadiance)) and \
+                isinstance(ex.scattering_albedo, Grid3D):
+            ag = ex.scattering_albedo.grid
+        em = ex.emission if isinstance(ex, MCScatteredEmittedRadiance) else ex
+        if isinstance(em, Grid3D):
+            eg = em.grid
+        return self._sigma_grid3d().grid, ag, eg
+
+
+class MCCollisionIntegrator(_CollisionIntegrator):
+    """MCCollisionIntegrator (_maps.py:2792-2808, include/maps/collision_integrator_mc.h):
+    C * exitance_radiance(x_t, -w) + T * environment(w) from one collision sample."""
+    FW, BW = 2, 6
+
+    def __init__(self, collision_sampler: MapBase, exitance_radiance: MapBase, environment: MapBase):
+        super().__init__(collision_sampler=collision_sampler, exitance_radiance=exitance_radiance,
+                         environment=environment)
+
+    def _sigma_grid3d(self) -> Grid3D:
+        return self.collision_sampler.sigma
+
+
+class GridDDACollisionIntegrator(_CollisionIntegrator):
+    """GridDDACollisionIntegrator (_maps.py:2811-2852, include/vr_collision_integrator_DDA.h):
+    emission-absorption along the grid's DDA walk, one random point per cell."""
+    FW, BW = 3, 7
+
+    def __init__(self, sigma_grid: Grid3D, exitance_radiance: MapBase, environment: MapBase, boundary: MapBase):
+        super().__init__(sigma_grid=sigma_grid, exitance_radiance=exitance_radiance, environment=environment,
+                         boundary=boundary)
+        self.grid = sigma_grid.grid
+        self.box_min = sigma_grid.bmin.clone()
+        self.box_max = sigma_grid.bmax.clone()
+
+    def _sigma_grid3d(self) -> Grid3D:
+        return self.sigma_grid
+
+    def update_grid(self, grid: typing.Optional[Grid3D] = None):
+        if grid is not None:
+            self.sigma_grid = grid
+        self.grid = self.sigma_grid.grid
+        self.box_min = self.sigma_grid.bmin.clone()
+        self.box_max = self.sigma_grid.bmax.clone()
+
+
 # ------------------------------------------------------------------ sensors --
 class _CaptureFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, sigma_grid, albedo_grid, camera, field, desc, fw_samples, bw_samples, seed, sensors):
+    def forward(ctx, sigma_grid, albedo_grid, emission_grid, camera, field, desc, fw_samples, bw_samples, seed,
+                sensors):
         ffi, lib = _lib.ffi_lib()
         dev = sigma_grid.device
         if sensors is None:
@@ -671,17 +853,19 @@ class _CaptureFn(torch.autograd.Function):
             raise NotImplementedError(f"{type(ctx.field).__name__} has no adjoint here yet")
         gs = torch.zeros_like(desc.sigma) if ctx.needs_input_grad[0] else None
         ga = torch.zeros_like(desc.albedo_grid) if (ctx.needs_input_grad[1] and desc.albedo_grid is not None) else None
-        if gs is not None or ga is not None:
+        ge = (torch.zeros_like(desc.emission_grid)
+              if (ctx.needs_input_grad[2] and desc.emission_grid is not None) else None)
+        if gs is not None or ga is not None or ge is not None:
             ffi, lib = _lib.ffi_lib()
             dev = desc.sigma.device
-            m = desc.to_struct(sigma_grad=gs, albedo_grad=ga)
+            m = desc.to_struct(sigma_grad=gs, albedo_grad=ga, emission_grad=ge)
             cam, keep = ctx.camera.to_struct(dev, ctx.sensors)
             d = dI.contiguous().float()
             vctx = _lib.context(dev)
             _lib.check(lib.vrt_capture_bw(vctx.ptr, m, ctx.field.BW, cam, ctx.bw_samples, ctx.seed, _lib.fptr(d),
                                           _lib.stream_handle(dev)), "vrt_capture_bw")
             _after_call(dev)
-        return gs, ga, None, None, None, None, None, None, None
+        return gs, ga, ge, None, None, None, None, None, None, None
 
 
 class PerspectiveCameraSensor(MapBase):
@@ -753,12 +937,12 @@ class PerspectiveCameraSensor(MapBase):
         if debug_out is not None:
             raise NotImplementedError("debug_out counters are reported by rendervous_b200.check() instead")
         if not isinstance(field, _PathIntegrator):
-            raise NotImplementedError("capture supports path-integrator fields")
+            raise NotImplementedError("capture supports path-integrator and collision-integrator fields")
         field = field.cast(input_dim=6)
         desc = field.lower()
-        sg, ag = field.grid_tensors()
+        sg, ag, eg = field.grid_tensors()
         sensors = None if sensors_batch is None else self._checked_sensors(sensors_batch, sg.device)
-        return _CaptureFn.apply(sg, ag, self, field, desc, int(fw_samples), int(bw_samples),
+        return _CaptureFn.apply(sg, ag, eg, self, field, desc, int(fw_samples), int(bw_samples),
                                 next_seed() if seed is None else int(seed), sensors)
 
 

@@ -12,7 +12,8 @@ from rendervous_b200.lowering import MediumDesc
 
 def oracle_desc(sigma: np.ndarray, *, albedo=0.9, albedo_grid: np.ndarray | None = None, emission=0.0, env=1.0,
                 sun_dir=None, sun_radiance=3.0, phase_mode=0, g=0.0, majorant="global", brick=8, tr="rt",
-                max_bounces=0, ds_epsilon=0.1, ds_compat=0, box=None) -> dict:
+                max_bounces=0, ds_epsilon=0.1, ds_compat=0, box=None, exitance_mode=0,
+                emission_grid: np.ndarray | None = None) -> dict:
     """A medium description for the oracle built directly from numpy arrays."""
     import oracle
     sigma = np.ascontiguousarray(sigma, np.float32)
@@ -44,6 +45,9 @@ def oracle_desc(sigma: np.ndarray, *, albedo=0.9, albedo_grid: np.ndarray | None
     desc.max_bounces = max_bounces
     desc.ds_epsilon = ds_epsilon
     desc.ds_compat = ds_compat
+    desc.exitance_mode = exitance_mode
+    if emission_grid is not None:
+        desc.emission_grid = torch.from_numpy(np.ascontiguousarray(emission_grid, np.float32))
     return desc.to_numpy()
 
 

@@ -144,3 +144,36 @@ def test_cpu_tensors_never_reach_the_kernels():
     d = lower_integrator(build_field(sig))
     with pytest.raises(ValueError):
         d.to_struct()
+
+
+def test_lowering_of_collision_integrators():
+    """MCCollisionIntegrator / GridDDACollisionIntegrator graphs as the
+    reference's builders assemble them (_objects.py:243-307) lower to the
+    exitance forms the kernels run; other radiance maps are refused."""
+    from rendervous_b200.lowering import lower_collision_integrator
+    sig = torch.rand(9, 9, 9, 1)
+    bmin, bmax = maps.normalized_box(sig)
+    g = maps.Grid3D(sig, bmin, bmax)
+    boundary = maps.ray_box_intersection[bmin, bmax]
+    maj = maps.const[[1.0, 1e6]]
+    env = maps.const[0.5, 0.6, 0.7]
+    alb = maps.Grid3D(torch.rand(9, 9, 9, 3), bmin, bmax)
+    tr = maps.RatiotrackingTransmittance(g, boundary, maj)
+    ps = maps.VHGPhaseSampler(maps.const[0.3])
+    scat = maps.MCScatteredEmittedRadiance(alb, maps.const[1.0, 2.0, 3.0], ps, tr * env.after(maps.ray_direction))
+    mc = maps.MCCollisionIntegrator(maps.DeltatrackingCollisionSampler(g, boundary, maj, 0.2), scat, env)
+    d = lower_collision_integrator(mc)
+    assert d.exitance_mode == 2 and d.albedo_grid is alb.grid and d.emission == (1.0, 2.0, 3.0)
+    assert d.phase_mode == 1 and abs(d.phase_g - 0.3) < 1e-7 and abs(d.ds_epsilon - 0.2) < 1e-7
+    assert d.transmittance_mode == 0 and np.allclose(d.env, (0.5, 0.6, 0.7))
+    em = maps.Grid3D(torch.rand(9, 9, 9, 3), bmin, bmax)
+    dda = maps.GridDDACollisionIntegrator(g, em, env, boundary)
+    d2 = lower_collision_integrator(dda)
+    assert d2.exitance_mode == 0 and d2.emission_grid is em.grid
+    with pytest.raises(NotImplementedError):   # a radiance map that is not transmittance * environment
+        lower_collision_integrator(maps.GridDDACollisionIntegrator(
+            g, maps.MCScatteredRadiance(alb, ps, env.after(maps.ray_direction)), env, boundary))
+    with pytest.raises(NotImplementedError):   # environments must agree
+        lower_collision_integrator(maps.GridDDACollisionIntegrator(
+            g, maps.MCScatteredRadiance(alb, ps, tr * maps.const[1.0, 1.0, 1.0].after(maps.ray_direction)), env,
+            boundary))
