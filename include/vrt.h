@@ -108,6 +108,18 @@ typedef struct vrt_medium {
     int32_t exitance_mode;
     int32_t emission_is_grid;        /* 0: emission[3] constant; 1: emission_grid (Grid3D, C 1 or 3, sigma's box) */
     vrt_grid emission_grid;
+    /* environment (_objects.py:165-199): 0 the constant env[3]; 1 an equirectangular
+       image env_image [env_hw[0], env_hw[1], 3] (Image2D(img).after(xr_projection)),
+       not differentiated.  NEE directions: env_sampler 0 uniform sphere
+       (UniformDirectionSampler), 1 the image's probability quadtree
+       (XRQuadtreeRandomDirection; env_quadtree holds 4 + 16 + ... + 4^env_levels
+       node probabilities, children of node k at 4k+1..4k+4 in Morton order). */
+    int32_t env_mode;
+    const float* env_image;
+    int32_t env_hw[2];
+    int32_t env_sampler;
+    const float* env_quadtree;
+    int32_t env_levels;
 } vrt_medium;
 
 /* PerspectiveCameraSensor (rendervous _maps.py:1765-1802).  sensors == NULL:

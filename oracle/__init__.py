@@ -108,6 +108,18 @@ class OracleScene:
         s.ds_epsilon = float(desc["ds_epsilon"])
         s.ds_compat = int(desc["ds_compat"])
         s.exitance_mode = int(desc.get("exitance_mode", 0))
+        img = desc.get("env_image")
+        if img is not None:
+            self.env_image = np.ascontiguousarray(img, dtype=np.float32)
+            s.env_mode = 1
+            s.env_image = ptr(ffi, self.env_image)
+            s.env_hw[0], s.env_hw[1] = int(self.env_image.shape[0]), int(self.env_image.shape[1])
+        qt = desc.get("env_quadtree")
+        if qt is not None:
+            self.env_quadtree = np.ascontiguousarray(qt, dtype=np.float32).reshape(-1)
+            s.env_sampler = 1
+            s.env_quadtree = ptr(ffi, self.env_quadtree)
+            s.env_levels = int(desc["env_levels"])
         em = desc.get("emission_grid")
         self.emission_grad = None
         if em is not None:

@@ -65,6 +65,12 @@ typedef struct orc_scene {
     int32_t exitance_mode;        /* collision integrators: 0 emission, 1 scattered, 2 scattered + emitted */
     int32_t emission_is_grid;     /* emission: 0 const emission[3], 1 emission_grid (C 1 or 3, sigma's box) */
     orc_grid emission_grid;
+    int32_t env_mode;             /* 0 constant env[3], 1 equirectangular image env_image [H, W, 3] */
+    const float* env_image;
+    int32_t env_hw[2];
+    int32_t env_sampler;          /* NEE directions: 0 uniform sphere, 1 the image's quadtree */
+    const float* env_quadtree;    /* 4 + 16 + ... + 4^env_levels node probabilities */
+    int32_t env_levels;
 } orc_scene;
 
 typedef struct orc_camera {

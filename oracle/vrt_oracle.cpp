@@ -326,7 +326,30 @@ template <typename T> struct Scene {
         if (s.emission_grid.C == 1) { T g = dL.x + dL.y + dL.z; grid_bw(s.emission_grid, x, &g); }
         else { T g[3] = {dL.x, dL.y, dL.z}; grid_bw(s.emission_grid, x, g); }
     }
-    V3<T> environment() const { return V3<T>::load(s.env); }
+    // the environment radiance towards w: const env, or Image2D(image).after(xr_projection)
+    // (_objects.py:165-172; include/maps/image2d.h:1-26 with the default box [-1, 1]^2;
+    // include/maths.h:172-178 dir2xr)
+    V3<T> environment(V3<T> w) const {
+        if (s.env_mode == 0) return V3<T>::load(s.env);
+        if (w.x == T(0) && w.z == T(0)) w.x += T(0.0000001);
+        const T cx = std::atan2(w.x, w.z) * (T(1) / K<T>::pi);
+        const T cy = T(-2) * std::asin(std::min(std::max(w.y, T(-1)), T(1))) * (T(1) / K<T>::pi);
+        const T nx = std::min(std::max((cx - T(-1)) * T(0.5), T(0)), T(1));
+        const T ny = std::min(std::max((cy - T(-1)) * T(0.5), T(0)), T(1));
+        const int H = s.env_hw[0], W = s.env_hw[1];
+        const T gx = nx * T(W) - T(0.5), gy = ny * T(H) - T(0.5);
+        const T fx = std::floor(gx), fy = std::floor(gy);
+        const int px = (int)fx, py = (int)fy;
+        const T ax = gx - fx, ay = gy - fy;
+        const int x0 = std::min(std::max(px, 0), W - 1), x1 = std::min(std::max(px + 1, 0), W - 1);
+        const int y0 = std::min(std::max(py, 0), H - 1), y1 = std::min(std::max(py + 1, 0), H - 1);
+        const float* r0 = s.env_image + 3 * ((int64_t)y0 * W);
+        const float* r1 = s.env_image + 3 * ((int64_t)y1 * W);
+        V3<T> o;
+        for (int c = 0; c < 3; ++c)
+            o[c] = mix(mix((T)r0[3 * x0 + c], (T)r0[3 * x1 + c], ax), mix((T)r1[3 * x0 + c], (T)r1[3 * x1 + c], ax), ay);
+        return o;
+    }
 
     // include/vr_majorant.h:1-7.  Mode 0: const[[max sigma, 1e6]] (_objects.py:96-101).
     // Mode 1 (extension): majorant grid of bricks; returns the brick's bound and
@@ -835,10 +858,45 @@ template <typename T> T phase_sampler(const Scene<T>& S, Rng& rng, V3<T> w, V3<T
 }
 // include/vr_environment_sampler.h over _functionsampler(UniformDirectionSampler, const env)
 // (_maps.py:2552-2585, include/maps/uniform_direction_sampler.h:1-5)
+// or over XRQuadtreeRandomDirection (_maps.py:2494-2549): a pixel drawn down
+// the probability quadtree with one uniform, then a direction uniform in its
+// solid angle (include/randoms.h:186-199 randomDirection); weight = pixel
+// solid angle / p.
 template <typename T> V3<T> environment_sampler(const Scene<T>& S, Rng& rng, V3<T>& wo) {
-    wo = random_direction(rng, V3<T>(T(0), T(1), T(0)));
-    T weight = T(4) * K<T>::pi;
-    return S.environment() * weight;
+    if (S.s.env_sampler == 0) {
+        wo = random_direction(rng, V3<T>(T(0), T(1), T(0)));
+        T weight = T(4) * K<T>::pi;
+        return S.environment(wo) * weight;
+    }
+    float sel = rng.uniform();
+    int64_t node = 0;
+    float p0x = 0.0f, p0y = 0.0f, p1x = 1.0f, p1y = 1.0f, prob = 1.0f;
+    for (int i = 0; i < S.s.env_levels; ++i) {
+        const float* d = S.s.env_quadtree + node * 4;
+        int child = 3;
+        prob = d[3];
+        for (int c = 0; c < 3; ++c) {
+            if (sel < d[c]) {
+                child = c;
+                prob = d[c];
+                break;
+            }
+            sel -= d[c];
+        }
+        const float xmed = (p1x + p0x) / 2.0f, ymed = (p1y + p0y) / 2.0f;
+        if (child % 2 == 0) p1x = xmed; else p0x = xmed;
+        if (child / 2 == 0) p1y = ymed; else p0y = ymed;
+        node = node * 4 + 1 + child;
+    }
+    const T pi = K<T>::pi;
+    const T pixel_area = T(2) * pi * (std::cos((T)p0y * pi) - std::cos((T)p1y * pi)) / T(1 << S.s.env_levels);
+    const T weight = pixel_area / std::max(T(0.000000001), (T)prob);
+    const T a0 = ((T)p0x * T(2) - T(1)) * pi, a1 = ((T)p1x * T(2) - T(1)) * pi, b0 = (T)p0y * pi, b1 = (T)p1y * pi;
+    const T r1 = (T)rng.uniform() * (a1 - a0) + a0;
+    const T r2 = std::cos(b0) - (T)rng.uniform() * (std::cos(b0) - std::cos(b1));
+    const T sq = std::sqrt(std::max(T(0), T(1) - r2 * r2));
+    wo = V3<T>(std::sin(r1) * sq, r2, std::cos(r1) * sq);
+    return S.environment(wo) * weight;
 }
 
 // ---------------------------------------------------------------------------
@@ -867,7 +925,7 @@ V3<T> path_integrator_NEE(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, bool on
     x += w * tMin;
     T d = tMax - tMin;
     V3<T> R(T(0)), W(T(1));
-    if (!only_scatters) R += transmittance(S, rng, x, w, &cnt.steps) * S.environment();
+    if (!only_scatters) R += transmittance(S, rng, x, w, &cnt.steps) * S.environment(w);
     const T EPS = T(0.00001);
     int bounces = 0;
     const V3<T> sun_dir = V3<T>::load(S.s.sun_dir), sun_L = V3<T>::load(S.s.sun_radiance);
@@ -954,7 +1012,7 @@ template <typename T> V3<T> path_integrator_DT(const Scene<T>& S, Rng& rng, V3<T
         S.boundary(x, w, tMin, d);
         ff.bk.reset();
     }
-    return W * S.environment() + R;
+    return W * S.environment(w) + R;
 }
 
 // include/vr_path_integrator_DT.h:59-235 path_integrator_DT_bw
@@ -996,7 +1054,7 @@ template <typename T> void path_integrator_DT_bw(const Scene<T>& S, Rng& rng, V3
         S.boundary(x, w, tMin, d);
         ff.bk.reset();
     }
-    V3<T> env = S.environment();
+    V3<T> env = S.environment(w);
     V3<T> dL_dW = dL_dR * env;
     rng = before_path;
     x = ini_x;
@@ -1103,7 +1161,7 @@ template <typename T> void path_integrator_NEE_DS_bw(const Scene<T>& S, Rng& rng
         S.boundary(x, w, tMin, d);
         ff.bk.reset();
     }
-    if (!scattered) R += S.environment() * W;
+    if (!scattered) R += S.environment(w) * W;
 
     rng = before_path;
     x = ini_x;
@@ -1219,7 +1277,7 @@ template <typename T> void path_integrator_NEE_DRT_bw(const Scene<T>& S, Rng& rn
     sec.ntr = 0;
     Counters dummy;
     T direct_T = transmittance(S, rng, x, w, nullptr);
-    V3<T> direct_env = S.environment();
+    V3<T> direct_env = S.environment(w);
     T dL_ddT = dot(dL_dR, direct_env);
     transmittance_bw(S, sec, x, w, dL_ddT);
     V3<T> R(T(0)), W(T(1));
@@ -1387,7 +1445,7 @@ template <typename T> void path_integrator_NEE_DRTQ_bw(const Scene<T>& S, Rng& r
     sec.n = 0;
     sec.ntr = 0;
     (void)transmittance(S, rng, x, w, nullptr);
-    transmittance_bw(S, sec, x, w, dot(dL_dR, S.environment()));
+    transmittance_bw(S, sec, x, w, dot(dL_dR, S.environment(w)));
     V3<T> R(T(0)), W(T(1));
     const V3<T> ini_x = x, ini_w = w;
     const T ini_d = d;
@@ -1516,7 +1574,7 @@ void path_integrator_NEE_DRTDS_bw(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w,
     sec.n = 0;
     sec.ntr = 0;
     (void)transmittance(S, rng, x, w, nullptr);
-    transmittance_bw(S, sec, x, w, dot(dL_dR, S.environment()));
+    transmittance_bw(S, sec, x, w, dot(dL_dR, S.environment(w)));
     V3<T> R(T(0)), W(T(1));
     V3<T> res_x = x, res_w = w, res_W = W;
     T res_P = 3, total_weight = 3;
@@ -1698,7 +1756,7 @@ template <typename T> void path_integrator_NEE_SPS_bw(const Scene<T>& S, Rng& rn
     sec.n = 0;
     sec.ntr = 0;
     (void)transmittance(S, rng, x, w, nullptr);
-    transmittance_bw(S, sec, x, w, dot(dL_dR, S.environment()));
+    transmittance_bw(S, sec, x, w, dot(dL_dR, S.environment(w)));
     const V3<T> sun_dir = V3<T>::load(S.s.sun_dir), sun_L = V3<T>::load(S.s.sun_radiance);
     V3<T> R(T(0)), Rf(T(0)), W(T(1));
     T W_singular = 1;
@@ -1937,7 +1995,7 @@ template <typename T> V3<T> exitance(const Scene<T>& S, Rng& rng, V3<T> x, V3<T>
     V3<T> wo;
     const T rho = phase_sampler(S, rng, -wout, wo);
     const V3<T> sa = S.albedo(x);
-    const V3<T> rad = S.environment() * transmittance(S, rng, x, wo, (int64_t*)nullptr);
+    const V3<T> rad = S.environment(wo) * transmittance(S, rng, x, wo, (int64_t*)nullptr);
     V3<T> R = sa * rho * rad;
     if (mode == 2) R += (V3<T>(T(1)) - sa) * S.emission_at(x);
     return R;
@@ -1954,7 +2012,7 @@ template <typename T> void exitance_bw(const Scene<T>& S, Rng& rng, V3<T> x, V3<
     const V3<T> sa = S.albedo(x);
     Rng tr_rng = rng;
     const T Tr = transmittance(S, rng, x, wo, (int64_t*)nullptr);
-    const V3<T> env = S.environment();
+    const V3<T> env = S.environment(wo);
     const V3<T> rad = env * Tr;
     V3<T> dL_dsa = dL * rad * rho;
     const V3<T> dL_drad = dL * sa * rho;
@@ -1981,7 +2039,7 @@ template <typename T> V3<T> collision_integrator_MC(const Scene<T>& S, Rng& rng,
     const V3<T> xt = w * t + x;
     Rng xr = rng.with_stream(exitance_stream(0));
     const V3<T> eR = C != T(0) ? exitance(S, xr, xt, -w) : V3<T>(T(0));
-    return eR * C + S.environment() * Tt;
+    return eR * C + S.environment(w) * Tt;
 }
 // include/maps/collision_integrator_mc.h:20-41 (BACKWARD): the forward's
 // collision (same stream), the sampler's adjoint on its own stream, the
@@ -1993,7 +2051,7 @@ template <typename T> void collision_integrator_MC_bw(const Scene<T>& S, Rng& rn
     const V3<T> xt = w * t + x;
     Rng xr = rng.with_stream(exitance_stream(0));
     const V3<T> eR = C != T(0) ? exitance(S, xr, xt, -w) : V3<T>(T(0));
-    const V3<T> env = S.environment();
+    const V3<T> env = S.environment(w);
     Rng cb = rng.with_stream(4);
     collision_sampler_DT_bw(S, cb, x, w, (T)S.s.ds_epsilon, dot(dL, eR), dot(dL, env));
     if (C != T(0)) {
@@ -2006,7 +2064,7 @@ template <typename T> void collision_integrator_MC_bw(const Scene<T>& S, Rng& rn
 // one random point per cell (the path stream): per cell the homogeneous
 // transmittance exp(-dt sigma(point)) and the exitance at the point.
 template <typename T> V3<T> collision_integrator_DDA(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, Counters& c) {
-    const V3<T> env = S.environment();
+    const V3<T> env = S.environment(w);
     DDA<T> dda(S, x, w);
     if (!dda.valid) return env;
     T Tr = T(1), ct = T(0);
@@ -2055,7 +2113,7 @@ template <typename T> void collision_integrator_DDA_bw(const Scene<T>& S, Rng& r
         dda.step();
         ++k;
     }
-    const V3<T> env = S.environment();
+    const V3<T> env = S.environment(w);
     const T fw_T = Tr;
     rng = before;
     dda.reset_march();

@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(256, 2) k_nee_ds_bw(DMedium M, PathSrc S, uint
                     ev = begin_segment(M, L, S_TRFW, tl, &sc->status);
                 } else if (ev == E_END && !L.replay) {
                     // end of the primal pass (_NEE_DS.h:106-121): restart for the replay
-                    if (!L.scattered) L.R = L.R + M.env * L.W;
+                    if (!L.scattered) L.R = L.R + env_radiance(M, L.w) * L.W;
                     L.replay = true;
                     L.ff = Flight();
                     L.rng.seek(L.pos0);

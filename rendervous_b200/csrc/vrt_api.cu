@@ -264,6 +264,16 @@ static int to_dmedium(const vrt_medium* m, DMedium& M) {
     if (m->transmittance_mode < 0 || m->transmittance_mode > 5) return VRT_E_INVALID_ARGUMENT;
     if (m->max_bounces < 0) return VRT_E_INVALID_ARGUMENT;
     if (m->exitance_mode < 0 || m->exitance_mode > 2) return VRT_E_INVALID_ARGUMENT;
+    if (m->env_mode < 0 || m->env_mode > 1 || m->env_sampler < 0 || m->env_sampler > 1) return VRT_E_INVALID_ARGUMENT;
+    if (m->env_mode == 1) {
+        if (!m->env_image) return VRT_E_NULL_POINTER;
+        if (m->env_hw[0] < 1 || m->env_hw[1] < 1 || (int64_t)m->env_hw[0] * m->env_hw[1] * 3 >= (int64_t)INT32_MAX)
+            return VRT_E_BAD_SHAPE;
+    }
+    if (m->env_sampler == 1) {
+        if (!m->env_quadtree) return VRT_E_NULL_POINTER;
+        if (m->env_levels < 1 || m->env_levels > 14) return VRT_E_BAD_SHAPE;
+    }
     if (m->emission_is_grid) {
         st = to_dgrid(m->emission_grid, 0, M.emission_grid);
         if (st) return st;
@@ -293,6 +303,13 @@ static int to_dmedium(const vrt_medium* m, DMedium& M) {
     M.ds_compat = m->ds_compat;
     M.exitance_mode = m->exitance_mode;
     M.emission_is_grid = m->emission_is_grid ? 1 : 0;
+    M.env_mode = m->env_mode;
+    M.env_img = m->env_image;
+    M.env_h = m->env_hw[0];
+    M.env_w = m->env_hw[1];
+    M.env_sampler = m->env_sampler;
+    M.env_qt = m->env_quadtree;
+    M.env_levels = m->env_levels;
     return VRT_OK;
 }
 

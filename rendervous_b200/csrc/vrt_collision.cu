@@ -159,7 +159,7 @@ __device__ float3 exitance(const DMedium& M, Rng& rng, float3 x, float3 wout, Ta
     if (M.exitance_mode == 0) return emission_at(M, x);
     const float3 wo = phase_sample(M, rng, -wout);
     const float3 sa = albedo(M, x, tl);
-    const float3 rad = M.env * transmittance(M, rng, x, wo, tl, status);
+    const float3 rad = env_radiance(M, wo) * transmittance(M, rng, x, wo, tl, status);
     float3 R = sa * 1.0f * rad;
     if (M.exitance_mode == 2) R = R + (f3(1.0f) - sa) * emission_at(M, x);
     return R;
@@ -178,7 +178,7 @@ __device__ void exitance_bw(const DMedium& M, Rng& rng, float3 x, float3 wout, f
     const float3 sa = albedo(M, x, tl);
     Rng tr_rng = rng;
     const float Tr = transmittance(M, rng, x, wo, tl, status);
-    const float3 env = M.env;
+    const float3 env = env_radiance(M, wo);
     const float3 rad = env * Tr;
     float3 dL_dsa = dL * rad * 1.0f;
     const float3 dL_drad = dL * sa * 1.0f;
@@ -203,7 +203,7 @@ __device__ float3 collision_integrate_mc(const DMedium& M, const Rng& rng, float
         Rng xr = with_stream(rng, exitance_stream(0));
         eR = exitance(M, xr, w * t + x, -w, tl, status);
     }
-    return eR * C + M.env * Tt;
+    return eR * C + env_radiance(M, w) * Tt;
 }
 // include/maps/collision_integrator_mc.h:20-41: the forward's collision (same
 // stream), the sampler's adjoint on its own stream, the exitance's adjoint on
@@ -220,7 +220,7 @@ __device__ void collision_integrate_mc_bw(const DMedium& M, const Rng& rng, floa
         eR = exitance(M, xr, xt, -w, tl, status);
     }
     Rng cb = with_stream(rng, 4);
-    collision_sample_dt_bw(M, cb, x, w, M.ds_eps, dot(dL, eR), dot(dL, M.env), tl, status);
+    collision_sample_dt_bw(M, cb, x, w, M.ds_eps, dot(dL, eR), dot(dL, env_radiance(M, w)), tl, status);
     if (C != 0.0f) {
         Rng xb = with_stream(rng, exitance_stream(0));
         exitance_bw(M, xb, xt, -w, dL * C, tl, status);
@@ -233,7 +233,7 @@ __device__ void collision_integrate_mc_bw(const DMedium& M, const Rng& rng, floa
 __device__ float3 collision_integrate_dda(const DMedium& M, Rng& rng, float3 x, float3 w, Tally& tl,
                                           uint32_t* status) {
     DDA q;
-    if (!q.init(M, x, w)) return M.env;
+    if (!q.init(M, x, w)) return env_radiance(M, w);
     q.load_all(M.sigma);
     float Tr = 1.0f, ct = 0.0f;
     float3 R = f3(0.0f);
@@ -258,7 +258,7 @@ __device__ float3 collision_integrate_dda(const DMedium& M, Rng& rng, float3 x, 
         q.shift_load(M.sigma, axis);
         ++k;
     }
-    return R + M.env * Tr;
+    return R + env_radiance(M, w) * Tr;
 }
 // include/vr_collision_integrator_DDA.h:85-207: the walk again for fw_T and
 // the emitted part, then a replay from the same cell draws scattering
@@ -291,7 +291,7 @@ __device__ void collision_integrate_dda_bw(const DMedium& M, Rng& rng, float3 x,
         q.shift_load(M.sigma, axis);
         ++k;
     }
-    const float3 env = M.env;
+    const float3 env = env_radiance(M, w);
     const float fw_T = Tr;
     rng = before;
     q.reset(M);

@@ -409,11 +409,83 @@ __device__ __forceinline__ float3 phase_sample(const DMedium& M, Rng& rng, float
     }
     return hg_phase_sample(rng, w, g);
 }
-// include/vr_environment_sampler.h over _functionsampler(UniformDirectionSampler, const)
-// (_maps.py:2552-2585, include/maps/uniform_direction_sampler.h:1-5): E * 4pi
+// ------------------------------------------------------------ environment --
+// include/maths.h:172-178 dir2xr: equirectangular coordinates in [-1, 1]^2.
+__device__ __forceinline__ float2 dir2xr(float3 w) {
+    if (w.x == 0.0f && w.z == 0.0f) w.x += 0.0000001f;
+    const float x = atan2f(w.x, w.z) * (1.0f / kPi);
+    const float y = -2.0f * asinf(fminf(fmaxf(w.y, -1.0f), 1.0f)) * (1.0f / kPi);
+    return make_float2(x, y);
+}
+// The environment radiance towards w: the constant env, or
+// Image2D(env image).after(xr_projection) (_objects.py:165-172,
+// include/maps/image2d.h:1-26 with its default box [-1, 1]^2: clamped
+// coordinates, bilinear over pixel centres, clamped pixel indices).
+__device__ __forceinline__ float3 env_radiance(const DMedium& M, float3 w) {
+    if (M.env_mode == 0) return M.env;
+    const float2 c = dir2xr(w);
+    const float nx = fminf(fmaxf((c.x - (-1.0f)) * 0.5f, 0.0f), 1.0f);
+    const float ny = fminf(fmaxf((c.y - (-1.0f)) * 0.5f, 0.0f), 1.0f);
+    const float gx = nx * (float)M.env_w - 0.5f, gy = ny * (float)M.env_h - 0.5f;
+    const float fx = floorf(gx), fy = floorf(gy);
+    const int px = (int)fx, py = (int)fy;
+    const float ax = gx - fx, ay = gy - fy;
+    const int x0 = min(max(px, 0), M.env_w - 1), x1 = min(max(px + 1, 0), M.env_w - 1);
+    const int y0 = min(max(py, 0), M.env_h - 1), y1 = min(max(py + 1, 0), M.env_h - 1);
+    const float* r0 = M.env_img + 3 * (y0 * M.env_w);
+    const float* r1 = M.env_img + 3 * (y1 * M.env_w);
+    float3 o;
+    o.x = mixf(mixf(ldg(r0 + 3 * x0), ldg(r0 + 3 * x1), ax), mixf(ldg(r1 + 3 * x0), ldg(r1 + 3 * x1), ax), ay);
+    o.y = mixf(mixf(ldg(r0 + 3 * x0 + 1), ldg(r0 + 3 * x1 + 1), ax), mixf(ldg(r1 + 3 * x0 + 1), ldg(r1 + 3 * x1 + 1), ax), ay);
+    o.z = mixf(mixf(ldg(r0 + 3 * x0 + 2), ldg(r0 + 3 * x1 + 2), ax), mixf(ldg(r1 + 3 * x0 + 2), ldg(r1 + 3 * x1 + 2), ax), ay);
+    return o;
+}
+// include/randoms.h:186-199 randomDirection(alpha0, alpha1, beta0, beta1):
+// azimuth uniform in [alpha0, alpha1], cos of the polar angle (about +y)
+// uniform between cos(beta0) and cos(beta1).
+__device__ __forceinline__ float3 random_direction_range(Rng& rng, float a0, float a1, float b0, float b1) {
+    const float r1 = rng.uniform() * (a1 - a0) + a0;
+    const float r2 = cosf(b0) - rng.uniform() * (cosf(b0) - cosf(b1));
+    const float s = sqrtf(gmax(0.0f, 1.0f - r2 * r2));
+    return make_float3(sinf(r1) * s, r2, cosf(r1) * s);
+}
+// include/vr_environment_sampler.h over _functionsampler(point sampler, environment)
+// (_maps.py:2552-2585): [E(w) * weight, w] with the point sampler
+//   UniformDirectionSampler (include/maps/uniform_direction_sampler.h:1-5): weight 4 pi, or
+//   XRQuadtreeRandomDirection (_maps.py:2494-2549): a pixel of the image drawn
+//   down the probability quadtree with one uniform (node k's children at
+//   4k + 1 .. 4k + 4, child c = 2 * (lower half) + (right half)), then a
+//   direction uniform in its solid angle; weight = pixel solid angle / p.
 __device__ __forceinline__ float3 environment_sample(const DMedium& M, Rng& rng, float3& wo) {
-    wo = random_direction_y(rng);
-    return M.env * (4.0f * kPi);
+    if (M.env_sampler == 0) {
+        wo = random_direction_y(rng);
+        return env_radiance(M, wo) * (4.0f * kPi);
+    }
+    float sel = rng.uniform();
+    int node = 0;
+    float p0x = 0.0f, p0y = 0.0f, p1x = 1.0f, p1y = 1.0f, prob = 1.0f;
+    for (int i = 0; i < M.env_levels; ++i) {
+        const float* d = M.env_qt + node * 4;
+        int child = 3;
+        prob = ldg(d + 3);
+        for (int c = 0; c < 3; ++c) {
+            const float dc = ldg(d + c);
+            if (sel < dc) {
+                child = c;
+                prob = dc;
+                break;
+            }
+            sel -= dc;
+        }
+        const float xmed = (p1x + p0x) / 2.0f, ymed = (p1y + p0y) / 2.0f;
+        if (child % 2 == 0) p1x = xmed; else p0x = xmed;
+        if (child / 2 == 0) p1y = ymed; else p0y = ymed;
+        node = node * 4 + 1 + child;
+    }
+    const float pixel_area = 2.0f * kPi * (cosf(p0y * kPi) - cosf(p1y * kPi)) / (float)(1 << M.env_levels);
+    const float weight = pixel_area / gmax(0.000000001f, prob);
+    wo = random_direction_range(rng, (p0x * 2.0f - 1.0f) * kPi, (p1x * 2.0f - 1.0f) * kPi, p0y * kPi, p1y * kPi);
+    return env_radiance(M, wo) * weight;
 }
 
 // ---------------------------------------------------------------- camera --

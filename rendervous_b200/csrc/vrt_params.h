@@ -39,6 +39,12 @@ struct DMedium {
     int exitance_mode;     // collision integrators: 0 emission, 1 scattered, 2 scattered + emitted
     int emission_is_grid;  // emission: 0 const, 1 emission_grid
     DGrid emission_grid;
+    int env_mode;          // environment: 0 the constant env, 1 an equirectangular (xr) image
+    const float* env_img;  // [env_h, env_w, 3], contiguous
+    int env_h, env_w;
+    int env_sampler;       // NEE direction sampling: 0 uniform sphere, 1 the image's quadtree
+    const float* env_qt;   // quadtree node probabilities (4 + 16 + ... + 4^levels floats)
+    int env_levels;
 };
 
 struct DCamera {

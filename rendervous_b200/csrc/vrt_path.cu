@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(256, 3) k_nee_fw(DMedium M, PathSrc S, uint64_
                     ++n_paths_done;
                     int ev = start_shadow(M, L, L.x, L.w, tl);
                     if (ev == EV_SHADOW_DONE) {
-                        L.R = L.R + L.T * M.env;
+                        L.R = L.R + L.T * env_radiance(M, L.w);
                         L.state = L.d > EPS ? ST_PRIMARY : ST_DEAD;
                         if (L.state == ST_DEAD) end_path<MODE>(S, L, out, scale, io);
                     }
@@ -355,7 +355,7 @@ __global__ void __launch_bounds__(256, 3) k_nee_fw(DMedium M, PathSrc S, uint64_
                 }
                 L.ff = Flight();
                 if (L.kind == SH_DIRECT) {  // vr_path_integrator_NEE.h:13-14
-                    L.R = L.R + L.T * M.env;
+                    L.R = L.R + L.T * env_radiance(M, L.w);
                     L.state = ST_PRIMARY;
                     ev = L.d > EPS ? EV_NONE : EV_ESCAPE;
                 } else if (L.kind == SH_ENV) {  // :51-52
@@ -394,7 +394,7 @@ __device__ float3 path_nee_seq(const DMedium& M, Rng& rng, float3 x, float3 w, b
     x = x + w * tMin;
     float d = tMax - tMin;
     float3 R = f3(0.0f), W = f3(1.0f);
-    if (!only_scatters) R = R + transmittance(M, rng, x, w, tl, status) * M.env;
+    if (!only_scatters) R = R + transmittance(M, rng, x, w, tl, status) * env_radiance(M, w);
     const float EPS = 0.00001f;
     int bounces = 0;
     for (Flight ff; d > EPS; ++ff.it) {
@@ -465,7 +465,7 @@ __device__ float3 path_dt_seq(const DMedium& M, Rng& rng, float3 x, float3 w, ui
         boundary(M, x, w, tMin, d);
         ff.bk.reset();
     }
-    return W * M.env + R;
+    return W * env_radiance(M, w) + R;
 }
 
 // vr_path_integrator_DT.h:59-235
@@ -509,7 +509,7 @@ __device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float
         boundary(M, x, w, tMin, d);
         ff.bk.reset();
     }
-    const float3 dL_dW = dL_dR * M.env;
+    const float3 dL_dW = dL_dR * env_radiance(M, w);
     rng.seek(before_path);
     x = ini_x;
     w = ini_w;
@@ -608,7 +608,7 @@ __device__ void path_nee_ds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, f
         boundary(M, x, w, tMin, d);
         ff.bk.reset();
     }
-    if (!scattered) R = R + M.env * W;
+    if (!scattered) R = R + env_radiance(M, w) * W;
 
     rng.seek(before_path);
     x = ini_x;
@@ -729,7 +729,7 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
     sec.ntr = 0;
     uint32_t verts = 0;
     (void)transmittance(M, rng, x, w, tl, status);
-    transmittance_bw(M, sec, x, w, dot(dL_dR, M.env), tl, status);
+    transmittance_bw(M, sec, x, w, dot(dL_dR, env_radiance(M, w)), tl, status);
     float3 R = f3(0.0f), W = f3(1.0f);
     float3 res_x = x, res_w = w, res_W = W;
     float res_P = 3.0f, total_weight = 3.0f;
@@ -885,7 +885,7 @@ __device__ void path_nee_drtq_bw(const DMedium& M, Rng& rng, float3 x, float3 w,
     if (d <= 0.0f) return;
     Rng sec = branch_stream(rng);
     (void)transmittance(M, rng, x, w, tl, status);
-    transmittance_bw(M, sec, x, w, dot(dL_dR, M.env), tl, status);
+    transmittance_bw(M, sec, x, w, dot(dL_dR, env_radiance(M, w)), tl, status);
     float3 R = f3(0.0f), W = f3(1.0f);
     const float3 ini_x = x, ini_w = w;
     const float ini_d = d;
@@ -1006,7 +1006,7 @@ __device__ void path_nee_drtds_bw(const DMedium& M, Rng& rng, float3 x, float3 w
     Rng sec = branch_stream(rng);
     uint32_t verts = 0;
     (void)transmittance(M, rng, x, w, tl, status);
-    transmittance_bw(M, sec, x, w, dot(dL_dR, M.env), tl, status);
+    transmittance_bw(M, sec, x, w, dot(dL_dR, env_radiance(M, w)), tl, status);
     float3 R = f3(0.0f), W = f3(1.0f);
     float3 res_x = x, res_w = w, res_W = W;
     float res_P = 3.0f, total_weight = 3.0f;
@@ -1177,7 +1177,7 @@ __device__ void path_nee_sps_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
     if (d <= 0.0f) return;
     Rng sec = branch_stream(rng);
     (void)transmittance(M, rng, x, w, tl, status);
-    transmittance_bw(M, sec, x, w, dot(dL_dR, M.env), tl, status);
+    transmittance_bw(M, sec, x, w, dot(dL_dR, env_radiance(M, w)), tl, status);
     float3 R = f3(0.0f), Rf = f3(0.0f), W = f3(1.0f);
     float W_singular = 1.0f;
     bool mis_allowed = true;

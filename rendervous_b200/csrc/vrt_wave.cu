@@ -113,13 +113,13 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                     }
                     const uint32_t f = rng.ntr++;
                     if (dslot != ~0ull) {
-                        put_job(wv.jobs, dslot, x, w, M.env, job_key(pid, f));
+                        put_job(wv.jobs, dslot, x, w, env_radiance(M, w), job_key(pid, f));
                         dslot = ~0ull;
                     } else {
                         njobs = 1;
                         jx = x;
                         jd = w;
-                        jw = M.env;
+                        jw = env_radiance(M, w);
                         jfork = f;
                     }
                     alive = d > EPS;

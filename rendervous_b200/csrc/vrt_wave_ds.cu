@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
             if (nj == 2) put_job(wv.jobs, j + 1, x, M.sun_dir, W * M.sun_L * ph_sun, job_key(pid, jfork + 1), tgt | 1u);
         }
         if (finish) {  // end of the primal (_NEE_DS.h:106-110): escape term, then the path's totals
-            if (!scattered) Racc = Racc + M.env * W;
+            if (!scattered) Racc = Racc + env_radiance(M, w) * W;
             const uint64_t k = pid - wv.p_begin;
             float* io = wv.info + 8 * k;
             __stcs(reinterpret_cast<float4*>(io), make_float4(Racc.x, Racc.y, Racc.z, Rspacc.x));

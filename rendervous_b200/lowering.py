@@ -57,6 +57,9 @@ class MediumDesc:
     ds_compat: int = 0
     exitance_mode: int = 0                   # collision integrators: 0 emission, 1 scattered, 2 scattered+emitted
     emission_grid: typing.Optional[torch.Tensor] = None  # [D,H,W,C], C 1 or 3, sigma's box
+    env_image: typing.Optional[torch.Tensor] = None      # [H,W,3] equirectangular environment (else env is constant)
+    env_quadtree: typing.Optional[torch.Tensor] = None   # NEE directions from the image's quadtree (else uniform)
+    env_levels: int = 0
 
     # -- derived quantities, computed in float32 exactly as the kernels read them
     def inv_bsize(self) -> np.ndarray:
@@ -90,7 +93,8 @@ class MediumDesc:
             maj_grid=f(self.maj_grid), maj_dims=self.maj_dims(), maj_scale=self.maj_scale(),
             transmittance_mode=self.transmittance_mode, max_bounces=self.max_bounces,
             ds_epsilon=self.ds_epsilon, ds_compat=self.ds_compat, exitance_mode=self.exitance_mode,
-            emission_grid=f(self.emission_grid))
+            emission_grid=f(self.emission_grid), env_image=f(self.env_image), env_quadtree=f(self.env_quadtree),
+            env_levels=self.env_levels)
 
     # -- the C struct (device pointers); keep the returned object alive during the call
     def to_struct(self, sigma_grad: torch.Tensor | None = None, albedo_grad: torch.Tensor | None = None,
@@ -131,6 +135,17 @@ class MediumDesc:
         m.ds_epsilon = float(self.ds_epsilon)
         m.ds_compat = int(self.ds_compat)
         m.exitance_mode = int(self.exitance_mode)
+        if self.env_image is not None:
+            img = self.env_image
+            if img.dim() != 3 or img.shape[-1] != 3 or not img.is_contiguous() or not img.is_cuda:
+                raise ValueError("the environment image must be a contiguous CUDA [H, W, 3] float32 tensor")
+            m.env_mode = 1
+            m.env_image = _lib.fptr(img)
+            m.env_hw[0], m.env_hw[1] = int(img.shape[0]), int(img.shape[1])
+        if self.env_quadtree is not None:
+            m.env_sampler = 1
+            m.env_quadtree = _lib.fptr(self.env_quadtree)
+            m.env_levels = int(self.env_levels)
         if self.emission_grid is not None:
             m.emission_is_grid = 1
             _fill_grid(m.emission_grid, self.emission_grid, emission_grad)
@@ -252,6 +267,58 @@ def lower_phase(phase, sampler, desc_kwargs: dict):
     desc_kwargs.update(phase_mode=mode, phase_g=g)
 
 
+def lower_environment(env, kw: dict):
+    """A constant environment, or Image2D(image).after(xr_projection) with the
+    image's default box (_objects.py:165-172)."""
+    from . import maps
+    if isinstance(env, maps.CompositionMap) and isinstance(env.map_a, maps.XRProjection) and \
+            isinstance(env.map_b, maps.Image2D):
+        img = env.map_b
+        if img.grid.shape[-1] != 3:
+            raise NotImplementedError("an environment image has 3 channels")
+        if not (torch.allclose(img.bmin.cpu(), torch.tensor([-1.0, -1.0])) and
+                torch.allclose(img.inv_bsize.cpu(), torch.tensor([0.5, 0.5]))):
+            raise NotImplementedError("an environment image keeps Image2D's default box [-1, 1]^2")
+        kw["env_image"] = img.grid.detach().contiguous()
+        kw["env"] = (0.0, 0.0, 0.0)
+        return
+    kw["env"] = _const_values(env, 3)
+
+
+def _same_environment(a, b) -> bool:
+    from . import maps
+    if a is b:
+        return True
+    if isinstance(a, maps.ConstantMap) and isinstance(b, maps.ConstantMap):
+        return _const_values(a, 3) == _const_values(b, 3)
+    if isinstance(a, maps.CompositionMap) and isinstance(b, maps.CompositionMap):
+        return a.map_b is b.map_b
+    return False
+
+
+def lower_environment_sampler(es, env, kw: dict):
+    """_functionsampler(UniformDirectionSampler | XRQuadtreeRandomDirection,
+    environment) (_objects.py:180-203) over the integrator's environment."""
+    from . import maps
+    if not isinstance(es, maps._functionsampler):
+        raise NotImplementedError("the environment sampler must be a _functionsampler")
+    if not _same_environment(es.function_map, env):
+        raise NotImplementedError("the environment sampler must sample the integrator's environment")
+    ps = es.point_sampler
+    if isinstance(ps, maps.UniformDirectionSampler):
+        return
+    if isinstance(ps, maps.XRQuadtreeRandomDirection):
+        if ps.levels < 1 or ps.levels > 14:
+            raise NotImplementedError("quadtree levels must be in 1..14")
+        qt = ps.densities() if callable(ps.densities) else ps.densities
+        if qt.numel() != sum(4 ** l for l in range(1, ps.levels + 1)):
+            raise NotImplementedError("quadtree size does not match its levels")
+        kw["env_quadtree"] = qt.detach().reshape(-1).contiguous().to(torch.float32)
+        kw["env_levels"] = ps.levels
+        return
+    raise NotImplementedError(f"environment direction sampler {type(ps).__name__} is not supported")
+
+
 def lower_integrator(pi) -> MediumDesc:
     """MediumDesc of a path-integrator map (DeltatrackingPathIntegrator, ...)."""
     from . import maps
@@ -267,13 +334,10 @@ def lower_integrator(pi) -> MediumDesc:
     else:
         kw["albedo_const"] = _const_values(alb, 3)
     kw["emission"] = _const_values(pi.emission, 3)
-    kw["env"] = _const_values(pi.environment, 3)
+    lower_environment(pi.environment, kw)
     es = getattr(pi, "environment_sampler", None)
     if es is not None:
-        if not (isinstance(es, maps._functionsampler) and isinstance(es.point_sampler, maps.UniformDirectionSampler)):
-            raise NotImplementedError("environment sampler must be _functionsampler(UniformDirectionSampler, const)")
-        if _const_values(es.function_map, 3) != kw["env"]:
-            raise NotImplementedError("environment sampler and environment must be the same constant")
+        lower_environment_sampler(es, pi.environment, kw)
     lower_phase(getattr(pi, "phase", None), pi.phase_sampler, kw)
     lower_boundary(pi.boundary, kw)
     lower_majorant(pi.majorant, pi.sigma, kw)
@@ -341,7 +405,7 @@ def _transmitted_environment(radiance):
         a, b = b, a
     if not (isinstance(b, maps.CompositionMap) and isinstance(b.map_a, maps.RayDirection)):
         raise NotImplementedError("the radiance of a scattered exitance must be transmittance * environment")
-    return a, _const_values(b.map_b, 3)
+    return a, b.map_b
 
 
 def lower_collision_integrator(ci) -> MediumDesc:
@@ -365,14 +429,14 @@ def lower_collision_integrator(ci) -> MediumDesc:
         sigma = ci.sigma_grid
         lower_sigma(sigma, kw)
         lower_boundary(ci.boundary, kw)
-    kw["env"] = _const_values(ci.environment, 3)
+    lower_environment(ci.environment, kw)
     ex = ci.exitance_radiance
     if isinstance(ex, (maps.MCScatteredRadiance, maps.MCScatteredEmittedRadiance)):
         kw["exitance_mode"] = 1 if isinstance(ex, maps.MCScatteredRadiance) else 2
         _lower_albedo(ex.scattering_albedo, sigma, kw)
         _lower_phase_sampler(ex.phase_sampler, kw)
         tr, env = _transmitted_environment(ex.radiance)
-        if env != kw["env"]:
+        if not _same_environment(env, ci.environment):
             raise NotImplementedError("the scattered radiance's environment must be the integrator's environment")
         lower_transmittance(tr, sigma, kw)
         tmaj = getattr(tr, "majorant", None)

@@ -344,6 +344,89 @@ class GridMaximumMajorant(ConstantMap):
         pass
 
 
+# ---------------------------------------------------- image environments --
+class Image2D(MapBase):
+    """Image2D (_maps.py:2288-2316, include/maps/image2d.h): bilinear lookup of an
+    [H, W, C] image over the box [bmin, bmax] (clamped to the border)."""
+
+    def __init__(self, grid: torch.Tensor, bmin=None, bmax=None):
+        assert len(grid.shape) == 3
+        super().__init__(2, grid.shape[-1])
+        self.grid = parameter(grid)
+        self.bmin = torch.tensor([-1.0, -1.0]) if bmin is None else torch.as_tensor(bmin, dtype=torch.float32)
+        bmax = torch.tensor([1.0, 1.0]) if bmax is None else torch.as_tensor(bmax, dtype=torch.float32)
+        self.inv_bsize = 1.0 / (bmax - self.bmin)
+
+
+class XRProjection(MapBase):
+    """XRProjection (_maps.py:2405-2425, include/maps/xr_projection.h): a direction
+    (or the direction of a ray) to equirectangular coordinates in [-1, 1]^2."""
+
+    def __init__(self, ray_input: bool = False):
+        super().__init__(6 if ray_input else 3, 2)
+        self.ray_input = ray_input
+
+
+xr_projection = XRProjection(False)
+
+
+class XRQuadtreeRandomDirection(MapBase):
+    """XRQuadtreeRandomDirection (_maps.py:2494-2549): [w, weight] with w drawn
+    from a probability quadtree over an equirectangular image (see
+    create_density_quadtree) and weight = pixel solid angle / probability."""
+
+    def __init__(self, input_dim: int, densities: torch.Tensor, levels: int):
+        super().__init__(input_dim, 4)
+        self.densities = densities
+        self.levels = int(levels)
+
+
+def create_density_quadtree(densities: torch.Tensor) -> torch.Tensor:
+    """_functions.py:509-530: the node probabilities of a square power-of-two
+    [R, R, 1] density image, coarsest level first (2x2, 4x4, ..., RxR), each
+    level in Morton order (x in the low bit), each node the sum of its four
+    children -- so node k's children sit at 4k+1 .. 4k+4 counted from the
+    start (the layout XRQuadtreeRandomDirection walks)."""
+    R = densities.shape[0]
+    assert densities.dim() == 3 and densities.shape[1] == R and densities.shape[2] == 1
+    assert R >= 2 and (R & (R - 1)) == 0, "resolution must be a power of two"
+    d = densities[..., 0].to(torch.float32)
+    levels = []
+    while d.shape[0] > 1:
+        levels.append(_morton_flatten(d))
+        d = d.reshape(d.shape[0] // 2, 2, d.shape[1] // 2, 2).sum(dim=(1, 3))
+    levels.reverse()
+    return torch.cat(levels).reshape(-1, 1)
+
+
+def _morton_flatten(img: torch.Tensor) -> torch.Tensor:
+    """img[y, x] in Morton order of (x, y) with x in the low bit."""
+    n = img.shape[0]
+    bits = n.bit_length() - 1
+    ys, xs = torch.meshgrid(torch.arange(n), torch.arange(n), indexing="ij")
+    code = torch.zeros_like(xs)
+    for b in range(bits):
+        code |= ((xs >> b) & 1) << (2 * b)
+        code |= ((ys >> b) & 1) << (2 * b + 1)
+    out = torch.empty(n * n, dtype=img.dtype, device=img.device)
+    out[code.reshape(-1).to(img.device)] = img.reshape(-1)
+    return out
+
+
+def environment_quadtree(env_image: torch.Tensor, levels: int = 10) -> torch.Tensor:
+    """The sampling quadtree of an equirectangular environment image
+    (_objects.py:180-193): luminance resampled to 2^levels square, each row
+    weighted by its solid angle, normalised, then create_density_quadtree."""
+    res = 1 << int(levels)
+    lum = env_image.detach().to(torch.float32).sum(-1)[None, None]
+    img = torch.nn.functional.interpolate(lum, size=(res, res), mode="bilinear", align_corners=False)[0, 0]
+    py = torch.arange(res, dtype=torch.float64, device=img.device)
+    wrow = (torch.cos(py * math.pi / res) - torch.cos((py + 1) * math.pi / res)).to(torch.float32)
+    img = img.clamp_min(0.0) * wrow[:, None]
+    img = img / img.sum().clamp_min(1e-8)
+    return create_density_quadtree(img[..., None])
+
+
 # ----------------------------------------------------- phase and sampling --
 class HGPhase(MapBase):
     """HGPhase (_maps.py:4436-4460): evaluates 0.8*HG(g) + 0.2*HG(g/5)."""

@@ -120,20 +120,44 @@ def medium_emission(ds):
 
 
 def medium_environment(ds):
+    """_objects.py:160-177: a constant, or an equirectangular image
+    Image2D(tensor).after(xr_projection)."""
     if not ds.ensures("environment", maps.MapBase):
         ds.assert_ensures("environment_tensor", torch.Tensor)
-        if len(ds.environment_tensor.shape) != 1:
-            raise NotImplementedError("image environments are not part of this path")
-        ds.add_parameters(environment=maps.const[ds.environment_tensor])
+        t = ds.environment_tensor
+        if len(t.shape) == 1:
+            ds.add_parameters(environment=maps.const[t])
+        else:
+            ds.add_parameters(environment=maps.Image2D(t).after(maps.xr_projection))
+
+
+def medium_environment_sampler_uniform(ds):
+    ds.requires(medium_environment)
+    ds.add_parameters(environment_sampler=maps._functionsampler(maps.UniformDirectionSampler(6), ds.environment))
+
+
+def medium_environment_sampler_quadtree(ds, *, levels: int = 10):
+    """_objects.py:180-199: NEE directions from the probability quadtree of an
+    image environment."""
+    ds.requires(medium_environment)
+    ds.assert_ensures("environment_tensor", torch.Tensor)
+    if len(ds.environment_tensor.shape) != 3:
+        raise NotImplementedError("a quadtree sampler needs an image environment")
+    qt = maps.environment_quadtree(ds.environment_tensor, levels=levels)
+    ds.add_parameters(environment_sampler_quadtree=qt)
+    sampler = maps.XRQuadtreeRandomDirection(6, qt, levels)
+    ds.add_parameters(environment_sampler=maps._functionsampler(sampler, ds.environment))
 
 
 def medium_environment_sampler(ds):
-    if not ds.ensures("environment_sampler", maps.MapBase):
-        ds.requires(medium_environment)
-        ds.add_parameters(environment_sampler=maps._functionsampler(maps.UniformDirectionSampler(6), ds.environment))
-
-
-medium_environment_sampler_uniform = medium_environment_sampler
+    """_objects.py:205-212: the quadtree sampler for image environments, else uniform."""
+    if ds.ensures("environment_sampler", maps.MapBase):
+        return
+    ds.requires(medium_environment)
+    if len(ds.environment_tensor.shape) == 3:
+        medium_environment_sampler_quadtree(ds)
+    else:
+        medium_environment_sampler_uniform(ds)
 
 
 def medium_phase_g(ds):
