@@ -145,8 +145,11 @@ __device__ __forceinline__ void path_resume(Lane& L) {
 
 }  // namespace
 
+// pids: when not null, work item q is path pids[q] (the paths the NEE_DS
+// wavefront handed over); else path q.
 __global__ void __launch_bounds__(256, 2) k_nee_ds_bw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
-                                                    const float* __restrict__ dL, float div, DScratch* sc) {
+                                                    const float* __restrict__ dL, float div, DScratch* sc,
+                                                    const unsigned long long* __restrict__ pids) {
     const unsigned lane = threadIdx.x & 31u;
     const float EPS = 0.00000001f;
     const float eps = M.ds_eps;
@@ -169,6 +172,7 @@ __global__ void __launch_bounds__(256, 2) k_nee_ds_bw(DMedium M, PathSrc S, uint
                 if (pid >= n_paths) {
                     exhausted = true;
                 } else {
+                    if (pids) pid = pids[pid];
                     L.rng.init(seed, pid, 0);
                     if (S.is_camera) {
                         long long p = (long long)(pid % (uint64_t)S.npix);
@@ -471,13 +475,13 @@ __global__ void __launch_bounds__(256, 2) k_nee_ds_bw(DMedium M, PathSrc S, uint
 }
 
 int launch_nee_ds_bw(const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed, const float* dL, float div,
-                     DScratch* scratch, int num_sms, cudaStream_t stream) {
+                     DScratch* scratch, int num_sms, cudaStream_t stream, const unsigned long long* pids) {
     cudaError_t e = cudaMemsetAsync(&scratch->next_path, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return launch_status(e);
     int blocks = persistent_blocks((const void*)k_nee_ds_bw, 256, num_sms);
     uint64_t need = (n_paths + 255) / 256;
     if ((uint64_t)blocks > need) blocks = (int)need;
-    k_nee_ds_bw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
+    k_nee_ds_bw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch, pids);
     count_launches(1);
     return launch_status(cudaGetLastError());
 }

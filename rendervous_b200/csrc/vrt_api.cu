@@ -79,15 +79,16 @@ KernelScope::~KernelScope() {
     t.pending.push_back({kid, e0, e1});
 }
 
-// The wavefront serves the NEE forward of capped paths (its job buffer is sized
-// from the bounce cap); uncapped paths run the persistent state machine.
+// The wavefront serves the NEE forward, capped or not (an uncapped path walks
+// at most kUncappedPass vertices per round and resumes in the next).
 static bool use_wave(const DMedium& M, int integrator) {
-    return integrator == VRT_PI_NEE && M.max_bounces > 0 && M.max_bounces <= 4096;
+    return integrator == VRT_PI_NEE && M.max_bounces <= 4096;
 }
 // The NEE_DS adjoint wavefront reuses the primal's shadow transmittances in the
-// replay, which retraces the primal only with the default replay majorant.
+// replay, which retraces the primal only with the default replay majorant;
+// uncapped paths longer than kUncappedPass vertices finish on the state machine.
 static bool use_wave_bw(const DMedium& M, int bw_mode) {
-    return bw_mode == VRT_BW_NEE_DS && M.max_bounces > 0 && M.max_bounces <= 4096 && !M.ds_compat;
+    return bw_mode == VRT_BW_NEE_DS && M.max_bounces <= 4096 && !M.ds_compat;
 }
 
 static bool is_collision(int integrator) {

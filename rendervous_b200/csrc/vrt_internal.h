@@ -77,8 +77,10 @@ int launch_collision_bw(const DMedium& M, int integrator, const PathSrc& src, ui
 int launch_collision_sample(const DMedium& M, const float* rays, int64_t n, uint64_t seed, float* out3,
                             const float* dL3, DScratch* scratch, int num_sms, cudaStream_t stream);
 
-// The NEE_DS adjoint as a persistent state machine (vrt_adjoint.cu).
+// The NEE_DS adjoint as a persistent state machine (vrt_adjoint.cu); with
+// pids, over the n_paths paths listed there (device array).
 int launch_nee_ds_bw(const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed, const float* dL,
-                     float div, DScratch* scratch, int num_sms, cudaStream_t stream);
+                     float div, DScratch* scratch, int num_sms, cudaStream_t stream,
+                     const unsigned long long* pids = nullptr);
 
 }  // namespace vrt

@@ -23,8 +23,11 @@
 // The job buffer is bounded: a warp takes new paths only while the job count
 // plus the worst case of every lane of the launch (1 + lights x max_bounces
 // jobs per path) fits, and the host repeats walk + shadow rounds until every
-// path is done.  Used for capped NEE paths; the persistent state machine of
-// vrt_path.cu serves uncapped ones.
+// path is done.  An uncapped path (the reference's default) walks at most
+// kUncappedPass vertices in a round; then its state at the start of its next
+// segment (position, direction, throughput, emission sum, stream position)
+// is saved and the next round resumes it before taking new paths, so it
+// draws exactly what the sequential definition draws.
 //
 // This file also holds the shadow kernels of the NEE_DS adjoint wavefront
 // (vrt_wave_ds.cu): ratio / delta tracking as persistent kernels that advance
@@ -44,6 +47,17 @@ struct WaveFw {
     int cut;          // >= 0: paths stop into the radiance cache at their (cut+1)-th real collision
     float* q;         // the cache queries: 3 planes [rows, 3] (position, direction, throughput)
     long long rows;
+    // uncapped paths: after kpass vertices in a pass a path's state at the
+    // start of its next segment is saved (5 float4: x, w, W, the emission
+    // sum, pid, bounces and the stream position) and resumed in the next
+    // round, before new paths; kpass == 0 with a bounce cap or a cut
+    int kpass;
+    const float4* cin;
+    unsigned long long n_cin;
+    unsigned long long* cin_head;
+    float4* cout;
+    unsigned long long* cout_count;
+    unsigned long long cap_cont, lanes;
 };
 
 __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, float* out,
@@ -57,6 +71,7 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
     int bounces = 0;
     uint64_t pid = 0;
     uint32_t steps_path = 0;
+    int pass_verts = 0;  // vertices of the current path in this pass (uncapped paths)
     bool alive = false, exhausted = false;
     uint32_t n_paths_done = 0, n_verts = 0;
     // the job slot reserved for the direct term of the lane's next path (taken
@@ -73,17 +88,51 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
         unsigned want = __ballot_sync(kAll, !alive && !exhausted);
         if (want) {
             const int leader = __ffs(want) - 1;
-            unsigned long long base = 0;
+            const unsigned nw = (unsigned)__popc(want);
+            // saved paths are resumed first (nres of the lanes), new paths fill the rest
+            unsigned long long base = 0, rb = 0;
+            unsigned nres = 0;
             if ((int)lane == leader) {
                 const unsigned long long used = *((volatile unsigned long long*)wv.count);
-                base = used + wv.reserve > wv.cap ? ~0ull
-                                                  : atomicAdd(&sc->next_path, (unsigned long long)__popc(want));
+                bool room = used + wv.reserve <= wv.cap;
+                if (room && wv.kpass > 0)
+                    room = *((volatile unsigned long long*)wv.cout_count) + wv.lanes <= wv.cap_cont;
+                if (!room) {
+                    base = ~0ull;
+                } else {
+                    if (wv.n_cin && *((volatile unsigned long long*)wv.cin_head) < wv.n_cin) {
+                        rb = atomicAdd(wv.cin_head, (unsigned long long)nw);
+                        if (rb < wv.n_cin) nres = (unsigned)(wv.n_cin - rb < nw ? wv.n_cin - rb : nw);
+                    }
+                    base = nres < nw ? atomicAdd(&sc->next_path, (unsigned long long)(nw - nres)) : 0ull;
+                }
             }
             base = __shfl_sync(kAll, base, leader);
+            rb = __shfl_sync(kAll, rb, leader);
+            nres = __shfl_sync(kAll, nres, leader);
+            const unsigned rank = __popc(want & ((1u << lane) - 1u));
             if (base == ~0ull) {
                 exhausted = true;  // no room this round: finish the lanes in flight
+            } else if (!alive && !exhausted && rank < nres) {
+                // resume a saved path at the start of its next segment
+                const float4* c = wv.cin + 5 * (rb + rank);
+                const float4 c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3], c4 = c[4];
+                x = make_float3(c0.x, c0.y, c0.z);
+                w = make_float3(c0.w, c1.x, c1.y);
+                W = make_float3(c1.z, c1.w, c2.x);
+                Rem = make_float3(c2.y, c2.z, c2.w);
+                pid = (uint64_t)__float_as_uint(c3.x) | ((uint64_t)__float_as_uint(c3.y) << 32);
+                bounces = (int)__float_as_uint(c3.z);
+                rng.init(seed, pid, 0);
+                rng.seek(Rng::Pos{__float_as_uint(c3.w), __float_as_uint(c4.x)});
+                float tMin;
+                boundary(M, x, w, tMin, d);
+                ff = Flight();
+                steps_path = 0;
+                pass_verts = 0;
+                alive = true;
             } else if (!alive && !exhausted) {
-                const uint64_t p = base + __popc(want & ((1u << lane) - 1u));
+                const uint64_t p = base + (rank - nres);
                 if (p >= n_paths) {
                     exhausted = true;
                 } else {
@@ -102,6 +151,7 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                     Rem = f3(0.0f);
                     bounces = 0;
                     steps_path = 0;
+                    pass_verts = 0;
                     ff = Flight();
                     ++n_paths_done;
                     if (wv.cut >= 0) {  // no query unless the path reaches the cut
@@ -214,6 +264,22 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                         ff = Flight();
                         ev = d > EPS ? 0 : 2;
                     }
+                }
+                if (ev == 0 && wv.kpass > 0 && ++pass_verts >= wv.kpass) {
+                    // an uncapped path at the pass's vertex budget: save it for the next round
+                    const unsigned long long o = atomicAdd(wv.cout_count, 1ull);
+                    if (o < wv.cap_cont) {
+                        float4* c = wv.cout + 5 * o;
+                        c[0] = make_float4(x.x, x.y, x.z, w.x);
+                        c[1] = make_float4(w.y, w.z, W.x, W.y);
+                        c[2] = make_float4(W.z, Rem.x, Rem.y, Rem.z);
+                        c[3] = make_float4(__uint_as_float((uint32_t)pid), __uint_as_float((uint32_t)(pid >> 32)),
+                                           __uint_as_float((uint32_t)bounces), __uint_as_float(rng.n));
+                        c[4] = make_float4(__uint_as_float(rng.ntr), 0.0f, 0.0f, 0.0f);
+                    } else {
+                        guard(sc, 11);
+                    }
+                    alive = false;
                 }
             }
             if (ev == 2) {  // the path's estimate is complete (its shadow terms arrive through the jobs)
@@ -431,12 +497,14 @@ __global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, const ShadowJo
 int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed, float* out,
                    float scale, cudaStream_t stream, int cut, float* queries) {
     if (n_paths == 0) return 0;
-    if (M.max_bounces <= 0 && cut < 0) return VRT_E_UNSUPPORTED;  // the reserve needs a bound on vertices
     if (cut >= 0 && !queries) return VRT_E_NULL_POINTER;
     const unsigned long long lights = M.has_sun ? 2ull : 1ull;
-    // light jobs come from the vertices before the cap or the cut
+    // light jobs come from the vertices before the cap or the cut; an uncapped
+    // path walks at most kUncappedPass vertices per pass and resumes later
     unsigned long long verts = M.max_bounces > 0 ? (unsigned long long)M.max_bounces : ~0ull;
     if (cut >= 0 && (unsigned long long)cut < verts) verts = (unsigned long long)cut;
+    const int kpass = verts == ~0ull ? kUncappedPass : 0;
+    if (kpass) verts = (unsigned long long)kpass;
     const unsigned long long per_path = 1ull + lights * verts;
     int blocks = persistent_blocks((const void*)k_walk_fw, 256, ctx->num_sms);
     const uint64_t need = (n_paths + 255) / 256;
@@ -446,16 +514,32 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
     if (inflight > n_paths) inflight = n_paths;
     const unsigned long long reserve = inflight * (per_path + 1);  // + the reserved direct-term slot
     const unsigned long long cap = reserve + batch_jobs(n_paths, 1ull + lights);
-    int st = ensure_wave_buffer(ctx, 256 + cap * sizeof(ShadowJob));
+    // saved-path buffers (two, swapped per round): every lane in flight may save once more
+    const unsigned long long cap_cont = kpass ? 4ull * (unsigned long long)blocks * 256ull : 0ull;
+    const size_t o_cont = 256 + cap * sizeof(ShadowJob), cont_bytes = (size_t)cap_cont * 5 * sizeof(float4);
+    int st = ensure_wave_buffer(ctx, o_cont + 2 * cont_bytes);
     if (st) return st;
     WaveFw wv;
-    wv.count = reinterpret_cast<unsigned long long*>(ctx->wave);
+    // header words: [0] jobs written, [1] shadow-kernel head, [2] resume head, [3] / [4] saved-path counts
+    unsigned long long* hdr = reinterpret_cast<unsigned long long*>(ctx->wave);
+    wv.count = hdr;
     wv.jobs = reinterpret_cast<ShadowJob*>(static_cast<char*>(ctx->wave) + 256);
     wv.cap = cap;
     wv.reserve = reserve;
     wv.cut = cut;
     wv.q = queries;
     wv.rows = (long long)n_paths;
+    wv.kpass = kpass;
+    wv.cap_cont = cap_cont;
+    wv.lanes = (unsigned long long)blocks * 256ull;
+    float4* cont[2] = {reinterpret_cast<float4*>(static_cast<char*>(ctx->wave) + o_cont),
+                       reinterpret_cast<float4*>(static_cast<char*>(ctx->wave) + o_cont + cont_bytes)};
+    int side = 0;
+    wv.cin = cont[1];
+    wv.n_cin = 0;
+    wv.cin_head = hdr + 2;
+    wv.cout = cont[0];
+    wv.cout_count = hdr + 3;
     cudaError_t e = cudaMemsetAsync(&ctx->scratch->next_path, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return launch_status(e);
     const int sblocks = ctx->num_sms * 8;
@@ -463,8 +547,11 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
                                                          : (const void*)k_shadow_run<1, OUT_IMAGE>, 256, ctx->num_sms);
     const ShadowOut so = {out, scale, nullptr, nullptr, 0};
     for (int round = 0;; ++round) {
-        // count of the jobs written, and the head the persistent shadow kernel takes them from
-        if ((e = cudaMemsetAsync(wv.count, 0, 2 * sizeof(unsigned long long), stream)) != cudaSuccess)
+        // count of the jobs written, the head the persistent shadow kernel takes
+        // them from, the resume head and this round's saved-path count
+        if ((e = cudaMemsetAsync(hdr, 0, 3 * sizeof(unsigned long long), stream)) != cudaSuccess)
+            return launch_status(e);
+        if ((e = cudaMemsetAsync(wv.cout_count, 0, sizeof(unsigned long long), stream)) != cudaSuccess)
             return launch_status(e);
         {
             KernelScope ks(VRT_K_WALK_FW, stream);
@@ -483,13 +570,23 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
         }
         count_launches(2);
         if ((st = launch_status(cudaGetLastError()))) return st;
-        unsigned long long taken = 0;
+        unsigned long long taken = 0, saved = 0;
         if ((e = cudaMemcpyAsync(&taken, &ctx->scratch->next_path, sizeof(taken), cudaMemcpyDeviceToHost, stream)) !=
             cudaSuccess)
             return launch_status(e);
+        if (kpass &&
+            (e = cudaMemcpyAsync(&saved, wv.cout_count, sizeof(saved), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+            return launch_status(e);
         if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return launch_status(e);
-        if (taken >= n_paths) break;
+        if (saved > cap_cont) return VRT_E_ITER_CAP;  // (the admission test keeps this from happening)
+        if (taken >= n_paths && saved == 0) break;
         if (round > (1 << 20)) return VRT_E_ITER_CAP;
+        // the paths saved this round are resumed in the next
+        wv.cin = cont[side];
+        wv.n_cin = saved;
+        side ^= 1;
+        wv.cout = cont[side];
+        wv.cout_count = hdr + 3 + side;
     }
     return 0;
 }

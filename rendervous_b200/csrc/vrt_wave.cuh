@@ -262,6 +262,11 @@ constexpr int kCrossBw = 8;  // the transmittance adjoint's first pass (k_shadow
 constexpr int kWalkCross = 12;  // k_walk_fw
 constexpr int kDsCross = 8;     // k_ds_primal, k_ds_rewalk
 
+// Vertices an uncapped path (max_bounces == 0, the reference's default) walks
+// in one pass of a wavefront; a longer path continues in a later pass
+// (forward) or is run whole by the state-machine adjoint (NEE_DS).
+constexpr int kUncappedPass = 64;
+
 template <int TR, bool BW>
 __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tally& tl, DScratch* sc, bool& hit,
                                              float& hmaj, float& hf) {
@@ -388,6 +393,13 @@ struct WaveBw {
     unsigned long long cap_jobs, cap_recs, cap_paths, cap_evs;
     unsigned long long res_jobs, res_recs, res_evs, lanes;
     uint64_t p_begin;
+    // uncapped paths (max_bounces == 0): a path still going after kpass
+    // vertices is handed to the state-machine adjoint (its global id into
+    // spill, count in *spill_count); kpass == 0 with a bounce cap
+    int kpass;
+    unsigned long long* spill;
+    unsigned long long* spill_count;
+    unsigned long long cap_spill;
 };
 
 }  // namespace wave

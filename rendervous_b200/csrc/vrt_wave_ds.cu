@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
     // ev_next), so every path leaves one reserved slot of each kind unused
     uint32_t steps_path = 0, first = kNone, rec_next = kNone, first_ev = kNone, ev_next = kNone, n_ev = 0;
     uint32_t n_paths_done = 0;
-    bool logged = false;
+    bool logged = false, spilled = false;
     Tally tl;
 
     while (true) {
@@ -106,6 +106,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                     ev_next = kNone;
                     n_ev = 0;
                     logged = true;
+                    spilled = false;
                     ff = Flight();
                     alive = true;
                     ++n_paths_done;
@@ -184,8 +185,10 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                             jfork = rng.ntr;
                             rng.ntr += (uint32_t)lights;
                             const bool capped = M.max_bounces > 0 && bounces + 1 >= M.max_bounces;
+                            // an uncapped path at the pass's vertex budget goes to the state machine
+                            const bool at_budget = wv.kpass > 0 && bounces + 1 >= wv.kpass;
                             float3 wo = w;
-                            if (!capped) wo = phase_sample(M, rng, w);
+                            if (!capped && !at_budget) wo = phase_sample(M, rng, w);
                             rsp = null_W < EPS;
                             if (rsp) Rspacc = Rspacc + acc;
                             else Racc = Racc + acc;
@@ -194,6 +197,9 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                             ++bounces;
                             if (capped || all_less(W, EPS)) {
                                 ev = 2;  // W stays: the light jobs below weigh with it
+                            } else if (at_budget) {
+                                ev = 2;
+                                spilled = true;
                             } else {
                                 w = wo;
                                 float tMin;
@@ -212,7 +218,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
         }
         // ---- one reservation for the T jobs, the vertex record, the collision
         // record and (at the end of a path with logged collisions) its replay-list entry
-        const int nl = (finish && logged && (first_ev != kNone || nev)) ? 1 : 0;
+        const int nl = (finish && logged && !spilled && (first_ev != kNone || nev)) ? 1 : 0;
         const Slots4 sl = reserve_slots4(&wv.hdr[0], &wv.hdr[1], &wv.hdr[5], &wv.hdr[8],
                                          (uint32_t)nj | ((uint32_t)nrec << 8) | ((uint32_t)nev << 16) |
                                              ((uint32_t)nl << 24));
@@ -258,7 +264,11 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                                                                   __uint_as_float(logged ? first_ev : kUnlogged)));
             // an entry whose last collision found the log full is skipped by the replay
             if (nl) __stcs(wv.list + sl.s3, make_uint4((uint32_t)k, logged ? first_ev : kUnlogged, n_ev, 0u));
-            if (!logged) {
+            if (spilled) {  // its records are ignored; the state machine runs the whole path
+                const unsigned long long o = atomicAdd(wv.spill_count, 1ull);
+                if (o < wv.cap_spill) wv.spill[o] = (unsigned long long)pid;
+                else guard(sc, 10);
+            } else if (!logged) {
                 const unsigned long long o = atomicAdd(&wv.hdr[6], 1ull);
                 if (o < wv.cap_paths) wv.over[o] = (uint32_t)k;
                 else guard(sc, 8);
@@ -564,8 +574,12 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, cons
 int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed,
                       const float* dL, float div, cudaStream_t stream) {
     if (n_paths == 0) return 0;
-    if (M.max_bounces <= 0 || M.ds_compat) return VRT_E_UNSUPPORTED;
-    const unsigned long long lights = M.has_sun ? 2ull : 1ull, B = (unsigned long long)M.max_bounces;
+    if (M.ds_compat) return VRT_E_UNSUPPORTED;
+    // uncapped paths walk at most kUncappedPass vertices here; the few that go on
+    // are run whole by the state machine afterwards
+    const int kpass = M.max_bounces > 0 ? 0 : kUncappedPass;
+    const unsigned long long lights = M.has_sun ? 2ull : 1ull;
+    const unsigned long long B = (unsigned long long)(M.max_bounces > 0 ? M.max_bounces : kpass);
     int blocksA = persistent_blocks((const void*)k_ds_primal, 256, ctx->num_sms);
     int blocksC = persistent_blocks((const void*)k_ds_replay, 256, ctx->num_sms);
     int blocksW = persistent_blocks((const void*)k_ds_rewalk, 256, ctx->num_sms);
@@ -595,7 +609,10 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     const size_t o_recs = o_dldt + ((wv.cap_jobs * 4 + 255) & ~(size_t)255);
     const size_t o_info = o_recs + wv.cap_recs * sizeof(VertexRec), o_over = o_info + wv.cap_paths * 32;
     const size_t o_list = o_over + ((wv.cap_paths * 4 + 255) & ~(size_t)255);
-    const size_t o_evs = o_list + ((wv.cap_paths * 16 + 255) & ~(size_t)255), bytes = o_evs + wv.cap_evs * 32;
+    const size_t o_evs = o_list + ((wv.cap_paths * 16 + 255) & ~(size_t)255);
+    wv.kpass = kpass;
+    wv.cap_spill = kpass > 0 ? (unsigned long long)n_paths : 0ull;
+    const size_t o_spill = o_evs + wv.cap_evs * 32, bytes = o_spill + wv.cap_spill * 8;
     int st = ensure_wave_buffer(ctx, bytes);
     if (st) return st;
     char* base = static_cast<char*>(ctx->wave);
@@ -607,9 +624,13 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     wv.over = reinterpret_cast<uint32_t*>(base + o_over);
     wv.list = reinterpret_cast<uint4*>(base + o_list);
     wv.evs = reinterpret_cast<CollisionRec*>(base + o_evs);
+    wv.spill = reinterpret_cast<unsigned long long*>(base + o_spill);
+    wv.spill_count = &wv.hdr[10];  // kept across rounds
     wv.p_begin = 0;
     cudaError_t e = cudaMemsetAsync(&ctx->scratch->next_path, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return launch_status(e);
+    if ((e = cudaMemsetAsync(wv.spill_count, 0, sizeof(unsigned long long), stream)) != cudaSuccess)
+        return launch_status(e);
     for (int round = 0;; ++round) {
         // [0] jobs, [1] records, [2] re-walk queue, [3] / [4] heads of the shadow kernels,
         // [5] collisions, [6] paths left out of the log, [7] replay-list head, [8] replay list
@@ -644,6 +665,16 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
         if (taken >= n_paths) break;
         wv.p_begin = taken;
         if (round > (1 << 20)) return VRT_E_ITER_CAP;
+    }
+    if (kpass > 0) {  // the uncapped paths longer than the pass budget, whole, on the state machine
+        unsigned long long spilled = 0;
+        if ((e = cudaMemcpyAsync(&spilled, wv.spill_count, sizeof(spilled), cudaMemcpyDeviceToHost, stream)) !=
+            cudaSuccess)
+            return launch_status(e);
+        if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return launch_status(e);
+        if (spilled > wv.cap_spill) spilled = wv.cap_spill;
+        if (spilled)
+            return launch_nee_ds_bw(M, src, spilled, seed, dL, div, ctx->scratch, ctx->num_sms, stream, wv.spill);
     }
     return 0;
 }

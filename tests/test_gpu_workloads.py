@@ -155,3 +155,41 @@ def test_dda_workload_adjoint_matches_fp64_central_differences(cuda):
         errs.append(abs(grad[z, y, x] - fd) / max(abs(fd), 1e-3 * np.abs(grad).max()))
     errs = np.array(errs)
     assert np.median(errs) < 1e-4 and errs.max() < 1e-3, (np.median(errs), errs.max())
+
+
+def test_uncapped_paths_run_on_the_wavefront(cuda):
+    """The reference's default (no bounce cap) runs on the wavefront kernels: in
+    a dense, high-albedo medium many paths outlive the 64-vertex pass, so the
+    forward resumes them in later rounds and the NEE_DS adjoint hands them to
+    the state machine -- image and gradients still match the oracle's
+    uncapped paths."""
+    from rendervous_b200 import _lib
+    from tests.helpers import build_field, front_camera
+    ffi, lib = _lib.ffi_lib()
+    ctx = _lib.context(cuda)
+    stream = _lib.stream_handle(cuda)
+    sig = torch.from_numpy(synthetic.gaussian_blobs(33, 6, 80.0, seed=4)).to(cuda)
+    alb = torch.nn.Parameter(torch.full((33, 33, 33, 3), 0.985, device=cuda))
+    field = build_field(sig, albedo_grid=alb, env=1.0, sun_dir=(0.3, 0.8, 0.5), sun_radiance=2.0, g=0.3,
+                        max_bounces=0, majorant="grid", brick=4, sigma_requires_grad=True)
+    H = W = 24
+    cam = maps.PerspectiveCameraSensor(W, H, front_camera(1).to(cuda), jittered=True)
+    ks = ffi.new("vrt_kernel_stat[]", lib.VRT_K_COUNT)
+    maps.check()
+    _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
+    img = cam.capture(field, fw_samples=4, bw_samples=4, seed=21)
+    dimg = torch.from_numpy(np.random.default_rng(6).random(img.shape).astype(np.float32)).to(cuda)
+    (img * dimg).sum().backward()
+    maps.check()
+    _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
+    assert ks[lib.VRT_K_WALK_FW].launches >= 2          # more than one round: paths were resumed
+    assert ks[lib.VRT_K_DS_PRIMAL].launches >= 1
+    sc = oracle.OracleScene(field.lower().to_numpy(), with_grads=True)
+    ref, cnt = oracle.capture_fw(sc, "nee", front_camera(1).numpy(), W, H, math.pi / 4, True, 4, 21)
+    oracle.capture_bw(sc, "ds", front_camera(1).numpy(), W, H, math.pi / 4, True, 4, 21, dimg.cpu().numpy())
+    assert cnt["vertices"] > 64 * 50                    # long paths exist
+    close = np.isclose(img.detach().cpu().numpy(), ref, rtol=1e-3, atol=1e-5).all(axis=-1)
+    assert close.mean() >= 0.98, close.mean()
+    for g, rg in ((field.sigma.grid.grad, sc.sigma_grad), (alb.grad, sc.albedo_grad)):
+        rel = np.abs(g.cpu().numpy() - rg).sum() / max(np.abs(rg).sum(), 1e-30)
+        assert rel < 2e-2, rel
