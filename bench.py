@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--small", action="store_true", help="a 128x128, 8 spp image of the same medium (profiling)")
     ap.add_argument("--width", type=int, default=None, help="square image size of the same medium (profiling)")
     ap.add_argument("--spp", type=int, default=None, help="samples per pixel (profiling)")
+    ap.add_argument("--max-bounces", type=int, default=None,
+                    help="bounce cap of the same medium (0 = uncapped, the reference's default)")
     return ap.parse_args()
 
 
@@ -74,7 +76,7 @@ def _workload_arrays():
     return wl, sigma, albedo, target_sigma, sun, poses
 
 
-def build_field(sigma_t, albedo_t, wl, sun):
+def build_field(sigma_t, albedo_t, wl, sun, max_bounces=None):
     from rendervous_b200 import maps
     bmin, bmax = maps.normalized_box(sigma_t)
     sg = maps.Grid3D(sigma_t, bmin, bmax)
@@ -87,7 +89,7 @@ def build_field(sigma_t, albedo_t, wl, sun):
     return maps.DeltatrackingNEEPathIntegrator(
         sg, ag, maps.ZERO, env, maps._functionsampler(maps.UniformDirectionSampler(6), env),
         maps.HenyeyGreensteinPhase(g), maps.HenyeyGreensteinPhaseSampler(g), boundary, maj, tr, 0.1,
-        max_bounces=wl["max_bounces"],
+        max_bounces=wl["max_bounces"] if max_bounces is None else max_bounces,
         directional_light=maps.DirectionalLight(sun, wl["sun_intensity"]))
 
 
@@ -273,10 +275,11 @@ def run_ours(args):
     spp = args.spp or (8 if args.small else wl["spp"])
     sigma_t = torch.nn.Parameter(torch.from_numpy(sigma).to(dev))
     albedo_t = torch.nn.Parameter(torch.from_numpy(albedo).to(dev))
-    field = build_field(sigma_t, albedo_t, wl, sun)
+    mb = wl["max_bounces"] if args.max_bounces is None else args.max_bounces
+    field = build_field(sigma_t, albedo_t, wl, sun, mb)
     cam = maps.PerspectiveCameraSensor(W, H, torch.from_numpy(poses_np).to(dev), jittered=True)
     with torch.no_grad():
-        tfield = build_field(torch.from_numpy(target_sigma).to(dev), albedo_t.detach(), wl, sun)
+        tfield = build_field(torch.from_numpy(target_sigma).to(dev), albedo_t.detach(), wl, sun, mb)
         target = cam.capture(tfield, fw_samples=spp, seed=777)
     maps.check()
 
@@ -423,8 +426,9 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
-            "config": {"workload": WORKLOAD + ("" if (H, spp) == (wl["width"], wl["spp"]) else f"_{W}px_{spp}spp"), "grid": list(sigma.shape[:3]),
-                       "image": [H, W], "spp": spp, "max_bounces": wl["max_bounces"], "phase_g": wl["phase_g"],
+            "config": {"workload": WORKLOAD + ("" if (H, spp, mb) == (wl["width"], wl["spp"], wl["max_bounces"])
+                                               else f"_{W}px_{spp}spp_{mb}bounces"), "grid": list(sigma.shape[:3]),
+                       "image": [H, W], "spp": spp, "max_bounces": mb, "phase_g": wl["phase_g"],
                        "transmittance": "ratio tracking", "majorant": "8^3-brick grid", "adjoint": "NEE_DS",
                        "l2": "flushed between steps (512 MB write)", "parallelism": f"dp{world}"},
             "e2e": e2e,
