@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-c5", action="store_true", help="skip the radiance-cache equal-time comparison")
     ap.add_argument("--small", action="store_true", help="a 128x128, 8 spp image of the same medium (profiling)")
     ap.add_argument("--width", type=int, default=None, help="square image size of the same medium (profiling)")
     ap.add_argument("--spp", type=int, default=None, help="samples per pixel (profiling)")
@@ -412,6 +413,17 @@ def run_ours(args):
                "d2h_bytes_per_step": int(h_gs.numel() * 4 + h_ga.numel() * 4 + 4),
                "ms_per_step": e2e_total / max(1, args.steps)}
 
+    # the metric's second half, outside the timed region: equal-time error of the
+    # radiance-cache renderer against the plain tracer on the cache workload,
+    # both measured against an FP64 high-spp estimate of 4 crops (a bounded run)
+    c5 = None
+    if rank == 0 and world == 1 and not args.no_c5:
+        from rendervous_b200 import cache_eval
+        del flush
+        torch.cuda.empty_cache()
+        c5 = cache_eval.equal_time(ref_spp=4096, budget=3.0, warmup=64)
+        maps.set_sync_checks(False)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, sample, thr, secs = cpu_sample()
@@ -449,6 +461,7 @@ def run_ours(args):
             "kernels": ktable,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
+            "c5_equal_time_mse": c5,
         }
         print(json.dumps(line))
     if world > 1:

@@ -190,6 +190,13 @@ typedef struct vrt_kernel_stat {
    collisions do not fit are replayed by walking them again (same gradients,
    more time). */
 int vrt_set_collision_log_limit(vrt_context* ctx, int64_t events);
+/* Caps the items (shadow jobs, vertex records) a wavefront round holds beyond
+   the worst case of the paths in flight; 0 restores the automatic size (up to
+   2^27).  A smaller cap means a smaller device footprint and more rounds;
+   uncapped paths that outgrow a round's room resume in the next round
+   (forward) or finish on the state-machine adjoint (NEE_DS); results are the
+   same up to the order of float sums. */
+int vrt_set_wave_batch_limit(vrt_context* ctx, int64_t items);
 void vrt_set_kernel_timing(int32_t on);
 /* Gather microbenchmark (the roofline of the lookups): threads x per_thread
    random 32-byte loads (L1 bypassed) from `buffer` (bytes long, 32-byte
@@ -306,6 +313,16 @@ int vrt_capture_fw(vrt_context* ctx, const vrt_medium* m, int32_t integrator, co
                    uint64_t seed, float* rgb, void* stream);
 int vrt_capture_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const vrt_camera* cam, int32_t spp,
                    uint64_t seed, const float* dL_drgb, void* stream);
+/* The NEE capture in FP64 (no reference counterpart: the reference renders in
+   FP32): the high-accuracy estimate that the radiance cache's error is
+   measured against.  Same paths as vrt_capture_fw with VRT_PI_NEE (sample s
+   of pixel p is Philox path s * npix + p), every quantity in double; rgb is a
+   double [pixels, 3] (cleared here).  Supports constant environments with
+   uniform NEE, ratio- or delta-tracking shadow rays, const or grid albedo and
+   majorant; other media return VRT_E_UNSUPPORTED. */
+int vrt_capture_fw_fp64(vrt_context* ctx, const vrt_medium* m, const vrt_camera* cam, int32_t spp, uint64_t seed,
+                        double* rgb, void* stream);
+
 /* Radiance-cache forms of the NEE capture (no reference counterpart).
    Prefix: the integrator of vrt_capture_fw, but a path stops at its (cut+1)-th
    real collision and records a query there; rgb ACCUMULATES prefix / spp (not

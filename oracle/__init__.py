@@ -349,6 +349,15 @@ def capture_fw(scene: OracleScene, integrator: str, poses, width, height, fov, j
     return out, dict(paths=c.paths, vertices=c.vertices, steps=c.steps)
 
 
+def capture_fw_fp64(scene: OracleScene, poses, width, height, fov, jittered, spp, seed, sensors=None) -> np.ndarray:
+    """The NEE capture in double precision: float64 [..., 3]."""
+    ffi, L = lib()
+    cam, keep = make_camera(poses, width, height, fov, jittered, sensors=sensors)
+    out = np.empty(keep.shape + (3,), np.float64)
+    L.orc_capture_fw_fp64(scene.s, cam, spp, seed, ptr(ffi, out, "double *"))
+    return out
+
+
 def capture_bw(scene: OracleScene, bw_mode: str, poses, width, height, fov, jittered, spp, seed, dL_drgb,
                sensors=None) -> None:
     ffi, L = lib()

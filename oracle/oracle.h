@@ -122,6 +122,8 @@ void orc_radiance_bw(const orc_scene* s, int32_t bw_mode, const float* rays, int
 
 void orc_capture_fw(const orc_scene* s, int32_t integrator, const orc_camera* cam, int32_t spp, uint64_t seed, float* rgb, orc_counters* c);
 void orc_capture_bw(const orc_scene* s, int32_t bw_mode, const orc_camera* cam, int32_t spp, uint64_t seed, const float* dL_drgb);
+/* The NEE capture with every quantity in double: rgb [pixels, 3] doubles */
+void orc_capture_fw_fp64(const orc_scene* s, const orc_camera* cam, int32_t spp, uint64_t seed, double* rgb);
 /* Radiance-cache forms of the NEE capture.  prefix: paths stop at their
    (cut+1)-th real collision; rgb += prefix / spp; queries = 3 planes [n,3]
    (position, direction, throughput W; W = 0 where the path ended earlier),

@@ -2434,6 +2434,27 @@ void orc_capture_fw(const orc_scene* s, int32_t integrator, const orc_camera* ca
     if (c) { c->paths = npix * spp; c->vertices = verts; c->steps = steps; }
 }
 
+void orc_capture_fw_fp64(const orc_scene* s, const orc_camera* cam, int32_t spp, uint64_t seed, double* rgb) {
+    Scene<double> S(*s);
+    int64_t npix = camera_npix(*cam);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t p = 0; p < npix; ++p) {
+        int view, row, col;
+        camera_pixel(*cam, p, view, row, col);
+        V3<double> acc(0.0);
+        Counters cnt;
+        for (int sidx = 0; sidx < spp; ++sidx) {
+            Rng rng(seed, capture_path_id(p, sidx, npix), 0);
+            V3<double> x, w;
+            camera_ray(*cam, view, row, col, rng, x, w);
+            acc += path_integrator_NEE(S, rng, x, w, false, cnt) * (1.0 / (double)spp);
+        }
+        rgb[3 * p] = acc.x;
+        rgb[3 * p + 1] = acc.y;
+        rgb[3 * p + 2] = acc.z;
+    }
+}
+
 void orc_capture_prefix(const orc_scene* s, const orc_camera* cam, int32_t spp, uint64_t seed, int32_t cut, float* rgb,
                         float* queries) {
     Scene<float> S(*s);

@@ -7,11 +7,9 @@ shadow rays over an 8^3-brick majorant grid.  The plain tracer runs up to 512
 bounces; the cached renderer traces 2 bounces and stops into the cache.
 
 Error is measured on a fixed set of square crops against a high-spp estimate of
-the same pixels from the plain tracer (the FP32 GPU tracer, whose paths agree
-with the CPU oracle path for path in the parity tests; at thousands of samples
-per pixel its Monte Carlo error dominates FP32 rounding by orders of
-magnitude).  Reference pixels are rendered in ray mode from jittered camera
-rays generated here with the sensor's own camera model.
+the same pixels from the FP64 plain tracer (vrt_capture_fw_fp64: every quantity
+in double, path for path with the CPU restatement's double instantiation in
+the parity tests), rendered as a sensors batch of the crop pixels.
 
 Run: python -m rendervous_b200.cache_eval [--res 512 --size 1024 ...]
 Prints one JSON line per method checkpoint and a summary line.
@@ -108,6 +106,31 @@ def reference_pixels(field, pose, width, height, fov, znear, pixels, spp, seed, 
     return (acc / spp).float()
 
 
+def reference_pixels_fp64(field, cam, pixels, spp, seed, chunk_paths=1 << 24):
+    """FP64 mean radiance of `pixels` (row * width + col of view 0) over spp
+    paths each, as float64 [n, 3]."""
+    dev = pixels.device
+    ffi, lib = _lib.ffi_lib()
+    desc = field.cast(input_dim=6).lower()
+    m = desc.to_struct()
+    sens = torch.stack([torch.zeros_like(pixels), pixels // cam.width, pixels % cam.width], dim=-1).to(torch.int64)
+    sens = sens.contiguous()
+    c, keep = cam.to_struct(dev, sens)
+    acc = torch.zeros(pixels.shape[0], 3, dtype=torch.float64, device=dev)
+    out = torch.empty_like(acc)
+    per = max(1, min(spp, chunk_paths // max(1, pixels.shape[0])))
+    done, k = 0, 0
+    vctx = _lib.context(dev)
+    while done < spp:
+        n = min(per, spp - done)
+        _lib.check(lib.vrt_capture_fw_fp64(vctx.ptr, m, c, n, seed * 1000003 + k, ffi.cast("double *", out.data_ptr()),
+                                           _lib.stream_handle(dev)), "vrt_capture_fw_fp64")
+        acc += out * n
+        done += n
+        k += 1
+    return acc / spp
+
+
 class Timer:
     def __init__(self):
         self.total = 0.0
@@ -170,6 +193,46 @@ def time_to_reach(curve, mse):
     return None
 
 
+def equal_time(res=512, size=1024, max_sigma=200.0, crops=4, crop=32, ref_spp=4096, budget=20.0, plain_chunk=1,
+               cache_budget=None, cache_spp=1, warmup=64, train_paths=1 << 14, train_cut=16, rec=4, cut=2, lr=1e-2,
+               seed=11, curves=None):
+    """Equal-time comparison of the cached renderer against the plain tracer on
+    the cache workload; returns the summary dict (curves, when a list is
+    given, receives the per-frame checkpoints)."""
+    dev = torch.device("cuda", torch.cuda.current_device())
+    maps.set_sync_checks(False)
+    t0 = time.time()
+    sigma = synthetic.value_noise(res, 6, max_sigma, seed, device=dev)
+    field = build_field(sigma)
+    poses = torch.from_numpy(synthetic.ring_poses(1, radius=2.0, elevation_deg=20.0)).to(dev)
+    cam = maps.PerspectiveCameraSensor(size, size, poses, jittered=True)
+    pixels = crop_pixels(size, size, crops, crop).to(dev)
+    tr = Timer()
+    ref = {}
+    tr.run(lambda: ref.setdefault("x", reference_pixels_fp64(field, cam, pixels, ref_spp, seed=7)))
+    ref = ref["x"].float()
+    plain = plain_curve(field, cam, pixels, ref, budget, plain_chunk, seed=1000)
+    cached, loss = cached_curve(field, cam, pixels, ref, cache_budget or budget, cache_spp, warmup, seed=5, cut=cut,
+                                train_paths=train_paths, rec=rec, train_cut=train_cut, lr=lr)
+    if curves is not None:
+        for name, curve in (("plain", plain), ("cached", cached)):
+            for t, e, s in curve:
+                curves.append(dict(method=name, seconds=round(t, 4), mse=e, spp=s))
+    target = plain[-1][1]
+    t_cache = time_to_reach(cached, target)
+    maps.check()
+    return dict(
+        workload="radiance_cache_512" if (res, size) == (512, 1024) else f"noise_{res}_{size}",
+        res=res, size=size, max_sigma=max_sigma, eval_pixels=int(pixels.shape[0]), oracle="fp64",
+        ref_spp=ref_spp, ref_seconds=round(tr.total, 3), ref_pixel_mean=float(ref.mean()),
+        plain_seconds=round(plain[-1][0], 3), plain_spp=plain[-1][2], plain_mse=target,
+        cached_seconds_to_plain_mse=None if t_cache is None else round(t_cache, 3),
+        speedup=None if t_cache is None else round(plain[-1][0] / t_cache, 2),
+        cached_final_mse=cached[-1][1], cached_final_seconds=round(cached[-1][0], 3), cached_spp=cached[-1][2],
+        cache_loss=loss, cut=cut, train_cut=train_cut, train_paths=train_paths, rec=rec, warmup_frames=warmup,
+        wall_s=round(time.time() - t0, 1))
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--res", type=int, default=512)
@@ -191,39 +254,13 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--out", type=str, default=None)
     args = ap.parse_args(argv)
-    dev = torch.device("cuda", 0)
-    maps.set_sync_checks(False)
-    t0 = time.time()
-    sigma = synthetic.value_noise(args.res, 6, args.max_sigma, args.seed, device=dev)
-    field = build_field(sigma)
-    poses = torch.from_numpy(synthetic.ring_poses(1, radius=2.0, elevation_deg=20.0)).to(dev)
-    cam = maps.PerspectiveCameraSensor(args.size, args.size, poses, jittered=True)
-    pixels = crop_pixels(args.size, args.size, args.crops, args.crop).to(dev)
-    tr = Timer()
-    ref = {}
-    tr.run(lambda: ref.setdefault("x", reference_pixels(field, poses[0].reshape(-1), args.size, args.size, cam.fov,
-                                                        cam.znear, pixels, args.ref_spp, seed=7)))
-    ref = ref["x"]
+    torch.cuda.set_device(0)
     lines = []
-    plain = plain_curve(field, cam, pixels, ref, args.budget, args.plain_chunk, seed=1000)
-    cached, loss = cached_curve(field, cam, pixels, ref, args.cache_budget or args.budget, args.cache_spp,
-                                args.warmup, seed=5, cut=args.cut, train_paths=args.train_paths, rec=args.rec,
-                                train_cut=args.train_cut, lr=args.lr)
-    for name, curve in (("plain", plain), ("cached", cached)):
-        for t, e, s in curve:
-            lines.append(dict(method=name, seconds=round(t, 4), mse=e, spp=s))
-    target = plain[-1][1]
-    t_cache = time_to_reach(cached, target)
-    summary = dict(
-        workload="radiance_cache_512" if (args.res, args.size) == (512, 1024) else f"noise_{args.res}_{args.size}",
-        res=args.res, size=args.size, max_sigma=args.max_sigma, eval_pixels=int(pixels.shape[0]),
-        ref_spp=args.ref_spp, ref_seconds=round(tr.total, 3), ref_pixel_mean=float(ref.mean()),
-        plain_seconds=round(plain[-1][0], 3), plain_spp=plain[-1][2], plain_mse=target,
-        cached_seconds_to_plain_mse=None if t_cache is None else round(t_cache, 3),
-        speedup=None if t_cache is None else round(plain[-1][0] / t_cache, 2),
-        cached_final_mse=cached[-1][1], cached_final_seconds=round(cached[-1][0], 3), cached_spp=cached[-1][2],
-        cache_loss=loss, cut=args.cut, train_cut=args.train_cut, train_paths=args.train_paths, rec=args.rec,
-        warmup_frames=args.warmup, wall_s=round(time.time() - t0, 1))
+    summary = equal_time(res=args.res, size=args.size, max_sigma=args.max_sigma, crops=args.crops, crop=args.crop,
+                         ref_spp=args.ref_spp, budget=args.budget, plain_chunk=args.plain_chunk,
+                         cache_budget=args.cache_budget, cache_spp=args.cache_spp, warmup=args.warmup,
+                         train_paths=args.train_paths, train_cut=args.train_cut, rec=args.rec, cut=args.cut,
+                         lr=args.lr, seed=args.seed, curves=lines)
     for l in lines:
         print(json.dumps(l))
     print(json.dumps(summary))

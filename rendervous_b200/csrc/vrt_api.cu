@@ -366,6 +366,14 @@ int vrt_gather_peak(const void* buffer, int64_t bytes, int64_t threads, int32_t 
     return launch_status(cudaGetLastError());
 }
 
+int vrt_set_wave_batch_limit(vrt_context* ctx, int64_t items) {
+    int st = check_ctx(ctx);
+    if (st) return st;
+    if (items < 0) return VRT_E_BAD_SHAPE;
+    ctx->batch_limit = (unsigned long long)items;
+    return VRT_OK;
+}
+
 int vrt_set_collision_log_limit(vrt_context* ctx, int64_t events) {
     int st = check_ctx(ctx);
     if (st) return st;
@@ -444,6 +452,7 @@ int vrt_context_create(int32_t device, vrt_context** out) {
     ctx->wave = nullptr;
     ctx->wave_bytes = 0;
     ctx->log_limit = 0;
+    ctx->batch_limit = 0;
     if (cudaMalloc(&ctx->scratch, sizeof(DScratch)) != cudaSuccess) { delete ctx; return VRT_E_CUDA; }
     if (cudaMemset(ctx->scratch, 0, sizeof(DScratch)) != cudaSuccess) { cudaFree(ctx->scratch); delete ctx; return VRT_E_CUDA; }
     *out = ctx;
@@ -685,6 +694,25 @@ int vrt_capture_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const
                                  (cudaStream_t)stream);
     return launch_radiance_bw(M, bw_mode, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
                               ctx->scratch, ctx->num_sms, (cudaStream_t)stream);
+}
+
+int vrt_capture_fw_fp64(vrt_context* ctx, const vrt_medium* m, const vrt_camera* cam, int32_t spp, uint64_t seed,
+                        double* rgb, void* stream) {
+    int st = check_ctx(ctx);
+    if (st) return st;
+    if (spp < 1) return VRT_E_INVALID_ARGUMENT;
+    DMedium M;
+    if ((st = to_dmedium(m, M))) return st;
+    if (M.env_mode != 0 || M.env_sampler != 0 || M.tr_mode > 1) return VRT_E_UNSUPPORTED;
+    PathSrc S;
+    std::memset(&S, 0, sizeof(S));
+    if ((st = to_dcamera(cam, S.cam))) return st;
+    if (!rgb) return VRT_E_NULL_POINTER;
+    S.is_camera = 1;
+    S.npix = capture_pixels(cam);
+    cudaError_t e = cudaMemsetAsync(rgb, 0, sizeof(double) * 3 * S.npix, (cudaStream_t)stream);
+    if (e != cudaSuccess) return launch_status(e);
+    return launch_capture_fp64(M, S, spp, seed, rgb, ctx->scratch, ctx->num_sms, (cudaStream_t)stream);
 }
 
 int vrt_capture_prefix_fw(vrt_context* ctx, const vrt_medium* m, const vrt_camera* cam, int32_t spp, uint64_t seed,

@@ -12,6 +12,7 @@ struct vrt_context {
     void* wave;              // wavefront job buffer (grown on demand)
     size_t wave_bytes;
     unsigned long long log_limit;  // NEE_DS collision-log cap in records (0: automatic)
+    unsigned long long batch_limit;  // wavefront items per round beyond the reserve (0: automatic)
 };
 
 namespace vrt {
@@ -76,6 +77,10 @@ int launch_collision_bw(const DMedium& M, int integrator, const PathSrc& src, ui
 // DeltatrackingCollisionSampler on rays: forward when out3 != null, else backward with dL3.
 int launch_collision_sample(const DMedium& M, const float* rays, int64_t n, uint64_t seed, float* out3,
                             const float* dL3, DScratch* scratch, int num_sms, cudaStream_t stream);
+
+// The FP64 NEE capture (vrt_fp64.cu): rgb [pixels, 3] doubles, accumulated.
+int launch_capture_fp64(const DMedium& M, const PathSrc& S, int spp, uint64_t seed, double* rgb, DScratch* sc,
+                        int num_sms, cudaStream_t stream);
 
 // The NEE_DS adjoint as a persistent state machine (vrt_adjoint.cu); with
 // pids, over the n_paths paths listed there (device array).

@@ -265,8 +265,12 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                         ev = d > EPS ? 0 : 2;
                     }
                 }
-                if (ev == 0 && wv.kpass > 0 && ++pass_verts >= wv.kpass) {
-                    // an uncapped path at the pass's vertex budget: save it for the next round
+                // an uncapped path past the pass's vertex budget goes on while the job
+                // buffer holds every lane's worst case plus one more vertex per lane;
+                // else it is saved for the next round
+                if (ev == 0 && wv.kpass > 0 && ++pass_verts >= wv.kpass &&
+                    *((volatile unsigned long long*)wv.count) + wv.reserve + wv.lanes * (unsigned long long)njobs >
+                        wv.cap) {
                     const unsigned long long o = atomicAdd(wv.cout_count, 1ull);
                     if (o < wv.cap_cont) {
                         float4* c = wv.cout + 5 * o;
@@ -513,7 +517,7 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
     unsigned long long inflight = (unsigned long long)blocks * 256ull;
     if (inflight > n_paths) inflight = n_paths;
     const unsigned long long reserve = inflight * (per_path + 1);  // + the reserved direct-term slot
-    const unsigned long long cap = reserve + batch_jobs(n_paths, 1ull + lights);
+    const unsigned long long cap = reserve + batch_jobs(n_paths, 1ull + lights, ctx->batch_limit);
     // saved-path buffers (two, swapped per round): every lane in flight may save once more
     const unsigned long long cap_cont = kpass ? 4ull * (unsigned long long)blocks * 256ull : 0ull;
     const size_t o_cont = 256 + cap * sizeof(ShadowJob), cont_bytes = (size_t)cap_cont * 5 * sizeof(float4);

@@ -205,10 +205,11 @@ __device__ __forceinline__ void start_ray(const PathSrc& S, uint64_t pid, Rng& r
 // Items a round aims to hold beyond the reserve: twice `per_path` per path,
 // at least 2^20 and at most 2^27 (a 512x512 x 64 spp capture then runs in one
 // round: fewer kernel tails and host syncs, for about 18 GB of HBM).
-inline unsigned long long batch_jobs(uint64_t n_paths, unsigned long long per_path) {
+inline unsigned long long batch_jobs(uint64_t n_paths, unsigned long long per_path, unsigned long long limit = 0) {
     unsigned long long c = (unsigned long long)n_paths * per_path * 2ull;
     if (c < (1ull << 20)) c = 1ull << 20;
     if (c > (1ull << 27)) c = 1ull << 27;
+    if (limit && c > limit) c = limit;  // vrt_set_wave_batch_limit: a smaller footprint, more rounds
     return c;
 }
 

@@ -185,8 +185,17 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                             jfork = rng.ntr;
                             rng.ntr += (uint32_t)lights;
                             const bool capped = M.max_bounces > 0 && bounces + 1 >= M.max_bounces;
-                            // an uncapped path at the pass's vertex budget goes to the state machine
-                            const bool at_budget = wv.kpass > 0 && bounces + 1 >= wv.kpass;
+                            // an uncapped path past the pass's vertex budget goes on while the
+                            // buffers hold every lane's worst case plus one more vertex per lane
+                            // (at most one such approval per lane is ever outstanding); else it
+                            // goes to the state machine
+                            bool at_budget = wv.kpass > 0 && bounces + 1 >= wv.kpass;
+                            if (at_budget) {
+                                const unsigned long long uj = *((volatile unsigned long long*)&wv.hdr[0]);
+                                const unsigned long long ur = *((volatile unsigned long long*)&wv.hdr[1]);
+                                at_budget = !(uj + wv.res_jobs + wv.lanes * (unsigned long long)lights <= wv.cap_jobs &&
+                                              ur + wv.res_recs + wv.lanes * 2ull <= wv.cap_recs);
+                            }
                             float3 wo = w;
                             if (!capped && !at_budget) wo = phase_sample(M, rng, w);
                             rsp = null_W < EPS;
@@ -595,14 +604,14 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     // room for three vertex records per path (the NEE_DS primal's majorant and
     // epsilon collisions make more vertices than the forward's: 2.3 per path
     // on the benchmark medium)
-    wv.cap_jobs = wv.res_jobs + batch_jobs(n_paths, 3ull * lights);
-    wv.cap_recs = wv.res_recs + batch_jobs(n_paths, 3);
+    wv.cap_jobs = wv.res_jobs + batch_jobs(n_paths, 3ull * lights, ctx->batch_limit);
+    wv.cap_recs = wv.res_recs + batch_jobs(n_paths, 3, ctx->batch_limit);
     if (wv.cap_recs > (1ull << 30)) return VRT_E_UNSUPPORTED;  // record indices are 30-bit in a job
     wv.cap_paths = (n_paths < (1ull << 24) ? n_paths : (1ull << 24)) + wv.lanes;
     // the collision log: room for about four collisions per vertex record of a
     // round, and admission of new paths stops while less than 16 collisions per
     // lane in flight are left; a path that still finds it full is re-walked
-    wv.cap_evs = ctx->log_limit ? ctx->log_limit : 4ull * batch_jobs(n_paths, 1) + inflight * 16ull;
+    wv.cap_evs = ctx->log_limit ? ctx->log_limit : 4ull * batch_jobs(n_paths, 1, ctx->batch_limit) + inflight * 16ull;
     if (wv.cap_evs > 0xfff00000ull) wv.cap_evs = 0xfff00000ull;  // 32-bit links, kNone / kUnlogged reserved
     wv.res_evs = inflight * 16ull < wv.cap_evs / 2 ? inflight * 16ull : wv.cap_evs / 2;
     const size_t o_jobs = 256, o_dldt = o_jobs + wv.cap_jobs * sizeof(ShadowJob);

@@ -158,38 +158,52 @@ def test_dda_workload_adjoint_matches_fp64_central_differences(cuda):
 
 
 def test_uncapped_paths_run_on_the_wavefront(cuda):
-    """The reference's default (no bounce cap) runs on the wavefront kernels: in
-    a dense, high-albedo medium many paths outlive the 64-vertex pass, so the
-    forward resumes them in later rounds and the NEE_DS adjoint hands them to
-    the state machine -- image and gradients still match the oracle's
-    uncapped paths."""
+    """The reference's default (no bounce cap) runs on the wavefront kernels.  In
+    a dense, high-albedo medium many paths outlive the 64-vertex pass: with the
+    automatic buffers they go on in place; with a round capped at 4096 items
+    the forward saves and resumes them in later rounds and the NEE_DS adjoint
+    hands them to the state machine.  Image and gradients match the oracle's
+    uncapped paths either way."""
     from rendervous_b200 import _lib
     from tests.helpers import build_field, front_camera
     ffi, lib = _lib.ffi_lib()
     ctx = _lib.context(cuda)
     stream = _lib.stream_handle(cuda)
     sig = torch.from_numpy(synthetic.gaussian_blobs(33, 6, 80.0, seed=4)).to(cuda)
-    alb = torch.nn.Parameter(torch.full((33, 33, 33, 3), 0.985, device=cuda))
-    field = build_field(sig, albedo_grid=alb, env=1.0, sun_dir=(0.3, 0.8, 0.5), sun_radiance=2.0, g=0.3,
-                        max_bounces=0, majorant="grid", brick=4, sigma_requires_grad=True)
     H = W = 24
     cam = maps.PerspectiveCameraSensor(W, H, front_camera(1).to(cuda), jittered=True)
+    dimg = torch.from_numpy(np.random.default_rng(6).random((1, H, W, 3)).astype(np.float32)).to(cuda)
     ks = ffi.new("vrt_kernel_stat[]", lib.VRT_K_COUNT)
-    maps.check()
-    _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
-    img = cam.capture(field, fw_samples=4, bw_samples=4, seed=21)
-    dimg = torch.from_numpy(np.random.default_rng(6).random(img.shape).astype(np.float32)).to(cuda)
-    (img * dimg).sum().backward()
-    maps.check()
-    _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
-    assert ks[lib.VRT_K_WALK_FW].launches >= 2          # more than one round: paths were resumed
-    assert ks[lib.VRT_K_DS_PRIMAL].launches >= 1
-    sc = oracle.OracleScene(field.lower().to_numpy(), with_grads=True)
+    runs = []
+    for limit in (0, 4096):
+        alb = torch.nn.Parameter(torch.full((33, 33, 33, 3), 0.985, device=cuda))
+        field = build_field(sig, albedo_grid=alb, env=1.0, sun_dir=(0.3, 0.8, 0.5), sun_radiance=2.0, g=0.3,
+                            max_bounces=0, majorant="grid", brick=4, sigma_requires_grad=True)
+        _lib.check(lib.vrt_set_wave_batch_limit(ctx.ptr, limit))
+        try:
+            maps.check()
+            _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
+            img = cam.capture(field, fw_samples=4, bw_samples=4, seed=21)
+            (img * dimg).sum().backward()
+            maps.check()
+            _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
+        finally:
+            _lib.check(lib.vrt_set_wave_batch_limit(ctx.ptr, 0))
+        runs.append((img.detach().cpu().numpy(), field.sigma.grid.grad.cpu().numpy(), alb.grad.cpu().numpy(),
+                     ks[lib.VRT_K_WALK_FW].launches, ks[lib.VRT_K_DS_PRIMAL].launches))
+    assert runs[0][3] >= 1 and runs[0][4] >= 1                 # the wavefront ran
+    assert runs[1][3] >= 2                                     # small rounds: paths were saved and resumed
+    field = build_field(sig, albedo=0.985, env=1.0, sun_dir=(0.3, 0.8, 0.5), sun_radiance=2.0, g=0.3,
+                        max_bounces=0, majorant="grid", brick=4)
+    d = field.lower()
+    d.albedo_grid = torch.full((33, 33, 33, 3), 0.985)
+    sc = oracle.OracleScene(d.to_numpy(), with_grads=True)
     ref, cnt = oracle.capture_fw(sc, "nee", front_camera(1).numpy(), W, H, math.pi / 4, True, 4, 21)
     oracle.capture_bw(sc, "ds", front_camera(1).numpy(), W, H, math.pi / 4, True, 4, 21, dimg.cpu().numpy())
-    assert cnt["vertices"] > 64 * 50                    # long paths exist
-    close = np.isclose(img.detach().cpu().numpy(), ref, rtol=1e-3, atol=1e-5).all(axis=-1)
-    assert close.mean() >= 0.98, close.mean()
-    for g, rg in ((field.sigma.grid.grad, sc.sigma_grad), (alb.grad, sc.albedo_grad)):
-        rel = np.abs(g.cpu().numpy() - rg).sum() / max(np.abs(rg).sum(), 1e-30)
-        assert rel < 2e-2, rel
+    assert cnt["vertices"] > 64 * 50                            # long paths exist
+    for img, gs, ga, _, _ in runs:
+        close = np.isclose(img, ref, rtol=1e-3, atol=1e-5).all(axis=-1)
+        assert close.mean() >= 0.98, close.mean()
+        for g, rg in ((gs, sc.sigma_grad), (ga, sc.albedo_grad)):
+            rel = np.abs(g - rg).sum() / max(np.abs(rg).sum(), 1e-30)
+            assert rel < 2e-2, rel
