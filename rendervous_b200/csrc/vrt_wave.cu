@@ -413,33 +413,42 @@ __global__ void __launch_bounds__(256, 4) k_shadow_run(DMedium M, PathSrc S, con
     flush_counters(sc, OUT == OUT_IMAGE ? VRT_K_SHADOW_FW : VRT_K_SHADOW_T, 0, 0, tl);
 }
 
-// The transmittance adjoint (vr_transmittance_RT.h:51-141 / _DT.h:30-90): the
-// first pass runs as events and keeps its tracking collisions; the second pass
-// of the reference replays the same draws and scatters at exactly those
-// points, so the scatter is done from the kept list once the first pass's
-// estimate is known.  A ray with more than kKeep collisions replays its
-// second pass as events instead.
+// A transmittance adjoint keeps the tracking collisions of its first pass (at
+// most kKeep) and scatters from them once that pass's estimate is known (the
+// reference's second pass replays exactly those points); a ray with more
+// collisions replays its second pass as events instead.
 constexpr int kKeep = 16;
 
+// The NEE_DS adjoint's light jobs, fused: the job's transmittance (the
+// primal's T, into its vertex record and weight * T into its path's R / Rsp),
+// then at once its transmittance adjoint (vr_transmittance_RT.h:51-141 /
+// _DT.h:30-90, first pass as events keeping its collisions, the scatter from
+// the kept list).  dL/dT of a light job is dL/dR of its pixel (/ div) dotted
+// with the job's weight W * L * phase -- the operands the log replay
+// recomputes for the vertex bit for bit -- so the adjoint needs neither the replay nor a
+// second pass over the jobs, and it walks the ray while the forward walk's
+// sigma lines are still in L2.  Jobs of paths handed to the state machine
+// (their first-collision word kSpilled) get no adjoint here.
 template <int TR>
-__global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, const ShadowJob* __restrict__ jobs,
-                                                     const float* __restrict__ dldt,
-                                                     const unsigned long long* __restrict__ count,
-                                                     unsigned long long cap, unsigned long long* head, uint64_t seed,
-                                                     DScratch* sc) {
+__global__ void __launch_bounds__(256, 4) k_shadow_fused(DMedium M, PathSrc S, const ShadowJob* __restrict__ jobs,
+                                                       const unsigned long long* __restrict__ count,
+                                                       unsigned long long cap, unsigned long long* head, uint64_t seed,
+                                                       ShadowOut so, const float* __restrict__ dL, float div,
+                                                       DScratch* sc) {
     unsigned long long n = *count;
     if (n > cap) n = cap;
     ShadowRay s;
     JobView jv;
     float4 keep[kKeep];  // position, majorant
     float keepf[kKeep];  // RT: r; DT: Pc
-    int nkeep = 0, phase = 0;  // 0 idle, 1 first pass, 2 second pass (more than kKeep collisions)
-    float outT = 0.0f;
+    int nkeep = 0, phase = 0;  // 0 idle, 1 T, 2 adjoint first pass, 3 adjoint second pass (> kKeep collisions)
+    float outT = 0.0f, dLdT = 0.0f;
     bool exhausted = false;
     WarpQueue wq;
     Tally tl;
     while (true) {
         const unsigned want = __ballot_sync(kAll, phase == 0 && !exhausted);
+        bool start_adj = false;
         if (want) {
             unsigned long long i;
             const bool got = wq.take(head, n, 64, want, i);  // 64 jobs per warp and atomic
@@ -448,19 +457,26 @@ __global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, const ShadowJo
                     exhausted = wq.drained;
                 } else {
                     jv = get_job(jobs, i);
-                    jv.wt.x = dldt[i];  // the replay's dL/dT (0: no adjoint for this ray)
-                    nkeep = 0;
-                    if (jv.wt.x != 0.0f && shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork)) phase = 1;
+                    if (shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork)) {
+                        phase = 1;
+                    } else {
+                        shadow_finish<OUT_RECORD>(S, so, jv, 1.0f);
+                        start_adj = true;
+                    }
                 }
             }
         }
         if (__all_sync(kAll, phase == 0 && exhausted)) break;
-        if (phase != 0) {
-            bool hit;
-            float hm, hf;
+        bool hit;
+        float hm, hf;
+        if (phase == 1) {
+            if (shadow_event<TR, false>(M, s, tl, sc, hit, hm, hf)) {
+                shadow_finish<OUT_RECORD>(S, so, jv, s.T);
+                start_adj = true;
+            }
+        } else if (phase >= 2) {
             const bool done = shadow_event<TR, true>(M, s, tl, sc, hit, hm, hf);
-            const float dLdT = jv.wt.x;
-            if (phase == 1) {
+            if (phase == 2) {
                 if (hit) {
                     if (nkeep < kKeep) {
                         keep[nkeep] = make_float4(s.x.x, s.x.y, s.x.z, hm);
@@ -482,7 +498,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, const ShadowJo
                         phase = 0;
                     } else {  // replay the second pass
                         shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork);
-                        phase = 2;
+                        phase = 3;
                     }
                 }
             } else {
@@ -493,8 +509,21 @@ __global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, const ShadowJo
                 if (done) phase = 0;
             }
         }
+        if (start_adj) {
+            phase = 0;
+            const float* io = so.info + 8 * (jv.pid - so.p_begin);
+            // no adjoint for rays from or after a singular (zero-density) vertex, where the
+            // reference's replay stops (vr_path_integrator_NEE_DS.h:153-154), nor for paths
+            // the state machine runs
+            if (!(jv.tgt & 2u) && __float_as_uint(io[7]) != kSpilled) {
+                const float3 dLdR = ld3(dL + 3 * out_index(S, jv.pid)) / div;
+                dLdT = dot(dLdR, jv.wt);
+                nkeep = 0;
+                if (dLdT != 0.0f && shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork)) phase = 2;
+            }
+        }
     }
-    flush_counters(sc, VRT_K_SHADOW_ADJ, 0, 0, tl);
+    flush_counters(sc, VRT_K_SHADOW_T, 0, 0, tl);
 }
 
 // Host: rounds of walk + shadow until every path has been taken.
@@ -595,9 +624,14 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
     return 0;
 }
 
+// One job per thread for the DDA and grid-tracking forms: T into the record
+// and the path's R / Rsp, then the DDA adjoint with dL/dT as in
+// k_shadow_fused (GRT / GDT have no backward).
 template <int TR>
-__global__ void __launch_bounds__(256, 4) k_shadow_T(DMedium M, WaveBw wv, uint64_t seed, DScratch* sc) {
-    const unsigned long long n = wv.hdr[0];
+__global__ void __launch_bounds__(256, 4) k_shadow_T(DMedium M, PathSrc S, WaveBw wv, uint64_t seed,
+                                                   const float* __restrict__ dL, float div, DScratch* sc) {
+    unsigned long long n = wv.hdr[0];
+    if (n > wv.cap_jobs) n = wv.cap_jobs;
     Tally tl;
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
          i += (unsigned long long)gridDim.x * blockDim.x) {
@@ -609,73 +643,38 @@ __global__ void __launch_bounds__(256, 4) k_shadow_T(DMedium M, WaveBw wv, uint6
         if (jv.tgt & 1u) rp->Ts = T;
         else rp->Te = T;
         const float3 c3 = jv.wt * T;
+        float* io = wv.info + 8 * (jv.pid - wv.p_begin);
         if (c3.x != 0.0f || c3.y != 0.0f || c3.z != 0.0f) {
-            float* io = wv.info + 8 * (jv.pid - wv.p_begin) + ((jv.tgt & 2u) ? 3 : 0);
-            atomicAdd(io + 0, c3.x);
-            atomicAdd(io + 1, c3.y);
-            atomicAdd(io + 2, c3.z);
+            float* o = io + ((jv.tgt & 2u) ? 3 : 0);
+            atomicAdd(o + 0, c3.x);
+            atomicAdd(o + 1, c3.y);
+            atomicAdd(o + 2, c3.z);
+        }
+        if ((TR == 2 || TR == 3) && !(jv.tgt & 2u) && __float_as_uint(io[7]) != kSpilled) {
+            const float dLdT = dot(ld3(dL + 3 * out_index(S, jv.pid)) / div, jv.wt);
+            transmittance_dda_bw<TR == 3>(M, jv.x, jv.dir, dLdT, tl);
         }
     }
     flush_counters(sc, VRT_K_SHADOW_T, 0, 0, tl);
 }
 
-template <int TR>
-__global__ void __launch_bounds__(256, 4) k_shadow_bw(DMedium M, WaveBw wv, uint64_t seed, DScratch* sc) {
-    unsigned long long n = wv.hdr[0];
-    if (n > wv.cap_jobs) n = wv.cap_jobs;
-    Tally tl;
-    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
-         i += (unsigned long long)gridDim.x * blockDim.x) {
-        JobView jv = get_job(wv.jobs, i);
-        jv.wt.x = wv.dldt[i];  // the replay's dL/dT (0: no adjoint for this ray)
-        if (jv.wt.x == 0.0f) continue;
-        Rng r;
-        r.init(seed, jv.pid, 2u * (1u + jv.fork));
-        if (TR == 0) transmittance_rt_bw(M, r, jv.x, jv.dir, jv.wt.x, tl, &sc->status);
-        else if (TR == 1) transmittance_dt_bw(M, r, jv.x, jv.dir, jv.wt.x, tl, &sc->status);
-        else if (TR == 2) transmittance_dda_bw<false>(M, jv.x, jv.dir, jv.wt.x, tl);
-        else transmittance_dda_bw<true>(M, jv.x, jv.dir, jv.wt.x, tl);
-    }
-    flush_counters(sc, VRT_K_SHADOW_ADJ, 0, 0, tl);
-}
-
-int launch_shadow_record(const DMedium& M, const PathSrc& src, const WaveBw& wv, uint64_t seed, DScratch* sc,
-                         int num_sms, cudaStream_t stream) {
+int launch_shadow_record(const DMedium& M, const PathSrc& src, const WaveBw& wv, uint64_t seed, const float* dL,
+                         float div, DScratch* sc, int num_sms, cudaStream_t stream) {
     const ShadowOut so = {nullptr, 0.0f, wv.recs, wv.info, wv.p_begin};
     KernelScope ks(VRT_K_SHADOW_T, stream);
     switch (M.tr_mode) {
         case 0:
-            k_shadow_run<0, OUT_RECORD><<<persistent_blocks((const void*)k_shadow_run<0, OUT_RECORD>, 256, num_sms), 256,
-                                          0, stream>>>(M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[3], seed, so, sc);
+            k_shadow_fused<0><<<persistent_blocks((const void*)k_shadow_fused<0>, 256, num_sms), 256, 0, stream>>>(
+                M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[3], seed, so, dL, div, sc);
             break;
         case 1:
-            k_shadow_run<1, OUT_RECORD><<<persistent_blocks((const void*)k_shadow_run<1, OUT_RECORD>, 256, num_sms), 256,
-                                          0, stream>>>(M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[3], seed, so, sc);
+            k_shadow_fused<1><<<persistent_blocks((const void*)k_shadow_fused<1>, 256, num_sms), 256, 0, stream>>>(
+                M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[3], seed, so, dL, div, sc);
             break;
-        case 2: k_shadow_T<2><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
-        case 3: k_shadow_T<3><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
-        case 4: k_shadow_T<4><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
-        default: k_shadow_T<5><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
-    }
-    count_launches(1);
-    return launch_status(cudaGetLastError());
-}
-
-int launch_shadow_adjoint(const DMedium& M, const WaveBw& wv, uint64_t seed, DScratch* sc, int num_sms,
-                          cudaStream_t stream) {
-    KernelScope ks(VRT_K_SHADOW_ADJ, stream);
-    switch (M.tr_mode) {
-        case 0:
-            k_shadow_adj<0><<<persistent_blocks((const void*)k_shadow_adj<0>, 256, num_sms), 256, 0, stream>>>(
-                M, wv.jobs, wv.dldt, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, sc);
-            break;
-        case 1:
-            k_shadow_adj<1><<<persistent_blocks((const void*)k_shadow_adj<1>, 256, num_sms), 256, 0, stream>>>(
-                M, wv.jobs, wv.dldt, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, sc);
-            break;
-        case 2: k_shadow_bw<2><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
-        case 3: k_shadow_bw<3><<<num_sms * 8, 256, 0, stream>>>(M, wv, seed, sc); break;
-        default: return VRT_OK;  // GRT / GDT shadow rays carry no gradient (no backward in the reference)
+        case 2: k_shadow_T<2><<<num_sms * 8, 256, 0, stream>>>(M, src, wv, seed, dL, div, sc); break;
+        case 3: k_shadow_T<3><<<num_sms * 8, 256, 0, stream>>>(M, src, wv, seed, dL, div, sc); break;
+        case 4: k_shadow_T<4><<<num_sms * 8, 256, 0, stream>>>(M, src, wv, seed, dL, div, sc); break;
+        default: k_shadow_T<5><<<num_sms * 8, 256, 0, stream>>>(M, src, wv, seed, dL, div, sc); break;
     }
     count_launches(1);
     return launch_status(cudaGetLastError());

@@ -256,7 +256,7 @@ __device__ __forceinline__ bool shadow_begin(const DMedium& M, ShadowRay& s, flo
 // factor the adjoint's second pass scatters with (RT: r = 1 - sigma/maj; DT:
 // Pc = sigma/maj).
 constexpr int kCross = 6;    // forward transmittances (k_shadow_run)
-constexpr int kCrossBw = 8;  // the transmittance adjoint's first pass (k_shadow_adj)
+constexpr int kCrossBw = 8;  // the transmittance adjoint's first pass (k_shadow_fused)
 // The same bound for the path walks (measured per kernel): a flight that needs
 // more brick crossings leaves the crossing loop without an event and resumes
 // in the next iteration, so the warp's long flights do not hold the others.
@@ -354,6 +354,7 @@ __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tal
 
 constexpr uint32_t kNone = 0xffffffffu;
 constexpr uint32_t kUnlogged = 0xfffffffeu;  // a path whose collisions did not fit the log
+constexpr uint32_t kSpilled = 0xfffffffdu;   // a path handed to the state-machine adjoint
 // A real-collision vertex of the NEE_DS primal (48 bytes): its two shadow
 // transmittances (filled by the shadow kernel), the next vertex of the same
 // path, the slot of its environment job (the sun job follows it), and what the
@@ -381,7 +382,6 @@ static_assert(sizeof(CollisionRec) == 32, "collision records are two 16-byte wor
 // Buffers of one round of the NEE_DS adjoint wavefront (vrt_wave_ds.cu).
 struct WaveBw {
     ShadowJob* jobs;
-    float* dldt;               // per job slot: dL/dT from the replay (0: no transmittance adjoint)
     VertexRec* recs;
     CollisionRec* evs;         // the collision log
     float* info;               // per path: R (3), Rsp (3), first record, first collision (or kUnlogged)
@@ -405,13 +405,11 @@ struct WaveBw {
 
 }  // namespace wave
 
-// Shadow kernels of the NEE_DS adjoint rounds (defined in vrt_wave.cu, so they
+// The light jobs of the NEE_DS adjoint rounds (defined in vrt_wave.cu, so they
 // are compiled with the forward's floating-point contraction): T of the
-// primal's jobs into their vertex records and paths (head: hdr[3]), and the
-// transmittance adjoints of the same jobs with the replay's dL/dT (head: hdr[4]).
-int launch_shadow_record(const DMedium& M, const PathSrc& src, const wave::WaveBw& wv, uint64_t seed, DScratch* sc,
-                         int num_sms, cudaStream_t stream);
-int launch_shadow_adjoint(const DMedium& M, const wave::WaveBw& wv, uint64_t seed, DScratch* sc, int num_sms,
-                          cudaStream_t stream);
+// primal's jobs into their vertex records and paths, and their transmittance
+// adjoints with dL/dT = dL/dR(pixel) / div . weight (head: hdr[3]).
+int launch_shadow_record(const DMedium& M, const PathSrc& src, const wave::WaveBw& wv, uint64_t seed, const float* dL,
+                         float div, DScratch* sc, int num_sms, cudaStream_t stream);
 
 }  // namespace vrt

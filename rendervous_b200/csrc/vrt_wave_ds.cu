@@ -22,21 +22,22 @@ using namespace wave;
 // collision and a 48-byte vertex record per scattering vertex; a vertex's
 // shadow transmittances are computed once into its record, and the
 // transmittance adjoints (which feed nothing back into the path) run over the
-// primal's light jobs (same rays, same forks) with the replay's dL/dT:
+// primal's light jobs (same rays, same forks) right after their T:
 //
 //   A k_ds_primal   the primal walk: per tracking collision a collision record,
 //                   per real collision a vertex record (both linked per path)
 //                   and a T job per light; per path the emission and escape
 //                   terms of R and Rsp
 //   B (vrt_wave.cu) T of each job into its record, weight * T into its
-//                   path's R (or Rsp after a zero-density collision)
+//                   path's R (or Rsp after a zero-density collision), then the
+//                   job's transmittance adjoint (ratio / delta tracking or
+//                   DDA) with dL/dT = dL/dR(pixel) / div . weight -- from the
+//                   operands the replay would use for the vertex; none from
+//                   or after a singular vertex, where the replay stops
 //   C k_ds_replay   the replay from the log: dL/dsigma at every collision,
-//                   dL/dalbedo at real ones, the R bookkeeping from the stored
-//                   T, and dL/dT of each light ray into its job slot
+//                   dL/dalbedo at real ones, the R bookkeeping from the stored T
 //     k_ds_rewalk   the same for the paths the log had no room for, by walking
 //                   them again with the primal's draws
-//   D (vrt_wave.cu) the ratio / delta tracking adjoint or the DDA adjoint of
-//                   each job with dL/dT != 0
 //
 // Rounds bound the buffers as in the forward wavefront.
 // ------------------------------------------------------------------------
@@ -269,8 +270,9 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
             const uint64_t k = pid - wv.p_begin;
             float* io = wv.info + 8 * k;
             __stcs(reinterpret_cast<float4*>(io), make_float4(Racc.x, Racc.y, Racc.z, Rspacc.x));
-            __stcs(reinterpret_cast<float4*>(io) + 1, make_float4(Rspacc.y, Rspacc.z, __uint_as_float(first),
-                                                                  __uint_as_float(logged ? first_ev : kUnlogged)));
+            __stcs(reinterpret_cast<float4*>(io) + 1,
+                   make_float4(Rspacc.y, Rspacc.z, __uint_as_float(first),
+                               __uint_as_float(spilled ? kSpilled : (logged ? first_ev : kUnlogged))));
             // an entry whose last collision found the log full is skipped by the replay
             if (nl) __stcs(wv.list + sl.s3, make_uint4((uint32_t)k, logged ? first_ev : kUnlogged, n_ev, 0u));
             if (spilled) {  // its records are ignored; the state machine runs the whole path
@@ -409,7 +411,6 @@ __global__ void __launch_bounds__(256, 3) k_ds_rewalk(DMedium M, PathSrc S, uint
                             const float3 wo = phase_sample(M, rng, w);
                             W = W * sa;
                             float Te = 1.0f, Ts = 1.0f;
-                            uint32_t job = 0;
                             if (cur == kNone) {
                                 guard(sc, 5);  // the replay left the primal's path
                                 ev = 2;
@@ -417,18 +418,12 @@ __global__ void __launch_bounds__(256, 3) k_ds_rewalk(DMedium M, PathSrc S, uint
                                 const VertexRec rec = wv.recs[cur];
                                 Te = rec.Te;
                                 Ts = rec.Ts;
-                                job = rec.job;
                                 cur = rec.next;
                             }
                             if (ev != 2) {
-                                const float dTe = dot(dLdR, W * Le * ph_nee);
+                                // (the light rays' transmittance adjoints run with the T jobs)
                                 R = R - W * Te * Le * ph_nee;
-                                if (dTe != 0.0f) wv.dldt[job] = dTe;  // into the primal's job slots
-                                if (M.has_sun) {
-                                    const float dTs = dot(dLdR, W * M.sun_L * ph_sun);
-                                    R = R - W * Ts * M.sun_L * ph_sun;
-                                    if (dTs != 0.0f) wv.dldt[job + 1] = dTs;
-                                }
+                                if (M.has_sun) R = R - W * Ts * M.sun_L * ph_sun;
                                 ++bounces;
                                 if ((M.max_bounces > 0 && bounces >= M.max_bounces) || all_less(W, EPS)) {
                                     ev = 2;
@@ -557,16 +552,9 @@ __global__ void __launch_bounds__(256, 3) k_ds_replay(DMedium M, PathSrc S, cons
                     dL_dsa = dL_dsa + dLdR * R / make_float3(gmax(EPS, sa.x), gmax(EPS, sa.y), gmax(EPS, sa.z));
                     albedo_bw(M, x, dL_dsa, tl);
                     W = W * sa;
-                    // dL/dT of the vertex's light rays into their primal job slots
-                    const uint32_t job = r0.w;
-                    const float dTe = dot(dLdR, W * Le * ph_nee);
+                    // the vertex's light rays (their transmittance adjoints ran with the T jobs)
                     R = R - W * Te * Le * ph_nee;
-                    if (dTe != 0.0f) wv.dldt[job] = dTe;
-                    if (M.has_sun) {
-                        const float dTs = dot(dLdR, W * M.sun_L * ph_sun);
-                        R = R - W * Ts * M.sun_L * ph_sun;
-                        if (dTs != 0.0f) wv.dldt[job + 1] = dTs;
-                    }
+                    if (M.has_sun) R = R - W * Ts * M.sun_L * ph_sun;
                     ++bounces;
                     if ((M.max_bounces > 0 && bounces >= M.max_bounces) || all_less(W, EPS)) end = true;
                 }
@@ -614,8 +602,7 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     wv.cap_evs = ctx->log_limit ? ctx->log_limit : 4ull * batch_jobs(n_paths, 1, ctx->batch_limit) + inflight * 16ull;
     if (wv.cap_evs > 0xfff00000ull) wv.cap_evs = 0xfff00000ull;  // 32-bit links, kNone / kUnlogged reserved
     wv.res_evs = inflight * 16ull < wv.cap_evs / 2 ? inflight * 16ull : wv.cap_evs / 2;
-    const size_t o_jobs = 256, o_dldt = o_jobs + wv.cap_jobs * sizeof(ShadowJob);
-    const size_t o_recs = o_dldt + ((wv.cap_jobs * 4 + 255) & ~(size_t)255);
+    const size_t o_jobs = 256, o_recs = o_jobs + wv.cap_jobs * sizeof(ShadowJob);
     const size_t o_info = o_recs + wv.cap_recs * sizeof(VertexRec), o_over = o_info + wv.cap_paths * 32;
     const size_t o_list = o_over + ((wv.cap_paths * 4 + 255) & ~(size_t)255);
     const size_t o_evs = o_list + ((wv.cap_paths * 16 + 255) & ~(size_t)255);
@@ -627,7 +614,6 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     char* base = static_cast<char*>(ctx->wave);
     wv.hdr = reinterpret_cast<unsigned long long*>(base);
     wv.jobs = reinterpret_cast<ShadowJob*>(base + o_jobs);
-    wv.dldt = reinterpret_cast<float*>(base + o_dldt);
     wv.recs = reinterpret_cast<VertexRec*>(base + o_recs);
     wv.info = reinterpret_cast<float*>(base + o_info);
     wv.over = reinterpret_cast<uint32_t*>(base + o_over);
@@ -649,11 +635,8 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
             KernelScope ks(VRT_K_DS_PRIMAL, stream);
             k_ds_primal<<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
         }
-        if ((st = launch_shadow_record(M, src, wv, seed, ctx->scratch, ctx->num_sms, stream))) return st;
-        // dL/dT per job slot of the round: the replays fill in the vertices they redo; the
-        // transmittance adjoints then run over the primal's jobs and skip the zeros
-        if ((e = cudaMemsetAsync(wv.dldt, 0, wv.cap_jobs * sizeof(float), stream)) != cudaSuccess)
-            return launch_status(e);
+        // the primal's light jobs: T into the records and paths, and the transmittance adjoints
+        if ((st = launch_shadow_record(M, src, wv, seed, dL, div, ctx->scratch, ctx->num_sms, stream))) return st;
         {
             KernelScope ks(VRT_K_DS_REPLAY, stream);
             k_ds_replay<<<blocksC, 256, 0, stream>>>(M, src, dL, div, ctx->scratch, wv);
@@ -663,7 +646,6 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
             KernelScope ks(VRT_K_DS_REWALK, stream);
             k_ds_rewalk<<<blocksW, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, ctx->scratch, wv);
         }
-        if ((st = launch_shadow_adjoint(M, wv, seed, ctx->scratch, ctx->num_sms, stream))) return st;
         count_launches(3);
         if ((st = launch_status(cudaGetLastError()))) return st;
         unsigned long long taken = 0;
