@@ -46,6 +46,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-c5", action="store_true", help="skip the radiance-cache equal-time comparison")
+    ap.add_argument("--workload", default=WORKLOAD,
+                    choices=[WORKLOAD, "plain_forward_64", "dda_transmittance_256"],
+                    help="the timed workload (default: the differentiable path tracer); the others print "
+                         "their own metric line (1 GPU)")
     ap.add_argument("--small", action="store_true", help="a 128x128, 8 spp image of the same medium (profiling)")
     ap.add_argument("--width", type=int, default=None, help="square image size of the same medium (profiling)")
     ap.add_argument("--spp", type=int, default=None, help="samples per pixel (profiling)")
@@ -503,8 +507,120 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------- other workloads --
+def _timed(fn, steps, warmup, flush):
+    """Device ms per call of fn (CUDA events around each call, L2 flushed before it)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return ts
+
+
+def run_other(args):
+    """The plain forward path tracer (64^3 blobs, 128 x 128, 16 spp, 16 bounces:
+    path vertices/s) or the DDA transmittance operator (256^3 four-octave noise,
+    2^20 rays, forward and backward: rays/s, roofline at 32 B per DDA cell fw
+    and 16 B of atomics per cell bw)."""
+    import torch
+    from rendervous_b200 import _lib, build as vbuild, maps, synthetic
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    vbuild.build()
+    maps.set_sync_checks(False)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    wl = synthetic.WORKLOADS[args.workload]
+    sig = torch.from_numpy(synthetic.make_sigma(wl["sigma"])).to(dev)
+    maps.check()
+    if args.workload == "plain_forward_64":
+        bmin, bmax = maps.normalized_box(sig)
+        sg = maps.Grid3D(sig, bmin, bmax)
+        env = maps.const[wl["env"], wl["env"], wl["env"]]
+        boundary = maps.ray_box_intersection[bmin, bmax]
+        maj = maps.const[[float(sig.max()), 1e6]]
+        g = maps.const[wl["phase_g"]]
+        field = maps.DeltatrackingNEEPathIntegrator(
+            sg, maps.const[wl["albedo"], wl["albedo"], wl["albedo"]], maps.ZERO, env,
+            maps._functionsampler(maps.UniformDirectionSampler(6), env), maps.HenyeyGreensteinPhase(g),
+            maps.HenyeyGreensteinPhaseSampler(g), boundary, maj, maps.RatiotrackingTransmittance(sg, boundary, maj),
+            0.1, max_bounces=wl["max_bounces"],
+            directional_light=maps.DirectionalLight(synthetic.gaussian_direction(wl["sun_seed"]), wl["sun_intensity"]))
+        cam = maps.PerspectiveCameraSensor(wl["width"], wl["height"],
+                                           torch.from_numpy(synthetic.ring_poses(wl["views"])).to(dev), jittered=True)
+        k = {"i": 0}
+
+        def fn():
+            k["i"] += 1
+            cam.capture(field, fw_samples=wl["spp"], seed=k["i"])
+        maps.check()
+        ts = _timed(fn, args.steps, args.warmup, flush)
+        c = maps.check()
+        ms = statistics.mean(ts)
+        per = {key: v / (args.steps + args.warmup) for key, v in c.items() if key != "status"}
+        line = {"metric": "vertices/s fwd", "value": per["vertices"] / (ms / 1e3), "unit": "path vertices/s",
+                "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup, "n_gpus": 1, "higher_is_better": True,
+                "dtype": "f32", "data": "synthetic (seeded generators)",
+                "config": {"workload": args.workload, "grid": [64, 64, 64], "image": [wl["height"], wl["width"]],
+                           "spp": wl["spp"], "max_bounces": wl["max_bounces"], "majorant": "constant (reference)",
+                           "transmittance": "ratio tracking", "l2": "flushed between steps (512 MB write)"},
+                "counters_per_step": per,
+                "roofline": {"bound": "hbm", "achieved": 32.0 * per["lookups"] / (ms / 1e3) / 1e9,
+                             "peak": measured_peaks()["hbm_gbs"], "unit": "GB/s",
+                             "note": "32 B per sigma lookup over the whole forward (walk + shadow kernels)"}}
+    else:
+        bmin, bmax = maps.normalized_box(sig)
+        sp = torch.nn.Parameter(sig)
+        tr = maps.GridDDATransmittance(maps.Grid3D(sp, bmin, bmax), maps.ray_box_intersection[bmin, bmax])
+        rays = torch.from_numpy(synthetic.sphere_rays(wl["n_rays"], seed=wl["ray_seed"])).to(dev)
+        w = torch.from_numpy(synthetic.uniform_weights(wl["n_rays"], wl["weight_seed"])).to(dev)
+        res = {}
+
+        def fw():
+            res["T"] = tr(rays)
+
+        def fwbw():
+            sp.grad = None
+            ((tr(rays)[:, 0]) * w).sum().backward()
+        maps.check()
+        t_fw = statistics.mean(_timed(fw, args.steps, args.warmup, flush))
+        c_fw = maps.check()
+        t_all = statistics.mean(_timed(fwbw, args.steps, args.warmup, flush))
+        c_all = maps.check()
+        n_calls = args.steps + args.warmup
+        cells = c_fw["lookups"] / n_calls
+        reds_bw = c_all["reds"] / n_calls
+        t_bw = t_all - t_fw
+        peak = measured_peaks()["hbm_gbs"]
+        line = {"metric": "rays/s fwd+bwd", "value": wl["n_rays"] / (t_all / 1e3), "unit": "rays/s",
+                "ms_per_step": t_all, "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
+                "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded generators)",
+                "config": {"workload": args.workload, "grid": [256, 256, 256], "rays": wl["n_rays"],
+                           "rule": "midpoint (reference)", "l2": "flushed between calls (512 MB write)"},
+                "fw": {"ms": t_fw, "cells_per_ray": cells / wl["n_rays"], "cells_per_s": cells / (t_fw / 1e3),
+                       "gbs": 32.0 * cells / (t_fw / 1e3) / 1e9, "frac": 32.0 * cells / (t_fw / 1e3) / 1e9 / peak},
+                "bw": {"ms": t_bw, "reds": reds_bw, "gbs": 4.0 * reds_bw / (t_bw / 1e3) / 1e9,
+                       "frac": 4.0 * reds_bw / (t_bw / 1e3) / 1e9 / peak,
+                       "note": "the backward call re-marches for T (32 B per cell) and scatters 4 atomic adds per cell"},
+                "roofline": {"bound": "hbm", "kernel": "k_transmittance_fw<2>",
+                             "achieved": 32.0 * cells / (t_fw / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": 32.0 * cells / (t_fw / 1e3) / 1e9 / peak}}
+    print(json.dumps(line))
+
+
 if __name__ == "__main__":
     a = parse()
+    if a.impl == "ours" and a.workload != WORKLOAD:
+        run_other(a)
+        sys.exit(0)
     if a.impl == "reference":
         run_reference(a)
     else:

@@ -413,42 +413,39 @@ __global__ void __launch_bounds__(256, 4) k_shadow_run(DMedium M, PathSrc S, con
     flush_counters(sc, OUT == OUT_IMAGE ? VRT_K_SHADOW_FW : VRT_K_SHADOW_T, 0, 0, tl);
 }
 
-// A transmittance adjoint keeps the tracking collisions of its first pass (at
-// most kKeep) and scatters from them once that pass's estimate is known (the
-// reference's second pass replays exactly those points); a ray with more
-// collisions replays its second pass as events instead.
-constexpr int kKeep = 16;
+constexpr int kKeep = 16;  // first-pass collisions a transmittance adjoint keeps (k_shadow_adj)
 
-// The NEE_DS adjoint's light jobs, fused: the job's transmittance (the
-// primal's T, into its vertex record and weight * T into its path's R / Rsp),
-// then at once its transmittance adjoint (vr_transmittance_RT.h:51-141 /
-// _DT.h:30-90, first pass as events keeping its collisions, the scatter from
-// the kept list).  dL/dT of a light job is dL/dR of its pixel (/ div) dotted
-// with the job's weight W * L * phase -- the operands the log replay
-// recomputes for the vertex bit for bit -- so the adjoint needs neither the replay nor a
-// second pass over the jobs, and it walks the ray while the forward walk's
-// sigma lines are still in L2.  Jobs of paths handed to the state machine
-// (their first-collision word kSpilled) get no adjoint here.
+// The transmittance adjoints of the NEE_DS primal's light jobs
+// (vr_transmittance_RT.h:51-141 / _DT.h:30-90): the first pass runs as events
+// and keeps its tracking collisions; the reference's second pass replays the
+// same draws and scatters at exactly those points, so the scatter is done from
+// the kept list once the first pass's estimate is known (a ray with more than
+// kKeep collisions replays its second pass as events instead).  dL/dT of a
+// light job is dL/dR of its pixel (/ div) dotted with the job's weight
+// W * L * phase -- the operands the log replay recomputes for the vertex bit
+// for bit -- so this kernel needs nothing from the replay.  No adjoint runs
+// for rays from or after a singular (zero-density) vertex, where the
+// reference's replay stops (vr_path_integrator_NEE_DS.h:153-154), nor for
+// paths the state machine runs (first-collision word kSpilled).
 template <int TR>
-__global__ void __launch_bounds__(256, 4) k_shadow_fused(DMedium M, PathSrc S, const ShadowJob* __restrict__ jobs,
-                                                       const unsigned long long* __restrict__ count,
-                                                       unsigned long long cap, unsigned long long* head, uint64_t seed,
-                                                       ShadowOut so, const float* __restrict__ dL, float div,
-                                                       DScratch* sc) {
+__global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, PathSrc S, const ShadowJob* __restrict__ jobs,
+                                                     const unsigned long long* __restrict__ count,
+                                                     unsigned long long cap, unsigned long long* head, uint64_t seed,
+                                                     const float* __restrict__ info, uint64_t p_begin,
+                                                     const float* __restrict__ dL, float div, DScratch* sc) {
     unsigned long long n = *count;
     if (n > cap) n = cap;
     ShadowRay s;
     JobView jv;
     float4 keep[kKeep];  // position, majorant
     float keepf[kKeep];  // RT: r; DT: Pc
-    int nkeep = 0, phase = 0;  // 0 idle, 1 T, 2 adjoint first pass, 3 adjoint second pass (> kKeep collisions)
+    int nkeep = 0, phase = 0;  // 0 idle, 1 first pass, 2 second pass (more than kKeep collisions)
     float outT = 0.0f, dLdT = 0.0f;
     bool exhausted = false;
     WarpQueue wq;
     Tally tl;
     while (true) {
         const unsigned want = __ballot_sync(kAll, phase == 0 && !exhausted);
-        bool start_adj = false;
         if (want) {
             unsigned long long i;
             const bool got = wq.take(head, n, 64, want, i);  // 64 jobs per warp and atomic
@@ -457,26 +454,20 @@ __global__ void __launch_bounds__(256, 4) k_shadow_fused(DMedium M, PathSrc S, c
                     exhausted = wq.drained;
                 } else {
                     jv = get_job(jobs, i);
-                    if (shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork)) {
-                        phase = 1;
-                    } else {
-                        shadow_finish<OUT_RECORD>(S, so, jv, 1.0f);
-                        start_adj = true;
-                    }
+                    dLdT = 0.0f;
+                    if (!(jv.tgt & 2u) && __float_as_uint(info[8 * (jv.pid - p_begin) + 7]) != kSpilled)
+                        dLdT = dot(ld3(dL + 3 * out_index(S, jv.pid)) / div, jv.wt);
+                    nkeep = 0;
+                    if (dLdT != 0.0f && shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork)) phase = 1;
                 }
             }
         }
         if (__all_sync(kAll, phase == 0 && exhausted)) break;
-        bool hit;
-        float hm, hf;
-        if (phase == 1) {
-            if (shadow_event<TR, false>(M, s, tl, sc, hit, hm, hf)) {
-                shadow_finish<OUT_RECORD>(S, so, jv, s.T);
-                start_adj = true;
-            }
-        } else if (phase >= 2) {
+        if (phase != 0) {
+            bool hit;
+            float hm, hf;
             const bool done = shadow_event<TR, true>(M, s, tl, sc, hit, hm, hf);
-            if (phase == 2) {
+            if (phase == 1) {
                 if (hit) {
                     if (nkeep < kKeep) {
                         keep[nkeep] = make_float4(s.x.x, s.x.y, s.x.z, hm);
@@ -498,7 +489,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow_fused(DMedium M, PathSrc S, c
                         phase = 0;
                     } else {  // replay the second pass
                         shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork);
-                        phase = 3;
+                        phase = 2;
                     }
                 }
             } else {
@@ -509,21 +500,8 @@ __global__ void __launch_bounds__(256, 4) k_shadow_fused(DMedium M, PathSrc S, c
                 if (done) phase = 0;
             }
         }
-        if (start_adj) {
-            phase = 0;
-            const float* io = so.info + 8 * (jv.pid - so.p_begin);
-            // no adjoint for rays from or after a singular (zero-density) vertex, where the
-            // reference's replay stops (vr_path_integrator_NEE_DS.h:153-154), nor for paths
-            // the state machine runs
-            if (!(jv.tgt & 2u) && __float_as_uint(io[7]) != kSpilled) {
-                const float3 dLdR = ld3(dL + 3 * out_index(S, jv.pid)) / div;
-                dLdT = dot(dLdR, jv.wt);
-                nkeep = 0;
-                if (dLdT != 0.0f && shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork)) phase = 2;
-            }
-        }
     }
-    flush_counters(sc, VRT_K_SHADOW_T, 0, 0, tl);
+    flush_counters(sc, VRT_K_SHADOW_ADJ, 0, 0, tl);
 }
 
 // Host: rounds of walk + shadow until every path has been taken.
@@ -626,7 +604,7 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
 
 // One job per thread for the DDA and grid-tracking forms: T into the record
 // and the path's R / Rsp, then the DDA adjoint with dL/dT as in
-// k_shadow_fused (GRT / GDT have no backward).
+// k_shadow_adj (GRT / GDT have no backward).
 template <int TR>
 __global__ void __launch_bounds__(256, 4) k_shadow_T(DMedium M, PathSrc S, WaveBw wv, uint64_t seed,
                                                    const float* __restrict__ dL, float div, DScratch* sc) {
@@ -664,18 +642,32 @@ int launch_shadow_record(const DMedium& M, const PathSrc& src, const WaveBw& wv,
     KernelScope ks(VRT_K_SHADOW_T, stream);
     switch (M.tr_mode) {
         case 0:
-            k_shadow_fused<0><<<persistent_blocks((const void*)k_shadow_fused<0>, 256, num_sms), 256, 0, stream>>>(
-                M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[3], seed, so, dL, div, sc);
+            k_shadow_run<0, OUT_RECORD><<<persistent_blocks((const void*)k_shadow_run<0, OUT_RECORD>, 256, num_sms), 256,
+                                          0, stream>>>(M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[3], seed, so, sc);
             break;
         case 1:
-            k_shadow_fused<1><<<persistent_blocks((const void*)k_shadow_fused<1>, 256, num_sms), 256, 0, stream>>>(
-                M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[3], seed, so, dL, div, sc);
+            k_shadow_run<1, OUT_RECORD><<<persistent_blocks((const void*)k_shadow_run<1, OUT_RECORD>, 256, num_sms), 256,
+                                          0, stream>>>(M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[3], seed, so, sc);
             break;
         case 2: k_shadow_T<2><<<num_sms * 8, 256, 0, stream>>>(M, src, wv, seed, dL, div, sc); break;
         case 3: k_shadow_T<3><<<num_sms * 8, 256, 0, stream>>>(M, src, wv, seed, dL, div, sc); break;
         case 4: k_shadow_T<4><<<num_sms * 8, 256, 0, stream>>>(M, src, wv, seed, dL, div, sc); break;
         default: k_shadow_T<5><<<num_sms * 8, 256, 0, stream>>>(M, src, wv, seed, dL, div, sc); break;
     }
+    count_launches(1);
+    return launch_status(cudaGetLastError());
+}
+
+int launch_shadow_adjoint(const DMedium& M, const PathSrc& src, const WaveBw& wv, uint64_t seed, const float* dL,
+                          float div, DScratch* sc, int num_sms, cudaStream_t stream) {
+    if (M.tr_mode > 1) return VRT_OK;  // DDA: in k_shadow_T; GRT / GDT: no backward
+    KernelScope ks(VRT_K_SHADOW_ADJ, stream);
+    if (M.tr_mode == 0)
+        k_shadow_adj<0><<<persistent_blocks((const void*)k_shadow_adj<0>, 256, num_sms), 256, 0, stream>>>(
+            M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, wv.info, wv.p_begin, dL, div, sc);
+    else
+        k_shadow_adj<1><<<persistent_blocks((const void*)k_shadow_adj<1>, 256, num_sms), 256, 0, stream>>>(
+            M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, wv.info, wv.p_begin, dL, div, sc);
     count_launches(1);
     return launch_status(cudaGetLastError());
 }

@@ -256,7 +256,7 @@ __device__ __forceinline__ bool shadow_begin(const DMedium& M, ShadowRay& s, flo
 // factor the adjoint's second pass scatters with (RT: r = 1 - sigma/maj; DT:
 // Pc = sigma/maj).
 constexpr int kCross = 6;    // forward transmittances (k_shadow_run)
-constexpr int kCrossBw = 8;  // the transmittance adjoint's first pass (k_shadow_fused)
+constexpr int kCrossBw = 8;  // the transmittance adjoint's first pass (k_shadow_adj)
 // The same bound for the path walks (measured per kernel): a flight that needs
 // more brick crossings leaves the crossing loop without an event and resumes
 // in the next iteration, so the warp's long flights do not hold the others.
@@ -407,9 +407,12 @@ struct WaveBw {
 
 // The light jobs of the NEE_DS adjoint rounds (defined in vrt_wave.cu, so they
 // are compiled with the forward's floating-point contraction): T of the
-// primal's jobs into their vertex records and paths, and their transmittance
-// adjoints with dL/dT = dL/dR(pixel) / div . weight (head: hdr[3]).
+// primal's jobs into their vertex records and paths (head: hdr[3]; the DDA
+// forms also run the DDA adjoint), and the ratio / delta tracking adjoints of
+// the same jobs with dL/dT = dL/dR(pixel) / div . weight (head: hdr[4]).
 int launch_shadow_record(const DMedium& M, const PathSrc& src, const wave::WaveBw& wv, uint64_t seed, const float* dL,
                          float div, DScratch* sc, int num_sms, cudaStream_t stream);
+int launch_shadow_adjoint(const DMedium& M, const PathSrc& src, const wave::WaveBw& wv, uint64_t seed, const float* dL,
+                          float div, DScratch* sc, int num_sms, cudaStream_t stream);
 
 }  // namespace vrt

@@ -29,11 +29,11 @@ using namespace wave;
 //                   and a T job per light; per path the emission and escape
 //                   terms of R and Rsp
 //   B (vrt_wave.cu) T of each job into its record, weight * T into its
-//                   path's R (or Rsp after a zero-density collision), then the
-//                   job's transmittance adjoint (ratio / delta tracking or
-//                   DDA) with dL/dT = dL/dR(pixel) / div . weight -- from the
-//                   operands the replay would use for the vertex; none from
-//                   or after a singular vertex, where the replay stops
+//                   path's R (or Rsp after a zero-density collision); then
+//                   each job's transmittance adjoint (ratio / delta tracking
+//                   or DDA) with dL/dT = dL/dR(pixel) / div . weight -- from
+//                   the operands the replay would use for the vertex; none
+//                   from or after a singular vertex, where the replay stops
 //   C k_ds_replay   the replay from the log: dL/dsigma at every collision,
 //                   dL/dalbedo at real ones, the R bookkeeping from the stored T
 //     k_ds_rewalk   the same for the paths the log had no room for, by walking
@@ -635,8 +635,9 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
             KernelScope ks(VRT_K_DS_PRIMAL, stream);
             k_ds_primal<<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
         }
-        // the primal's light jobs: T into the records and paths, and the transmittance adjoints
+        // the primal's light jobs: T into the records and paths, then their transmittance adjoints
         if ((st = launch_shadow_record(M, src, wv, seed, dL, div, ctx->scratch, ctx->num_sms, stream))) return st;
+        if ((st = launch_shadow_adjoint(M, src, wv, seed, dL, div, ctx->scratch, ctx->num_sms, stream))) return st;
         {
             KernelScope ks(VRT_K_DS_REPLAY, stream);
             k_ds_replay<<<blocksC, 256, 0, stream>>>(M, src, dL, div, ctx->scratch, wv);
