@@ -171,8 +171,9 @@ def profiled_traffic(kernel: str):
 
 
 KERNELS = ["k_walk_fw", "k_shadow_fw", "k_ds_primal", "k_shadow_T", "k_ds_replay", "k_shadow_adj", "k_ds_rewalk"]
-# the kernel functions each slot covers (ratio-tracking shadows run k_shadow_run / k_shadow_adj)
-KERNEL_FUNCS = {"k_walk_fw": "k_walk_fw", "k_shadow_fw": "k_shadow_run<0, 0>", "k_ds_primal": "k_ds_primal",
+# the kernel functions each slot covers (ratio-tracking shadows run k_shadow_run / k_shadow_adj; the
+# capped walks under a constant environment run the FULL = false instances of the walk kernels)
+KERNEL_FUNCS = {"k_walk_fw": "k_walk_fw<false>", "k_shadow_fw": "k_shadow_run<0, 0>", "k_ds_primal": "k_ds_primal<false>",
                 "k_shadow_T": "k_shadow_run<0, 1>", "k_ds_replay": "k_ds_replay", "k_shadow_adj": "k_shadow_adj<0>",
                 "k_ds_rewalk": "k_ds_rewalk"}
 

@@ -76,6 +76,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
     into one shared library with nvcc."""
     if not force and up_to_date():
         return LIB
+    digest = _digest()  # of the sources as compiled (a file edited during the build leaves the stamp stale)
     os.makedirs(OBJ_DIR, exist_ok=True)
     procs = []
     for src in SOURCES:
@@ -100,7 +101,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
         raise RuntimeError("libvrt link failed:\n" + out.stdout + out.stderr)
     if not extra_flags:
         with open(STAMP, "w") as f:
-            f.write(_digest())
+            f.write(digest)
     return LIB
 
 

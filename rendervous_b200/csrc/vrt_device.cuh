@@ -488,6 +488,21 @@ __device__ __forceinline__ float3 environment_sample(const DMedium& M, Rng& rng,
     return env_radiance(M, wo) * weight;
 }
 
+// The path walks are compiled twice: with IMG false they handle only the
+// constant environment under the uniform direction sampler (the same values as
+// env_radiance / environment_sample give for it), which keeps the image lookup
+// and the quadtree descent out of the kernels that do not need them.
+template <bool IMG>
+__device__ __forceinline__ float3 env_radiance_t(const DMedium& M, float3 w) {
+    return IMG ? env_radiance(M, w) : M.env;
+}
+template <bool IMG>
+__device__ __forceinline__ float3 environment_sample_t(const DMedium& M, Rng& rng, float3& wo) {
+    if (IMG) return environment_sample(M, rng, wo);
+    wo = random_direction_y(rng);
+    return M.env * (4.0f * kPi);
+}
+
 // ---------------------------------------------------------------- camera --
 // include/maps/sensor_perspective_camera.h:1-27
 __device__ __forceinline__ void camera_ray(const DCamera& C, int view, int row, int col, Rng& rng, float3& x, float3& w) {

@@ -60,6 +60,10 @@ struct WaveFw {
     unsigned long long cap_cont, lanes;
 };
 
+// FULL: uncapped passes, the radiance-cache cut and image environments; the
+// host launches the FULL = false instance when the medium and call need none
+// of them.
+template <bool FULL>
 __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, float* out,
                                                   float scale, DScratch* sc, WaveFw wv) {
     const unsigned lane = threadIdx.x & 31u;
@@ -95,12 +99,12 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
             if ((int)lane == leader) {
                 const unsigned long long used = *((volatile unsigned long long*)wv.count);
                 bool room = used + wv.reserve <= wv.cap;
-                if (room && wv.kpass > 0)
+                if (FULL && room && wv.kpass > 0)
                     room = *((volatile unsigned long long*)wv.cout_count) + wv.lanes <= wv.cap_cont;
                 if (!room) {
                     base = ~0ull;
                 } else {
-                    if (wv.n_cin && *((volatile unsigned long long*)wv.cin_head) < wv.n_cin) {
+                    if (FULL && wv.n_cin && *((volatile unsigned long long*)wv.cin_head) < wv.n_cin) {
                         rb = atomicAdd(wv.cin_head, (unsigned long long)nw);
                         if (rb < wv.n_cin) nres = (unsigned)(wv.n_cin - rb < nw ? wv.n_cin - rb : nw);
                     }
@@ -163,13 +167,13 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                     }
                     const uint32_t f = rng.ntr++;
                     if (dslot != ~0ull) {
-                        put_job(wv.jobs, dslot, x, w, env_radiance(M, w), job_key(pid, f));
+                        put_job(wv.jobs, dslot, x, w, env_radiance_t<FULL>(M, w), job_key(pid, f));
                         dslot = ~0ull;
                     } else {
                         njobs = 1;
                         jx = x;
                         jd = w;
-                        jw = env_radiance(M, w);
+                        jw = env_radiance_t<FULL>(M, w);
                         jfork = f;
                     }
                     alive = d > EPS;
@@ -229,7 +233,7 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                 guard(sc, 1);
                 ev = 2;
             }
-            if (ev == 1 && wv.cut >= 0 && bounces == wv.cut) {  // the rest of the path comes from the cache
+            if (FULL && ev == 1 && wv.cut >= 0 && bounces == wv.cut) {  // the rest of the path comes from the cache
                 ++n_verts;
                 float* q = wv.q + 3 * pid;
                 q[0] = x.x; q[1] = x.y; q[2] = x.z;
@@ -242,7 +246,7 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                 Rem = Rem + W * (f3(1.0f) - sa) * M.emission;
                 W = W * sa;
                 float3 wnee;
-                const float3 pay = environment_sample(M, rng, wnee);
+                const float3 pay = environment_sample_t<FULL>(M, rng, wnee);
                 njobs = M.has_sun ? 2 : 1;
                 jx = x;
                 jd = wnee;
@@ -268,7 +272,7 @@ __global__ void __launch_bounds__(256, 4) k_walk_fw(DMedium M, PathSrc S, uint64
                 // an uncapped path past the pass's vertex budget goes on while the job
                 // buffer holds every lane's worst case plus one more vertex per lane;
                 // else it is saved for the next round
-                if (ev == 0 && wv.kpass > 0 && ++pass_verts >= wv.kpass &&
+                if (FULL && ev == 0 && wv.kpass > 0 && ++pass_verts >= wv.kpass &&
                     *((volatile unsigned long long*)wv.count) + wv.reserve + wv.lanes * (unsigned long long)njobs >
                         wv.cap) {
                     const unsigned long long o = atomicAdd(wv.cout_count, 1ull);
@@ -517,7 +521,9 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
     const int kpass = verts == ~0ull ? kUncappedPass : 0;
     if (kpass) verts = (unsigned long long)kpass;
     const unsigned long long per_path = 1ull + lights * verts;
-    int blocks = persistent_blocks((const void*)k_walk_fw, 256, ctx->num_sms);
+    const bool full = kpass > 0 || cut >= 0 || M.env_mode != 0 || M.env_sampler != 0;
+    const void* walk = full ? (const void*)k_walk_fw<true> : (const void*)k_walk_fw<false>;
+    int blocks = persistent_blocks(walk, 256, ctx->num_sms);
     const uint64_t need = (n_paths + 255) / 256;
     if ((uint64_t)blocks > need) blocks = (int)need;
     // the worst case of every path in flight, plus room for a round's expected jobs
@@ -566,7 +572,8 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
             return launch_status(e);
         {
             KernelScope ks(VRT_K_WALK_FW, stream);
-            k_walk_fw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, ctx->scratch, wv);
+            if (full) k_walk_fw<true><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, ctx->scratch, wv);
+            else k_walk_fw<false><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, ctx->scratch, wv);
         }
         {
             KernelScope ks(VRT_K_SHADOW_FW, stream);

@@ -42,6 +42,9 @@ using namespace wave;
 // Rounds bound the buffers as in the forward wavefront.
 // ------------------------------------------------------------------------
 
+// FULL: uncapped passes and image environments (the FULL = false instance
+// serves the capped walks under a constant environment).
+template <bool FULL>
 __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
                                                     DScratch* sc, WaveBw wv) {
     const unsigned lane = threadIdx.x & 31u;
@@ -180,7 +183,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                             sa = albedo(M, x, tl);
                             const float3 acc = W * (f3(1.0f) - sa) * M.emission;
                             W = W * sa;
-                            Le = environment_sample(M, rng, wnee);
+                            Le = environment_sample_t<FULL>(M, rng, wnee);
                             ph_env = phase(M, w, wnee);
                             if (M.has_sun) ph_sun = phase(M, w, M.sun_dir);
                             jfork = rng.ntr;
@@ -190,7 +193,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
                             // buffers hold every lane's worst case plus one more vertex per lane
                             // (at most one such approval per lane is ever outstanding); else it
                             // goes to the state machine
-                            bool at_budget = wv.kpass > 0 && bounces + 1 >= wv.kpass;
+                            bool at_budget = FULL && wv.kpass > 0 && bounces + 1 >= wv.kpass;
                             if (at_budget) {
                                 const unsigned long long uj = *((volatile unsigned long long*)&wv.hdr[0]);
                                 const unsigned long long ur = *((volatile unsigned long long*)&wv.hdr[1]);
@@ -266,7 +269,7 @@ __global__ void __launch_bounds__(256, 3) k_ds_primal(DMedium M, PathSrc S, uint
             if (nj == 2) put_job(wv.jobs, j + 1, x, M.sun_dir, W * M.sun_L * ph_sun, job_key(pid, jfork + 1), tgt | 1u);
         }
         if (finish) {  // end of the primal (_NEE_DS.h:106-110): escape term, then the path's totals
-            if (!scattered) Racc = Racc + env_radiance(M, w) * W;
+            if (!scattered) Racc = Racc + env_radiance_t<FULL>(M, w) * W;
             const uint64_t k = pid - wv.p_begin;
             float* io = wv.info + 8 * k;
             __stcs(reinterpret_cast<float4*>(io), make_float4(Racc.x, Racc.y, Racc.z, Rspacc.x));
@@ -577,7 +580,9 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     const int kpass = M.max_bounces > 0 ? 0 : kUncappedPass;
     const unsigned long long lights = M.has_sun ? 2ull : 1ull;
     const unsigned long long B = (unsigned long long)(M.max_bounces > 0 ? M.max_bounces : kpass);
-    int blocksA = persistent_blocks((const void*)k_ds_primal, 256, ctx->num_sms);
+    const bool full = kpass > 0 || M.env_mode != 0 || M.env_sampler != 0;
+    int blocksA = persistent_blocks(full ? (const void*)k_ds_primal<true> : (const void*)k_ds_primal<false>, 256,
+                                    ctx->num_sms);
     int blocksC = persistent_blocks((const void*)k_ds_replay, 256, ctx->num_sms);
     int blocksW = persistent_blocks((const void*)k_ds_rewalk, 256, ctx->num_sms);
     const uint64_t need = (n_paths + 255) / 256;
@@ -633,7 +638,8 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
             return launch_status(e);
         {
             KernelScope ks(VRT_K_DS_PRIMAL, stream);
-            k_ds_primal<<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
+            if (full) k_ds_primal<true><<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
+            else k_ds_primal<false><<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
         }
         // the primal's light jobs: T into the records and paths, then their transmittance adjoints
         if ((st = launch_shadow_record(M, src, wv, seed, dL, div, ctx->scratch, ctx->num_sms, stream))) return st;
