@@ -170,6 +170,34 @@ def profiled_traffic(kernel: str):
     return None
 
 
+def atomic_peaks(dev, reps: int = 5) -> dict:
+    """Random float atomic adds per second (G/s) over an L2-resident 64 MB
+    buffer (the size of a 256^3 gradient grid) and a 4 GB buffer; scalar adds
+    and x-neighbour pairs by one vector atomic (counted as two adds)."""
+    import torch
+    from rendervous_b200 import _lib
+    ffi, lib = _lib.ffi_lib()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    threads, per_thread = sms * 2048, 64
+    stream = _lib.stream_handle(dev)
+    out = {}
+    for name, nbytes in (("l2", 64 << 20), ("hbm", 4 << 30)):
+        buf = torch.zeros(nbytes // 4, dtype=torch.float32, device=dev)
+        for pairs in (0, 1):
+            args = (ffi.cast("float *", buf.data_ptr()), nbytes // 4, threads, per_thread, pairs)
+            _lib.check(lib.vrt_atomic_peak(*args, 1, stream))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for r in range(reps):
+                _lib.check(lib.vrt_atomic_peak(*args, 2 + r, stream))
+            e1.record()
+            e1.synchronize()
+            adds = threads * per_thread * reps * (2 if pairs else 1)
+            out[name + ("_pairs" if pairs else "")] = adds / (e0.elapsed_time(e1) / 1e3) / 1e9
+        del buf
+    return out
+
+
 KERNELS = ["k_walk_fw", "k_shadow_fw", "k_ds_primal", "k_shadow_T", "k_ds_replay", "k_shadow_adj", "k_ds_rewalk"]
 # the kernel functions each slot covers (ratio-tracking shadows run k_shadow_run / k_shadow_adj; the
 # capped walks under a constant environment run the FULL = false instances of the walk kernels)
@@ -381,6 +409,16 @@ def run_ours(args):
     kd = ktable[kern]
     peaks = measured_peaks()
     gpeaks = gather_peaks(dev)
+    apeaks = atomic_peaks(dev)
+    # the gradient scatter of the log replay against the measured atomic-add rate
+    rp = ktable.get("k_ds_replay")
+    atomics = None
+    if rp and rp["ms_per_step"] > 0:
+        rate = rp["reds_per_step"] / (rp["ms_per_step"] / 1e3) / 1e9
+        atomics = {"kernel": "k_ds_replay", "adds_per_s_g": rate, "peak_g": apeaks,
+                   "frac_of_l2_atomic": rate / apeaks["l2_pairs"],
+                   "note": "float atomic adds (G/s); the replay adds x-neighbour pairs by vector atomics, so the "
+                           "pair figure is its ceiling"}
     achieved = kd["gbs"]
     traffic = profiled_traffic(kern)
 
@@ -462,7 +500,7 @@ def run_ours(args):
                          # whose grids stay in L2 (the kernel's DRAM traffic also holds streaming record
                          # writes, so no HBM-gather fraction is given)
                          "gather_peak_gbs": gpeaks, "frac_of_l2_gather": achieved / gpeaks["l2"],
-                         "split_ms": {k: roof[k]["ms"] for k in roof}},
+                         "split_ms": {k: roof[k]["ms"] for k in roof}, "atomics": atomics},
             "kernels": ktable,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
@@ -601,6 +639,7 @@ def run_other(args):
         reds_bw = c_all["reds"] / n_calls
         t_bw = t_all - t_fw
         peak = measured_peaks()["hbm_gbs"]
+        apeaks = atomic_peaks(dev)
         line = {"metric": "rays/s fwd+bwd", "value": wl["n_rays"] / (t_all / 1e3), "unit": "rays/s",
                 "ms_per_step": t_all, "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
                 "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded generators)",
@@ -610,6 +649,8 @@ def run_other(args):
                        "gbs": 32.0 * cells / (t_fw / 1e3) / 1e9, "frac": 32.0 * cells / (t_fw / 1e3) / 1e9 / peak},
                 "bw": {"ms": t_bw, "reds": reds_bw, "gbs": 4.0 * reds_bw / (t_bw / 1e3) / 1e9,
                        "frac": 4.0 * reds_bw / (t_bw / 1e3) / 1e9 / peak,
+                       "adds_per_s_g": reds_bw / (t_bw / 1e3) / 1e9, "atomic_peak_g": apeaks,
+                       "frac_of_l2_atomic": reds_bw / (t_bw / 1e3) / 1e9 / apeaks["l2"],
                        "note": "the backward call re-marches for T (32 B per cell) and scatters 4 atomic adds per cell"},
                 "roofline": {"bound": "hbm", "kernel": "k_transmittance_fw<2>",
                              "achieved": 32.0 * cells / (t_fw / 1e3) / 1e9, "peak": peak, "unit": "GB/s",

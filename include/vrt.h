@@ -203,6 +203,12 @@ void vrt_set_kernel_timing(int32_t on);
    aligned); the caller times it.  sink: one device uint32 the kernel may write. */
 int vrt_gather_peak(const void* buffer, int64_t bytes, int64_t threads, int32_t per_thread, uint32_t seed,
                     uint32_t* sink, void* stream);
+/* Atomic-add microbenchmark (the roofline of the gradient scatters): threads x
+   per_thread float atomic adds of 1/2^20 at random words of `buffer` (n floats,
+   4-byte aligned); pairs != 0 adds x-neighbour pairs with one vector atomic
+   (two adds each).  The caller times it; buffer's contents change. */
+int vrt_atomic_peak(float* buffer, int64_t n, int64_t threads, int32_t per_thread, int32_t pairs, uint32_t seed,
+                    void* stream);
 int vrt_kernel_stats(vrt_context* ctx, void* stream, vrt_kernel_stat* out);
 int32_t vrt_version(void);
 

@@ -143,6 +143,31 @@ __global__ void __launch_bounds__(256) k_gather_peak(const uint4* __restrict__ b
     if (acc == 0x9e3779b9u) atomicAdd(sink, 1u);
 }
 
+// Random float atomic adds (red.global.add, the result unused) over n words:
+// four independent address chains per thread; pairs: one vector atomic adds
+// two x-neighbours (the scatter form of the adjoints).
+__global__ void __launch_bounds__(256) k_atomic_peak(float* __restrict__ buf, unsigned long long n, int per_thread,
+                                                     int pairs, uint32_t seed) {
+    uint32_t h[4];
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) h[c] = (t * 4u + (uint32_t)c) * 2654435761u ^ seed;
+    const float v = 1.0f / 1048576.0f;
+    for (int i = 0; i < per_thread; i += 4) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            h[c] = h[c] * 1664525u + 1013904223u;  // LCG (Numerical Recipes constants)
+            if (pairs) {
+                const unsigned long long s = ((unsigned long long)(h[c] ^ (h[c] >> 15)) * (n / 2)) >> 32;
+                atomicAdd(reinterpret_cast<float2*>(buf) + s, make_float2(v, v));
+            } else {
+                const unsigned long long s = ((unsigned long long)(h[c] ^ (h[c] >> 15)) * n) >> 32;
+                atomicAdd(buf + s, v);
+            }
+        }
+    }
+}
+
 __global__ void k_ray_box(const float* __restrict__ rays, int64_t n, float3 bmin, float3 bmax, float* __restrict__ out) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         float tMin, tMax;
@@ -362,6 +387,19 @@ int vrt_gather_peak(const void* buffer, int64_t bytes, int64_t threads, int32_t 
     const int blocks = (int)(threads / 256);
     k_gather_peak<<<blocks, 256, 0, (cudaStream_t)stream>>>(static_cast<const uint4*>(buffer), sectors, per_thread,
                                                             seed, sink);
+    count_launches(1);
+    return launch_status(cudaGetLastError());
+}
+
+int vrt_atomic_peak(float* buffer, int64_t n, int64_t threads, int32_t per_thread, int32_t pairs, uint32_t seed,
+                    void* stream) {
+    if (!buffer) return VRT_E_NULL_POINTER;
+    if (n < 2 || threads < 256 || per_thread < 4 || (per_thread & 3) || ((uintptr_t)buffer & 7u))
+        return VRT_E_INVALID_ARGUMENT;
+    if ((unsigned long long)n > (1ull << 32)) return VRT_E_BAD_SHAPE;
+    const int blocks = (int)(threads / 256);
+    k_atomic_peak<<<blocks, 256, 0, (cudaStream_t)stream>>>(buffer, (unsigned long long)n, per_thread, pairs ? 1 : 0,
+                                                            seed);
     count_launches(1);
     return launch_status(cudaGetLastError());
 }
