@@ -200,8 +200,8 @@ def atomic_peaks(dev, reps: int = 5) -> dict:
 
 KERNELS = ["k_walk_fw", "k_shadow_fw", "k_ds_primal", "k_shadow_T", "k_ds_replay", "k_shadow_adj", "k_ds_rewalk"]
 # the kernel functions each slot covers (ratio-tracking shadows run k_shadow_run / k_shadow_adj; the
-# capped walks under a constant environment run the FULL = false instances of the walk kernels)
-KERNEL_FUNCS = {"k_walk_fw": "k_walk_fw<false>", "k_shadow_fw": "k_shadow_run<0, 0>", "k_ds_primal": "k_ds_primal<false>",
+# capped walks under a constant environment run the FULL = false instances, <0> in profiler names)
+KERNEL_FUNCS = {"k_walk_fw": "k_walk_fw<0>", "k_shadow_fw": "k_shadow_run<0, 0>", "k_ds_primal": "k_ds_primal<0>",
                 "k_shadow_T": "k_shadow_run<0, 1>", "k_ds_replay": "k_ds_replay", "k_shadow_adj": "k_shadow_adj<0>",
                 "k_ds_rewalk": "k_ds_rewalk"}
 
