@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-c5", action="store_true", help="skip the radiance-cache equal-time comparison")
     ap.add_argument("--workload", default=WORKLOAD,
-                    choices=[WORKLOAD, "plain_forward_64", "dda_transmittance_256"],
+                    choices=[WORKLOAD, "plain_forward_64", "dda_transmittance_256", "path_adjoints_64"],
                     help="the timed workload (default: the differentiable path tracer); the others print "
                          "their own metric line (1 GPU)")
     ap.add_argument("--small", action="store_true", help="a 128x128, 8 spp image of the same medium (profiling)")
@@ -202,7 +202,7 @@ KERNELS = ["k_walk_fw", "k_shadow_fw", "k_ds_primal", "k_shadow_T", "k_ds_replay
 # the kernel functions each slot covers (ratio-tracking shadows run k_shadow_run / k_shadow_adj; the
 # capped walks under a constant environment run the FULL = false instances, <0> in profiler names)
 KERNEL_FUNCS = {"k_walk_fw": "k_walk_fw<0>", "k_shadow_fw": "k_shadow_run<0, 0>", "k_ds_primal": "k_ds_primal<0>",
-                "k_shadow_T": "k_shadow_run<0, 1>", "k_ds_replay": "k_ds_replay", "k_shadow_adj": "k_shadow_adj<0>",
+                "k_shadow_T": "k_shadow_run<0, 1>", "k_ds_replay": "k_ds_replay", "k_shadow_adj": "k_shadow_adj<0, 0>",
                 "k_ds_rewalk": "k_ds_rewalk"}
 
 
@@ -341,7 +341,7 @@ def run_ours(args):
     times = []
     vffi, vlib = _lib.ffi_lib()
     launches0 = int(vlib.vrt_launch_count())
-    kstats = vffi.new("vrt_kernel_stat[]", len(KERNELS))
+    kstats = vffi.new("vrt_kernel_stat[]", vlib.VRT_K_COUNT)
     _lib.check(vlib.vrt_kernel_stats(_lib.context(dev).ptr, _lib.stream_handle(dev), kstats))  # clear
     vlib.vrt_set_kernel_timing(1)
     with ClockSampler(local) as clk:
@@ -565,6 +565,70 @@ def _timed(fn, steps, warmup, flush):
     return ts
 
 
+def run_path_adjoints(args, wl, sig, flush, dev):
+    """Capture backward of every path adjoint on the first configuration's
+    medium (64^3 blobs, 128 x 128 x 4 spp, 16 bounces, constant majorant,
+    environment + sun): device ms of the forward capture, of forward +
+    backward, and their difference, per adjoint; adjoint paths/s."""
+    import torch
+    from rendervous_b200 import maps, synthetic
+    sp = torch.nn.Parameter(sig.clone())
+    bmin, bmax = maps.normalized_box(sp)
+    sg = maps.Grid3D(sp, bmin, bmax)
+    a = wl["albedo"]
+    alb = maps.const[a, a, a]
+    env = maps.const[wl["env"], wl["env"], wl["env"]]
+    boundary = maps.ray_box_intersection[bmin, bmax]
+    maj = maps.const[[float(sig.max()), 1e6]]
+    g = maps.const[wl["phase_g"]]
+    sun = maps.DirectionalLight(synthetic.gaussian_direction(wl["sun_seed"]), wl["sun_intensity"])
+    envs = maps._functionsampler(maps.UniformDirectionSampler(6), env)
+    tr = maps.RatiotrackingTransmittance(sg, boundary, maj)
+    nee = (sg, alb, maps.ZERO, env, envs, maps.HenyeyGreensteinPhase(g), maps.HenyeyGreensteinPhaseSampler(g),
+           boundary, maj, tr)
+    kw = dict(max_bounces=wl["max_bounces"], directional_light=sun)
+    fields = {
+        "NEE_DS": maps.DeltatrackingNEEPathIntegrator(*nee, wl["ds_epsilon"], **kw),
+        "DT": maps.DeltatrackingPathIntegrator(sg, alb, maps.ZERO, env, maps.HenyeyGreensteinPhaseSampler(g),
+                                               boundary, maj, wl["ds_epsilon"], **kw),
+        "DRT": maps.DRTPathIntegrator(*nee, **kw),
+        "DRTQ": maps.DRTQPathIntegrator(*nee, **kw),
+        "DRTDS": maps.DRTDSPathIntegrator(*nee, wl["ds_epsilon"], **kw),
+        "SPS": maps.SPSPathIntegrator(*nee, **kw),
+    }
+    cam = maps.PerspectiveCameraSensor(wl["width"], wl["height"],
+                                       torch.from_numpy(synthetic.ring_poses(wl["views"])).to(dev), jittered=True)
+    n_paths = wl["width"] * wl["height"] * wl["views"] * wl["spp"]
+    out = {}
+    for name, field in fields.items():
+        k = {"i": 0}
+
+        def fw():
+            k["i"] += 1
+            with torch.no_grad():
+                cam.capture(field, fw_samples=wl["spp"], seed=k["i"])
+
+        def fwbw():
+            k["i"] += 1
+            sp.grad = None
+            img = cam.capture(field, fw_samples=wl["spp"], bw_samples=wl["spp"], seed=k["i"])
+            img.sum().backward()
+        maps.check()
+        t_fw = statistics.mean(_timed(fw, args.steps, args.warmup, flush))
+        t_all = statistics.mean(_timed(fwbw, args.steps, args.warmup, flush))
+        maps.check()
+        t_bw = max(t_all - t_fw, 1e-6)
+        out[name] = {"fw_ms": t_fw, "fwbw_ms": t_all, "bw_ms": t_bw, "bw_paths_per_s": n_paths / (t_bw / 1e3)}
+    return {"metric": "adjoint paths/s", "value": out["DRT"]["bw_paths_per_s"], "unit": "paths/s",
+            "ms_per_step": out["DRT"]["fwbw_ms"], "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded generators)",
+            "config": {"workload": args.workload, "grid": [64, 64, 64], "image": [wl["height"], wl["width"]],
+                       "spp": wl["spp"], "max_bounces": wl["max_bounces"], "majorant": "constant (reference)",
+                       "transmittance": "ratio tracking", "l2": "flushed between steps (512 MB write)",
+                       "value_is": "the DRT adjoint's paths/s; every adjoint in 'adjoints'"},
+            "adjoints": out}
+
+
 def run_other(args):
     """The plain forward path tracer (64^3 blobs, 128 x 128, 16 spp, 16 bounces:
     path vertices/s) or the DDA transmittance operator (256^3 four-octave noise,
@@ -580,6 +644,10 @@ def run_other(args):
     wl = synthetic.WORKLOADS[args.workload]
     sig = torch.from_numpy(synthetic.make_sigma(wl["sigma"])).to(dev)
     maps.check()
+    if args.workload == "path_adjoints_64":
+        line = run_path_adjoints(args, wl, sig, flush, dev)
+        print(json.dumps(line))
+        return
     if args.workload == "plain_forward_64":
         bmin, bmax = maps.normalized_box(sig)
         sg = maps.Grid3D(sig, bmin, bmax)

@@ -178,7 +178,10 @@ enum {
     VRT_K_DS_REPLAY = 4,   /* NEE_DS adjoint: replay of the logged collisions (sigma / albedo scatters) */
     VRT_K_SHADOW_ADJ = 5,  /* NEE_DS adjoint: transmittance adjoints */
     VRT_K_DS_REWALK = 6,   /* NEE_DS adjoint: replay walk of the paths the log could not hold */
-    VRT_K_COUNT = 7
+    VRT_K_DRT_PRIMAL = 7,  /* DRT adjoint: primal walk (collision log, light jobs, reservoir) */
+    VRT_K_DRT_REPLAY = 8,  /* DRT adjoint: replay of the logged collisions (sigma scatters) */
+    VRT_K_DRT_BRANCH = 9,  /* DRT adjoint: the reservoir vertex's branch, one per path */
+    VRT_K_COUNT = 10
 };
 typedef struct vrt_kernel_stat {
     int64_t launches;

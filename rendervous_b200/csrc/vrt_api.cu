@@ -90,6 +90,10 @@ static bool use_wave(const DMedium& M, int integrator) {
 static bool use_wave_bw(const DMedium& M, int bw_mode) {
     return bw_mode == VRT_BW_NEE_DS && M.max_bounces <= 4096 && !M.ds_compat;
 }
+// the DRT adjoint on the wavefront: capped paths, ratio / delta tracking light rays
+static bool use_wave_drt(const DMedium& M, int bw_mode) {
+    return bw_mode == VRT_BW_NEE_DRT && M.max_bounces > 0 && M.max_bounces <= 4096 && M.tr_mode <= 1;
+}
 
 static bool is_collision(int integrator) {
     return integrator == VRT_PI_MC_COLLISION || integrator == VRT_PI_DDA_COLLISION;
@@ -432,7 +436,8 @@ int vrt_kernel_stats(vrt_context* ctx, void* stream, vrt_kernel_stat* out) {
     if (!out) return VRT_E_NULL_POINTER;
     cudaStream_t s = (cudaStream_t)stream;
     if (cudaStreamSynchronize(s) != cudaSuccess) return launch_status(cudaGetLastError());
-    unsigned long long k[8][5];
+    unsigned long long k[VRT_K_COUNT][5];
+    static_assert(sizeof(k) == sizeof(DScratch::kstat), "one counter slot per kernel");
     if (cudaMemcpy(k, ctx->scratch->kstat, sizeof(k), cudaMemcpyDeviceToHost) != cudaSuccess) return VRT_E_CUDA;
     if (cudaMemset(ctx->scratch->kstat, 0, sizeof(k)) != cudaSuccess) return VRT_E_CUDA;
     KernelTiming& t = timing();
@@ -680,6 +685,8 @@ int vrt_radiance_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, cons
         return launch_collision_bw(M, collision_of(bw_mode), S, (uint64_t)n, seed, dL_dR, 1.0f, ctx->scratch,
                                    ctx->num_sms, (cudaStream_t)stream);
     if (use_wave_bw(M, bw_mode)) return launch_wave_ds_bw(ctx, M, S, (uint64_t)n, seed, dL_dR, 1.0f, (cudaStream_t)stream);
+    if (use_wave_drt(M, bw_mode))
+        return launch_wave_drt_bw(ctx, M, S, (uint64_t)n, seed, dL_dR, 1.0f, (cudaStream_t)stream);
     return launch_radiance_bw(M, bw_mode, S, (uint64_t)n, seed, dL_dR, 1.0f, ctx->scratch, ctx->num_sms,
                               (cudaStream_t)stream);
 }
@@ -730,6 +737,9 @@ int vrt_capture_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const
     if (use_wave_bw(M, bw_mode))
         return launch_wave_ds_bw(ctx, M, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
                                  (cudaStream_t)stream);
+    if (use_wave_drt(M, bw_mode))
+        return launch_wave_drt_bw(ctx, M, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
+                                  (cudaStream_t)stream);
     return launch_radiance_bw(M, bw_mode, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
                               ctx->scratch, ctx->num_sms, (cudaStream_t)stream);
 }

@@ -59,8 +59,19 @@ int launch_radiance_fw(const DMedium& M, int integrator, const PathSrc& src, uin
                        float* out, float scale, DScratch* scratch, int num_sms, cudaStream_t stream);
 // dL: rays mode dL[i]; camera mode dL[pixel] / div (div = spp, as the reference's
 // capture backward divides dL/dI by the sample count, _maps.py:707-708).
+// pids: the n_paths paths listed there (device array), else paths 0 .. n_paths-1.
 int launch_radiance_bw(const DMedium& M, int bw_mode, const PathSrc& src, uint64_t n_paths, uint64_t seed,
-                       const float* dL, float div, DScratch* scratch, int num_sms, cudaStream_t stream);
+                       const float* dL, float div, DScratch* scratch, int num_sms, cudaStream_t stream,
+                       const unsigned long long* pids = nullptr);
+
+// Wavefront DRT adjoint (vrt_wave_drt.cu): capped paths, ratio or delta
+// tracking light rays; and its per-path reservoir branch (vrt_path.cu) over
+// the round's paths [p_begin, min(*next_path, n_paths)) (at most max_round).
+int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed,
+                       const float* dL, float div, cudaStream_t stream);
+int launch_drt_branch(const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t p_begin,
+                      const unsigned long long* next_path, uint64_t seed, const float* dL, float div, const float* info,
+                      const float4* resv, uint64_t max_round, DScratch* scratch, int num_sms, cudaStream_t stream);
 
 // Radiance-cache forms of the forward NEE kernel (mode FW_CUT or FW_TRAIN).
 int launch_cache_paths(const DMedium& M, int mode, const PathSrc& src, uint64_t n_paths, uint64_t seed, float* out,

@@ -17,6 +17,7 @@
 // saved seeds, and scatter dL/dsigma and dL/dalbedo with atomics.
 #include <cuda_runtime.h>
 
+#include "../../include/vrt.h"
 #include "vrt_device.cuh"
 #include "vrt_internal.h"
 #include "vrt_tracking.cuh"
@@ -714,6 +715,30 @@ __device__ float sample_transmittance_position(const DMedium& M, Rng& rng, float
     return Tr;
 }
 
+// vr_path_integrator_NEE_DRT.h:232-268: the branch from the reservoir vertex
+// (res_x, res_w, throughput res_W picked with weight res_P of total_weight) --
+// a transmittance-sampled position, its light rays and a nested scattered-only
+// NEE path -- and its sigma scatter.  rng is the path's stream where the
+// replay left it (the primal's end).
+__device__ void drt_branch(const DMedium& M, Rng& rng, float3 res_x, float3 res_w, float3 res_W, float res_P,
+                           float total_weight, float3 dL_dR, uint32_t& verts, Tally& tl, uint32_t* status) {
+    float tMin, d;
+    boundary(M, res_x, res_w, tMin, d);
+    float s_t, weight_t;
+    sample_transmittance_position(M, rng, res_x, res_w, d, s_t, weight_t, tl, status);
+    float3 xs = res_x + res_w * s_t;
+    float3 ls_dir;
+    float3 Ls_env = environment_sample(M, rng, ls_dir);
+    float3 Ls = transmittance(M, rng, xs, ls_dir, tl, status) * Ls_env * phase(M, res_w, ls_dir);
+    if (M.has_sun) Ls = Ls + transmittance(M, rng, xs, M.sun_dir, tl, status) * M.sun_L * phase(M, res_w, M.sun_dir);
+    float3 ws = phase_sample(M, rng, res_w);
+    Ls = Ls + 1.0f * path_nee_seq(M, rng, xs, ws, true, verts, tl, status);
+    Ls = Ls * res_W * weight_t * albedo(M, xs, tl);
+    float sigma_xs = sigma(M, xs, tl);
+    float mis_T = 1.0f / (1.0f + sigma_xs * sigma_xs);
+    sigma_bw(M, xs, dot(dL_dR, Ls) * mis_T * total_weight / res_P, tl);
+}
+
 // vr_path_integrator_NEE_DRT.h:62-270.  The branch seed is Philox stream 1.
 __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float3 dL_dR, Tally& tl,
                                 uint32_t* status) {
@@ -826,20 +851,7 @@ __device__ void path_nee_drt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
         rng.advance();
         if (all_less(W, EPS) || capped) break;
     }
-    boundary(M, res_x, res_w, tMin, d);
-    float s_t, weight_t;
-    sample_transmittance_position(M, rng, res_x, res_w, d, s_t, weight_t, tl, status);
-    float3 xs = res_x + res_w * s_t;
-    float3 ls_dir;
-    float3 Ls_env = environment_sample(M, rng, ls_dir);
-    float3 Ls = transmittance(M, rng, xs, ls_dir, tl, status) * Ls_env * phase(M, res_w, ls_dir);
-    if (M.has_sun) Ls = Ls + transmittance(M, rng, xs, M.sun_dir, tl, status) * M.sun_L * phase(M, res_w, M.sun_dir);
-    float3 ws = phase_sample(M, rng, res_w);
-    Ls = Ls + 1.0f * path_nee_seq(M, rng, xs, ws, true, verts, tl, status);
-    Ls = Ls * res_W * weight_t * albedo(M, xs, tl);
-    float sigma_xs = sigma(M, xs, tl);
-    float mis_T = 1.0f / (1.0f + sigma_xs * sigma_xs);
-    sigma_bw(M, xs, dot(dL_dR, Ls) * mis_T * total_weight / res_P, tl);
+    drt_branch(M, rng, res_x, res_w, res_W, res_P, total_weight, dL_dR, verts, tl, status);
 }
 
 __device__ __forceinline__ Rng branch_stream(const Rng& rng) {
@@ -1290,13 +1302,15 @@ __global__ void __launch_bounds__(256) k_dt_fw(DMedium M, PathSrc S, uint64_t n_
     warp_add_counters(sc, paths, verts, tl);
 }
 
+// pids: the n_paths paths listed there (device array), else paths 0 .. n_paths-1
 template <int MODE>
 __global__ void __launch_bounds__(256) k_path_bw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, const float* dL,
-                                                  float div, DScratch* sc) {
+                                                  float div, DScratch* sc, const unsigned long long* pids) {
     uint32_t paths = 0;
     Tally tl;
-    for (uint64_t pid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; pid < n_paths;
-         pid += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_paths;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t pid = pids ? (uint64_t)pids[i] : i;
         Rng rng;
         rng.init(seed, pid, 0);
         float3 x, w;
@@ -1312,6 +1326,67 @@ __global__ void __launch_bounds__(256) k_path_bw(DMedium M, PathSrc S, uint64_t 
         else path_nee_sps_bw(M, rng, x, w, g, tl, &sc->status);
     }
     warp_add_counters(sc, paths, 0, tl);
+}
+
+// The reservoir branch of the DRT wavefront (vrt_wave_drt.cu), one thread per
+// path of the round: the primal left the reservoir vertex and the stream
+// position at its end in resv (4 float4 per path: vertex and its weight,
+// direction and the running total -- 0 for a primary ray that missed the
+// medium --, throughput, stream position); paths handed to the sequential
+// form (first-collision word kSpilled) are skipped.
+__global__ void __launch_bounds__(256) k_drt_branch(DMedium M, PathSrc S, uint64_t n_paths, uint64_t p_begin,
+                                                     const unsigned long long* next_path, uint64_t seed,
+                                                     const float* dL, float div, const float* __restrict__ info,
+                                                     const float4* __restrict__ resv, DScratch* sc) {
+    constexpr uint32_t kSpilledPath = 0xfffffffdu;  // the first-collision word of a handed-over path
+    unsigned long long end = *next_path;
+    if (end > n_paths) end = n_paths;
+    const uint64_t n_round = end > p_begin ? end - p_begin : 0;
+    uint32_t verts = 0;
+    Tally tl;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n_round;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const float4 r1 = resv[4 * k + 1];
+        if (!(r1.w > 0.0f)) continue;  // the primary ray missed the medium: no branch
+        if (__float_as_uint(info[8 * k + 7]) == kSpilledPath) continue;
+        const float4 r0 = resv[4 * k], r2 = resv[4 * k + 2], r3 = resv[4 * k + 3];
+        const uint64_t pid = p_begin + k;
+        Rng rng;
+        rng.init(seed, pid, 0);
+        rng.seek(Rng::Pos{__float_as_uint(r3.x), __float_as_uint(r3.y)});
+        const long long o = S.is_camera ? (long long)(pid % (uint64_t)S.npix) : (long long)pid;
+        const float3 g = ld3(dL + 3 * o) / div;
+        drt_branch(M, rng, make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), make_float3(r2.x, r2.y, r2.z),
+                   r0.w, r1.w, g, verts, tl, &sc->status);
+    }
+    warp_add_counters(sc, 0, 0, tl);
+    // the per-kernel slot (vrt_kernel_stats)
+    unsigned long long st = tl.steps, lk = tl.lookups, rd = tl.reds, al = tl.albedo;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        st += __shfl_down_sync(kFull, st, o);
+        lk += __shfl_down_sync(kFull, lk, o);
+        rd += __shfl_down_sync(kFull, rd, o);
+        al += __shfl_down_sync(kFull, al, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&sc->kstat[VRT_K_DRT_BRANCH][0], st);
+        atomicAdd(&sc->kstat[VRT_K_DRT_BRANCH][1], lk);
+        atomicAdd(&sc->kstat[VRT_K_DRT_BRANCH][2], rd);
+        atomicAdd(&sc->kstat[VRT_K_DRT_BRANCH][3], al);
+    }
+}
+
+int launch_drt_branch(const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t p_begin,
+                      const unsigned long long* next_path, uint64_t seed, const float* dL, float div, const float* info,
+                      const float4* resv, uint64_t max_round, DScratch* scratch, int num_sms, cudaStream_t stream) {
+    if (max_round == 0) return 0;
+    const uint64_t need = (max_round + 255) / 256;
+    const int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
+    KernelScope ks(VRT_K_DRT_BRANCH, stream);
+    k_drt_branch<<<blocks, 256, 0, stream>>>(M, src, n_paths, p_begin, next_path, seed, dL, div, info, resv, scratch);
+    count_launches(1);
+    return launch_status(cudaGetLastError());
 }
 
 // ------------------------------------------------------------------------
@@ -1374,17 +1449,17 @@ int launch_cache_targets(float* smp, const float* pR, long long n_paths, int rec
 }
 
 int launch_radiance_bw(const DMedium& M, int bw_mode, const PathSrc& src, uint64_t n_paths, uint64_t seed,
-                       const float* dL, float div, DScratch* scratch, int num_sms, cudaStream_t stream) {
+                       const float* dL, float div, DScratch* scratch, int num_sms, cudaStream_t stream,
+                       const unsigned long long* pids) {
     if (n_paths == 0) return 0;
-    if (bw_mode == 0) return launch_nee_ds_bw(M, src, n_paths, seed, dL, div, scratch, num_sms, stream);
+    if (bw_mode == 0) return launch_nee_ds_bw(M, src, n_paths, seed, dL, div, scratch, num_sms, stream, pids);
     uint64_t need = (n_paths + 255) / 256;
     int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
-    if (bw_mode == 0) k_path_bw<0><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
-    else if (bw_mode == 1) k_path_bw<1><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
-    else if (bw_mode == 2) k_path_bw<2><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
-    else if (bw_mode == 3) k_path_bw<3><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
-    else if (bw_mode == 4) k_path_bw<4><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
-    else k_path_bw<5><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
+    if (bw_mode == 1) k_path_bw<1><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch, pids);
+    else if (bw_mode == 2) k_path_bw<2><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch, pids);
+    else if (bw_mode == 3) k_path_bw<3><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch, pids);
+    else if (bw_mode == 4) k_path_bw<4><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch, pids);
+    else k_path_bw<5><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch, pids);
     count_launches(1);
     return launch_status(cudaGetLastError());
 }

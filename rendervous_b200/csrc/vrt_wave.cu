@@ -399,8 +399,12 @@ __global__ void __launch_bounds__(256, 4) k_shadow_run(DMedium M, PathSrc S, con
                     exhausted = wq.drained;
                 } else {
                     jv = get_job(jobs, i);
-                    alive = shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork);
-                    if (!alive) shadow_finish<OUT>(S, so, jv, 1.0f);
+                    if (OUT == OUT_RECORD && jv.tgt == kAdjOnly) {
+                        alive = false;  // an adjoint-only job: nothing to estimate here
+                    } else {
+                        alive = shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork);
+                        if (!alive) shadow_finish<OUT>(S, so, jv, 1.0f);
+                    }
                 }
             }
         }
@@ -430,8 +434,10 @@ constexpr int kKeep = 16;  // first-pass collisions a transmittance adjoint keep
 // for bit -- so this kernel needs nothing from the replay.  No adjoint runs
 // for rays from or after a singular (zero-density) vertex, where the
 // reference's replay stops (vr_path_integrator_NEE_DS.h:153-154), nor for
-// paths the state machine runs (first-collision word kSpilled).
-template <int TR>
+// paths the state machine runs (first-collision word kSpilled).  DRT: the jobs
+// of the DRT adjoint (vr_path_integrator_NEE_DRT.h:68-69, 165-167): every job
+// has an adjoint, drawn from fork j of the adjoint's own stream 1.
+template <int TR, bool DRT>
 __global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, PathSrc S, const ShadowJob* __restrict__ jobs,
                                                      const unsigned long long* __restrict__ count,
                                                      unsigned long long cap, unsigned long long* head, uint64_t seed,
@@ -459,10 +465,11 @@ __global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, PathSrc S, con
                 } else {
                     jv = get_job(jobs, i);
                     dLdT = 0.0f;
-                    if (!(jv.tgt & 2u) && __float_as_uint(info[8 * (jv.pid - p_begin) + 7]) != kSpilled)
+                    if ((DRT || !(jv.tgt & 2u)) && __float_as_uint(info[8 * (jv.pid - p_begin) + 7]) != kSpilled)
                         dLdT = dot(ld3(dL + 3 * out_index(S, jv.pid)) / div, jv.wt);
                     nkeep = 0;
-                    if (dLdT != 0.0f && shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork)) phase = 1;
+                    if (dLdT != 0.0f && shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork, DRT ? 1u : 0u))
+                        phase = 1;
                 }
             }
         }
@@ -492,7 +499,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, PathSrc S, con
                         }
                         phase = 0;
                     } else {  // replay the second pass
-                        shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork);
+                        shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork, DRT ? 1u : 0u);
                         phase = 2;
                     }
                 }
@@ -666,15 +673,18 @@ int launch_shadow_record(const DMedium& M, const PathSrc& src, const WaveBw& wv,
 }
 
 int launch_shadow_adjoint(const DMedium& M, const PathSrc& src, const WaveBw& wv, uint64_t seed, const float* dL,
-                          float div, DScratch* sc, int num_sms, cudaStream_t stream) {
+                          float div, DScratch* sc, int num_sms, cudaStream_t stream, bool drt) {
     if (M.tr_mode > 1) return VRT_OK;  // DDA: in k_shadow_T; GRT / GDT: no backward
     KernelScope ks(VRT_K_SHADOW_ADJ, stream);
-    if (M.tr_mode == 0)
-        k_shadow_adj<0><<<persistent_blocks((const void*)k_shadow_adj<0>, 256, num_sms), 256, 0, stream>>>(
-            M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, wv.info, wv.p_begin, dL, div, sc);
-    else
-        k_shadow_adj<1><<<persistent_blocks((const void*)k_shadow_adj<1>, 256, num_sms), 256, 0, stream>>>(
-            M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, wv.info, wv.p_begin, dL, div, sc);
+#define VRT_ADJ(TR, D)                                                                                             \
+    k_shadow_adj<TR, D><<<persistent_blocks((const void*)k_shadow_adj<TR, D>, 256, num_sms), 256, 0, stream>>>( \
+        M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, wv.info, wv.p_begin, dL, div, sc)
+    if (M.tr_mode == 0) {
+        if (drt) VRT_ADJ(0, true); else VRT_ADJ(0, false);
+    } else {
+        if (drt) VRT_ADJ(1, true); else VRT_ADJ(1, false);
+    }
+#undef VRT_ADJ
     count_launches(1);
     return launch_status(cudaGetLastError());
 }

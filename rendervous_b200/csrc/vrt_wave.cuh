@@ -231,9 +231,11 @@ struct ShadowRay {
 
 // Starts the ray (x, dir) on fork `fork` of path pid; false when it misses the
 // medium (T = 1).
+// sbase: the stream the forks come from (0: the path's stream; 1: the DRT
+// adjoint's stream for the transmittance adjoints).
 __device__ __forceinline__ bool shadow_begin(const DMedium& M, ShadowRay& s, float3 x, float3 dir, uint64_t seed,
-                                             uint64_t pid, uint32_t fork) {
-    s.r.init(seed, pid, 2u * (1u + fork));
+                                             uint64_t pid, uint32_t fork, uint32_t sbase = 0u) {
+    s.r.init(seed, pid, sbase + 2u * (1u + fork));
     s.T = 1.0f;
     s.it = 0;
     s.ff = Flight();
@@ -355,6 +357,9 @@ __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tal
 constexpr uint32_t kNone = 0xffffffffu;
 constexpr uint32_t kUnlogged = 0xfffffffeu;  // a path whose collisions did not fit the log
 constexpr uint32_t kSpilled = 0xfffffffdu;   // a path handed to the state-machine adjoint
+// the record word of a light job that only has a transmittance adjoint (the
+// DRT adjoint's primary ray toward the environment): no T, no record
+constexpr uint32_t kAdjOnly = 0xffffffffu;
 // A real-collision vertex of the NEE_DS primal (48 bytes): its two shadow
 // transmittances (filled by the shadow kernel), the next vertex of the same
 // path, the slot of its environment job (the sun job follows it), and what the
@@ -401,6 +406,10 @@ struct WaveBw {
     unsigned long long* spill;
     unsigned long long* spill_count;
     unsigned long long cap_spill;
+    // the DRT adjoint's reservoir per path of the round (4 float4: vertex and
+    // its weight, direction and the running total, throughput and the stream
+    // position at the end of the primal); null for NEE_DS
+    float4* resv;
 };
 
 }  // namespace wave
@@ -412,7 +421,9 @@ struct WaveBw {
 // the same jobs with dL/dT = dL/dR(pixel) / div . weight (head: hdr[4]).
 int launch_shadow_record(const DMedium& M, const PathSrc& src, const wave::WaveBw& wv, uint64_t seed, const float* dL,
                          float div, DScratch* sc, int num_sms, cudaStream_t stream);
+// drt: the DRT adjoint's jobs (forks of stream 1, every job but those of
+// handed-over paths, kAdjOnly jobs included).
 int launch_shadow_adjoint(const DMedium& M, const PathSrc& src, const wave::WaveBw& wv, uint64_t seed, const float* dL,
-                          float div, DScratch* sc, int num_sms, cudaStream_t stream);
+                          float div, DScratch* sc, int num_sms, cudaStream_t stream, bool drt = false);
 
 }  // namespace vrt

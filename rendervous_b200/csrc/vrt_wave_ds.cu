@@ -626,6 +626,7 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     wv.evs = reinterpret_cast<CollisionRec*>(base + o_evs);
     wv.spill = reinterpret_cast<unsigned long long*>(base + o_spill);
     wv.spill_count = &wv.hdr[10];  // kept across rounds
+    wv.resv = nullptr;
     wv.p_begin = 0;
     cudaError_t e = cudaMemsetAsync(&ctx->scratch->next_path, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return launch_status(e);

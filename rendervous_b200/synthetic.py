@@ -145,13 +145,19 @@ def ring_poses(views: int, radius: float = 2.0, elevation_deg: float = 20.0, tar
 
 
 # ---------------------------------------------------------------------------
-# The five benchmark workloads, by name.
+# The benchmark workloads, by name.
 # ---------------------------------------------------------------------------
 WORKLOADS = {
     "plain_forward_64": dict(
         sigma=("blobs", dict(res=64, n_blobs=12, max_sigma=20.0, seed=1)),
         albedo=0.9, phase_g=0.0, env=1.0, sun_intensity=3.0, sun_seed=1,
         width=128, height=128, spp=16, max_bounces=16, views=1, render_seed=2),
+    # the one-path-per-thread adjoints (DT, DRT, DRTQ, DRTDS, SPS) beside the NEE_DS wavefront, on the
+    # first configuration's medium with a trainable sigma
+    "path_adjoints_64": dict(
+        sigma=("blobs", dict(res=64, n_blobs=12, max_sigma=20.0, seed=1)),
+        albedo=0.9, phase_g=0.4, env=1.0, sun_intensity=3.0, sun_seed=1, ds_epsilon=0.1,
+        width=128, height=128, spp=4, max_bounces=16, views=1),
     "dda_transmittance_256": dict(
         sigma=("noise", dict(res=256, octaves=4, max_sigma=50.0, seed=3)),
         n_rays=1 << 20, ray_seed=4, weight_seed=5, brick=8),

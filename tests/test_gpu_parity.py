@@ -262,6 +262,7 @@ def test_dt_integrator_matches_oracle(cuda):
     ("ds", dict(ds_compat=True)),
     ("dt", dict(integrator="dt", sun_dir=None)),
     ("drt", dict(integrator="drt")),
+    ("drt", dict(integrator="drt", majorant="grid", brick=8)),
     ("drtq", dict(integrator="drtq")),
     ("drtds", dict(integrator="drtds")),
     ("sps", dict(integrator="sps")),
@@ -328,6 +329,44 @@ def test_ds_collision_log_overflow_rewalks(cuda, limit):
     for a, b in zip(grads[0], grads[1]):
         rel = np.abs(a - b).sum() / max(np.abs(a).sum(), 1e-30)
         assert np.abs(a).sum() > 0 and rel < 1e-4, rel
+
+
+@pytest.mark.parametrize("limit", [1, 3000])
+def test_drt_wavefront_matches_sequential_form(cuda, limit):
+    """The DRT adjoint's wavefront (primal with collision log, light-ray T and
+    adjoint jobs, log replay, reservoir branch) against its sequential form:
+    with the collision log capped at `limit` records, the paths that do not fit
+    run whole on the sequential form (all of them at 1), so the gradients of
+    both runs agree up to the order of the float sums."""
+    ffi, lib = _lib.ffi_lib()
+    stream = _lib.stream_handle(cuda)
+    ctx = _lib.context(cuda)
+    wl = synthetic.WORKLOADS["plain_forward_64"]
+    sig = torch.from_numpy(synthetic.make_sigma(wl["sigma"])).to(cuda)
+    ks = ffi.new("vrt_kernel_stat[]", lib.VRT_K_COUNT)
+    dimg, grads, stats = None, [], []
+    for lim in (0, limit):
+        field = build_field(sig, albedo=0.9, env=1.0, sun_dir=(0.3, 0.8, 0.5), sun_radiance=3.0, g=0.4,
+                            max_bounces=16, sigma_requires_grad=True, integrator="drt", majorant="grid", brick=8)
+        _lib.check(lib.vrt_set_collision_log_limit(ctx.ptr, lim))
+        try:
+            maps.check()
+            _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
+            cam, img = _capture(field, cuda, 32, 32, 4, seed=17)
+            if dimg is None:
+                dimg = torch.from_numpy(np.random.default_rng(1).random(img.shape).astype(np.float32)).to(cuda)
+            (img * dimg).sum().backward()
+            maps.check()
+            _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
+        finally:
+            _lib.check(lib.vrt_set_collision_log_limit(ctx.ptr, 0))
+        grads.append(field.sigma.grid.grad.cpu().numpy())
+        stats.append({k: getattr(ks[lib.VRT_K_DRT_REPLAY], k) for k in ("steps", "reds")})
+    assert stats[0]["steps"] > 0 and stats[0]["reds"] > 0, stats  # the automatic log holds the paths
+    if limit == 1:
+        assert stats[1]["steps"] == 0, stats  # nothing fit: every path ran on the sequential form
+    rel = np.abs(grads[0] - grads[1]).sum() / max(np.abs(grads[0]).sum(), 1e-30)
+    assert np.abs(grads[0]).sum() > 0 and rel < 1e-4, rel
 
 
 def test_ds_adjoint_matches_finite_difference(cuda):
@@ -457,7 +496,9 @@ def test_kernel_stats_add_up(cuda):
     finally:
         lib.vrt_set_kernel_timing(0)
         maps.set_sync_checks(True)
-    assert all(ks[i].launches > 0 and ks[i].ms > 0 for i in range(nk))
+    nee = range(lib.VRT_K_DS_REWALK + 1)  # the NEE forward and NEE_DS adjoint kernels (not the DRT ones)
+    assert all(ks[i].launches > 0 and ks[i].ms > 0 for i in nee)
+    assert all(ks[i].launches == 0 for i in range(lib.VRT_K_DS_REWALK + 1, nk))
     assert sum(ks[i].lookups for i in range(nk)) == totals["lookups"]
     assert ks[1].steps > 0 and ks[4].reds > 0
     # the replay reads the primal's collision log (no lookups of its own); with
