@@ -90,9 +90,9 @@ static bool use_wave(const DMedium& M, int integrator) {
 static bool use_wave_bw(const DMedium& M, int bw_mode) {
     return bw_mode == VRT_BW_NEE_DS && M.max_bounces <= 4096 && !M.ds_compat;
 }
-// the DRT adjoint on the wavefront: capped paths, ratio / delta tracking light rays
+// the DRT and DRTDS adjoints on the wavefront (capped or not): ratio / delta tracking light rays
 static bool use_wave_drt(const DMedium& M, int bw_mode) {
-    return bw_mode == VRT_BW_NEE_DRT && M.max_bounces > 0 && M.max_bounces <= 4096 && M.tr_mode <= 1;
+    return (bw_mode == VRT_BW_NEE_DRT || bw_mode == VRT_BW_NEE_DRTDS) && M.max_bounces <= 4096 && M.tr_mode <= 1;
 }
 
 static bool is_collision(int integrator) {
@@ -686,7 +686,7 @@ int vrt_radiance_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, cons
                                    ctx->num_sms, (cudaStream_t)stream);
     if (use_wave_bw(M, bw_mode)) return launch_wave_ds_bw(ctx, M, S, (uint64_t)n, seed, dL_dR, 1.0f, (cudaStream_t)stream);
     if (use_wave_drt(M, bw_mode))
-        return launch_wave_drt_bw(ctx, M, S, (uint64_t)n, seed, dL_dR, 1.0f, (cudaStream_t)stream);
+        return launch_wave_drt_bw(ctx, M, bw_mode, S, (uint64_t)n, seed, dL_dR, 1.0f, (cudaStream_t)stream);
     return launch_radiance_bw(M, bw_mode, S, (uint64_t)n, seed, dL_dR, 1.0f, ctx->scratch, ctx->num_sms,
                               (cudaStream_t)stream);
 }
@@ -738,7 +738,7 @@ int vrt_capture_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const
         return launch_wave_ds_bw(ctx, M, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
                                  (cudaStream_t)stream);
     if (use_wave_drt(M, bw_mode))
-        return launch_wave_drt_bw(ctx, M, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
+        return launch_wave_drt_bw(ctx, M, bw_mode, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
                                   (cudaStream_t)stream);
     return launch_radiance_bw(M, bw_mode, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
                               ctx->scratch, ctx->num_sms, (cudaStream_t)stream);

@@ -64,12 +64,13 @@ int launch_radiance_bw(const DMedium& M, int bw_mode, const PathSrc& src, uint64
                        const float* dL, float div, DScratch* scratch, int num_sms, cudaStream_t stream,
                        const unsigned long long* pids = nullptr);
 
-// Wavefront DRT adjoint (vrt_wave_drt.cu): capped paths, ratio or delta
-// tracking light rays; and its per-path reservoir branch (vrt_path.cu) over
-// the round's paths [p_begin, min(*next_path, n_paths)) (at most max_round).
-int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed,
-                       const float* dL, float div, cudaStream_t stream);
-int launch_drt_branch(const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t p_begin,
+// Wavefront DRT / DRTDS adjoint (vrt_wave_drt.cu; bw_mode VRT_BW_NEE_DRT or
+// VRT_BW_NEE_DRTDS): capped paths, ratio or delta tracking light rays; and its
+// per-path reservoir branch (vrt_path.cu; ds: the DRTDS form) over the round's
+// paths [p_begin, min(*next_path, n_paths)) (at most max_round).
+int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, int bw_mode, const PathSrc& src, uint64_t n_paths,
+                       uint64_t seed, const float* dL, float div, cudaStream_t stream);
+int launch_drt_branch(const DMedium& M, bool ds, const PathSrc& src, uint64_t n_paths, uint64_t p_begin,
                       const unsigned long long* next_path, uint64_t seed, const float* dL, float div, const float* info,
                       const float4* resv, uint64_t max_round, DScratch* scratch, int num_sms, cudaStream_t stream);
 

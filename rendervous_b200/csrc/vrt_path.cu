@@ -1007,6 +1007,28 @@ __device__ void sample_collision_position_ds(const DMedium& M, Rng& rng, float3 
     weight_t = 0.0f;
 }
 
+// vr_path_integrator_NEE_DRTDS.h:230-252: the branch from the reservoir vertex
+// with a defensively sampled collision position (no MIS weight).
+__device__ void drtds_branch(const DMedium& M, Rng& rng, float3 res_x, float3 res_w, float3 res_W, float res_P,
+                             float total_weight, float epsilon, float3 dL_dR, uint32_t& verts, Tally& tl,
+                             uint32_t* status) {
+    float tMin, d;
+    boundary(M, res_x, res_w, tMin, d);
+    float s_t, weight_t;
+    sample_collision_position_ds(M, rng, res_x, res_w, d, epsilon, s_t, weight_t, tl, status);
+    if (weight_t > 0.0f) {
+        float3 xs = res_x + res_w * s_t;
+        float3 ls_dir;
+        float3 Ls_env = environment_sample(M, rng, ls_dir);
+        float3 Ls = transmittance(M, rng, xs, ls_dir, tl, status) * Ls_env * phase(M, res_w, ls_dir);
+        if (M.has_sun) Ls = Ls + transmittance(M, rng, xs, M.sun_dir, tl, status) * M.sun_L * phase(M, res_w, M.sun_dir);
+        float3 ws = phase_sample(M, rng, res_w);
+        Ls = Ls + 1.0f * path_nee_seq(M, rng, xs, ws, true, verts, tl, status);
+        Ls = Ls * res_W * weight_t * albedo(M, xs, tl);
+        sigma_bw(M, xs, dot(dL_dR, Ls) * total_weight / res_P, tl);
+    }
+}
+
 // vr_path_integrator_NEE_DRTDS.h:40-253 (branch seed = Philox stream 1)
 __device__ void path_nee_drtds_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float epsilon, float3 dL_dR,
                                   Tally& tl, uint32_t* status) {
@@ -1106,20 +1128,7 @@ __device__ void path_nee_drtds_bw(const DMedium& M, Rng& rng, float3 x, float3 w
         rng.advance();
         if (all_less(W, EPS) || capped) break;
     }
-    boundary(M, res_x, res_w, tMin, d);
-    float s_t, weight_t;
-    sample_collision_position_ds(M, rng, res_x, res_w, d, epsilon, s_t, weight_t, tl, status);
-    if (weight_t > 0.0f) {
-        float3 xs = res_x + res_w * s_t;
-        float3 ls_dir;
-        float3 Ls_env = environment_sample(M, rng, ls_dir);
-        float3 Ls = transmittance(M, rng, xs, ls_dir, tl, status) * Ls_env * phase(M, res_w, ls_dir);
-        if (M.has_sun) Ls = Ls + transmittance(M, rng, xs, M.sun_dir, tl, status) * M.sun_L * phase(M, res_w, M.sun_dir);
-        float3 ws = phase_sample(M, rng, res_w);
-        Ls = Ls + 1.0f * path_nee_seq(M, rng, xs, ws, true, verts, tl, status);
-        Ls = Ls * res_W * weight_t * albedo(M, xs, tl);
-        sigma_bw(M, xs, dot(dL_dR, Ls) * total_weight / res_P, tl);
-    }
+    drtds_branch(M, rng, res_x, res_w, res_W, res_P, total_weight, epsilon, dL_dR, verts, tl, status);
 }
 
 // vr_path_integrator_NEE_SPS.h:1-59 (majorant at the current sample point;
@@ -1328,12 +1337,13 @@ __global__ void __launch_bounds__(256) k_path_bw(DMedium M, PathSrc S, uint64_t 
     warp_add_counters(sc, paths, 0, tl);
 }
 
-// The reservoir branch of the DRT wavefront (vrt_wave_drt.cu), one thread per
+// The reservoir branch of the DRT / DRTDS wavefront (vrt_wave_drt.cu), one thread per
 // path of the round: the primal left the reservoir vertex and the stream
 // position at its end in resv (4 float4 per path: vertex and its weight,
 // direction and the running total -- 0 for a primary ray that missed the
 // medium --, throughput, stream position); paths handed to the sequential
 // form (first-collision word kSpilled) are skipped.
+template <bool DS>
 __global__ void __launch_bounds__(256) k_drt_branch(DMedium M, PathSrc S, uint64_t n_paths, uint64_t p_begin,
                                                      const unsigned long long* next_path, uint64_t seed,
                                                      const float* dL, float div, const float* __restrict__ info,
@@ -1356,8 +1366,10 @@ __global__ void __launch_bounds__(256) k_drt_branch(DMedium M, PathSrc S, uint64
         rng.seek(Rng::Pos{__float_as_uint(r3.x), __float_as_uint(r3.y)});
         const long long o = S.is_camera ? (long long)(pid % (uint64_t)S.npix) : (long long)pid;
         const float3 g = ld3(dL + 3 * o) / div;
-        drt_branch(M, rng, make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), make_float3(r2.x, r2.y, r2.z),
-                   r0.w, r1.w, g, verts, tl, &sc->status);
+        const float3 rx = make_float3(r0.x, r0.y, r0.z), rw = make_float3(r1.x, r1.y, r1.z);
+        const float3 rW = make_float3(r2.x, r2.y, r2.z);
+        if (DS) drtds_branch(M, rng, rx, rw, rW, r0.w, r1.w, M.ds_eps, g, verts, tl, &sc->status);
+        else drt_branch(M, rng, rx, rw, rW, r0.w, r1.w, g, verts, tl, &sc->status);
     }
     warp_add_counters(sc, 0, 0, tl);
     // the per-kernel slot (vrt_kernel_stats)
@@ -1377,14 +1389,17 @@ __global__ void __launch_bounds__(256) k_drt_branch(DMedium M, PathSrc S, uint64
     }
 }
 
-int launch_drt_branch(const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t p_begin,
+int launch_drt_branch(const DMedium& M, bool ds, const PathSrc& src, uint64_t n_paths, uint64_t p_begin,
                       const unsigned long long* next_path, uint64_t seed, const float* dL, float div, const float* info,
                       const float4* resv, uint64_t max_round, DScratch* scratch, int num_sms, cudaStream_t stream) {
     if (max_round == 0) return 0;
     const uint64_t need = (max_round + 255) / 256;
     const int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
     KernelScope ks(VRT_K_DRT_BRANCH, stream);
-    k_drt_branch<<<blocks, 256, 0, stream>>>(M, src, n_paths, p_begin, next_path, seed, dL, div, info, resv, scratch);
+    if (ds) k_drt_branch<true><<<blocks, 256, 0, stream>>>(M, src, n_paths, p_begin, next_path, seed, dL, div, info, resv,
+                                                            scratch);
+    else k_drt_branch<false><<<blocks, 256, 0, stream>>>(M, src, n_paths, p_begin, next_path, seed, dL, div, info, resv,
+                                                          scratch);
     count_launches(1);
     return launch_status(cudaGetLastError());
 }

@@ -1,7 +1,9 @@
 // vrt_wave_drt.cu -- the DRT adjoint as a wavefront (sm_100a).
 //
 // The reference's differential-ratio-tracking adjoint
-// (include/vr_path_integrator_NEE_DRT.h:62-270) walks each path three times:
+// (include/vr_path_integrator_NEE_DRT.h:62-270; its DRTDS form,
+// _NEE_DRTDS.h:40-253, differs only in the replay's real collisions and the
+// branch's position sampler) walks each path three times:
 // the primal (majorant x1.05 + 0.1, R from the light rays of every real
 // collision, a reservoir vertex kept in proportion to the throughput), the
 // replay with the same draws (a sigma scatter at every tracking collision, the
@@ -26,8 +28,9 @@
 //
 // Compiled with -fmad=false, like the sequential form (vrt_path.cu), so a
 // walk here rounds as the sequential definition does.  Paths the collision log
-// cannot hold run whole on the sequential form afterwards, over a list of
-// their ids (their jobs here are skipped: first-collision word kSpilled).
+// cannot hold, and uncapped paths still going after kUncappedPass vertices,
+// run whole on the sequential form afterwards, over a list of their ids (their
+// jobs here are skipped: first-collision word kSpilled).
 #include "vrt_wave.cuh"
 
 namespace vrt {
@@ -184,7 +187,8 @@ __global__ void __launch_bounds__(256, 3) k_drt_primal(DMedium M, PathSrc S, uin
                         if (M.has_sun) ph_sun = phase(M, w, M.sun_dir);
                         jfork = rng.ntr;  // the forks of the vertex's light rays
                         rng.ntr += (uint32_t)lights;
-                        const bool capped = M.max_bounces > 0 && ++bounces >= M.max_bounces;
+                        ++bounces;
+                        const bool capped = M.max_bounces > 0 && bounces >= M.max_bounces;
                         w = phase_sample(M, rng, w);
                         float tMin;
                         boundary(M, x, w, tMin, d);
@@ -200,7 +204,12 @@ __global__ void __launch_bounds__(256, 3) k_drt_primal(DMedium M, PathSrc S, uin
                         }
                         nrec = rec_next == kNone ? 2 : 1;
                         nj = lights;
-                        if (all_less(W, EPS) || capped) ev = 2;
+                        if (all_less(W, EPS) || capped) {
+                            ev = 2;
+                        } else if (wv.kpass > 0 && bounces >= wv.kpass) {
+                            ev = 2;  // an uncapped path past the pass budget: whole, on the sequential form
+                            spill = true;
+                        }
                     }
                 }
             }
@@ -274,10 +283,12 @@ __global__ void __launch_bounds__(256, 3) k_drt_primal(DMedium M, PathSrc S, uin
 
 // The DRT replay from the log (_NEE_DRT.h:168-230 without the walk): at a null
 // collision dL/dsigma = dL/dR . -R / m / (1 - sigma / m); at a real one the
-// MIS-weighted dL/dR . (sigma^2 / (1 + sigma^2)) R / sigma, then R loses the
-// vertex's light terms (T from its record).  Lanes take paths from the
-// primal's list; the next collision and the vertex record load one iteration
-// ahead, as in k_ds_replay.
+// MIS-weighted dL/dR . (sigma^2 / (1 + sigma^2)) R / sigma (DS: none,
+// vr_path_integrator_NEE_DRTDS.h:178-222), then R loses the vertex's light
+// terms (T from its record).  Lanes take paths from the primal's list; the
+// next collision and the vertex record load one iteration ahead, as in
+// k_ds_replay.
+template <bool DS>
 __global__ void __launch_bounds__(256, 3) k_drt_replay(DMedium M, PathSrc S, const float* __restrict__ dL, float div,
                                                      DScratch* sc, WaveBw wv) {
     const float EPS = 0.00000001f;
@@ -349,8 +360,8 @@ __global__ void __launch_bounds__(256, 3) k_drt_replay(DMedium M, PathSrc S, con
                 end = true;
             } else {      // _NEE_DRT.h:187-228
                 tl.logb += (uint32_t)sizeof(VertexRec);
-                const float mis_Ts = s * s / (1.0f + s * s);
-                const float dL_dsigma = dot(dLdR, mis_Ts * R / s);
+                const float mis_Ts = DS ? 0.0f : s * s / (1.0f + s * s);
+                const float dL_dsigma = DS ? 0.0f : dot(dLdR, mis_Ts * R / s);
                 const float Te = __uint_as_float(r0.x), Ts = __uint_as_float(r0.y);
                 const float3 sa = make_float3(r1.x, r1.y, r1.z);
                 const float ph_nee = r1.w, ph_sun = r2.w;
@@ -358,7 +369,7 @@ __global__ void __launch_bounds__(256, 3) k_drt_replay(DMedium M, PathSrc S, con
                 W = W * sa;
                 R = R - W * Te * Le * ph_nee;
                 if (M.has_sun) R = R - W * Ts * M.sun_L * ph_sun;
-                sigma_bw(M, x, dL_dsigma, tl);
+                if (!DS) sigma_bw(M, x, dL_dsigma, tl);
                 ++bounces;
                 if (all_less(W, EPS) || (M.max_bounces > 0 && bounces >= M.max_bounces)) end = true;
             }
@@ -374,14 +385,20 @@ __global__ void __launch_bounds__(256, 3) k_drt_replay(DMedium M, PathSrc S, con
 // Host: rounds of primal, light-ray T, their adjoints, replay and reservoir
 // branch until every path has been taken; then the handed-over paths on the
 // sequential form.
-int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed,
-                       const float* dL, float div, cudaStream_t stream) {
+int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, int bw_mode, const PathSrc& src, uint64_t n_paths,
+                       uint64_t seed, const float* dL, float div, cudaStream_t stream) {
     if (n_paths == 0) return 0;
-    if (M.max_bounces <= 0 || M.tr_mode > 1) return VRT_E_UNSUPPORTED;
+    if (M.max_bounces < 0 || M.max_bounces > 4096 || M.tr_mode > 1) return VRT_E_UNSUPPORTED;
+    if (bw_mode != VRT_BW_NEE_DRT && bw_mode != VRT_BW_NEE_DRTDS) return VRT_E_INVALID_ARGUMENT;
+    const bool ds = bw_mode == VRT_BW_NEE_DRTDS;
     const unsigned long long lights = M.has_sun ? 2ull : 1ull;
-    const unsigned long long B = (unsigned long long)M.max_bounces;
+    // uncapped paths (the reference's default) walk at most kUncappedPass
+    // vertices here; the few that go on run whole on the sequential form
+    const int kpass = M.max_bounces > 0 ? 0 : kUncappedPass;
+    const unsigned long long B = (unsigned long long)(M.max_bounces > 0 ? M.max_bounces : kpass);
     int blocksA = persistent_blocks((const void*)k_drt_primal, 256, ctx->num_sms);
-    int blocksC = persistent_blocks((const void*)k_drt_replay, 256, ctx->num_sms);
+    int blocksC = persistent_blocks(ds ? (const void*)k_drt_replay<true> : (const void*)k_drt_replay<false>, 256,
+                                    ctx->num_sms);
     const uint64_t need = (n_paths + 255) / 256;
     if ((uint64_t)blocksA > need) blocksA = (int)need;
     if ((uint64_t)blocksC > need) blocksC = (int)need;
@@ -397,7 +414,7 @@ int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, u
     wv.cap_evs = ctx->log_limit ? ctx->log_limit : 4ull * batch_jobs(n_paths, 1, ctx->batch_limit) + inflight * 16ull;
     if (wv.cap_evs > 0xfff00000ull) wv.cap_evs = 0xfff00000ull;  // 32-bit links, kNone / kUnlogged reserved
     wv.res_evs = inflight * 16ull < wv.cap_evs / 2 ? inflight * 16ull : wv.cap_evs / 2;
-    wv.kpass = 0;
+    wv.kpass = kpass;
     wv.cap_spill = (unsigned long long)n_paths;
     const size_t o_jobs = 256, o_recs = o_jobs + wv.cap_jobs * sizeof(ShadowJob);
     const size_t o_info = o_recs + wv.cap_recs * sizeof(VertexRec), o_resv = o_info + wv.cap_paths * 32;
@@ -437,11 +454,12 @@ int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, u
             return st;
         {
             KernelScope ks(VRT_K_DRT_REPLAY, stream);
-            k_drt_replay<<<blocksC, 256, 0, stream>>>(M, src, dL, div, ctx->scratch, wv);
+            if (ds) k_drt_replay<true><<<blocksC, 256, 0, stream>>>(M, src, dL, div, ctx->scratch, wv);
+            else k_drt_replay<false><<<blocksC, 256, 0, stream>>>(M, src, dL, div, ctx->scratch, wv);
         }
         count_launches(1);
         if ((st = launch_status(cudaGetLastError()))) return st;
-        if ((st = launch_drt_branch(M, src, n_paths, wv.p_begin, &ctx->scratch->next_path, seed, dL, div, wv.info,
+        if ((st = launch_drt_branch(M, ds, src, n_paths, wv.p_begin, &ctx->scratch->next_path, seed, dL, div, wv.info,
                                     wv.resv, wv.cap_paths, ctx->scratch, ctx->num_sms, stream)))
             return st;
         unsigned long long taken = 0;
@@ -459,7 +477,7 @@ int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, u
     if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return launch_status(e);
     if (spilled > wv.cap_spill) spilled = wv.cap_spill;
     if (spilled)  // the paths the log could not hold, whole, on the sequential form
-        return launch_radiance_bw(M, VRT_BW_NEE_DRT, src, spilled, seed, dL, div, ctx->scratch, ctx->num_sms, stream,
+        return launch_radiance_bw(M, bw_mode, src, spilled, seed, dL, div, ctx->scratch, ctx->num_sms, stream,
                                   wv.spill);
     return 0;
 }

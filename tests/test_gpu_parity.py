@@ -263,8 +263,10 @@ def test_dt_integrator_matches_oracle(cuda):
     ("dt", dict(integrator="dt", sun_dir=None)),
     ("drt", dict(integrator="drt")),
     ("drt", dict(integrator="drt", majorant="grid", brick=8)),
+    ("drt", dict(integrator="drt", max_bounces=0)),
     ("drtq", dict(integrator="drtq")),
     ("drtds", dict(integrator="drtds")),
+    ("drtds", dict(integrator="drtds", majorant="grid", brick=8)),
     ("sps", dict(integrator="sps")),
     ("sps", dict(integrator="sps", majorant="grid", brick=8)),
 ])
@@ -331,9 +333,10 @@ def test_ds_collision_log_overflow_rewalks(cuda, limit):
         assert np.abs(a).sum() > 0 and rel < 1e-4, rel
 
 
+@pytest.mark.parametrize("integrator", ["drt", "drtds"])
 @pytest.mark.parametrize("limit", [1, 3000])
-def test_drt_wavefront_matches_sequential_form(cuda, limit):
-    """The DRT adjoint's wavefront (primal with collision log, light-ray T and
+def test_drt_wavefront_matches_sequential_form(cuda, limit, integrator):
+    """The DRT (and DRTDS) adjoint's wavefront (primal with collision log, light-ray T and
     adjoint jobs, log replay, reservoir branch) against its sequential form:
     with the collision log capped at `limit` records, the paths that do not fit
     run whole on the sequential form (all of them at 1), so the gradients of
@@ -347,7 +350,7 @@ def test_drt_wavefront_matches_sequential_form(cuda, limit):
     dimg, grads, stats = None, [], []
     for lim in (0, limit):
         field = build_field(sig, albedo=0.9, env=1.0, sun_dir=(0.3, 0.8, 0.5), sun_radiance=3.0, g=0.4,
-                            max_bounces=16, sigma_requires_grad=True, integrator="drt", majorant="grid", brick=8)
+                            max_bounces=16, sigma_requires_grad=True, integrator=integrator, majorant="grid", brick=8)
         _lib.check(lib.vrt_set_collision_log_limit(ctx.ptr, lim))
         try:
             maps.check()
