@@ -571,7 +571,7 @@ def run_path_adjoints(args, wl, sig, flush, dev):
     environment + sun): device ms of the forward capture, of forward +
     backward, and their difference, per adjoint; adjoint paths/s."""
     import torch
-    from rendervous_b200 import maps, synthetic
+    from rendervous_b200 import _lib, maps, synthetic
     sp = torch.nn.Parameter(sig.clone())
     bmin, bmax = maps.normalized_box(sp)
     sg = maps.Grid3D(sp, bmin, bmax)
@@ -599,6 +599,11 @@ def run_path_adjoints(args, wl, sig, flush, dev):
     cam = maps.PerspectiveCameraSensor(wl["width"], wl["height"],
                                        torch.from_numpy(synthetic.ring_poses(wl["views"])).to(dev), jittered=True)
     n_paths = wl["width"] * wl["height"] * wl["views"] * wl["spp"]
+    ffi, lib = _lib.ffi_lib()
+    kid = {"walk_fw": lib.VRT_K_WALK_FW, "shadow_fw": lib.VRT_K_SHADOW_FW, "ds_primal": lib.VRT_K_DS_PRIMAL,
+           "shadow_T": lib.VRT_K_SHADOW_T, "ds_replay": lib.VRT_K_DS_REPLAY, "shadow_adj": lib.VRT_K_SHADOW_ADJ,
+           "drt_primal": lib.VRT_K_DRT_PRIMAL, "drt_replay": lib.VRT_K_DRT_REPLAY, "drt_branch": lib.VRT_K_DRT_BRANCH,
+           "sps_primal": lib.VRT_K_SPS_PRIMAL, "sps_replay": lib.VRT_K_SPS_REPLAY}
     out = {}
     for name, field in fields.items():
         k = {"i": 0}
@@ -615,10 +620,21 @@ def run_path_adjoints(args, wl, sig, flush, dev):
             img.sum().backward()
         maps.check()
         t_fw = statistics.mean(_timed(fw, args.steps, args.warmup, flush))
-        t_all = statistics.mean(_timed(fwbw, args.steps, args.warmup, flush))
+        # per-kernel event times of the wavefront adjoints over the timed forward + backward calls
+        ks = ffi.new("vrt_kernel_stat[]", lib.VRT_K_COUNT)
+        _lib.check(lib.vrt_kernel_stats(_lib.context(dev).ptr, _lib.stream_handle(dev), ks))
+        lib.vrt_set_kernel_timing(1)
+        try:
+            t_all = statistics.mean(_timed(fwbw, args.steps, args.warmup, flush))
+            _lib.check(lib.vrt_kernel_stats(_lib.context(dev).ptr, _lib.stream_handle(dev), ks))
+        finally:
+            lib.vrt_set_kernel_timing(0)
         maps.check()
         t_bw = max(t_all - t_fw, 1e-6)
-        out[name] = {"fw_ms": t_fw, "fwbw_ms": t_all, "bw_ms": t_bw, "bw_paths_per_s": n_paths / (t_bw / 1e3)}
+        calls = args.steps + args.warmup
+        kms = {kn: ks[ki].ms / calls for kn, ki in kid.items() if ks[ki].launches}
+        out[name] = {"fw_ms": t_fw, "fwbw_ms": t_all, "bw_ms": t_bw, "bw_paths_per_s": n_paths / (t_bw / 1e3),
+                     "kernel_ms": kms}
     return {"metric": "adjoint paths/s", "value": out["DRT"]["bw_paths_per_s"], "unit": "paths/s",
             "ms_per_step": out["DRT"]["fwbw_ms"], "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
             "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded generators)",

@@ -181,7 +181,9 @@ enum {
     VRT_K_DRT_PRIMAL = 7,  /* DRT adjoint: primal walk (collision log, light jobs, reservoir) */
     VRT_K_DRT_REPLAY = 8,  /* DRT adjoint: replay of the logged collisions (sigma scatters) */
     VRT_K_DRT_BRANCH = 9,  /* DRT adjoint: the reservoir vertex's branch, one per path */
-    VRT_K_COUNT = 10
+    VRT_K_SPS_PRIMAL = 10, /* SPS adjoint: primal walk (segment log, light jobs) */
+    VRT_K_SPS_REPLAY = 11, /* SPS adjoint: replay of the logged vertices (sigma and dL/dtau scatters) */
+    VRT_K_COUNT = 12
 };
 typedef struct vrt_kernel_stat {
     int64_t launches;

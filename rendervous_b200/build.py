@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvrt.so")
 SOURCES = ["vrt_api.cu", "vrt_transmittance.cu", "vrt_path.cu", "vrt_adjoint.cu", "vrt_wave.cu", "vrt_wave_ds.cu",
-           "vrt_cache.cu", "vrt_noalloc.cu", "vrt_collision.cu", "vrt_fp64.cu", "vrt_wave_drt.cu"]
+           "vrt_cache.cu", "vrt_noalloc.cu", "vrt_collision.cu", "vrt_fp64.cu", "vrt_wave_drt.cu", "vrt_wave_sps.cu"]
 HEADERS = ["vrt_device.cuh", "vrt_tracking.cuh", "vrt_params.h", "vrt_internal.h", "vrt_wave.cuh"]
 
 NVCC_FLAGS = [
@@ -66,9 +66,11 @@ def up_to_date() -> bool:
 # draws a sample takes; rounding as the CPU restatement does keeps them on the
 # same paths.  vrt_collision.cu and vrt_fp64.cu: the collision integrators and
 # the FP64 tracer follow the CPU restatement's rounding the same way.
-# vrt_wave_drt.cu: the DRT wavefront's primal takes the sequential form's paths.
+# vrt_wave_drt.cu, vrt_wave_sps.cu: the DRT and SPS wavefronts' primals take the
+# sequential forms' paths.
 PER_FILE_FLAGS = {"vrt_wave_ds.cu": ["-fmad=false"], "vrt_path.cu": ["-fmad=false"], "vrt_collision.cu": ["-fmad=false"],
-                  "vrt_fp64.cu": ["-fmad=false"], "vrt_wave_drt.cu": ["-fmad=false"]}
+                  "vrt_fp64.cu": ["-fmad=false"], "vrt_wave_drt.cu": ["-fmad=false"],
+                  "vrt_wave_sps.cu": ["-fmad=false"]}
 OBJ_DIR = os.path.join(HERE, "_build")
 
 

@@ -94,6 +94,10 @@ static bool use_wave_bw(const DMedium& M, int bw_mode) {
 static bool use_wave_drt(const DMedium& M, int bw_mode) {
     return (bw_mode == VRT_BW_NEE_DRT || bw_mode == VRT_BW_NEE_DRTDS) && M.max_bounces <= 4096 && M.tr_mode <= 1;
 }
+// the SPS adjoint on the wavefront (capped or not): ratio / delta tracking light rays
+static bool use_wave_sps(const DMedium& M, int bw_mode) {
+    return bw_mode == VRT_BW_NEE_SPS && M.max_bounces <= 4096 && M.tr_mode <= 1;
+}
 
 static bool is_collision(int integrator) {
     return integrator == VRT_PI_MC_COLLISION || integrator == VRT_PI_DDA_COLLISION;
@@ -687,6 +691,8 @@ int vrt_radiance_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, cons
     if (use_wave_bw(M, bw_mode)) return launch_wave_ds_bw(ctx, M, S, (uint64_t)n, seed, dL_dR, 1.0f, (cudaStream_t)stream);
     if (use_wave_drt(M, bw_mode))
         return launch_wave_drt_bw(ctx, M, bw_mode, S, (uint64_t)n, seed, dL_dR, 1.0f, (cudaStream_t)stream);
+    if (use_wave_sps(M, bw_mode))
+        return launch_wave_sps_bw(ctx, M, S, (uint64_t)n, seed, dL_dR, 1.0f, (cudaStream_t)stream);
     return launch_radiance_bw(M, bw_mode, S, (uint64_t)n, seed, dL_dR, 1.0f, ctx->scratch, ctx->num_sms,
                               (cudaStream_t)stream);
 }
@@ -739,6 +745,9 @@ int vrt_capture_bw(vrt_context* ctx, const vrt_medium* m, int32_t bw_mode, const
                                  (cudaStream_t)stream);
     if (use_wave_drt(M, bw_mode))
         return launch_wave_drt_bw(ctx, M, bw_mode, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
+                                  (cudaStream_t)stream);
+    if (use_wave_sps(M, bw_mode))
+        return launch_wave_sps_bw(ctx, M, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
                                   (cudaStream_t)stream);
     return launch_radiance_bw(M, bw_mode, S, (uint64_t)S.npix * (uint64_t)spp, seed, dL_drgb, (float)spp,
                               ctx->scratch, ctx->num_sms, (cudaStream_t)stream);

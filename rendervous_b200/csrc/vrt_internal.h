@@ -70,6 +70,9 @@ int launch_radiance_bw(const DMedium& M, int bw_mode, const PathSrc& src, uint64
 // paths [p_begin, min(*next_path, n_paths)) (at most max_round).
 int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, int bw_mode, const PathSrc& src, uint64_t n_paths,
                        uint64_t seed, const float* dL, float div, cudaStream_t stream);
+// Wavefront SPS adjoint (vrt_wave_sps.cu): ratio or delta tracking light rays.
+int launch_wave_sps_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed,
+                       const float* dL, float div, cudaStream_t stream);
 int launch_drt_branch(const DMedium& M, bool ds, const PathSrc& src, uint64_t n_paths, uint64_t p_begin,
                       const unsigned long long* next_path, uint64_t seed, const float* dL, float div, const float* info,
                       const float4* resv, uint64_t max_round, DScratch* scratch, int num_sms, cudaStream_t stream);

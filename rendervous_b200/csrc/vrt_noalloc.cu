@@ -9,7 +9,7 @@
 // kernel updates live in a fixed array compiled into libvrt.so.
 //
 //   - The array holds at most kMaxBricks majorant bricks (64^3 = 262144, one
-//     float each: 1 MiB) after a 512-byte block for the kernel counters.  Every
+//     float each: 1 MiB) after a 1024-byte block for the kernel counters.  Every
 //     GPU that loads the library keeps this memory until the process exits.
 //   - Every call shares the array and overwrites it; the counters are cleared
 //     at the start of each call.  Calls whose kernels overlap on the GPU (on
@@ -33,7 +33,7 @@ namespace vrt {
 namespace {
 
 constexpr int kMaxBricks = 64 * 64 * 64;
-constexpr size_t kCounterBytes = 512;
+constexpr size_t kCounterBytes = 1024;
 constexpr size_t kScratchBytes = kCounterBytes + sizeof(float) * (size_t)kMaxBricks;
 constexpr int kCacheSlots = 64;
 

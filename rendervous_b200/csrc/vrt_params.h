@@ -68,7 +68,7 @@ struct DScratch {
     unsigned int detail;           // which guard raised a device error (bit per site)
     // per-kernel tallies of the wavefront kernels (VRT_K_*): steps, lookups, atomics, albedo lookups,
     // collision-log bytes; not cleared by vrt_context_sync, read and cleared by vrt_kernel_stats
-    unsigned long long kstat[10][5];
+    unsigned long long kstat[12][5];
 };
 
 }  // namespace vrt

@@ -434,15 +434,19 @@ constexpr int kKeep = 16;  // first-pass collisions a transmittance adjoint keep
 // for bit -- so this kernel needs nothing from the replay.  No adjoint runs
 // for rays from or after a singular (zero-density) vertex, where the
 // reference's replay stops (vr_path_integrator_NEE_DS.h:153-154), nor for
-// paths the state machine runs (first-collision word kSpilled).  DRT: the jobs
-// of the DRT adjoint (vr_path_integrator_NEE_DRT.h:68-69, 165-167): every job
-// has an adjoint, drawn from fork j of the adjoint's own stream 1.
-template <int TR, bool DRT>
+// paths the state machine runs (first-collision word kSpilled).  MODE
+// ADJ_DRT: the jobs of the DRT adjoint (vr_path_integrator_NEE_DRT.h:68-69,
+// 165-167): every job has an adjoint, drawn from fork j of the adjoint's own
+// stream 1.  ADJ_SPS: the same for the SPS adjoint (_NEE_SPS.h:115-116,
+// 228-234), whose rays after the singular vertex (record word bit 1) weigh
+// dL/dT by that vertex's sigma (per path in aux[k].w).
+template <int TR, int MODE>
 __global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, PathSrc S, const ShadowJob* __restrict__ jobs,
                                                      const unsigned long long* __restrict__ count,
                                                      unsigned long long cap, unsigned long long* head, uint64_t seed,
                                                      const float* __restrict__ info, uint64_t p_begin,
-                                                     const float* __restrict__ dL, float div, DScratch* sc) {
+                                                     const float* __restrict__ dL, float div, DScratch* sc,
+                                                     const float4* __restrict__ aux) {
     unsigned long long n = *count;
     if (n > cap) n = cap;
     ShadowRay s;
@@ -465,10 +469,13 @@ __global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, PathSrc S, con
                 } else {
                     jv = get_job(jobs, i);
                     dLdT = 0.0f;
-                    if ((DRT || !(jv.tgt & 2u)) && __float_as_uint(info[8 * (jv.pid - p_begin) + 7]) != kSpilled)
+                    if ((MODE != ADJ_DS || !(jv.tgt & 2u)) &&
+                        __float_as_uint(info[8 * (jv.pid - p_begin) + 7]) != kSpilled) {
                         dLdT = dot(ld3(dL + 3 * out_index(S, jv.pid)) / div, jv.wt);
+                        if (MODE == ADJ_SPS && jv.tgt != kAdjOnly && (jv.tgt & 2u)) dLdT *= aux[jv.pid - p_begin].w;
+                    }
                     nkeep = 0;
-                    if (dLdT != 0.0f && shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork, DRT ? 1u : 0u))
+                    if (dLdT != 0.0f && shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork, MODE != ADJ_DS ? 1u : 0u))
                         phase = 1;
                 }
             }
@@ -499,7 +506,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, PathSrc S, con
                         }
                         phase = 0;
                     } else {  // replay the second pass
-                        shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork, DRT ? 1u : 0u);
+                        shadow_begin(M, s, jv.x, jv.dir, seed, jv.pid, jv.fork, MODE != ADJ_DS ? 1u : 0u);
                         phase = 2;
                     }
                 }
@@ -673,16 +680,20 @@ int launch_shadow_record(const DMedium& M, const PathSrc& src, const WaveBw& wv,
 }
 
 int launch_shadow_adjoint(const DMedium& M, const PathSrc& src, const WaveBw& wv, uint64_t seed, const float* dL,
-                          float div, DScratch* sc, int num_sms, cudaStream_t stream, bool drt) {
+                          float div, DScratch* sc, int num_sms, cudaStream_t stream, int mode) {
     if (M.tr_mode > 1) return VRT_OK;  // DDA: in k_shadow_T; GRT / GDT: no backward
     KernelScope ks(VRT_K_SHADOW_ADJ, stream);
 #define VRT_ADJ(TR, D)                                                                                             \
     k_shadow_adj<TR, D><<<persistent_blocks((const void*)k_shadow_adj<TR, D>, 256, num_sms), 256, 0, stream>>>( \
-        M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, wv.info, wv.p_begin, dL, div, sc)
+        M, src, wv.jobs, &wv.hdr[0], wv.cap_jobs, &wv.hdr[4], seed, wv.info, wv.p_begin, dL, div, sc, wv.resv)
     if (M.tr_mode == 0) {
-        if (drt) VRT_ADJ(0, true); else VRT_ADJ(0, false);
+        if (mode == ADJ_DRT) VRT_ADJ(0, ADJ_DRT);
+        else if (mode == ADJ_SPS) VRT_ADJ(0, ADJ_SPS);
+        else VRT_ADJ(0, ADJ_DS);
     } else {
-        if (drt) VRT_ADJ(1, true); else VRT_ADJ(1, false);
+        if (mode == ADJ_DRT) VRT_ADJ(1, ADJ_DRT);
+        else if (mode == ADJ_SPS) VRT_ADJ(1, ADJ_SPS);
+        else VRT_ADJ(1, ADJ_DS);
     }
 #undef VRT_ADJ
     count_launches(1);

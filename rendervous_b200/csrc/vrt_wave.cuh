@@ -406,9 +406,10 @@ struct WaveBw {
     unsigned long long* spill;
     unsigned long long* spill_count;
     unsigned long long cap_spill;
-    // the DRT adjoint's reservoir per path of the round (4 float4: vertex and
+    // per path of the round: the DRT adjoint's reservoir (4 float4: vertex and
     // its weight, direction and the running total, throughput and the stream
-    // position at the end of the primal); null for NEE_DS
+    // position at the end of the primal), or the SPS adjoint's entry point and
+    // singular-vertex sigma (1 float4); null for NEE_DS
     float4* resv;
 };
 
@@ -421,9 +422,11 @@ struct WaveBw {
 // the same jobs with dL/dT = dL/dR(pixel) / div . weight (head: hdr[4]).
 int launch_shadow_record(const DMedium& M, const PathSrc& src, const wave::WaveBw& wv, uint64_t seed, const float* dL,
                          float div, DScratch* sc, int num_sms, cudaStream_t stream);
-// drt: the DRT adjoint's jobs (forks of stream 1, every job but those of
-// handed-over paths, kAdjOnly jobs included).
+// mode ADJ_DRT / ADJ_SPS: the DRT or SPS adjoint's jobs (forks of stream 1,
+// every job but those of handed-over paths, kAdjOnly jobs included; SPS: the
+// rays after the singular vertex weighed by its sigma, wv.resv[k].w).
+enum : int { ADJ_DS = 0, ADJ_DRT = 1, ADJ_SPS = 2 };
 int launch_shadow_adjoint(const DMedium& M, const PathSrc& src, const wave::WaveBw& wv, uint64_t seed, const float* dL,
-                          float div, DScratch* sc, int num_sms, cudaStream_t stream, bool drt = false);
+                          float div, DScratch* sc, int num_sms, cudaStream_t stream, int mode = ADJ_DS);
 
 }  // namespace vrt

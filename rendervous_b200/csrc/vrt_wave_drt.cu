@@ -450,7 +450,7 @@ int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, int bw_mode, const Pa
         }
         count_launches(1);
         if ((st = launch_shadow_record(M, src, wv, seed, dL, div, ctx->scratch, ctx->num_sms, stream))) return st;
-        if ((st = launch_shadow_adjoint(M, src, wv, seed, dL, div, ctx->scratch, ctx->num_sms, stream, true)))
+        if ((st = launch_shadow_adjoint(M, src, wv, seed, dL, div, ctx->scratch, ctx->num_sms, stream, ADJ_DRT)))
             return st;
         {
             KernelScope ks(VRT_K_DRT_REPLAY, stream);

@@ -269,6 +269,7 @@ def test_dt_integrator_matches_oracle(cuda):
     ("drtds", dict(integrator="drtds", majorant="grid", brick=8)),
     ("sps", dict(integrator="sps")),
     ("sps", dict(integrator="sps", majorant="grid", brick=8)),
+    ("sps", dict(integrator="sps", max_bounces=0)),
 ])
 def test_capture_backward_matches_oracle(cuda, bw, kw):
     wl = synthetic.WORKLOADS["plain_forward_64"]
@@ -333,10 +334,10 @@ def test_ds_collision_log_overflow_rewalks(cuda, limit):
         assert np.abs(a).sum() > 0 and rel < 1e-4, rel
 
 
-@pytest.mark.parametrize("integrator", ["drt", "drtds"])
+@pytest.mark.parametrize("integrator", ["drt", "drtds", "sps"])
 @pytest.mark.parametrize("limit", [1, 3000])
 def test_drt_wavefront_matches_sequential_form(cuda, limit, integrator):
-    """The DRT (and DRTDS) adjoint's wavefront (primal with collision log, light-ray T and
+    """The DRT (DRTDS, SPS) adjoint's wavefront (primal with collision log, light-ray T and
     adjoint jobs, log replay, reservoir branch) against its sequential form:
     with the collision log capped at `limit` records, the paths that do not fit
     run whole on the sequential form (all of them at 1), so the gradients of
@@ -364,7 +365,8 @@ def test_drt_wavefront_matches_sequential_form(cuda, limit, integrator):
         finally:
             _lib.check(lib.vrt_set_collision_log_limit(ctx.ptr, 0))
         grads.append(field.sigma.grid.grad.cpu().numpy())
-        stats.append({k: getattr(ks[lib.VRT_K_DRT_REPLAY], k) for k in ("steps", "reds")})
+        replay = lib.VRT_K_SPS_REPLAY if integrator == "sps" else lib.VRT_K_DRT_REPLAY
+        stats.append({k: getattr(ks[replay], k) for k in ("steps", "reds")})
     assert stats[0]["steps"] > 0 and stats[0]["reds"] > 0, stats  # the automatic log holds the paths
     if limit == 1:
         assert stats[1]["steps"] == 0, stats  # nothing fit: every path ran on the sequential form
