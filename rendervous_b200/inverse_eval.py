@@ -1,6 +1,7 @@
 """Inverse-rendering loop (workload inverse_rendering_128).
 
-Target: a seeded 256^3 blob volume rendered from 8 cameras on a ring of radius
+Target: a seeded 256^3 blob volume (64 blobs, max sigma 40, like the
+differentiable tracer's) rendered from 8 cameras on a ring of radius
 2 (elevation 20 degrees) at 256x256, 128 spp.  Optimised: a 128^3 FP32 sigma
 grid initialised to 1.0, albedo fixed at 0.9, HG g = 0.3, unit environment
 plus a directional light.  Each iteration captures all 8 views in one call (16
@@ -122,10 +123,11 @@ def main(argv=None):
     ap.add_argument("--res", type=int, default=128)
     ap.add_argument("--target-res", type=int, default=256)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--lr", type=float, default=None, help="Adam learning rate (default: the workload's 0.01)")
     ap.add_argument("--out", type=str, default=None)
     a = ap.parse_args(argv)
     out = run(a.iterations, a.width, a.spp, a.target_spp, a.views, a.res, a.target_res, a.seed,
-              log=lambda d: print(json.dumps(d), flush=True))
+              log=lambda d: print(json.dumps(d), flush=True), lr=a.lr)
     print(json.dumps(out))
     if a.out:
         with open(a.out, "w") as f:

@@ -165,8 +165,10 @@ WORKLOADS = {
         sigma=("blobs", dict(res=256, n_blobs=64, max_sigma=40.0, seed=6)),
         albedo=("uniform", dict(res=256, lo=0.6, hi=0.95, seed=8)), phase_g=0.6, env=1.0, sun_intensity=3.0,
         sun_seed=6, width=512, height=512, spp=64, max_bounces=64, views=1, render_seed=9, target_seed=7),
+    # the target: a 256^3 seeded blob volume like the differentiable tracer's (64 blobs, max sigma 40),
+    # with its own seed
     "inverse_rendering_128": dict(
-        target_sigma=("blobs", dict(res=256, n_blobs=12, max_sigma=20.0, seed=10)), res=128, init_sigma=1.0,
+        target_sigma=("blobs", dict(res=256, n_blobs=64, max_sigma=40.0, seed=10)), res=128, init_sigma=1.0,
         albedo=0.9, phase_g=0.3, views=8, width=256, height=256, target_spp=128, spp=16, max_bounces=32,
         lr=0.01, iterations=500),
     "radiance_cache_512": dict(
