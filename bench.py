@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-c5", action="store_true", help="skip the radiance-cache equal-time comparison")
+    ap.add_argument("--no-c4", action="store_true", help="skip the inverse-rendering loop")
     ap.add_argument("--workload", default=WORKLOAD,
                     choices=[WORKLOAD, "plain_forward_64", "dda_transmittance_256", "path_adjoints_64"],
                     help="the timed workload (default: the differentiable path tracer); the others print "
@@ -467,6 +468,18 @@ def run_ours(args):
         c5 = cache_eval.equal_time(ref_spp=4096, budget=3.0, warmup=64)
         maps.set_sync_checks(False)
 
+    # the inverse-rendering loop (8-view capture, NEE_DS adjoint, Adam; 500
+    # iterations at lr 0.01 on the 128^3 grid), outside the timed region
+    c4 = None
+    if rank == 0 and world == 1 and not args.no_c4:
+        from rendervous_b200 import inverse_eval
+        torch.cuda.empty_cache()
+        r = inverse_eval.run(device=dev)
+        c4 = {k: r[k] for k in ("workload", "iterations", "views", "width", "spp", "res", "lr", "iterations_per_s",
+                                "loss_first", "loss_final", "heldout_loss_initial", "heldout_loss_final",
+                                "sigma_rel_err_initial", "sigma_rel_err_final")}
+        maps.set_sync_checks(False)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, sample, thr, secs = cpu_sample()
@@ -505,6 +518,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "c5_equal_time_mse": c5,
+            "c4_inverse_rendering": c4,
         }
         print(json.dumps(line))
     if world > 1:
