@@ -138,7 +138,9 @@ template <typename T> struct Scene;
 // over the brick grid started at the segment's first query.  The brick of the
 // start point is chosen with the 1e-4-brick nudge of Scene::majorant, the face
 // distances use correctly rounded reciprocals, and outside the grid's box the
-// bound is 0.  With the constant majorant it is inert.
+// bound is 0.  A segment that never reaches the grid (tested at its start)
+// gets no face to cross; one that leaves it walks on through bound-0 bricks
+// until it ends.  With the constant majorant it is inert.
 template <typename T> struct BrickWalk {
     bool live = false;
     int c[3] = {0, 0, 0}, st[3] = {0, 0, 0};
@@ -169,6 +171,7 @@ template <typename T> struct BrickWalk {
             }
         }
         m = lookup(s);
+        if (never_enters(s)) tn[0] = tn[1] = tn[2] = inf;  // a segment that never reaches the grid: no face
     }
     int axis() const { return (tn[0] <= tn[1] && tn[0] <= tn[2]) ? 0 : (tn[1] <= tn[2] ? 1 : 2); }
     bool never_enters(const orc_scene& s) const {
@@ -179,7 +182,6 @@ template <typename T> struct BrickWalk {
     T query(const orc_scene& s, V3<T> x, V3<T> w, T& md) {
         if (s.majorant_mode == 0) { md = T(1000000.0); return (T)s.global_majorant; }
         if (!live) init(s, x, w);
-        if (never_enters(s)) { md = T(1000000.0); return T(0); }
         md = tn[axis()] - t;
         return m;
     }

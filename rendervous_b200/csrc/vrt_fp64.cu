@@ -119,6 +119,7 @@ struct BrickWalkD {
             }
         }
         m = lookup(M);
+        if (never_enters(M)) tn[0] = tn[1] = tn[2] = inf;  // a segment that never reaches the grid: no face
     }
     __device__ __forceinline__ int axis() const { return (tn[0] <= tn[1] && tn[0] <= tn[2]) ? 0 : (tn[1] <= tn[2] ? 1 : 2); }
     __device__ __forceinline__ bool never_enters(const DMedium& M) const {
@@ -130,7 +131,6 @@ struct BrickWalkD {
     __device__ __forceinline__ double query(const DMedium& M, D3 x, D3 w, double& md) {
         if (M.maj_mode == 0) { md = 1000000.0; return (double)M.gmaj; }
         if (!live) init(M, x, w);
-        if (never_enters(M)) { md = 1000000.0; return 0.0; }
         md = tn[axis()] - t;
         return m;
     }

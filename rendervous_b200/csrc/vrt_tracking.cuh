@@ -31,7 +31,10 @@ constexpr int kStepCap = 1 << 24;  // per-segment iteration bound (error VRT_E_I
 // start point gets the 1e-4-brick nudge of majorant(), face distances use
 // correctly rounded reciprocals, and outside the grid's box the bound is 0.
 // Inert with the constant majorant.  Axis selection is by branches so the
-// state stays in registers.
+// state stays in registers.  Whether the segment reaches the grid at all is
+// tested once, at the start (a segment that does not gets no face: infinite
+// face distances); one that leaves the grid walks on through bound-0 bricks
+// until it ends, so a query tests nothing but the three face distances.
 struct BrickWalk {
     bool live = false;
     int c0, c1, c2, s0, s1, s2;
@@ -39,7 +42,8 @@ struct BrickWalk {
 
     __device__ __forceinline__ void reset() { live = false; }
     __device__ __forceinline__ float lookup(const DMedium& M) const {
-        if (c0 < 0 || c0 >= M.Mx || c1 < 0 || c1 >= M.My || c2 < 0 || c2 >= M.Mz) return 0.0f;
+        if ((unsigned)c0 >= (unsigned)M.Mx || (unsigned)c1 >= (unsigned)M.My || (unsigned)c2 >= (unsigned)M.Mz)
+            return 0.0f;
         return __ldg(M.maj + ((c2 * M.My + c1) * M.Mx + c0));
     }
     __device__ __forceinline__ static void axis_init(float x, float bmin, float scale, float w, int& c, int& st, float& n,
@@ -66,6 +70,10 @@ struct BrickWalk {
         axis_init(x.y, M.bmin.y, M.maj_scale.y, w.y, c1, s1, n1, d1);
         axis_init(x.z, M.bmin.z, M.maj_scale.z, w.z, c2, s2, n2, d2);
         m = lookup(M);
+        if (never_enters(M)) {  // a segment that never reaches the grid: no face to cross
+            const float inf = __int_as_float(0x7f800000);
+            n0 = inf; n1 = inf; n2 = inf;
+        }
     }
     __device__ __forceinline__ bool never_enters(const DMedium& M) const {
         return (c0 < 0 && s0 <= 0) || (c0 >= M.Mx && s0 >= 0) || (c1 < 0 && s1 <= 0) || (c1 >= M.My && s1 >= 0) ||
@@ -75,7 +83,6 @@ struct BrickWalk {
     __device__ __forceinline__ float query(const DMedium& M, float3 x, float3 w, float& md) {
         if (M.maj_mode == 0) { md = 1000000.0f; return M.gmaj; }
         if (!live) init(M, x, w);
-        if (never_enters(M)) { md = 1000000.0f; return 0.0f; }
         float nt = (n0 <= n1 && n0 <= n2) ? n0 : (n1 <= n2 ? n1 : n2);
         md = nt - t;
         return m;
