@@ -276,6 +276,9 @@ __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tal
     hit = false;
     const float EPS = 0.0000001f;
     float md, maj, t;
+    // a flight draws its optical depth once (crossings keep it positive)
+    if (!BW && s.ff.tau < 0.0f) ++tl.steps;
+    s.ff.sample(s.r);
     for (int c = 0;; ++c) {
         if (++s.it > kStepCap) {
             raise_status(&sc->status, 4);
@@ -283,12 +286,11 @@ __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tal
         }
         const float q = s.ff.bk.query(M, s.x, s.dir, md);
         maj = BW ? gmax(EPS, q + 0.1f) : gmax(EPS, q);
-        if (!BW && s.ff.tau < 0.0f) ++tl.steps;
         // the flight crosses the brick face when its optical depth exceeds
         // majorant x distance to the face: tested without a division, and the
         // crossing leaves the depth positive
         if (TR == 0) {
-            const float tau = s.ff.sample(s.r);
+            const float tau = s.ff.tau;
             if (md < s.d && tau > md * maj) {
                 s.x = s.x + s.dir * md;
                 s.d -= md;
@@ -299,7 +301,7 @@ __device__ __forceinline__ bool shadow_event(const DMedium& M, ShadowRay& s, Tal
             }
             t = tau / maj;
         } else {
-            const float tau = s.ff.sample(s.r);
+            const float tau = s.ff.tau;
             const bool crosses = tau > md * maj;
             t = md;
             if (!crosses) t = gmin(md, tau / maj);
