@@ -85,15 +85,19 @@ struct PathSrc {
 };
 
 // Radiance-cache forms of the forward NEE kernel.
-enum : int { FW_PLAIN = 0, FW_CUT = 1, FW_TRAIN = 2 };
+enum : int { FW_PLAIN = 0, FW_CUT = 1, FW_TRAIN = 2, FW_BRANCH = 3 };
 struct CacheIO {
     int cut;         // >= 0: a path stops at its (cut+1)-th real collision and records a query there
                      // (always in FW_CUT; FW_TRAIN with cut < 0 traces full paths)
     int rec;         // FW_TRAIN: collisions recorded per path as training samples
     float* q;        // 3 planes [n_paths, 3]: position, direction, throughput (0: no query)
     float* smp;      // FW_TRAIN: 4 planes [n_paths*rec, 3]: position, direction, R at arrival, throughput
-    float* pR;       // FW_TRAIN: [n_paths, 3] the path's estimate without its cache query
+    float* pR;       // FW_TRAIN: [n_paths, 3] the path's estimate without its cache query; FW_BRANCH: the estimates
     long long rows;  // rows of a query plane (n_paths)
+    // FW_BRANCH: per item 3 float4 -- start point and stream draw count, direction and fork count,
+    // path id (low, high words) -- a scattered-only NEE path from a given stream position
+    const float4* branch;
+    unsigned long long* queue;  // FW_BRANCH: the items' work counter (zeroed by the caller)
 };
 
 }  // namespace vrt

@@ -100,6 +100,10 @@ __device__ __forceinline__ void st3(float* p, float3 v) {
 template <int MODE>
 __device__ __forceinline__ void end_path(const PathSrc& S, const NeeLane& L, float* out, float scale,
                                          const CacheIO& io) {
+    if (MODE == FW_BRANCH) {  // the scattered-only path's estimate, per item
+        st3(io.pR + 3 * L.oidx, L.R);
+        return;
+    }
     if (MODE == FW_TRAIN) {
         const long long n = io.rows * io.rec;
         st3(io.pR + 3 * L.pid, L.R);
@@ -184,7 +188,8 @@ __global__ void __launch_bounds__(256, 3) k_nee_fw(DMedium M, PathSrc S, uint64_
         if (want) {
             int leader = __ffs(want) - 1;
             unsigned long long base = 0;
-            if ((int)lane == leader) base = atomicAdd(&sc->next_path, (unsigned long long)__popc(want));
+            if ((int)lane == leader)
+                base = atomicAdd(MODE == FW_BRANCH ? io.queue : &sc->next_path, (unsigned long long)__popc(want));
             base = __shfl_sync(kFull, base, leader);
             if (L.state == ST_DEAD && !exhausted) {
                 uint64_t pid = base + __popc(want & ((1u << lane) - 1u));
@@ -192,13 +197,23 @@ __global__ void __launch_bounds__(256, 3) k_nee_fw(DMedium M, PathSrc S, uint64_
                     exhausted = true;
                 } else {
                     // path_integrator_NEE prologue (vr_path_integrator_NEE.h:3-14)
-                    L.rng.init(seed, pid, 0);
                     float3 x0, w0;
-                    if (MODE == FW_TRAIN && S.is_camera) {  // a random pixel: the path's first draw
-                        const uint64_t px = ((uint64_t)L.rng.u32() * (uint64_t)S.npix) >> 32;
-                        primary_ray(S, px, L.rng, x0, w0, L.oidx);
+                    if (MODE == FW_BRANCH) {  // a given start, on its path's stream where the caller left it
+                        const float4 a = io.branch[3 * pid], b = io.branch[3 * pid + 1], c = io.branch[3 * pid + 2];
+                        const uint64_t gp = (uint64_t)__float_as_uint(c.x) | ((uint64_t)__float_as_uint(c.y) << 32);
+                        L.rng.init(seed, gp, 0);
+                        L.rng.seek(Rng::Pos{__float_as_uint(a.w), __float_as_uint(b.w)});
+                        x0 = make_float3(a.x, a.y, a.z);
+                        w0 = make_float3(b.x, b.y, b.z);
+                        L.oidx = (long long)pid;
                     } else {
-                        primary_ray(S, pid, L.rng, x0, w0, L.oidx);
+                        L.rng.init(seed, pid, 0);
+                        if (MODE == FW_TRAIN && S.is_camera) {  // a random pixel: the path's first draw
+                            const uint64_t px = ((uint64_t)L.rng.u32() * (uint64_t)S.npix) >> 32;
+                            primary_ray(S, px, L.rng, x0, w0, L.oidx);
+                        } else {
+                            primary_ray(S, pid, L.rng, x0, w0, L.oidx);
+                        }
                     }
                     L.pid = (long long)pid;
                     L.nrec = 0;
@@ -220,11 +235,17 @@ __global__ void __launch_bounds__(256, 3) k_nee_fw(DMedium M, PathSrc S, uint64_
                     L.kind = SH_DIRECT;
                     L.parked = false;
                     ++n_paths_done;
-                    int ev = start_shadow(M, L, L.x, L.w, tl);
-                    if (ev == EV_SHADOW_DONE) {
-                        L.R = L.R + L.T * env_radiance(M, L.w);
+                    if (MODE == FW_BRANCH) {  // scattered light only: no direct term
+                        L.ff = Flight();
                         L.state = L.d > EPS ? ST_PRIMARY : ST_DEAD;
                         if (L.state == ST_DEAD) end_path<MODE>(S, L, out, scale, io);
+                    } else {
+                        int ev = start_shadow(M, L, L.x, L.w, tl);
+                        if (ev == EV_SHADOW_DONE) {
+                            L.R = L.R + L.T * env_radiance(M, L.w);
+                            L.state = L.d > EPS ? ST_PRIMARY : ST_DEAD;
+                            if (L.state == ST_DEAD) end_path<MODE>(S, L, out, scale, io);
+                        }
                     }
                 }
             }
@@ -1337,22 +1358,28 @@ __global__ void __launch_bounds__(256) k_path_bw(DMedium M, PathSrc S, uint64_t 
     warp_add_counters(sc, paths, 0, tl);
 }
 
-// The reservoir branch of the DRT / DRTDS wavefront (vrt_wave_drt.cu), one thread per
-// path of the round: the primal left the reservoir vertex and the stream
-// position at its end in resv (4 float4 per path: vertex and its weight,
-// direction and the running total -- 0 for a primary ray that missed the
-// medium --, throughput, stream position); paths handed to the sequential
-// form (first-collision word kSpilled) are skipped.
+// The reservoir branch of the DRT / DRTDS wavefront (vrt_wave_drt.cu) in three
+// steps.  k_drt_branch_pre, one thread per path of the round: the primal left
+// the reservoir vertex and the stream position at its end in resv (4 float4
+// per path: vertex and its weight, direction and the running total -- 0 for a
+// primary ray that missed the medium --, throughput, stream position); paths
+// handed to the sequential form (first-collision word kSpilled) are skipped.
+// It samples the branch position (_NEE_DRT.h:233-235; DS: the defensive
+// collision position, no branch at weight 0) and its light rays, and appends
+// an item: the nested path's start (position, direction, stream position, path
+// id) and what the scatter needs (light terms, weights).  The nested
+// scattered-only NEE paths run on the state machine (k_nee_fw<FW_BRANCH>);
+// k_drt_branch_post adds their estimates and scatters at the branch position.
 template <bool DS>
-__global__ void __launch_bounds__(256) k_drt_branch(DMedium M, PathSrc S, uint64_t n_paths, uint64_t p_begin,
-                                                     const unsigned long long* next_path, uint64_t seed,
-                                                     const float* dL, float div, const float* __restrict__ info,
-                                                     const float4* __restrict__ resv, DScratch* sc) {
+__global__ void __launch_bounds__(256) k_drt_branch_pre(DMedium M, PathSrc S, uint64_t n_paths, uint64_t p_begin,
+                                                         const unsigned long long* next_path, uint64_t seed,
+                                                         const float* __restrict__ info,
+                                                         const float4* __restrict__ resv, float4* items,
+                                                         float4* post, unsigned long long* n_items, DScratch* sc) {
     constexpr uint32_t kSpilledPath = 0xfffffffdu;  // the first-collision word of a handed-over path
     unsigned long long end = *next_path;
     if (end > n_paths) end = n_paths;
     const uint64_t n_round = end > p_begin ? end - p_begin : 0;
-    uint32_t verts = 0;
     Tally tl;
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n_round;
          k += (uint64_t)gridDim.x * blockDim.x) {
@@ -1364,43 +1391,98 @@ __global__ void __launch_bounds__(256) k_drt_branch(DMedium M, PathSrc S, uint64
         Rng rng;
         rng.init(seed, pid, 0);
         rng.seek(Rng::Pos{__float_as_uint(r3.x), __float_as_uint(r3.y)});
-        const long long o = S.is_camera ? (long long)(pid % (uint64_t)S.npix) : (long long)pid;
-        const float3 g = ld3(dL + 3 * o) / div;
-        const float3 rx = make_float3(r0.x, r0.y, r0.z), rw = make_float3(r1.x, r1.y, r1.z);
-        const float3 rW = make_float3(r2.x, r2.y, r2.z);
-        if (DS) drtds_branch(M, rng, rx, rw, rW, r0.w, r1.w, M.ds_eps, g, verts, tl, &sc->status);
-        else drt_branch(M, rng, rx, rw, rW, r0.w, r1.w, g, verts, tl, &sc->status);
+        const float3 res_x = make_float3(r0.x, r0.y, r0.z), res_w = make_float3(r1.x, r1.y, r1.z);
+        float tMin, d;
+        boundary(M, res_x, res_w, tMin, d);
+        float s_t, weight_t;
+        if (DS) sample_collision_position_ds(M, rng, res_x, res_w, d, M.ds_eps, s_t, weight_t, tl, &sc->status);
+        else sample_transmittance_position(M, rng, res_x, res_w, d, s_t, weight_t, tl, &sc->status);
+        if (DS && !(weight_t > 0.0f)) continue;
+        const float3 xs = res_x + res_w * s_t;
+        float3 ls_dir;
+        const float3 Ls_env = environment_sample(M, rng, ls_dir);
+        float3 Ls = transmittance(M, rng, xs, ls_dir, tl, &sc->status) * Ls_env * phase(M, res_w, ls_dir);
+        if (M.has_sun)
+            Ls = Ls + transmittance(M, rng, xs, M.sun_dir, tl, &sc->status) * M.sun_L * phase(M, res_w, M.sun_dir);
+        const float3 ws = phase_sample(M, rng, res_w);
+        const unsigned long long i = atomicAdd(n_items, 1ull);
+        items[3 * i] = make_float4(xs.x, xs.y, xs.z, __uint_as_float(rng.n));
+        items[3 * i + 1] = make_float4(ws.x, ws.y, ws.z, __uint_as_float(rng.ntr));
+        items[3 * i + 2] = make_float4(__uint_as_float((uint32_t)pid), __uint_as_float((uint32_t)(pid >> 32)), 0.0f, 0.0f);
+        post[3 * i] = make_float4(Ls.x, Ls.y, Ls.z, weight_t);
+        post[3 * i + 1] = make_float4(r2.x, r2.y, r2.z, r1.w);
+        post[3 * i + 2] = make_float4(r0.w, 0.0f, 0.0f, 0.0f);
     }
     warp_add_counters(sc, 0, 0, tl);
-    // the per-kernel slot (vrt_kernel_stats)
-    unsigned long long st = tl.steps, lk = tl.lookups, rd = tl.reds, al = tl.albedo;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        st += __shfl_down_sync(kFull, st, o);
-        lk += __shfl_down_sync(kFull, lk, o);
-        rd += __shfl_down_sync(kFull, rd, o);
-        al += __shfl_down_sync(kFull, al, o);
+}
+
+// _NEE_DRT.h:261-268 (DS: _NEE_DRTDS.h:248-251): the branch estimate (light
+// terms + the nested path's) weighed by the reservoir and scattered at the
+// branch position.
+template <bool DS>
+__global__ void __launch_bounds__(256) k_drt_branch_post(DMedium M, PathSrc S, uint64_t n_items,
+                                                          const float4* __restrict__ items,
+                                                          const float4* __restrict__ post, const float* __restrict__ R,
+                                                          const float* dL, float div, DScratch* sc) {
+    Tally tl;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_items;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float4 a = items[3 * i], c = items[3 * i + 2];
+        const float4 p0 = post[3 * i], p1 = post[3 * i + 1], p2 = post[3 * i + 2];
+        const uint64_t pid = (uint64_t)__float_as_uint(c.x) | ((uint64_t)__float_as_uint(c.y) << 32);
+        const long long o = S.is_camera ? (long long)(pid % (uint64_t)S.npix) : (long long)pid;
+        const float3 dL_dR = ld3(dL + 3 * o) / div;
+        const float3 xs = make_float3(a.x, a.y, a.z);
+        float3 Ls = make_float3(p0.x, p0.y, p0.z) + 1.0f * ld3(R + 3 * i);
+        Ls = Ls * make_float3(p1.x, p1.y, p1.z) * p0.w * albedo(M, xs, tl);
+        const float total_weight = p1.w, res_P = p2.x;
+        if (DS) {
+            sigma_bw(M, xs, dot(dL_dR, Ls) * total_weight / res_P, tl);
+        } else {
+            const float sigma_xs = sigma(M, xs, tl);
+            const float mis_T = 1.0f / (1.0f + sigma_xs * sigma_xs);
+            sigma_bw(M, xs, dot(dL_dR, Ls) * mis_T * total_weight / res_P, tl);
+        }
     }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&sc->kstat[VRT_K_DRT_BRANCH][0], st);
-        atomicAdd(&sc->kstat[VRT_K_DRT_BRANCH][1], lk);
-        atomicAdd(&sc->kstat[VRT_K_DRT_BRANCH][2], rd);
-        atomicAdd(&sc->kstat[VRT_K_DRT_BRANCH][3], al);
-    }
+    warp_add_counters(sc, 0, 0, tl);
 }
 
 int launch_drt_branch(const DMedium& M, bool ds, const PathSrc& src, uint64_t n_paths, uint64_t p_begin,
                       const unsigned long long* next_path, uint64_t seed, const float* dL, float div, const float* info,
-                      const float4* resv, uint64_t max_round, DScratch* scratch, int num_sms, cudaStream_t stream) {
+                      const float4* resv, uint64_t max_round, float4* items, float4* post, float* R,
+                      unsigned long long* n_items, DScratch* scratch, int num_sms, cudaStream_t stream) {
     if (max_round == 0) return 0;
-    const uint64_t need = (max_round + 255) / 256;
-    const int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
     KernelScope ks(VRT_K_DRT_BRANCH, stream);
-    if (ds) k_drt_branch<true><<<blocks, 256, 0, stream>>>(M, src, n_paths, p_begin, next_path, seed, dL, div, info, resv,
-                                                            scratch);
-    else k_drt_branch<false><<<blocks, 256, 0, stream>>>(M, src, n_paths, p_begin, next_path, seed, dL, div, info, resv,
-                                                          scratch);
-    count_launches(1);
+    // n_items[0]: the items appended, n_items[1]: the nested paths' work counter
+    cudaError_t e = cudaMemsetAsync(n_items, 0, 2 * sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return launch_status(e);
+    const uint64_t need = (max_round + 255) / 256;
+    int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
+    if (ds) k_drt_branch_pre<true><<<blocks, 256, 0, stream>>>(M, src, n_paths, p_begin, next_path, seed, info, resv,
+                                                                 items, post, n_items, scratch);
+    else k_drt_branch_pre<false><<<blocks, 256, 0, stream>>>(M, src, n_paths, p_begin, next_path, seed, info, resv,
+                                                               items, post, n_items, scratch);
+    unsigned long long n = 0;
+    if ((e = cudaMemcpyAsync(&n, n_items, sizeof(n), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+        return launch_status(e);
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return launch_status(e);
+    int launches = 1;
+    if (n) {  // the nested paths on the state machine, then the scatters
+        CacheIO io = {};
+        io.pR = R;
+        io.branch = items;
+        io.queue = n_items + 1;
+        int pb = persistent_blocks((const void*)k_nee_fw<FW_BRANCH>, 256, num_sms);
+        const uint64_t nb = (n + 255) / 256;
+        if ((uint64_t)pb > nb) pb = (int)nb;
+        k_nee_fw<FW_BRANCH><<<pb, 256, 0, stream>>>(M, src, n, seed, nullptr, 1.0f, scratch, io);
+        const uint64_t np = (n + 255) / 256;
+        blocks = (int)(np < (uint64_t)num_sms * 16 ? np : (uint64_t)num_sms * 16);
+        if (ds) k_drt_branch_post<true><<<blocks, 256, 0, stream>>>(M, src, n, items, post, R, dL, div, scratch);
+        else k_drt_branch_post<false><<<blocks, 256, 0, stream>>>(M, src, n, items, post, R, dL, div, scratch);
+        launches += 2;
+    }
+    count_launches(launches);
     return launch_status(cudaGetLastError());
 }
 

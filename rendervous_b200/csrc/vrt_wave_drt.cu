@@ -22,9 +22,11 @@
 //                  dL/dT = dL/dR(pixel) / div . weight -- the fork numbers of
 //                  the two streams agree (fork 0 is the primary ray's in both)
 //   k_drt_replay   the sigma scatters of the log, R taken down vertex by vertex
-//   k_drt_branch   (vrt_path.cu) the reservoir branch, one thread per path,
-//                  from the stream position the primal ended at (the replay
-//                  draws exactly the primal's)
+//   k_drt_branch_pre / _post (vrt_path.cu) the reservoir branch from the
+//                  stream position the primal ended at (the replay draws
+//                  exactly the primal's): its position and light rays one
+//                  thread per path, its nested scattered-only NEE path on the
+//                  state machine (k_nee_fw<FW_BRANCH>), then the scatter
 //
 // Compiled with -fmad=false, like the sequential form (vrt_path.cu), so a
 // walk here rounds as the sequential definition does.  Paths the collision log
@@ -420,7 +422,10 @@ int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, int bw_mode, const Pa
     const size_t o_info = o_recs + wv.cap_recs * sizeof(VertexRec), o_resv = o_info + wv.cap_paths * 32;
     const size_t o_list = o_resv + wv.cap_paths * 64;
     const size_t o_evs = o_list + ((wv.cap_paths * 16 + 255) & ~(size_t)255);
-    const size_t o_spill = o_evs + wv.cap_evs * 32, bytes = o_spill + wv.cap_spill * 8;
+    const size_t o_spill = o_evs + wv.cap_evs * 32, o_items = o_spill + ((wv.cap_spill * 8 + 255) & ~(size_t)255);
+    // the reservoir branches' items, their scatter data and the nested paths' estimates
+    const size_t o_post = o_items + wv.cap_paths * 48, o_bR = o_post + wv.cap_paths * 48;
+    const size_t bytes = o_bR + wv.cap_paths * 12;
     int st = ensure_wave_buffer(ctx, bytes);
     if (st) return st;
     char* base = static_cast<char*>(ctx->wave);
@@ -429,6 +434,9 @@ int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, int bw_mode, const Pa
     wv.recs = reinterpret_cast<VertexRec*>(base + o_recs);
     wv.info = reinterpret_cast<float*>(base + o_info);
     wv.resv = reinterpret_cast<float4*>(base + o_resv);
+    float4* b_items = reinterpret_cast<float4*>(base + o_items);
+    float4* b_post = reinterpret_cast<float4*>(base + o_post);
+    float* b_R = reinterpret_cast<float*>(base + o_bR);
     wv.over = nullptr;
     wv.list = reinterpret_cast<uint4*>(base + o_list);
     wv.evs = reinterpret_cast<CollisionRec*>(base + o_evs);
@@ -460,7 +468,8 @@ int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, int bw_mode, const Pa
         count_launches(1);
         if ((st = launch_status(cudaGetLastError()))) return st;
         if ((st = launch_drt_branch(M, ds, src, n_paths, wv.p_begin, &ctx->scratch->next_path, seed, dL, div, wv.info,
-                                    wv.resv, wv.cap_paths, ctx->scratch, ctx->num_sms, stream)))
+                                    wv.resv, wv.cap_paths, b_items, b_post, b_R, &wv.hdr[12], ctx->scratch,
+                                    ctx->num_sms, stream)))
             return st;
         unsigned long long taken = 0;
         if ((e = cudaMemcpyAsync(&taken, &ctx->scratch->next_path, sizeof(taken), cudaMemcpyDeviceToHost, stream)) !=
