@@ -1332,6 +1332,160 @@ __global__ void __launch_bounds__(256) k_dt_fw(DMedium M, PathSrc S, uint64_t n_
     warp_add_counters(sc, paths, verts, tl);
 }
 
+// The DT adjoint (path_dt_bw, vr_path_integrator_DT.h:59-150) as a persistent
+// state machine: every lane advances its path by one free flight per
+// iteration -- at most 12 brick crossings, then a collision -- first through
+// the primal walk, then through the replay of the same draws, and takes a new
+// path when both are done (warp refill by ballot, one atomic per warp), so
+// lanes do not wait for the longest path of their warp.  The replay restarts
+// from the primary ray, drawn again from the path's stream; the arithmetic is
+// path_dt_bw's, operation for operation.
+__global__ void __launch_bounds__(256, 3) k_dt_bw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
+                                                const float* __restrict__ dL, float div, DScratch* sc) {
+    constexpr int kCrossIt = 12;  // brick crossings per iteration
+    const unsigned lane = threadIdx.x & 31u;
+    const float EPS = 0.00000001f;
+    const float eps = M.ds_eps;
+    Flight ff;
+    Rng rng;
+    float3 x = f3(0.0f), w = f3(0.0f), W = f3(0.0f), W_out = f3(0.0f), dL_dW = f3(0.0f);
+    float d = 0.0f, null_W = 1.0f;
+    int bounces = 0, phase = 0;  // 0 idle, 1 primal, 2 replay
+    bool exhausted = false;
+    uint64_t pid = 0;
+    uint32_t paths = 0, steps_path = 0;
+    Tally tl;
+    while (true) {
+        const unsigned want = __ballot_sync(kFull, phase == 0 && !exhausted);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(&sc->next_path, (unsigned long long)__popc(want));
+            base = __shfl_sync(kFull, base, leader);
+            if (phase == 0 && !exhausted) {
+                const uint64_t p = base + __popc(want & ((1u << lane) - 1u));
+                if (p >= n_paths) {
+                    exhausted = true;
+                } else {
+                    pid = p;
+                    phase = 1;
+                    null_W = 1.0f;
+                    steps_path = 0;
+                    ++paths;
+                }
+            }
+        }
+        if (__all_sync(kFull, phase == 0 && exhausted)) break;
+        if (phase == 0) continue;
+        if (steps_path == 0) {  // the start of a walk: the primary ray (the replay draws it again)
+            rng.init(seed, pid, 0);
+            long long oidx;
+            float3 x0, w0;
+            primary_ray(S, pid, rng, x0, w0, oidx);
+            if (phase == 1) dL_dW = ld3(dL + 3 * oidx) / div;  // dL/dR for now; times the escape radiance below
+            float tMin, tMax;
+            boundary(M, x0, w0, tMin, tMax);
+            x = x0 + w0 * tMin;
+            w = w0;
+            d = tMax - tMin;
+            W = f3(1.0f);
+            bounces = 0;
+            ff = Flight();
+        }
+        bool end = !(d > EPS);
+        if (!end) {
+            float m = 0.0f, t = 0.0f;
+            bool need = false;
+            for (int k = 0;; ++k) {
+                float md;
+                m = gmax(EPS, ff.bk.query(M, x, w, md) + 2.0f * eps);
+                if (ff.tau < 0.0f) ++tl.steps;
+                t = ff.sample(rng) / m;
+                x = x + w * gmin(t, md);
+                if (t > md) {
+                    d -= md;
+                    ff.cross(m, md);
+                    ff.bk.advance(M);
+                    if (!(d > EPS)) { end = true; break; }
+                    if (k + 1 >= kCrossIt) break;  // the flight resumes in the next iteration
+                    continue;
+                }
+                ff.used();
+                if (t > d) end = true;
+                else need = true;
+                if (need) ff.bk.move(t);
+                break;
+            }
+            if (need) {
+                const float s = sigma(M, x, tl);
+                const float Pc = (s + eps) / m;
+                if (rng.uniform() >= Pc) {  // null collision
+                    if (phase == 2) sigma_bw(M, x, dot(dL_dW, -W_out * null_W / m / (1.0f - s / m)), tl);
+                    d -= t;
+                    W = W * ((1.0f - s / m) / (1.0f - Pc));
+                    if (!(d > EPS)) end = true;
+                } else if (phase == 1) {  // real collision of the primal (_DT.h:82-101)
+                    bool stop = false;
+                    if (s == 0.0f) {
+                        if (null_W == 0.0f) { W = f3(0.0f); stop = true; }
+                        else null_W = 0.0f;
+                    } else {
+                        W = W * ((s / m) / Pc);
+                    }
+                    if (!stop) {
+                        const float3 sa = albedo(M, x, tl);
+                        const float3 wo = phase_sample(M, rng, w);
+                        W = W * (sa * 1.0f);
+                        if (all_less(W, EPS)) { W = f3(0.0f); stop = true; }
+                        else if (M.max_bounces > 0 && ++bounces >= M.max_bounces) { W = f3(0.0f); stop = true; }
+                        else {
+                            w = wo;
+                            float tMin;
+                            boundary(M, x, w, tMin, d);
+                            ff.bk.reset();
+                        }
+                    }
+                    if (stop) end = true;
+                } else {  // real collision of the replay (_DT.h:125-148)
+                    sigma_bw(M, x, dot(dL_dW, s == 0.0f ? W_out : W_out * null_W / s), tl);
+                    W = W * (s / m / Pc);
+                    if (s == 0.0f) {
+                        end = true;
+                    } else {
+                        const float3 sa = albedo(M, x, tl);
+                        const float3 wo = phase_sample(M, rng, w);
+                        W = W * sa;
+                        if (all_less(W, EPS) || (M.max_bounces > 0 && ++bounces >= M.max_bounces)) {
+                            end = true;
+                        } else {
+                            w = wo;
+                            float tMin;
+                            boundary(M, x, w, tMin, d);
+                            ff.bk.reset();
+                        }
+                    }
+                }
+            }
+        }
+        if (++steps_path > (uint32_t)kPathStepCap) {
+            raise_status(&sc->status, 4);
+            phase = 0;  // abandoned (the error word reports it)
+            continue;
+        }
+        if (end) {
+            if (phase == 1) {  // the primal's end: the escape radiance's weight, then the replay
+                dL_dW = dL_dW * env_radiance(M, w);
+                W_out = W;
+                phase = 2;
+                steps_path = 0;
+            } else {
+                phase = 0;
+            }
+        }
+    }
+    warp_add_counters(sc, paths, 0, tl);
+}
+
 // pids: the n_paths paths listed there (device array), else paths 0 .. n_paths-1
 template <int MODE>
 __global__ void __launch_bounds__(256) k_path_bw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, const float* dL,
@@ -1550,6 +1704,16 @@ int launch_radiance_bw(const DMedium& M, int bw_mode, const PathSrc& src, uint64
                        const unsigned long long* pids) {
     if (n_paths == 0) return 0;
     if (bw_mode == 0) return launch_nee_ds_bw(M, src, n_paths, seed, dL, div, scratch, num_sms, stream, pids);
+    if (bw_mode == 1 && !pids) {  // DT: the persistent state machine
+        cudaError_t e = cudaMemsetAsync(&scratch->next_path, 0, sizeof(unsigned long long), stream);
+        if (e != cudaSuccess) return launch_status(e);
+        int blocks = persistent_blocks((const void*)k_dt_bw, 256, num_sms);
+        const uint64_t nb = (n_paths + 255) / 256;
+        if ((uint64_t)blocks > nb) blocks = (int)nb;
+        k_dt_bw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch);
+        count_launches(1);
+        return launch_status(cudaGetLastError());
+    }
     uint64_t need = (n_paths + 255) / 256;
     int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
     if (bw_mode == 1) k_path_bw<1><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch, pids);
