@@ -454,42 +454,6 @@ __device__ float3 path_nee_seq(const DMedium& M, Rng& rng, float3 x, float3 w, b
     return R;
 }
 
-// vr_path_integrator_DT.h:7-57
-__device__ float3 path_dt_seq(const DMedium& M, Rng& rng, float3 x, float3 w, uint32_t& verts, Tally& tl,
-                              uint32_t* status) {
-    float tMin, tMax;
-    boundary(M, x, w, tMin, tMax);
-    x = x + w * tMin;
-    float d = tMax - tMin;
-    float3 R = f3(0.0f), W = f3(1.0f);
-    int bounces = 0;
-    for (Flight ff; d > 0.00000001f; ++ff.it) {
-        if (ff.it >= kPathStepCap) { raise_status(status, 4); break; }
-        float md;
-        float m = gmax(0.00000001f, ff.bk.query(M, x, w, md));
-        if (ff.tau < 0.0f) ++tl.steps;
-        float t = ff.sample(rng) / m;
-        x = x + w * gmin(t, md);
-        if (t > md) { d -= md; ff.cross(m, md); ff.bk.advance(M); continue; }
-        ff.used();
-        if (t > d) break;
-        ff.bk.move(t);
-        float s = sigma(M, x, tl);
-        if (rng.uniform() >= s / m) { d -= t; continue; }
-        ++verts;
-        float3 sa = albedo(M, x, tl);
-        R = R + W * (f3(1.0f) - sa) * M.emission;
-        W = W * sa;
-        float3 wo = phase_sample(M, rng, w);
-        if (all_less(W, 0.0000001f)) return R;
-        if (M.max_bounces > 0 && ++bounces >= M.max_bounces) return R;
-        w = wo;
-        boundary(M, x, w, tMin, d);
-        ff.bk.reset();
-    }
-    return W * env_radiance(M, w) + R;
-}
-
 // vr_path_integrator_DT.h:59-235
 __device__ void path_dt_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float eps, float3 dL_dR, Tally& tl,
                            uint32_t* status) {
@@ -1304,29 +1268,126 @@ __device__ void path_nee_sps_bw(const DMedium& M, Rng& rng, float3 x, float3 w, 
 }
 
 // ------------------------------------------------------------------------
-// Kernels over paths (grid-stride, one path per thread at a time)
+// Kernels over paths: the DT forms as persistent state machines, the other
+// adjoints one path per thread (grid-stride)
 // ------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_dt_fw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, float* out,
-                                                float scale, DScratch* sc) {
-    uint32_t paths = 0, verts = 0;
+
+// The DT forward (vr_path_integrator_DT.h:7-57) as a persistent
+// state machine: one free flight (at most 12 brick crossings, then a
+// collision) per lane and iteration, lanes refilled by ballot.
+__global__ void __launch_bounds__(256, 3) k_dt_fw_sm(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed, float* out,
+                                                   float scale, DScratch* sc) {
+    constexpr int kCrossIt = 12;  // brick crossings per iteration
+    const unsigned lane = threadIdx.x & 31u;
+    const float EPS = 0.00000001f;
+    Flight ff;
+    Rng rng;
+    float3 x = f3(0.0f), w = f3(0.0f), W = f3(0.0f), R = f3(0.0f);
+    float d = 0.0f;
+    int bounces = 0;
+    bool alive = false, exhausted = false;
+    long long oidx = 0;
+    uint32_t paths = 0, verts = 0, steps_path = 0;
     Tally tl;
-    for (uint64_t pid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; pid < n_paths;
-         pid += (uint64_t)gridDim.x * blockDim.x) {
-        Rng rng;
-        rng.init(seed, pid, 0);
-        float3 x, w;
-        long long oidx;
-        primary_ray(S, pid, rng, x, w, oidx);
-        float3 R = path_dt_seq(M, rng, x, w, verts, tl, &sc->status);
-        ++paths;
-        if (S.is_camera) {
-            atomicAdd(out + 3 * oidx + 0, R.x * scale);
-            atomicAdd(out + 3 * oidx + 1, R.y * scale);
-            atomicAdd(out + 3 * oidx + 2, R.z * scale);
+    while (true) {
+        const unsigned want = __ballot_sync(kFull, !alive && !exhausted);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(&sc->next_path, (unsigned long long)__popc(want));
+            base = __shfl_sync(kFull, base, leader);
+            if (!alive && !exhausted) {
+                const uint64_t pid = base + __popc(want & ((1u << lane) - 1u));
+                if (pid >= n_paths) {
+                    exhausted = true;
+                } else {
+                    rng.init(seed, pid, 0);
+                    float3 x0, w0;
+                    primary_ray(S, pid, rng, x0, w0, oidx);
+                    float tMin, tMax;
+                    boundary(M, x0, w0, tMin, tMax);
+                    x = x0 + w0 * tMin;
+                    w = w0;
+                    d = tMax - tMin;
+                    W = f3(1.0f);
+                    R = f3(0.0f);
+                    bounces = 0;
+                    steps_path = 0;
+                    ff = Flight();
+                    alive = true;
+                    ++paths;
+                }
+            }
+        }
+        if (__all_sync(kFull, !alive && exhausted)) break;
+        if (!alive) continue;
+        int ev = 0;  // 0 going on, 1 escaped (W * env + R), 2 ended (R)
+        if (!(d > EPS)) {
+            ev = 1;
         } else {
-            out[3 * oidx + 0] = R.x;
-            out[3 * oidx + 1] = R.y;
-            out[3 * oidx + 2] = R.z;
+            float m = 0.0f, t = 0.0f;
+            bool need = false;
+            for (int k = 0;; ++k) {
+                float md;
+                m = gmax(EPS, ff.bk.query(M, x, w, md));
+                if (ff.tau < 0.0f) ++tl.steps;
+                t = ff.sample(rng) / m;
+                x = x + w * gmin(t, md);
+                if (t > md) {
+                    d -= md;
+                    ff.cross(m, md);
+                    ff.bk.advance(M);
+                    if (!(d > EPS)) { ev = 1; break; }
+                    if (k + 1 >= kCrossIt) break;  // the flight resumes in the next iteration
+                    continue;
+                }
+                ff.used();
+                if (t > d) {
+                    ev = 1;
+                } else {
+                    need = true;
+                    ff.bk.move(t);
+                }
+                break;
+            }
+            if (need) {
+                const float s = sigma(M, x, tl);
+                if (rng.uniform() >= s / m) {
+                    d -= t;
+                    if (!(d > EPS)) ev = 1;
+                } else {  // a real collision (_DT.h:39-52)
+                    ++verts;
+                    const float3 sa = albedo(M, x, tl);
+                    R = R + W * (f3(1.0f) - sa) * M.emission;
+                    W = W * sa;
+                    const float3 wo = phase_sample(M, rng, w);
+                    if (all_less(W, 0.0000001f) || (M.max_bounces > 0 && ++bounces >= M.max_bounces)) {
+                        ev = 2;
+                    } else {
+                        w = wo;
+                        float tMin;
+                        boundary(M, x, w, tMin, d);
+                        ff.bk.reset();
+                    }
+                }
+            }
+        }
+        if (++steps_path > (uint32_t)kPathStepCap) {
+            raise_status(&sc->status, 4);
+            ev = 1;  // (the reference's loop ends with the escape term)
+        }
+        if (ev) {
+            if (ev == 1) R = W * env_radiance(M, w) + R;
+            if (S.is_camera) {
+                atomicAdd(out + 3 * oidx + 0, R.x * scale);
+                atomicAdd(out + 3 * oidx + 1, R.y * scale);
+                atomicAdd(out + 3 * oidx + 2, R.z * scale);
+            } else {
+                out[3 * oidx + 0] = R.x;
+                out[3 * oidx + 1] = R.y;
+                out[3 * oidx + 2] = R.z;
+            }
+            alive = false;
         }
     }
     warp_add_counters(sc, paths, verts, tl);
@@ -1654,10 +1715,13 @@ int launch_radiance_fw(const DMedium& M, int integrator, const PathSrc& src, uin
         if ((uint64_t)blocks > need) blocks = (int)need;
         CacheIO io = {};
         k_nee_fw<FW_PLAIN><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, scratch, io);
-    } else {
-        uint64_t need = (n_paths + 255) / 256;
-        int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
-        k_dt_fw<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, scratch);
+    } else {  // DT: the persistent state machine
+        cudaError_t e = cudaMemsetAsync(&scratch->next_path, 0, sizeof(unsigned long long), stream);
+        if (e != cudaSuccess) return launch_status(e);
+        int blocks = persistent_blocks((const void*)k_dt_fw_sm, 256, num_sms);
+        const uint64_t nb = (n_paths + 255) / 256;
+        if ((uint64_t)blocks > nb) blocks = (int)nb;
+        k_dt_fw_sm<<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, out, scale, scratch);
     }
     count_launches(1);
     return launch_status(cudaGetLastError());
