@@ -610,6 +610,14 @@ def run_path_adjoints(args, wl, sig, flush, dev):
         "DRTDS": maps.DRTDSPathIntegrator(*nee, wl["ds_epsilon"], **kw),
         "SPS": maps.SPSPathIntegrator(*nee, **kw),
     }
+    # the collision integrators (one path per thread): emission + scattered exitance over RT light rays
+    gal = maps.Grid3D(torch.from_numpy(synthetic.uniform_grid(64, 0.5, 0.95, seed=22, channels=3)).to(dev), bmin, bmax)
+    gem = maps.Grid3D(torch.from_numpy(synthetic.uniform_grid(64, 0.1, 0.5, seed=23, channels=3)).to(dev), bmin, bmax)
+    radiance = maps.RatiotrackingTransmittance(sg, boundary, maj) * env.after(maps.ray_direction)
+    ex = maps.MCScatteredEmittedRadiance(gal, gem, maps.HenyeyGreensteinPhaseSampler(g), radiance)
+    fields["MC_COLLISION"] = maps.MCCollisionIntegrator(
+        maps.DeltatrackingCollisionSampler(sg, boundary, maj, wl["ds_epsilon"]), ex, env)
+    fields["DDA_COLLISION"] = maps.GridDDACollisionIntegrator(sg, ex, env, boundary)
     cam = maps.PerspectiveCameraSensor(wl["width"], wl["height"],
                                        torch.from_numpy(synthetic.ring_poses(wl["views"])).to(dev), jittered=True)
     n_paths = wl["width"] * wl["height"] * wl["views"] * wl["spp"]

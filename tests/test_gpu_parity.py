@@ -334,6 +334,34 @@ def test_ds_collision_log_overflow_rewalks(cuda, limit):
         assert np.abs(a).sum() > 0 and rel < 1e-4, rel
 
 
+@pytest.mark.parametrize("integrator", ["drt", "sps"])
+def test_drt_wavefront_on_rays_matches_sequential_form(cuda, integrator):
+    """The same on rays (the map evaluated on a ray batch, backward through
+    vrt_radiance_bw): the wavefront against the sequential form (collision log
+    capped at one record), delta-tracking light rays, an uncapped path budget."""
+    ffi, lib = _lib.ffi_lib()
+    ctx = _lib.context(cuda)
+    wl = synthetic.WORKLOADS["plain_forward_64"]
+    sig = torch.from_numpy(synthetic.make_sigma(wl["sigma"])).to(cuda)
+    rays = torch.from_numpy(synthetic.sphere_rays(4096, seed=12)).to(cuda)
+    wts = torch.from_numpy(np.random.default_rng(2).random((4096, 3)).astype(np.float32)).to(cuda)
+    grads = []
+    for lim in (0, 1):
+        field = build_field(sig, albedo=0.9, env=1.0, sun_dir=(0.3, 0.8, 0.5), sun_radiance=3.0, g=0.4,
+                            max_bounces=0, sigma_requires_grad=True, integrator=integrator, tr="dt")
+        _lib.check(lib.vrt_set_collision_log_limit(ctx.ptr, lim))
+        try:
+            maps.check()
+            R = field(rays, seed=23)
+            (R * wts).sum().backward()
+            maps.check()
+        finally:
+            _lib.check(lib.vrt_set_collision_log_limit(ctx.ptr, 0))
+        grads.append(field.sigma.grid.grad.cpu().numpy())
+    rel = np.abs(grads[0] - grads[1]).sum() / max(np.abs(grads[0]).sum(), 1e-30)
+    assert np.abs(grads[0]).sum() > 0 and rel < 1e-4, rel
+
+
 @pytest.mark.parametrize("integrator", ["drt", "drtds", "sps"])
 @pytest.mark.parametrize("limit", [1, 3000])
 def test_drt_wavefront_matches_sequential_form(cuda, limit, integrator):
