@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow_run(DMedium M, PathSrc S, con
     flush_counters(sc, OUT == OUT_IMAGE ? VRT_K_SHADOW_FW : VRT_K_SHADOW_T, 0, 0, tl);
 }
 
-constexpr int kKeep = 16;  // first-pass collisions a transmittance adjoint keeps (k_shadow_adj)
+constexpr int kKeep = 8;  // first-pass collisions a transmittance adjoint keeps (k_shadow_adj)
 
 // The transmittance adjoints of the NEE_DS primal's light jobs
 // (vr_transmittance_RT.h:51-141 / _DT.h:30-90): the first pass runs as events
