@@ -164,31 +164,36 @@ __device__ float3 exitance(const DMedium& M, Rng& rng, float3 x, float3 wout, Ta
     if (M.exitance_mode == 2) R = R + (f3(1.0f) - sa) * emission_at(M, x);
     return R;
 }
-// The adjoint of exitance() on the same draws: each factor gets the adjoint of
-// the forward's expression (the reference's scattered maps hand (w, dL/dR) to
-// the radiance map's backward and drop the dL/dR factor of the emission term
-// of dL/dsa).
-__device__ void exitance_bw(const DMedium& M, Rng& rng, float3 x, float3 wout, float3 dL, Tally& tl,
-                            uint32_t* status) {
+// exitance() and its adjoint at one point on the same draws: the value
+// (returned) and the adjoint of that value for dL, the phase sample, albedo and
+// transmittance evaluated once.  Each factor gets the adjoint of the forward's
+// expression (the reference's scattered maps hand (w, dL/dR) to the radiance
+// map's backward and drop the dL/dR factor of the emission term of dL/dsa).
+__device__ float3 exitance_fw_bw(const DMedium& M, const Rng& stream, float3 x, float3 wout, float3 dL, Tally& tl,
+                                 uint32_t* status) {
     if (M.exitance_mode == 0) {
         emission_bw(M, x, dL, tl);
-        return;
+        return emission_at(M, x);
     }
+    Rng rng = stream;
     const float3 wo = phase_sample(M, rng, -wout);
     const float3 sa = albedo(M, x, tl);
     Rng tr_rng = rng;
     const float Tr = transmittance(M, rng, x, wo, tl, status);
     const float3 env = env_radiance(M, wo);
     const float3 rad = env * Tr;
+    float3 R = sa * 1.0f * rad;
     float3 dL_dsa = dL * rad * 1.0f;
     const float3 dL_drad = dL * sa * 1.0f;
     if (M.exitance_mode == 2) {
         const float3 em = emission_at(M, x);
+        R = R + (f3(1.0f) - sa) * em;
         dL_dsa = dL_dsa - dL * em;
         emission_bw(M, x, dL * (f3(1.0f) - sa), tl);
     }
     albedo_bw(M, x, dL_dsa, tl);
     transmittance_bw(M, tr_rng, x, wo, dot(dL_drad, env), tl, status);
+    return R;
 }
 
 // include/maps/collision_integrator_mc.h:8-18
@@ -215,16 +220,9 @@ __device__ void collision_integrate_mc_bw(const DMedium& M, const Rng& rng, floa
     const float C = collision_sample_dt(M, cs, x, w, t, Tt, tl, status);
     const float3 xt = w * t + x;
     float3 eR = f3(0.0f);
-    if (C != 0.0f) {
-        Rng xr = with_stream(rng, exitance_stream(0));
-        eR = exitance(M, xr, xt, -w, tl, status);
-    }
+    if (C != 0.0f) eR = exitance_fw_bw(M, with_stream(rng, exitance_stream(0)), xt, -w, dL * C, tl, status);
     Rng cb = with_stream(rng, 4);
     collision_sample_dt_bw(M, cb, x, w, M.ds_eps, dot(dL, eR), dot(dL, env_radiance(M, w)), tl, status);
-    if (C != 0.0f) {
-        Rng xb = with_stream(rng, exitance_stream(0));
-        exitance_bw(M, xb, xt, -w, dL * C, tl, status);
-    }
 }
 
 // include/vr_collision_integrator_DDA.h:1-82: per DDA cell a random point (the
@@ -307,10 +305,8 @@ __device__ void collision_integrate_dda_bw(const DMedium& M, Rng& rng, float3 x,
         const float dt = nt - ct;
         const float vt = expf(-dt * sv);
         const float3 xp = q.x + w * cell_t;
-        Rng xr = with_stream(rng, exitance_stream(k));
-        const float3 Le = exitance(M, xr, xp, -w, tl, status);
-        Rng xb = with_stream(rng, exitance_stream(k));
-        exitance_bw(M, xb, xp, -w, dL * (Tr * (1.0f - vt)), tl, status);
+        const float3 Le = exitance_fw_bw(M, with_stream(rng, exitance_stream(k)), xp, -w, dL * (Tr * (1.0f - vt)), tl,
+                                         status);
         R = R - Le * (Tr * (1.0f - vt));
         Tr *= vt;
         const float g = dot(dL, (Le * Tr - env * fw_T - R) * dt);
