@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow_fw(DMedium M, PathSrc S, cons
 
 // ---------------------------------------------------------------------------
 // Persistent shadow kernels for ratio / delta tracking: one event per lane per
-// iteration, finished lanes refilled from the job buffer (a warp claims 64
+// iteration, finished lanes refilled from the job buffer (a warp claims 128
 // jobs per atomic and hands them out by ballot rank).
 // ---------------------------------------------------------------------------
 struct ShadowOut {
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow_run(DMedium M, PathSrc S, con
         const unsigned want = __ballot_sync(kAll, !alive && !exhausted);
         if (want) {
             unsigned long long i;
-            const bool got = wq.take(head, n, 64, want, i);  // 64 jobs per warp and atomic
+            const bool got = wq.take(head, n, 128, want, i);  // 128 jobs per warp and atomic
             if (!alive && !exhausted) {
                 if (!got) {
                     exhausted = wq.drained;
@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow_adj(DMedium M, PathSrc S, con
         const unsigned want = __ballot_sync(kAll, phase == 0 && !exhausted);
         if (want) {
             unsigned long long i;
-            const bool got = wq.take(head, n, 64, want, i);  // 64 jobs per warp and atomic
+            const bool got = wq.take(head, n, 128, want, i);  // 128 jobs per warp and atomic
             if (phase == 0 && !exhausted) {
                 if (!got) {
                     exhausted = wq.drained;

@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(256, 3) k_drt_replay(DMedium M, PathSrc S, con
         const unsigned want = __ballot_sync(kAll, !alive && !exhausted);
         if (want) {
             unsigned long long q;
-            const bool got = wq.take(&wv.hdr[7], n_list, 64, want, q);
+            const bool got = wq.take(&wv.hdr[7], n_list, 32, want, q);
             if (!alive && !exhausted) {
                 if (!got) {
                     exhausted = wq.drained;
