@@ -334,6 +334,42 @@ def test_ds_collision_log_overflow_rewalks(cuda, limit):
         assert np.abs(a).sum() > 0 and rel < 1e-4, rel
 
 
+@pytest.mark.parametrize("integrator", ["drt", "drtds", "sps"])
+def test_drt_wavefront_in_rounds_matches_one_round(cuda, integrator):
+    """With the wavefront's round size capped (vrt_set_wave_batch_limit), the
+    DRT / DRTDS / SPS adjoints take their paths in several rounds (primal,
+    light rays, replay, branch per round); the gradients equal the one-round
+    run's up to the order of the float sums."""
+    ffi, lib = _lib.ffi_lib()
+    stream = _lib.stream_handle(cuda)
+    ctx = _lib.context(cuda)
+    wl = synthetic.WORKLOADS["plain_forward_64"]
+    sig = torch.from_numpy(synthetic.make_sigma(wl["sigma"])).to(cuda)
+    ks = ffi.new("vrt_kernel_stat[]", lib.VRT_K_COUNT)
+    primal = lib.VRT_K_SPS_PRIMAL if integrator == "sps" else lib.VRT_K_DRT_PRIMAL
+    dimg, grads, launches = None, [], []
+    for limit in (0, 4096):
+        field = build_field(sig, albedo=0.9, env=1.0, sun_dir=(0.3, 0.8, 0.5), sun_radiance=3.0, g=0.4,
+                            max_bounces=16, sigma_requires_grad=True, integrator=integrator, majorant="grid", brick=8)
+        _lib.check(lib.vrt_set_wave_batch_limit(ctx.ptr, limit))
+        try:
+            maps.check()
+            _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
+            cam, img = _capture(field, cuda, 128, 128, 8, seed=29)  # more paths than lanes: rounds can split
+            if dimg is None:
+                dimg = torch.from_numpy(np.random.default_rng(3).random(img.shape).astype(np.float32)).to(cuda)
+            (img * dimg).sum().backward()
+            maps.check()
+            _lib.check(lib.vrt_kernel_stats(ctx.ptr, stream, ks))
+        finally:
+            _lib.check(lib.vrt_set_wave_batch_limit(ctx.ptr, 0))
+        grads.append(field.sigma.grid.grad.cpu().numpy())
+        launches.append(ks[primal].launches)
+    assert launches[0] == 1 and launches[1] > 1, launches
+    rel = np.abs(grads[0] - grads[1]).sum() / max(np.abs(grads[0]).sum(), 1e-30)
+    assert np.abs(grads[0]).sum() > 0 and rel < 1e-4, rel
+
+
 @pytest.mark.parametrize("integrator", ["drt", "sps"])
 def test_drt_wavefront_on_rays_matches_sequential_form(cuda, integrator):
     """The same on rays (the map evaluated on a ray batch, backward through
