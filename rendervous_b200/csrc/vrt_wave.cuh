@@ -415,6 +415,36 @@ struct WaveBw {
     float4* resv;
 };
 
+// Path admission of the DRT and SPS primals (all lanes call it with the
+// ballot of the lanes that want a path; the leader decides): new paths are
+// taken while the round's buffers hold every lane's worst case, and each new
+// path also gets one job slot (its primary ray's adjoint-only job).  Returns
+// the warp's first path id (~0: no room this round) and, in jb, the first of
+// those job slots.
+__device__ __forceinline__ unsigned long long admit_paths(const WaveBw& wv, DScratch* sc, uint64_t n_paths,
+                                                          unsigned want, unsigned long long& jb) {
+    const unsigned lane = threadIdx.x & 31u;
+    const int leader = __ffs(want) - 1;
+    unsigned long long base = 0;
+    jb = 0;
+    if ((int)lane == leader) {
+        const unsigned long long uj = *((volatile unsigned long long*)&wv.hdr[0]);
+        const unsigned long long ur = *((volatile unsigned long long*)&wv.hdr[1]);
+        const unsigned long long ue = *((volatile unsigned long long*)&wv.hdr[5]);
+        const unsigned long long up = *((volatile unsigned long long*)&sc->next_path) - wv.p_begin;
+        const bool room = uj + wv.res_jobs <= wv.cap_jobs && ur + wv.res_recs <= wv.cap_recs &&
+                          ue + wv.res_evs <= wv.cap_evs && up + wv.lanes <= wv.cap_paths;
+        base = room ? atomicAdd(&sc->next_path, (unsigned long long)__popc(want)) : ~0ull;
+        if (base != ~0ull && base < n_paths) {
+            const unsigned long long nv =
+                n_paths - base < (unsigned long long)__popc(want) ? n_paths - base : (unsigned long long)__popc(want);
+            jb = atomicAdd(&wv.hdr[0], nv);
+        }
+    }
+    jb = __shfl_sync(kAll, jb, leader);
+    return __shfl_sync(kAll, base, leader);
+}
+
 }  // namespace wave
 
 // The light jobs of the NEE_DS adjoint rounds (defined in vrt_wave.cu, so they

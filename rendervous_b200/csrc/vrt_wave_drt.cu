@@ -59,26 +59,8 @@ __global__ void __launch_bounds__(256, 3) k_drt_primal(DMedium M, PathSrc S, uin
     while (true) {
         const unsigned want = __ballot_sync(kAll, !alive && !exhausted);
         if (want) {
-            const int leader = __ffs(want) - 1;
-            unsigned long long base = 0, jb = 0;
-            if ((int)lane == leader) {
-                const unsigned long long uj = *((volatile unsigned long long*)&wv.hdr[0]);
-                const unsigned long long ur = *((volatile unsigned long long*)&wv.hdr[1]);
-                const unsigned long long ue = *((volatile unsigned long long*)&wv.hdr[5]);
-                const unsigned long long up = *((volatile unsigned long long*)&sc->next_path) - wv.p_begin;
-                const bool room = uj + wv.res_jobs <= wv.cap_jobs && ur + wv.res_recs <= wv.cap_recs &&
-                                  ue + wv.res_evs <= wv.cap_evs && up + wv.lanes <= wv.cap_paths;
-                base = room ? atomicAdd(&sc->next_path, (unsigned long long)__popc(want)) : ~0ull;
-                // one job slot per new path: its primary ray's environment adjoint
-                if (base != ~0ull && base < n_paths) {
-                    const unsigned long long nv = n_paths - base < (unsigned long long)__popc(want)
-                                                      ? n_paths - base
-                                                      : (unsigned long long)__popc(want);
-                    jb = atomicAdd(&wv.hdr[0], nv);
-                }
-            }
-            base = __shfl_sync(kAll, base, leader);
-            jb = __shfl_sync(kAll, jb, leader);
+            unsigned long long jb;
+            const unsigned long long base = admit_paths(wv, sc, n_paths, want, jb);
             if (base == ~0ull) {
                 exhausted = true;
             } else if (!alive && !exhausted) {
