@@ -258,10 +258,28 @@ __device__ float3 collision_integrate_dda(const DMedium& M, Rng& rng, float3 x, 
     }
     return R + env_radiance(M, w) * Tr;
 }
-// include/vr_collision_integrator_DDA.h:85-207: the walk again for fw_T and
-// the emitted part, then a replay from the same cell draws scattering
-// dL/dsigma = dL/dR . (T Le - fw_T env - R_rest) dt into the cell's corners,
-// and the exitance's adjoint dL/dR T (1 - v) at each point.
+// dL/dsigma of a DDA cell, g, scattered into its 8 corners at the sample point a
+__device__ __forceinline__ void dda_cell_scatter(const DMedium& M, const DDA& q, float3 a, float g, Tally& tl) {
+    if (g == 0.0f || !M.sigma.grad) return;
+    const float bx = 1.0f - a.x, by = 1.0f - a.y, bz = 1.0f - a.z;
+    const float wt[8] = {g * bx * by * bz, g * a.x * by * bz, g * bx * a.y * bz, g * a.x * a.y * bz,
+                         g * bx * by * a.z, g * a.x * by * a.z, g * bx * a.y * a.z, g * a.x * a.y * a.z};
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+        red_add(M.sigma.grad + q.node(M.sigma, q.cx + (c & 1), q.cy + ((c >> 1) & 1), q.cz + (c >> 2)), wt[c]);
+    tl.reds += 8;
+}
+
+// include/vr_collision_integrator_DDA.h:85-207: the reference walks the cells
+// twice -- for fw_T and the emitted total R, then again from the same cell
+// draws scattering dL/dsigma = dL/dR . (T Le - fw_T env - R_rest) dt into the
+// cell's corners and the exitance's adjoint dL/dR T (1 - v) at each point.
+// With R_rest = R - P (P: the emitted part up to and including the cell) the
+// scatter splits into dL/dR . (T Le + P) dt, known on the first walk, and
+// -dL/dR . (fw_T env + R) dt, whose factor is known only at its end: so the
+// first walk evaluates each exitance once with its adjoint and scatters the
+// first part, and a second walk over the same cells and draws -- without the
+// exitances' light rays -- scatters the second.
 __device__ void collision_integrate_dda_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float3 dL, Tally& tl,
                                            uint32_t* status) {
     if (dL.x == 0.0f && dL.y == 0.0f && dL.z == 0.0f) return;
@@ -269,7 +287,7 @@ __device__ void collision_integrate_dda_bw(const DMedium& M, Rng& rng, float3 x,
     if (!q.init(M, x, w)) return;
     const Rng before = rng;
     float Tr = 1.0f, ct = 0.0f;
-    float3 R = f3(0.0f);
+    float3 P = f3(0.0f);
     q.load_all(M.sigma);
     long long k = 0;
     while (ct < q.d - 0.0001f) {
@@ -279,50 +297,31 @@ __device__ void collision_integrate_dda_bw(const DMedium& M, Rng& rng, float3 x,
         }
         const float nt = gmin(q.d, gmin(q.alpha.x, gmin(q.alpha.y, q.alpha.z)));
         const float cell_t = mixf(ct, nt, rng.uniform());
-        const float sv = q.interp(q.ialpha(cell_t));
-        const float vt = expf(-(nt - ct) * sv);
-        Rng xr = with_stream(rng, exitance_stream(k));
-        R = R + exitance(M, xr, q.x + w * cell_t, -w, tl, status) * (Tr * (1.0f - vt));
+        const float3 a = q.ialpha(cell_t);
+        const float sv = q.interp(a);
+        const float dt = nt - ct;
+        const float vt = expf(-dt * sv);
+        const float3 Le = exitance_fw_bw(M, with_stream(rng, exitance_stream(k)), q.x + w * cell_t, -w,
+                                         dL * (Tr * (1.0f - vt)), tl, status);
+        P = P + Le * (Tr * (1.0f - vt));
         Tr *= vt;
+        dda_cell_scatter(M, q, a, dot(dL, (Le * Tr + P) * dt), tl);
         ct = nt;
         const int axis = q.advance_cell();
         q.shift_load(M.sigma, axis);
         ++k;
     }
-    const float3 env = env_radiance(M, w);
-    const float fw_T = Tr;
+    const float G = dot(dL, env_radiance(M, w) * Tr + P);  // fw_T env + R
+    if (G == 0.0f || !M.sigma.grad) return;
     rng = before;
-    q.reset(M);
-    q.load_all(M.sigma);
-    Tr = 1.0f;
+    q.reset(M);  // (the second walk reads no corner values: no loads)
     ct = 0.0f;
-    k = 0;
     while (ct < q.d - 0.0001f) {
         const float nt = gmin(q.d, gmin(q.alpha.x, gmin(q.alpha.y, q.alpha.z)));
         const float cell_t = mixf(ct, nt, rng.uniform());
-        const float3 a = q.ialpha(cell_t);
-        const float sv = q.interp(a);
-        const float dt = nt - ct;
-        const float vt = expf(-dt * sv);
-        const float3 xp = q.x + w * cell_t;
-        const float3 Le = exitance_fw_bw(M, with_stream(rng, exitance_stream(k)), xp, -w, dL * (Tr * (1.0f - vt)), tl,
-                                         status);
-        R = R - Le * (Tr * (1.0f - vt));
-        Tr *= vt;
-        const float g = dot(dL, (Le * Tr - env * fw_T - R) * dt);
-        if (g != 0.0f && M.sigma.grad) {
-            const float bx = 1.0f - a.x, by = 1.0f - a.y, bz = 1.0f - a.z;
-            const float wt[8] = {g * bx * by * bz, g * a.x * by * bz, g * bx * a.y * bz, g * a.x * a.y * bz,
-                                 g * bx * by * a.z, g * a.x * by * a.z, g * bx * a.y * a.z, g * a.x * a.y * a.z};
-#pragma unroll
-            for (int c = 0; c < 8; ++c)
-                red_add(M.sigma.grad + q.node(M.sigma, q.cx + (c & 1), q.cy + ((c >> 1) & 1), q.cz + (c >> 2)), wt[c]);
-            tl.reds += 8;
-        }
+        dda_cell_scatter(M, q, q.ialpha(cell_t), -G * (nt - ct), tl);
         ct = nt;
-        const int axis = q.advance_cell();
-        q.shift_load(M.sigma, axis);
-        ++k;
+        q.advance_cell();
     }
 }
 
