@@ -174,9 +174,9 @@ enum {
     VRT_K_WALK_FW = 0,     /* forward walk (primary paths, shadow jobs) */
     VRT_K_SHADOW_FW = 1,   /* forward shadow transmittances */
     VRT_K_DS_PRIMAL = 2,   /* NEE_DS adjoint: primal walk (writes the collision log) */
-    VRT_K_SHADOW_T = 3,    /* NEE_DS adjoint: the primal's shadow transmittances */
+    VRT_K_SHADOW_T = 3,    /* NEE_DS (DRT, DRTDS, SPS) adjoint: the primal's light-ray transmittances */
     VRT_K_DS_REPLAY = 4,   /* NEE_DS adjoint: replay of the logged collisions (sigma / albedo scatters) */
-    VRT_K_SHADOW_ADJ = 5,  /* NEE_DS adjoint: transmittance adjoints */
+    VRT_K_SHADOW_ADJ = 5,  /* NEE_DS (DRT, DRTDS, SPS) adjoint: the light rays' transmittance adjoints */
     VRT_K_DS_REWALK = 6,   /* NEE_DS adjoint: replay walk of the paths the log could not hold */
     VRT_K_DRT_PRIMAL = 7,  /* DRT adjoint: primal walk (collision log, light jobs, reservoir) */
     VRT_K_DRT_REPLAY = 8,  /* DRT adjoint: replay of the logged collisions (sigma scatters) */
