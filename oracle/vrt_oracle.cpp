@@ -79,6 +79,19 @@ struct Rng {
         r.ntr = 0;
         return r;
     }
+    // The DRTQ adjoint's scatter term of segment k (0: the primary ray's, k:
+    // the one after the k-th scattering vertex) draws from a stream of its
+    // own: stream s + 1 of the path id with k + 1 in bits 40-63 (path ids
+    // below 2^40, k + 1 below 2^24).  No term depends on another's draws, so
+    // the terms can run in any order.
+    Rng segment_stream(uint32_t k) const {
+        Rng r = *this;
+        r.phi = phi | ((k + 1u) << 8);
+        r.stream = stream + 1u;
+        r.n = 0;
+        r.ntr = 0;
+        return r;
+    }
 };
 
 template <typename T> struct V3 {
@@ -1419,11 +1432,11 @@ template <typename T> V3<T> in_scattering(const Scene<T>& S, Rng& rng, V3<T> x, 
     return S.albedo(x) * Ls;
 }
 
-// Shared by the DRT family: the scatter-gradient term at a transmittance-
-// sampled position of the segment (x, w, d) on the branch stream
-// (vr_path_integrator_NEE_DRTQ.h:156-165 and :249-259).
+// The scatter-gradient term at a transmittance-sampled position of the
+// segment (x, w, d) (vr_path_integrator_NEE_DRTQ.h:156-165 and :249-259), on
+// the segment's own stream (Rng::segment_stream).
 template <typename T>
-void drtq_scatter_term(const Scene<T>& S, Rng& sec, V3<T> x, V3<T> w, T d, V3<T> W, V3<T> dL_dR) {
+void drtq_scatter_term(const Scene<T>& S, Rng sec, V3<T> x, V3<T> w, T d, V3<T> W, V3<T> dL_dR) {
     T s_t, weight_t;
     sample_transmittance_position(S, sec, x, w, d, s_t, weight_t);
     V3<T> xs = x + w * s_t;
@@ -1435,7 +1448,9 @@ void drtq_scatter_term(const Scene<T>& S, Rng& sec, V3<T> x, V3<T> w, T d, V3<T>
 
 // include/vr_path_integrator_NEE_DRTQ.h:58-260 path_integrator_NEE_DRTQ_bw:
 // the DRT primal without a reservoir, and a scatter-gradient term on every
-// segment of the replay.  Branch seed = Philox stream 1.
+// segment of the replay.  Branch seed = Philox stream 1 for the light rays'
+// adjoints (fork j of it beside fork j of the path's stream, as in DRT); each
+// scatter term on its segment's stream.  A path stops at 2^24 - 1 segments.
 template <typename T> void path_integrator_NEE_DRTQ_bw(const Scene<T>& S, Rng& rng, V3<T> x, V3<T> w, V3<T> dL_dR) {
     T tMin, tMax;
     S.boundary(x, w, tMin, tMax);
@@ -1486,7 +1501,8 @@ template <typename T> void path_integrator_NEE_DRTQ_bw(const Scene<T>& S, Rng& r
     d = ini_d;
     rng = before_path;
     bounces = 0;
-    drtq_scatter_term(S, sec, x, w, d, W, dL_dR);
+    uint32_t vertex = 0;  // scattering vertices so far: the next segment's number
+    drtq_scatter_term(S, rng.segment_stream(0), x, w, d, W, dL_dR);
     for (Flight<T> ff; d > EPS;) {
         T md;
         T m = ff.bk.query(S.s, x, w, md) * T(1.05) + T(0.1);
@@ -1531,8 +1547,8 @@ template <typename T> void path_integrator_NEE_DRTQ_bw(const Scene<T>& S, Rng& r
         w = wo;
         S.boundary(x, w, tMin, d);
         ff.bk.reset();
-        if (all_less(W, EPS) || capped) break;
-        drtq_scatter_term(S, sec, x, w, d, W, dL_dR);
+        if (all_less(W, EPS) || capped || ++vertex + 1u >= (1u << 24)) break;
+        drtq_scatter_term(S, rng.segment_stream(vertex), x, w, d, W, dL_dR);
     }
 }
 

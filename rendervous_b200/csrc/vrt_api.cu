@@ -90,9 +90,10 @@ static bool use_wave(const DMedium& M, int integrator) {
 static bool use_wave_bw(const DMedium& M, int bw_mode) {
     return bw_mode == VRT_BW_NEE_DS && M.max_bounces <= 4096 && !M.ds_compat;
 }
-// the DRT and DRTDS adjoints on the wavefront (capped or not): ratio / delta tracking light rays
+// the DRT, DRTDS and DRTQ adjoints on the wavefront (capped or not): ratio / delta tracking light rays
 static bool use_wave_drt(const DMedium& M, int bw_mode) {
-    return (bw_mode == VRT_BW_NEE_DRT || bw_mode == VRT_BW_NEE_DRTDS) && M.max_bounces <= 4096 && M.tr_mode <= 1;
+    return (bw_mode == VRT_BW_NEE_DRT || bw_mode == VRT_BW_NEE_DRTDS || bw_mode == VRT_BW_NEE_DRTQ) &&
+           M.max_bounces <= 4096 && M.tr_mode <= 1;
 }
 // the SPS adjoint on the wavefront (capped or not): ratio / delta tracking light rays
 static bool use_wave_sps(const DMedium& M, int bw_mode) {

@@ -63,6 +63,18 @@ struct Rng {
         return __uint_as_float((u32() & 0x007FFFFFu) | 0x3F800000u) - 1.0f;
     }
     __device__ __forceinline__ void advance() { (void)u32(); }  // randoms.h:35-41 advance_random
+    // The DRTQ adjoint's scatter term of segment k (0: the primary ray's, k:
+    // the one after the k-th scattering vertex): stream s + 1 of the path id
+    // with k + 1 in bits 40-63 (path ids below 2^40, k + 1 below 2^24), so the
+    // terms draw independently of one another and of the path.
+    __device__ __forceinline__ Rng segment_stream(uint32_t k) const {
+        Rng r = *this;
+        r.phi = phi | ((k + 1u) << 8);
+        r.stream = stream + 1u;
+        r.n = 0;
+        r.ntr = 0;
+        return r;
+    }
     // Position of the stream (draw index and forks taken) for replays.
     struct Pos { uint32_t n, ntr; };
     __device__ __forceinline__ Pos pos() const { return Pos{n, ntr}; }

@@ -73,11 +73,15 @@ int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, int bw_mode, const Pa
 // Wavefront SPS adjoint (vrt_wave_sps.cu): ratio or delta tracking light rays.
 int launch_wave_sps_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint64_t n_paths, uint64_t seed,
                        const float* dL, float div, cudaStream_t stream);
-// items / post: 3 float4 per path of the round each, R: 3 floats each, n_items: 2 counters.
-int launch_drt_branch(const DMedium& M, bool ds, const PathSrc& src, uint64_t n_paths, uint64_t p_begin,
+// The DRT-family branches (vrt_path.cu): mode 0 DRT, 1 DRTDS (one per path of
+// the round), 2 DRTQ (one scatter term per segment: segment 0s in resv, then
+// *n_segs in segs).  items / post: 3 float4 per branch each, R: 3 floats each,
+// n_items: 2 counters.
+int launch_drt_branch(const DMedium& M, int mode, const PathSrc& src, uint64_t n_paths, uint64_t p_begin,
                       const unsigned long long* next_path, uint64_t seed, const float* dL, float div, const float* info,
-                      const float4* resv, uint64_t max_round, float4* items, float4* post, float* R,
-                      unsigned long long* n_items, DScratch* scratch, int num_sms, cudaStream_t stream);
+                      const float4* resv, uint64_t max_round, const float4* segs, const unsigned long long* n_segs,
+                      uint64_t max_segs, float4* items, float4* post, float* R, unsigned long long* n_items,
+                      DScratch* scratch, int num_sms, cudaStream_t stream);
 
 // Radiance-cache forms of the forward NEE kernel (mode FW_CUT or FW_TRAIN).
 int launch_cache_paths(const DMedium& M, int mode, const PathSrc& src, uint64_t n_paths, uint64_t seed, float* out,

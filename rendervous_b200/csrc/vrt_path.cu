@@ -198,10 +198,10 @@ __global__ void __launch_bounds__(256, 3) k_nee_fw(DMedium M, PathSrc S, uint64_
                 } else {
                     // path_integrator_NEE prologue (vr_path_integrator_NEE.h:3-14)
                     float3 x0, w0;
-                    if (MODE == FW_BRANCH) {  // a given start, on its path's stream where the caller left it
+                    if (MODE == FW_BRANCH) {  // a given start, on the stream where the caller left it
                         const float4 a = io.branch[3 * pid], b = io.branch[3 * pid + 1], c = io.branch[3 * pid + 2];
                         const uint64_t gp = (uint64_t)__float_as_uint(c.x) | ((uint64_t)__float_as_uint(c.y) << 32);
-                        L.rng.init(seed, gp, 0);
+                        L.rng.init(seed, gp, __float_as_uint(c.z));
                         L.rng.seek(Rng::Pos{__float_as_uint(a.w), __float_as_uint(b.w)});
                         x0 = make_float3(a.x, a.y, a.z);
                         w0 = make_float3(b.x, b.y, b.z);
@@ -860,8 +860,9 @@ __device__ float3 in_scattering(const DMedium& M, Rng& rng, float3 x, float3 w, 
     return albedo(M, x, tl) * Ls;
 }
 
-// scatter-gradient term of a segment on the branch stream (_DRTQ.h:156-165, :249-259)
-__device__ void drtq_scatter_term(const DMedium& M, Rng& sec, float3 x, float3 w, float d, float3 W, float3 dL_dR,
+// scatter-gradient term of a segment (_DRTQ.h:156-165, :249-259) on the
+// segment's own stream (Rng::segment_stream)
+__device__ void drtq_scatter_term(const DMedium& M, Rng sec, float3 x, float3 w, float d, float3 W, float3 dL_dR,
                                   Tally& tl, uint32_t* status) {
     float s_t, weight_t;
     sample_transmittance_position(M, sec, x, w, d, s_t, weight_t, tl, status);
@@ -872,7 +873,10 @@ __device__ void drtq_scatter_term(const DMedium& M, Rng& sec, float3 x, float3 w
     sigma_bw(M, xs, mis_T * weight_t * dot(dL_dR, W * Ls), tl);
 }
 
-// vr_path_integrator_NEE_DRTQ.h:58-260 (branch seed = Philox stream 1)
+// vr_path_integrator_NEE_DRTQ.h:58-260.  The light rays' adjoints take fork j
+// of stream 1 beside fork j of the path's stream (as in DRT); each segment's
+// scatter term draws from its own stream, so the wavefront form can run them
+// as independent items.  A path stops at 2^24 - 1 segments (error 4).
 __device__ void path_nee_drtq_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float3 dL_dR, Tally& tl,
                                  uint32_t* status) {
     float tMin, tMax;
@@ -919,7 +923,8 @@ __device__ void path_nee_drtq_bw(const DMedium& M, Rng& rng, float3 x, float3 w,
     d = ini_d;
     rng.seek(before_path);
     bounces = 0;
-    drtq_scatter_term(M, sec, x, w, d, W, dL_dR, tl, status);
+    uint32_t vertex = 0;  // scattering vertices so far: the next segment's number
+    drtq_scatter_term(M, rng.segment_stream(0), x, w, d, W, dL_dR, tl, status);
     for (Flight ff; d > EPS; ++ff.it) {
         if (ff.it >= kPathStepCap) { raise_status(status, 4); return; }
         float md;
@@ -963,7 +968,8 @@ __device__ void path_nee_drtq_bw(const DMedium& M, Rng& rng, float3 x, float3 w,
         boundary(M, x, w, tMin, d);
         ff.bk.reset();
         if (all_less(W, EPS) || capped) break;
-        drtq_scatter_term(M, sec, x, w, d, W, dL_dR, tl, status);
+        if (++vertex + 1u >= (1u << 24)) { raise_status(status, 4); return; }
+        drtq_scatter_term(M, rng.segment_stream(vertex), x, w, d, W, dL_dR, tl, status);
     }
 }
 
@@ -1582,9 +1588,10 @@ __global__ void __launch_bounds__(256) k_path_bw(DMedium M, PathSrc S, uint64_t 
 // It samples the branch position (_NEE_DRT.h:233-235; DS: the defensive
 // collision position, no branch at weight 0) and its light rays, and appends
 // an item: the nested path's start (position, direction, stream position, path
-// id) and what the scatter needs (light terms, weights).  The nested
-// scattered-only NEE paths run on the state machine (k_nee_fw<FW_BRANCH>);
-// k_drt_branch_post adds their estimates and scatters at the branch position.
+// id and stream word) and what the scatter needs (light terms, weights).  The
+// nested scattered-only NEE paths run on the state machine
+// (k_nee_fw<FW_BRANCH>); k_drt_branch_post adds their estimates and scatters
+// at the branch position.
 template <bool DS>
 __global__ void __launch_bounds__(256) k_drt_branch_pre(DMedium M, PathSrc S, uint64_t n_paths, uint64_t p_begin,
                                                          const unsigned long long* next_path, uint64_t seed,
@@ -1623,7 +1630,8 @@ __global__ void __launch_bounds__(256) k_drt_branch_pre(DMedium M, PathSrc S, ui
         const unsigned long long i = atomicAdd(n_items, 1ull);
         items[3 * i] = make_float4(xs.x, xs.y, xs.z, __uint_as_float(rng.n));
         items[3 * i + 1] = make_float4(ws.x, ws.y, ws.z, __uint_as_float(rng.ntr));
-        items[3 * i + 2] = make_float4(__uint_as_float((uint32_t)pid), __uint_as_float((uint32_t)(pid >> 32)), 0.0f, 0.0f);
+        items[3 * i + 2] = make_float4(__uint_as_float((uint32_t)pid), __uint_as_float((uint32_t)(pid >> 32)),
+                                       __uint_as_float(0u), 0.0f);
         post[3 * i] = make_float4(Ls.x, Ls.y, Ls.z, weight_t);
         post[3 * i + 1] = make_float4(r2.x, r2.y, r2.z, r1.w);
         post[3 * i + 2] = make_float4(r0.w, 0.0f, 0.0f, 0.0f);
@@ -1631,10 +1639,66 @@ __global__ void __launch_bounds__(256) k_drt_branch_pre(DMedium M, PathSrc S, ui
     warp_add_counters(sc, 0, 0, tl);
 }
 
-// _NEE_DRT.h:261-268 (DS: _NEE_DRTDS.h:248-251): the branch estimate (light
-// terms + the nested path's) weighed by the reservoir and scattered at the
-// branch position.
-template <bool DS>
+// The DRTQ adjoint's scatter terms (_NEE_DRTQ.h:156-165, :249-259), one
+// thread per segment: the round's segment 0s (the primal wrote them in resv,
+// 3 float4 per path, length 0 for a primary ray that missed the medium) and
+// the segments after scattering vertices (segs, *n_segs of them); segments of
+// paths handed to the sequential form are skipped.  Each term draws from its
+// segment's stream (Rng::segment_stream): the transmittance-sampled position,
+// then in_scattering's light rays and direction; its nested scattered-only
+// NEE path is appended as an item for k_nee_fw<FW_BRANCH> and
+// k_drt_branch_post<2> scatters.
+__global__ void __launch_bounds__(256) k_drtq_segment_pre(DMedium M, uint64_t n_paths, uint64_t p_begin,
+                                                           const unsigned long long* next_path,
+                                                           const unsigned long long* n_segs, uint64_t cap_segs,
+                                                           uint64_t seed, const float* __restrict__ info,
+                                                           const float4* __restrict__ resv,
+                                                           const float4* __restrict__ segs, float4* items, float4* post,
+                                                           unsigned long long* n_items, DScratch* sc) {
+    constexpr uint32_t kSpilledPath = 0xfffffffdu;  // the first-collision word of a handed-over path
+    unsigned long long end = *next_path;
+    if (end > n_paths) end = n_paths;
+    const uint64_t n_round = end > p_begin ? end - p_begin : 0;
+    unsigned long long ns = *n_segs;
+    if (ns > cap_segs) ns = cap_segs;
+    Tally tl;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_round + ns;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float4* g = i < n_round ? resv + 4 * i : segs + 3 * (i - n_round);
+        const float4 a = g[0], b = g[1], c = g[2];
+        if (i < n_round && !(a.w > 0.0f)) continue;  // the primary ray missed the medium
+        const uint64_t k = __float_as_uint(c.w);     // the path's index in the round
+        if (__float_as_uint(info[8 * k + 7]) == kSpilledPath) continue;
+        const uint64_t pid = p_begin + k;
+        Rng rng;
+        rng.init(seed, pid, 0);
+        rng = rng.segment_stream(__float_as_uint(b.w));
+        const float3 x = make_float3(a.x, a.y, a.z), w = make_float3(b.x, b.y, b.z);
+        float s_t, weight_t;
+        sample_transmittance_position(M, rng, x, w, a.w, s_t, weight_t, tl, &sc->status);
+        const float3 xs = x + w * s_t;
+        float3 ls_dir;  // in_scattering (_NEE_DRTQ.h:45-55) up to its nested path
+        const float3 Ls_env = environment_sample(M, rng, ls_dir);
+        float3 Ls = transmittance(M, rng, xs, ls_dir, tl, &sc->status) * Ls_env * phase(M, w, ls_dir);
+        if (M.has_sun) Ls = Ls + transmittance(M, rng, xs, M.sun_dir, tl, &sc->status) * M.sun_L * phase(M, w, M.sun_dir);
+        const float3 ws = phase_sample(M, rng, w);
+        const unsigned long long o = atomicAdd(n_items, 1ull);
+        items[3 * o] = make_float4(xs.x, xs.y, xs.z, __uint_as_float(rng.n));
+        items[3 * o + 1] = make_float4(ws.x, ws.y, ws.z, __uint_as_float(rng.ntr));
+        items[3 * o + 2] = make_float4(__uint_as_float(rng.plo), __uint_as_float(rng.phi), __uint_as_float(rng.stream),
+                                       __uint_as_float((uint32_t)k));
+        post[3 * o] = make_float4(Ls.x, Ls.y, Ls.z, weight_t);
+        post[3 * o + 1] = make_float4(c.x, c.y, c.z, 0.0f);
+        post[3 * o + 2] = make_float4(__uint_as_float((uint32_t)pid), __uint_as_float((uint32_t)(pid >> 32)), 0.0f, 0.0f);
+    }
+    warp_add_counters(sc, 0, 0, tl);
+}
+
+// _NEE_DRT.h:261-268 (MODE 1, DRTDS: _NEE_DRTDS.h:248-251): the branch
+// estimate (light terms + the nested path's) weighed by the reservoir and
+// scattered at the branch position.  MODE 2, DRTQ (_NEE_DRTQ.h:52-54,
+// :162-164): a segment's in-scattered light times W, MIS-weighted.
+template <int MODE>
 __global__ void __launch_bounds__(256) k_drt_branch_post(DMedium M, PathSrc S, uint64_t n_items,
                                                           const float4* __restrict__ items,
                                                           const float4* __restrict__ post, const float* __restrict__ R,
@@ -1642,16 +1706,23 @@ __global__ void __launch_bounds__(256) k_drt_branch_post(DMedium M, PathSrc S, u
     Tally tl;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_items;
          i += (uint64_t)gridDim.x * blockDim.x) {
-        const float4 a = items[3 * i], c = items[3 * i + 2];
+        const float4 a = items[3 * i], c = MODE == 2 ? post[3 * i + 2] : items[3 * i + 2];
         const float4 p0 = post[3 * i], p1 = post[3 * i + 1], p2 = post[3 * i + 2];
         const uint64_t pid = (uint64_t)__float_as_uint(c.x) | ((uint64_t)__float_as_uint(c.y) << 32);
         const long long o = S.is_camera ? (long long)(pid % (uint64_t)S.npix) : (long long)pid;
         const float3 dL_dR = ld3(dL + 3 * o) / div;
         const float3 xs = make_float3(a.x, a.y, a.z);
         float3 Ls = make_float3(p0.x, p0.y, p0.z) + 1.0f * ld3(R + 3 * i);
+        if (MODE == 2) {
+            Ls = albedo(M, xs, tl) * Ls;
+            const float sigma_t = sigma(M, xs, tl);
+            const float mis_T = 1.0f / (1.0f + sigma_t * sigma_t);
+            sigma_bw(M, xs, mis_T * p0.w * dot(dL_dR, make_float3(p1.x, p1.y, p1.z) * Ls), tl);
+            continue;
+        }
         Ls = Ls * make_float3(p1.x, p1.y, p1.z) * p0.w * albedo(M, xs, tl);
         const float total_weight = p1.w, res_P = p2.x;
-        if (DS) {
+        if (MODE == 1) {
             sigma_bw(M, xs, dot(dL_dR, Ls) * total_weight / res_P, tl);
         } else {
             const float sigma_xs = sigma(M, xs, tl);
@@ -1662,21 +1733,30 @@ __global__ void __launch_bounds__(256) k_drt_branch_post(DMedium M, PathSrc S, u
     warp_add_counters(sc, 0, 0, tl);
 }
 
-int launch_drt_branch(const DMedium& M, bool ds, const PathSrc& src, uint64_t n_paths, uint64_t p_begin,
+// mode 0 DRT, 1 DRTDS (one branch per path of the round, from resv), 2 DRTQ
+// (one scatter term per segment: the round's segment 0s in resv, then the
+// *n_segs segments in segs)
+int launch_drt_branch(const DMedium& M, int mode, const PathSrc& src, uint64_t n_paths, uint64_t p_begin,
                       const unsigned long long* next_path, uint64_t seed, const float* dL, float div, const float* info,
-                      const float4* resv, uint64_t max_round, float4* items, float4* post, float* R,
-                      unsigned long long* n_items, DScratch* scratch, int num_sms, cudaStream_t stream) {
+                      const float4* resv, uint64_t max_round, const float4* segs, const unsigned long long* n_segs,
+                      uint64_t max_segs, float4* items, float4* post, float* R, unsigned long long* n_items,
+                      DScratch* scratch, int num_sms, cudaStream_t stream) {
     if (max_round == 0) return 0;
     KernelScope ks(VRT_K_DRT_BRANCH, stream);
     // n_items[0]: the items appended, n_items[1]: the nested paths' work counter
     cudaError_t e = cudaMemsetAsync(n_items, 0, 2 * sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return launch_status(e);
-    const uint64_t need = (max_round + 255) / 256;
+    const uint64_t need = (max_round + (mode == 2 ? max_segs : 0) + 255) / 256;
     int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
-    if (ds) k_drt_branch_pre<true><<<blocks, 256, 0, stream>>>(M, src, n_paths, p_begin, next_path, seed, info, resv,
-                                                                 items, post, n_items, scratch);
-    else k_drt_branch_pre<false><<<blocks, 256, 0, stream>>>(M, src, n_paths, p_begin, next_path, seed, info, resv,
-                                                               items, post, n_items, scratch);
+    if (mode == 2)
+        k_drtq_segment_pre<<<blocks, 256, 0, stream>>>(M, n_paths, p_begin, next_path, n_segs, max_segs, seed, info,
+                                                        resv, segs, items, post, n_items, scratch);
+    else if (mode == 1)
+        k_drt_branch_pre<true><<<blocks, 256, 0, stream>>>(M, src, n_paths, p_begin, next_path, seed, info, resv,
+                                                             items, post, n_items, scratch);
+    else
+        k_drt_branch_pre<false><<<blocks, 256, 0, stream>>>(M, src, n_paths, p_begin, next_path, seed, info, resv,
+                                                              items, post, n_items, scratch);
     unsigned long long n = 0;
     if ((e = cudaMemcpyAsync(&n, n_items, sizeof(n), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
         return launch_status(e);
@@ -1693,8 +1773,9 @@ int launch_drt_branch(const DMedium& M, bool ds, const PathSrc& src, uint64_t n_
         k_nee_fw<FW_BRANCH><<<pb, 256, 0, stream>>>(M, src, n, seed, nullptr, 1.0f, scratch, io);
         const uint64_t np = (n + 255) / 256;
         blocks = (int)(np < (uint64_t)num_sms * 16 ? np : (uint64_t)num_sms * 16);
-        if (ds) k_drt_branch_post<true><<<blocks, 256, 0, stream>>>(M, src, n, items, post, R, dL, div, scratch);
-        else k_drt_branch_post<false><<<blocks, 256, 0, stream>>>(M, src, n, items, post, R, dL, div, scratch);
+        if (mode == 2) k_drt_branch_post<2><<<blocks, 256, 0, stream>>>(M, src, n, items, post, R, dL, div, scratch);
+        else if (mode == 1) k_drt_branch_post<1><<<blocks, 256, 0, stream>>>(M, src, n, items, post, R, dL, div, scratch);
+        else k_drt_branch_post<0><<<blocks, 256, 0, stream>>>(M, src, n, items, post, R, dL, div, scratch);
         launches += 2;
     }
     count_launches(launches);
@@ -1778,6 +1859,8 @@ int launch_radiance_bw(const DMedium& M, int bw_mode, const PathSrc& src, uint64
         count_launches(1);
         return launch_status(cudaGetLastError());
     }
+    // DRTQ's segment streams carry the path id in 40 bits
+    if (bw_mode == 3 && !pids && n_paths >= (1ull << 40)) return VRT_E_UNSUPPORTED;
     uint64_t need = (n_paths + 255) / 256;
     int blocks = (int)(need < (uint64_t)num_sms * 16 ? need : (uint64_t)num_sms * 16);
     if (bw_mode == 1) k_path_bw<1><<<blocks, 256, 0, stream>>>(M, src, n_paths, seed, dL, div, scratch, pids);

@@ -410,9 +410,15 @@ struct WaveBw {
     unsigned long long cap_spill;
     // per path of the round: the DRT adjoint's reservoir (4 float4: vertex and
     // its weight, direction and the running total, throughput and the stream
-    // position at the end of the primal), or the SPS adjoint's entry point and
+    // position at the end of the primal), the DRTQ adjoint's segment 0 (3
+    // float4, as in segs), or the SPS adjoint's entry point and
     // singular-vertex sigma (1 float4); null for NEE_DS
     float4* resv;
+    // DRTQ: the segments after scattering vertices (3 float4 each: start and
+    // length, direction and segment number, throughput and the path's index in
+    // the round), *hdr[14] of them; null otherwise
+    float4* segs;
+    unsigned long long cap_segs;
 };
 
 // Path admission of the DRT and SPS primals (all lanes call it with the

@@ -28,6 +28,14 @@
 //                  thread per path, its nested scattered-only NEE path on the
 //                  state machine (k_nee_fw<FW_BRANCH>), then the scatter
 //
+// DRTQ (_NEE_DRTQ.h:58-260) is the same primal without the reservoir and the
+// same replay; instead of one branch it takes a scatter term on every segment
+// (the primary ray and the segment after each scattering vertex that does not
+// end the path), each from a stream of its own (Rng::segment_stream), so the
+// primal writes the segments (segment 0 in resv, the others in segs) and
+// k_drtq_segment_pre + k_nee_fw<FW_BRANCH> + k_drt_branch_post<2>
+// (vrt_path.cu) run one term per thread and item.
+//
 // Compiled with -fmad=false, like the sequential form (vrt_path.cu), so a
 // walk here rounds as the sequential definition does.  Paths the collision log
 // cannot hold, and uncapped paths still going after kUncappedPass vertices,
@@ -39,6 +47,7 @@ namespace vrt {
 
 using namespace wave;
 
+template <bool Q>
 __global__ void __launch_bounds__(256, 3) k_drt_primal(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
                                                      DScratch* sc, WaveBw wv) {
     const unsigned lane = threadIdx.x & 31u;
@@ -87,7 +96,8 @@ __global__ void __launch_bounds__(256, 3) k_drt_primal(DMedium M, PathSrc S, uin
                         __stcs(reinterpret_cast<float4*>(io), make_float4(0.0f, 0.0f, 0.0f, 0.0f));
                         __stcs(reinterpret_cast<float4*>(io) + 1,
                                make_float4(0.0f, 0.0f, __uint_as_float(kNone), __uint_as_float(kNone)));
-                        __stcs(rv + 1, make_float4(w.x, w.y, w.z, 0.0f));
+                        if (Q) __stcs(rv, make_float4(x.x, x.y, x.z, 0.0f));  // no scatter term either
+                        else __stcs(rv + 1, make_float4(w.x, w.y, w.z, 0.0f));
                     } else {
                         // _NEE_DRT.h:68-69: the primal's T of the primary ray takes fork 0 of the
                         // path's stream (its value is unused); its adjoint, fork 0 of stream 1
@@ -95,9 +105,15 @@ __global__ void __launch_bounds__(256, 3) k_drt_primal(DMedium M, PathSrc S, uin
                         put_job(wv.jobs, jb + rank, x, w, env_radiance(M, w), job_key(pid, 0), kAdjOnly);
                         W = f3(1.0f);
                         total_weight = 3.0f;
-                        __stcs(rv, make_float4(x.x, x.y, x.z, 3.0f));  // the reservoir starts at the primary ray
-                        __stcs(rv + 1, make_float4(w.x, w.y, w.z, 3.0f));
-                        __stcs(rv + 2, make_float4(1.0f, 1.0f, 1.0f, 0.0f));
+                        if (Q) {  // DRTQ: segment 0, the primary ray's, for its scatter term
+                            __stcs(rv, make_float4(x.x, x.y, x.z, d));
+                            __stcs(rv + 1, make_float4(w.x, w.y, w.z, __uint_as_float(0u)));
+                            __stcs(rv + 2, make_float4(1.0f, 1.0f, 1.0f, __uint_as_float((uint32_t)k)));
+                        } else {  // the reservoir starts at the primary ray
+                            __stcs(rv, make_float4(x.x, x.y, x.z, 3.0f));
+                            __stcs(rv + 1, make_float4(w.x, w.y, w.z, 3.0f));
+                            __stcs(rv + 2, make_float4(1.0f, 1.0f, 1.0f, 0.0f));
+                        }
                         bounces = 0;
                         steps_path = 0;
                         first = kNone;
@@ -115,6 +131,7 @@ __global__ void __launch_bounds__(256, 3) k_drt_primal(DMedium M, PathSrc S, uin
         if (__all_sync(kAll, !alive && exhausted)) break;
 
         int nrec = 0, nj = 0, nev = 0;
+        uint32_t nseg = 0;  // DRTQ: the segment after this vertex takes a scatter term
         bool finish = false, spill = false;
         float3 wnee = f3(0.0f), sa = f3(0.0f), Le = f3(0.0f);
         float ev_s = 0.0f, ev_m = 0.0f, ph_env = 0.0f, ph_sun = 0.0f;
@@ -177,14 +194,15 @@ __global__ void __launch_bounds__(256, 3) k_drt_primal(DMedium M, PathSrc S, uin
                         float tMin;
                         boundary(M, x, w, tMin, d);
                         ff.bk.reset();
-                        // the reservoir: this vertex replaces the kept one with probability P / total
-                        const float current_P = W.x + W.y + W.z;
-                        total_weight += current_P;
-                        if (rng.uniform() < current_P / total_weight) {
-                            float4* rv = wv.resv + 4 * (pid - wv.p_begin);
-                            __stcs(rv, make_float4(x.x, x.y, x.z, current_P));
-                            __stcs(rv + 1, make_float4(w.x, w.y, w.z, 0.0f));  // total written at the end
-                            __stcs(rv + 2, make_float4(W.x, W.y, W.z, 0.0f));
+                        if (!Q) {  // the reservoir: this vertex replaces the kept one with probability P / total
+                            const float current_P = W.x + W.y + W.z;
+                            total_weight += current_P;
+                            if (rng.uniform() < current_P / total_weight) {
+                                float4* rv = wv.resv + 4 * (pid - wv.p_begin);
+                                __stcs(rv, make_float4(x.x, x.y, x.z, current_P));
+                                __stcs(rv + 1, make_float4(w.x, w.y, w.z, 0.0f));  // total written at the end
+                                __stcs(rv + 2, make_float4(W.x, W.y, W.z, 0.0f));
+                            }
                         }
                         nrec = rec_next == kNone ? 2 : 1;
                         nj = lights;
@@ -193,6 +211,8 @@ __global__ void __launch_bounds__(256, 3) k_drt_primal(DMedium M, PathSrc S, uin
                         } else if (wv.kpass > 0 && bounces >= wv.kpass) {
                             ev = 2;  // an uncapped path past the pass budget: whole, on the sequential form
                             spill = true;
+                        } else if (Q) {
+                            nseg = 1u;  // _NEE_DRTQ.h:249-259: the next segment's scatter term
                         }
                     }
                 }
@@ -237,6 +257,19 @@ __global__ void __launch_bounds__(256, 3) k_drt_primal(DMedium M, PathSrc S, uin
                 ++n_ev;
             }
         }
+        if (Q) {  // DRTQ: the segment after the vertex (start, direction, throughput, number)
+            const Slots4 sq = reserve_slots4(&wv.hdr[14], &wv.hdr[14], &wv.hdr[14], &wv.hdr[14], nseg);
+            if (nseg) {
+                if (sq.s0 >= wv.cap_segs) {
+                    guard(sc, 16);
+                } else {
+                    float4* g = wv.segs + 3 * sq.s0;
+                    __stcs(g, make_float4(x.x, x.y, x.z, d));
+                    __stcs(g + 1, make_float4(w.x, w.y, w.z, __uint_as_float((uint32_t)bounces)));
+                    __stcs(g + 2, make_float4(W.x, W.y, W.z, __uint_as_float((uint32_t)(pid - wv.p_begin))));
+                }
+            }
+        }
         if (nj) {  // the light rays of the vertex, weighted W * L * phase (W after the albedo)
             const unsigned long long j = sl.s0;
             const uint32_t tgt = (uint32_t)r << 2;
@@ -251,9 +284,11 @@ __global__ void __launch_bounds__(256, 3) k_drt_primal(DMedium M, PathSrc S, uin
                    make_float4(0.0f, 0.0f, __uint_as_float(first), __uint_as_float(spill ? kSpilled : first_ev)));
             // an entry whose last collision found the log full is skipped by the replay
             if (nl) __stcs(wv.list + sl.s3, make_uint4((uint32_t)k, logged ? first_ev : kUnlogged, n_ev, 0u));
-            float4* rv = wv.resv + 4 * k;
-            reinterpret_cast<float*>(rv + 1)[3] = total_weight;
-            __stcs(rv + 3, make_float4(__uint_as_float(rng.n), __uint_as_float(rng.ntr), 0.0f, 0.0f));
+            if (!Q) {
+                float4* rv = wv.resv + 4 * k;
+                reinterpret_cast<float*>(rv + 1)[3] = total_weight;
+                __stcs(rv + 3, make_float4(__uint_as_float(rng.n), __uint_as_float(rng.ntr), 0.0f, 0.0f));
+            }
             if (spill) {
                 const unsigned long long o = atomicAdd(wv.spill_count, 1ull);
                 if (o < wv.cap_spill) wv.spill[o] = (unsigned long long)pid;
@@ -373,20 +408,23 @@ int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, int bw_mode, const Pa
                        uint64_t seed, const float* dL, float div, cudaStream_t stream) {
     if (n_paths == 0) return 0;
     if (M.max_bounces < 0 || M.max_bounces > 4096 || M.tr_mode > 1) return VRT_E_UNSUPPORTED;
-    if (bw_mode != VRT_BW_NEE_DRT && bw_mode != VRT_BW_NEE_DRTDS) return VRT_E_INVALID_ARGUMENT;
-    const bool ds = bw_mode == VRT_BW_NEE_DRTDS;
+    if (bw_mode != VRT_BW_NEE_DRT && bw_mode != VRT_BW_NEE_DRTDS && bw_mode != VRT_BW_NEE_DRTQ)
+        return VRT_E_INVALID_ARGUMENT;
+    const bool ds = bw_mode == VRT_BW_NEE_DRTDS, q = bw_mode == VRT_BW_NEE_DRTQ;
+    if (q && n_paths >= (1ull << 40)) return VRT_E_UNSUPPORTED;  // segment streams take path ids below 2^40
     const unsigned long long lights = M.has_sun ? 2ull : 1ull;
     // uncapped paths (the reference's default) walk at most kUncappedPass
     // vertices here; the few that go on run whole on the sequential form
     const int kpass = M.max_bounces > 0 ? 0 : kUncappedPass;
     const unsigned long long B = (unsigned long long)(M.max_bounces > 0 ? M.max_bounces : kpass);
-    int blocksA = persistent_blocks((const void*)k_drt_primal, 256, ctx->num_sms);
+    int blocksA = persistent_blocks(q ? (const void*)k_drt_primal<true> : (const void*)k_drt_primal<false>, 256,
+                                    ctx->num_sms);
     int blocksC = persistent_blocks(ds ? (const void*)k_drt_replay<true> : (const void*)k_drt_replay<false>, 256,
                                     ctx->num_sms);
     const uint64_t need = (n_paths + 255) / 256;
     if ((uint64_t)blocksA > need) blocksA = (int)need;
     if ((uint64_t)blocksC > need) blocksC = (int)need;
-    WaveBw wv;
+    WaveBw wv{};
     wv.lanes = (unsigned long long)blocksA * 256ull;
     const unsigned long long inflight = wv.lanes < n_paths ? wv.lanes : n_paths;
     wv.res_jobs = inflight * (lights * B + 1ull);  // the vertices' light rays and the primary ray's adjoint
@@ -405,9 +443,14 @@ int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, int bw_mode, const Pa
     const size_t o_list = o_resv + wv.cap_paths * 64;
     const size_t o_evs = o_list + ((wv.cap_paths * 16 + 255) & ~(size_t)255);
     const size_t o_spill = o_evs + wv.cap_evs * 32, o_items = o_spill + ((wv.cap_spill * 8 + 255) & ~(size_t)255);
-    // the reservoir branches' items, their scatter data and the nested paths' estimates
-    const size_t o_post = o_items + wv.cap_paths * 48, o_bR = o_post + wv.cap_paths * 48;
-    const size_t bytes = o_bR + wv.cap_paths * 12;
+    // DRTQ: the segments after scattering vertices (at most one per vertex record)
+    wv.cap_segs = q ? wv.cap_recs : 0;
+    // the branches' items (DRT, DRTDS: one per path; DRTQ: one per segment), their
+    // scatter data and the nested paths' estimates
+    const unsigned long long cap_items = wv.cap_paths + wv.cap_segs;
+    const size_t o_post = o_items + cap_items * 48, o_bR = o_post + cap_items * 48;
+    const size_t o_segs = o_bR + ((cap_items * 12 + 255) & ~(size_t)255);
+    const size_t bytes = o_segs + wv.cap_segs * 48;
     int st = ensure_wave_buffer(ctx, bytes);
     if (st) return st;
     char* base = static_cast<char*>(ctx->wave);
@@ -419,6 +462,7 @@ int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, int bw_mode, const Pa
     float4* b_items = reinterpret_cast<float4*>(base + o_items);
     float4* b_post = reinterpret_cast<float4*>(base + o_post);
     float* b_R = reinterpret_cast<float*>(base + o_bR);
+    wv.segs = q ? reinterpret_cast<float4*>(base + o_segs) : nullptr;
     wv.over = nullptr;
     wv.list = reinterpret_cast<uint4*>(base + o_list);
     wv.evs = reinterpret_cast<CollisionRec*>(base + o_evs);
@@ -434,9 +478,13 @@ int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, int bw_mode, const Pa
         // [7] replay-list head, [8] replay list
         if ((e = cudaMemsetAsync(wv.hdr, 0, 9 * sizeof(unsigned long long), stream)) != cudaSuccess)
             return launch_status(e);
+        // [14] DRTQ's segment count
+        if (q && (e = cudaMemsetAsync(&wv.hdr[14], 0, sizeof(unsigned long long), stream)) != cudaSuccess)
+            return launch_status(e);
         {
             KernelScope ks(VRT_K_DRT_PRIMAL, stream);
-            k_drt_primal<<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
+            if (q) k_drt_primal<true><<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
+            else k_drt_primal<false><<<blocksA, 256, 0, stream>>>(M, src, n_paths, seed, ctx->scratch, wv);
         }
         count_launches(1);
         if ((st = launch_shadow_record(M, src, wv, seed, dL, div, ctx->scratch, ctx->num_sms, stream))) return st;
@@ -449,9 +497,9 @@ int launch_wave_drt_bw(vrt_context* ctx, const DMedium& M, int bw_mode, const Pa
         }
         count_launches(1);
         if ((st = launch_status(cudaGetLastError()))) return st;
-        if ((st = launch_drt_branch(M, ds, src, n_paths, wv.p_begin, &ctx->scratch->next_path, seed, dL, div, wv.info,
-                                    wv.resv, wv.cap_paths, b_items, b_post, b_R, &wv.hdr[12], ctx->scratch,
-                                    ctx->num_sms, stream)))
+        if ((st = launch_drt_branch(M, ds ? 1 : (q ? 2 : 0), src, n_paths, wv.p_begin, &ctx->scratch->next_path,
+                                    seed, dL, div, wv.info, wv.resv, wv.cap_paths, wv.segs, &wv.hdr[14], wv.cap_segs,
+                                    b_items, b_post, b_R, &wv.hdr[12], ctx->scratch, ctx->num_sms, stream)))
             return st;
         unsigned long long taken = 0;
         if ((e = cudaMemcpyAsync(&taken, &ctx->scratch->next_path, sizeof(taken), cudaMemcpyDeviceToHost, stream)) !=

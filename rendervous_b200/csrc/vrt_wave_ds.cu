@@ -589,7 +589,7 @@ int launch_wave_ds_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, ui
     if ((uint64_t)blocksA > need) blocksA = (int)need;
     if ((uint64_t)blocksC > need) blocksC = (int)need;
     if ((uint64_t)blocksW > need) blocksW = (int)need;
-    WaveBw wv;
+    WaveBw wv{};
     wv.lanes = (unsigned long long)blocksA * 256ull;
     const unsigned long long inflight = wv.lanes < n_paths ? wv.lanes : n_paths;
     wv.res_jobs = inflight * lights * B;

@@ -382,7 +382,7 @@ int launch_wave_sps_bw(vrt_context* ctx, const DMedium& M, const PathSrc& src, u
     const uint64_t need = (n_paths + 255) / 256;
     if ((uint64_t)blocksA > need) blocksA = (int)need;
     if ((uint64_t)blocksC > need) blocksC = (int)need;
-    WaveBw wv;
+    WaveBw wv{};
     wv.lanes = (unsigned long long)blocksA * 256ull;
     const unsigned long long inflight = wv.lanes < n_paths ? wv.lanes : n_paths;
     wv.res_jobs = inflight * (lights * B + 1ull);  // the vertices' light rays and the primary ray's adjoint

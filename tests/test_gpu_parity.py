@@ -265,6 +265,8 @@ def test_dt_integrator_matches_oracle(cuda):
     ("drt", dict(integrator="drt", majorant="grid", brick=8)),
     ("drt", dict(integrator="drt", max_bounces=0)),
     ("drtq", dict(integrator="drtq")),
+    ("drtq", dict(integrator="drtq", majorant="grid", brick=8)),
+    ("drtq", dict(integrator="drtq", max_bounces=0)),
     ("drtds", dict(integrator="drtds")),
     ("drtds", dict(integrator="drtds", majorant="grid", brick=8)),
     ("sps", dict(integrator="sps")),
@@ -334,12 +336,12 @@ def test_ds_collision_log_overflow_rewalks(cuda, limit):
         assert np.abs(a).sum() > 0 and rel < 1e-4, rel
 
 
-@pytest.mark.parametrize("integrator", ["drt", "drtds", "sps"])
+@pytest.mark.parametrize("integrator", ["drt", "drtds", "drtq", "sps"])
 def test_drt_wavefront_in_rounds_matches_one_round(cuda, integrator):
     """With the wavefront's round size capped (vrt_set_wave_batch_limit), the
-    DRT / DRTDS / SPS adjoints take their paths in several rounds (primal,
-    light rays, replay, branch per round); the gradients equal the one-round
-    run's up to the order of the float sums."""
+    DRT / DRTDS / DRTQ / SPS adjoints take their paths in several rounds
+    (primal, light rays, replay, branches per round); the gradients equal the
+    one-round run's up to the order of the float sums."""
     ffi, lib = _lib.ffi_lib()
     stream = _lib.stream_handle(cuda)
     ctx = _lib.context(cuda)
@@ -370,7 +372,7 @@ def test_drt_wavefront_in_rounds_matches_one_round(cuda, integrator):
     assert np.abs(grads[0]).sum() > 0 and rel < 1e-4, rel
 
 
-@pytest.mark.parametrize("integrator", ["drt", "sps"])
+@pytest.mark.parametrize("integrator", ["drt", "drtq", "sps"])
 def test_drt_wavefront_on_rays_matches_sequential_form(cuda, integrator):
     """The same on rays (the map evaluated on a ray batch, backward through
     vrt_radiance_bw): the wavefront against the sequential form (collision log
@@ -398,11 +400,12 @@ def test_drt_wavefront_on_rays_matches_sequential_form(cuda, integrator):
     assert np.abs(grads[0]).sum() > 0 and rel < 1e-4, rel
 
 
-@pytest.mark.parametrize("integrator", ["drt", "drtds", "sps"])
+@pytest.mark.parametrize("integrator", ["drt", "drtds", "drtq", "sps"])
 @pytest.mark.parametrize("limit", [1, 3000])
 def test_drt_wavefront_matches_sequential_form(cuda, limit, integrator):
-    """The DRT (DRTDS, SPS) adjoint's wavefront (primal with collision log, light-ray T and
-    adjoint jobs, log replay, reservoir branch) against its sequential form:
+    """The DRT (DRTDS, DRTQ, SPS) adjoint's wavefront (primal with collision log, light-ray T
+    and adjoint jobs, log replay, reservoir branch or per-segment scatter terms) against its
+    sequential form:
     with the collision log capped at `limit` records, the paths that do not fit
     run whole on the sequential form (all of them at 1), so the gradients of
     both runs agree up to the order of the float sums."""
