@@ -603,7 +603,7 @@ int vrt_transmittance_fw(vrt_context* ctx, const vrt_medium* m, int32_t mode, co
     if (n == 0) return VRT_OK;
     if (!rays || !T) return VRT_E_NULL_POINTER;
     if (!aligned8(rays)) return VRT_E_INVALID_ARGUMENT;
-    return launch_transmittance_fw(M, mode, rays, n, seed, T, ctx->scratch, (cudaStream_t)stream);
+    return launch_transmittance_fw(M, mode, rays, n, seed, T, ctx->scratch, ctx->num_sms, (cudaStream_t)stream);
 }
 
 int vrt_transmittance_bw(vrt_context* ctx, const vrt_medium* m, int32_t mode, const float* rays, int64_t n,
@@ -618,7 +618,13 @@ int vrt_transmittance_bw(vrt_context* ctx, const vrt_medium* m, int32_t mode, co
     if (n == 0 || !M.sigma.grad || mode >= 4) return VRT_OK;
     if (!rays || !dL_dT) return VRT_E_NULL_POINTER;
     if (!aligned8(rays)) return VRT_E_INVALID_ARGUMENT;
-    return launch_transmittance_bw(M, mode, rays, n, seed, dL_dT, ctx->scratch, (cudaStream_t)stream);
+    float* tmp = nullptr;  // the DDA adjoint's dL/dtau per ray, in the context's work buffer
+    if (mode == 2 || mode == 3) {
+        if ((st = ensure_wave_buffer(ctx, (size_t)n * sizeof(float)))) return st;
+        tmp = static_cast<float*>(ctx->wave);
+    }
+    return launch_transmittance_bw(M, mode, rays, n, seed, dL_dT, tmp, ctx->scratch, ctx->num_sms,
+                                   (cudaStream_t)stream);
 }
 
 int vrt_collision_sample_fw(vrt_context* ctx, const vrt_medium* m, const float* rays, int64_t n, uint64_t seed,

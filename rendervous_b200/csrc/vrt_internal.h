@@ -49,10 +49,12 @@ int launch_wave_fw(vrt_context* ctx, const DMedium& M, const PathSrc& src, uint6
 
 int persistent_blocks(const void* kernel, int block, int num_sms);
 
+// num_sms < 1: the DDA modes' persistent grid is sized from the device's SM count
 int launch_transmittance_fw(const DMedium& M, int mode, const float* rays, int64_t n, uint64_t seed, float* T,
-                            DScratch* scratch, cudaStream_t stream);
+                            DScratch* scratch, int num_sms, cudaStream_t stream);
+// tmp: n floats (the DDA modes' dL/dtau per ray between their two marches)
 int launch_transmittance_bw(const DMedium& M, int mode, const float* rays, int64_t n, uint64_t seed,
-                            const float* dL_dT, DScratch* scratch, cudaStream_t stream);
+                            const float* dL_dT, float* tmp, DScratch* scratch, int num_sms, cudaStream_t stream);
 
 // out: rays mode writes R [n,3]; camera mode accumulates R * scale into out[pixel].
 int launch_radiance_fw(const DMedium& M, int integrator, const PathSrc& src, uint64_t n_paths, uint64_t seed,

@@ -172,80 +172,95 @@ struct DDA {
     __device__ __forceinline__ float3 ialpha(float t) const {
         return (vm * t + vn) - make_float3((float)cx, (float)cy, (float)cz);
     }
-    // vr_transmittance_DDA.h:48-55; returns the axis stepped (0,1,2)
+    // vr_transmittance_DDA.h:48-55: the axis of the next step (0,1,2)
+    __device__ __forceinline__ int next_axis() const {
+        return (alpha.x <= alpha.y && alpha.x <= alpha.z) ? 0 : ((alpha.x > alpha.y && alpha.y <= alpha.z) ? 1 : 2);
+    }
+    // one step along `axis` (selects, no branch on the axis)
+    __device__ __forceinline__ void step(int axis) {
+        alpha.x = axis == 0 ? alpha.x + alpha_inc.x : alpha.x;
+        alpha.y = axis == 1 ? alpha.y + alpha_inc.y : alpha.y;
+        alpha.z = axis == 2 ? alpha.z + alpha_inc.z : alpha.z;
+        cx += axis == 0 ? sx : 0;
+        cy += axis == 1 ? sy : 0;
+        cz += axis == 2 ? sz : 0;
+    }
+    // returns the axis stepped
     __device__ __forceinline__ int advance_cell() {
-        if (alpha.x <= alpha.y && alpha.x <= alpha.z) { alpha.x += alpha_inc.x; cx += sx; return 0; }
-        if (alpha.x > alpha.y && alpha.y <= alpha.z) { alpha.y += alpha_inc.y; cy += sy; return 1; }
-        alpha.z += alpha_inc.z; cz += sz; return 2;
+        const int axis = next_axis();
+        step(axis);
+        return axis;
     }
-    // After a step along `axis`, keep the face crossed into and load the other.
-    // Corner slots are compile-time constants in every branch so s[] stays in
-    // registers.  KEEP is the slot offset of the face the ray crossed into.
-    template <int KEEP>
-    __device__ __forceinline__ void shift_x(const DGrid& g) {
-#pragma unroll
-        for (int k = 0; k < 8; k += 2) {
-            s[k + 1 - KEEP] = s[k + KEEP];
-            s[k + KEEP] = ldg(g.data + node(g, cx + KEEP, cy + ((k >> 1) & 1), cz + (k >> 2)));
-        }
+    // Node offsets of the current cell's corners, clamped as sigma_at clamps
+    // (vr_sigma_grid.h:1-7): o[0..1] along x, o[2..3] along y, o[4..5] along z.
+    __device__ __forceinline__ void corner_offsets(const DGrid& g, int* o) const {
+        o[0] = min(max(cx, 0), dimx) * g.sW;
+        o[1] = min(max(cx + 1, 0), dimx) * g.sW;
+        o[2] = min(max(cy, 0), dimy) * g.sH;
+        o[3] = min(max(cy + 1, 0), dimy) * g.sH;
+        o[4] = min(max(cz, 0), dimz) * g.sD;
+        o[5] = min(max(cz + 1, 0), dimz) * g.sD;
     }
-    template <int KEEP>  // 0 or 2
-    __device__ __forceinline__ void shift_y(const DGrid& g) {
-#pragma unroll
-        for (int z = 0; z < 2; ++z)
-#pragma unroll
-            for (int xx = 0; xx < 2; ++xx) {
-                s[z * 4 + (2 - KEEP) + xx] = s[z * 4 + KEEP + xx];
-                s[z * 4 + KEEP + xx] = ldg(g.data + node(g, cx + xx, cy + (KEEP >> 1), cz + z));
-            }
-    }
-    template <int KEEP>  // 0 or 4
-    __device__ __forceinline__ void shift_z(const DGrid& g) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            s[(4 - KEEP) + k] = s[KEEP + k];
-            s[KEEP + k] = ldg(g.data + node(g, cx + (k & 1), cy + (k >> 1), cz + (KEEP >> 2)));
-        }
-    }
+    // After a step along `axis`: the corners on the face crossed into (slots
+    // whose `axis` bit is 1 after a step up, 0 after a step down) load at the
+    // new cell; the opposite face takes the values they had.  Selects and
+    // predicated loads instead of a branch per axis and sign, so lanes that
+    // step along different axes stay converged; every slot gets the value the
+    // per-axis form gave it.
     __device__ __forceinline__ void shift_load(const DGrid& g, int axis) {
-        if (axis == 0) {
-            if (sx > 0) shift_x<1>(g); else if (sx < 0) shift_x<0>(g);
-        } else if (axis == 1) {
-            if (sy > 0) shift_y<2>(g); else if (sy < 0) shift_y<0>(g);
-        } else {
-            if (sz > 0) shift_z<4>(g); else if (sz < 0) shift_z<0>(g);
+        const int st = axis == 0 ? sx : (axis == 1 ? sy : sz);
+        if (st == 0) return;
+        const int m = 1 << axis, far = st > 0 ? m : 0;
+        int o[6];
+        corner_offsets(g, o);
+        float ns[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            float v = axis == 0 ? s[k ^ 1] : (axis == 1 ? s[k ^ 2] : s[k ^ 4]);
+            if ((k & m) == far) v = ldg(g.data + (o[4 + (k >> 2)] + o[2 + ((k >> 1) & 1)] + o[k & 1]));
+            ns[k] = v;
         }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s[k] = ns[k];
     }
 
     static constexpr float kGL = 0.28867513459481288225f;  // 1 / (2 sqrt 3)
 
+    // One cell of tau: its (midpoint or Gauss-Legendre) integral into the
+    // compensated (Kahan) sum, then the step and the new face's loads.
+    template <bool EXACT>
+    __device__ __forceinline__ void tau_cell(const DGrid& g, float& acc, float& comp_err, float& ct) {
+        float nt = gmin(d, gmin(alpha.x, gmin(alpha.y, alpha.z)));
+        float dt = nt - ct;
+        float term;
+        if (!EXACT) {
+            term = interp(ialpha(mixf(ct, nt, 0.5f))) * dt;
+        } else {
+            float mid = mixf(ct, nt, 0.5f), h = dt * kGL;
+            term = (interp(ialpha(mid - h)) + interp(ialpha(mid + h))) * (dt * 0.5f);
+        }
+        float yk = term - comp_err;
+        float tk = acc + yk;
+        comp_err = (tk - acc) - yk;
+        acc = tk;
+        ct = nt;
+        int axis = advance_cell();
+        shift_load(g, axis);
+    }
+    // the reference stops 1e-4 short of the exit (vr_transmittance_DDA.h:38);
+    // the exact mode integrates the whole segment
+    template <bool EXACT>
+    __device__ __forceinline__ float tau_stop() const { return EXACT ? d : d - 0.0001f; }
+
     // tau over the segment; one step and one (8-corner) lookup per cell
     template <bool EXACT>
     __device__ __forceinline__ float tau(const DGrid& g, Tally& tl) {
-        // compensated (Kahan) sum of the per-cell integrals
         float acc = 0.0f, comp_err = 0.0f, ct = 0.0f;
         load_all(g);
         int it = 0;
-        // the reference stops 1e-4 short of the exit (vr_transmittance_DDA.h:38);
-        // the exact mode integrates the whole segment
-        const float stop = EXACT ? d : d - 0.0001f;
+        const float stop = tau_stop<EXACT>();
         while (ct < stop && it < kStepCap) {
-            float nt = gmin(d, gmin(alpha.x, gmin(alpha.y, alpha.z)));
-            float dt = nt - ct;
-            float term;
-            if (!EXACT) {
-                term = interp(ialpha(mixf(ct, nt, 0.5f))) * dt;
-            } else {
-                float mid = mixf(ct, nt, 0.5f), h = dt * kGL;
-                term = (interp(ialpha(mid - h)) + interp(ialpha(mid + h))) * (dt * 0.5f);
-            }
-            float yk = term - comp_err;
-            float tk = acc + yk;
-            comp_err = (tk - acc) - yk;
-            acc = tk;
-            ct = nt;
-            int axis = advance_cell();
-            shift_load(g, axis);
+            tau_cell<EXACT>(g, acc, comp_err, ct);
             ++tl.steps;
             ++tl.lookups;
             ++it;
@@ -268,28 +283,54 @@ struct DDA {
         if (acc[k] != 0.0f) red_add(g.grad + node(g, cx + (k & 1), cy + ((k >> 1) & 1), cz + (k >> 2)), acc[k]);
         acc[k] = 0.0f;
     }
-    template <int KEEP>
-    __device__ __forceinline__ void carry_x(const DGrid& g, float* acc) const {
+    // Before a step along `axis`: the sums of the face left behind go to the
+    // gradient, those of the face crossed into move to the opposite slots
+    // (they are that face's corners in the next cell).  Selects and predicated
+    // atomics, as in shift_load.
+    __device__ __forceinline__ void carry(const DGrid& g, float* acc, int axis) const {
+        const int st = axis == 0 ? sx : (axis == 1 ? sy : sz);
+        if (st == 0) return;
+        const int m = 1 << axis, far = st > 0 ? m : 0;
+        int o[6];
+        corner_offsets(g, o);
+        float na[8];
 #pragma unroll
-        for (int k = 0; k < 8; k += 2) { flush(g, acc, k + 1 - KEEP); acc[k + 1 - KEEP] = acc[k + KEEP]; acc[k + KEEP] = 0.0f; }
+        for (int k = 0; k < 8; ++k) {
+            const bool behind = (k & m) != far;
+            if (behind && acc[k] != 0.0f) red_add(g.grad + (o[4 + (k >> 2)] + o[2 + ((k >> 1) & 1)] + o[k & 1]), acc[k]);
+            const float v = axis == 0 ? acc[k ^ 1] : (axis == 1 ? acc[k ^ 2] : acc[k ^ 4]);
+            na[k] = behind ? v : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = na[k];
     }
-    template <int KEEP>
-    __device__ __forceinline__ void carry_y(const DGrid& g, float* acc) const {
-#pragma unroll
-        for (int z = 0; z < 2; ++z)
-#pragma unroll
-            for (int xx = 0; xx < 2; ++xx) {
-                const int kf = z * 4 + (2 - KEEP) + xx, kk = z * 4 + KEEP + xx;
-                flush(g, acc, kf); acc[kf] = acc[kk]; acc[kk] = 0.0f;
-            }
+    // One cell of the second march (vr_transmittance_DDA.h:121-153): the
+    // cell's dL/dsigma per corner into acc, then the step (the face shared with
+    // the next cell stays in registers).
+    template <bool EXACT>
+    __device__ __forceinline__ void scatter_cell(const DGrid& g, float dL_dtau, float* acc, float& ct) {
+        float nt = gmin(d, gmin(alpha.x, gmin(alpha.y, alpha.z)));
+        float dt = nt - ct;
+        if (!EXACT) {
+            add_weights(ialpha(mixf(ct, nt, 0.5f)), dL_dtau * dt, acc);
+        } else {
+            float mid = mixf(ct, nt, 0.5f), h = dt * kGL;
+            add_weights(ialpha(mid - h), dL_dtau * dt * 0.5f, acc);
+            add_weights(ialpha(mid + h), dL_dtau * dt * 0.5f, acc);
+        }
+        ct = nt;
+        // flush the face left behind, move the crossed face to its new slot
+        const int axis = next_axis();
+        carry(g, acc, axis);
+        step(axis);
     }
-    template <int KEEP>
-    __device__ __forceinline__ void carry_z(const DGrid& g, float* acc) const {
+    // acc holds the corners of the cell the march stopped in (the face
+    // carried over from the last cell plus zeros): flush at these indices
+    __device__ __forceinline__ void scatter_end(const DGrid& g, float* acc) const {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) { flush(g, acc, (4 - KEEP) + k); acc[(4 - KEEP) + k] = acc[KEEP + k]; acc[KEEP + k] = 0.0f; }
+        for (int k = 0; k < 8; ++k) flush(g, acc, k);
     }
-    // vr_transmittance_DDA.h:121-153 second march: dL/dsigma per corner; the
-    // face shared with the next cell stays in registers.
+    // vr_transmittance_DDA.h:121-153 second march: dL/dsigma per corner
     template <bool EXACT>
     __device__ __forceinline__ void scatter(const DGrid& g, float dL_dtau, Tally& tl) {
         float acc[8];
@@ -297,37 +338,14 @@ struct DDA {
         for (int k = 0; k < 8; ++k) acc[k] = 0.0f;
         float ct = 0.0f;
         int it = 0;
-        const float stop = EXACT ? d : d - 0.0001f;
+        const float stop = tau_stop<EXACT>();
         while (ct < stop && it < kStepCap) {
-            float nt = gmin(d, gmin(alpha.x, gmin(alpha.y, alpha.z)));
-            float dt = nt - ct;
-            if (!EXACT) {
-                add_weights(ialpha(mixf(ct, nt, 0.5f)), dL_dtau * dt, acc);
-            } else {
-                float mid = mixf(ct, nt, 0.5f), h = dt * kGL;
-                add_weights(ialpha(mid - h), dL_dtau * dt * 0.5f, acc);
-                add_weights(ialpha(mid + h), dL_dtau * dt * 0.5f, acc);
-            }
-            ct = nt;
-            // flush the face left behind, move the crossed face to its new slot
-            if (alpha.x <= alpha.y && alpha.x <= alpha.z) {
-                if (sx > 0) carry_x<1>(g, acc); else if (sx < 0) carry_x<0>(g, acc);
-                alpha.x += alpha_inc.x; cx += sx;
-            } else if (alpha.x > alpha.y && alpha.y <= alpha.z) {
-                if (sy > 0) carry_y<2>(g, acc); else if (sy < 0) carry_y<0>(g, acc);
-                alpha.y += alpha_inc.y; cy += sy;
-            } else {
-                if (sz > 0) carry_z<4>(g, acc); else if (sz < 0) carry_z<0>(g, acc);
-                alpha.z += alpha_inc.z; cz += sz;
-            }
+            scatter_cell<EXACT>(g, dL_dtau, acc, ct);
             tl.reds += 4;
             ++it;
         }
         tl.reds += 4;
-        // acc now holds the corners of the cell the march stopped in (the face
-        // carried over from the last cell plus zeros): flush at these indices.
-#pragma unroll
-        for (int k = 0; k < 8; ++k) flush(g, acc, k);
+        scatter_end(g, acc);
     }
 };
 

@@ -1,6 +1,7 @@
 // vrt_transmittance.cu -- transmittance maps evaluated on rays [n, 6] (sm_100a).
 //
-// One thread per ray; ray i draws from Philox path id i.  These are the
+// One thread per ray (the DDA modes: persistent lanes refilled ray by ray);
+// ray i draws from Philox path id i.  These are the
 // operator forms of GridDDATransmittance / RatiotrackingTransmittance /
 // DeltatrackingTransmittance, GridRatiotrackingTransmittance and
 // GridDeltatrackingTransmittance (include/maps/transmittance_{dda,rt,dt,grt,gdt}.h).
@@ -79,20 +80,177 @@ __global__ void __launch_bounds__(256) k_transmittance_bw(DMedium M, const float
     warp_tally(sc, count, tl);
 }
 
+// The DDA modes as persistent lanes: a lane takes the next ray as soon as its
+// march ends (one atomic per warp refill, from the scratch's work counter), so
+// the short and missing rays of a warp do not wait for its longest (one ray
+// per thread kept 7.7 of 32 lanes active).  A ray's arithmetic is
+// transmittance_dda's, cell for cell; at most kCells cells per lane between
+// refills.
+constexpr int kCells = 8;
+
+__device__ __forceinline__ bool take_ray(DScratch* sc, int64_t n, bool want_ray, int64_t& i) {
+    const unsigned want = __ballot_sync(0xffffffffu, want_ray);
+    if (!want) return false;
+    const unsigned lane = threadIdx.x & 31u;
+    const int leader = __ffs(want) - 1;
+    unsigned long long base = 0;
+    if ((int)lane == leader) base = atomicAdd(&sc->next_path, (unsigned long long)__popc(want));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (!want_ray) return false;
+    i = (int64_t)(base + __popc(want & ((1u << lane) - 1u)));
+    return true;
+}
+__device__ __forceinline__ void load_ray(const float* rays, int64_t i, float3& x, float3& w) {
+    const float2* r2 = reinterpret_cast<const float2*>(rays + 6 * i);  // rows are 8-byte aligned
+    const float2 a = __ldg(r2), b = __ldg(r2 + 1), c = __ldg(r2 + 2);
+    x = make_float3(a.x, a.y, b.x);
+    w = make_float3(b.y, c.x, c.y);
+}
+
+// BW = false: T of every ray into out.  BW = true, the adjoint's first march:
+// dL/dtau = -dL/dT T into out (0 for a ray with dL/dT = 0, which it skips,
+// and for a miss), for k_dda_scatter.
+template <bool EXACT, bool BW>
+__global__ void __launch_bounds__(256) k_dda_fw(DMedium M, const float* __restrict__ rays, int64_t n,
+                                                const float* __restrict__ dL_dT, float* __restrict__ out,
+                                                DScratch* sc) {
+    DDA q;
+    float acc = 0.0f, comp = 0.0f, ct = 0.0f, stop = 0.0f, g = 0.0f;
+    int it = 0;
+    int64_t ray = -1;
+    bool exhausted = false;
+    uint32_t count = 0;
+    Tally tl;
+    while (true) {
+        int64_t i;
+        if (take_ray(sc, n, ray < 0 && !exhausted, i)) {
+            if (i >= n) {
+                exhausted = true;
+            } else {
+                float3 x, w;
+                load_ray(rays, i, x, w);
+                if (BW) g = __ldg(dL_dT + i);
+                else ++count;
+                if ((BW && g == 0.0f) || !q.init(M, x, w)) {
+                    out[i] = BW ? 0.0f : 1.0f;  // no gradient, or a miss
+                } else {
+                    q.load_all(M.sigma);
+                    acc = 0.0f;
+                    comp = 0.0f;
+                    ct = 0.0f;
+                    it = 0;
+                    stop = q.tau_stop<EXACT>();
+                    ray = i;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, ray < 0 && exhausted)) break;
+        if (ray >= 0) {
+            for (int c = 0; c < kCells; ++c) {
+                if (!(ct < stop && it < kStepCap)) {
+                    out[ray] = BW ? -g * expf(-acc) : expf(-acc);
+                    ray = -1;
+                    break;
+                }
+                q.tau_cell<EXACT>(M.sigma, acc, comp, ct);
+                ++tl.steps;
+                ++tl.lookups;
+                ++it;
+            }
+        }
+    }
+    warp_tally(sc, count, tl);
+}
+
+// The adjoint's second march (transmittance_dda_bw after its tau): rays with
+// dL/dtau != 0 scatter from the segment's start.
+template <bool EXACT>
+__global__ void __launch_bounds__(256) k_dda_scatter(DMedium M, const float* __restrict__ rays, int64_t n,
+                                                     const float* __restrict__ dL_dtau, DScratch* sc) {
+    DDA q;
+    float ct = 0.0f, stop = 0.0f, g = 0.0f;
+    float gacc[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) gacc[k] = 0.0f;
+    int it = 0;
+    bool busy = false, exhausted = false;
+    uint32_t count = 0;
+    Tally tl;
+    while (true) {
+        int64_t i;
+        if (take_ray(sc, n, !busy && !exhausted, i)) {
+            if (i >= n) {
+                exhausted = true;
+            } else {
+                ++count;
+                g = __ldg(dL_dtau + i);
+                float3 x, w;
+                load_ray(rays, i, x, w);
+                if (g != 0.0f && q.init(M, x, w)) {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) gacc[k] = 0.0f;
+                    ct = 0.0f;
+                    it = 0;
+                    stop = q.tau_stop<EXACT>();
+                    busy = true;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, !busy && exhausted)) break;
+        if (busy) {
+            for (int c = 0; c < kCells; ++c) {
+                if (!(ct < stop && it < kStepCap)) {
+                    tl.reds += 4;
+                    q.scatter_end(M.sigma, gacc);
+                    busy = false;
+                    break;
+                }
+                q.scatter_cell<EXACT>(M.sigma, g, gacc, ct);
+                tl.reds += 4;
+                ++it;
+            }
+        }
+    }
+    warp_tally(sc, count, tl);
+}
+
 static int grid_for(int64_t n) {
     int64_t b = (n + 255) / 256;
     return (int)(b < 65535 * 8 ? (b < 1 ? 1 : b) : 65535 * 8);
 }
 
+// persistent blocks for the DDA kernels (num_sms < 1: asked of the device)
+static int dda_blocks(const void* kernel, int num_sms, int64_t n) {
+    if (num_sms < 1) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || num_sms < 1)
+            num_sms = 1;
+    }
+    int b = persistent_blocks(kernel, 256, num_sms);
+    const int64_t need = (n + 255) / 256;
+    return (int64_t)b > need ? (int)need : b;
+}
+
 int launch_transmittance_fw(const DMedium& M, int mode, const float* rays, int64_t n, uint64_t seed, float* T,
-                            DScratch* scratch, cudaStream_t stream) {
+                            DScratch* scratch, int num_sms, cudaStream_t stream) {
     if (n == 0) return 0;
+    if (mode == 2 || mode == 3) {
+        cudaError_t e = cudaMemsetAsync(&scratch->next_path, 0, sizeof(unsigned long long), stream);
+        if (e != cudaSuccess) return launch_status(e);
+        if (mode == 2)
+            k_dda_fw<false, false><<<dda_blocks((const void*)k_dda_fw<false, false>, num_sms, n), 256, 0, stream>>>(
+                M, rays, n, nullptr, T, scratch);
+        else
+            k_dda_fw<true, false><<<dda_blocks((const void*)k_dda_fw<true, false>, num_sms, n), 256, 0, stream>>>(
+                M, rays, n, nullptr, T, scratch);
+        count_launches(1);
+        return launch_status(cudaGetLastError());
+    }
     int g = grid_for(n);
     switch (mode) {
         case 0: k_transmittance_fw<0><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
         case 1: k_transmittance_fw<1><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
-        case 2: k_transmittance_fw<2><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
-        case 3: k_transmittance_fw<3><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
         case 4: k_transmittance_fw<4><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
         default: k_transmittance_fw<5><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
     }
@@ -101,14 +259,32 @@ int launch_transmittance_fw(const DMedium& M, int mode, const float* rays, int64
 }
 
 int launch_transmittance_bw(const DMedium& M, int mode, const float* rays, int64_t n, uint64_t seed,
-                            const float* dL_dT, DScratch* scratch, cudaStream_t stream) {
+                            const float* dL_dT, float* tmp, DScratch* scratch, int num_sms, cudaStream_t stream) {
     if (n == 0) return 0;
+    if (mode == 2 || mode == 3) {  // the tau march into tmp (dL/dtau per ray), then the scatter march
+        cudaError_t e = cudaMemsetAsync(&scratch->next_path, 0, sizeof(unsigned long long), stream);
+        if (e != cudaSuccess) return launch_status(e);
+        if (mode == 2)
+            k_dda_fw<false, true><<<dda_blocks((const void*)k_dda_fw<false, true>, num_sms, n), 256, 0, stream>>>(
+                M, rays, n, dL_dT, tmp, scratch);
+        else
+            k_dda_fw<true, true><<<dda_blocks((const void*)k_dda_fw<true, true>, num_sms, n), 256, 0, stream>>>(
+                M, rays, n, dL_dT, tmp, scratch);
+        if ((e = cudaMemsetAsync(&scratch->next_path, 0, sizeof(unsigned long long), stream)) != cudaSuccess)
+            return launch_status(e);
+        if (mode == 2)
+            k_dda_scatter<false><<<dda_blocks((const void*)k_dda_scatter<false>, num_sms, n), 256, 0, stream>>>(
+                M, rays, n, tmp, scratch);
+        else
+            k_dda_scatter<true><<<dda_blocks((const void*)k_dda_scatter<true>, num_sms, n), 256, 0, stream>>>(
+                M, rays, n, tmp, scratch);
+        count_launches(2);
+        return launch_status(cudaGetLastError());
+    }
     int g = grid_for(n);
     switch (mode) {
         case 0: k_transmittance_bw<0><<<g, 256, 0, stream>>>(M, rays, n, seed, dL_dT, scratch); break;
-        case 1: k_transmittance_bw<1><<<g, 256, 0, stream>>>(M, rays, n, seed, dL_dT, scratch); break;
-        case 2: k_transmittance_bw<2><<<g, 256, 0, stream>>>(M, rays, n, seed, dL_dT, scratch); break;
-        default: k_transmittance_bw<3><<<g, 256, 0, stream>>>(M, rays, n, seed, dL_dT, scratch); break;
+        default: k_transmittance_bw<1><<<g, 256, 0, stream>>>(M, rays, n, seed, dL_dT, scratch); break;
     }
     count_launches(1);
     return launch_status(cudaGetLastError());
