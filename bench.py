@@ -757,8 +757,9 @@ def run_other(args):
                        "frac": 4.0 * reds_bw / (t_bw / 1e3) / 1e9 / peak,
                        "adds_per_s_g": reds_bw / (t_bw / 1e3) / 1e9, "atomic_peak_g": apeaks,
                        "frac_of_l2_atomic": reds_bw / (t_bw / 1e3) / 1e9 / apeaks["l2"],
-                       "note": "the backward call re-marches for T (32 B per cell) and scatters 4 atomic adds per cell"},
-                "roofline": {"bound": "hbm", "kernel": "k_transmittance_fw<2>",
+                       "note": "the backward call re-marches for T (k_dda_fw<0, 1>: 32 B per cell), then scatters "
+                               "4 atomic adds per cell (k_dda_scatter<0>)"},
+                "roofline": {"bound": "hbm", "kernel": "k_dda_fw<0, 0>",
                              "achieved": 32.0 * cells / (t_fw / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                              "frac": 32.0 * cells / (t_fw / 1e3) / 1e9 / peak}}
     print(json.dumps(line))
