@@ -10,10 +10,9 @@
 //                                  scattered_emitted_radiance_mc.h) over
 //                                  radiance = transmittance x environment
 //
-// One path per thread, grid-stride: these are emission-absorption and single
-// scattering integrators whose per-path work is one tracking walk (MC) or one
-// DDA walk with an exitance evaluation per cell (DDA), so lanes stay in step
-// far better than on multi-bounce paths.  A path's draws come from streams of
+// MC: one path per thread, grid-stride (one tracking walk and one exitance per
+// path).  DDA: persistent lanes refilled path by path, one cell (and its
+// exitance) per iteration, so misses and short walks do not hold a warp.  A path's draws come from streams of
 // its own Philox key: the collision sampler on stream 2, its adjoint on stream
 // 4, exitance evaluation k on stream (k + 1) << 16 (its transmittance on the
 // fork after it), the DDA's per-cell points on the path stream after the
@@ -225,39 +224,6 @@ __device__ void collision_integrate_mc_bw(const DMedium& M, const Rng& rng, floa
     collision_sample_dt_bw(M, cb, x, w, M.ds_eps, dot(dL, eR), dot(dL, env_radiance(M, w)), tl, status);
 }
 
-// include/vr_collision_integrator_DDA.h:1-82: per DDA cell a random point (the
-// path stream), the homogeneous transmittance exp(-dt sigma(point)) and the
-// exitance there.
-__device__ float3 collision_integrate_dda(const DMedium& M, Rng& rng, float3 x, float3 w, Tally& tl,
-                                          uint32_t* status) {
-    DDA q;
-    if (!q.init(M, x, w)) return env_radiance(M, w);
-    q.load_all(M.sigma);
-    float Tr = 1.0f, ct = 0.0f;
-    float3 R = f3(0.0f);
-    long long k = 0;
-    while (ct < q.d - 0.0001f) {
-        if (k >= kStepCap) {
-            raise_status(status, 4);
-            break;
-        }
-        const float nt = gmin(q.d, gmin(q.alpha.x, gmin(q.alpha.y, q.alpha.z)));
-        const float cell_t = mixf(ct, nt, rng.uniform());
-        const float sv = q.interp(q.ialpha(cell_t));
-        const float vt = expf(-(nt - ct) * sv);
-        Rng xr = with_stream(rng, exitance_stream(k));
-        const float3 Le = exitance(M, xr, q.x + w * cell_t, -w, tl, status);
-        R = R + Le * (Tr * (1.0f - vt));
-        Tr *= vt;
-        ++tl.steps;
-        ++tl.lookups;
-        ct = nt;
-        const int axis = q.advance_cell();
-        q.shift_load(M.sigma, axis);
-        ++k;
-    }
-    return R + env_radiance(M, w) * Tr;
-}
 // dL/dsigma of a DDA cell, g, scattered into its 8 corners at the sample point a
 __device__ __forceinline__ void dda_cell_scatter(const DMedium& M, const DDA& q, float3 a, float g, Tally& tl) {
     if (g == 0.0f || !M.sigma.grad) return;
@@ -270,6 +236,26 @@ __device__ __forceinline__ void dda_cell_scatter(const DMedium& M, const DDA& q,
     tl.reds += 8;
 }
 
+// One cell of the DDA collision integrator (vr_collision_integrator_DDA.h:1-82):
+// a random point of the cell (the path stream), the homogeneous transmittance
+// exp(-dt sigma(point)) and the exitance there (stream exitance_stream(k)).
+__device__ __forceinline__ void dda_collision_cell(const DMedium& M, DDA& q, Rng& rng, float3 w, long long k, float& Tr,
+                                                   float& ct, float3& R, Tally& tl, uint32_t* status) {
+    const float nt = gmin(q.d, gmin(q.alpha.x, gmin(q.alpha.y, q.alpha.z)));
+    const float cell_t = mixf(ct, nt, rng.uniform());
+    const float sv = q.interp(q.ialpha(cell_t));
+    const float vt = expf(-(nt - ct) * sv);
+    Rng xr = with_stream(rng, exitance_stream(k));
+    const float3 Le = exitance(M, xr, q.x + w * cell_t, -w, tl, status);
+    R = R + Le * (Tr * (1.0f - vt));
+    Tr *= vt;
+    ++tl.steps;
+    ++tl.lookups;
+    ct = nt;
+    const int axis = q.advance_cell();
+    q.shift_load(M.sigma, axis);
+}
+
 // include/vr_collision_integrator_DDA.h:85-207: the reference walks the cells
 // twice -- for fw_T and the emitted total R, then again from the same cell
 // draws scattering dL/dsigma = dL/dR . (T Le - fw_T env - R_rest) dt into the
@@ -277,51 +263,62 @@ __device__ __forceinline__ void dda_cell_scatter(const DMedium& M, const DDA& q,
 // With R_rest = R - P (P: the emitted part up to and including the cell) the
 // scatter splits into dL/dR . (T Le + P) dt, known on the first walk, and
 // -dL/dR . (fw_T env + R) dt, whose factor is known only at its end: so the
-// first walk evaluates each exitance once with its adjoint and scatters the
-// first part, and a second walk over the same cells and draws -- without the
-// exitances' light rays -- scatters the second.
-__device__ void collision_integrate_dda_bw(const DMedium& M, Rng& rng, float3 x, float3 w, float3 dL, Tally& tl,
-                                           uint32_t* status) {
-    if (dL.x == 0.0f && dL.y == 0.0f && dL.z == 0.0f) return;
-    DDA q;
-    if (!q.init(M, x, w)) return;
-    const Rng before = rng;
-    float Tr = 1.0f, ct = 0.0f;
-    float3 P = f3(0.0f);
-    q.load_all(M.sigma);
-    long long k = 0;
-    while (ct < q.d - 0.0001f) {
-        if (k >= kStepCap) {
-            raise_status(status, 4);
-            return;
-        }
-        const float nt = gmin(q.d, gmin(q.alpha.x, gmin(q.alpha.y, q.alpha.z)));
-        const float cell_t = mixf(ct, nt, rng.uniform());
-        const float3 a = q.ialpha(cell_t);
-        const float sv = q.interp(a);
-        const float dt = nt - ct;
-        const float vt = expf(-dt * sv);
-        const float3 Le = exitance_fw_bw(M, with_stream(rng, exitance_stream(k)), q.x + w * cell_t, -w,
-                                         dL * (Tr * (1.0f - vt)), tl, status);
-        P = P + Le * (Tr * (1.0f - vt));
-        Tr *= vt;
-        dda_cell_scatter(M, q, a, dot(dL, (Le * Tr + P) * dt), tl);
-        ct = nt;
-        const int axis = q.advance_cell();
-        q.shift_load(M.sigma, axis);
-        ++k;
-    }
-    const float G = dot(dL, env_radiance(M, w) * Tr + P);  // fw_T env + R
-    if (G == 0.0f || !M.sigma.grad) return;
-    rng = before;
-    q.reset(M);  // (the second walk reads no corner values: no loads)
-    ct = 0.0f;
-    while (ct < q.d - 0.0001f) {
-        const float nt = gmin(q.d, gmin(q.alpha.x, gmin(q.alpha.y, q.alpha.z)));
-        const float cell_t = mixf(ct, nt, rng.uniform());
-        dda_cell_scatter(M, q, q.ialpha(cell_t), -G * (nt - ct), tl);
-        ct = nt;
-        q.advance_cell();
+// first walk (dda_collision_bw_cell) evaluates each exitance once with its
+// adjoint and scatters the first part, and a second walk over the same cells
+// and draws -- without the exitances' light rays or corner loads -- scatters
+// the second (dda_collision_g_cell).
+__device__ __forceinline__ void dda_collision_bw_cell(const DMedium& M, DDA& q, Rng& rng, float3 w, float3 dL,
+                                                      long long k, float& Tr, float& ct, float3& P, Tally& tl,
+                                                      uint32_t* status) {
+    const float nt = gmin(q.d, gmin(q.alpha.x, gmin(q.alpha.y, q.alpha.z)));
+    const float cell_t = mixf(ct, nt, rng.uniform());
+    const float3 a = q.ialpha(cell_t);
+    const float sv = q.interp(a);
+    const float dt = nt - ct;
+    const float vt = expf(-dt * sv);
+    const float3 Le = exitance_fw_bw(M, with_stream(rng, exitance_stream(k)), q.x + w * cell_t, -w,
+                                     dL * (Tr * (1.0f - vt)), tl, status);
+    P = P + Le * (Tr * (1.0f - vt));
+    Tr *= vt;
+    dda_cell_scatter(M, q, a, dot(dL, (Le * Tr + P) * dt), tl);
+    ct = nt;
+    const int axis = q.advance_cell();
+    q.shift_load(M.sigma, axis);
+}
+__device__ __forceinline__ void dda_collision_g_cell(const DMedium& M, DDA& q, Rng& rng, float G, float& ct,
+                                                     Tally& tl) {
+    const float nt = gmin(q.d, gmin(q.alpha.x, gmin(q.alpha.y, q.alpha.z)));
+    const float cell_t = mixf(ct, nt, rng.uniform());
+    dda_cell_scatter(M, q, q.ialpha(cell_t), -G * (nt - ct), tl);
+    ct = nt;
+    q.advance_cell();
+}
+
+// A lane's next path from the scratch's work counter (one atomic per warp
+// refill); all lanes call it together.
+__device__ __forceinline__ bool take_path(DScratch* sc, bool want_path, uint64_t& p) {
+    const unsigned want = __ballot_sync(0xffffffffu, want_path);
+    if (!want) return false;
+    const unsigned lane = threadIdx.x & 31u;
+    const int leader = __ffs(want) - 1;
+    unsigned long long base = 0;
+    if ((int)lane == leader) base = atomicAdd(&sc->next_path, (unsigned long long)__popc(want));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (!want_path) return false;
+    p = base + __popc(want & ((1u << lane) - 1u));
+    return true;
+}
+
+__device__ __forceinline__ void write_radiance(const PathSrc& S, float* out, float scale, uint64_t pid, float3 R) {
+    const long long o = out_index(S, pid);
+    if (S.is_camera) {
+        atomicAdd(out + 3 * o + 0, R.x * scale);
+        atomicAdd(out + 3 * o + 1, R.y * scale);
+        atomicAdd(out + 3 * o + 2, R.z * scale);
+    } else {
+        out[3 * o + 0] = R.x;
+        out[3 * o + 1] = R.y;
+        out[3 * o + 2] = R.z;
     }
 }
 
@@ -362,19 +359,9 @@ __global__ void __launch_bounds__(256) k_collision_fw(DMedium M, PathSrc S, uint
         rng.init(seed, pid, 0);
         float3 x0, w0;
         start_ray(S, pid, rng, x0, w0, sc);
-        const float3 R = INTEG == VRT_PI_MC_COLLISION ? collision_integrate_mc(M, rng, x0, w0, verts, tl, &sc->status)
-                                                      : collision_integrate_dda(M, rng, x0, w0, tl, &sc->status);
+        const float3 R = collision_integrate_mc(M, rng, x0, w0, verts, tl, &sc->status);
         ++paths;
-        const long long o = out_index(S, pid);
-        if (S.is_camera) {
-            atomicAdd(out + 3 * o + 0, R.x * scale);
-            atomicAdd(out + 3 * o + 1, R.y * scale);
-            atomicAdd(out + 3 * o + 2, R.z * scale);
-        } else {
-            out[3 * o + 0] = R.x;
-            out[3 * o + 1] = R.y;
-            out[3 * o + 2] = R.z;
-        }
+        write_radiance(S, out, scale, pid, R);
     }
     collision_tally(sc, paths, verts, tl);
 }
@@ -392,8 +379,129 @@ __global__ void __launch_bounds__(256) k_collision_bw(DMedium M, PathSrc S, uint
         float3 x0, w0;
         start_ray(S, pid, rng, x0, w0, sc);
         const float3 d = ld3(dL + 3 * out_index(S, pid)) / div;
-        if (INTEG == VRT_PI_MC_COLLISION) collision_integrate_mc_bw(M, rng, x0, w0, d, tl, &sc->status);
-        else collision_integrate_dda_bw(M, rng, x0, w0, d, tl, &sc->status);
+        collision_integrate_mc_bw(M, rng, x0, w0, d, tl, &sc->status);
+    }
+    collision_tally(sc, 0, 0, tl);
+}
+
+// The DDA collision integrator on persistent lanes: a lane takes the next
+// path as soon as its walk ends, one cell (random point, transmittance,
+// exitance and its light ray) per iteration, so misses and short walks do not
+// wait for the warp's longest.  A path's draws and arithmetic are those of the
+// per-path walk, cell for cell.
+__global__ void __launch_bounds__(256) k_collision_dda_fw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
+                                                          float* __restrict__ out, float scale, DScratch* sc) {
+    DDA q;
+    Rng rng;
+    float3 w = f3(0.0f), R = f3(0.0f);
+    float Tr = 1.0f, ct = 0.0f;
+    long long k = 0;
+    uint64_t pid = 0;
+    bool busy = false, exhausted = false;
+    uint32_t paths = 0;
+    Tally tl;
+    while (true) {
+        uint64_t p;
+        if (take_path(sc, !busy && !exhausted, p)) {
+            if (p >= n_paths) {
+                exhausted = true;
+            } else {
+                pid = p;
+                rng.init(seed, pid, 0);
+                float3 x0;
+                start_ray(S, pid, rng, x0, w, sc);
+                ++paths;
+                if (!q.init(M, x0, w)) {
+                    write_radiance(S, out, scale, pid, env_radiance(M, w));
+                } else {
+                    q.load_all(M.sigma);
+                    Tr = 1.0f;
+                    ct = 0.0f;
+                    R = f3(0.0f);
+                    k = 0;
+                    busy = true;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, !busy && exhausted)) break;
+        if (busy) {
+            if (ct < q.d - 0.0001f && k < kStepCap) {
+                dda_collision_cell(M, q, rng, w, k, Tr, ct, R, tl, &sc->status);
+                ++k;
+            } else {
+                if (ct < q.d - 0.0001f) raise_status(&sc->status, 4);
+                write_radiance(S, out, scale, pid, R + env_radiance(M, w) * Tr);
+                busy = false;
+            }
+        }
+    }
+    collision_tally(sc, paths, 0, tl);
+}
+
+// Its adjoint: phase 0 the first walk (exitances and their adjoints), phase 1
+// the second (the total-scaled part of the sigma scatter), from the stream
+// position the first started at.
+__global__ void __launch_bounds__(256) k_collision_dda_bw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
+                                                          const float* __restrict__ dL, float div, DScratch* sc) {
+    DDA q;
+    Rng rng;
+    Rng::Pos before = {0u, 0u};
+    float3 w = f3(0.0f), g = f3(0.0f), P = f3(0.0f);
+    float Tr = 1.0f, ct = 0.0f, G = 0.0f;
+    long long k = 0;
+    int phase = 0;
+    bool busy = false, exhausted = false;
+    Tally tl;
+    while (true) {
+        uint64_t p;
+        if (take_path(sc, !busy && !exhausted, p)) {
+            if (p >= n_paths) {
+                exhausted = true;
+            } else {
+                rng.init(seed, p, 0);
+                float3 x0;
+                start_ray(S, p, rng, x0, w, sc);
+                g = ld3(dL + 3 * out_index(S, p)) / div;
+                if (!(g.x == 0.0f && g.y == 0.0f && g.z == 0.0f) && q.init(M, x0, w)) {
+                    before = rng.pos();
+                    q.load_all(M.sigma);
+                    Tr = 1.0f;
+                    ct = 0.0f;
+                    P = f3(0.0f);
+                    k = 0;
+                    phase = 0;
+                    busy = true;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, !busy && exhausted)) break;
+        if (busy) {
+            if (phase == 0) {
+                if (ct < q.d - 0.0001f) {
+                    if (k >= kStepCap) {
+                        raise_status(&sc->status, 4);
+                        busy = false;
+                    } else {
+                        dda_collision_bw_cell(M, q, rng, w, g, k, Tr, ct, P, tl, &sc->status);
+                        ++k;
+                    }
+                } else {
+                    G = dot(g, env_radiance(M, w) * Tr + P);  // fw_T env + R
+                    if (G == 0.0f || !M.sigma.grad) {
+                        busy = false;
+                    } else {
+                        rng.seek(before);
+                        q.reset(M);  // (the second walk reads no corner values: no loads)
+                        ct = 0.0f;
+                        phase = 1;
+                    }
+                }
+            } else if (ct < q.d - 0.0001f) {
+                dda_collision_g_cell(M, q, rng, G, ct, tl);
+            } else {
+                busy = false;
+            }
+        }
     }
     collision_tally(sc, 0, 0, tl);
 }
@@ -444,16 +552,28 @@ int grid_blocks(uint64_t n, int num_sms) {
     return (int)(b < 1 ? 1 : b);
 }
 
+// persistent grid of the lane kernels, at most one lane per path
+int lane_blocks(const void* kernel, uint64_t n, int num_sms) {
+    int b = persistent_blocks(kernel, 256, num_sms);
+    const uint64_t need = (n + 255) / 256;
+    if ((uint64_t)b > need) b = (int)need;
+    return b < 1 ? 1 : b;
+}
+
 }  // namespace
 
 int launch_collision_fw(const DMedium& M, int integrator, const PathSrc& S, uint64_t n_paths, uint64_t seed,
                         float* out, float scale, DScratch* sc, int num_sms, cudaStream_t stream) {
     if (n_paths == 0) return VRT_OK;
-    const int g = grid_blocks(n_paths, num_sms);
-    if (integrator == VRT_PI_MC_COLLISION)
-        k_collision_fw<VRT_PI_MC_COLLISION><<<g, 256, 0, stream>>>(M, S, n_paths, seed, out, scale, sc);
-    else
-        k_collision_fw<VRT_PI_DDA_COLLISION><<<g, 256, 0, stream>>>(M, S, n_paths, seed, out, scale, sc);
+    if (integrator == VRT_PI_MC_COLLISION) {
+        k_collision_fw<VRT_PI_MC_COLLISION><<<grid_blocks(n_paths, num_sms), 256, 0, stream>>>(M, S, n_paths, seed,
+                                                                                                out, scale, sc);
+    } else {
+        cudaError_t e = cudaMemsetAsync(&sc->next_path, 0, sizeof(unsigned long long), stream);
+        if (e != cudaSuccess) return launch_status(e);
+        k_collision_dda_fw<<<lane_blocks((const void*)k_collision_dda_fw, n_paths, num_sms), 256, 0, stream>>>(
+            M, S, n_paths, seed, out, scale, sc);
+    }
     count_launches(1);
     return launch_status(cudaGetLastError());
 }
@@ -461,11 +581,15 @@ int launch_collision_fw(const DMedium& M, int integrator, const PathSrc& S, uint
 int launch_collision_bw(const DMedium& M, int integrator, const PathSrc& S, uint64_t n_paths, uint64_t seed,
                         const float* dL, float div, DScratch* sc, int num_sms, cudaStream_t stream) {
     if (n_paths == 0) return VRT_OK;
-    const int g = grid_blocks(n_paths, num_sms);
-    if (integrator == VRT_PI_MC_COLLISION)
-        k_collision_bw<VRT_PI_MC_COLLISION><<<g, 256, 0, stream>>>(M, S, n_paths, seed, dL, div, sc);
-    else
-        k_collision_bw<VRT_PI_DDA_COLLISION><<<g, 256, 0, stream>>>(M, S, n_paths, seed, dL, div, sc);
+    if (integrator == VRT_PI_MC_COLLISION) {
+        k_collision_bw<VRT_PI_MC_COLLISION><<<grid_blocks(n_paths, num_sms), 256, 0, stream>>>(M, S, n_paths, seed,
+                                                                                                dL, div, sc);
+    } else {
+        cudaError_t e = cudaMemsetAsync(&sc->next_path, 0, sizeof(unsigned long long), stream);
+        if (e != cudaSuccess) return launch_status(e);
+        k_collision_dda_bw<<<lane_blocks((const void*)k_collision_dda_bw, n_paths, num_sms), 256, 0, stream>>>(
+            M, S, n_paths, seed, dL, div, sc);
+    }
     count_launches(1);
     return launch_status(cudaGetLastError());
 }
