@@ -293,11 +293,21 @@ struct DDA {
         const int m = 1 << axis, far = st > 0 ? m : 0;
         int o[6];
         corner_offsets(g, o);
+        // after a y or z step the face left behind holds two x-neighbour pairs:
+        // one vector atomic each where the nodes are adjacent (red_add2 falls
+        // back to two scalar adds where the pair is not 8-byte aligned)
+        const bool pairs = axis != 0 && g.sW == 1 && o[1] == o[0] + 1;
         float na[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             const bool behind = (k & m) != far;
-            if (behind && acc[k] != 0.0f) red_add(g.grad + (o[4 + (k >> 2)] + o[2 + ((k >> 1) & 1)] + o[k & 1]), acc[k]);
+            float* a = g.grad + (o[4 + (k >> 2)] + o[2 + ((k >> 1) & 1)] + o[k & 1]);
+            if (pairs) {
+                if (behind && (k & 1) == 0 && (acc[k] != 0.0f || acc[(k + 1) & 7] != 0.0f))
+                    red_add2(a, acc[k], acc[(k + 1) & 7]);
+            } else if (behind && acc[k] != 0.0f) {
+                red_add(a, acc[k]);
+            }
             const float v = axis == 0 ? acc[k ^ 1] : (axis == 1 ? acc[k ^ 2] : acc[k ^ 4]);
             na[k] = behind ? v : 0.0f;
         }
