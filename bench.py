@@ -746,13 +746,15 @@ def run_other(args):
         t_bw = t_all - t_fw
         peak = measured_peaks()["hbm_gbs"]
         apeaks = atomic_peaks(dev)
+        gl2 = gather_peaks(dev)["l2"]  # the 64 MB grid is L2-resident: the gather ceiling that applies
         line = {"metric": "rays/s fwd+bwd", "value": wl["n_rays"] / (t_all / 1e3), "unit": "rays/s",
                 "ms_per_step": t_all, "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
                 "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded generators)",
                 "config": {"workload": args.workload, "grid": [256, 256, 256], "rays": wl["n_rays"],
                            "rule": "midpoint (reference)", "l2": "flushed between calls (512 MB write)"},
                 "fw": {"ms": t_fw, "cells_per_ray": cells / wl["n_rays"], "cells_per_s": cells / (t_fw / 1e3),
-                       "gbs": 32.0 * cells / (t_fw / 1e3) / 1e9, "frac": 32.0 * cells / (t_fw / 1e3) / 1e9 / peak},
+                       "gbs": 32.0 * cells / (t_fw / 1e3) / 1e9, "frac": 32.0 * cells / (t_fw / 1e3) / 1e9 / peak,
+                       "l2_gather_peak_gbs": gl2, "frac_of_l2_gather": 32.0 * cells / (t_fw / 1e3) / 1e9 / gl2},
                 "bw": {"ms": t_bw, "reds": reds_bw, "gbs": 4.0 * reds_bw / (t_bw / 1e3) / 1e9,
                        "frac": 4.0 * reds_bw / (t_bw / 1e3) / 1e9 / peak,
                        "adds_per_s_g": reds_bw / (t_bw / 1e3) / 1e9, "atomic_peak_g": apeaks,

@@ -384,6 +384,48 @@ __device__ __forceinline__ void transmittance_dda_bw(const DMedium& M, float3 x,
 // tracked against max - min: ratio tracking multiplies T by 1 - Pc, delta
 // tracking ends the ray (T = 0) at a collision.  Forward only: the
 // reference's maps define no backward.
+// One cell of it: the minorant part in closed form, the residual tracked to
+// the cell's end.  False when the ray ends in the cell (DELTA: a collision,
+// T = 0; or the step cap, error 4).
+template <bool DELTA>
+__device__ __forceinline__ bool grid_tracking_cell(const DMedium& M, DDA& q, Rng& rng, float& T, float& ct, int& it,
+                                                   Tally& tl, uint32_t* status) {
+    const float nt = gmin(q.d, gmin(q.alpha.x, gmin(q.alpha.y, q.alpha.z)));
+    float mx = q.s[0], mn = q.s[0];
+#pragma unroll
+    for (int k = 1; k < 8; ++k) {
+        mx = fmaxf(mx, q.s[k]);
+        mn = fminf(mn, q.s[k]);
+    }
+    ++tl.steps;
+    ++tl.lookups;
+    T *= expf(-mn * (nt - ct));
+    const float rm = gmax(0.000001f, mx - mn);
+    float cell_t = ct;
+    while (true) {
+        if (++it > kStepCap) {
+            raise_status(status, 4);
+            return false;
+        }
+        const float dt = -logf(1.0f - rng.uniform()) / rm;
+        if (cell_t + dt > nt) break;
+        cell_t += dt;
+        const float Pc = (q.interp(q.ialpha(cell_t)) - mn) / rm;
+        ++tl.steps;
+        if (DELTA) {
+            if (rng.uniform() < Pc) {
+                T = 0.0f;
+                return false;
+            }
+        } else {
+            T *= (1.0f - Pc);
+        }
+    }
+    ct = nt;
+    const int axis = q.advance_cell();
+    q.shift_load(M.sigma, axis);
+    return true;
+}
 template <bool DELTA>
 __device__ __forceinline__ float transmittance_grid_tracking(const DMedium& M, Rng& rng, float3 x, float3 w,
                                                              Tally& tl, uint32_t* status) {
@@ -398,37 +440,7 @@ __device__ __forceinline__ float transmittance_grid_tracking(const DMedium& M, R
             raise_status(status, 4);
             return T;
         }
-        const float nt = gmin(q.d, gmin(q.alpha.x, gmin(q.alpha.y, q.alpha.z)));
-        float mx = q.s[0], mn = q.s[0];
-#pragma unroll
-        for (int k = 1; k < 8; ++k) {
-            mx = fmaxf(mx, q.s[k]);
-            mn = fminf(mn, q.s[k]);
-        }
-        ++tl.steps;
-        ++tl.lookups;
-        T *= expf(-mn * (nt - ct));
-        const float rm = gmax(0.000001f, mx - mn);
-        float cell_t = ct;
-        while (true) {
-            if (++it > kStepCap) {
-                raise_status(status, 4);
-                return T;
-            }
-            const float dt = -logf(1.0f - rng.uniform()) / rm;
-            if (cell_t + dt > nt) break;
-            cell_t += dt;
-            const float Pc = (q.interp(q.ialpha(cell_t)) - mn) / rm;
-            ++tl.steps;
-            if (DELTA) {
-                if (rng.uniform() < Pc) return 0.0f;
-            } else {
-                T *= (1.0f - Pc);
-            }
-        }
-        ct = nt;
-        const int axis = q.advance_cell();
-        q.shift_load(M.sigma, axis);
+        if (!grid_tracking_cell<DELTA>(M, q, rng, T, ct, it, tl, status)) return T;
     }
     return T;
 }

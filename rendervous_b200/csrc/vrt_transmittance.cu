@@ -1,7 +1,7 @@
 // vrt_transmittance.cu -- transmittance maps evaluated on rays [n, 6] (sm_100a).
 //
-// One thread per ray (the DDA modes: persistent lanes refilled ray by ray);
-// ray i draws from Philox path id i.  These are the
+// RT / DT / GRT: one thread per ray; DDA, GDT: persistent lanes refilled ray
+// by ray.  Ray i draws from Philox path id i.  These are the
 // operator forms of GridDDATransmittance / RatiotrackingTransmittance /
 // DeltatrackingTransmittance, GridRatiotrackingTransmittance and
 // GridDeltatrackingTransmittance (include/maps/transmittance_{dda,rt,dt,grt,gdt}.h).
@@ -39,15 +39,13 @@ __global__ void __launch_bounds__(256) k_transmittance_fw(DMedium M, const float
         float2 a = __ldg(r2), b = __ldg(r2 + 1), c = __ldg(r2 + 2);
         float3 x = make_float3(a.x, a.y, b.x), w = make_float3(b.y, c.x, c.y);
         float v;
-        if (MODE == 2) v = transmittance_dda<false>(M, x, w, tl);
-        else if (MODE == 3) v = transmittance_dda<true>(M, x, w, tl);
-        else {
+        {
             Rng path;
             path.init(seed, (uint64_t)i, 0);
             Rng rng = path.fork();  // as the dispatch of a path integrator would
             if (MODE == 0) v = transmittance_rt(M, rng, x, w, tl, &sc->status);
             else if (MODE == 1) v = transmittance_dt(M, rng, x, w, tl, &sc->status);
-            else v = transmittance_grid_tracking<MODE == 5>(M, rng, x, w, tl, &sc->status);
+            else v = transmittance_grid_tracking<false>(M, rng, x, w, tl, &sc->status);
         }
         T[i] = v;
         ++count;
@@ -66,9 +64,7 @@ __global__ void __launch_bounds__(256) k_transmittance_bw(DMedium M, const float
         float2 a = __ldg(r2), b = __ldg(r2 + 1), c = __ldg(r2 + 2);
         float3 x = make_float3(a.x, a.y, b.x), w = make_float3(b.y, c.x, c.y);
         float g = __ldg(dL_dT + i);
-        if (MODE == 2) transmittance_dda_bw<false>(M, x, w, g, tl);
-        else if (MODE == 3) transmittance_dda_bw<true>(M, x, w, g, tl);
-        else {
+        {
             Rng path;
             path.init(seed, (uint64_t)i, 0);
             Rng rng = path.fork();
@@ -162,6 +158,64 @@ __global__ void __launch_bounds__(256) k_dda_fw(DMedium M, const float* __restri
     warp_tally(sc, count, tl);
 }
 
+// GridDeltatracking (DELTA) on the same refilled lanes, one cell (its
+// minorant part and its tracking steps) per iteration; ray i draws from fork 0
+// of path i's stream, as transmittance_grid_tracking does.
+template <bool DELTA>
+__global__ void __launch_bounds__(256) k_grid_tracking_fw(DMedium M, const float* __restrict__ rays, int64_t n,
+                                                          uint64_t seed, float* __restrict__ out, DScratch* sc) {
+    DDA q;
+    Rng rng;
+    float T = 1.0f, ct = 0.0f, stop = 0.0f;
+    int it = 0;
+    int64_t ray = -1;
+    bool exhausted = false;
+    uint32_t count = 0;
+    Tally tl;
+    while (true) {
+        int64_t i;
+        if (take_ray(sc, n, ray < 0 && !exhausted, i)) {
+            if (i >= n) {
+                exhausted = true;
+            } else {
+                float3 x, w;
+                load_ray(rays, i, x, w);
+                ++count;
+                if (!q.init(M, x, w)) {
+                    out[i] = 1.0f;  // a miss
+                } else {
+                    Rng path;
+                    path.init(seed, (uint64_t)i, 0);
+                    rng = path.fork();  // as the dispatch of a path integrator would
+                    q.load_all(M.sigma);
+                    T = 1.0f;
+                    ct = 0.0f;
+                    it = 0;
+                    stop = q.d - 0.0001f;
+                    ray = i;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, ray < 0 && exhausted)) break;
+        if (ray >= 0) {
+            bool done = !(ct < stop);
+            if (!done) {
+                if (++it > kStepCap) {
+                    raise_status(&sc->status, 4);
+                    done = true;
+                } else {
+                    done = !grid_tracking_cell<DELTA>(M, q, rng, T, ct, it, tl, &sc->status);
+                }
+            }
+            if (done) {
+                out[ray] = T;
+                ray = -1;
+            }
+        }
+    }
+    warp_tally(sc, count, tl);
+}
+
 // The adjoint's second march (transmittance_dda_bw after its tau): rays with
 // dL/dtau != 0 scatter from the segment's start.
 template <bool EXACT>
@@ -247,12 +301,20 @@ int launch_transmittance_fw(const DMedium& M, int mode, const float* rays, int64
         count_launches(1);
         return launch_status(cudaGetLastError());
     }
+    if (mode == 5) {  // GDT: rays end at their first collision, so lengths vary and refilling pays
+        // (GRT walks every ray to its end: one ray per thread was faster, 8.6 against 9.9 ms)
+        cudaError_t e = cudaMemsetAsync(&scratch->next_path, 0, sizeof(unsigned long long), stream);
+        if (e != cudaSuccess) return launch_status(e);
+        k_grid_tracking_fw<true><<<dda_blocks((const void*)k_grid_tracking_fw<true>, num_sms, n), 256, 0, stream>>>(
+            M, rays, n, seed, T, scratch);
+        count_launches(1);
+        return launch_status(cudaGetLastError());
+    }
     int g = grid_for(n);
     switch (mode) {
         case 0: k_transmittance_fw<0><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
         case 1: k_transmittance_fw<1><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
-        case 4: k_transmittance_fw<4><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
-        default: k_transmittance_fw<5><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
+        default: k_transmittance_fw<4><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
     }
     count_launches(1);
     return launch_status(cudaGetLastError());
