@@ -344,8 +344,8 @@ __device__ __forceinline__ void collision_tally(DScratch* sc, uint32_t paths, ui
     }
 }
 
-template <int INTEG>
-__global__ void __launch_bounds__(256) k_collision_fw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
+// MC collision integrator, one path per thread, grid-stride
+__global__ void __launch_bounds__(256) k_collision_mc_fw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
                                                       float* __restrict__ out, float scale, DScratch* sc) {
     uint32_t paths = 0, verts = 0;
     Tally tl;
@@ -366,8 +366,7 @@ __global__ void __launch_bounds__(256) k_collision_fw(DMedium M, PathSrc S, uint
     collision_tally(sc, paths, verts, tl);
 }
 
-template <int INTEG>
-__global__ void __launch_bounds__(256) k_collision_bw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
+__global__ void __launch_bounds__(256) k_collision_mc_bw(DMedium M, PathSrc S, uint64_t n_paths, uint64_t seed,
                                                       const float* __restrict__ dL, float div, DScratch* sc) {
     Tally tl;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -566,7 +565,7 @@ int launch_collision_fw(const DMedium& M, int integrator, const PathSrc& S, uint
                         float* out, float scale, DScratch* sc, int num_sms, cudaStream_t stream) {
     if (n_paths == 0) return VRT_OK;
     if (integrator == VRT_PI_MC_COLLISION) {
-        k_collision_fw<VRT_PI_MC_COLLISION><<<grid_blocks(n_paths, num_sms), 256, 0, stream>>>(M, S, n_paths, seed,
+        k_collision_mc_fw<<<grid_blocks(n_paths, num_sms), 256, 0, stream>>>(M, S, n_paths, seed,
                                                                                                 out, scale, sc);
     } else {
         cudaError_t e = cudaMemsetAsync(&sc->next_path, 0, sizeof(unsigned long long), stream);
@@ -582,7 +581,7 @@ int launch_collision_bw(const DMedium& M, int integrator, const PathSrc& S, uint
                         const float* dL, float div, DScratch* sc, int num_sms, cudaStream_t stream) {
     if (n_paths == 0) return VRT_OK;
     if (integrator == VRT_PI_MC_COLLISION) {
-        k_collision_bw<VRT_PI_MC_COLLISION><<<grid_blocks(n_paths, num_sms), 256, 0, stream>>>(M, S, n_paths, seed,
+        k_collision_mc_bw<<<grid_blocks(n_paths, num_sms), 256, 0, stream>>>(M, S, n_paths, seed,
                                                                                                 dL, div, sc);
     } else {
         cudaError_t e = cudaMemsetAsync(&sc->next_path, 0, sizeof(unsigned long long), stream);
