@@ -448,6 +448,37 @@ __device__ __forceinline__ float transmittance_grid_tracking(const DMedium& M, R
 // vr_transmittance_RT.h:1-49.  The "grid crossing" branch restarts at a
 // majorant-brick face without a collision; it cannot trigger with the
 // constant majorant (distance 1e6).
+// One iteration of its loop (a brick crossing or a tracking collision): true
+// when the estimate is complete (in T).
+__device__ __forceinline__ bool rt_step(const DMedium& M, Rng& rng, Flight& ff, float3& x, float3 w, float& d,
+                                        float& T, Tally& tl) {
+    float md;
+    float maj = gmax(0.0000001f, ff.bk.query(M, x, w, md));
+    if (ff.tau < 0.0f) ++tl.steps;
+    float t = ff.sample(rng) / maj;
+    if (md < d && t > md) {
+        x = x + w * md;
+        d -= md;
+        ff.cross(maj, md);
+        ff.bk.advance(M);
+        return false;
+    }
+    ff.used();
+    float dt = gmin(t, gmin(d, md));
+    ff.bk.move(dt);
+    x = x + w * dt;
+    d -= dt;
+    if (d <= 0.0000001f) return true;
+    T *= (1.0f - sigma(M, x, tl) / maj);
+    if (T < 0.01f) {
+        if (rng.uniform() < 1.0f - T) {
+            T = 0.0f;
+            return true;
+        }
+        T = 1.0f;
+    }
+    return false;
+}
 __device__ __forceinline__ float transmittance_rt(const DMedium& M, Rng& rng, float3 x, float3 w, Tally& tl,
                                                   uint32_t* status) {
     float T = 1.0f;
@@ -456,24 +487,8 @@ __device__ __forceinline__ float transmittance_rt(const DMedium& M, Rng& rng, fl
     x = x + w * tMin;
     float d = tMax - tMin;
     Flight ff;
-    for (int it = 0; it < kStepCap; ++it) {
-        float md;
-        float maj = gmax(0.0000001f, ff.bk.query(M, x, w, md));
-        if (ff.tau < 0.0f) ++tl.steps;
-        float t = ff.sample(rng) / maj;
-        if (md < d && t > md) { x = x + w * md; d -= md; ff.cross(maj, md); ff.bk.advance(M); continue; }
-        ff.used();
-        float dt = gmin(t, gmin(d, md));
-        ff.bk.move(dt);
-        x = x + w * dt;
-        d -= dt;
-        if (d <= 0.0000001f) return T;
-        T *= (1.0f - sigma(M, x, tl) / maj);
-        if (T < 0.01f) {
-            if (rng.uniform() < 1.0f - T) return 0.0f;
-            T = 1.0f;
-        }
-    }
+    for (int it = 0; it < kStepCap; ++it)
+        if (rt_step(M, rng, ff, x, w, d, T, tl)) return T;
     raise_status(status, 4);
     return T;
 }
@@ -539,6 +554,30 @@ __device__ __forceinline__ void transmittance_rt_bw(const DMedium& M, Rng& rng, 
 }
 
 // vr_transmittance_DT.h:1-28
+// One iteration of its loop: 0 the ray goes on, 1 it left the segment (T = 1),
+// 2 a real collision (T = 0).
+__device__ __forceinline__ int dt_step(const DMedium& M, Rng& rng, Flight& ff, float3& x, float3 w, float& d,
+                                       Tally& tl) {
+    float md;
+    float maj = gmax(0.0000001f, ff.bk.query(M, x, w, md));
+    if (ff.tau < 0.0f) ++tl.steps;
+    float dt = ff.sample(rng) / maj;
+    float t = gmin(md, dt);
+    x = x + w * t;
+    d -= t;
+    // the end test precedes the brick-crossing restart (the reference's
+    // order, which the constant majorant never distinguishes)
+    if (d <= 0.0000001f) return 1;
+    if (dt > md) {
+        ff.cross(maj, md);
+        ff.bk.advance(M);
+        return 0;
+    }
+    ff.used();
+    ff.bk.move(t);
+    if (rng.uniform() < sigma(M, x, tl) / maj) return 2;
+    return 0;
+}
 __device__ __forceinline__ float transmittance_dt(const DMedium& M, Rng& rng, float3 x, float3 w, Tally& tl,
                                                   uint32_t* status) {
     float tMin, tMax;
@@ -547,20 +586,8 @@ __device__ __forceinline__ float transmittance_dt(const DMedium& M, Rng& rng, fl
     float d = tMax - tMin;
     Flight ff;
     for (int it = 0; it < kStepCap; ++it) {
-        float md;
-        float maj = gmax(0.0000001f, ff.bk.query(M, x, w, md));
-        if (ff.tau < 0.0f) ++tl.steps;
-        float dt = ff.sample(rng) / maj;
-        float t = gmin(md, dt);
-        x = x + w * t;
-        d -= t;
-        // the end test precedes the brick-crossing restart (the reference's
-        // order, which the constant majorant never distinguishes)
-        if (d <= 0.0000001f) return 1.0f;
-        if (dt > md) { ff.cross(maj, md); ff.bk.advance(M); continue; }
-        ff.used();
-        ff.bk.move(t);
-        if (rng.uniform() < sigma(M, x, tl) / maj) return 0.0f;
+        const int r = dt_step(M, rng, ff, x, w, d, tl);
+        if (r) return r == 1 ? 1.0f : 0.0f;
     }
     raise_status(status, 4);
     return 1.0f;

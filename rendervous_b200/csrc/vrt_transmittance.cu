@@ -1,7 +1,8 @@
 // vrt_transmittance.cu -- transmittance maps evaluated on rays [n, 6] (sm_100a).
 //
-// RT / DT / GRT: one thread per ray; DDA, GDT: persistent lanes refilled ray
-// by ray.  Ray i draws from Philox path id i.  These are the
+// GRT and the RT / DT adjoints: one thread per ray; the DDA, GDT, RT and DT
+// forwards: persistent lanes refilled ray by ray.  Ray i draws from Philox
+// path id i.  These are the
 // operator forms of GridDDATransmittance / RatiotrackingTransmittance /
 // DeltatrackingTransmittance, GridRatiotrackingTransmittance and
 // GridDeltatrackingTransmittance (include/maps/transmittance_{dda,rt,dt,grt,gdt}.h).
@@ -216,6 +217,76 @@ __global__ void __launch_bounds__(256) k_grid_tracking_fw(DMedium M, const float
     warp_tally(sc, count, tl);
 }
 
+// RatiotrackingTransmittance / DeltatrackingTransmittance (DELTA) on the
+// refilled lanes, at most kTrackSteps tracking steps (crossings or
+// collisions) per lane between refills; ray i draws from fork 0 of path i's
+// stream, as transmittance_rt / _dt do.
+constexpr int kTrackSteps = 4;
+template <bool DELTA>
+__global__ void __launch_bounds__(256) k_track_fw(DMedium M, const float* __restrict__ rays, int64_t n, uint64_t seed,
+                                                  float* __restrict__ out, DScratch* sc) {
+    Flight ff;
+    Rng rng;
+    float3 x = make_float3(0.0f, 0.0f, 0.0f), w = x;
+    float d = 0.0f, T = 1.0f;
+    int it = 0;
+    int64_t ray = -1;
+    bool exhausted = false;
+    uint32_t count = 0;
+    Tally tl;
+    while (true) {
+        int64_t i;
+        if (take_ray(sc, n, ray < 0 && !exhausted, i)) {
+            if (i >= n) {
+                exhausted = true;
+            } else {
+                float3 x0;
+                load_ray(rays, i, x0, w);
+                ++count;
+                float tMin, tMax;
+                if (!boundary(M, x0, w, tMin, tMax)) {
+                    out[i] = 1.0f;  // a miss
+                } else {
+                    Rng path;
+                    path.init(seed, (uint64_t)i, 0);
+                    rng = path.fork();  // as the dispatch of a path integrator would
+                    x = x0 + w * tMin;
+                    d = tMax - tMin;
+                    ff = Flight();
+                    T = 1.0f;
+                    it = 0;
+                    ray = i;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, ray < 0 && exhausted)) break;
+        if (ray >= 0) {
+            for (int c = 0; c < kTrackSteps; ++c) {
+                if (it >= kStepCap) {
+                    raise_status(&sc->status, 4);
+                    out[ray] = DELTA ? 1.0f : T;
+                    ray = -1;
+                    break;
+                }
+                ++it;
+                if (DELTA) {
+                    const int r = dt_step(M, rng, ff, x, w, d, tl);
+                    if (r) {
+                        out[ray] = r == 1 ? 1.0f : 0.0f;
+                        ray = -1;
+                        break;
+                    }
+                } else if (rt_step(M, rng, ff, x, w, d, T, tl)) {
+                    out[ray] = T;
+                    ray = -1;
+                    break;
+                }
+            }
+        }
+    }
+    warp_tally(sc, count, tl);
+}
+
 // The adjoint's second march (transmittance_dda_bw after its tau): rays with
 // dL/dtau != 0 scatter from the segment's start.
 template <bool EXACT>
@@ -310,12 +381,20 @@ int launch_transmittance_fw(const DMedium& M, int mode, const float* rays, int64
         count_launches(1);
         return launch_status(cudaGetLastError());
     }
-    int g = grid_for(n);
-    switch (mode) {
-        case 0: k_transmittance_fw<0><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
-        case 1: k_transmittance_fw<1><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
-        default: k_transmittance_fw<4><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch); break;
+    if (mode == 0 || mode == 1) {
+        cudaError_t e = cudaMemsetAsync(&scratch->next_path, 0, sizeof(unsigned long long), stream);
+        if (e != cudaSuccess) return launch_status(e);
+        if (mode == 0)
+            k_track_fw<false><<<dda_blocks((const void*)k_track_fw<false>, num_sms, n), 256, 0, stream>>>(
+                M, rays, n, seed, T, scratch);
+        else
+            k_track_fw<true><<<dda_blocks((const void*)k_track_fw<true>, num_sms, n), 256, 0, stream>>>(
+                M, rays, n, seed, T, scratch);
+        count_launches(1);
+        return launch_status(cudaGetLastError());
     }
+    int g = grid_for(n);
+    k_transmittance_fw<4><<<g, 256, 0, stream>>>(M, rays, n, seed, T, scratch);
     count_launches(1);
     return launch_status(cudaGetLastError());
 }
